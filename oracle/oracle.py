@@ -1,0 +1,377 @@
+"""CPU ORACLE — test infrastructure only.
+
+Python face of ``liboracle.so`` (plain-C restatement of rust-inla's INLA inner
+path, ``oracle/inla_oracle.c``) plus pure-Python restatements of the small
+theta-level algorithms (Nelder-Mead, finite-difference Hessian, CCD / grid
+designs, weight normalisation). Only ``tests/``, ``__graft_entry__.smoke()``
+and ``bench.py``'s CPU-baseline / ``--impl reference`` leg use this module; the
+product library never calls it.
+
+Parity status: pinned against the reference's own known-answer tests for the
+path (see ``tests/test_oracle.py``) and dense numpy references; the reference
+itself (Rust + faer 0.24) cannot be built here.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import scipy.sparse as sp
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+
+_lib = None
+DP = C.POINTER(C.c_double)
+LP = C.POINTER(C.c_int64)
+
+
+def build(force: bool = False) -> Path:
+    src = [HERE / "inla_oracle.c", HERE / "inla_oracle.h"]
+    if force or not LIB.exists() or any(p.stat().st_mtime > LIB.stat().st_mtime for p in src):
+        subprocess.run(["make", "-C", str(HERE), "-B" if force else "all"], check=True,
+                       stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
+    return LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(str(LIB))
+        sig = {
+            "orc_lower_bandwidth": (C.c_int64, [C.c_int64, LP, LP]),
+            "orc_bandwidth_with_fwd": (C.c_int64, [C.c_int64, LP, LP, LP]),
+            "orc_try_time_major": (C.c_int, [C.c_int64, LP, LP, LP]),
+            "orc_rcm": (None, [C.c_int64, LP, LP, LP]),
+            "orc_choose_order": (C.c_int, [C.c_int64, LP, LP, LP]),
+            "orc_factor_create": (C.c_int, [C.c_int64, LP, LP, DP, LP, C.POINTER(C.c_void_p)]),
+            "orc_factor_free": (None, [C.c_void_p]),
+            "orc_factor_nnz": (C.c_int64, [C.c_void_p]),
+            "orc_logdet": (C.c_double, [C.c_void_p]),
+            "orc_solve": (None, [C.c_void_p, DP, DP]),
+            "orc_takahashi_diag": (C.c_int, [C.c_void_p, DP]),
+            "orc_takahashi_pattern": (C.c_int, [C.c_void_p, LP, LP, DP]),
+            "orc_eval_lik": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, DP, DP, DP]),
+            "orc_log_gamma": (C.c_double, [C.c_double]),
+            "orc_laplace": (C.c_int, [C.c_int64, LP, LP, DP, C.c_int64, LP, LP, DP, C.c_int, DP, DP, DP,
+                                      C.c_int, DP, DP, C.c_int, C.c_double, LP, DP, DP, DP]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _i64(a):
+    return np.ascontiguousarray(a, dtype=np.int64)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _p(a, t=DP):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+def _csc(q):
+    q = sp.csc_matrix(q)
+    q.sort_indices()
+    return q.shape[0], _i64(q.indptr), _i64(q.indices), _f64(q.data)
+
+
+# ---------------------------------------------------------------------------
+# ordering.rs
+# ---------------------------------------------------------------------------
+
+def lower_bandwidth(q) -> int:
+    n, cp, ri, _ = _csc(q)
+    return int(lib().orc_lower_bandwidth(n, _p(cp, LP), _p(ri, LP)))
+
+
+def choose_order(q):
+    """(branch, fwd): 5 time-major, 2 RCM, 1 AMD (fwd None for AMD)."""
+    n, cp, ri, _ = _csc(q)
+    fwd = np.zeros(n, dtype=np.int64)
+    k = int(lib().orc_choose_order(n, _p(cp, LP), _p(ri, LP), _p(fwd, LP)))
+    return k, (fwd if k in (2, 5) else None)
+
+
+def rcm(q):
+    n, cp, ri, _ = _csc(q)
+    fwd = np.zeros(n, dtype=np.int64)
+    lib().orc_rcm(n, _p(cp, LP), _p(ri, LP), _p(fwd, LP))
+    return fwd
+
+
+def default_perm(q):
+    """perm[new] = old from the reference choice (AMD branch -> natural order)."""
+    k, fwd = choose_order(q)
+    n = q.shape[0]
+    if fwd is None:
+        return np.arange(n, dtype=np.int64)
+    perm = np.empty(n, dtype=np.int64)
+    perm[fwd] = np.arange(n)
+    return perm
+
+
+# ---------------------------------------------------------------------------
+# factor
+# ---------------------------------------------------------------------------
+
+class OracleError(RuntimeError):
+    pass
+
+
+class Factor:
+    """Simplicial LDL^T of a full-symmetric CSC (only row >= col entries read)."""
+
+    def __init__(self, q, perm=None):
+        n, cp, ri, v = _csc(q)
+        self.n = n
+        self._q = (cp, ri)
+        h = C.c_void_p()
+        pp = None if perm is None else _i64(perm)
+        rc = lib().orc_factor_create(n, _p(cp, LP), _p(ri, LP), _p(v), _p(pp, LP), C.byref(h))
+        self._h = h
+        self.singular = rc != 0
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().orc_factor_free(self._h)
+            self._h = None
+
+    def nnz(self) -> int:
+        return int(lib().orc_factor_nnz(self._h))
+
+    def logdet(self) -> float:
+        return float(lib().orc_logdet(self._h))
+
+    def solve(self, b) -> np.ndarray:
+        b = _f64(b)
+        x = np.empty(self.n)
+        lib().orc_solve(self._h, _p(b), _p(x))
+        return x
+
+    def diag_inv(self) -> np.ndarray:
+        d = np.empty(self.n)
+        if lib().orc_takahashi_diag(self._h, _p(d)):
+            raise OracleError("Takahashi failed")
+        return d
+
+    def sigma_on_pattern(self, q) -> np.ndarray:
+        n, cp, ri, _ = _csc(q)
+        out = np.empty(len(ri))
+        if lib().orc_takahashi_pattern(self._h, _p(cp, LP), _p(ri, LP), _p(out)):
+            raise OracleError("Takahashi failed")
+        return out
+
+
+# ---------------------------------------------------------------------------
+# likelihoods / Laplace
+# ---------------------------------------------------------------------------
+
+FAMILIES = {"gaussian": 0, "poisson": 1, "binomial": 2, "nbinomial": 3}
+
+
+def eval_lik(family, eta, y, p1=1.0, p2=1.0):
+    lp, g, h = C.c_double(), C.c_double(), C.c_double()
+    rc = lib().orc_eval_lik(FAMILIES.get(family, family), float(eta), float(y), float(p1), float(p2),
+                            C.byref(lp), C.byref(g), C.byref(h))
+    if rc:
+        raise OracleError("likelihood evaluation failed")
+    return lp.value, g.value, h.value
+
+
+def log_gamma(z: float) -> float:
+    return float(lib().orc_log_gamma(float(z)))
+
+
+def laplace(q, a, family, y, p1=None, p2=None, constraints=None, max_iter=200, tol=1e-5, perm=None,
+            want_var=False):
+    """find_latent_mode_a_with_solver (inference.rs:776-975) -> dict."""
+    n, cp, ri, v = _csc(q)
+    y = _f64(y)
+    nobs = len(y)
+    if a is not None:
+        a = sp.csr_matrix(a)
+        a.sort_indices()
+        acp, aci, av = _i64(a.indptr), _i64(a.indices), _f64(a.data)
+    else:
+        acp = aci = av = None
+    p1 = None if p1 is None else _f64(np.broadcast_to(p1, (nobs,)))
+    p2 = None if p2 is None else _f64(np.broadcast_to(p2, (nobs,)))
+    kc = 0
+    ca = ce = None
+    if constraints is not None:
+        ca = _f64(np.atleast_2d(constraints[0]))
+        ce = _f64(constraints[1])
+        kc = ca.shape[0]
+    x = np.zeros(n)
+    out = np.zeros(4)
+    var = np.zeros(n) if want_var else None
+    pp = None if perm is None else _i64(perm)
+    rc = lib().orc_laplace(n, _p(cp, LP), _p(ri, LP), _p(v), nobs, _p(acp, LP), _p(aci, LP), _p(av),
+                           FAMILIES.get(family, family), _p(y), _p(p1), _p(p2), kc, _p(ca), _p(ce),
+                           int(max_iter), float(tol), _p(pp, LP), _p(x), _p(out), _p(var))
+    if rc:
+        raise OracleError(f"laplace failed with code {rc}")
+    return {"x": x, "mlik": out[0], "logdet_prior": out[1], "logdet_post": out[2], "iters": int(out[3]),
+            "var": var}
+
+
+# ---------------------------------------------------------------------------
+# theta-level algorithms (pure Python restatements)
+# ---------------------------------------------------------------------------
+
+def nelder_mead(x0, step, max_iter, tol, f):
+    """inla_math/src/hyper_opt.rs:15-183 (reflect 1, expand 2, contract 0.5, shrink 0.5)."""
+    m = len(x0)
+    verts = [list(map(float, x0))]
+    fv = [f(verts[0])]
+    for i in range(m):
+        v = list(map(float, x0))
+        v[i] += step
+        verts.append(v)
+        fv.append(f(v))
+    for _ in range(max_iter):
+        idx = sorted(range(m + 1), key=lambda k: fv[k])
+        verts = [verts[k] for k in idx]
+        fv = [fv[k] for k in idx]
+        mean = sum(fv) / (m + 1)
+        var = sum((v - mean) ** 2 for v in fv) / (m + 1)
+        if math.sqrt(var) < tol:
+            return verts[0]
+        cen = [sum(verts[i][j] for i in range(m)) / m for j in range(m)]
+        refl = [cen[j] + 1.0 * (cen[j] - verts[m][j]) for j in range(m)]
+        fr = f(refl)
+        if fv[0] <= fr < fv[m - 1]:
+            verts[m], fv[m] = refl, fr
+            continue
+        if fr < fv[0]:
+            exp_ = [cen[j] + 2.0 * (refl[j] - cen[j]) for j in range(m)]
+            fe = f(exp_)
+            if fe < fr:
+                verts[m], fv[m] = exp_, fe
+            else:
+                verts[m], fv[m] = refl, fr
+            continue
+        contract = False
+        if fr < fv[m]:
+            con = [cen[j] + 0.5 * (refl[j] - cen[j]) for j in range(m)]
+            fc = f(con)
+            if fc < fr:
+                verts[m], fv[m] = con, fc
+                contract = True
+        else:
+            con = [cen[j] + 0.5 * (verts[m][j] - cen[j]) for j in range(m)]
+            fc = f(con)
+            if fc < fv[m]:
+                verts[m], fv[m] = con, fc
+                contract = True
+        if contract:
+            continue
+        for i in range(1, m + 1):
+            verts[i] = [verts[0][j] + 0.5 * (verts[i][j] - verts[0][j]) for j in range(m)]
+            fv[i] = f(verts[i])
+    return verts[0]
+
+
+def fd_hessian(mode, f, h):
+    """inla_math/src/hyper_opt.rs:197-259: Hessian of g = -f by central differences."""
+    m = len(mode)
+    H = np.zeros((m, m))
+
+    def g(t):
+        return -f(list(t))
+
+    g0 = g(mode)
+    for i in range(m):
+        for j in range(m):
+            if i == j:
+                tp = list(mode); tp[i] += h
+                tm = list(mode); tm[i] -= h
+                H[i, i] = (g(tp) - 2.0 * g0 + g(tm)) / (h * h)
+            elif i < j:
+                pp = list(mode); pp[i] += h; pp[j] += h
+                pm = list(mode); pm[i] += h; pm[j] -= h
+                mp = list(mode); mp[i] -= h; mp[j] += h
+                mm = list(mode); mm[i] -= h; mm[j] -= h
+                v = (g(pp) - g(pm) - g(mp) + g(mm)) / (4.0 * h * h)
+                H[i, j] = H[j, i] = v
+    return H
+
+
+def fd_gradient(theta, f, h=1e-4):
+    """Central-difference gradient of f with the stencil fd_hessian uses."""
+    m = len(theta)
+    gr = np.zeros(m)
+    for i in range(m):
+        tp = list(theta); tp[i] += h
+        tm = list(theta); tm[i] -= h
+        gr[i] = (f(tp) - f(tm)) / (2.0 * h)
+    return gr
+
+
+def ccd_design(m, f0=1.0):
+    """inla_math/src/integration.rs:1-62."""
+    pts = [[0.0] * m]
+    for i in range(m):
+        p1 = [0.0] * m; p1[i] = f0
+        p2 = [0.0] * m; p2[i] = -f0
+        pts += [p1, p2]
+    if 2 <= m <= 4:
+        val = f0 / math.sqrt(m)
+        for k in range(1 << m):
+            pts.append([(1.0 if (k >> i) & 1 else -1.0) * val for i in range(m)])
+    elif m == 5:
+        val = f0 / math.sqrt(5.0)
+        for k in range(16):
+            p = [0.0] * 5
+            sp_ = 1.0
+            for i in range(4):
+                s = 1.0 if (k >> i) & 1 else -1.0
+                p[i] = s * val
+                sp_ *= s
+            p[4] = sp_ * val
+            pts.append(p)
+    elif m > 5:
+        raise ValueError(f"CCD strategy for m={m} is not supported")
+    ne = len(pts)
+    if ne > 1:
+        w = 1.0 / ((ne - 1) * (1.0 + math.exp(-0.5 * f0 * f0) * (f0 * f0 / m - 1.0)))
+    else:
+        w = 1.0
+    ws = [w] * ne
+    ws[0] = 1.0 - (ne - 1) * w
+    return np.array(pts), np.array(ws)
+
+
+def integrate(mode, hessian, eval_node, f0=1.0):
+    """run_inla_inference_a_cancellable node map + aggregation (inference.rs:1262-1466).
+
+    ``eval_node(theta) -> (x_star, variances, log_post)``.
+    """
+    m = len(mode)
+    sigma = np.linalg.inv(-np.asarray(hessian))
+    lam, V = np.linalg.eigh(sigma)
+    z, w = ccd_design(m, f0)
+    thetas = [np.asarray(mode) + V @ (np.sqrt(np.abs(lam)) * zk) for zk in z]
+    res = [eval_node(t) for t in thetas]
+    lps = np.array([r[2] for r in res])
+    mx = lps.max()
+    dens = np.exp(lps - mx)
+    sw = float(np.sum(w * dens))
+    nw = w * dens / sw
+    means = np.stack([r[0] for r in res])
+    vars_ = np.stack([r[1] for r in res])
+    mean = nw @ means
+    var = nw @ (vars_ + (means - mean) ** 2)
+    return {"thetas": np.array(thetas), "weights": nw, "mean": mean, "var": var, "log_posts": lps,
+            "mlik": mx + math.log(abs(sw))}

@@ -1,0 +1,27 @@
+// Device view of one symbolic analysis (plain pointers into device arrays).
+#pragma once
+#include <cstdint>
+
+namespace inla {
+
+struct DevSym {
+  int n = 0, ns = 0;
+  const int* first = nullptr;      // ns+1
+  const int* rowptr = nullptr;     // ns+1
+  const int* rows = nullptr;       // sum m : permuted row indices
+  const int* relx = nullptr;       // sum m : position of below-row in parent's structure
+  const int64_t* fptr = nullptr;   // ns+1 : front offsets
+  const int64_t* lptr = nullptr;   // ns+1 : panel offsets (compact m*k numbering)
+  const int* child_ptr = nullptr;  // ns+1
+  const int* child_list = nullptr;
+  const int* parent = nullptr;     // ns
+  const int* uoff = nullptr;       // ns+1 : offsets of the per-supernode update vectors (sum r)
+  const int64_t* dpos = nullptr;   // n : front offset of D_j
+  const int* perm = nullptr;       // n : perm[new] = old
+};
+
+constexpr int kStatusOk = 0;
+constexpr int kStatusSingular = 1;
+constexpr int kStatusNotFinite = 2;
+
+}  // namespace inla

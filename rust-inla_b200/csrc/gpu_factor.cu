@@ -1,0 +1,280 @@
+// Host orchestration of the batched supernodal kernels.
+#include <algorithm>
+#include <cstring>
+
+#include "gpu_factor.hpp"
+#include "snode_kernels.cuh"
+
+namespace inla {
+
+namespace {
+inline int cdiv(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+template <class K>
+void set_smem(K kernel, int bytes) {
+  INLA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+}
+}  // namespace
+
+GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
+    : sym_(sym), max_batch_(max_batch), stream_(stream) {
+  if (max_batch < 1) throw std::runtime_error("max_batch must be >= 1");
+  const Symbolic& S = sym_;
+  const int64_t ns = S.nsuper, n = S.n;
+  nnz_ = (int64_t)S.rowidx.size();
+  if (n >= (1LL << 31) || (int64_t)S.sn_rows.size() >= (1LL << 31) || nnz_ >= (1LL << 31))
+    throw std::runtime_error("problem too large for 32-bit indices");
+
+  std::vector<int> first(ns + 1), rowptr(ns + 1), rows(S.sn_rows.size()), relx(S.sn_rows.size(), -1),
+      child_ptr(ns + 1), child_list(S.child_list.size()), parent(ns), uoff(ns + 1, 0), perm(n);
+  std::vector<int64_t> fptr(ns + 1, 0), lptr(ns + 1), dpos(n);
+  for (int64_t s = 0; s <= ns; ++s) {
+    first[s] = (int)S.sn_first[s];
+    rowptr[s] = (int)S.sn_rowptr[s];
+    child_ptr[s] = (int)S.child_ptr[s];
+    lptr[s] = S.sn_lptr[s];
+  }
+  for (size_t i = 0; i < S.sn_rows.size(); ++i) rows[i] = (int)S.sn_rows[i];
+  for (size_t i = 0; i < S.child_list.size(); ++i) child_list[i] = (int)S.child_list[i];
+  for (int64_t s = 0; s < ns; ++s) {
+    int64_t k = S.sn_first[s + 1] - S.sn_first[s], m = S.sn_rowptr[s + 1] - S.sn_rowptr[s];
+    parent[s] = (int)S.sn_parent[s];
+    fptr[s + 1] = fptr[s] + m * m;
+    uoff[s + 1] = uoff[s] + (int)(m - k);
+    for (int64_t t = 0; t < m - k; ++t) relx[S.sn_rowptr[s] + k + t] = S.rel[S.rel_ptr[s] + t];
+    for (int64_t j = S.sn_first[s]; j < S.sn_first[s + 1]; ++j) {
+      int64_t c = j - S.sn_first[s];
+      dpos[j] = fptr[s] + c * (m + 1);
+    }
+  }
+  for (int64_t j = 0; j < n; ++j) perm[j] = (int)S.perm[j];
+  ftotal_ = fptr[ns];
+  usum_ = uoff[ns];
+
+  // panel map (compact panel index -> input entry) and front positions of input entries
+  std::vector<int> pmap(S.nnz_l_stored, -1);
+  std::vector<int64_t> spos(nnz_, -1);
+  for (int64_t c = 0; c < n; ++c)
+    for (int64_t p = S.colptr[c]; p < S.colptr[c + 1]; ++p) {
+      int64_t q = S.qmap[p];
+      if (q < 0) continue;
+      pmap[q] = (int)p;
+      int64_t i = S.iperm[S.rowidx[p]], j = S.iperm[c];
+      int64_t jj = std::min(i, j);
+      int64_t s = S.col_to_sn[jj];
+      spos[p] = fptr[s] + (q - S.sn_lptr[s]);
+    }
+
+  d_first_.upload(first, stream_);
+  d_rowptr_.upload(rowptr, stream_);
+  d_rows_.upload(rows, stream_);
+  d_relx_.upload(relx, stream_);
+  d_child_ptr_.upload(child_ptr, stream_);
+  d_child_list_.upload(child_list, stream_);
+  d_parent_.upload(parent, stream_);
+  d_uoff_.upload(uoff, stream_);
+  d_perm_.upload(perm, stream_);
+  d_fptr_.upload(fptr, stream_);
+  d_lptr_.upload(lptr, stream_);
+  d_dpos_.upload(dpos, stream_);
+  d_pmap_.upload(pmap, stream_);
+  spos_.upload(spos, stream_);
+
+  ds_.n = (int)n;
+  ds_.ns = (int)ns;
+  ds_.first = d_first_.p;
+  ds_.rowptr = d_rowptr_.p;
+  ds_.rows = d_rows_.p;
+  ds_.relx = d_relx_.p;
+  ds_.fptr = d_fptr_.p;
+  ds_.lptr = d_lptr_.p;
+  ds_.child_ptr = d_child_ptr_.p;
+  ds_.child_list = d_child_list_.p;
+  ds_.parent = d_parent_.p;
+  ds_.uoff = d_uoff_.p;
+  ds_.dpos = d_dpos_.p;
+  ds_.perm = d_perm_.p;
+
+  plan_levels();
+
+  F_.alloc((size_t)max_batch_ * ftotal_);
+  xp_.alloc((size_t)max_batch_ * n);
+  ub_.alloc((size_t)max_batch_ * std::max<int64_t>(usum_, 1));
+  logdet_.alloc(max_batch_);
+  status_.alloc(max_batch_);
+
+  set_smem(k_factor_small<128>, kSmallA * kSmallA * 8);
+  set_smem(k_factor_small<256>, kSmallB * kSmallB * 8);
+  set_smem(k_selinv_small<256>, (kSiSmall * kSiSmall * 2) * 8);
+  INLA_CUDA(cudaStreamSynchronize(stream_));
+}
+
+GpuFactor::~GpuFactor() = default;
+
+void GpuFactor::plan_levels() {
+  const Symbolic& S = sym_;
+  levels_.assign(S.nlevels, LevelPlan());
+  std::vector<int> flat;
+  for (int32_t l = 0; l < S.nlevels; ++l) {
+    LevelPlan& P = levels_[l];
+    for (int64_t t = S.level_ptr[l]; t < S.level_ptr[l + 1]; ++t) {
+      int s = (int)S.level_list[t];
+      int k = (int)(S.sn_first[s + 1] - S.sn_first[s]);
+      int m = (int)(S.sn_rowptr[s + 1] - S.sn_rowptr[s]);
+      P.all.push_back(s);
+      P.mmax_all = std::max(P.mmax_all, m);
+      if (m <= kSmallA) {
+        P.small_a.push_back(s);
+        P.mmax_a = std::max(P.mmax_a, m);
+      } else if (m <= kSmallB) {
+        P.small_b.push_back(s);
+        P.mmax_b = std::max(P.mmax_b, m);
+      } else {
+        P.large.push_back(s);
+        P.kmax_large = std::max(P.kmax_large, k);
+        P.mmax_large = std::max(P.mmax_large, m);
+      }
+      if (m <= kSiSmall) {
+        P.si_small.push_back(s);
+        P.mmax_si_small = std::max(P.mmax_si_small, m);
+      } else {
+        P.si_large.push_back(s);
+        P.kmax_si_large = std::max(P.kmax_si_large, k);
+        P.mmax_si_large = std::max(P.mmax_si_large, m);
+        P.rmax_si_large = std::max(P.rmax_si_large, m - k);
+      }
+    }
+    auto put = [&](const std::vector<int>& v) {
+      int off = (int)flat.size();
+      flat.insert(flat.end(), v.begin(), v.end());
+      return off;
+    };
+    P.off_small_a = put(P.small_a);
+    P.off_small_b = put(P.small_b);
+    P.off_large = put(P.large);
+    P.off_all = put(P.all);
+    P.off_si_small = put(P.si_small);
+    P.off_si_large = put(P.si_large);
+  }
+  d_lists_.upload(flat, stream_);
+}
+
+void GpuFactor::run_factor_levels(int B) {
+  const int64_t fs = ftotal_;
+  for (const LevelPlan& P : levels_) {
+    if (!P.small_a.empty()) {
+      dim3 g((unsigned)P.small_a.size(), B);
+      k_factor_small<128><<<g, 128, P.mmax_a * P.mmax_a * 8, stream_>>>(ds_, d_lists_.p + P.off_small_a, F_.p, fs);
+      ++launches_;
+    }
+    if (!P.small_b.empty()) {
+      dim3 g((unsigned)P.small_b.size(), B);
+      k_factor_small<256><<<g, 256, P.mmax_b * P.mmax_b * 8, stream_>>>(ds_, d_lists_.p + P.off_small_b, F_.p, fs);
+      ++launches_;
+    }
+    if (!P.large.empty()) {
+      const int nl = (int)P.large.size();
+      const int* lst = d_lists_.p + P.off_large;
+      k_gather_large<<<dim3(nl, B, cdiv(P.mmax_large, kGatherCW)), 128, 0, stream_>>>(ds_, lst, F_.p, fs);
+      ++launches_;
+      for (int j0 = 0; j0 < P.kmax_large; j0 += kNB) {
+        k_diag_large<<<dim3(nl, B), 128, 0, stream_>>>(ds_, lst, j0, F_.p, fs);
+        int rows = P.mmax_large - j0;
+        k_trsm_large<<<dim3(nl, B, cdiv(rows, kTrsmRows)), kTrsmRows, 0, stream_>>>(ds_, lst, j0, F_.p, fs);
+        int nt = cdiv(rows, kUT);
+        k_update_large<<<dim3(nl, B, nt * (nt + 1) / 2), 128, 0, stream_>>>(ds_, lst, j0, F_.p, fs);
+        launches_ += 3;
+      }
+    }
+  }
+  k_logdet<256><<<B, 256, 0, stream_>>>(ds_, F_.p, fs, logdet_.p, status_.p);
+  ++launches_;
+}
+
+void GpuFactor::factor_values(const double* d_vals, int B) {
+  if (B < 1 || B > max_batch_) throw std::runtime_error("batch size out of range");
+  k_fill_panels<<<dim3((unsigned)sym_.nsuper, B), 128, 0, stream_>>>(ds_, d_pmap_.p, d_vals, nnz_, F_.p, ftotal_);
+  ++launches_;
+  run_factor_levels(B);
+  INLA_CUDA(cudaGetLastError());
+}
+
+void GpuFactor::factor_model(int ncomp, const double* d_comp, const double* d_coef, const int* d_cptr,
+                             const int* d_cobs, const double* d_cprod, const double* d_w, int64_t wstride, int B) {
+  if (B < 1 || B > max_batch_) throw std::runtime_error("batch size out of range");
+  k_fill_panels_model<<<dim3((unsigned)sym_.nsuper, B), 128, 0, stream_>>>(
+      ds_, d_pmap_.p, ncomp, d_comp, nnz_, d_coef, d_cptr, d_cobs, d_cprod, d_w, wstride, F_.p, ftotal_);
+  ++launches_;
+  run_factor_levels(B);
+  INLA_CUDA(cudaGetLastError());
+}
+
+void GpuFactor::solve(double* d_x, int64_t xstride, int B) {
+  if (B < 1 || B > max_batch_) throw std::runtime_error("batch size out of range");
+  const int n = (int)sym_.n;
+  const int64_t fs = ftotal_;
+  dim3 gp(cdiv(n, 256) > 1024 ? 1024 : cdiv(n, 256), B);
+  k_permute_in<<<gp, 256, 0, stream_>>>(n, d_perm_.p, d_x, xstride, xp_.p);
+  ++launches_;
+  for (const LevelPlan& P : levels_) {
+    k_fwd<128><<<dim3((unsigned)P.all.size(), B), 128, P.mmax_all * 8, stream_>>>(
+        ds_, d_lists_.p + P.off_all, F_.p, fs, xp_.p, ub_.p, std::max<int64_t>(usum_, 1));
+    ++launches_;
+  }
+  for (int l = (int)levels_.size() - 1; l >= 0; --l) {
+    const LevelPlan& P = levels_[l];
+    k_bwd<128><<<dim3((unsigned)P.all.size(), B), 128, P.mmax_all * 8, stream_>>>(ds_, d_lists_.p + P.off_all,
+                                                                                  F_.p, fs, xp_.p);
+    ++launches_;
+  }
+  k_permute_out<<<gp, 256, 0, stream_>>>(n, d_perm_.p, xp_.p, d_x, xstride);
+  ++launches_;
+  INLA_CUDA(cudaGetLastError());
+}
+
+void GpuFactor::selinv(int B) {
+  if (B < 1 || B > max_batch_) throw std::runtime_error("batch size out of range");
+  Sg_.alloc((size_t)max_batch_ * ftotal_);
+  const int64_t fs = ftotal_;
+  for (int l = (int)levels_.size() - 1; l >= 0; --l) {
+    const LevelPlan& P = levels_[l];
+    if (!P.si_small.empty()) {
+      int mm = P.mmax_si_small;
+      k_selinv_small<256><<<dim3((unsigned)P.si_small.size(), B), 256, (mm * mm * 2) * 8, stream_>>>(
+          ds_, d_lists_.p + P.off_si_small, F_.p, Sg_.p, fs);
+      ++launches_;
+    }
+    if (!P.si_large.empty()) {
+      const int nl = (int)P.si_large.size();
+      const int* lst = d_lists_.p + P.off_si_large;
+      if (P.rmax_si_large > 0) {
+        k_si_gather_large<<<dim3(nl, B, cdiv(P.rmax_si_large, kGatherCW)), 128, 0, stream_>>>(ds_, lst, Sg_.p, fs);
+        ++launches_;
+      }
+      int nblk = cdiv(P.kmax_si_large, kNB);
+      for (int jb = 0; jb < nblk; ++jb) {
+        k_si_panel_large<<<dim3(nl, B, cdiv(P.mmax_si_large, kSiRows)), kSiRows, 0, stream_>>>(ds_, lst, jb, F_.p,
+                                                                                              Sg_.p, fs);
+        k_si_diag_large<<<dim3(nl, B), 256, 0, stream_>>>(ds_, lst, jb, F_.p, Sg_.p, fs);
+        launches_ += 2;
+      }
+    }
+  }
+  INLA_CUDA(cudaGetLastError());
+}
+
+void GpuFactor::extract_diag(double* d_out, int64_t ostride, int B) {
+  const int n = (int)sym_.n;
+  k_extract_diag<<<dim3(std::min(cdiv(n, 256), 1024), B), 256, 0, stream_>>>(ds_, Sg_.p, ftotal_, d_out, ostride);
+  ++launches_;
+  INLA_CUDA(cudaGetLastError());
+}
+
+void GpuFactor::sigma_on_pattern(double* d_out, int B) {
+  k_pattern_values<<<dim3(std::min(cdiv(nnz_, 256), 2048), B), 256, 0, stream_>>>(nnz_, spos_.p, Sg_.p, ftotal_,
+                                                                                  d_out);
+  ++launches_;
+  INLA_CUDA(cudaGetLastError());
+}
+
+}  // namespace inla

@@ -1,0 +1,123 @@
+// Device-resident numeric engine for one symbolic analysis: batched
+// multifrontal LDL^T, log-determinants, solves and selected inversion.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "devsym.hpp"
+#include "symbolic.hpp"
+
+namespace inla {
+
+struct CudaError : std::runtime_error {
+  int code;
+  CudaError(const std::string& s, int c) : std::runtime_error(s), code(c) {}
+};
+
+#define INLA_CUDA(call)                                                                    \
+  do {                                                                                     \
+    cudaError_t _e = (call);                                                               \
+    if (_e != cudaSuccess)                                                                 \
+      throw ::inla::CudaError(std::string(#call) + ": " + cudaGetErrorString(_e), (int)_e); \
+  } while (0)
+
+// Small RAII device buffer.
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    if (count <= n && p) return;
+    release();
+    if (count == 0) count = 1;
+    INLA_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    n = count;
+  }
+  void upload(const T* h, size_t count, cudaStream_t st = 0) {
+    alloc(count);
+    if (count) INLA_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, st));
+  }
+  void upload(const std::vector<T>& v, cudaStream_t st = 0) { upload(v.data(), v.size(), st); }
+};
+
+struct LevelPlan {
+  std::vector<int> small_a, small_b, large, all;  // host copies (supernode ids)
+  int off_small_a = 0, off_small_b = 0, off_large = 0, off_all = 0;  // offsets into one device list
+  int mmax_a = 0, mmax_b = 0, mmax_all = 0, kmax_large = 0, mmax_large = 0;
+  // selected inversion grouping
+  std::vector<int> si_small, si_large;
+  int off_si_small = 0, off_si_large = 0, mmax_si_small = 0, kmax_si_large = 0, mmax_si_large = 0, rmax_si_large = 0;
+};
+
+class GpuFactor {
+ public:
+  // Size classes (rows of the front): <= kSmallA uses 128 threads, <= kSmallB 256
+  // threads, larger fronts use the blocked multi-CTA kernels.
+  static constexpr int kSmallA = 64;
+  static constexpr int kSmallB = 128;
+  static constexpr int kSiSmall = 96;
+
+  GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream);
+  ~GpuFactor();
+
+  const Symbolic& sym() const { return sym_; }
+  int max_batch() const { return max_batch_; }
+  cudaStream_t stream() const { return stream_; }
+  int64_t front_total() const { return ftotal_; }
+  int64_t nnz() const { return nnz_; }
+
+  // Factorize B problems whose full-CSC values (input pattern order) are at
+  // d_vals [B][nnz] on the device. Results stay resident.
+  void factor_values(const double* d_vals, int B);
+  // Factorize from the component model (see k_fill_panels_model).
+  void factor_model(int ncomp, const double* d_comp, const double* d_coef, const int* d_cptr,
+                    const int* d_cobs, const double* d_cprod, const double* d_w, int64_t wstride, int B);
+  // log|Q_b| and status words (after factor_*) -> device arrays of length B.
+  const double* d_logdet() const { return logdet_.p; }
+  const int* d_status() const { return status_.p; }
+  // Solve Q_b x = rhs_b in place; d_x is [B][xstride] in original order.
+  void solve(double* d_x, int64_t xstride, int B);
+  // Selected inverse on the filled pattern; then extract diag / pattern values.
+  void selinv(int B);
+  void extract_diag(double* d_out, int64_t ostride, int B);
+  void sigma_on_pattern(double* d_out, int B);  // [B][nnz], lower entries, upper = 0
+  const int64_t* d_spos() const { return spos_.p; }
+  double* d_front() { return F_.p; }
+  double* d_sigma() { return Sg_.p; }
+
+  // Launch counters (kernels issued by this engine since construction).
+  int64_t launches() const { return launches_; }
+
+ private:
+  void plan_levels();
+  void run_factor_levels(int B);
+
+  Symbolic sym_;
+  int max_batch_;
+  cudaStream_t stream_;
+  int64_t ftotal_ = 0, nnz_ = 0, usum_ = 0;
+  DevSym ds_;
+  std::vector<LevelPlan> levels_;
+  DBuf<int> d_first_, d_rowptr_, d_rows_, d_relx_, d_child_ptr_, d_child_list_, d_parent_, d_uoff_, d_perm_;
+  DBuf<int64_t> d_fptr_, d_lptr_, d_dpos_, spos_;
+  DBuf<int> d_pmap_, d_lists_;
+  DBuf<double> F_, Sg_, xp_, ub_, logdet_;
+  DBuf<int> status_;
+  int64_t launches_ = 0;
+};
+
+}  // namespace inla

@@ -1,0 +1,660 @@
+// CUDA kernels (sm_100a, FP64) for the multifrontal supernodal LDL^T, its
+// triangular solves, the log-determinant and the supernodal Takahashi
+// selected inverse.
+//
+// Storage ("front layout"): supernode s owns a dense m_s x m_s column-major
+// block at offset fptr[s] inside one buffer per problem. Its first k_s
+// columns are the L panel (unit-lower L below the diagonal, D on the
+// diagonal); the trailing r_s x r_s lower block holds the Schur-complement
+// update that the parent pulls (factorization), or Sigma restricted to the
+// supernode's below-rows (selected inversion). Children are always
+// assembled by the parent in a fixed order (deterministic, no atomics).
+//
+// Reference recurrences being computed:
+//   LDL^T without pivoting, D gate |D| < 1e-14 or non-finite => Singular
+//       (crates/inla_math/src/sparse_ldlt.rs:104-149)
+//   log|Q| = sum log|D_i|            (crates/inla_math/src/ldlt.rs:65-67)
+//   Takahashi: S_ij = -sum_{l>j} L_lj S_li (i>j), S_jj = 1/D_j - sum_{l>j} L_lj S_lj
+//                                      (crates/inla_math/src/sparse_ldlt.rs:366-432)
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "devsym.hpp"
+
+namespace inla {
+
+__device__ __forceinline__ int sn_k(const DevSym& S, int s) { return S.first[s + 1] - S.first[s]; }
+__device__ __forceinline__ int sn_m(const DevSym& S, int s) { return S.rowptr[s + 1] - S.rowptr[s]; }
+
+// ---------------------------------------------------------------------------
+// value fill: every panel entry written exactly once (value or zero)
+// ---------------------------------------------------------------------------
+
+// vals: [B][nnz] full-CSC values; pmap: compact panel index -> input entry or -1.
+__global__ void k_fill_panels(DevSym S, const int* __restrict__ pmap, const double* __restrict__ vals,
+                              int64_t vstride, double* __restrict__ F, int64_t fstride) {
+  const int s = blockIdx.x, b = blockIdx.y;
+  const int k = sn_k(S, s), m = sn_m(S, s);
+  const int64_t mk = (int64_t)m * k;
+  const int* pm = pmap + S.lptr[s];
+  const double* v = vals + (int64_t)b * vstride;
+  double* Fs = F + (int64_t)b * fstride + S.fptr[s];
+  for (int64_t e = threadIdx.x; e < mk; e += blockDim.x) {
+    int src = pm[e];
+    Fs[e] = src >= 0 ? v[src] : 0.0;
+  }
+}
+
+// Component model: value(p) = sum_t coef[b][t] * comp[t][p] + sum_q w[b][obs_q] * prod_q
+// over the observation contributions of entry p (A^T diag(w) A on the pattern).
+__global__ void k_fill_panels_model(DevSym S, const int* __restrict__ pmap, int ncomp,
+                                    const double* __restrict__ comp, int64_t nnz,
+                                    const double* __restrict__ coef,
+                                    const int* __restrict__ cptr, const int* __restrict__ cobs,
+                                    const double* __restrict__ cprod, const double* __restrict__ w,
+                                    int64_t wstride, double* __restrict__ F, int64_t fstride) {
+  const int s = blockIdx.x, b = blockIdx.y;
+  const int k = sn_k(S, s), m = sn_m(S, s);
+  const int64_t mk = (int64_t)m * k;
+  const int* pm = pmap + S.lptr[s];
+  const double* cb = coef + (int64_t)b * ncomp;
+  const double* wb = w ? w + (int64_t)b * wstride : nullptr;
+  double* Fs = F + (int64_t)b * fstride + S.fptr[s];
+  for (int64_t e = threadIdx.x; e < mk; e += blockDim.x) {
+    int src = pm[e];
+    double v = 0.0;
+    if (src >= 0) {
+      for (int t = 0; t < ncomp; ++t) v += cb[t] * comp[(int64_t)t * nnz + src];
+      if (wb) {
+        double acc = 0.0;
+        for (int q = cptr[src]; q < cptr[src + 1]; ++q) acc += wb[cobs[q]] * cprod[q];
+        v += acc;
+      }
+    }
+    Fs[e] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// small fronts: whole front in shared memory, one CTA per (supernode, problem)
+// ---------------------------------------------------------------------------
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_factor_small(DevSym S, const int* __restrict__ list,
+                                                     double* __restrict__ F, int64_t fstride) {
+  extern __shared__ double sm[];
+  const int s = list[blockIdx.x];
+  const int b = blockIdx.y;
+  double* Fb = F + (int64_t)b * fstride;
+  const int k = sn_k(S, s), m = sn_m(S, s);
+  double* Fs = Fb + S.fptr[s];
+  const int mm = m * m;
+  for (int e = threadIdx.x; e < mm; e += NT) {
+    int col = e / m;
+    sm[e] = col < k ? Fs[e] : 0.0;
+  }
+  __syncthreads();
+  for (int q = S.child_ptr[s]; q < S.child_ptr[s + 1]; ++q) {
+    const int c = S.child_list[q];
+    const int kc = sn_k(S, c), mc = sn_m(S, c), rc = mc - kc;
+    const double* Uc = Fb + S.fptr[c] + (int64_t)kc * mc + kc;
+    const int* relc = S.relx + S.rowptr[c] + kc;
+    const int rr = rc * rc;
+    for (int e = threadIdx.x; e < rr; e += NT) {
+      int jj = e / rc, ii = e - jj * rc;
+      if (ii >= jj) sm[relc[ii] + relc[jj] * m] += Uc[ii + (int64_t)jj * mc];
+    }
+    __syncthreads();
+  }
+  for (int j = 0; j < k; ++j) {
+    const double dinv = 1.0 / sm[j + j * m];
+    const int w = m - j - 1;
+    const int ww = w * w;
+    const double* colj = sm + j * m + j + 1;
+    for (int e = threadIdx.x; e < ww; e += NT) {
+      int tt = e / w, ii = e - tt * w;
+      if (ii >= tt) sm[(j + 1 + ii) + (j + 1 + tt) * m] -= colj[ii] * colj[tt] * dinv;
+    }
+    __syncthreads();
+    for (int i = j + 1 + threadIdx.x; i < m; i += NT) sm[i + j * m] *= dinv;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < mm; e += NT) {
+    int col = e / m, row = e - col * m;
+    if (col < k || row >= col) Fs[e] = sm[e];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// large fronts: blocked right-looking partial LDL^T in global memory
+// ---------------------------------------------------------------------------
+
+constexpr int kNB = 32;       // block-column width
+constexpr int kGatherCW = 32; // parent columns per gather CTA
+
+// Zero the update part of columns [c0,c1) and pull every child's update into
+// those columns (children in fixed order; targets unique within one child).
+__global__ void k_gather_large(DevSym S, const int* __restrict__ list, double* __restrict__ F,
+                               int64_t fstride) {
+  const int s = list[blockIdx.x], b = blockIdx.y;
+  const int k = sn_k(S, s), m = sn_m(S, s);
+  const int c0 = blockIdx.z * kGatherCW;
+  if (c0 >= m) return;
+  const int c1 = min(c0 + kGatherCW, m);
+  double* Fb = F + (int64_t)b * fstride;
+  double* Fs = Fb + S.fptr[s];
+  for (int col = max(c0, k); col < c1; ++col)
+    for (int row = col + threadIdx.x; row < m; row += blockDim.x) Fs[row + (int64_t)col * m] = 0.0;
+  __syncthreads();
+  for (int q = S.child_ptr[s]; q < S.child_ptr[s + 1]; ++q) {
+    const int c = S.child_list[q];
+    const int kc = sn_k(S, c), mc = sn_m(S, c), rc = mc - kc;
+    const double* Uc = Fb + S.fptr[c] + (int64_t)kc * mc + kc;
+    const int* relc = S.relx + S.rowptr[c] + kc;
+    // source columns whose target column lies in [c0,c1): relc is increasing
+    int lo = 0, hi = rc;
+    {
+      int a = 0, z = rc;
+      while (a < z) { int mid = (a + z) >> 1; if (relc[mid] < c0) a = mid + 1; else z = mid; }
+      lo = a;
+      a = lo; z = rc;
+      while (a < z) { int mid = (a + z) >> 1; if (relc[mid] < c1) a = mid + 1; else z = mid; }
+      hi = a;
+    }
+    for (int jj = lo; jj < hi; ++jj) {
+      const int tj = relc[jj];
+      for (int ii = jj + threadIdx.x; ii < rc; ii += blockDim.x)
+        Fs[relc[ii] + (int64_t)tj * m] += Uc[ii + (int64_t)jj * mc];
+    }
+    __syncthreads();
+  }
+}
+
+// Unblocked LDL^T of the diagonal block [j0, j0+w) of every listed front.
+__global__ void k_diag_large(DevSym S, const int* __restrict__ list, int j0, double* __restrict__ F,
+                             int64_t fstride) {
+  __shared__ double sm[kNB * kNB];
+  const int s = list[blockIdx.x], b = blockIdx.y;
+  const int k = sn_k(S, s), m = sn_m(S, s);
+  if (j0 >= k) return;
+  const int w = min(kNB, k - j0);
+  double* Fs = F + (int64_t)b * fstride + S.fptr[s];
+  double* D0 = Fs + j0 + (int64_t)j0 * m;
+  for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+    int c = e / w, r = e - c * w;
+    sm[r + c * kNB] = D0[r + (int64_t)c * m];
+  }
+  __syncthreads();
+  for (int j = 0; j < w; ++j) {
+    const double dinv = 1.0 / sm[j + j * kNB];
+    const int ww = w - j - 1;
+    for (int e = threadIdx.x; e < ww * ww; e += blockDim.x) {
+      int tt = e / ww, ii = e - tt * ww;
+      if (ii >= tt) sm[(j + 1 + ii) + (j + 1 + tt) * kNB] -= sm[j + 1 + ii + j * kNB] * sm[j + 1 + tt + j * kNB] * dinv;
+    }
+    __syncthreads();
+    for (int i = j + 1 + threadIdx.x; i < w; i += blockDim.x) sm[i + j * kNB] *= dinv;
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+    int c = e / w, r = e - c * w;
+    if (r >= c) D0[r + (int64_t)c * m] = sm[r + c * kNB];
+  }
+}
+
+// Rows below the diagonal block: L_i = F_i L11^-T D^-1 (one thread per row).
+constexpr int kTrsmRows = 128;
+__global__ void __launch_bounds__(kTrsmRows) k_trsm_large(DevSym S, const int* __restrict__ list, int j0,
+                                                          double* __restrict__ F, int64_t fstride) {
+  __shared__ double dl[kNB * kNB];  // dl[t*kNB+u] = d_u * L_tu (u < t)
+  __shared__ double dinv[kNB];
+  const int s = list[blockIdx.x], b = blockIdx.y;
+  const int k = sn_k(S, s), m = sn_m(S, s);
+  if (j0 >= k) return;
+  const int w = min(kNB, k - j0);
+  const int r0 = j0 + w + blockIdx.z * kTrsmRows;
+  if (r0 >= m) return;
+  double* Fs = F + (int64_t)b * fstride + S.fptr[s];
+  const double* D0 = Fs + j0 + (int64_t)j0 * m;
+  for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+    int t = e / w, u = e - t * w;
+    dl[t * kNB + u] = (u < t) ? D0[u + (int64_t)u * m] * D0[t + (int64_t)u * m] : 0.0;
+  }
+  for (int t = threadIdx.x; t < w; t += blockDim.x) dinv[t] = 1.0 / D0[t + (int64_t)t * m];
+  __syncthreads();
+  const int i = r0 + threadIdx.x;
+  if (i >= m) return;
+  double x[kNB];
+  double* Fi = Fs + i + (int64_t)j0 * m;
+#pragma unroll
+  for (int t = 0; t < kNB; ++t) {
+    if (t < w) {
+      double y = Fi[(int64_t)t * m];
+#pragma unroll
+      for (int u = 0; u < kNB; ++u)
+        if (u < t) y -= x[u] * dl[t * kNB + u];
+      x[t] = y * dinv[t];
+      Fi[(int64_t)t * m] = x[t];
+    }
+  }
+}
+
+// Trailing update F[i,j] -= sum_t L[i,t] d_t L[j,t] over the block [j0,j0+w),
+// for the lower triangle of the trailing region [c, m), 64x64 tiles, FP64
+// tensor-core tiles (mma.sync m8n8k4).
+constexpr int kUT = 64;
+__device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(128) k_update_large(DevSym S, const int* __restrict__ list, int j0,
+                                                     double* __restrict__ F, int64_t fstride) {
+  __shared__ double As[kNB][kUT + 1];  // As[t][i] = L[I0+i, j0+t]
+  __shared__ double Bs[kNB][kUT + 1];  // Bs[t][j] = d_t L[J0+j, j0+t]
+  const int s = list[blockIdx.x], b = blockIdx.y;
+  const int k = sn_k(S, s), m = sn_m(S, s);
+  if (j0 >= k) return;
+  const int w = min(kNB, k - j0);
+  const int c = j0 + w;
+  const int T = m - c;
+  if (T <= 0) return;
+  const int nt = (T + kUT - 1) / kUT;
+  const int tile = blockIdx.z;
+  if (tile >= nt * (nt + 1) / 2) return;
+  // tile -> (I,J), I >= J, column-major over the lower triangle of tiles
+  int J = 0, rem = tile;
+  while (rem >= nt - J) { rem -= nt - J; ++J; }
+  const int I = J + rem;
+  const int I0 = c + I * kUT, J0 = c + J * kUT;
+  double* Fs = F + (int64_t)b * fstride + S.fptr[s];
+  const double* Lb = Fs + (int64_t)j0 * m;
+  for (int e = threadIdx.x; e < kNB * kUT; e += blockDim.x) {
+    int t = e / kUT, i = e - t * kUT;
+    double a = 0.0, bb = 0.0;
+    if (t < w) {
+      if (I0 + i < m) a = Lb[I0 + i + (int64_t)t * m];
+      if (J0 + i < m) bb = Lb[J0 + i + (int64_t)t * m] * Lb[j0 + t + (int64_t)t * m];
+    }
+    As[t][i] = a;
+    Bs[t][i] = bb;
+  }
+  __syncthreads();
+  // 4 warps, each a 32x32 quadrant made of 4x4 mma tiles of 8x8
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wi = (warp & 1) * 32, wj = (warp >> 1) * 32;
+  const int g = lane >> 2, tg = lane & 3;
+  double acc[4][4][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int bq = 0; bq < 4; ++bq) acc[a][bq][0] = acc[a][bq][1] = 0.0;
+#pragma unroll
+  for (int t0 = 0; t0 < kNB; t0 += 4) {
+    double af[4], bf[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) af[a] = As[t0 + tg][wi + a * 8 + g];
+#pragma unroll
+    for (int bq = 0; bq < 4; ++bq) bf[bq] = Bs[t0 + tg][wj + bq * 8 + g];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int bq = 0; bq < 4; ++bq) dmma_8x8x4(acc[a][bq][0], acc[a][bq][1], af[a], bf[bq]);
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int bq = 0; bq < 4; ++bq)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int i = I0 + wi + a * 8 + g;
+        const int j = J0 + wj + bq * 8 + tg * 2 + h;
+        if (i < m && j < m && i >= j) Fs[i + (int64_t)j * m] -= acc[a][bq][h];
+      }
+}
+
+// ---------------------------------------------------------------------------
+// log-determinant + singularity gate (one CTA per problem, fixed reduction tree)
+// ---------------------------------------------------------------------------
+template <int NT>
+__global__ void __launch_bounds__(NT) k_logdet(DevSym S, const double* __restrict__ F, int64_t fstride,
+                                               double* __restrict__ logdet, int* __restrict__ status) {
+  __shared__ double red[NT];
+  __shared__ int bad[NT];
+  const int b = blockIdx.x;
+  const double* Fb = F + (int64_t)b * fstride;
+  double acc = 0.0;
+  int flag = 0;
+  for (int j = threadIdx.x; j < S.n; j += NT) {
+    double d = Fb[S.dpos[j]];
+    double ad = fabs(d);
+    if (!isfinite(d)) flag |= kStatusNotFinite;
+    else if (ad < 1e-14) flag |= kStatusSingular;
+    acc += log(ad);
+  }
+  red[threadIdx.x] = acc;
+  bad[threadIdx.x] = flag;
+  __syncthreads();
+  for (int o = NT / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      red[threadIdx.x] += red[threadIdx.x + o];
+      bad[threadIdx.x] |= bad[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    logdet[b] = red[0];
+    status[b] = bad[0];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// triangular solves: forward (bottom-up levels) then backward (top-down)
+// xp: [B][n] permuted working vector; ub: [B][sum r] child update vectors
+// ---------------------------------------------------------------------------
+
+__global__ void k_permute_in(int n, const int* __restrict__ perm, const double* __restrict__ x,
+                             int64_t xstride, double* __restrict__ xp) {
+  const int b = blockIdx.y;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    xp[(int64_t)b * n + j] = x[(int64_t)b * xstride + perm[j]];
+}
+__global__ void k_permute_out(int n, const int* __restrict__ perm, const double* __restrict__ xp,
+                              double* __restrict__ x, int64_t xstride) {
+  const int b = blockIdx.y;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    x[(int64_t)b * xstride + perm[j]] = xp[(int64_t)b * n + j];
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_fwd(DevSym S, const int* __restrict__ list, const double* __restrict__ F,
+                                            int64_t fstride, double* __restrict__ xp, double* __restrict__ ub,
+                                            int64_t ustride) {
+  extern __shared__ double y[];
+  const int s = list[blockIdx.x], b = blockIdx.y;
+  const int k = sn_k(S, s), m = sn_m(S, s), f = S.first[s];
+  const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
+  double* xb = xp + (int64_t)b * S.n;
+  double* ubb = ub + (int64_t)b * ustride;
+  for (int t = threadIdx.x; t < m; t += NT) y[t] = t < k ? xb[f + t] : 0.0;
+  __syncthreads();
+  for (int q = S.child_ptr[s]; q < S.child_ptr[s + 1]; ++q) {
+    const int c = S.child_list[q];
+    const int kc = sn_k(S, c), rc = sn_m(S, c) - kc;
+    const int* relc = S.relx + S.rowptr[c] + kc;
+    const double* uc = ubb + S.uoff[c];
+    for (int t = threadIdx.x; t < rc; t += NT) y[relc[t]] += uc[t];
+    __syncthreads();
+  }
+  for (int j = 0; j < k; ++j) {
+    const double yj = y[j];
+    const double* Lj = Fs + (int64_t)j * m;
+    for (int i = j + 1 + threadIdx.x; i < m; i += NT) y[i] -= Lj[i] * yj;
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < m; t += NT) {
+    if (t < k) xb[f + t] = y[t] / Fs[t + (int64_t)t * m];
+    else ubb[S.uoff[s] + t - k] = y[t];
+  }
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_bwd(DevSym S, const int* __restrict__ list, const double* __restrict__ F,
+                                            int64_t fstride, double* __restrict__ xp) {
+  extern __shared__ double x[];
+  const int s = list[blockIdx.x], b = blockIdx.y;
+  const int k = sn_k(S, s), m = sn_m(S, s), f = S.first[s];
+  const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
+  double* xb = xp + (int64_t)b * S.n;
+  const int* R = S.rows + S.rowptr[s];
+  for (int t = threadIdx.x; t < m; t += NT) x[t] = xb[R[t]];
+  __syncthreads();
+  // x_j -= sum_{i>=k} L_ij x_i for j < k (one warp per column)
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int j = warp; j < k; j += NT / 32) {
+    const double* Lj = Fs + (int64_t)j * m;
+    double acc = 0.0;
+    for (int i = k + lane; i < m; i += 32) acc += Lj[i] * x[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) x[j] -= acc;
+  }
+  __syncthreads();
+  for (int i = k - 1; i > 0; --i) {
+    const double xi = x[i];
+    for (int j = threadIdx.x; j < i; j += NT) x[j] -= Fs[i + (int64_t)j * m] * xi;
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < k; t += NT) xb[f + t] = x[t];
+}
+
+// ---------------------------------------------------------------------------
+// selected inverse (supernodal Takahashi), top-down levels
+// L: factored fronts; Sg: Sigma fronts (same layout)
+// ---------------------------------------------------------------------------
+
+// Gather Sigma restricted to the below-rows of s from the parent's Sigma front.
+__device__ __forceinline__ double parent_sigma(const double* Sp, int mp, int pi, int pj) {
+  return pi >= pj ? Sp[pi + (int64_t)pj * mp] : Sp[pj + (int64_t)pi * mp];
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_selinv_small(DevSym S, const int* __restrict__ list,
+                                                     const double* __restrict__ F, double* __restrict__ Sg,
+                                                     int64_t fstride) {
+  extern __shared__ double smem[];
+  const int s = list[blockIdx.x], b = blockIdx.y;
+  const int k = sn_k(S, s), m = sn_m(S, s), r = m - k;
+  double* sig = smem;           // m*m, lower used
+  double* Lp = smem + m * m;    // m*k panel
+  __shared__ double red[NT / 32];
+  const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
+  double* Ss = Sg + (int64_t)b * fstride + S.fptr[s];
+  for (int e = threadIdx.x; e < m * k; e += NT) Lp[e] = Fs[e];
+  if (r > 0) {
+    const int p = S.parent[s];
+    const int mp = sn_m(S, p);
+    const double* Sp = Sg + (int64_t)b * fstride + S.fptr[p];
+    const int* rel = S.relx + S.rowptr[s] + k;
+    for (int e = threadIdx.x; e < r * r; e += NT) {
+      int jj = e / r, ii = e - jj * r;
+      if (ii >= jj) sig[(k + ii) + (k + jj) * m] = parent_sigma(Sp, mp, rel[ii], rel[jj]);
+    }
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int j = k - 1; j >= 0; --j) {
+    const double* Lj = Lp + j * m;
+    for (int i = j + 1 + threadIdx.x; i < m; i += NT) {
+      double acc = 0.0;
+      for (int l = j + 1; l < m; ++l) {
+        double sv = l >= i ? sig[l + i * m] : sig[i + l * m];
+        acc += Lj[l] * sv;
+      }
+      sig[i + j * m] = -acc;
+    }
+    __syncthreads();
+    double acc = 0.0;
+    for (int l = j + 1 + threadIdx.x; l < m; l += NT) acc += Lj[l] * sig[l + j * m];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) red[warp] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < NT / 32; ++w) t += red[w];
+      sig[j + j * m] = 1.0 / Lj[j] - t;
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < m * m; e += NT) {
+    int col = e / m, row = e - col * m;
+    if (row >= col) Ss[e] = sig[e];
+  }
+}
+
+// Large fronts: gather Sigma_RR from the parent into the trailing block.
+__global__ void k_si_gather_large(DevSym S, const int* __restrict__ list, double* __restrict__ Sg,
+                                  int64_t fstride) {
+  const int s = list[blockIdx.x], b = blockIdx.y;
+  const int k = sn_k(S, s), m = sn_m(S, s), r = m - k;
+  if (r == 0) return;
+  const int c0 = blockIdx.z * kGatherCW;
+  if (c0 >= r) return;
+  const int c1 = min(c0 + kGatherCW, r);
+  const int p = S.parent[s];
+  const int mp = sn_m(S, p);
+  const double* Sp = Sg + (int64_t)b * fstride + S.fptr[p];
+  double* Ss = Sg + (int64_t)b * fstride + S.fptr[s];
+  const int* rel = S.relx + S.rowptr[s] + k;
+  for (int jj = c0; jj < c1; ++jj)
+    for (int ii = jj + threadIdx.x; ii < r; ii += blockDim.x)
+      Ss[(k + ii) + (int64_t)(k + jj) * m] = parent_sigma(Sp, mp, rel[ii], rel[jj]);
+}
+
+// Block J = [j0, j1): for rows i in A = [j1, m):
+//   G[i,j] = sum_{l in A} Sigma[i,l] L[l,j];  X = -G L_JJ^{-1};  Sigma[i,j] = X[i,j]
+constexpr int kSiRows = 64;
+__global__ void __launch_bounds__(kSiRows) k_si_panel_large(DevSym S, const int* __restrict__ list, int jb,
+                                                            const double* __restrict__ F, double* __restrict__ Sg,
+                                                            int64_t fstride) {
+  __shared__ double Lt[kNB][kNB + 1];   // L[j0+u, j0+t]
+  __shared__ double Ls[32][kNB + 1];    // chunk of L[A, J]
+  __shared__ double Sc[32][kSiRows + 1];  // chunk of Sigma[rows, l]
+  const int s = list[blockIdx.x], b = blockIdx.y;
+  const int k = sn_k(S, s), m = sn_m(S, s);
+  const int nblk = (k + kNB - 1) / kNB;
+  if (jb >= nblk) return;
+  const int bi = nblk - 1 - jb;  // right-to-left
+  const int j0 = bi * kNB, j1 = min(k, j0 + kNB), w = j1 - j0;
+  const int r0 = j1 + blockIdx.z * kSiRows;
+  if (r0 >= m) return;
+  const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
+  double* Ss = Sg + (int64_t)b * fstride + S.fptr[s];
+  for (int e = threadIdx.x; e < kNB * kNB; e += kSiRows) {
+    int t = e / kNB, u = e - t * kNB;
+    Lt[u][t] = (u < w && t < w) ? Fs[(j0 + u) + (int64_t)(j0 + t) * m] : 0.0;
+  }
+  const int i = r0 + threadIdx.x;
+  double g[kNB];
+#pragma unroll
+  for (int t = 0; t < kNB; ++t) g[t] = 0.0;
+  for (int l0 = j1; l0 < m; l0 += 32) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < 32 * kNB; e += kSiRows) {
+      int t = e / 32, l = e - t * 32;
+      Ls[l][t] = (l0 + l < m && t < w) ? Fs[(l0 + l) + (int64_t)(j0 + t) * m] : 0.0;
+    }
+    for (int e = threadIdx.x; e < 32 * kSiRows; e += kSiRows) {
+      int l = e / kSiRows, ii = e - l * kSiRows;
+      int row = r0 + ii, col = l0 + l;
+      double v = 0.0;
+      if (row < m && col < m) v = row >= col ? Ss[row + (int64_t)col * m] : Ss[col + (int64_t)row * m];
+      Sc[l][ii] = v;
+    }
+    __syncthreads();
+    const int lmax = min(32, m - l0);
+    for (int l = 0; l < lmax; ++l) {
+      const double sv = Sc[l][threadIdx.x];
+#pragma unroll
+      for (int t = 0; t < kNB; ++t) g[t] += sv * Ls[l][t];
+    }
+  }
+  if (i >= m) return;
+  // X L_JJ = -G  (unit lower L_JJ), solved right-to-left
+  double x[kNB];
+#pragma unroll
+  for (int t = kNB - 1; t >= 0; --t) {
+    if (t < w) {
+      double v = -g[t];
+#pragma unroll
+      for (int u = kNB - 1; u > 0; --u)
+        if (u > t && u < w) v -= x[u] * Lt[u][t];
+      x[t] = v;
+    } else {
+      x[t] = 0.0;
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < kNB; ++t)
+    if (t < w) Ss[i + (int64_t)(j0 + t) * m] = x[t];
+}
+
+// Diagonal block of J: P[j,i] = sum_{l in A} L[l,j] Sigma[l,i]; then the
+// in-block recurrence right-to-left.
+__global__ void __launch_bounds__(256) k_si_diag_large(DevSym S, const int* __restrict__ list, int jb,
+                                                       const double* __restrict__ F, double* __restrict__ Sg,
+                                                       int64_t fstride) {
+  __shared__ double P[kNB][kNB + 1];
+  __shared__ double Sd[kNB][kNB + 1];
+  __shared__ double Ld[kNB][kNB + 1];
+  const int s = list[blockIdx.x], b = blockIdx.y;
+  const int k = sn_k(S, s), m = sn_m(S, s);
+  const int nblk = (k + kNB - 1) / kNB;
+  if (jb >= nblk) return;
+  const int bi = nblk - 1 - jb;
+  const int j0 = bi * kNB, j1 = min(k, j0 + kNB), w = j1 - j0;
+  const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
+  double* Ss = Sg + (int64_t)b * fstride + S.fptr[s];
+  // P: warp per (j,i) pair set, lanes over l
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int pr = warp; pr < w * w; pr += 8) {
+    int jj = pr / w, ii = pr - jj * w;
+    double acc = 0.0;
+    if (ii >= jj) {
+      const double* Lc = Fs + (int64_t)(j0 + jj) * m;
+      const double* Sc = Ss + (int64_t)(j0 + ii) * m;
+      for (int l = j1 + lane; l < m; l += 32) acc += Lc[l] * Sc[l];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) P[jj][ii] = acc;
+  }
+  for (int e = threadIdx.x; e < w * w; e += 256) {
+    int c = e / w, rr = e - c * w;
+    Ld[rr][c] = Fs[(j0 + rr) + (int64_t)(j0 + c) * m];
+  }
+  __syncthreads();
+  for (int j = w - 1; j >= 0; --j) {
+    // S_ij for i in (j, w): -sum_{l in J, l>j} L_lj S_li - P[j][i]
+    for (int i = j + 1 + threadIdx.x; i < w; i += 256) {
+      double acc = P[j][i];
+      for (int l = j + 1; l < w; ++l) acc += Ld[l][j] * (l >= i ? Sd[l][i] : Sd[i][l]);
+      Sd[i][j] = -acc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double acc = P[j][j];
+      for (int l = j + 1; l < w; ++l) acc += Ld[l][j] * Sd[l][j];
+      Sd[j][j] = 1.0 / Ld[j][j] - acc;
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < w * w; e += 256) {
+    int c = e / w, rr = e - c * w;
+    if (rr >= c) Ss[(j0 + rr) + (int64_t)(j0 + c) * m] = Sd[rr][c];
+  }
+}
+
+// diag(Q^-1) in original order
+__global__ void k_extract_diag(DevSym S, const double* __restrict__ Sg, int64_t fstride, double* __restrict__ out,
+                               int64_t ostride) {
+  const int b = blockIdx.y;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < S.n; j += gridDim.x * blockDim.x)
+    out[(int64_t)b * ostride + S.perm[j]] = Sg[(int64_t)b * fstride + S.dpos[j]];
+}
+
+// Sigma (or L) values back on the lower entries of the input pattern:
+// out[b][p] = buf[b][spos[p]] for lower entries, 0 for upper entries.
+__global__ void k_pattern_values(int64_t nnz, const int64_t* __restrict__ spos, const double* __restrict__ buf,
+                                 int64_t fstride, double* __restrict__ out) {
+  const int b = blockIdx.y;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < nnz; p += (int64_t)gridDim.x * blockDim.x) {
+    int64_t q = spos[p];
+    out[(int64_t)b * nnz + p] = q >= 0 ? buf[(int64_t)b * fstride + q] : 0.0;
+  }
+}
+
+}  // namespace inla

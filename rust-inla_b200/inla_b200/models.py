@@ -1,0 +1,316 @@
+"""Seeded synthetic inputs for the INLA hot path (input side of the Laplace loop).
+
+Each latent precision is written as a linear combination of fixed-pattern
+component matrices, ``Q(theta) = sum_t c_t(theta) * M_t``, so that every
+theta-point, Newton iterate and batched problem shares one symbolic analysis
+and the device only refreshes values.
+
+Reference behaviour restated here (inputs only; none of this is timed):
+
+* SPDE precision ``tau^2 (kappa^4 C~ + 2 kappa^2 G + G C~^-1 G)`` —
+  crates/inla_stats/src/spde.rs:70-140.
+* P1 FEM blocks: lumped mass ``C~_ii = sum area/3`` and stiffness
+  ``G_ij = e_i . e_j / (4 area)`` — crates/inla_fmesher/src/fmesher.rs:544-626.
+* Barycentric projector rows, weights with ``|w| <= 1e-15`` dropped —
+  crates/inla_fmesher/src/fmesher.rs:175-219, 822-831.
+* Besag graph Laplacian — crates/inla_stats/src/besag.rs:127-152.
+* AR1 conditional-precision form ``tau * tridiag(1, 1+rho^2, ..., 1; -rho)`` —
+  crates/inla_stats/src/ar1.rs:9-69.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+GEOM_EPSILON = 1e-15
+SEED_BASE = 20261203
+
+
+# ---------------------------------------------------------------------------
+# meshes and FEM
+# ---------------------------------------------------------------------------
+
+def grid_mesh(nx: int, rng: np.random.Generator, jitter: float = 0.2):
+    """Structured triangulation of the unit square from an ``nx x nx`` vertex grid.
+
+    Interior vertices are jittered by ``U(+-jitter*h)`` per axis (x draws first,
+    then y), boundary vertices stay on the boundary. Every cell is split on the
+    same diagonal; triangles are counter-clockwise.
+    """
+    h = 1.0 / (nx - 1)
+    gx, gy = np.meshgrid(np.arange(nx) * h, np.arange(nx) * h, indexing="xy")
+    vx = gx.ravel().copy()
+    vy = gy.ravel().copy()
+    ii = np.arange(nx * nx) % nx
+    jj = np.arange(nx * nx) // nx
+    interior = (ii > 0) & (ii < nx - 1) & (jj > 0) & (jj < nx - 1)
+    k = int(interior.sum())
+    dx = rng.uniform(-jitter * h, jitter * h, size=k)
+    dy = rng.uniform(-jitter * h, jitter * h, size=k)
+    vx[interior] += dx
+    vy[interior] += dy
+    c = np.arange((nx - 1) * (nx - 1))
+    ci = c % (nx - 1)
+    cj = c // (nx - 1)
+    v00 = cj * nx + ci
+    v10 = v00 + 1
+    v01 = v00 + nx
+    v11 = v01 + 1
+    t1 = np.stack([v00, v10, v11], axis=1)
+    t2 = np.stack([v00, v11, v01], axis=1)
+    tris = np.empty((2 * len(c), 3), dtype=np.int64)
+    tris[0::2] = t1
+    tris[1::2] = t2
+    verts = np.stack([vx, vy], axis=1)
+    return verts, tris
+
+
+def fem_matrices(verts: np.ndarray, tris: np.ndarray):
+    """Lumped mass diagonal ``c0`` and stiffness ``G`` (CSC) of P1 elements."""
+    nv = len(verts)
+    s0, s1, s2 = verts[tris[:, 0]], verts[tris[:, 1]], verts[tris[:, 2]]
+    e0 = s2 - s1
+    e1 = s0 - s2
+    e2 = s1 - s0
+    area2 = (s1[:, 0] - s0[:, 0]) * (s2[:, 1] - s0[:, 1]) - (s1[:, 1] - s0[:, 1]) * (s2[:, 0] - s0[:, 0])
+    area = 0.5 * np.abs(area2)
+    fa = 0.5 * np.abs(e0[:, 0] * e1[:, 1] - e0[:, 1] * e1[:, 0])
+    fa = np.where(fa <= GEOM_EPSILON, area, fa)
+    e = [e0, e1, e2]
+    c0 = np.zeros(nv)
+    for i in range(3):
+        np.add.at(c0, tris[:, i], area / 3.0)
+    rows, cols, vals = [], [], []
+    for i in range(3):
+        for j in range(3):
+            eij = e[i][:, 0] * e[j][:, 0] + e[i][:, 1] * e[j][:, 1]
+            rows.append(tris[:, i])
+            cols.append(tris[:, j])
+            vals.append(eij / (4.0 * fa))
+    g = sp.coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                      shape=(nv, nv)).tocsc()
+    g.sum_duplicates()
+    g.sort_indices()
+    return c0, g
+
+
+def _signed_area2(ax, ay, bx, by, cx, cy):
+    return (bx - ax) * (cy - ay) - (by - ay) * (cx - ax)
+
+
+def grid_projector(verts: np.ndarray, tris: np.ndarray, nx: int, pts: np.ndarray) -> sp.csr_matrix:
+    """Barycentric projector for points inside the jittered grid mesh.
+
+    Any triangle containing the point gives the same non-zero weights; the
+    candidate triangles are those of the 3x3 cells around the point's
+    unjittered cell.
+    """
+    h = 1.0 / (nx - 1)
+    nc = nx - 1
+    n = len(pts)
+    ci0 = np.clip((pts[:, 0] / h).astype(np.int64), 0, nc - 1)
+    cj0 = np.clip((pts[:, 1] / h).astype(np.int64), 0, nc - 1)
+    found = np.zeros(n, dtype=bool)
+    wts = np.zeros((n, 3))
+    tv = np.zeros((n, 3), dtype=np.int64)
+    for dj in (0, -1, 1):
+        for di in (0, -1, 1):
+            ci = np.clip(ci0 + di, 0, nc - 1)
+            cj = np.clip(cj0 + dj, 0, nc - 1)
+            for half in (0, 1):
+                t = 2 * (cj * nc + ci) + half
+                a, b, c = verts[tris[t, 0]], verts[tris[t, 1]], verts[tris[t, 2]]
+                den = _signed_area2(a[:, 0], a[:, 1], b[:, 0], b[:, 1], c[:, 0], c[:, 1])
+                w0 = _signed_area2(b[:, 0], b[:, 1], c[:, 0], c[:, 1], pts[:, 0], pts[:, 1]) / den
+                w1 = _signed_area2(c[:, 0], c[:, 1], a[:, 0], a[:, 1], pts[:, 0], pts[:, 1]) / den
+                w2 = 1.0 - w0 - w1
+                inside = (w0 >= -GEOM_EPSILON) & (w1 >= -GEOM_EPSILON) & (w2 >= -GEOM_EPSILON)
+                take = inside & ~found
+                wts[take] = np.stack([w0, w1, w2], axis=1)[take]
+                tv[take] = tris[t][take]
+                found |= take
+    if not found.all():
+        raise ValueError("observation point outside the mesh")
+    rows = np.repeat(np.arange(n), 3)
+    w = wts.ravel()
+    keep = np.abs(w) > GEOM_EPSILON
+    a = sp.coo_matrix((w[keep], (rows[keep], tv.ravel()[keep])), shape=(n, len(verts))).tocsr()
+    a.sum_duplicates()
+    a.sort_indices()
+    return a
+
+
+# ---------------------------------------------------------------------------
+# component model container
+# ---------------------------------------------------------------------------
+
+@dataclass
+class LatentModel:
+    """``Q(theta) = sum_t coef_t(theta) * comps[t]`` on one shared pattern.
+
+    ``pattern`` is the full symmetric CSC pattern (both triangles, sorted
+    indices, diagonal present) that every component is expressed on, and
+    ``comp_values[t]`` holds component ``t``'s values on that pattern.
+    """
+
+    n: int
+    pattern: sp.csc_matrix
+    comp_values: np.ndarray  # (T, nnz)
+    kind: str
+    info: dict = field(default_factory=dict)
+
+    @property
+    def n_comp(self) -> int:
+        return self.comp_values.shape[0]
+
+    def values(self, coefs) -> np.ndarray:
+        return np.asarray(coefs, dtype=np.float64) @ self.comp_values
+
+    def matrix(self, coefs) -> sp.csc_matrix:
+        q = self.pattern.copy()
+        q.data = self.values(coefs)
+        return q
+
+
+def _on_pattern(pattern: sp.csc_matrix, m: sp.spmatrix) -> np.ndarray:
+    """Values of ``m`` on ``pattern`` (zero where ``m`` has no entry)."""
+    m = sp.csc_matrix(m)
+    m.sum_duplicates()
+    pc = pattern.tocoo()
+    key_p = pc.col.astype(np.int64) * pattern.shape[0] + pc.row
+    mc = m.tocoo()
+    key_m = mc.col.astype(np.int64) * pattern.shape[0] + mc.row
+    order = np.argsort(key_m)
+    key_m = key_m[order]
+    vals = mc.data[order]
+    pos = np.searchsorted(key_m, key_p)
+    pos = np.clip(pos, 0, max(len(key_m) - 1, 0))
+    out = np.zeros(len(key_p))
+    if len(key_m):
+        hit = key_m[pos] == key_p
+        out[hit] = vals[pos[hit]]
+    return out
+
+
+def union_pattern(n: int, mats) -> sp.csc_matrix:
+    acc = sp.identity(n, format="csc") * 0.0
+    acc = acc + sp.identity(n, format="csc")  # diagonal always present
+    for m in mats:
+        mm = sp.csc_matrix(m, copy=True)
+        mm.data = np.ones_like(mm.data)
+        acc = acc + abs(mm) + abs(mm.T)
+    acc = sp.csc_matrix(acc)
+    acc.sum_duplicates()
+    acc.sort_indices()
+    acc.data = np.ones_like(acc.data)
+    return acc
+
+
+def build_latent(n: int, comps, kind: str, extra_pattern=(), info=None) -> LatentModel:
+    pat = union_pattern(n, list(comps) + list(extra_pattern))
+    vals = np.stack([_on_pattern(pat, c) for c in comps])
+    return LatentModel(n=n, pattern=pat, comp_values=vals, kind=kind, info=info or {})
+
+
+def spde_components(c0: np.ndarray, g: sp.csc_matrix):
+    """Components of ``tau^2 (kappa^4 C + 2 kappa^2 G + G C^-1 G)``."""
+    cinv = sp.diags(1.0 / c0)
+    gcg = (g @ cinv @ g).tocsc()
+    return [sp.diags(c0).tocsc(), g.tocsc(), gcg]
+
+
+def spde_coefs(log_tau: float, log_kappa: float):
+    """Coefficients (and d/d log_tau, d/d log_kappa) for :func:`spde_components`."""
+    t2 = np.exp(2 * log_tau)
+    k2 = np.exp(2 * log_kappa)
+    c = np.array([t2 * k2 * k2, 2 * t2 * k2, t2])
+    d_tau = 2 * c
+    d_kappa = np.array([4 * c[0], 2 * c[1], 0.0])
+    return c, np.stack([d_tau, d_kappa])
+
+
+# ---------------------------------------------------------------------------
+# graphs
+# ---------------------------------------------------------------------------
+
+def lattice_adjacency(nr: int, nc: int) -> sp.csr_matrix:
+    """Rook adjacency of an ``nr x nc`` lattice (row-major node numbering)."""
+    idx = np.arange(nr * nc).reshape(nr, nc)
+    a = np.concatenate([idx[:, :-1].ravel(), idx[:-1, :].ravel()])
+    b = np.concatenate([idx[:, 1:].ravel(), idx[1:, :].ravel()])
+    n = nr * nc
+    m = sp.coo_matrix((np.ones(len(a)), (a, b)), shape=(n, n))
+    return (m + m.T).tocsr()
+
+
+def besag_structure(adj: sp.spmatrix) -> sp.csc_matrix:
+    """Graph Laplacian ``R = D - W`` (intrinsic Besag structure)."""
+    adj = sp.csr_matrix(adj)
+    deg = np.asarray(adj.sum(axis=1)).ravel()
+    return (sp.diags(deg) - adj).tocsc()
+
+
+def ar1_components(n: int):
+    """``tau * (M0 + rho^2 M1 - rho M2)`` pieces of the AR1 conditional precision."""
+    m0 = sp.identity(n, format="csc")
+    d1 = np.ones(n)
+    d1[0] = d1[-1] = 0.0
+    m1 = sp.diags(d1).tocsc()
+    off = np.ones(n - 1)
+    m2 = sp.diags([off, off], [-1, 1]).tocsc()
+    return m0, m1, m2
+
+
+def ar1_precision(n: int, rho: float, tau: float) -> sp.csc_matrix:
+    m0, m1, m2 = ar1_components(n)
+    return (tau * (m0 + rho * rho * m1 - rho * m2)).tocsc()
+
+
+# ---------------------------------------------------------------------------
+# configurations
+# ---------------------------------------------------------------------------
+
+@dataclass
+class SpdeProblem:
+    model: LatentModel
+    a: sp.csr_matrix       # n_obs x n projector
+    y: np.ndarray
+    verts: np.ndarray
+    tris: np.ndarray
+    truth: dict
+    theta_init: np.ndarray  # [log prec_eps, log tau, log kappa]
+
+
+def make_spde_problem(nx: int = 200, n_obs: int = 20_000, seed: int = SEED_BASE + 2,
+                      range_true: float = 0.2, sigma_true: float = 1.0,
+                      noise_sd: float = 0.1) -> SpdeProblem:
+    """SPDE Matern alpha=2 on the jittered ``nx x nx`` grid with Gaussian data.
+
+    Draw order: interior jitter x, jitter y, field innovations z (n), point
+    locations (n_obs x 2), observation noise (n_obs). The field is an exact
+    draw ``x = K^-1 C~^{1/2} z`` with ``K = tau (kappa^2 C~ + G)``, whose
+    covariance ``K^-1 C~ K^-1`` is the SPDE ``Q^-1``.
+    """
+    rng = np.random.default_rng(seed)
+    verts, tris = grid_mesh(nx, rng)
+    c0, g = fem_matrices(verts, tris)
+    comps = spde_components(c0, g)
+    n = len(verts)
+    kappa = np.sqrt(8.0) / range_true
+    tau = 1.0 / (2.0 * np.sqrt(np.pi) * kappa * sigma_true)
+    z = rng.standard_normal(n)
+    k = (tau * (kappa * kappa * sp.diags(c0) + g)).tocsc()
+    x = spla.spsolve(k, np.sqrt(c0) * z)
+    pts = rng.uniform(0.0, 1.0, size=(n_obs, 2))
+    a = grid_projector(verts, tris, nx, pts)
+    y = a @ x + noise_sd * rng.standard_normal(n_obs)
+    ata = (a.T @ a).tocsc()
+    model = build_latent(n, comps, "spde", extra_pattern=[ata],
+                         info={"nx": nx, "c0": c0})
+    truth = {"log_prec": float(np.log(1.0 / noise_sd ** 2)), "log_tau": float(np.log(tau)),
+             "log_kappa": float(np.log(kappa)), "x": x}
+    return SpdeProblem(model=model, a=a, y=y, verts=verts, tris=tris, truth=truth,
+                       theta_init=np.zeros(3))
