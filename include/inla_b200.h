@@ -141,6 +141,89 @@ int inla_batch_solve_dev(inla_batch* h, int B, double* d_x, void* stream);
 int inla_batch_diag_inv_dev(inla_batch* h, int B, double* d_diag, void* stream);
 int inla_batch_selinv_pattern_dev(inla_batch* h, int B, double* d_sigma, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Laplace engine: find_latent_mode_a_with_solver (crates/inla_stats/src/
+ * inference.rs:776-975) for B theta-points at once. The latent precision is
+ * a linear combination of fixed-pattern components,
+ *   Q(theta_b) = sum_t coef[b][t] * comp[t]      (value refresh, no re-assembly),
+ * on a full symmetric pattern that must contain A^T A and the diagonal.
+ * A is the n_obs x n projector in CSR (a_rowptr == NULL: identity, eta = x).
+ * family: 0 gaussian/identity (p1 = precision), 1 poisson/log (p1 = exposure),
+ * 2 binomial/logit (p1 = trials), 3 negative binomial/log (p1 = size,
+ * p2 = exposure) (inference.rs:170-311). p1 is multiplied by p1scale[b].
+ * ---------------------------------------------------------------------- */
+typedef struct inla_laplace inla_laplace;
+
+enum { INLA_LAP_VARIANCES = 1, INLA_LAP_GRADIENT = 2 };
+
+int inla_laplace_create(int64_t n, const int64_t* colptr, const int64_t* rowidx, int ncomp, const double* comp,
+                        int64_t nobs, const int64_t* a_rowptr, const int64_t* a_colidx, const double* a_vals,
+                        int family, const double* y, const double* p1, const double* p2, int ordering,
+                        int max_batch, inla_laplace** out);
+void inla_laplace_free(inla_laplace* h);
+/* scalars: [B][8] = {mlik, log|Q+1e-12 I|, log|Q_post|, loglik, x'Qx, newton iterations,
+ * status (0 ok, 1 singular prior, 2 singular posterior, 3 invalid likelihood, 4 non-finite
+ * step, 5 not converged), d loglik / d log p1scale}. x, var: [B][n] or NULL (modes and
+ * Takahashi marginal variances). grad_terms: [B][4][ncomp+1] or NULL = {tr(S_prior M_t),
+ * tr(S_post M_t) + [tr(S_post A^T W A)], x'M_t x, z'M_t x (implicit GLM term)}. */
+int inla_laplace_eval(inla_laplace* h, int B, const double* coef, const double* p1scale, int flags,
+                      double* scalars, double* x, double* var, double* grad_terms);
+
+/* ------------------------------------------------------------------------
+ * Hyperpriors (crates/inla_stats/src/priors.rs): log pi(theta) and gradient.
+ * ---------------------------------------------------------------------- */
+enum {
+  INLA_PRIOR_PC_PREC = 1,   /* p = {u, alpha}: priors.rs:532-548 */
+  INLA_PRIOR_LOGGAMMA = 2,  /* p = {shape, rate}: priors.rs:836-855 */
+  INLA_PRIOR_PC_SPDE = 3,   /* p = {r0, alpha_r, s0, alpha_s}, slots (log tau, log kappa): priors.rs:127-147,813-834 */
+  INLA_PRIOR_GAUSSIAN = 4   /* p = {mean, precision} */
+};
+typedef struct {
+  int kind;
+  int slot;
+  double p[4];
+} inla_prior_spec;
+double inla_prior_log_density(const inla_prior_spec* specs, int nspec, const double* theta, int m, double* grad);
+
+/* A prior stack usable directly as the inla_fit prior callback (user = inla_prior_set*). */
+typedef struct {
+  int nspec;
+  inla_prior_spec specs[8];
+} inla_prior_set;
+double inla_log_prior_set(const double* theta, int m, double* grad, void* user);
+
+/* ------------------------------------------------------------------------
+ * INLA fit: run_inla_inference_a_cancellable (inference.rs:1116-1466).
+ * map(theta) gives coef[ncomp], dcoef[m][ncomp], p1scale, dp1scale[m]
+ * (the build_prior / build_obs callbacks of the reference, as value
+ * refreshes); prior(theta) gives log pi(theta) and its gradient.
+ * ---------------------------------------------------------------------- */
+typedef int (*inla_theta_map_fn)(const double* theta, int m, double* coef, double* dcoef, double* p1scale,
+                                 double* dp1scale, void* user);
+typedef double (*inla_log_prior_fn)(const double* theta, int m, double* grad, void* user);
+
+typedef struct {
+  int mode_search; /* 0 Nelder-Mead on values (reference), 1 BFGS on adjoint gradients */
+  int batched;     /* 0 one theta-point per evaluation (plain drop-in), 1 batched theta-sets */
+  int strategy;    /* 0 CCD, 1 grid (m <= 2; CCD f0 = 2.5 above) */
+  double f0;       /* CCD f0 / grid step (0 = 1.0) */
+  int hessian;     /* 0 FD of log-posterior values (reference stencil), 1 FD of adjoint gradients */
+  int max_iter;    /* 0 = 200 (NM) / 100 (BFGS) */
+  double tol;      /* 0 = 1e-6 (NM f-spread) / 1e-4 (BFGS gradient inf-norm) */
+  double nm_step;  /* 0 = 0.1 */
+} inla_fit_options;
+
+/* node_theta: up to [64][m]; node_weight: up to [64]; info: [6] = {mlik, seconds,
+ * theta-evaluations, batches, mode-search iterations, integration nodes}. */
+int inla_fit(inla_laplace* h, int m, const double* theta0, inla_theta_map_fn map, inla_log_prior_fn prior,
+             void* user, const inla_fit_options* opt, double* mode, double* hessian, double* latent_mean,
+             double* latent_var, double* node_theta, double* node_weight, double* info);
+
+/* Built-in theta map of the SPDE Gaussian model: theta = [log prec_eps, log tau, log kappa],
+ * components [C~, G, G C~^-1 G] (crates/inla_stats/src/spde.rs:70-140). */
+int inla_theta_map_spde(const double* theta, int m, double* coef, double* dcoef, double* p1scale,
+                        double* dp1scale, void* user);
+
 #ifdef __cplusplus
 }
 #endif

@@ -375,3 +375,49 @@ def integrate(mode, hessian, eval_node, f0=1.0):
     var = nw @ (vars_ + (means - mean) ** 2)
     return {"thetas": np.array(thetas), "weights": nw, "mean": mean, "var": var, "log_posts": lps,
             "mlik": mx + math.log(abs(sw))}
+
+
+# ---------------------------------------------------------------------------
+# hyperpriors (crates/inla_stats/src/priors.rs) and the SPDE theta map
+# ---------------------------------------------------------------------------
+
+def pc_prec_log_dens(theta, u, alpha):
+    """priors.rs:532-548 with lambda = -ln(alpha)/u (priors.rs:78-86)."""
+    lam = -math.log(alpha) / u
+    return math.log(lam) - math.log(2.0) - lam * math.exp(-0.5 * theta) - 0.5 * theta
+
+
+def loggamma_log_dens(theta, shape, rate):
+    """priors.rs:836-855 (rate convention, with the Jacobian of theta = log x)."""
+    return shape * math.log(rate) - log_gamma(shape) + shape * theta - rate * math.exp(theta)
+
+
+def pc_spde_log_dens(t1, t2, r0, alpha_r, s0, alpha_s, d=2.0):
+    """priors.rs:127-147 (lambdas from quantiles) and 813-834 (density on log tau, log kappa)."""
+    lam1 = -math.log(alpha_r) * r0 ** (d / 2.0)
+    lam2 = -math.log(alpha_s) / s0
+    log_rho = 0.5 * math.log(8.0) - t2
+    log_sigma = -0.5 * math.log(4.0 * math.pi) - t1 - t2
+    dh = d / 2.0
+    s_rho = math.log(lam1 * dh) - dh * log_rho - lam1 * math.exp(-dh * log_rho)
+    s_sig = math.log(lam2) + log_sigma - lam2 * math.exp(log_sigma)
+    return s_rho + s_sig
+
+
+def spde_coefs(log_tau, log_kappa):
+    """spde.rs:70-140: Q = tau^2 (kappa^4 C + 2 kappa^2 G + G C^-1 G) coefficients."""
+    t2 = math.exp(2 * log_tau)
+    k2 = math.exp(2 * log_kappa)
+    return np.array([t2 * k2 * k2, 2 * t2 * k2, t2])
+
+
+def spde_neg_log_posterior(theta, model, a, y, max_iter=200, tol=1e-5, perm=None):
+    """evaluate_neg_log_posterior (inla_stats/src/hyper_opt.rs:21-47) for the SPDE Gaussian model,
+    theta = [log prec_eps, log tau, log kappa], default priors loggamma(1, 5e-5) + pc.spde(1, .05, 1, .01)."""
+    q = model.matrix(spde_coefs(theta[1], theta[2]))
+    try:
+        r = laplace(q, a, "gaussian", y, p1=math.exp(theta[0]), max_iter=max_iter, tol=tol, perm=perm)
+    except OracleError:
+        return 1e12
+    lp = loggamma_log_dens(theta[0], 1.0, 5e-5) + pc_spde_log_dens(theta[1], theta[2], 1.0, 0.05, 1.0, 0.01)
+    return -(r["mlik"] + lp)

@@ -1,0 +1,241 @@
+// extern "C" boundary of the Laplace engine and the INLA fit driver, plus
+// the hyperprior densities used by the configurations.
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+#include "capi_common.hpp"
+#include "driver.hpp"
+#include "inla_b200.h"
+
+using namespace inla;
+
+struct inla_laplace {
+  cudaStream_t stream = nullptr;
+  std::unique_ptr<LaplaceEngine> eng;
+};
+
+namespace {
+
+// priors.rs:532-548 (pc.prec), 813-834 (pc.spde, d = 2), 836-855 (loggamma)
+double prior_one(const inla_prior_spec& s, const double* th, double* g) {
+  switch (s.kind) {
+    case INLA_PRIOR_PC_PREC: {
+      const double lam = -std::log(s.p[1]) / s.p[0];
+      const double e = std::exp(-0.5 * th[s.slot]);
+      if (g) g[s.slot] += 0.5 * lam * e - 0.5;
+      return std::log(lam) - M_LN2 - lam * e - 0.5 * th[s.slot];
+    }
+    case INLA_PRIOR_LOGGAMMA: {
+      const double a = s.p[0], b = s.p[1], e = std::exp(th[s.slot]);
+      if (g) g[s.slot] += a - b * e;
+      return a * std::log(b) - std::lgamma(a) + a * th[s.slot] - b * e;
+    }
+    case INLA_PRIOR_PC_SPDE: {
+      const double d = 2.0, dh = d / 2.0;
+      const double lam1 = -std::log(s.p[1]) * std::pow(s.p[0], dh);
+      const double lam2 = -std::log(s.p[3]) / s.p[2];
+      const double t1 = th[s.slot], t2 = th[s.slot + 1];
+      const double log_rho = 0.5 * std::log(8.0) - t2;
+      const double log_sigma = -0.5 * std::log(4.0 * M_PI) - t1 - t2;
+      const double er = std::exp(-dh * log_rho), es = std::exp(log_sigma);
+      const double s_rho = std::log(lam1 * dh) - dh * log_rho - lam1 * er;
+      const double s_sig = std::log(lam2) + log_sigma - lam2 * es;
+      if (g) {
+        const double dsr = -dh + lam1 * dh * er;  // d s_rho / d log_rho
+        const double dss = 1.0 - lam2 * es;       // d s_sig / d log_sigma
+        g[s.slot] += -dss;
+        g[s.slot + 1] += -dsr - dss;
+      }
+      return s_rho + s_sig;
+    }
+    case INLA_PRIOR_GAUSSIAN: {
+      const double mu = s.p[0], prec = s.p[1], r = th[s.slot] - mu;
+      if (g) g[s.slot] += -prec * r;
+      return -0.9189385332046728 + 0.5 * std::log(prec) - 0.5 * prec * r * r;
+    }
+  }
+  return NAN;
+}
+
+}  // namespace
+
+extern "C" {
+
+double inla_prior_log_density(const inla_prior_spec* specs, int nspec, const double* theta, int m, double* grad) {
+  if (grad)
+    for (int i = 0; i < m; ++i) grad[i] = 0.0;
+  double s = 0.0;
+  for (int k = 0; k < nspec; ++k) {
+    const int need = specs[k].kind == INLA_PRIOR_PC_SPDE ? 2 : 1;
+    if (specs[k].slot < 0 || specs[k].slot + need > m) return NAN;
+    s += prior_one(specs[k], theta, grad);
+  }
+  return s;
+}
+
+double inla_log_prior_set(const double* theta, int m, double* grad, void* user) {
+  const inla_prior_set* ps = (const inla_prior_set*)user;
+  if (!ps || ps->nspec < 0 || ps->nspec > 8) return NAN;
+  return inla_prior_log_density(ps->specs, ps->nspec, theta, m, grad);
+}
+
+int inla_theta_map_spde(const double* theta, int m, double* coef, double* dcoef, double* p1scale, double* dp1scale,
+                        void* user) {
+  (void)user;
+  // theta = [log prec_eps, log tau, log kappa]; Q = tau^2 (kappa^4 C + 2 kappa^2 G + G C^-1 G)
+  if (m != 3) return 1;
+  const double t2 = std::exp(2.0 * theta[1]), k2 = std::exp(2.0 * theta[2]);
+  const double c[3] = {t2 * k2 * k2, 2.0 * t2 * k2, t2};
+  for (int t = 0; t < 3; ++t) coef[t] = c[t];
+  if (dcoef) {
+    // rows: d/d theta_0, theta_1, theta_2
+    for (int t = 0; t < 3; ++t) dcoef[t] = 0.0;
+    for (int t = 0; t < 3; ++t) dcoef[3 + t] = 2.0 * c[t];
+    dcoef[6] = 4.0 * c[0];
+    dcoef[7] = 2.0 * c[1];
+    dcoef[8] = 0.0;
+  }
+  *p1scale = std::exp(theta[0]);
+  if (dp1scale) {
+    dp1scale[0] = *p1scale;
+    dp1scale[1] = dp1scale[2] = 0.0;
+  }
+  return std::isfinite(c[0]) && std::isfinite(*p1scale) && c[2] > 0.0 ? 0 : 1;
+}
+
+int inla_laplace_create(int64_t n, const int64_t* colptr, const int64_t* rowidx, int ncomp, const double* comp,
+                        int64_t nobs, const int64_t* a_rowptr, const int64_t* a_colidx, const double* a_vals,
+                        int family, const double* y, const double* p1, const double* p2, int ordering, int max_batch,
+                        inla_laplace** out) {
+  inla_laplace* h = nullptr;
+  try {
+    if (!out || !colptr || !rowidx || !comp || !y || n <= 0 || nobs <= 0 || max_batch < 1)
+      return fail(INLA_ERR_INVALID, "invalid argument");
+    LaplaceSpec sp;
+    sp.n = n;
+    sp.colptr.assign(colptr, colptr + n + 1);
+    const int64_t nnz = colptr[n];
+    sp.rowidx.assign(rowidx, rowidx + nnz);
+    sp.ncomp = ncomp;
+    sp.comp.assign(comp, comp + (size_t)ncomp * nnz);
+    sp.nobs = nobs;
+    sp.identity_a = a_rowptr == nullptr;
+    if (!sp.identity_a) {
+      sp.acp.assign(a_rowptr, a_rowptr + nobs + 1);
+      sp.aci.assign(a_colidx, a_colidx + a_rowptr[nobs]);
+      sp.av.assign(a_vals, a_vals + a_rowptr[nobs]);
+    }
+    sp.family = family;
+    sp.y.assign(y, y + nobs);
+    if (p1) sp.p1.assign(p1, p1 + nobs);
+    if (p2) sp.p2.assign(p2, p2 + nobs);
+    sp.ordering = ordering;
+    h = new inla_laplace();
+    INLA_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->eng.reset(new LaplaceEngine(sp, max_batch, h->stream));
+    *out = h;
+    return INLA_OK;
+  } catch (...) {
+    int code = map_exception();
+    inla_laplace_free(h);
+    return code;
+  }
+}
+
+void inla_laplace_free(inla_laplace* h) {
+  if (!h) return;
+  h->eng.reset();
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+int inla_laplace_eval(inla_laplace* h, int B, const double* coef, const double* p1scale, int flags, double* scalars,
+                      double* x, double* var, double* grad_terms) {
+  try {
+    if (!h || !h->eng) return fail(INLA_ERR_INVALID, "null handle");
+    LaplaceEngine& E = *h->eng;
+    if (B < 1 || B > E.max_batch()) return fail(INLA_ERR_DIM_MISMATCH, "batch size out of range");
+    if (var) flags |= LAP_VARIANCES;
+    LaplaceOut R;
+    int64_t before = E.launches();
+    E.eval(B, coef, p1scale, flags, R);
+    g_launches += E.launches() - before;
+    const int T1 = E.ncomp() + 1;
+    for (int b = 0; b < B; ++b) {
+      double* s = scalars + (size_t)b * 8;
+      s[0] = R.mlik[b];
+      s[1] = R.ld_prior[b];
+      s[2] = R.ld_post[b];
+      s[3] = R.loglik[b];
+      s[4] = R.quad[b];
+      s[5] = R.iters[b];
+      s[6] = R.status[b];
+      s[7] = R.dll[b];
+      if (grad_terms) {
+        double* gt = grad_terms + (size_t)b * 4 * T1;
+        std::memcpy(gt, &R.trP[(size_t)b * T1], sizeof(double) * T1);
+        std::memcpy(gt + T1, &R.trQ[(size_t)b * T1], sizeof(double) * T1);
+        std::memcpy(gt + 2 * T1, &R.xMx[(size_t)b * T1], sizeof(double) * T1);
+        std::memcpy(gt + 3 * T1, &R.zMx[(size_t)b * T1], sizeof(double) * T1);
+      }
+    }
+    if (x)
+      INLA_CUDA(cudaMemcpyAsync(x, E.d_x(), sizeof(double) * B * E.n(), cudaMemcpyDeviceToHost, E.stream()));
+    if (var)
+      INLA_CUDA(cudaMemcpyAsync(var, E.d_var(), sizeof(double) * B * E.n(), cudaMemcpyDeviceToHost, E.stream()));
+    INLA_CUDA(cudaStreamSynchronize(E.stream()));
+    return INLA_OK;
+  } catch (...) {
+    return map_exception();
+  }
+}
+
+int inla_fit(inla_laplace* h, int m, const double* theta0, inla_theta_map_fn map, inla_log_prior_fn prior,
+             void* user, const inla_fit_options* opt, double* mode, double* hessian, double* latent_mean,
+             double* latent_var, double* node_theta, double* node_weight, double* info) {
+  try {
+    if (!h || !h->eng || !theta0 || !map || !prior || !opt || m < 1 || m > 5)
+      return fail(INLA_ERR_INVALID, "invalid argument");
+    LaplaceEngine& E = *h->eng;
+    ThetaMap tm = [&](const double* th, double* c, double* dc, double* s, double* ds) {
+      return map(th, m, c, dc, s, ds, user);
+    };
+    LogPrior lp = [&](const double* th, double* g) { return prior(th, m, g, user); };
+    InlaDriver drv(E, m, tm, lp);
+    FitOptions fo;
+    fo.mode_search = opt->mode_search;
+    fo.batched = opt->batched;
+    fo.strategy = opt->strategy;
+    fo.f0 = opt->f0 > 0 ? opt->f0 : 1.0;
+    fo.hessian = opt->hessian;
+    fo.max_iter = opt->max_iter > 0 ? opt->max_iter : (opt->mode_search ? 100 : 200);
+    fo.tol = opt->tol > 0 ? opt->tol : (opt->mode_search ? 1e-4 : 1e-6);
+    fo.nm_step = opt->nm_step > 0 ? opt->nm_step : 0.1;
+    FitResult R;
+    int64_t before = E.launches();
+    drv.fit(theta0, fo, R);
+    g_launches += E.launches() - before;
+    const int64_t n = E.n();
+    const int K = (int)R.node_weight.size();
+    if (mode) std::memcpy(mode, R.mode.data(), sizeof(double) * m);
+    if (hessian) std::memcpy(hessian, R.hessian.data(), sizeof(double) * m * m);
+    if (latent_mean) std::memcpy(latent_mean, R.latent_mean.data(), sizeof(double) * n);
+    if (latent_var) std::memcpy(latent_var, R.latent_var.data(), sizeof(double) * n);
+    if (node_theta) std::memcpy(node_theta, R.node_theta.data(), sizeof(double) * std::min(K, 64) * m);
+    if (node_weight) std::memcpy(node_weight, R.node_weight.data(), sizeof(double) * std::min(K, 64));
+    if (info) {
+      info[0] = R.mlik;
+      info[1] = R.seconds;
+      info[2] = R.n_evals;
+      info[3] = R.n_batches;
+      info[4] = R.mode_iters;
+      info[5] = K;
+    }
+    return INLA_OK;
+  } catch (...) {
+    return map_exception();
+  }
+}
+
+}  // extern "C"

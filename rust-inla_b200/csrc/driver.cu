@@ -1,0 +1,597 @@
+// Theta-level INLA driver (host) over the batched Laplace engine.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <stdexcept>
+
+#include "driver.hpp"
+
+namespace inla {
+
+// ---------------------------------------------------------------------------
+// integration.rs restatements
+// ---------------------------------------------------------------------------
+
+// integration.rs:1-62
+void ccd_design(int m, double f0, std::vector<double>& pts, std::vector<double>& w) {
+  if (m < 1) throw std::runtime_error("CCD requires at least 1 factor");
+  pts.assign(m, 0.0);
+  for (int i = 0; i < m; ++i) {
+    for (double s : {f0, -f0}) {
+      std::vector<double> p(m, 0.0);
+      p[i] = s;
+      pts.insert(pts.end(), p.begin(), p.end());
+    }
+  }
+  if (m >= 2 && m <= 4) {
+    const double val = f0 / std::sqrt((double)m);
+    for (int k = 0; k < (1 << m); ++k)
+      for (int i = 0; i < m; ++i) pts.push_back(((k >> i) & 1 ? 1.0 : -1.0) * val);
+  } else if (m == 5) {
+    const double val = f0 / std::sqrt(5.0);
+    for (int k = 0; k < 16; ++k) {
+      double sp = 1.0;
+      for (int i = 0; i < 4; ++i) {
+        double s = (k >> i) & 1 ? 1.0 : -1.0;
+        pts.push_back(s * val);
+        sp *= s;
+      }
+      pts.push_back(sp * val);
+    }
+  } else if (m > 5) {
+    throw std::runtime_error("CCD strategy for m > 5 is not supported");
+  }
+  const int ne = (int)(pts.size() / m);
+  const double wv = ne > 1 ? 1.0 / ((ne - 1) * (1.0 + std::exp(-0.5 * f0 * f0) * (f0 * f0 / m - 1.0))) : 1.0;
+  w.assign(ne, wv);
+  w[0] = 1.0 - (ne - 1) * wv;
+}
+
+// integration.rs:163-230 (Gauss-Jordan with partial pivoting)
+bool invert_symmetric_matrix(const std::vector<double>& h, int m, std::vector<double>& inv) {
+  const int cols = 2 * m;
+  std::vector<double> a(m * cols, 0.0);
+  for (int i = 0; i < m; ++i) {
+    for (int j = 0; j < m; ++j) a[i * cols + j] = h[i * m + j];
+    a[i * cols + m + i] = 1.0;
+  }
+  for (int i = 0; i < m; ++i) {
+    int mr = i;
+    for (int r = i + 1; r < m; ++r)
+      if (std::fabs(a[r * cols + i]) > std::fabs(a[mr * cols + i])) mr = r;
+    if (std::fabs(a[mr * cols + i]) < 1e-14) return false;
+    if (mr != i)
+      for (int c = 0; c < cols; ++c) std::swap(a[i * cols + c], a[mr * cols + c]);
+    const double piv = a[i * cols + i];
+    for (int c = 0; c < cols; ++c) a[i * cols + c] /= piv;
+    for (int r = 0; r < m; ++r) {
+      if (r == i) continue;
+      const double f = a[r * cols + i];
+      if (f == 0.0) continue;
+      for (int c = 0; c < cols; ++c) a[r * cols + c] -= f * a[i * cols + c];
+    }
+  }
+  inv.assign(m * m, 0.0);
+  for (int i = 0; i < m; ++i)
+    for (int j = 0; j < m; ++j) inv[i * m + j] = a[i * cols + m + j];
+  return true;
+}
+
+// Cyclic Jacobi eigen-decomposition of a small symmetric matrix (row-major);
+// V[i*m + j] = component i of eigenvector j. The CCD point set is invariant to
+// eigenvector signs and to the order of eigenpairs.
+void symmetric_eigen(const std::vector<double>& a0, int m, std::vector<double>& lambda, std::vector<double>& V) {
+  std::vector<double> a = a0;
+  V.assign(m * m, 0.0);
+  for (int i = 0; i < m; ++i) V[i * m + i] = 1.0;
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0;
+    for (int i = 0; i < m; ++i)
+      for (int j = i + 1; j < m; ++j) off += a[i * m + j] * a[i * m + j];
+    if (off < 1e-30) break;
+    for (int p = 0; p < m; ++p)
+      for (int q = p + 1; q < m; ++q) {
+        const double apq = a[p * m + q];
+        if (std::fabs(apq) < 1e-300) continue;
+        const double theta = (a[q * m + q] - a[p * m + p]) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+        for (int k = 0; k < m; ++k) {
+          const double akp = a[k * m + p], akq = a[k * m + q];
+          a[k * m + p] = c * akp - s * akq;
+          a[k * m + q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < m; ++k) {
+          const double apk = a[p * m + k], aqk = a[q * m + k];
+          a[p * m + k] = c * apk - s * aqk;
+          a[q * m + k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < m; ++k) {
+          const double vkp = V[k * m + p], vkq = V[k * m + q];
+          V[k * m + p] = c * vkp - s * vkq;
+          V[k * m + q] = s * vkp + c * vkq;
+        }
+      }
+  }
+  lambda.resize(m);
+  for (int i = 0; i < m; ++i) lambda[i] = a[i * m + i];
+}
+
+// ---------------------------------------------------------------------------
+// evaluation of f = -(mlik + log prior) (inla_stats/src/hyper_opt.rs:21-47)
+// ---------------------------------------------------------------------------
+
+void InlaDriver::evaluate(int K, const double* thetas, bool want_grad, bool batched, double* f, double* grad,
+                          std::vector<LaplaceOut>* keep) {
+  const int T = eng_.ncomp(), m = m_;
+  const int Bmax = batched ? eng_.max_batch() : 1;
+  std::vector<double> coef, dcoef, p1s, dp1s, gp(m);
+  for (int k0 = 0; k0 < K; k0 += Bmax) {
+    const int Bc = std::min(Bmax, K - k0);
+    coef.assign((size_t)Bc * T, 0.0);
+    dcoef.assign((size_t)Bc * m * T, 0.0);
+    p1s.assign(Bc, 1.0);
+    dp1s.assign((size_t)Bc * m, 0.0);
+    std::vector<char> ok(Bc, 1);
+    for (int b = 0; b < Bc; ++b) {
+      const double* th = thetas + (size_t)(k0 + b) * m;
+      if (map_(th, &coef[(size_t)b * T], &dcoef[(size_t)b * m * T], &p1s[b], &dp1s[(size_t)b * m]) != 0) {
+        ok[b] = 0;
+        // keep the batch well-formed: reuse a harmless copy of a valid point
+        for (int t = 0; t < T; ++t) coef[(size_t)b * T + t] = 1.0;
+        p1s[b] = 1.0;
+      }
+    }
+    LaplaceOut R;
+    eng_.eval(Bc, coef.data(), p1s.data(), (want_grad ? LAP_GRADIENT : 0) | (keep ? LAP_VARIANCES : 0), R);
+    n_evals_ += Bc;
+    n_batches_ += 1;
+    for (int b = 0; b < Bc; ++b) {
+      const int k = k0 + b;
+      const double* th = thetas + (size_t)k * m;
+      const bool good = ok[b] && R.status[b] == LAP_OK && std::isfinite(R.mlik[b]);
+      if (!good) {
+        f[k] = 1e12;  // hyper_opt.rs:39-45: keep the search alive on a failed Laplace
+        if (grad)
+          for (int i = 0; i < m; ++i) grad[(size_t)k * m + i] = 0.0;
+        continue;
+      }
+      const double lp = prior_(th, want_grad ? gp.data() : nullptr);
+      f[k] = -(R.mlik[b] + lp);
+      if (want_grad && grad) {
+        const int T1 = T + 1;
+        for (int i = 0; i < m; ++i) {
+          double d = 0.0;
+          for (int t = 0; t < T; ++t) {
+            const double dc = dcoef[(size_t)b * m * T + (size_t)i * T + t];
+            if (dc == 0.0) continue;
+            d += dc * (0.5 * R.trP[(size_t)b * T1 + t] - 0.5 * R.trQ[(size_t)b * T1 + t] -
+                       0.5 * R.xMx[(size_t)b * T1 + t] + 0.5 * R.zMx[(size_t)b * T1 + t]);
+          }
+          const double ds = dp1s[(size_t)b * m + i];
+          if (ds != 0.0) d += ds / p1s[b] * (R.dll[b] - 0.5 * R.trQ[(size_t)b * T1 + T]);
+          grad[(size_t)k * m + i] = -(d + gp[i]);
+        }
+      }
+    }
+    if (keep) keep->push_back(std::move(R));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Nelder-Mead (inla_math/src/hyper_opt.rs:15-183)
+// ---------------------------------------------------------------------------
+
+void InlaDriver::nelder_mead(std::vector<double>& x0, const FitOptions& opt, int& iters) {
+  const int m = m_;
+  const bool batched = opt.batched != 0;
+  std::vector<std::vector<double>> v(m + 1, x0);
+  std::vector<double> fv(m + 1);
+  {
+    std::vector<double> pts((size_t)(m + 1) * m);
+    for (int i = 0; i <= m; ++i) {
+      if (i > 0) v[i][i - 1] += opt.nm_step;
+      std::copy(v[i].begin(), v[i].end(), pts.begin() + (size_t)i * m);
+    }
+    evaluate(m + 1, pts.data(), false, batched, fv.data(), nullptr);
+  }
+  auto f1 = [&](const std::vector<double>& t) {
+    double r;
+    evaluate(1, t.data(), false, false, &r, nullptr);
+    return r;
+  };
+  iters = 0;
+  for (int it = 0; it < opt.max_iter; ++it) {
+    iters = it + 1;
+    std::vector<int> idx(m + 1);
+    for (int i = 0; i <= m; ++i) idx[i] = i;
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return fv[a] < fv[b]; });
+    std::vector<std::vector<double>> sv(m + 1);
+    std::vector<double> sf(m + 1);
+    for (int i = 0; i <= m; ++i) {
+      sv[i] = v[idx[i]];
+      sf[i] = fv[idx[i]];
+    }
+    v.swap(sv);
+    fv.swap(sf);
+    double mean = 0.0;
+    for (double x : fv) mean += x;
+    mean /= (m + 1);
+    double var = 0.0;
+    for (double x : fv) var += (x - mean) * (x - mean);
+    var /= (m + 1);
+    if (std::sqrt(var) < opt.tol) break;
+    std::vector<double> cen(m, 0.0), refl(m);
+    for (int i = 0; i < m; ++i)
+      for (int j = 0; j < m; ++j) cen[j] += v[i][j];
+    for (int j = 0; j < m; ++j) cen[j] /= m;
+    for (int j = 0; j < m; ++j) refl[j] = cen[j] + 1.0 * (cen[j] - v[m][j]);
+    const double fr = f1(refl);
+    if (fv[0] <= fr && fr < fv[m - 1]) {
+      v[m] = refl;
+      fv[m] = fr;
+      continue;
+    }
+    if (fr < fv[0]) {
+      std::vector<double> ex(m);
+      for (int j = 0; j < m; ++j) ex[j] = cen[j] + 2.0 * (refl[j] - cen[j]);
+      const double fe = f1(ex);
+      if (fe < fr) {
+        v[m] = ex;
+        fv[m] = fe;
+      } else {
+        v[m] = refl;
+        fv[m] = fr;
+      }
+      continue;
+    }
+    bool contract = false;
+    std::vector<double> con(m);
+    if (fr < fv[m]) {
+      for (int j = 0; j < m; ++j) con[j] = cen[j] + 0.5 * (refl[j] - cen[j]);
+      const double fc = f1(con);
+      if (fc < fr) {
+        v[m] = con;
+        fv[m] = fc;
+        contract = true;
+      }
+    } else {
+      for (int j = 0; j < m; ++j) con[j] = cen[j] + 0.5 * (v[m][j] - cen[j]);
+      const double fc = f1(con);
+      if (fc < fv[m]) {
+        v[m] = con;
+        fv[m] = fc;
+        contract = true;
+      }
+    }
+    if (contract) continue;
+    std::vector<double> pts((size_t)m * m);
+    for (int i = 1; i <= m; ++i) {
+      for (int j = 0; j < m; ++j) v[i][j] = v[0][j] + 0.5 * (v[i][j] - v[0][j]);
+      std::copy(v[i].begin(), v[i].end(), pts.begin() + (size_t)(i - 1) * m);
+    }
+    evaluate(m, pts.data(), false, batched, fv.data() + 1, nullptr);
+  }
+  x0 = v[0];
+}
+
+// ---------------------------------------------------------------------------
+// BFGS on exact adjoint gradients with a batched multi-step line search
+// ---------------------------------------------------------------------------
+
+void InlaDriver::bfgs(std::vector<double>& x, const FitOptions& opt, int& iters) {
+  const int m = m_;
+  const bool batched = opt.batched != 0;
+  double f;
+  std::vector<double> g(m), Hinv(m * m, 0.0);
+  evaluate(1, x.data(), true, batched, &f, g.data());
+  for (int i = 0; i < m; ++i) Hinv[i * m + i] = 1.0;
+  bool scaled = false;
+  static const double kAlphas[] = {1.0, 0.5, 0.25, 0.1, 0.03, 0.01};
+  const int na = batched ? 6 : 1;
+  iters = 0;
+  for (int it = 0; it < opt.max_iter; ++it) {
+    iters = it + 1;
+    double gmax = 0.0;
+    for (double gi : g) gmax = std::max(gmax, std::fabs(gi));
+    if (gmax < opt.tol) break;
+    std::vector<double> p(m, 0.0);
+    for (int i = 0; i < m; ++i)
+      for (int j = 0; j < m; ++j) p[i] -= Hinv[i * m + j] * g[j];
+    double slope = 0.0, pmax = 0.0;
+    for (int i = 0; i < m; ++i) {
+      slope += p[i] * g[i];
+      pmax = std::max(pmax, std::fabs(p[i]));
+    }
+    if (slope >= 0.0) {  // not a descent direction: restart from steepest descent
+      for (int i = 0; i < m * m; ++i) Hinv[i] = (i % (m + 1) == 0) ? 1.0 : 0.0;
+      for (int i = 0; i < m; ++i) p[i] = -g[i];
+      slope = 0.0;
+      pmax = 0.0;
+      for (int i = 0; i < m; ++i) {
+        slope += p[i] * g[i];
+        pmax = std::max(pmax, std::fabs(p[i]));
+      }
+    }
+    const double cap = 1.0;  // theta lives on log scales: at most one unit per step
+    const double base = pmax > cap ? cap / pmax : 1.0;
+    bool accepted = false;
+    double fa = 0.0, amax = 0.0;
+    std::vector<double> xa(m), ga(m);
+    double scale = base;
+    for (int round = 0; round < 6 && !accepted; ++round) {
+      const int K = batched ? na : 1;
+      std::vector<double> pts((size_t)K * m), fk(K), gk((size_t)K * m);
+      std::vector<double> al(K);
+      for (int k = 0; k < K; ++k) {
+        al[k] = scale * (batched ? kAlphas[k] : 1.0);
+        for (int i = 0; i < m; ++i) pts[(size_t)k * m + i] = x[i] + al[k] * p[i];
+      }
+      evaluate(K, pts.data(), true, batched, fk.data(), gk.data());
+      // best Armijo point among the candidates
+      int best = -1;
+      for (int k = 0; k < K; ++k) {
+        if (!(fk[k] < 1e11)) continue;
+        if (fk[k] <= f + 1e-4 * al[k] * slope && (best < 0 || fk[k] < fk[best])) best = k;
+      }
+      if (best >= 0) {
+        accepted = true;
+        fa = fk[best];
+        amax = al[best];
+        for (int i = 0; i < m; ++i) {
+          xa[i] = pts[(size_t)best * m + i];
+          ga[i] = gk[(size_t)best * m + i];
+        }
+      } else {
+        scale *= batched ? 0.003 : 0.5;
+      }
+    }
+    if (!accepted) break;
+    std::vector<double> s(m), y(m);
+    double sy = 0.0, yy = 0.0;
+    for (int i = 0; i < m; ++i) {
+      s[i] = xa[i] - x[i];
+      y[i] = ga[i] - g[i];
+      sy += s[i] * y[i];
+      yy += y[i] * y[i];
+    }
+    const double fprev = f;
+    x = xa;
+    f = fa;
+    g = ga;
+    (void)amax;
+    if (sy > 1e-12 * std::sqrt(yy) * 1.0) {
+      if (!scaled) {
+        const double gam = sy / yy;
+        for (int i = 0; i < m * m; ++i) Hinv[i] = (i % (m + 1) == 0) ? gam : 0.0;
+        scaled = true;
+      }
+      // Hinv <- (I - rho s y') Hinv (I - rho y s') + rho s s'
+      const double rho = 1.0 / sy;
+      std::vector<double> Hy(m, 0.0);
+      for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j) Hy[i] += Hinv[i * m + j] * y[j];
+      double yHy = 0.0;
+      for (int i = 0; i < m; ++i) yHy += y[i] * Hy[i];
+      for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j)
+          Hinv[i * m + j] += rho * ((1.0 + rho * yHy) * s[i] * s[j] - Hy[i] * s[j] - s[i] * Hy[j]);
+    }
+    if (std::fabs(fprev - f) < 1e-12 * (1.0 + std::fabs(f))) break;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Hessians
+// ---------------------------------------------------------------------------
+
+// inla_math/src/hyper_opt.rs:197-259: Hessian of g = -f, all stencil points in one batch.
+void InlaDriver::fd_hessian(const std::vector<double>& mode, double h, bool batched, std::vector<double>& H) {
+  const int m = m_;
+  std::vector<double> pts(mode);
+  auto add = [&](int i, double si, int j, double sj) {
+    std::vector<double> t(mode);
+    t[i] += si * h;
+    if (j >= 0) t[j] += sj * h;
+    pts.insert(pts.end(), t.begin(), t.end());
+  };
+  for (int i = 0; i < m; ++i)
+    for (int j = 0; j < m; ++j) {
+      if (i == j) {
+        add(i, 1, -1, 0);
+        add(i, -1, -1, 0);
+      } else if (i < j) {
+        add(i, 1, j, 1);
+        add(i, 1, j, -1);
+        add(i, -1, j, 1);
+        add(i, -1, j, -1);
+      }
+    }
+  const int K = (int)(pts.size() / m);
+  std::vector<double> f(K);
+  evaluate(K, pts.data(), false, batched, f.data(), nullptr);
+  auto g = [&](int k) { return -f[k]; };
+  H.assign(m * m, 0.0);
+  int k = 1;
+  const double g0 = g(0);
+  for (int i = 0; i < m; ++i)
+    for (int j = 0; j < m; ++j) {
+      if (i == j) {
+        H[i * m + i] = (g(k) - 2.0 * g0 + g(k + 1)) / (h * h);
+        k += 2;
+      } else if (i < j) {
+        const double v = (g(k) - g(k + 1) - g(k + 2) + g(k + 3)) / (4.0 * h * h);
+        H[i * m + j] = H[j * m + i] = v;
+        k += 4;
+      }
+    }
+}
+
+// Central differences of the adjoint gradient (2m points, one batch).
+void InlaDriver::grad_hessian(const std::vector<double>& mode, double h, bool batched, std::vector<double>& H) {
+  const int m = m_;
+  std::vector<double> pts;
+  for (int i = 0; i < m; ++i)
+    for (double s : {1.0, -1.0}) {
+      std::vector<double> t(mode);
+      t[i] += s * h;
+      pts.insert(pts.end(), t.begin(), t.end());
+    }
+  std::vector<double> f(2 * m), g((size_t)2 * m * m);
+  evaluate(2 * m, pts.data(), true, batched, f.data(), g.data());
+  H.assign(m * m, 0.0);
+  for (int i = 0; i < m; ++i)
+    for (int j = 0; j < m; ++j)
+      H[i * m + j] = -(g[(size_t)(2 * i) * m + j] - g[(size_t)(2 * i + 1) * m + j]) / (2.0 * h);
+  for (int i = 0; i < m; ++i)
+    for (int j = i + 1; j < m; ++j) H[i * m + j] = H[j * m + i] = 0.5 * (H[i * m + j] + H[j * m + i]);
+}
+
+// ---------------------------------------------------------------------------
+// fit (inference.rs:1116-1466)
+// ---------------------------------------------------------------------------
+
+void InlaDriver::fit(const double* theta0, const FitOptions& opt, FitResult& out) {
+  auto t0 = std::chrono::steady_clock::now();
+  const int m = m_;
+  const int64_t n = eng_.n();
+  n_evals_ = n_batches_ = 0;
+  std::vector<double> mode(theta0, theta0 + m);
+  int iters = 0;
+  if (opt.mode_search == 0) nelder_mead(mode, opt, iters);
+  else bfgs(mode, opt, iters);
+  out.mode = mode;
+  out.mode_iters = iters;
+
+  double hh = 1e-4;  // inference.rs:1264
+  for (double t : mode) hh = std::max(hh, 0.05 * std::fabs(t));
+  if (opt.hessian == 0) fd_hessian(mode, hh, opt.batched != 0, out.hessian);
+  else grad_hessian(mode, hh, opt.batched != 0, out.hessian);
+
+  std::vector<double> neg(m * m), sigma;
+  for (int i = 0; i < m * m; ++i) neg[i] = -out.hessian[i];
+  if (!invert_symmetric_matrix(neg, m, sigma)) throw std::runtime_error("Singular Hessian matrix");
+  std::vector<double> lam, V;
+  symmetric_eigen(sigma, m, lam, V);
+
+  std::vector<double> z, zw;
+  if (opt.strategy == 1 && m <= 2) {
+    // grid_design (integration.rs:64-156): expand until log-density drops by > 4
+    auto theta_of = [&](const std::vector<double>& zz) {
+      std::vector<double> th(mode);
+      for (int i = 0; i < m; ++i) {
+        double d = 0.0;
+        for (int j = 0; j < m; ++j) d += V[i * m + j] * std::sqrt(std::fabs(lam[j])) * zz[j];
+        th[i] += d;
+      }
+      return th;
+    };
+    auto logpost = [&](const std::vector<double>& zz) {
+      std::vector<double> th = theta_of(zz);
+      double fv;
+      evaluate(1, th.data(), false, false, &fv, nullptr);
+      return fv >= 1e12 ? -std::numeric_limits<double>::infinity() : -fv;
+    };
+    const double step = opt.f0, thr = 4.0;
+    std::vector<double> c0(m, 0.0);
+    const double g0 = logpost(c0);
+    if (m == 1) {
+      z = {0.0};
+      for (int dir : {1, -1})
+        for (int k = 1;; ++k) {
+          std::vector<double> zz = {dir * k * step};
+          if (g0 - logpost(zz) > thr) break;
+          z.push_back(zz[0]);
+        }
+    } else {
+      int lim[4] = {0, 0, 0, 0};
+      const int ax[4] = {0, 0, 1, 1};
+      const int sg[4] = {1, -1, 1, -1};
+      for (int d = 0; d < 4; ++d)
+        for (;;) {
+          std::vector<double> zz(2, 0.0);
+          zz[ax[d]] = sg[d] * (lim[d] + 1) * step;
+          if (g0 - logpost(zz) > thr) break;
+          ++lim[d];
+        }
+      for (int i = -lim[1]; i <= lim[0]; ++i)
+        for (int j = -lim[3]; j <= lim[2]; ++j) {
+          std::vector<double> zz = {i * step, j * step};
+          if (g0 - logpost(zz) <= thr) z.insert(z.end(), zz.begin(), zz.end());
+        }
+    }
+    zw.assign(z.size() / m, 1.0);
+  } else {
+    ccd_design(m, opt.strategy == 1 ? 2.5 : opt.f0, z, zw);
+  }
+  const int K = (int)zw.size();
+  std::vector<double> thetas((size_t)K * m);
+  for (int k = 0; k < K; ++k)
+    for (int i = 0; i < m; ++i) {
+      double d = 0.0;
+      for (int j = 0; j < m; ++j) d += V[i * m + j] * std::sqrt(std::fabs(lam[j])) * z[(size_t)k * m + j];
+      thetas[(size_t)k * m + i] = mode[i] + d;
+    }
+
+  // node evaluations (inference.rs:1306-1397): x*, Takahashi variances, log posterior
+  std::vector<double> lp(K), means((size_t)K * n), vars((size_t)K * n);
+  {
+    const int Bmax = opt.batched ? eng_.max_batch() : 1;
+    std::vector<double> fk(K);
+    for (int k0 = 0; k0 < K; k0 += Bmax) {
+      const int Bc = std::min(Bmax, K - k0);
+      std::vector<LaplaceOut> keep;
+      evaluate(Bc, thetas.data() + (size_t)k0 * m, false, true, fk.data() + k0, nullptr, &keep);
+      const LaplaceOut& R = keep.back();
+      INLA_CUDA(cudaMemcpyAsync(means.data() + (size_t)k0 * n, eng_.d_x(), sizeof(double) * Bc * n,
+                                cudaMemcpyDeviceToHost, eng_.stream()));
+      INLA_CUDA(cudaMemcpyAsync(vars.data() + (size_t)k0 * n, eng_.d_var(), sizeof(double) * Bc * n,
+                                cudaMemcpyDeviceToHost, eng_.stream()));
+      INLA_CUDA(cudaStreamSynchronize(eng_.stream()));
+      for (int b = 0; b < Bc; ++b) {
+        const int k = k0 + b;
+        if (R.status[b] != LAP_OK || fk[k] >= 1e12) {
+          lp[k] = -std::numeric_limits<double>::infinity();
+          std::fill(means.begin() + (size_t)k * n, means.begin() + (size_t)(k + 1) * n, 0.0);
+          std::fill(vars.begin() + (size_t)k * n, vars.begin() + (size_t)(k + 1) * n, 1.0);
+        } else {
+          lp[k] = -fk[k];
+        }
+      }
+    }
+  }
+  double mx = -std::numeric_limits<double>::infinity();
+  for (double v : lp) mx = std::max(mx, v);
+  if (!std::isfinite(mx)) throw std::runtime_error("Newton-Raphson did not converge at any integration node");
+  std::vector<double> dens(K), nw(K);
+  double sw = 0.0;
+  for (int k = 0; k < K; ++k) {
+    dens[k] = std::exp(lp[k] - mx);
+    sw += zw[k] * dens[k];
+  }
+  for (int k = 0; k < K; ++k) nw[k] = zw[k] * dens[k] / sw;
+  out.latent_mean.assign(n, 0.0);
+  out.latent_var.assign(n, 0.0);
+  for (int64_t i = 0; i < n; ++i) {
+    double mi = 0.0;
+    for (int k = 0; k < K; ++k) mi += nw[k] * means[(size_t)k * n + i];
+    double vi = 0.0;
+    for (int k = 0; k < K; ++k) {
+      const double d = means[(size_t)k * n + i] - mi;
+      vi += nw[k] * (vars[(size_t)k * n + i] + d * d);
+    }
+    out.latent_mean[i] = mi;
+    out.latent_var[i] = vi;
+  }
+  out.mlik = mx + std::log(std::fabs(sw));
+  out.node_theta = thetas;
+  out.node_weight = nw;
+  out.node_logpost = lp;
+  out.n_evals = n_evals_;
+  out.n_batches = n_batches_;
+  out.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+}  // namespace inla

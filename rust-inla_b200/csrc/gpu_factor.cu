@@ -53,16 +53,21 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
 
   // panel map (compact panel index -> input entry) and front positions of input entries
   std::vector<int> pmap(S.nnz_l_stored, -1);
-  std::vector<int64_t> spos(nnz_, -1);
+  std::vector<int64_t> spos(nnz_, -1), spos_full(nnz_, -1);
   for (int64_t c = 0; c < n; ++c)
     for (int64_t p = S.colptr[c]; p < S.colptr[c + 1]; ++p) {
+      int64_t i = S.iperm[S.rowidx[p]], j = S.iperm[c];
+      int64_t lo = std::min(i, j), hi = std::max(i, j);
+      int64_t s = S.col_to_sn[lo];
+      const int64_t* R = S.sn_rows.data() + S.sn_rowptr[s];
+      int64_t m = S.sn_rowptr[s + 1] - S.sn_rowptr[s];
+      const int64_t* it = std::lower_bound(R, R + m, hi);
+      if (it == R + m || *it != hi) throw std::runtime_error("entry outside the filled pattern");
+      spos_full[p] = fptr[s] + (lo - S.sn_first[s]) * m + (it - R);
       int64_t q = S.qmap[p];
       if (q < 0) continue;
       pmap[q] = (int)p;
-      int64_t i = S.iperm[S.rowidx[p]], j = S.iperm[c];
-      int64_t jj = std::min(i, j);
-      int64_t s = S.col_to_sn[jj];
-      spos[p] = fptr[s] + (q - S.sn_lptr[s]);
+      spos[p] = spos_full[p];
     }
 
   d_first_.upload(first, stream_);
@@ -79,6 +84,7 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
   d_dpos_.upload(dpos, stream_);
   d_pmap_.upload(pmap, stream_);
   spos_.upload(spos, stream_);
+  spos_full_.upload(spos_full, stream_);
 
   ds_.n = (int)n;
   ds_.ns = (int)ns;
@@ -199,11 +205,13 @@ void GpuFactor::factor_values(const double* d_vals, int B) {
   INLA_CUDA(cudaGetLastError());
 }
 
-void GpuFactor::factor_model(int ncomp, const double* d_comp, const double* d_coef, const int* d_cptr,
-                             const int* d_cobs, const double* d_cprod, const double* d_w, int64_t wstride, int B) {
+void GpuFactor::factor_model(int ncomp, const double* d_comp, const double* d_coef, double diag_add,
+                             const unsigned char* d_pdiag, const int* d_cptr, const int* d_cobs,
+                             const double* d_cprod, const double* d_w, int64_t wstride, int B) {
   if (B < 1 || B > max_batch_) throw std::runtime_error("batch size out of range");
-  k_fill_panels_model<<<dim3((unsigned)sym_.nsuper, B), 128, 0, stream_>>>(
-      ds_, d_pmap_.p, ncomp, d_comp, nnz_, d_coef, d_cptr, d_cobs, d_cprod, d_w, wstride, F_.p, ftotal_);
+  k_fill_panels_model<<<dim3((unsigned)sym_.nsuper, B), 128, 0, stream_>>>(ds_, d_pmap_.p, ncomp, d_comp, nnz_, d_coef,
+                                                                          diag_add, d_pdiag, d_cptr, d_cobs, d_cprod,
+                                                                          d_w, wstride, F_.p, ftotal_);
   ++launches_;
   run_factor_levels(B);
   INLA_CUDA(cudaGetLastError());

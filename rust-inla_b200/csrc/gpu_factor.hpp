@@ -84,8 +84,12 @@ class GpuFactor {
   // d_vals [B][nnz] on the device. Results stay resident.
   void factor_values(const double* d_vals, int B);
   // Factorize from the component model (see k_fill_panels_model).
-  void factor_model(int ncomp, const double* d_comp, const double* d_coef, const int* d_cptr,
-                    const int* d_cobs, const double* d_cprod, const double* d_w, int64_t wstride, int B);
+  void factor_model(int ncomp, const double* d_comp, const double* d_coef, double diag_add,
+                    const unsigned char* d_pdiag, const int* d_cptr, const int* d_cobs, const double* d_cprod,
+                    const double* d_w, int64_t wstride, int B);
+  // Front offset of every input entry's lower twin (both triangles), for
+  // reading Sigma / L on the full pattern.
+  const int64_t* d_spos_full() const { return spos_full_.p; }
   // log|Q_b| and status words (after factor_*) -> device arrays of length B.
   const double* d_logdet() const { return logdet_.p; }
   const int* d_status() const { return status_.p; }
@@ -113,7 +117,7 @@ class GpuFactor {
   DevSym ds_;
   std::vector<LevelPlan> levels_;
   DBuf<int> d_first_, d_rowptr_, d_rows_, d_relx_, d_child_ptr_, d_child_list_, d_parent_, d_uoff_, d_perm_;
-  DBuf<int64_t> d_fptr_, d_lptr_, d_dpos_, spos_;
+  DBuf<int64_t> d_fptr_, d_lptr_, d_dpos_, spos_, spos_full_;
   DBuf<int> d_pmap_, d_lists_;
   DBuf<double> F_, Sg_, xp_, ub_, logdet_;
   DBuf<int> status_;

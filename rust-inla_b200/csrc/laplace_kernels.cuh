@@ -1,0 +1,343 @@
+// CUDA kernels of the batched Laplace step (sm_100a, FP64): eta = A x,
+// likelihood Eval1D (value, gradient, Fisher/observed Hessian), the Newton
+// right-hand side A^T g - Q x, the log-likelihood / quadratic-form
+// reductions of the marginal likelihood and the trace contractions of the
+// adjoint. One problem (theta-point) per blockIdx.y; every reduction uses a
+// fixed tree, so results are run-to-run bit-identical.
+//
+// Reference:
+//   likelihoods            crates/inla_stats/src/inference.rs:170-311, 1641-1664
+//   Newton system          crates/inla_math/src/ldlt.rs:373-453, design.rs:52-139
+//   mlik                   crates/inla_stats/src/inference.rs:953-972
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace inla {
+
+enum Family : int { FAM_GAUSSIAN = 0, FAM_POISSON = 1, FAM_BINOMIAL = 2, FAM_NBINOMIAL = 3 };
+
+// Lanczos log-gamma, g = 7, 9 coefficients (inference.rs:1896-1920 uses the
+// same published series).
+__device__ __forceinline__ double d_log_gamma_pos(double z) {
+  const double PI = 3.14159265358979323846;
+  const double z1 = z - 1.0;
+  double x = 0.99999999999980993;
+  x += 676.5203681218851 / (z1 + 1.0);
+  x += -1259.1392167224028 / (z1 + 2.0);
+  x += 771.32342877765313 / (z1 + 3.0);
+  x += -176.61502916214059 / (z1 + 4.0);
+  x += 12.507343278686905 / (z1 + 5.0);
+  x += -0.13857109526572012 / (z1 + 6.0);
+  x += 9.9843695780195716e-6 / (z1 + 7.0);
+  x += 1.5056327351493116e-7 / (z1 + 8.0);
+  const double t = z1 + 7.5;
+  return 0.5 * log(2.0 * PI) + (z1 + 0.5) * log(t) - t + log(x);
+}
+__device__ __forceinline__ double d_log_gamma(double z) {
+  const double PI = 3.14159265358979323846;
+  if (z < 0.5) return log(PI) - log(sin(PI * z)) - d_log_gamma_pos(1.0 - z);
+  return d_log_gamma_pos(z);
+}
+
+__device__ __forceinline__ double d_logistic(double x) {
+  if (x >= 0.0) {
+    double z = exp(-x);
+    return 1.0 / (1.0 + z);
+  }
+  double z = exp(x);
+  return z / (1.0 + z);
+}
+
+// Eval1D: returns 0 on success, 1 on an invalid input (reference: Err).
+// p1: gaussian precision / poisson exposure / binomial trials / nb size.
+// p2: nb exposure. dw: d(-hess)/d eta (for the adjoint's implicit term).
+__device__ __forceinline__ int d_eval_lik(int fam, double eta, double y, double p1, double p2, double& logp,
+                                          double& grad, double& hess, double& dw) {
+  if (!isfinite(eta)) return 1;
+  switch (fam) {
+    case FAM_GAUSSIAN: {
+      if (!(p1 > 0.0) || !isfinite(p1) || !isfinite(y)) return 1;
+      const double r = eta - y;
+      logp = -0.9189385332046728 + 0.5 * log(p1) - 0.5 * p1 * r * r;
+      grad = -p1 * r;
+      hess = -p1;
+      dw = 0.0;
+      return 0;
+    }
+    case FAM_POISSON: {
+      if (p1 < 0.0 || !isfinite(p1) || y < 0.0 || !isfinite(y)) return 1;
+      const double lam = exp(eta);
+      const double mu = p1 * lam, dmu = p1 * lam;
+      if (mu > 0.0) {
+        logp = y * log(mu) - mu - d_log_gamma(y + 1.0);
+        grad = (y / mu - 1.0) * dmu;
+        hess = -(dmu * dmu) / mu;  // Fisher scoring
+        dw = mu;
+      } else {
+        logp = (y == 0.0) ? 0.0 : -INFINITY;
+        grad = -dmu;
+        hess = -fabs(p1 * lam);
+        dw = 0.0;
+      }
+      return 0;
+    }
+    case FAM_BINOMIAL: {
+      if (p1 < 0.0 || y < 0.0 || y > p1 || !isfinite(p1) || !isfinite(y)) return 1;
+      const double p = d_logistic(eta), dp = p * (1.0 - p);
+      const double lc = d_log_gamma(p1 + 1.0) - d_log_gamma(y + 1.0) - d_log_gamma(p1 - y + 1.0);
+      if (p == 0.0) logp = (y == 0.0) ? lc : -INFINITY;
+      else if (p == 1.0) logp = (y == p1) ? lc : -INFINITY;
+      else logp = lc + y * log(p) + (p1 - y) * log(1.0 - p);
+      const double a = (p > 0.0 && p < 1.0) ? y / p - (p1 - y) / (1.0 - p) : 0.0;
+      grad = a * dp;
+      hess = -p1 * dp;  // Fisher scoring
+      dw = p1 * dp * (1.0 - 2.0 * p);
+      return 0;
+    }
+    case FAM_NBINOMIAL: {
+      const double r = p1, E = p2;
+      if (y < 0.0 || !isfinite(y) || E < 0.0 || !isfinite(E) || !(r > 0.0) || !isfinite(r)) return 1;
+      const double base = exp(eta);
+      if (!(base > 0.0)) return 1;
+      const double mu = E * base;
+      if (!(mu > 0.0)) return 1;
+      const double mr = mu + r;
+      logp = d_log_gamma(y + r) - d_log_gamma(r) - d_log_gamma(y + 1.0) + r * log(r / mr) + y * log(mu / mr);
+      const double d1 = y / mu - (y + r) / mr;
+      const double d2 = -y / (mu * mu) + (y + r) / (mr * mr);
+      const double d3 = 2.0 * y / (mu * mu * mu) - 2.0 * (y + r) / (mr * mr * mr);
+      grad = d1 * mu;
+      hess = d2 * mu * mu + d1 * mu;  // observed Hessian
+      dw = -(d3 * mu * mu * mu + 3.0 * d2 * mu * mu + d1 * mu);
+      return 0;
+    }
+  }
+  return 1;
+}
+
+// eta[b][i] = sum_a A[i, col] x[b][col]  (A in CSR; acp == nullptr => identity)
+__global__ void k_spmv_a(int64_t nobs, int n, const int64_t* __restrict__ acp, const int* __restrict__ aci,
+                         const double* __restrict__ av, const double* __restrict__ x, double* __restrict__ eta) {
+  const int b = blockIdx.y;
+  const double* xb = x + (int64_t)b * n;
+  double* eb = eta + (int64_t)b * nobs;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nobs; i += (int64_t)gridDim.x * blockDim.x) {
+    if (!acp) {
+      eb[i] = xb[i];
+      continue;
+    }
+    double s = 0.0;
+    for (int64_t a = acp[i]; a < acp[i + 1]; ++a) s += av[a] * xb[aci[a]];
+    eb[i] = s;
+  }
+}
+
+// logp/grad/w(=-hess)/dw per observation; bad[b] |= 1 on an invalid evaluation,
+// 2 on a non-finite log-likelihood.
+__global__ void k_eval_lik(int fam, int64_t nobs, const double* __restrict__ eta, const double* __restrict__ y,
+                           const double* __restrict__ p1, const double* __restrict__ p2,
+                           const double* __restrict__ p1scale, double* __restrict__ logp, double* __restrict__ grad,
+                           double* __restrict__ w, double* __restrict__ dw, int* __restrict__ bad) {
+  const int b = blockIdx.y;
+  const double sc = p1scale ? p1scale[b] : 1.0;
+  int flag = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nobs; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t o = (int64_t)b * nobs + i;
+    double lp = 0, g = 0, h = 0, d = 0;
+    const double q1 = (p1 ? p1[i] : 1.0) * sc;
+    if (d_eval_lik(fam, eta[o], y[i], q1, p2 ? p2[i] : 1.0, lp, g, h, d)) {
+      flag |= 1;
+      lp = NAN;
+    } else if (!isfinite(lp)) {
+      flag |= 2;
+    }
+    logp[o] = lp;
+    grad[o] = g;
+    w[o] = -h;
+    if (dw) dw[o] = d;
+  }
+  if (flag) atomicOr(bad + b, flag);
+}
+
+// rhs[b][j] = sum_a A[a, j] g[b][a] - (Q x)[b][j]; Q values = sum_t coef[b][t] comp[t][p]
+// on the full symmetric pattern (column j of Q = row j). A^T in CSR (atp, ati, atv).
+__global__ void k_newton_rhs(int n, int ncomp, const int64_t* __restrict__ qcp, const int* __restrict__ qri,
+                             const double* __restrict__ comp, int64_t nnz, const double* __restrict__ coef,
+                             const int64_t* __restrict__ atp, const int* __restrict__ ati,
+                             const double* __restrict__ atv, int64_t nobs, const double* __restrict__ g,
+                             const double* __restrict__ x, double* __restrict__ rhs) {
+  const int b = blockIdx.y;
+  const double* xb = x + (int64_t)b * n;
+  const double* gb = g + (int64_t)b * nobs;
+  const double* cb = coef + (int64_t)b * ncomp;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    if (atp) {
+      for (int64_t a = atp[j]; a < atp[j + 1]; ++a) s += atv[a] * gb[ati[a]];
+    } else {
+      s = gb[j];
+    }
+    double qx = 0.0;
+    for (int64_t p = qcp[j]; p < qcp[j + 1]; ++p) {
+      double v = 0.0;
+      for (int t = 0; t < ncomp; ++t) v += cb[t] * comp[(int64_t)t * nnz + p];
+      qx += v * xb[qri[p]];
+    }
+    rhs[(int64_t)b * n + j] = s - qx;
+  }
+}
+
+// Newton update with the reference's step cap: x_trial = x + alpha step.
+__global__ void k_axpy_trial(int n, const double* __restrict__ x, const double* __restrict__ step,
+                             const double* __restrict__ alpha, double* __restrict__ xt) {
+  const int b = blockIdx.y;
+  const double a = alpha[b];
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const int64_t o = (int64_t)b * n + j;
+    xt[o] = x[o] + a * step[o];
+  }
+}
+
+// Per-problem block reductions (one CTA per problem, fixed tree).
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  red[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = NT / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  double r = red[0];
+  __syncthreads();
+  return r;
+}
+template <int NT>
+__device__ __forceinline__ double block_max(double v, double* red) {
+  red[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = NT / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
+    __syncthreads();
+  }
+  double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+// out[b] = {max|step|, all finite ? 1 : 0}
+template <int NT>
+__global__ void __launch_bounds__(NT) k_step_stats(int n, const double* __restrict__ step, double* __restrict__ out) {
+  __shared__ double red[NT];
+  const int b = blockIdx.x;
+  double mx = 0.0, fin = 1.0;
+  for (int j = threadIdx.x; j < n; j += NT) {
+    double s = step[(int64_t)b * n + j];
+    if (!isfinite(s)) fin = 0.0;
+    else mx = fmax(mx, fabs(s));
+  }
+  mx = block_max<NT>(mx, red);
+  fin = -block_max<NT>(-fin, red);
+  if (threadIdx.x == 0) {
+    out[2 * b] = mx;
+    out[2 * b + 1] = fin;
+  }
+}
+
+// sum of a [B][len] array per problem
+template <int NT>
+__global__ void __launch_bounds__(NT) k_row_sum(int64_t len, const double* __restrict__ v, double* __restrict__ out) {
+  __shared__ double red[NT];
+  const int b = blockIdx.x;
+  double s = 0.0;
+  for (int64_t i = threadIdx.x; i < len; i += NT) s += v[(int64_t)b * len + i];
+  s = block_sum<NT>(s, red);
+  if (threadIdx.x == 0) out[b] = s;
+}
+
+// x^T Q(theta_b) x and the per-component quadratic forms x^T M_t x
+// out[b][0] = x^T Q x, out[b][1+t] = x^T M_t x
+template <int NT>
+__global__ void __launch_bounds__(NT) k_quad_forms(int n, int ncomp, const int64_t* __restrict__ qcp,
+                                                   const int* __restrict__ qri, const double* __restrict__ comp,
+                                                   int64_t nnz, const double* __restrict__ coef,
+                                                   const double* __restrict__ x, double* __restrict__ out) {
+  __shared__ double red[NT];
+  const int b = blockIdx.x;
+  const double* xb = x + (int64_t)b * n;
+  double acc[8];
+  for (int t = 0; t < 8; ++t) acc[t] = 0.0;
+  for (int j = threadIdx.x; j < n; j += NT) {
+    const double xj = xb[j];
+    for (int64_t p = qcp[j]; p < qcp[j + 1]; ++p) {
+      const double xx = xj * xb[qri[p]];
+      for (int t = 0; t < ncomp && t < 8; ++t) acc[t] += comp[(int64_t)t * nnz + p] * xx;
+    }
+  }
+  double total = 0.0;
+  for (int t = 0; t < ncomp && t < 8; ++t) {
+    double s = block_sum<NT>(acc[t], red);
+    if (threadIdx.x == 0) out[(int64_t)b * (ncomp + 1) + 1 + t] = s;
+    total += coef[(int64_t)b * ncomp + t] * s;
+  }
+  if (threadIdx.x == 0) out[(int64_t)b * (ncomp + 1)] = total;
+}
+
+// Trace contractions of a selected inverse given on the full pattern
+// (both triangles): out[b][t] = sum_p sigma[b][p] comp[t][p]  (= tr(Sigma M_t)),
+// out[b][ncomp] = sum_p sigma[b][p] sum_q w2[b][obs_q] prod_q (= tr(Sigma A^T diag(w2) A)).
+template <int NT>
+__global__ void __launch_bounds__(NT) k_trace_contract(int64_t nnz, int ncomp, const double* __restrict__ comp,
+                                                       const double* __restrict__ sigma,
+                                                       const int* __restrict__ cptr, const int* __restrict__ cobs,
+                                                       const double* __restrict__ cprod,
+                                                       const double* __restrict__ w2, int64_t nobs,
+                                                       double* __restrict__ out) {
+  __shared__ double red[NT];
+  const int b = blockIdx.x;
+  const double* sb = sigma + (int64_t)b * nnz;
+  double acc[9];
+  for (int t = 0; t < 9; ++t) acc[t] = 0.0;
+  for (int64_t p = threadIdx.x; p < nnz; p += NT) {
+    const double s = sb[p];
+    for (int t = 0; t < ncomp && t < 8; ++t) acc[t] += s * comp[(int64_t)t * nnz + p];
+    if (w2) {
+      double a = 0.0;
+      for (int q = cptr[p]; q < cptr[p + 1]; ++q) a += w2[(int64_t)b * nobs + cobs[q]] * cprod[q];
+      acc[8] += s * a;
+    }
+  }
+  for (int t = 0; t < ncomp && t < 8; ++t) {
+    double s = block_sum<NT>(acc[t], red);
+    if (threadIdx.x == 0) out[(int64_t)b * (ncomp + 1) + t] = s;
+  }
+  double s = block_sum<NT>(acc[8], red);
+  if (threadIdx.x == 0) out[(int64_t)b * (ncomp + 1) + ncomp] = s;
+}
+
+// Mirror lower-entry values onto the upper entries of the full pattern:
+// out[b][p] = buf[b][spos_full[p]] (spos_full maps every entry to its lower twin).
+__global__ void k_pattern_full(int64_t nnz, const int64_t* __restrict__ spos_full, const double* __restrict__ buf,
+                               int64_t fstride, double* __restrict__ out) {
+  const int b = blockIdx.y;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < nnz; p += (int64_t)gridDim.x * blockDim.x)
+    out[(int64_t)b * nnz + p] = buf[(int64_t)b * fstride + spos_full[p]];
+}
+
+// Exact predictor variances v_i = a_i^T Sigma a_i from Sigma on the pattern
+// (A row pairs -> pattern positions in opos).
+__global__ void k_predictor_var(int64_t nobs, const int64_t* __restrict__ acp, const double* __restrict__ av,
+                                const int64_t* __restrict__ oppos, const int64_t* __restrict__ opptr,
+                                const double* __restrict__ sigma, int64_t nnz, double* __restrict__ v) {
+  const int b = blockIdx.y;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nobs; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t a0 = acp[i], na = acp[i + 1] - a0;
+    double s = 0.0;
+    int64_t q = opptr[i];
+    for (int64_t a = 0; a < na; ++a)
+      for (int64_t c = 0; c < na; ++c, ++q) s += av[a0 + a] * av[a0 + c] * sigma[(int64_t)b * nnz + oppos[q]];
+    v[(int64_t)b * nobs + i] = s;
+  }
+}
+
+}  // namespace inla

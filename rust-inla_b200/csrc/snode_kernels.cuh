@@ -48,9 +48,12 @@ __global__ void k_fill_panels(DevSym S, const int* __restrict__ pmap, const doub
 
 // Component model: value(p) = sum_t coef[b][t] * comp[t][p] + sum_q w[b][obs_q] * prod_q
 // over the observation contributions of entry p (A^T diag(w) A on the pattern).
+// diag_add is added on diagonal entries (pdiag[p] != 0), e.g. the 1e-12 jitter of
+// the prior log-determinant (inference.rs:831-837).
 __global__ void k_fill_panels_model(DevSym S, const int* __restrict__ pmap, int ncomp,
                                     const double* __restrict__ comp, int64_t nnz,
-                                    const double* __restrict__ coef,
+                                    const double* __restrict__ coef, double diag_add,
+                                    const unsigned char* __restrict__ pdiag,
                                     const int* __restrict__ cptr, const int* __restrict__ cobs,
                                     const double* __restrict__ cprod, const double* __restrict__ w,
                                     int64_t wstride, double* __restrict__ F, int64_t fstride) {
@@ -66,6 +69,7 @@ __global__ void k_fill_panels_model(DevSym S, const int* __restrict__ pmap, int 
     double v = 0.0;
     if (src >= 0) {
       for (int t = 0; t < ncomp; ++t) v += cb[t] * comp[(int64_t)t * nnz + src];
+      if (pdiag[src]) v += diag_add;
       if (wb) {
         double acc = 0.0;
         for (int q = cptr[src]; q < cptr[src + 1]; ++q) acc += wb[cobs[q]] * cprod[q];

@@ -90,6 +90,14 @@ SIGNATURES = [
     ("inla_batch_solve_dev", C.c_int, [P, C.c_int, P, P]),
     ("inla_batch_diag_inv_dev", C.c_int, [P, C.c_int, P, P]),
     ("inla_batch_selinv_pattern_dev", C.c_int, [P, C.c_int, P, P]),
+    ("inla_laplace_create", C.c_int, [I64, LP, LP, C.c_int, DP, I64, LP, LP, DP, C.c_int, DP, DP, DP, C.c_int,
+                                      C.c_int, C.POINTER(P)]),
+    ("inla_laplace_free", None, [P]),
+    ("inla_laplace_eval", C.c_int, [P, C.c_int, DP, DP, C.c_int, DP, DP, DP, DP]),
+    ("inla_prior_log_density", C.c_double, [P, C.c_int, DP, C.c_int, DP]),
+    ("inla_log_prior_set", C.c_double, [DP, C.c_int, DP, P]),
+    ("inla_fit", C.c_int, [P, C.c_int, DP, P, P, P, P, DP, DP, DP, DP, DP, DP, DP]),
+    ("inla_theta_map_spde", C.c_int, [DP, C.c_int, DP, DP, DP, DP, P]),
 ]
 
 

@@ -1,0 +1,76 @@
+"""GPU INLA fits: the plain reference control flow (Nelder-Mead, FD Hessian,
+CCD, one theta-point per evaluation) against the oracle's restatement, and
+the batched BFGS + adjoint path against the plain one."""
+import numpy as np
+import pytest
+
+import oracle as O
+from inla_b200 import models
+from inla_b200.laplace import LaplaceModel
+
+pytestmark = pytest.mark.gpu
+
+THETA0 = np.array([3.0, -2.5, 2.0])
+
+
+@pytest.fixture(scope="module")
+def problem():
+    p = models.make_spde_problem(nx=20, n_obs=300, seed=11)
+    lm = LaplaceModel(p.model, a=p.a, family="gaussian", y=p.y, max_batch=25)
+    return p, lm
+
+
+def oracle_f(p):
+    return lambda th: O.spde_neg_log_posterior(np.asarray(th), p.model, p.a, p.y)
+
+
+def test_plain_fit_follows_reference_nelder_mead(problem):
+    p, lm = problem
+    r = lm.fit(THETA0, mode_search="nm", batched=False)
+    mode_ref = O.nelder_mead(list(THETA0), 0.1, 200, 1e-6, oracle_f(p))
+    np.testing.assert_allclose(r["mode"], mode_ref, atol=1e-6)
+    h = max(1e-4, max(0.05 * abs(t) for t in mode_ref))
+    H_ref = O.fd_hessian(mode_ref, oracle_f(p), h)
+    np.testing.assert_allclose(r["hessian"], H_ref, rtol=1e-5, atol=1e-6)
+
+
+def test_integration_parity_at_fixed_nodes(problem):
+    """Weights, posterior means and marginal variances at the same mode/Hessian: 1e-8 relative."""
+    p, lm = problem
+    r = lm.fit(THETA0, mode_search="nm", batched=True)
+
+    def node(theta):
+        c = O.spde_coefs(theta[1], theta[2])
+        lr = O.laplace(p.model.matrix(c), p.a, "gaussian", p.y, p1=np.exp(theta[0]), want_var=True)
+        lp = O.loggamma_log_dens(theta[0], 1.0, 5e-5) + O.pc_spde_log_dens(theta[1], theta[2], 1.0, 0.05, 1.0, 0.01)
+        return lr["x"], lr["var"], lr["mlik"] + lp
+
+    ref = O.integrate(r["mode"], r["hessian"], node, f0=1.0)
+    # node sets agree as sets (eigenvector sign conventions may permute them)
+    got = sorted(map(tuple, np.round(r["node_theta"], 9)))
+    exp = sorted(map(tuple, np.round(ref["thetas"], 9)))
+    np.testing.assert_allclose(got, exp, atol=1e-8)
+    rel = lambda a, b: np.max(np.abs(a - b)) / np.max(np.abs(b))
+    assert rel(r["mean"], ref["mean"]) < 1e-8
+    assert rel(r["var"], ref["var"]) < 1e-8
+    assert abs(r["mlik"] - ref["mlik"]) < 1e-8 * abs(ref["mlik"])
+
+
+def test_batched_adjoint_fit_matches_plain(problem):
+    p, lm = problem
+    plain = lm.fit(THETA0, mode_search="nm", batched=False)
+    fast = lm.fit(THETA0, mode_search="bfgs", batched=True, tol=1e-5)
+    f = oracle_f(p)
+    # BFGS on exact gradients reaches the optimum at least as well as NM
+    assert f(fast["mode"]) <= f(plain["mode"]) + 1e-6
+    np.testing.assert_allclose(fast["mode"], plain["mode"], atol=5e-2)
+    assert np.max(np.abs(fast["mean"] - plain["mean"])) < 1e-2 * np.max(np.abs(plain["mean"]))
+    assert np.max(np.abs(fast["var"] - plain["var"]) / plain["var"]) < 5e-2
+    assert fast["n_batches"] < plain["n_batches"]
+
+
+def test_fit_with_gradient_hessian(problem):
+    p, lm = problem
+    a = lm.fit(THETA0, mode_search="bfgs", batched=True, tol=1e-5, hessian="fd")
+    b = lm.fit(THETA0, mode_search="bfgs", batched=True, tol=1e-5, hessian="grad")
+    np.testing.assert_allclose(a["hessian"], b["hessian"], rtol=0.1, atol=0.5)

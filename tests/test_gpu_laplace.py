@@ -1,0 +1,156 @@
+"""GPU parity of the batched Laplace engine and the adjoint gradient.
+
+Per theta-point against the CPU oracle's restatement of
+find_latent_mode_a_with_solver (inference.rs:776-975): log-determinants
+1e-10 relative, modes / marginal variances 1e-8 relative, mlik 1e-10
+relative. The adjoint gradient d(mlik + log prior)/d theta is checked
+against central finite differences (step 1e-4) of the oracle's
+evaluate_neg_log_posterior restatement.
+"""
+import math
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import oracle as O
+from inla_b200 import models
+from inla_b200.laplace import SPDE_DEFAULT_PRIORS, LaplaceModel, log_prior, prior_set, spde_gradient
+
+pytestmark = pytest.mark.gpu
+
+RT_LD = 1e-10
+RT_X = 1e-8
+
+
+def rel(a, b):
+    return np.max(np.abs(np.asarray(a) - np.asarray(b))) / max(np.max(np.abs(b)), 1e-300)
+
+
+@pytest.fixture(scope="module")
+def spde_small():
+    p = models.make_spde_problem(nx=30, n_obs=500)
+    lm = LaplaceModel(p.model, a=p.a, family="gaussian", y=p.y, max_batch=8)
+    return p, lm
+
+
+THETAS = [np.array([4.0, -3.0, 2.5]), np.array([3.0, -2.0, 1.5]), np.array([5.5, -3.8, 2.8])]
+
+
+def test_gaussian_spde_matches_oracle(spde_small):
+    p, lm = spde_small
+    coefs = np.stack([models.spde_coefs(t[1], t[2])[0] for t in THETAS])
+    scale = np.exp([t[0] for t in THETAS])
+    out = lm.eval(coefs, scale, variances=True)
+    assert np.all(out["status"] == 0)
+    for b, t in enumerate(THETAS):
+        q = p.model.matrix(coefs[b])
+        r = O.laplace(q, p.a, "gaussian", p.y, p1=scale[b], want_var=True, perm=None)
+        assert abs(out["logdet_prior"][b] - r["logdet_prior"]) <= RT_LD * abs(r["logdet_prior"])
+        assert abs(out["logdet_post"][b] - r["logdet_post"]) <= RT_LD * abs(r["logdet_post"])
+        assert abs(out["mlik"][b] - r["mlik"]) <= RT_LD * abs(r["logdet_post"])
+        assert rel(out["x"][b], r["x"]) < RT_X
+        assert rel(out["var"][b], r["var"]) < RT_X
+        assert out["iters"][b] == 1
+
+
+def test_batch_equals_single(spde_small):
+    p, lm = spde_small
+    coefs = np.stack([models.spde_coefs(t[1], t[2])[0] for t in THETAS])
+    scale = np.exp([t[0] for t in THETAS])
+    allb = lm.eval(coefs, scale, variances=True)
+    for b in range(len(THETAS)):
+        one = lm.eval(coefs[b:b + 1], scale[b:b + 1], variances=True)
+        assert one["mlik"][0] == allb["mlik"][b]
+        np.testing.assert_array_equal(one["x"][0], allb["x"][b])
+        np.testing.assert_array_equal(one["var"][0], allb["var"][b])
+
+
+def _spde_grad(lm, theta):
+    c, dc = models.spde_coefs(theta[1], theta[2])
+    dcoef = np.zeros((3, 3))
+    dcoef[1:] = dc
+    s = math.exp(theta[0])
+    out = lm.eval(c[None], [s], gradient=True)
+    ps = prior_set(SPDE_DEFAULT_PRIORS)
+    lp, gp = log_prior(ps, theta)
+    one = {k: out[k][0] for k in ("trP", "trQ", "xMx", "zMx", "dll")}
+    g = spde_gradient(one, dcoef, np.array([s, 0.0, 0.0]), s, gp)
+    return out["mlik"][0] + lp, g
+
+
+def test_prior_densities_match_oracle():
+    ps = prior_set(SPDE_DEFAULT_PRIORS)
+    for t in THETAS:
+        v, g = log_prior(ps, t)
+        ref = O.loggamma_log_dens(t[0], 1.0, 5e-5) + O.pc_spde_log_dens(t[1], t[2], 1.0, 0.05, 1.0, 0.01)
+        assert abs(v - ref) < 1e-10 * max(1, abs(ref))
+        h = 1e-6
+        for i in range(3):
+            tp, tm = t.copy(), t.copy()
+            tp[i] += h
+            tm[i] -= h
+            fd = (log_prior(ps, tp)[0] - log_prior(ps, tm)[0]) / (2 * h)
+            assert abs(g[i] - fd) < 1e-6 * max(1, abs(fd))
+
+
+def test_adjoint_gradient_vs_central_fd(spde_small):
+    """Adjoint d log pi(theta|y)/d theta vs central FD (step 1e-4) of the oracle objective."""
+    p, lm = spde_small
+    for t in THETAS[:2]:
+        val, g = _spde_grad(lm, t)
+        f0 = O.spde_neg_log_posterior(t, p.model, p.a, p.y)
+        assert abs(-f0 - val) <= 1e-10 * abs(f0)
+        fd = -O.fd_gradient(list(t), lambda th: O.spde_neg_log_posterior(np.array(th), p.model, p.a, p.y), h=1e-4)
+        assert np.max(np.abs(g - fd)) <= 1e-5 * max(1.0, np.max(np.abs(fd))), (g, fd)
+
+
+def _poisson_problem(nx=20, seed=5):
+    p = models.make_spde_problem(nx=nx, n_obs=300, seed=seed)
+    rng = np.random.default_rng(seed)
+    eta = p.a @ (0.6 * p.truth["x"]) + 0.3
+    y = rng.poisson(np.exp(eta)).astype(float)
+    return p, y
+
+
+@pytest.mark.parametrize("family", ["poisson", "nbinomial", "binomial"])
+def test_glm_newton_matches_oracle(family):
+    p, y = _poisson_problem()
+    kw = {}
+    if family == "nbinomial":
+        kw = dict(p1=5.0, p2=1.0)
+    if family == "binomial":
+        y = np.minimum(y, 10.0)
+        kw = dict(p1=10.0)
+    lm = LaplaceModel(p.model, a=p.a, family=family, y=y, max_batch=4, **kw)
+    thetas = [(-1.0, 1.5), (-0.5, 1.0)]
+    coefs = np.stack([models.spde_coefs(a, b)[0] for a, b in thetas])
+    out = lm.eval(coefs, variances=True)
+    assert np.all(out["status"] == 0)
+    for b in range(len(thetas)):
+        q = p.model.matrix(coefs[b])
+        r = O.laplace(q, p.a, family, y, want_var=True, **kw)
+        assert out["iters"][b] == r["iters"]
+        assert abs(out["mlik"][b] - r["mlik"]) <= 1e-9 * abs(r["logdet_post"])
+        assert rel(out["x"][b], r["x"]) < 1e-7
+        assert rel(out["var"][b], r["var"]) < 1e-7
+
+
+def test_glm_adjoint_includes_implicit_term():
+    """Poisson: d mlik / d theta including the -1/2 d log|Q_post|/dx dx*/dtheta term, vs FD."""
+    p, y = _poisson_problem()
+    lm = LaplaceModel(p.model, a=p.a, family="poisson", y=y, max_batch=2)
+    t = np.array([-0.7, 1.2])
+
+    def mlik_oracle(tt):
+        q = p.model.matrix(models.spde_coefs(tt[0], tt[1])[0])
+        return O.laplace(q, p.a, "poisson", y, tol=1e-10)["mlik"]
+
+    c, dc = models.spde_coefs(t[0], t[1])
+    out = lm.eval(c[None], gradient=True)
+    T = 3
+    g = dc @ (0.5 * out["trP"][0, :T] - 0.5 * out["trQ"][0, :T] - 0.5 * out["xMx"][0, :T] + 0.5 * out["zMx"][0, :T])
+    h = 1e-4
+    fd = np.array([(mlik_oracle(t + h * e) - mlik_oracle(t - h * e)) / (2 * h) for e in np.eye(2)])
+    # the reference's Newton tolerance (1e-5) leaves O(tol) stationarity error in the envelope term
+    assert np.max(np.abs(g - fd)) <= 2e-3 * max(1.0, np.max(np.abs(fd))), (g, fd)

@@ -153,7 +153,10 @@ def test_singular_matrix_reports_singular():
 
 def test_nonfinite_values_report_singular():
     q = grid_laplacian(8, 8)
-    q.data[3] = np.nan
+    # a lower-triangle entry (entries with row < col are never read, as in the reference)
+    col = 5
+    p = q.indptr[col] + int(np.searchsorted(q.indices[q.indptr[col]:q.indptr[col + 1]], col))
+    q.data[p] = np.nan
     s = GpuSolver()
     with pytest.raises(_lib.InlaError) as e:
         s.factorize(q)

@@ -18,7 +18,7 @@ ROOT = Path(__file__).resolve().parent.parent
 
 def header_symbols():
     text = (ROOT / "include" / "inla_b200.h").read_text()
-    return sorted(set(re.findall(r"^\s*(?:const char\*|int64_t|int|void)\s+(inla_\w+)\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:const char\*|int64_t|int|void|double)\s+(inla_\w+)\(", text, re.M)))
 
 
 def test_library_exports_every_declared_symbol():
