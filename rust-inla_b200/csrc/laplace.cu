@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(NT) k_gauss_dll(int64_t nobs, const double* __
   if (threadIdx.x == 0) out[b] = s;
 }
 
-__global__ void k_mul(int64_t len, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ c) {
+__global__ void k_mul(int64_t len, const double* a, const double* b, double* c) {  // c may alias a
   const int bb = blockIdx.y;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x)
     c[(int64_t)bb * len + i] = a[(int64_t)bb * len + i] * b[(int64_t)bb * len + i];

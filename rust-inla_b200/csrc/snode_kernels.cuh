@@ -72,7 +72,11 @@ __global__ void k_fill_panels_model(DevSym S, const int* __restrict__ pmap, int 
       if (pdiag[src]) v += diag_add;
       if (wb) {
         double acc = 0.0;
-        for (int q = cptr[src]; q < cptr[src + 1]; ++q) acc += wb[cobs[q]] * cprod[q];
+        // design.rs:100-115: observations with a zero or non-finite weight are skipped
+        for (int q = cptr[src]; q < cptr[src + 1]; ++q) {
+          const double wq = wb[cobs[q]];
+          if (wq != 0.0 && isfinite(wq)) acc += wq * cprod[q];
+        }
         v += acc;
       }
     }
