@@ -1,0 +1,391 @@
+#!/usr/bin/env python
+"""Headline benchmark: full INLA fit of the SPDE Matern model on the jittered
+200x200 mesh (n = 40 000 latent, 20 000 Gaussian observations, three
+hyperparameters, CCD integration with 15 theta-points), FP64.
+
+One step = one full fit (mode search + Hessian + CCD + marginal variances of
+every latent node) with the batched + adjoint path: BFGS on exact adjoint
+gradients with a batched line search, the reference's FD Hessian stencil in
+one batch, the 15 CCD nodes in one batch. The metric is theta-evaluations
+per second (full Laplace evaluations at one theta-point per second) and fit
+seconds; the plain GPU drop-in (the reference's control flow: Nelder-Mead,
+sequential FD Hessian, sequential CCD, one theta-point per evaluation) is
+timed in the same run.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: each rank fits an independent replica (replicas only, no
+collective on the data path); value = all ranks' theta-evaluations / max
+rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "rust-inla_b200"))
+
+METRIC = "INLA fit s & θ-evals/s, SPDE n≈40k: batched+adjoint vs plain GPU (var ≤1e-8)"
+UNIT = "theta-evals/s"
+THETA0 = [0.0, 0.0, 0.0]  # reference defaults: family 0.0, spde [log tau, log kappa] = [0, 0]
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nx", type=int, default=200)
+    ap.add_argument("--nobs", type=int, default=20000)
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain GPU drop-in fit")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0, help="bounded CPU-baseline sample")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return ws, rank, local, pg
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        if not self.proc:
+            return out
+        time.sleep(0.3)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.file.flush()
+        rows = [r.split(",") for r in Path(self.file.name).read_text().strip().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip().lower().startswith("active"):
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if sm:
+            out = {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                   "samples": len(sm)}
+        return out
+
+
+def make_problem(args):
+    from inla_b200 import models
+
+    return models.make_spde_problem(nx=args.nx, n_obs=args.nobs)
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the CPU oracle (restatement of the reference's CPU path)
+# ---------------------------------------------------------------------------
+
+def cpu_theta_evals(p, seconds: float, threads: int, perm):
+    """Oracle Laplace evaluations at CCD-like theta-points, `threads` in parallel
+    (the reference runs CCD nodes through Rayon). Returns (evals, elapsed)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    rng = np.random.default_rng(7)
+    base = np.array([4.6, -3.9, 2.65])
+
+    def one(k):
+        th = base + 0.05 * rng.standard_normal(3)
+        O.spde_neg_log_posterior(th, p.model, p.a, p.y, perm=perm)
+        return 1
+
+    done = 0
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        while time.perf_counter() - t0 < seconds or done == 0:
+            done += sum(ex.map(one, range(threads)))
+    return done, time.perf_counter() - t0
+
+
+def gpu_perm(p):
+    """AMD permutation of the same symbolic analysis the GPU uses (host-only)."""
+    from inla_b200 import GpuSolver
+
+    s = GpuSolver()
+    s.analyze(p.model.pattern)
+    return s.perm()
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return 0
+    p = make_problem(args)
+    threads = os.cpu_count() or 1
+    perm = gpu_perm(p)
+    per_step = max(args.cpu_seconds / max(args.steps, 1), 1.0)
+    for _ in range(args.warmup):
+        cpu_theta_evals(p, 0.0, threads, perm)
+    ev, el = 0, 0.0
+    for _ in range(args.steps):
+        e, t = cpu_theta_evals(p, per_step, threads, perm)
+        ev += e
+        el += t
+    value = ev / el
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded SPDE 200x200 jittered mesh, 20k Gaussian obs)",
+            "config": {"workload": "spde_200x200_gaussian_ccd15", "n_latent": int(p.model.n), "n_obs": args.nobs,
+                       "theta_dim": 3},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{ev} oracle Laplace evaluations (prior + posterior LDL^T, solve, mlik) at "
+                                       f"CCD-like theta-points, {threads} threads, AMD ordering"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def measured_dgemm_tflops(torch):
+    """cuBLAS DGEMM throughput on this GPU (FP64 denominator of the roofline)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def factor_roofline(p, torch, B=15, reps=10):
+    """Average duration of the batched supernodal LDL^T launch sequence (B theta-points),
+    CUDA events on the launching stream; algorithmic FLOPs F = sum_j (c_j^2 + 2 c_j) per problem."""
+    import ctypes as C
+
+    from inla_b200 import BatchSolver, GpuSolver, models
+    from inla_b200._lib import check, lib
+
+    c, _ = models.spde_coefs(math.log(0.02), math.log(14.14))
+    q = (p.model.matrix(c) + 100.0 * (p.a.T @ p.a)).tocsc()
+    q.sort_indices()
+    bs = BatchSolver(q, max_batch=B)
+    s = GpuSolver()
+    s.analyze(q)
+    cc = s.colcounts().astype(np.float64) - 1.0
+    flops = float(np.sum(cc * cc + 2 * cc))
+    vals = torch.tensor(np.tile(q.data, (B, 1)), device="cuda")
+    ld = torch.zeros(B, dtype=torch.float64, device="cuda")
+    st = torch.zeros(B, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def fac():
+        check(lib().inla_batch_factorize_dev(bs._h, B, C.c_void_p(vals.data_ptr()), C.c_void_p(ld.data_ptr()),
+                                             C.c_void_p(st.data_ptr()), C.c_void_p(stream)))
+
+    for _ in range(3):
+        fac()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fac()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    del bs
+    return {"flops_per_launch": flops * B, "ms": ms, "nnz_l": int(s.info()["nnz_l"])}
+
+
+def run_ours(args, ws, rank, local, dist):
+    import torch
+
+    from inla_b200 import lib as _l  # noqa: F401
+    from inla_b200._lib import lib
+    from inla_b200.laplace import LaplaceModel
+
+    torch.cuda.set_device(local)
+    p = make_problem(args)
+    lm = LaplaceModel(p.model, a=p.a, family="gaussian", y=p.y, max_batch=25)
+    fit_kw = dict(mode_search="bfgs", batched=True, tol=1e-4)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        lm.fit(THETA0, **fit_kw)
+    barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    launches0 = lib().inla_kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    evals = 0
+    fits = []
+    for _ in range(args.steps):
+        r = lm.fit(THETA0, **fit_kw)
+        evals += r["n_evals"]
+        fits.append(r)
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    launches = lib().inla_kernel_launches() - launches0
+    ms_total = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms_total, float(evals)], dtype=torch.float64, device="cuda")
+        tmax = t.clone()
+        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        ms_total, evals_all = float(tmax[0]), float(t[1])
+    else:
+        evals_all = float(evals)
+    value = evals_all / (ms_total * 1e-3)
+    last = fits[-1]
+
+    # e2e through the public API with host buffers: model creation (symbolic
+    # analysis + H2D of components, projector, data) + fit + D2H of results
+    e2e_ms, e2e_evals = 0.0, 0
+    nnz = p.model.pattern.nnz
+    h2d = 8 * (p.model.comp_values.size + p.y.size + p.a.nnz) + 8 * (p.model.n + 1 + nnz) + 8 * (
+        p.a.shape[0] + 1 + p.a.nnz)
+    d2h = 8 * (2 * p.model.n + 3 + 9 + 64 * 4 + 6)
+    for _ in range(args.e2e_steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        lm2 = LaplaceModel(p.model, a=p.a, family="gaussian", y=p.y, max_batch=25)
+        r2 = lm2.fit(THETA0, **fit_kw)
+        lm2.close()
+        e2e_ms += (time.perf_counter() - t0) * 1e3
+        e2e_evals += r2["n_evals"]
+    e2e_value = e2e_evals / (e2e_ms * 1e-3)
+
+    if rank != 0:
+        return 0
+
+    # plain GPU drop-in: the reference's control flow, one theta-point per evaluation
+    plain = None
+    if not args.no_plain:
+        t0 = time.perf_counter()
+        rp = lm.fit(THETA0, mode_search="nm", batched=False)
+        plain_s = time.perf_counter() - t0
+        plain = {"fit_s": plain_s, "theta_evals": rp["n_evals"], "theta_evals_per_s": rp["n_evals"] / plain_s,
+                 "mode": rp["mode"].tolist(), "mode_iters": rp["mode_iters"],
+                 "max_rel_var_diff_vs_batched": float(np.max(np.abs(rp["var"] - last["var"]) / rp["var"])),
+                 "max_abs_mean_diff_vs_batched": float(np.max(np.abs(rp["mean"] - last["mean"])))}
+
+    # roofline: the batched supernodal factorization (dominant FP64 contraction)
+    peak = measured_dgemm_tflops(torch)
+    fr = factor_roofline(p, torch)
+    achieved = fr["flops_per_launch"] / (fr["ms"] * 1e-3) / 1e12
+    roof = {"bound": "tensor", "kernel": "batched supernodal LDL^T (B=15 theta-points, sequence of level kernels)",
+            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64; the measured-peaks file has no FP64 entry)",
+            "traffic": None, "ms_per_launch": fr["ms"], "flops_per_launch": fr["flops_per_launch"]}
+
+    cpu = None
+    if ws == 1 and args.cpu_seconds > 0:
+        threads = os.cpu_count() or 1
+        ev, el = cpu_theta_evals(p, args.cpu_seconds, threads, gpu_perm(p))
+        cpu = {"value": ev / el, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{ev} oracle Laplace evaluations (prior + posterior LDL^T, solve, mlik) at CCD-like "
+                         f"theta-points in {el:.1f}s, {threads} threads, same AMD ordering"}
+
+    fit_s = ms_total * 1e-3 / args.steps
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded SPDE 200x200 jittered mesh, 20k Gaussian obs; inputs resident in HBM)",
+            "config": {"workload": "spde_200x200_gaussian_ccd15", "n_latent": int(p.model.n), "n_obs": args.nobs,
+                       "theta_dim": 3, "ccd_points": 15, "theta0": THETA0, "parallelism": f"replicas{ws}",
+                       "l2": "working set (front buffers, B x 213 MB) larger than L2; no flush needed",
+                       "mode_search": "bfgs+adjoint, batched line search"},
+            "fit_s": fit_s, "theta_evals_per_fit": evals / args.steps, "mode": last["mode"].tolist(),
+            "plain_gpu": plain,
+            "speedup_vs_plain_gpu": (plain["fit_s"] / fit_s) if plain else None,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "fit_s": e2e_ms * 1e-3 / max(args.e2e_steps, 1)},
+            "gpu_launches": int(launches), "clocks": clocks, "roofline": roof, "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    ws, rank, local, dist = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            return run_reference(args, ws, rank)
+        return run_ours(args, ws, rank, local, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())
