@@ -23,6 +23,9 @@
 #include "devsym.hpp"
 
 namespace inla {
+// Internal linkage: every translation unit that launches these kernels owns
+// its own copy (no cross-file kernel symbols).
+namespace {
 
 __device__ __forceinline__ int sn_k(const DevSym& S, int s) { return S.first[s + 1] - S.first[s]; }
 __device__ __forceinline__ int sn_m(const DevSym& S, int s) { return S.rowptr[s + 1] - S.rowptr[s]; }
@@ -665,4 +668,5 @@ __global__ void k_pattern_values(int64_t nnz, const int64_t* __restrict__ spos, 
   }
 }
 
+}  // namespace
 }  // namespace inla
