@@ -154,3 +154,22 @@ def test_glm_adjoint_includes_implicit_term():
     fd = np.array([(mlik_oracle(t + h * e) - mlik_oracle(t - h * e)) / (2 * h) for e in np.eye(2)])
     # the reference's Newton tolerance (1e-5) leaves O(tol) stationarity error in the envelope term
     assert np.max(np.abs(g - fd)) <= 2e-3 * max(1.0, np.max(np.abs(fd))), (g, fd)
+
+
+def test_torch_autograd_function(spde_small):
+    """torch.autograd.Function: backward returns the adjoint gradient; batched forward equals single."""
+    import torch
+
+    from inla_b200.autograd import log_posterior
+
+    p, lm = spde_small
+    th = torch.tensor(THETAS[0], dtype=torch.float64, requires_grad=True)
+    v = log_posterior(th, lm)
+    v.backward()
+    _, g = _spde_grad(lm, THETAS[0])
+    np.testing.assert_allclose(th.grad.numpy(), g, rtol=1e-12, atol=1e-12)
+    tb = torch.tensor(np.stack(THETAS), dtype=torch.float64, requires_grad=True)
+    vb = log_posterior(tb, lm)
+    assert abs(float(vb[0]) - float(v)) <= 1e-12 * abs(float(v))
+    vb.sum().backward()
+    np.testing.assert_allclose(tb.grad[0].numpy(), g, rtol=1e-12, atol=1e-12)
