@@ -219,6 +219,26 @@ int inla_fit(inla_laplace* h, int m, const double* theta0, inla_theta_map_fn map
              void* user, const inla_fit_options* opt, double* mode, double* hessian, double* latent_mean,
              double* latent_var, double* node_theta, double* node_weight, double* info);
 
+/* ------------------------------------------------------------------------
+ * Dense LDL^T + log|Q| + solve that allocates no device memory.
+ * No counterpart in the reference: it exists for host programs that embed
+ * this library but must own every device allocation themselves (pool
+ * allocators, framework plugins handed pre-sized buffers, code where a
+ * cudaMalloc/cudaFree would synchronize the device or is not allowed while
+ * other work is captured or scheduled). All pointers are caller-owned device
+ * memory: d_q is the n x n matrix (column-major, both triangles; the lower
+ * one is read), d_rhs / d_x are length n (both NULL to skip the solve),
+ * d_logdet / d_status receive log|Q| and the pivot status (0 ok, nonzero =
+ * singular or non-finite pivot). Work is queued on `stream` (NULL = default
+ * stream) without synchronizing. Limit: n <= 1024 (larger n returns
+ * INLA_ERR_DIM_MISMATCH). The factor lives in a fixed 8 MiB static device
+ * scratch per GPU, shared by every call and kept until process exit: calls
+ * whose GPU work overlaps race on it. The first call on a device resolves
+ * the scratch addresses; make it before any stream capture.
+ * ---------------------------------------------------------------------- */
+int inla_dense_ldlt_solve_noalloc(int n, const double* d_q, const double* d_rhs, double* d_x, double* d_logdet,
+                                  int* d_status, void* stream);
+
 /* Built-in theta map of the SPDE Gaussian model: theta = [log prec_eps, log tau, log kappa],
  * components [C~, G, G C~^-1 G] (crates/inla_stats/src/spde.rs:70-140). */
 int inla_theta_map_spde(const double* theta, int m, double* coef, double* dcoef, double* p1scale,

@@ -98,6 +98,7 @@ SIGNATURES = [
     ("inla_log_prior_set", C.c_double, [DP, C.c_int, DP, P]),
     ("inla_fit", C.c_int, [P, C.c_int, DP, P, P, P, P, DP, DP, DP, DP, DP, DP, DP]),
     ("inla_theta_map_spde", C.c_int, [DP, C.c_int, DP, DP, DP, DP, P]),
+    ("inla_dense_ldlt_solve_noalloc", C.c_int, [C.c_int, P, P, P, P, P, P]),
 ]
 
 
