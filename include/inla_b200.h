@@ -134,7 +134,9 @@ int inla_batch_diag_inv(inla_batch* h, int B, double* diag);
 int inla_batch_selinv_pattern(inla_batch* h, int B, double* sigma);
 
 /* Device-pointer variants, ordered on `stream` (a cudaStream_t; NULL = the
- * handle's own stream). Inputs/outputs live in device memory. */
+ * legacy default stream): the work starts after everything already queued on
+ * `stream` and later work queued on `stream` waits for it. The calls do not
+ * synchronize the host. Inputs/outputs live in device memory. */
 int inla_batch_factorize_dev(inla_batch* h, int B, const double* d_values, double* d_logdet, int* d_status,
                              void* stream);
 int inla_batch_solve_dev(inla_batch* h, int B, double* d_x, void* stream);
@@ -203,7 +205,8 @@ typedef int (*inla_theta_map_fn)(const double* theta, int m, double* coef, doubl
 typedef double (*inla_log_prior_fn)(const double* theta, int m, double* grad, void* user);
 
 typedef struct {
-  int mode_search; /* 0 Nelder-Mead on values (reference), 1 BFGS on adjoint gradients */
+  int mode_search; /* 0 Nelder-Mead on values (reference), 1 BFGS on adjoint gradients,
+                      2 batched Newton (adjoint gradients + FD-of-gradient Hessians, one batch per iteration) */
   int batched;     /* 0 one theta-point per evaluation (plain drop-in), 1 batched theta-sets */
   int strategy;    /* 0 CCD, 1 grid (m <= 2; CCD f0 = 2.5 above) */
   double f0;       /* CCD f0 / grid step (0 = 1.0) */

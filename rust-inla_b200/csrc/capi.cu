@@ -46,11 +46,13 @@ void check_pattern(int64_t n, const int64_t* colptr, const int64_t* rowidx) {
 }
 
 // Stream bridge: order our stream after `ext`, and `ext` after our work.
+// ext == NULL is the legacy default stream (it does not synchronize with the
+// handle's non-blocking stream by itself, so it is bridged like any other).
 struct StreamBridge {
   cudaStream_t own, ext;
   cudaEvent_t ev;
   StreamBridge(cudaStream_t own_, cudaStream_t ext_) : own(own_), ext(ext_), ev(nullptr) {
-    if (ext && ext != own) {
+    if (ext != own) {
       INLA_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
       INLA_CUDA(cudaEventRecord(ev, ext));
       INLA_CUDA(cudaStreamWaitEvent(own, ev, 0));

@@ -2,6 +2,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <stdexcept>
@@ -384,6 +386,120 @@ void InlaDriver::bfgs(std::vector<double>& x, const FitOptions& opt, int& iters)
 }
 
 // ---------------------------------------------------------------------------
+// Batched Newton: every iteration evaluates the line-search candidates
+// x + a p (a = 1, 1/2, 1/4) together with their +-h stencils in one batch, so
+// the accepted point comes with its exact adjoint gradient and a central-FD
+// Hessian of that gradient.
+// ---------------------------------------------------------------------------
+
+void InlaDriver::eval_stencils(const std::vector<std::vector<double>>& centers, double h, std::vector<double>& f,
+                               std::vector<double>& g, std::vector<double>& H) {
+  const int m = m_, C = (int)centers.size(), per = 1 + 2 * m;
+  std::vector<double> pts;
+  pts.reserve((size_t)C * per * m);
+  for (const auto& c : centers) {
+    pts.insert(pts.end(), c.begin(), c.end());
+    for (int i = 0; i < m; ++i)
+      for (double s : {1.0, -1.0}) {
+        std::vector<double> t(c);
+        t[i] += s * h;
+        pts.insert(pts.end(), t.begin(), t.end());
+      }
+  }
+  const int K = C * per;
+  std::vector<double> fk(K), gk((size_t)K * m);
+  evaluate(K, pts.data(), true, true, fk.data(), gk.data());
+  f.assign(C, 0.0);
+  g.assign((size_t)C * m, 0.0);
+  H.assign((size_t)C * m * m, 0.0);
+  for (int c = 0; c < C; ++c) {
+    const int b0 = c * per;
+    f[c] = fk[b0];
+    bool bad = !(fk[b0] < 1e11);
+    for (int i = 0; i < m; ++i) g[(size_t)c * m + i] = gk[(size_t)b0 * m + i];
+    for (int i = 0; i < m; ++i) {
+      const int kp = b0 + 1 + 2 * i, km = kp + 1;
+      if (!(fk[kp] < 1e11) || !(fk[km] < 1e11)) bad = true;
+      for (int j = 0; j < m; ++j)
+        H[(size_t)c * m * m + i * m + j] = (gk[(size_t)kp * m + j] - gk[(size_t)km * m + j]) / (2.0 * h);
+    }
+    double* Hc = &H[(size_t)c * m * m];
+    for (int i = 0; i < m; ++i)
+      for (int j = i + 1; j < m; ++j) Hc[i * m + j] = Hc[j * m + i] = 0.5 * (Hc[i * m + j] + Hc[j * m + i]);
+    if (bad) f[c] = 1e12;
+  }
+}
+
+void InlaDriver::newton(std::vector<double>& x, const FitOptions& opt, int& iters) {
+  const int m = m_;
+  const double h = 1e-3;
+  std::vector<double> f1, g, H;
+  eval_stencils({x}, h, f1, g, H);
+  double f = f1[0];
+  double delta = 1.0;  // trust bound on max |step| (theta lives on log scales)
+  iters = 0;
+  for (int it = 0; it < opt.max_iter; ++it) {
+    iters = it + 1;
+    double gmax = 0.0;
+    for (double gi : g) gmax = std::max(gmax, std::fabs(gi));
+    if (gmax < opt.tol) break;
+    // Newton direction on the |eigenvalue|-modified Hessian
+    std::vector<double> lam, V;
+    symmetric_eigen(H, m, lam, V);
+    double lmax = 0.0;
+    for (double l : lam) lmax = std::max(lmax, std::fabs(l));
+    std::vector<double> p(m, 0.0);
+    for (int j = 0; j < m; ++j) {
+      const double l = std::max(std::fabs(lam[j]), 1e-8 * std::max(lmax, 1e-300));
+      double vg = 0.0;
+      for (int i = 0; i < m; ++i) vg += V[i * m + j] * g[i];
+      for (int i = 0; i < m; ++i) p[i] -= V[i * m + j] * vg / l;
+    }
+    double pmax = 0.0, slope = 0.0;
+    for (int i = 0; i < m; ++i) {
+      pmax = std::max(pmax, std::fabs(p[i]));
+      slope += p[i] * g[i];
+    }
+    const bool capped = pmax > delta;
+    if (capped) {
+      for (double& v : p) v *= delta / pmax;
+      slope *= delta / pmax;
+    }
+    static const double kA[3] = {1.0, 0.5, 0.25};
+    std::vector<std::vector<double>> cands;
+    for (double a : kA) {
+      std::vector<double> c(x);
+      for (int i = 0; i < m; ++i) c[i] += a * p[i];
+      cands.push_back(c);
+    }
+    std::vector<double> fc, gc, Hc;
+    eval_stencils(cands, h, fc, gc, Hc);
+    int best = -1;
+    for (int k = 0; k < 3; ++k)
+      if (fc[k] < 1e11 && fc[k] <= f + 1e-4 * kA[k] * slope) {
+        best = k;
+        break;
+      }
+    if (best < 0) {
+      delta *= 0.25;
+      if (delta < 1e-8) break;
+      continue;
+    }
+    const double fprev = f;
+    x = cands[best];
+    f = fc[best];
+    g.assign(gc.begin() + (size_t)best * m, gc.begin() + (size_t)(best + 1) * m);
+    H.assign(Hc.begin() + (size_t)best * m * m, Hc.begin() + (size_t)(best + 1) * m * m);
+    if (std::getenv("INLA_DEBUG"))
+      std::fprintf(stderr, "newton it=%d f=%.10g |g|=%.3g delta=%.3g alpha=%.3g capped=%d\n", it, f, gmax, delta,
+                   kA[best], (int)capped);
+    if (best == 0 && capped) delta = std::min(4.0 * delta, 8.0);
+    else if (best > 0) delta = std::max(0.25, kA[best] * std::min(pmax, delta));
+    if (std::fabs(fprev - f) < 1e-12 * (1.0 + std::fabs(f))) break;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Hessians
 // ---------------------------------------------------------------------------
 
@@ -461,7 +577,8 @@ void InlaDriver::fit(const double* theta0, const FitOptions& opt, FitResult& out
   std::vector<double> mode(theta0, theta0 + m);
   int iters = 0;
   if (opt.mode_search == 0) nelder_mead(mode, opt, iters);
-  else bfgs(mode, opt, iters);
+  else if (opt.mode_search == 1) bfgs(mode, opt, iters);
+  else newton(mode, opt, iters);
   out.mode = mode;
   out.mode_iters = iters;
 

@@ -27,7 +27,7 @@ using ThetaMap = std::function<int(const double* theta, double* coef, double* dc
 using LogPrior = std::function<double(const double* theta, double* grad)>;
 
 struct FitOptions {
-  int mode_search = 0;  // 0 Nelder-Mead (reference), 1 BFGS with adjoint gradients
+  int mode_search = 0;  // 0 Nelder-Mead (reference), 1 BFGS on adjoint gradients, 2 batched Newton
   int batched = 0;      // 0: one theta-point per evaluation; 1: batched theta-sets
   int strategy = 0;     // 0 CCD, 1 grid
   double f0 = 1.0;      // CCD f0 (reference default 1.0) / grid step
@@ -59,6 +59,9 @@ class InlaDriver {
  private:
   void nelder_mead(std::vector<double>& theta, const FitOptions& opt, int& iters);
   void bfgs(std::vector<double>& theta, const FitOptions& opt, int& iters);
+  void newton(std::vector<double>& theta, const FitOptions& opt, int& iters);
+  void eval_stencils(const std::vector<std::vector<double>>& centers, double h, std::vector<double>& f,
+                     std::vector<double>& g, std::vector<double>& H);
   void fd_hessian(const std::vector<double>& mode, double h, bool batched, std::vector<double>& H);
   void grad_hessian(const std::vector<double>& mode, double h, bool batched, std::vector<double>& H);
 

@@ -4,6 +4,7 @@
 
 #include "gpu_factor.hpp"
 #include "snode_kernels.cuh"
+#include "snode_large.cuh"
 
 namespace inla {
 
@@ -109,13 +110,27 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
   logdet_.alloc(max_batch_);
   status_.alloc(max_batch_);
 
+  {
+    int64_t nlmax = 1, ppmax = 1;
+    for (const LevelPlan& P : levels_) {
+      nlmax = std::max<int64_t>(nlmax, (int64_t)P.large.size());
+      ppmax = std::max<int64_t>(ppmax, (int64_t)P.si_large.size() * cdiv(P.mmax_si_large, kSiT));
+    }
+    dcache_.alloc((size_t)nlmax * max_batch_ * kB64 * kB64);
+    ppart_.alloc((size_t)ppmax * max_batch_ * kB64 * kB64);
+  }
   set_smem(k_factor_small<128>, kSmallA * kSmallA * 8);
   set_smem(k_factor_small<256>, kSmallB * kSmallB * 8);
   set_smem(k_selinv_small<256>, (kSiSmall * kSiSmall * 2) * 8);
+  set_smem(k_panel64, kPanelSmem);
+  set_smem(k_si_gemm64, kSiGemmSmem);
+  set_smem(k_si_diag64, kSiDiagSmem);
   INLA_CUDA(cudaStreamSynchronize(stream_));
 }
 
-GpuFactor::~GpuFactor() = default;
+GpuFactor::~GpuFactor() {
+  for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second.exec);
+}
 
 void GpuFactor::plan_levels() {
   const Symbolic& S = sym_;
@@ -181,15 +196,16 @@ void GpuFactor::run_factor_levels(int B) {
     if (!P.large.empty()) {
       const int nl = (int)P.large.size();
       const int* lst = d_lists_.p + P.off_large;
-      k_gather_large<<<dim3(nl, B, cdiv(P.mmax_large, kGatherCW)), 128, 0, stream_>>>(ds_, lst, F_.p, fs);
+      k_gather8<<<dim3(nl, B, cdiv(P.mmax_large, kGatherCols)), 256, 0, stream_>>>(ds_, lst, F_.p, fs);
       ++launches_;
-      for (int j0 = 0; j0 < P.kmax_large; j0 += kNB) {
-        k_diag_large<<<dim3(nl, B), 128, 0, stream_>>>(ds_, lst, j0, F_.p, fs);
+      for (int j0 = 0; j0 < P.kmax_large; j0 += kB64) {
         int rows = P.mmax_large - j0;
-        k_trsm_large<<<dim3(nl, B, cdiv(rows, kTrsmRows)), kTrsmRows, 0, stream_>>>(ds_, lst, j0, F_.p, fs);
-        int nt = cdiv(rows, kUT);
-        k_update_large<<<dim3(nl, B, nt * (nt + 1) / 2), 128, 0, stream_>>>(ds_, lst, j0, F_.p, fs);
-        launches_ += 3;
+        k_panel64<<<dim3(nl, B, std::max(1, cdiv(rows, kPanelRows))), 256, kPanelSmem, stream_>>>(
+            ds_, lst, j0, F_.p, fs, dcache_.p);
+        int nt = cdiv(rows, kUT64);
+        k_update64<<<dim3(nl, B, std::max(1, nt * (nt + 1) / 2)), 128, 0, stream_>>>(ds_, lst, j0, F_.p, fs,
+                                                                                   dcache_.p);
+        launches_ += 2;
       }
     }
   }
@@ -197,24 +213,64 @@ void GpuFactor::run_factor_levels(int B) {
   ++launches_;
 }
 
+template <class Body>
+void GpuFactor::launch_cached(const std::vector<int64_t>& key, Body&& body) {
+  if (!use_graphs_) {
+    body();
+    INLA_CUDA(cudaGetLastError());
+    return;
+  }
+  auto it = graphs_.find(key);
+  if (it == graphs_.end()) {
+    const int64_t before = launches_;
+    INLA_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    try {
+      body();
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(stream_, &g);
+      if (g) cudaGraphDestroy(g);
+      launches_ = before;
+      throw;
+    }
+    cudaGraph_t g = nullptr;
+    INLA_CUDA(cudaStreamEndCapture(stream_, &g));
+    cudaGraphExec_t ex = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) throw CudaError(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e), (int)e);
+    it = graphs_.emplace(key, GraphEntry{ex, launches_ - before}).first;
+    launches_ = before;
+  }
+  INLA_CUDA(cudaGraphLaunch(it->second.exec, stream_));
+  launches_ += it->second.nkernels;
+}
+
 void GpuFactor::factor_values(const double* d_vals, int B) {
   if (B < 1 || B > max_batch_) throw std::runtime_error("batch size out of range");
-  k_fill_panels<<<dim3((unsigned)sym_.nsuper, B), 128, 0, stream_>>>(ds_, d_pmap_.p, d_vals, nnz_, F_.p, ftotal_);
-  ++launches_;
-  run_factor_levels(B);
-  INLA_CUDA(cudaGetLastError());
+  launch_cached({1, B, (int64_t)(uintptr_t)d_vals}, [&] {
+    k_fill_panels<<<dim3((unsigned)sym_.nsuper, B), 128, 0, stream_>>>(ds_, d_pmap_.p, d_vals, nnz_, F_.p, ftotal_);
+    ++launches_;
+    run_factor_levels(B);
+  });
 }
 
 void GpuFactor::factor_model(int ncomp, const double* d_comp, const double* d_coef, double diag_add,
                              const unsigned char* d_pdiag, const int* d_cptr, const int* d_cobs,
                              const double* d_cprod, const double* d_w, int64_t wstride, int B) {
   if (B < 1 || B > max_batch_) throw std::runtime_error("batch size out of range");
-  k_fill_panels_model<<<dim3((unsigned)sym_.nsuper, B), 128, 0, stream_>>>(ds_, d_pmap_.p, ncomp, d_comp, nnz_, d_coef,
-                                                                          diag_add, d_pdiag, d_cptr, d_cobs, d_cprod,
-                                                                          d_w, wstride, F_.p, ftotal_);
-  ++launches_;
-  run_factor_levels(B);
-  INLA_CUDA(cudaGetLastError());
+  int64_t dbits;
+  std::memcpy(&dbits, &diag_add, sizeof(dbits));
+  launch_cached({2, B, ncomp, (int64_t)(uintptr_t)d_comp, (int64_t)(uintptr_t)d_coef, dbits,
+                 (int64_t)(uintptr_t)d_pdiag, (int64_t)(uintptr_t)d_cptr, (int64_t)(uintptr_t)d_cobs,
+                 (int64_t)(uintptr_t)d_cprod, (int64_t)(uintptr_t)d_w, wstride},
+                [&] {
+                  k_fill_panels_model<<<dim3((unsigned)sym_.nsuper, B), 128, 0, stream_>>>(
+                      ds_, d_pmap_.p, ncomp, d_comp, nnz_, d_coef, diag_add, d_pdiag, d_cptr, d_cobs, d_cprod, d_w,
+                      wstride, F_.p, ftotal_);
+                  ++launches_;
+                  run_factor_levels(B);
+                });
 }
 
 void GpuFactor::solve(double* d_x, int64_t xstride, int B) {
@@ -222,27 +278,32 @@ void GpuFactor::solve(double* d_x, int64_t xstride, int B) {
   const int n = (int)sym_.n;
   const int64_t fs = ftotal_;
   dim3 gp(cdiv(n, 256) > 1024 ? 1024 : cdiv(n, 256), B);
-  k_permute_in<<<gp, 256, 0, stream_>>>(n, d_perm_.p, d_x, xstride, xp_.p);
-  ++launches_;
-  for (const LevelPlan& P : levels_) {
-    k_fwd<128><<<dim3((unsigned)P.all.size(), B), 128, P.mmax_all * 8, stream_>>>(
-        ds_, d_lists_.p + P.off_all, F_.p, fs, xp_.p, ub_.p, std::max<int64_t>(usum_, 1));
+  launch_cached({3, B, (int64_t)(uintptr_t)d_x, xstride}, [&] {
+    k_permute_in<<<gp, 256, 0, stream_>>>(n, d_perm_.p, d_x, xstride, xp_.p);
     ++launches_;
-  }
-  for (int l = (int)levels_.size() - 1; l >= 0; --l) {
-    const LevelPlan& P = levels_[l];
-    k_bwd<128><<<dim3((unsigned)P.all.size(), B), 128, P.mmax_all * 8, stream_>>>(ds_, d_lists_.p + P.off_all,
-                                                                                  F_.p, fs, xp_.p);
+    for (const LevelPlan& P : levels_) {
+      k_fwd32<128><<<dim3((unsigned)P.all.size(), B), 128, P.mmax_all * 8, stream_>>>(
+          ds_, d_lists_.p + P.off_all, F_.p, fs, xp_.p, ub_.p, std::max<int64_t>(usum_, 1));
+      ++launches_;
+    }
+    for (int l = (int)levels_.size() - 1; l >= 0; --l) {
+      const LevelPlan& P = levels_[l];
+      k_bwd32<128><<<dim3((unsigned)P.all.size(), B), 128, P.mmax_all * 8, stream_>>>(ds_, d_lists_.p + P.off_all,
+                                                                                    F_.p, fs, xp_.p);
+      ++launches_;
+    }
+    k_permute_out<<<gp, 256, 0, stream_>>>(n, d_perm_.p, xp_.p, d_x, xstride);
     ++launches_;
-  }
-  k_permute_out<<<gp, 256, 0, stream_>>>(n, d_perm_.p, xp_.p, d_x, xstride);
-  ++launches_;
-  INLA_CUDA(cudaGetLastError());
+  });
 }
 
 void GpuFactor::selinv(int B) {
   if (B < 1 || B > max_batch_) throw std::runtime_error("batch size out of range");
-  Sg_.alloc((size_t)max_batch_ * ftotal_);
+  Sg_.alloc((size_t)max_batch_ * ftotal_);  // outside any capture
+  launch_cached({4, B}, [&] { selinv_levels(B); });
+}
+
+void GpuFactor::selinv_levels(int B) {
   const int64_t fs = ftotal_;
   for (int l = (int)levels_.size() - 1; l >= 0; --l) {
     const LevelPlan& P = levels_[l];
@@ -256,19 +317,19 @@ void GpuFactor::selinv(int B) {
       const int nl = (int)P.si_large.size();
       const int* lst = d_lists_.p + P.off_si_large;
       if (P.rmax_si_large > 0) {
-        k_si_gather_large<<<dim3(nl, B, cdiv(P.rmax_si_large, kGatherCW)), 128, 0, stream_>>>(ds_, lst, Sg_.p, fs);
+        k_si_gather8<<<dim3(nl, B, cdiv(P.rmax_si_large, kGatherCols)), 256, 0, stream_>>>(ds_, lst, Sg_.p, fs);
         ++launches_;
       }
-      int nblk = cdiv(P.kmax_si_large, kNB);
+      const int nblk = cdiv(P.kmax_si_large, kB64);
+      const int ptiles = cdiv(P.mmax_si_large, kSiT);
       for (int jb = 0; jb < nblk; ++jb) {
-        k_si_panel_large<<<dim3(nl, B, cdiv(P.mmax_si_large, kSiRows)), kSiRows, 0, stream_>>>(ds_, lst, jb, F_.p,
-                                                                                              Sg_.p, fs);
-        k_si_diag_large<<<dim3(nl, B), 256, 0, stream_>>>(ds_, lst, jb, F_.p, Sg_.p, fs);
+        k_si_gemm64<<<dim3(nl, B, ptiles), 128, kSiGemmSmem, stream_>>>(ds_, lst, jb, F_.p, Sg_.p, fs, ppart_.p,
+                                                                        ptiles);
+        k_si_diag64<<<dim3(nl, B), 256, kSiDiagSmem, stream_>>>(ds_, lst, jb, F_.p, Sg_.p, fs, ppart_.p, ptiles);
         launches_ += 2;
       }
     }
   }
-  INLA_CUDA(cudaGetLastError());
 }
 
 void GpuFactor::extract_diag(double* d_out, int64_t ostride, int B) {

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -106,9 +107,23 @@ class GpuFactor {
   // Launch counters (kernels issued by this engine since construction).
   int64_t launches() const { return launches_; }
 
+  // Replay the fixed launch sequences (fill+factor, solve, selected inverse)
+  // from CUDA graphs captured on first use (default on).
+  void set_use_graphs(bool on) { use_graphs_ = on; }
+
  private:
   void plan_levels();
   void run_factor_levels(int B);
+  void selinv_levels(int B);
+  template <class Body>
+  void launch_cached(const std::vector<int64_t>& key, Body&& body);
+
+  struct GraphEntry {
+    cudaGraphExec_t exec;
+    int64_t nkernels;
+  };
+  std::map<std::vector<int64_t>, GraphEntry> graphs_;
+  bool use_graphs_ = true;
 
   Symbolic sym_;
   int max_batch_;
@@ -119,7 +134,7 @@ class GpuFactor {
   DBuf<int> d_first_, d_rowptr_, d_rows_, d_relx_, d_child_ptr_, d_child_list_, d_parent_, d_uoff_, d_perm_;
   DBuf<int64_t> d_fptr_, d_lptr_, d_dpos_, spos_, spos_full_;
   DBuf<int> d_pmap_, d_lists_;
-  DBuf<double> F_, Sg_, xp_, ub_, logdet_;
+  DBuf<double> F_, Sg_, xp_, ub_, logdet_, dcache_, ppart_;
   DBuf<int> status_;
   int64_t launches_ = 0;
 };

@@ -1,0 +1,812 @@
+// Large-front kernels (fronts with more than 128 rows), 64-column blocks.
+//
+// Factorization, per block J = [j0, j0+w) of a front (right-looking):
+//   k_panel64   every CTA factors the w x w diagonal block in shared memory
+//               (the redundant O(w^3) work removes a serial launch), CTA 0
+//               writes it back, each CTA solves its 128 rows
+//               L_i = F_i L_JJ^-T D_J^-1 (one thread per row);
+//   k_update64  F[i,j] -= sum_{t in J} L_it d_t L_jt on 64x64 tiles of the lower
+//               trailing matrix, FP64 tensor-core mma.sync.m8n8k4 tiles.
+// Selected inverse, per block J from right to left (A = rows after J):
+//   k_si_gemm64 G = Sigma[A,A] L[A,J] (tensor-core tiles, Sigma read from its
+//               lower triangle with coalesced loads on both sides of the
+//               diagonal), X = -G L_JJ^-1 per row, Sigma[A,J] = X, and the
+//               tile's partial P = L[I,J]^T X[I,J];
+//   k_si_diag64 P = sum of partials (fixed order), then the in-block Takahashi
+//               recurrence S_ij = -P_ji - sum_{l in J, l>j} L_lj S_li,
+//               S_jj = 1/d_j - P_jj - sum_{l in J, l>j} L_lj S_lj.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "devsym.hpp"
+
+namespace inla {
+namespace {
+
+constexpr int kB64 = 64;       // block-column width
+constexpr int kPanelRows = 128;  // rows per panel CTA (one thread per row)
+constexpr int kPanelSmem = (2 * kB64 * (kB64 + 1) + kB64 * 129 + 2 * kB64) * 8;
+constexpr int kSiGemmSmem = 3 * 64 * (kB64 + 1) * 8;
+constexpr int kSiDiagSmem = 3 * kB64 * (kB64 + 1) * 8;
+
+__device__ __forceinline__ int lg_k(const DevSym& S, int s) { return S.first[s + 1] - S.first[s]; }
+__device__ __forceinline__ int lg_m(const DevSym& S, int s) { return S.rowptr[s + 1] - S.rowptr[s]; }
+
+__device__ __forceinline__ void mma884(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+// Unblocked LDL^T of the w x w block held in smem (leading dimension ld), one
+// barrier per pivot: step j reads column j unscaled and updates columns > j;
+// column j is scaled after the barrier, concurrently with step j+1, which
+// touches columns > j only.
+__device__ __forceinline__ void smem_ldlt(double* sm, int w, int ld) {
+  for (int j = 0; j < w; ++j) {
+    const double dinv = 1.0 / sm[j + j * ld];
+    const int r = w - j - 1;
+    const double* cj = sm + j + 1 + j * ld;
+    for (int e = threadIdx.x; e < r * r; e += blockDim.x) {
+      const int tt = e / r, ii = e - tt * r;
+      if (ii >= tt) sm[(j + 1 + ii) + (j + 1 + tt) * ld] -= cj[ii] * cj[tt] * dinv;
+    }
+    __syncthreads();
+    for (int i = j + 1 + threadIdx.x; i < w; i += blockDim.x) sm[i + j * ld] *= dinv;
+  }
+  __syncthreads();
+}
+
+// Register-resident LDL^T of a w x w block (w <= 64) with 128 threads:
+// thread t owns row i = t % 64 and the columns j = t / 64 + 2b (b < 32) of it.
+// Pivot p: the owners of column p publish it to a double-buffered smem column
+// (one barrier per pivot), then every thread updates its entries (i, j),
+// p < j <= i, with v_ij -= (v_ip / d_p) v_jp. On exit Ds (ld 65) holds unit L
+// below the diagonal and D on it; piv[p] = d_p.
+__device__ __forceinline__ void reg_ldlt64(const double* __restrict__ A, int64_t lda, int w, double* Ds,
+                                           double* colbuf, double* piv) {
+  const int t = threadIdx.x, i = t & 63, q = t >> 6;
+  double v[32];
+#pragma unroll
+  for (int b = 0; b < 32; ++b) {
+    const int j = q + 2 * b;
+    v[b] = (i < w && j <= i) ? A[i + (int64_t)j * lda] : 0.0;
+  }
+  for (int p = 0; p < w; ++p) {
+    double* col = colbuf + (p & 1) * 64;
+    if ((p & 1) == q && i >= p && i < w) {
+      double val = 0.0;
+#pragma unroll
+      for (int b = 0; b < 32; ++b)
+        if (b == (p >> 1)) val = v[b];
+      col[i] = val;
+    }
+    __syncthreads();
+    const double dp = col[p];
+    if (t == 0) piv[p] = dp;
+    const double lip = (i > p && i < w) ? col[i] / dp : 0.0;
+#pragma unroll
+    for (int b = 0; b < 32; ++b) {
+      const int j = q + 2 * b;
+      if (j > p && j <= i) v[b] -= lip * col[j];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int b = 0; b < 32; ++b) {
+    const int j = q + 2 * b;
+    if (i < w && j <= i) Ds[i + j * (kB64 + 1)] = (j == i) ? piv[j] : v[b] / piv[j];
+  }
+  __syncthreads();
+}
+
+// 64x64 LDL^T with 256 threads, entries register-resident: thread t owns the
+// lower-triangle entries e = t + 256 s (s < 9) of the block (row-major
+// triangular numbering). Pivot p: owners of column p publish it (double-
+// buffered smem column, one barrier), then every owned entry (i, j), j > p,
+// takes v -= col[i] col[j] / d_p. On exit A (smem, ld 65) holds unit L below the
+// diagonal and D on it (entries outside the w x w block are left untouched).
+__device__ __forceinline__ void tri_index(int e, int& i, int& j) {
+  // row-major lower triangle: e = i (i + 1) / 2 + j
+  int r = (int)((sqrtf(8.0f * (float)e + 1.0f) - 1.0f) * 0.5f);
+  while ((r + 1) * (r + 2) / 2 <= e) ++r;
+  while (r * (r + 1) / 2 > e) --r;
+  i = r;
+  j = e - r * (r + 1) / 2;
+}
+
+__device__ __forceinline__ void ldlt64_256(double* A, int w, double* colbuf /*[2][64]*/) {
+  const int t = threadIdx.x;
+  double v[9];
+  int ei[9], ej[9];
+#pragma unroll
+  for (int s = 0; s < 9; ++s) {
+    const int e = t + 256 * s;
+    int i = 64, j = 64;
+    if (e < 2080) tri_index(e, i, j);
+    ei[s] = i;
+    ej[s] = j;
+    v[s] = (i < w && j < w) ? A[i + j * (kB64 + 1)] : 0.0;
+  }
+  for (int p = 0; p < w; ++p) {
+    double* col = colbuf + (p & 1) * 64;
+#pragma unroll
+    for (int s = 0; s < 9; ++s)
+      if (ej[s] == p && ei[s] < w) col[ei[s]] = v[s];
+    __syncthreads();
+    const double dinv = 1.0 / col[p];
+#pragma unroll
+    for (int s = 0; s < 9; ++s)
+      if (ej[s] > p && ei[s] < w) v[s] -= col[ei[s]] * col[ej[s]] * dinv;
+  }
+  __syncthreads();
+  // diagonal first, then L = v / d_j
+#pragma unroll
+  for (int s = 0; s < 9; ++s)
+    if (ei[s] < w && ei[s] == ej[s]) A[ei[s] + ej[s] * (kB64 + 1)] = v[s];
+  __syncthreads();
+#pragma unroll
+  for (int s = 0; s < 9; ++s)
+    if (ei[s] < w && ei[s] > ej[s]) A[ei[s] + ej[s] * (kB64 + 1)] = v[s] / A[ej[s] + ej[s] * (kB64 + 1)];
+  __syncthreads();
+}
+
+// Li = L^-1 of the unit lower w x w block L (smem, ld 65; Li zero-padded to 64x64).
+// 256 threads: 4 per column, the dot product of each substitution step split
+// across the 4 lanes and combined with shuffles.
+__device__ __forceinline__ void linv64(const double* L, double* Li, int w) {
+  const int sub = threadIdx.x & 3;
+  const unsigned gmask = 0xFu << ((threadIdx.x & 31) & ~3);  // the 4 lanes of this column
+  constexpr int ld = kB64 + 1;
+  for (int c = threadIdx.x >> 2; c < kB64; c += blockDim.x >> 2) {
+    for (int r = sub; r < kB64; r += 4) Li[r + c * ld] = (r == c && c < w) ? 1.0 : 0.0;
+    __syncwarp(gmask);
+    if (c < w) {
+      for (int r = c + 1; r < w; ++r) {
+        double a = 0.0;
+        for (int u = c + sub; u < r; u += 4) a += L[r + u * ld] * Li[u + c * ld];
+        a += __shfl_xor_sync(gmask, a, 1);
+        a += __shfl_xor_sync(gmask, a, 2);
+        if (sub == 0) Li[r + c * ld] = -a;
+        __syncwarp(gmask);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Extend-add of the children's updates into parent columns [c0, c1) (the
+// update part of those columns is zeroed first). Work is flattened over
+// (source column, row) pairs so each thread keeps several loads in flight;
+// targets are distinct within one child, children are added in fixed order.
+constexpr int kGatherCols = 8;
+__global__ void __launch_bounds__(256) k_gather8(DevSym S, const int* __restrict__ list, double* __restrict__ F,
+                                                 int64_t fstride) {
+  const int s = list[blockIdx.x], b = blockIdx.y;
+  const int k = lg_k(S, s), m = lg_m(S, s);
+  const int c0 = blockIdx.z * kGatherCols;
+  if (c0 >= m) return;
+  const int c1 = min(c0 + kGatherCols, m);
+  double* Fb = F + (int64_t)b * fstride;
+  double* Fs = Fb + S.fptr[s];
+  {
+    const int z0 = max(c0, k);
+    const int nz = (c1 > z0) ? (c1 - z0) : 0;
+    for (int e = threadIdx.x; e < nz * m; e += blockDim.x) {
+      const int cc = z0 + e / m, row = e - (e / m) * m;
+      if (row >= cc) Fs[row + (int64_t)cc * m] = 0.0;
+    }
+  }
+  __syncthreads();
+  for (int q = S.child_ptr[s]; q < S.child_ptr[s + 1]; ++q) {
+    const int c = S.child_list[q];
+    const int kc = lg_k(S, c), mc = lg_m(S, c), rc = mc - kc;
+    const double* __restrict__ Uc = Fb + S.fptr[c] + (int64_t)kc * mc + kc;
+    const int* __restrict__ relc = S.relx + S.rowptr[c] + kc;
+    int lo, hi;
+    {
+      int a = 0, z = rc;
+      while (a < z) {
+        const int mid = (a + z) >> 1;
+        if (relc[mid] < c0) a = mid + 1;
+        else z = mid;
+      }
+      lo = a;
+      z = rc;
+      while (a < z) {
+        const int mid = (a + z) >> 1;
+        if (relc[mid] < c1) a = mid + 1;
+        else z = mid;
+      }
+      hi = a;
+    }
+    const int total = (hi - lo) * rc;
+    int e = threadIdx.x;
+    for (; e + 3 * (int)blockDim.x < total; e += 4 * blockDim.x) {
+      double v[4];
+      int64_t dst[4];
+      bool ok[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int ee = e + u * blockDim.x;
+        const int jj = lo + ee / rc, ii = ee - (ee / rc) * rc;
+        ok[u] = ii >= jj;
+        v[u] = ok[u] ? Uc[ii + (int64_t)jj * mc] : 0.0;
+        dst[u] = relc[ii] + (int64_t)relc[jj] * m;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (ok[u]) Fs[dst[u]] += v[u];
+    }
+    for (; e < total; e += blockDim.x) {
+      const int jj = lo + e / rc, ii = e - (e / rc) * rc;
+      if (ii >= jj) Fs[relc[ii] + (int64_t)relc[jj] * m] += Uc[ii + (int64_t)jj * mc];
+    }
+    __syncthreads();
+  }
+}
+
+// Sigma restricted to the below-rows of s, gathered from the parent's Sigma
+// front into the trailing block (lower triangle), columns [c0, c1) of it.
+__global__ void __launch_bounds__(256) k_si_gather8(DevSym S, const int* __restrict__ list, double* __restrict__ Sg,
+                                                    int64_t fstride) {
+  const int s = list[blockIdx.x], b = blockIdx.y;
+  const int k = lg_k(S, s), m = lg_m(S, s), r = m - k;
+  if (r == 0) return;
+  const int c0 = blockIdx.z * kGatherCols;
+  if (c0 >= r) return;
+  const int c1 = min(c0 + kGatherCols, r);
+  const int p = S.parent[s];
+  const int mp = lg_m(S, p);
+  const double* __restrict__ Sp = Sg + (int64_t)b * fstride + S.fptr[p];
+  double* Ss = Sg + (int64_t)b * fstride + S.fptr[s];
+  const int* __restrict__ rel = S.relx + S.rowptr[s] + k;
+  const int total = (c1 - c0) * r;
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int jj = c0 + e / r, ii = e - (e / r) * r;
+    if (ii < jj) continue;
+    const int pi = rel[ii], pj = rel[jj];
+    Ss[(k + ii) + (int64_t)(k + jj) * m] = pi >= pj ? Sp[pi + (int64_t)pj * mp] : Sp[pj + (int64_t)pi * mp];
+  }
+}
+
+// The factored diagonal block goes to dcache[(list index, problem)] (written by
+// CTA 0): the other CTAs of this launch still read the unfactored block from
+// the front, so it is copied into the front by k_update64 of the same step.
+// Each CTA: LDL^T of the diagonal block (register-resident), L_JJ^-1, then its
+// 128 rows X = F_rows (L_JJ^-T D^-1) as one tensor-core GEMM.
+__global__ void __launch_bounds__(256) k_panel64(DevSym S, const int* __restrict__ list, int j0,
+                                                 double* __restrict__ F, int64_t fstride,
+                                                 double* __restrict__ dcache) {
+  extern __shared__ double smem64[];
+  constexpr int ld = kB64 + 1;
+  double* Ds = smem64;                // [64][65] diagonal block, factored in place
+  double* Li = Ds + kB64 * ld;        // [64][65] L_JJ^-1, then B = L^-T D^-1 (Bm[u][t] at u + t*ld)
+  double* Fa = Li + kB64 * ld;        // [64 cols][129] rows of this CTA: Fa[t * 129 + r]
+  double* colbuf = Fa + kB64 * 129;   // [2][64]
+  const int s = list[blockIdx.x], b = blockIdx.y;
+  const int k = lg_k(S, s), m = lg_m(S, s);
+  if (j0 >= k) return;
+  const int w = min(kB64, k - j0);
+  const int r0 = j0 + w + blockIdx.z * kPanelRows;
+  if (blockIdx.z > 0 && r0 >= m) return;
+  double* Fs = F + (int64_t)b * fstride + S.fptr[s];
+  const double* D0 = Fs + j0 + (int64_t)j0 * m;
+  for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) {
+    const int c = e >> 6, r = e & 63;
+    Ds[r + c * ld] = (r < w && c < w && r >= c) ? D0[r + (int64_t)c * m] : 0.0;
+  }
+  const int rows = max(0, min(kPanelRows, m - r0));
+  for (int e = threadIdx.x; e < kB64 * kPanelRows; e += blockDim.x) {
+    const int c = e / kPanelRows, r = e - c * kPanelRows;
+    Fa[c * 129 + r] = (r < rows && c < w) ? Fs[(r0 + r) + (int64_t)(j0 + c) * m] : 0.0;
+  }
+  __syncthreads();
+  ldlt64_256(Ds, w, colbuf);
+  if (blockIdx.z == 0) {
+    double* dc = dcache + ((int64_t)blockIdx.x * gridDim.y + b) * (kB64 * kB64);
+    for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) {
+      const int c = e >> 6, r = e & 63;
+      dc[e] = (r < w && c < w) ? Ds[r + c * ld] : 0.0;
+    }
+  }
+  if (rows == 0) return;
+  linv64(Ds, Li, w);
+  // B[u][t] = Li[t][u] / d_t  (stored into Li's slot after a barrier: read all first)
+  double bv[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const int e = threadIdx.x + 256 * q, u = e & 63, t = e >> 6;
+    bv[q] = (t < w && u < w) ? Li[t + u * ld] / Ds[t + t * ld] : 0.0;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const int e = threadIdx.x + 256 * q, u = e & 63, t = e >> 6;
+    Li[u + t * ld] = bv[q];
+  }
+  __syncthreads();
+  // X (128 x 64) = Fa (128 x 64) * B (64 x 64); warp tile 32 x 32
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wr = (warp & 3) * 32, wc = (warp >> 2) * 32;
+  const int g = lane >> 2, tg = lane & 3;
+  double acc[4][4][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[a][q][0] = acc[a][q][1] = 0.0;
+#pragma unroll 4
+  for (int kk = 0; kk < kB64; kk += 4) {
+    double af[4], bf[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) af[a] = Fa[(kk + tg) * 129 + wr + a * 8 + g];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) bf[q] = Li[(kk + tg) + (wc + q * 8 + g) * ld];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) mma884(acc[a][q][0], acc[a][q][1], af[a], bf[q]);
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int r = wr + a * 8 + g, t = wc + q * 8 + tg * 2 + h;
+        if (r < rows && t < w) Fs[(r0 + r) + (int64_t)(j0 + t) * m] = acc[a][q][h];
+      }
+}
+
+constexpr int kUT64 = 64;
+__global__ void __launch_bounds__(128) k_update64(DevSym S, const int* __restrict__ list, int j0,
+                                                 double* __restrict__ F, int64_t fstride,
+                                                 const double* __restrict__ dcache) {
+  __shared__ double As[32][kUT64 + 1];  // As[t][i] = L[I0+i, j0+t0+t]
+  __shared__ double Bs[32][kUT64 + 1];  // Bs[t][j] = d_t L[J0+j, j0+t0+t]
+  __shared__ double dsh[kB64];
+  const int s = list[blockIdx.x], b = blockIdx.y;
+  const int k = lg_k(S, s), m = lg_m(S, s);
+  if (j0 >= k) return;
+  const int w = min(kB64, k - j0);
+  const int c = j0 + w;
+  const int T = m - c;
+  const double* dc = dcache + ((int64_t)blockIdx.x * gridDim.y + b) * (kB64 * kB64);
+  if (blockIdx.z == 0) {  // factored diagonal block -> front
+    double* D0 = F + (int64_t)b * fstride + S.fptr[s] + j0 + (int64_t)j0 * m;
+    for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+      const int cc = e / w, r = e - cc * w;
+      if (r >= cc) D0[r + (int64_t)cc * m] = dc[r + cc * kB64];
+    }
+  }
+  if (T <= 0) return;
+  for (int t = threadIdx.x; t < kB64; t += blockDim.x) dsh[t] = t < w ? dc[t + t * kB64] : 0.0;
+  const int nt = (T + kUT64 - 1) / kUT64;
+  const int tile = blockIdx.z;
+  if (tile >= nt * (nt + 1) / 2) return;
+  int J = 0, rem = tile;
+  while (rem >= nt - J) {
+    rem -= nt - J;
+    ++J;
+  }
+  const int I = J + rem;
+  const int I0 = c + I * kUT64, J0 = c + J * kUT64;
+  double* Fs = F + (int64_t)b * fstride + S.fptr[s];
+  const double* Lb = Fs + (int64_t)j0 * m;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wi = (warp & 1) * 32, wj = (warp >> 1) * 32;
+  const int g = lane >> 2, tg = lane & 3;
+  double acc[4][4][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[a][q][0] = acc[a][q][1] = 0.0;
+  for (int t0 = 0; t0 < w; t0 += 32) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < 32 * kUT64; e += blockDim.x) {
+      const int t = e / kUT64, ii = e - t * kUT64;
+      double av = 0.0, bv = 0.0;
+      if (t0 + t < w) {
+        const int64_t col = (int64_t)(t0 + t) * m;
+        if (I0 + ii < m) av = Lb[I0 + ii + col];
+        if (J0 + ii < m) bv = Lb[J0 + ii + col] * dsh[t0 + t];
+      }
+      As[t][ii] = av;
+      Bs[t][ii] = bv;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 32; kk += 4) {
+      double af[4], bf[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) af[a] = As[kk + tg][wi + a * 8 + g];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) bf[q] = Bs[kk + tg][wj + q * 8 + g];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) mma884(acc[a][q][0], acc[a][q][1], af[a], bf[q]);
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int i = I0 + wi + a * 8 + g;
+        const int j = J0 + wj + q * 8 + tg * 2 + h;
+        if (i < m && j < m && i >= j) Fs[i + (int64_t)j * m] -= acc[a][q][h];
+      }
+}
+
+// ---------------------------------------------------------------------------
+// triangular sweeps in 32-column blocks: the diagonal block is solved by one
+// warp with shuffles, the rows below it are updated by the whole CTA
+// (two barriers per block instead of one per column)
+// ---------------------------------------------------------------------------
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_fwd32(DevSym S, const int* __restrict__ list, const double* __restrict__ F,
+                                              int64_t fstride, double* __restrict__ xp, double* __restrict__ ub,
+                                              int64_t ustride) {
+  extern __shared__ double y[];
+  const int s = list[blockIdx.x], b = blockIdx.y;
+  const int k = lg_k(S, s), m = lg_m(S, s), f = S.first[s];
+  const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
+  double* xb = xp + (int64_t)b * S.n;
+  double* ubb = ub + (int64_t)b * ustride;
+  for (int t = threadIdx.x; t < m; t += NT) y[t] = t < k ? xb[f + t] : 0.0;
+  __syncthreads();
+  for (int q = S.child_ptr[s]; q < S.child_ptr[s + 1]; ++q) {
+    const int c = S.child_list[q];
+    const int kc = lg_k(S, c), rc = lg_m(S, c) - kc;
+    const int* relc = S.relx + S.rowptr[c] + kc;
+    const double* uc = ubb + S.uoff[c];
+    for (int t = threadIdx.x; t < rc; t += NT) y[relc[t]] += uc[t];
+    __syncthreads();
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int jb = 0; jb < k; jb += 32) {
+    const int wb = min(32, k - jb);
+    if (warp == 0) {
+      double Lrow[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        Lrow[j] = (j < lane && lane < wb) ? Fs[(jb + lane) + (int64_t)(jb + j) * m] : 0.0;
+      double yi = lane < wb ? y[jb + lane] : 0.0;
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const double yj = __shfl_sync(0xffffffffu, yi, j);
+        if (j < lane) yi -= Lrow[j] * yj;
+      }
+      if (lane < wb) y[jb + lane] = yi;
+    }
+    __syncthreads();
+    for (int r = jb + wb + threadIdx.x; r < m; r += NT) {
+      double a0 = 0.0, a1 = 0.0;
+      const double* Lr = Fs + r + (int64_t)jb * m;
+      int j = 0;
+      for (; j + 1 < wb; j += 2) {
+        a0 += Lr[(int64_t)j * m] * y[jb + j];
+        a1 += Lr[(int64_t)(j + 1) * m] * y[jb + j + 1];
+      }
+      if (j < wb) a0 += Lr[(int64_t)j * m] * y[jb + j];
+      y[r] -= a0 + a1;
+    }
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < m; t += NT) {
+    if (t < k) xb[f + t] = y[t] / Fs[t + (int64_t)t * m];
+    else ubb[S.uoff[s] + t - k] = y[t];
+  }
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_bwd32(DevSym S, const int* __restrict__ list, const double* __restrict__ F,
+                                              int64_t fstride, double* __restrict__ xp) {
+  extern __shared__ double x[];
+  const int s = list[blockIdx.x], b = blockIdx.y;
+  const int k = lg_k(S, s), m = lg_m(S, s), f = S.first[s];
+  const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
+  double* xb = xp + (int64_t)b * S.n;
+  const int* R = S.rows + S.rowptr[s];
+  for (int t = threadIdx.x; t < m; t += NT) x[t] = xb[R[t]];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nblk = (k + 31) / 32;
+  for (int bi = nblk - 1; bi >= 0; --bi) {
+    const int jb = bi * 32, wb = min(32, k - jb), i0 = jb + wb;
+    // x_j -= sum_{i >= i0} L_ij x_i for the block's columns (warp per column)
+    for (int j = jb + warp; j < jb + wb; j += NT / 32) {
+      const double* Lj = Fs + (int64_t)j * m;
+      double acc = 0.0;
+      for (int i = i0 + lane; i < m; i += 32) acc += Lj[i] * x[i];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) x[j] -= acc;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      // lane j holds x_{jb+j}; unit upper L_JJ^T solved from the last row up
+      double Lcol[32];
+#pragma unroll
+      for (int i = 0; i < 32; ++i)
+        Lcol[i] = (i > lane && i < wb && lane < wb) ? Fs[(jb + i) + (int64_t)(jb + lane) * m] : 0.0;
+      double xj = lane < wb ? x[jb + lane] : 0.0;
+#pragma unroll
+      for (int i = 31; i >= 0; --i) {
+        const double xi = __shfl_sync(0xffffffffu, xj, i);
+        if (i > lane) xj -= Lcol[i] * xi;
+      }
+      if (lane < wb) x[jb + lane] = xj;
+    }
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < k; t += NT) xb[f + t] = x[t];
+}
+
+// ---------------------------------------------------------------------------
+// selected inverse
+// ---------------------------------------------------------------------------
+
+// Sigma[row, col] of a front stored as its lower triangle (column-major, ld m)
+__device__ __forceinline__ double sig_lower(const double* Ss, int m, int row, int col) {
+  return row >= col ? Ss[row + (int64_t)col * m] : Ss[col + (int64_t)row * m];
+}
+
+constexpr int kSiT = 64;  // rows of A per CTA
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// ppart: [list index][b][tile][64*64] partial P blocks; ptiles = tiles per (front, b).
+// Shared memory: two chunk buffers (Sa + Lb each, double-buffered with
+// cp.async) and G; L_JJ and L[I,J] reuse chunk buffer 0 after the GEMM.
+__global__ void __launch_bounds__(128) k_si_gemm64(DevSym S, const int* __restrict__ list, int jb,
+                                                  const double* __restrict__ F, double* __restrict__ Sg,
+                                                  int64_t fstride, double* __restrict__ ppart, int ptiles) {
+  extern __shared__ double smem64[];
+  constexpr int kBuf = 64 * (kB64 + 1);  // doubles per chunk buffer (Sa[32][65] + Lb[32][65])
+  typedef double Row65[kB64 + 1];
+  Row65* Gs = reinterpret_cast<Row65*>(smem64 + 2 * kBuf);  // [64][65]: G, then X
+  Row65* Lt = reinterpret_cast<Row65*>(smem64);             // [64][65]: L[j0+u, j0+t]  (after the GEMM)
+  const int s = list[blockIdx.x], b = blockIdx.y;
+  const int k = lg_k(S, s), m = lg_m(S, s);
+  const int nblk = (k + kB64 - 1) / kB64;
+  if (jb >= nblk) return;
+  const int bi = nblk - 1 - jb;
+  const int j0 = bi * kB64, j1 = min(k, j0 + kB64), w = j1 - j0;
+  const int I0 = j1 + blockIdx.z * kSiT;
+  if (I0 >= m) return;
+  const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
+  double* Ss = Sg + (int64_t)b * fstride + S.fptr[s];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wi = (warp & 1) * 32, wj = (warp >> 1) * 32;
+  const int g = lane >> 2, tg = lane & 3;
+
+  // chunk loader: Sigma[I0.., l0..l0+32) (lower-triangle storage) and L[l0.., j0..j0+w)
+  auto load_chunk = [&](int l0, int buf) {
+    Row65* Sa = reinterpret_cast<Row65*>(smem64 + buf * kBuf);
+    Row65* Lb = reinterpret_cast<Row65*>(smem64 + buf * kBuf + 32 * (kB64 + 1));
+    if (I0 >= l0 + 31) {  // on/below the diagonal: stored at (i, l), coalesced over i
+      for (int e = threadIdx.x; e < 32 * kSiT; e += blockDim.x) {
+        const int l = e / kSiT, ii = e - l * kSiT, row = I0 + ii, col = l0 + l;
+        if (row < m && col < m) cp_async8(&Sa[l][ii], Ss + row + (int64_t)col * m);
+        else Sa[l][ii] = 0.0;
+      }
+    } else if (I0 + kSiT - 1 < l0) {  // above: read the transposed entry (l, i), coalesced over l
+      for (int e = threadIdx.x; e < 32 * kSiT; e += blockDim.x) {
+        const int ii = e / 32, l = e - ii * 32, row = I0 + ii, col = l0 + l;
+        if (row < m && col < m) cp_async8(&Sa[l][ii], Ss + col + (int64_t)row * m);
+        else Sa[l][ii] = 0.0;
+      }
+    } else {
+      for (int e = threadIdx.x; e < 32 * kSiT; e += blockDim.x) {
+        const int l = e / kSiT, ii = e - l * kSiT, row = I0 + ii, col = l0 + l;
+        if (row < m && col < m)
+          cp_async8(&Sa[l][ii], row >= col ? Ss + row + (int64_t)col * m : Ss + col + (int64_t)row * m);
+        else Sa[l][ii] = 0.0;
+      }
+    }
+    for (int e = threadIdx.x; e < 32 * kB64; e += blockDim.x) {
+      const int t = e / 32, l = e - t * 32;
+      if (t < w && l0 + l < m) cp_async8(&Lb[l][t], Fs + (l0 + l) + (int64_t)(j0 + t) * m);
+      else Lb[l][t] = 0.0;
+    }
+    cp_async_commit();
+  };
+
+  double acc[4][4][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[a][q][0] = acc[a][q][1] = 0.0;
+  const int nch = (m - j1 + 31) / 32;
+  load_chunk(j1, 0);
+  for (int c = 0; c < nch; ++c) {
+    if (c + 1 < nch) {
+      load_chunk(j1 + 32 * (c + 1), (c + 1) & 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const Row65* Sa = reinterpret_cast<const Row65*>(smem64 + (c & 1) * kBuf);
+    const Row65* Lb = reinterpret_cast<const Row65*>(smem64 + (c & 1) * kBuf + 32 * (kB64 + 1));
+#pragma unroll
+    for (int kk = 0; kk < 32; kk += 4) {
+      double af[4], bf[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) af[a] = Sa[kk + tg][wi + a * 8 + g];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) bf[q] = Lb[kk + tg][wj + q * 8 + g];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) mma884(acc[a][q][0], acc[a][q][1], af[a], bf[q]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) Gs[wi + a * 8 + g][wj + q * 8 + tg * 2 + h] = acc[a][q][h];
+  // X = -G L_JJ^-1 as a tensor-core GEMM with the explicit inverse of the unit
+  // lower diagonal block
+  double* Lc = smem64;          // L_JJ, column-major ld 65 (chunk buffer 0)
+  double* Li = smem64 + kBuf;   // L_JJ^-1 (chunk buffer 1)
+  for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) {
+    const int c = e >> 6, r = e & 63;
+    Lc[r + c * (kB64 + 1)] = (r < w && c < w && r > c) ? Fs[(j0 + r) + (int64_t)(j0 + c) * m] : 0.0;
+  }
+  __syncthreads();
+  linv64(Lc, Li, w);
+  {
+    double xa[4][4][2];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) xa[a][q][0] = xa[a][q][1] = 0.0;
+#pragma unroll 4
+    for (int kk = 0; kk < kB64; kk += 4) {
+      double af[4], bf[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) af[a] = Gs[wi + a * 8 + g][kk + tg];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) bf[q] = Li[(kk + tg) + (wj + q * 8 + g) * (kB64 + 1)];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) mma884(xa[a][q][0], xa[a][q][1], af[a], bf[q]);
+    }
+    __syncthreads();  // all reads of G done before X overwrites it
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int ii = wi + a * 8 + g, t = wj + q * 8 + tg * 2 + h;
+          const double xv = -xa[a][q][h];
+          Gs[ii][t] = xv;
+          if (I0 + ii < m && t < w) Ss[(I0 + ii) + (int64_t)(j0 + t) * m] = xv;
+        }
+  }
+  __syncthreads();
+  // partial P[j][i] = sum_{rows l of this tile} L[I0+l, j0+j] X[l, i]  (tensor-core tiles)
+  const int rows = min(kSiT, m - I0);
+  Row65* Lij = Lt;  // Lij[l][j] = L[I0+l, j0+j]
+  for (int e = threadIdx.x; e < kSiT * kB64; e += blockDim.x) {
+    const int j = e / kSiT, l = e - j * kSiT;
+    Lij[l][j] = (l < rows && j < w) ? Fs[(I0 + l) + (int64_t)(j0 + j) * m] : 0.0;
+  }
+  __syncthreads();
+  double pa[4][4][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) pa[a][q][0] = pa[a][q][1] = 0.0;
+  const int wr = (warp & 1) * 32, wc = (warp >> 1) * 32;  // output rows j, cols i
+#pragma unroll 4
+  for (int kk = 0; kk < kSiT; kk += 4) {
+    double af[4], bf[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) af[a] = Lij[kk + tg][wr + a * 8 + g];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) bf[q] = Gs[kk + tg][wc + q * 8 + g];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) mma884(pa[a][q][0], pa[a][q][1], af[a], bf[q]);
+  }
+  double* pp = ppart + (((int64_t)blockIdx.x * gridDim.y + b) * ptiles + blockIdx.z) * (kB64 * kB64);
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) pp[(wr + a * 8 + g) * kB64 + wc + q * 8 + tg * 2 + h] = pa[a][q][h];
+}
+
+__global__ void __launch_bounds__(256) k_si_diag64(DevSym S, const int* __restrict__ list, int jb,
+                                                  const double* __restrict__ F, double* __restrict__ Sg,
+                                                  int64_t fstride, const double* __restrict__ ppart, int ptiles) {
+  // Sigma_JJ = L^-T (D^-1 L^-1 - P), L = L_JJ unit lower, P = L[A,J]^T Sigma[A,J]
+  // (the closed form of the in-block Takahashi recurrence), with L^-1 from
+  // linv64 and the product as a tensor-core GEMM.
+  extern __shared__ double smem64[];
+  constexpr int ld = kB64 + 1;
+  double* Pm = smem64;            // P, then M = D^-1 L^-1 - P  (Pm[r + c*ld] = entry (r, c))
+  double* Ld = Pm + kB64 * ld;    // L_JJ with D on the diagonal
+  double* Li = Ld + kB64 * ld;    // L_JJ^-1
+  const int s = list[blockIdx.x], b = blockIdx.y;
+  const int k = lg_k(S, s), m = lg_m(S, s);
+  const int nblk = (k + kB64 - 1) / kB64;
+  if (jb >= nblk) return;
+  const int bi = nblk - 1 - jb;
+  const int j0 = bi * kB64, j1 = min(k, j0 + kB64), w = j1 - j0;
+  const int ntiles = (m - j1 + kSiT - 1) / kSiT;
+  const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
+  double* Ss = Sg + (int64_t)b * fstride + S.fptr[s];
+  const double* pp = ppart + ((int64_t)blockIdx.x * gridDim.y + b) * ptiles * (kB64 * kB64);
+  for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) {
+    const int j = e >> 6, i = e & 63;  // partials are stored row-major: pp[j*64 + i] = P[j][i]
+    double acc = 0.0;
+    for (int z = 0; z < ntiles; ++z) acc += pp[(int64_t)z * kB64 * kB64 + e];
+    Pm[j + i * ld] = acc;
+    const int c = e >> 6, r = e & 63;
+    Ld[r + c * ld] = (r < w && c < w && r >= c) ? Fs[(j0 + r) + (int64_t)(j0 + c) * m] : 0.0;
+  }
+  __syncthreads();
+  linv64(Ld, Li, w);
+  for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) {
+    const int c = e >> 6, r = e & 63;
+    Pm[r + c * ld] = (r < w && c < w) ? Li[r + c * ld] / Ld[r + r * ld] - Pm[r + c * ld] : 0.0;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp < 4) {
+    const int wr = (warp & 1) * 32, wc = (warp >> 1) * 32;
+    const int g = lane >> 2, tg = lane & 3;
+    double acc[4][4][2];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[a][q][0] = acc[a][q][1] = 0.0;
+#pragma unroll 4
+    for (int kk = 0; kk < kB64; kk += 4) {
+      double af[4], bf[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) af[a] = Li[(kk + tg) + (wr + a * 8 + g) * ld];  // (L^-1)^T
+#pragma unroll
+      for (int q = 0; q < 4; ++q) bf[q] = Pm[(kk + tg) + (wc + q * 8 + g) * ld];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) mma884(acc[a][q][0], acc[a][q][1], af[a], bf[q]);
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int r = wr + a * 8 + g, c = wc + q * 8 + tg * 2 + h;
+          if (r < w && c < w && r >= c) Ss[(j0 + r) + (int64_t)(j0 + c) * m] = acc[a][q][h];
+        }
+  }
+}
+
+}  // namespace
+}  // namespace inla

@@ -1,0 +1,93 @@
+"""Workload driver for profiling the hot-path kernels (run under ncu).
+
+    python -m inla_b200.profile_ops --nx 200 --batch 15 --op factor|solve|selinv|all [--reps R]
+    python -m inla_b200.profile_ops --nx 200 --batch 21 --op laplace-grad
+
+``factor``/``solve``/``selinv`` run the batched supernodal kernels on the SPDE
+posterior precision ``Q(theta) + 100 A^T A`` (theta at the generating values);
+``laplace-grad`` runs one batched Laplace evaluation with the adjoint trace
+pieces (what one Newton iteration of the batched fit launches). Timings printed
+here are CUDA-event times on the launching stream.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import sys
+from pathlib import Path
+
+import numpy as np
+
+sys.path.insert(0, str(Path(__file__).resolve().parent.parent))
+
+
+def main():
+    import torch
+
+    from inla_b200 import BatchSolver, models
+    from inla_b200._lib import check, lib
+    from inla_b200.laplace import LaplaceModel
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--nx", type=int, default=200)
+    ap.add_argument("--batch", type=int, default=15)
+    ap.add_argument("--op", default="all")
+    ap.add_argument("--reps", type=int, default=1)
+    ap.add_argument("--warmup", type=int, default=1)
+    a = ap.parse_args()
+    p = models.make_spde_problem(nx=a.nx, n_obs=a.nx * a.nx // 2)
+    B = a.batch
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def timed(fn):
+        for _ in range(a.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / a.reps
+
+    out = {"nx": a.nx, "B": B}
+    if a.op in ("factor", "solve", "selinv", "all"):
+        c, _ = models.spde_coefs(math.log(0.02), math.log(14.14))
+        q = (p.model.matrix(c) + 100.0 * (p.a.T @ p.a)).tocsc()
+        q.sort_indices()
+        bs = BatchSolver(q, max_batch=B)
+        vals = torch.tensor(np.tile(q.data, (B, 1)), device="cuda")
+        ld = torch.zeros(B, dtype=torch.float64, device="cuda")
+        st = torch.zeros(B, dtype=torch.int32, device="cuda")
+        x = torch.ones(B, q.shape[0], dtype=torch.float64, device="cuda")
+        dg = torch.zeros_like(x)
+
+        def fac():
+            check(lib().inla_batch_factorize_dev(bs._h, B, C.c_void_p(vals.data_ptr()), C.c_void_p(ld.data_ptr()),
+                                                 C.c_void_p(st.data_ptr()), C.c_void_p(stream)))
+
+        def sol():
+            check(lib().inla_batch_solve_dev(bs._h, B, C.c_void_p(x.data_ptr()), C.c_void_p(stream)))
+
+        def sel():
+            check(lib().inla_batch_diag_inv_dev(bs._h, B, C.c_void_p(dg.data_ptr()), C.c_void_p(stream)))
+
+        fac()
+        for name, fn in (("factor", fac), ("solve", sol), ("selinv", sel)):
+            if a.op in (name, "all"):
+                out[name + "_ms"] = timed(fn)
+        del bs
+    if a.op == "laplace-grad":
+        lm = LaplaceModel(p.model, a=p.a, family="gaussian", y=p.y, max_batch=B)
+        th = np.array([4.6, -3.9, 2.6]) + 0.01 * np.random.default_rng(0).standard_normal((B, 3))
+        coefs = np.stack([models.spde_coefs(t[1], t[2])[0] for t in th])
+        scale = np.exp(th[:, 0])
+        out["laplace_grad_ms"] = timed(lambda: lm.eval(coefs, scale, gradient=True, mode=False))
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -56,10 +56,11 @@ def test_integration_parity_at_fixed_nodes(problem):
     assert abs(r["mlik"] - ref["mlik"]) < 1e-8 * abs(ref["mlik"])
 
 
-def test_batched_adjoint_fit_matches_plain(problem):
+@pytest.mark.parametrize("search", ["bfgs", "newton"])
+def test_batched_adjoint_fit_matches_plain(problem, search):
     p, lm = problem
     plain = lm.fit(THETA0, mode_search="nm", batched=False)
-    fast = lm.fit(THETA0, mode_search="bfgs", batched=True, tol=1e-5)
+    fast = lm.fit(THETA0, mode_search=search, batched=True, tol=1e-5)
     f = oracle_f(p)
     # BFGS on exact gradients reaches the optimum at least as well as NM
     assert f(fast["mode"]) <= f(plain["mode"]) + 1e-6
