@@ -18,6 +18,11 @@ struct DevSym {
   const int* uoff = nullptr;       // ns+1 : offsets of the per-supernode update vectors (sum r)
   const int64_t* dpos = nullptr;   // n : front offset of D_j
   const int* perm = nullptr;       // n : perm[new] = old
+  // 64 x 64 inverse-block cache of the large fronts: block (s, j0 / 64) of
+  // problem b at linv + (b * lstride + (lbo[s] + j0 / 64) * 4096); lbo[s] = -1
+  // for fronts that have no cached blocks.
+  const int* lbo = nullptr;        // ns
+  int64_t lstride = 0;
 };
 
 constexpr int kStatusOk = 0;

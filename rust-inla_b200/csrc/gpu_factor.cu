@@ -102,6 +102,42 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
   ds_.dpos = d_dpos_.p;
   ds_.perm = d_perm_.p;
 
+  // inverse-block cache: one 64 x 64 block per 64 pivot columns of every large front
+  {
+    std::vector<int> lbo(ns, -1);
+    int64_t nblk = 0;
+    for (int64_t s = 0; s < ns; ++s) {
+      const int64_t k = S.sn_first[s + 1] - S.sn_first[s], m = S.sn_rowptr[s + 1] - S.sn_rowptr[s];
+      if (m > kSmallB) {
+        lbo[s] = (int)nblk;
+        nblk += cdiv(k, kB64);
+      }
+    }
+    d_lbo_.upload(lbo, stream_);
+    ds_.lbo = d_lbo_.p;
+    ds_.lstride = nblk * kB64 * kB64;
+    linv_.alloc((size_t)max_batch_ * std::max<int64_t>(ds_.lstride, 1));
+  }
+  // value-fill chunks over the compact panel numbering
+  {
+    ntot_ = S.sn_lptr[ns];
+    nfill_ = std::max(1, cdiv(ntot_, kFillChunk));
+    std::vector<int> csn(nfill_ + 1);
+    int64_t s = 0;
+    for (int c = 0; c < nfill_; ++c) {
+      const int64_t e = (int64_t)c * kFillChunk;
+      while (s + 1 < ns && S.sn_lptr[s + 1] <= e) ++s;
+      csn[c] = (int)s;
+    }
+    csn[nfill_] = (int)(ns - 1);
+    d_csn_.upload(csn, stream_);
+  }
+  nldchunk_ = std::max(1, cdiv(n, kLogdetChunk));
+  ldpart_.alloc((size_t)max_batch_ * nldchunk_);
+  ldflag_.alloc((size_t)max_batch_ * nldchunk_);
+  ldticket_.alloc((size_t)max_batch_);
+  INLA_CUDA(cudaMemsetAsync(ldticket_.p, 0, sizeof(unsigned) * max_batch_, stream_));
+
   plan_levels();
 
   F_.alloc((size_t)max_batch_ * ftotal_);
@@ -119,10 +155,11 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
     dcache_.alloc((size_t)nlmax * max_batch_ * kB64 * kB64);
     ppart_.alloc((size_t)ppmax * max_batch_ * kB64 * kB64);
   }
-  set_smem(k_factor_small<128>, kSmallA * kSmallA * 8);
-  set_smem(k_factor_small<256>, kSmallB * kSmallB * 8);
+  set_smem(k_factor_small<128>, small_factor_smem(kSmallA));
+  set_smem(k_factor_small<256>, small_factor_smem(kSmallB));
   set_smem(k_selinv_small<256>, (kSiSmall * kSiSmall * 2) * 8);
   set_smem(k_panel64, kPanelSmem);
+  set_smem(k_update64, kUpdSmem);
   set_smem(k_si_gemm64, kSiGemmSmem);
   set_smem(k_si_diag64, kSiDiagSmem);
   INLA_CUDA(cudaStreamSynchronize(stream_));
@@ -185,12 +222,14 @@ void GpuFactor::run_factor_levels(int B) {
   for (const LevelPlan& P : levels_) {
     if (!P.small_a.empty()) {
       dim3 g((unsigned)P.small_a.size(), B);
-      k_factor_small<128><<<g, 128, P.mmax_a * P.mmax_a * 8, stream_>>>(ds_, d_lists_.p + P.off_small_a, F_.p, fs);
+      k_factor_small<128><<<g, 128, small_factor_smem(P.mmax_a), stream_>>>(ds_, d_lists_.p + P.off_small_a, F_.p,
+                                                                             fs);
       ++launches_;
     }
     if (!P.small_b.empty()) {
       dim3 g((unsigned)P.small_b.size(), B);
-      k_factor_small<256><<<g, 256, P.mmax_b * P.mmax_b * 8, stream_>>>(ds_, d_lists_.p + P.off_small_b, F_.p, fs);
+      k_factor_small<256><<<g, 256, small_factor_smem(P.mmax_b), stream_>>>(ds_, d_lists_.p + P.off_small_b, F_.p,
+                                                                             fs);
       ++launches_;
     }
     if (!P.large.empty()) {
@@ -201,15 +240,16 @@ void GpuFactor::run_factor_levels(int B) {
       for (int j0 = 0; j0 < P.kmax_large; j0 += kB64) {
         int rows = P.mmax_large - j0;
         k_panel64<<<dim3(nl, B, std::max(1, cdiv(rows, kPanelRows))), 256, kPanelSmem, stream_>>>(
-            ds_, lst, j0, F_.p, fs, dcache_.p);
+            ds_, lst, j0, F_.p, fs, dcache_.p, linv_.p);
         int nt = cdiv(rows, kUT64);
-        k_update64<<<dim3(nl, B, std::max(1, nt * (nt + 1) / 2)), 128, 0, stream_>>>(ds_, lst, j0, F_.p, fs,
-                                                                                   dcache_.p);
+        k_update64<<<dim3(nl, B, std::max(1, nt * (nt + 1) / 2)), 128, kUpdSmem, stream_>>>(ds_, lst, j0, F_.p, fs,
+                                                                                          dcache_.p);
         launches_ += 2;
       }
     }
   }
-  k_logdet<256><<<B, 256, 0, stream_>>>(ds_, F_.p, fs, logdet_.p, status_.p);
+  k_logdet_chunks<<<dim3(nldchunk_, B), 256, 0, stream_>>>(ds_, F_.p, fs, ldpart_.p, ldflag_.p, ldticket_.p,
+                                                           logdet_.p, status_.p);
   ++launches_;
 }
 
@@ -249,7 +289,8 @@ void GpuFactor::launch_cached(const std::vector<int64_t>& key, Body&& body) {
 void GpuFactor::factor_values(const double* d_vals, int B) {
   if (B < 1 || B > max_batch_) throw std::runtime_error("batch size out of range");
   launch_cached({1, B, (int64_t)(uintptr_t)d_vals}, [&] {
-    k_fill_panels<<<dim3((unsigned)sym_.nsuper, B), 128, 0, stream_>>>(ds_, d_pmap_.p, d_vals, nnz_, F_.p, ftotal_);
+    k_fill_panels<<<dim3(nfill_, B), 256, 0, stream_>>>(ds_, d_csn_.p, ntot_, d_pmap_.p, d_vals, nnz_, F_.p,
+                                                        ftotal_);
     ++launches_;
     run_factor_levels(B);
   });
@@ -265,9 +306,9 @@ void GpuFactor::factor_model(int ncomp, const double* d_comp, const double* d_co
                  (int64_t)(uintptr_t)d_pdiag, (int64_t)(uintptr_t)d_cptr, (int64_t)(uintptr_t)d_cobs,
                  (int64_t)(uintptr_t)d_cprod, (int64_t)(uintptr_t)d_w, wstride},
                 [&] {
-                  k_fill_panels_model<<<dim3((unsigned)sym_.nsuper, B), 128, 0, stream_>>>(
-                      ds_, d_pmap_.p, ncomp, d_comp, nnz_, d_coef, diag_add, d_pdiag, d_cptr, d_cobs, d_cprod, d_w,
-                      wstride, F_.p, ftotal_);
+                  k_fill_panels_model<<<dim3(nfill_, B), 256, 0, stream_>>>(
+                      ds_, d_csn_.p, ntot_, d_pmap_.p, ncomp, d_comp, nnz_, d_coef, diag_add, d_pdiag, d_cptr, d_cobs,
+                      d_cprod, d_w, wstride, F_.p, ftotal_);
                   ++launches_;
                   run_factor_levels(B);
                 });
@@ -324,8 +365,9 @@ void GpuFactor::selinv_levels(int B) {
       const int ptiles = cdiv(P.mmax_si_large, kSiT);
       for (int jb = 0; jb < nblk; ++jb) {
         k_si_gemm64<<<dim3(nl, B, ptiles), 128, kSiGemmSmem, stream_>>>(ds_, lst, jb, F_.p, Sg_.p, fs, ppart_.p,
-                                                                        ptiles);
-        k_si_diag64<<<dim3(nl, B), 256, kSiDiagSmem, stream_>>>(ds_, lst, jb, F_.p, Sg_.p, fs, ppart_.p, ptiles);
+                                                                        ptiles, linv_.p);
+        k_si_diag64<<<dim3(nl, B), 256, kSiDiagSmem, stream_>>>(ds_, lst, jb, F_.p, Sg_.p, fs, ppart_.p, ptiles,
+                                                                linv_.p);
         launches_ += 2;
       }
     }

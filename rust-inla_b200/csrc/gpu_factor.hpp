@@ -67,10 +67,11 @@ struct LevelPlan {
 class GpuFactor {
  public:
   // Size classes (rows of the front): <= kSmallA uses 128 threads, <= kSmallB 256
-  // threads, larger fronts use the blocked multi-CTA kernels.
+  // threads (one CTA per front), larger fronts use the blocked multi-CTA
+  // kernels in both the factorization and the selected inverse.
   static constexpr int kSmallA = 64;
-  static constexpr int kSmallB = 128;
-  static constexpr int kSiSmall = 96;
+  static constexpr int kSmallB = 96;
+  static constexpr int kSiSmall = kSmallB;
 
   GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream);
   ~GpuFactor();
@@ -133,9 +134,12 @@ class GpuFactor {
   std::vector<LevelPlan> levels_;
   DBuf<int> d_first_, d_rowptr_, d_rows_, d_relx_, d_child_ptr_, d_child_list_, d_parent_, d_uoff_, d_perm_;
   DBuf<int64_t> d_fptr_, d_lptr_, d_dpos_, spos_, spos_full_;
-  DBuf<int> d_pmap_, d_lists_;
-  DBuf<double> F_, Sg_, xp_, ub_, logdet_, dcache_, ppart_;
-  DBuf<int> status_;
+  DBuf<int> d_pmap_, d_lists_, d_csn_, d_lbo_;
+  DBuf<double> F_, Sg_, xp_, ub_, logdet_, dcache_, ppart_, linv_, ldpart_;
+  DBuf<int> status_, ldflag_;
+  DBuf<unsigned> ldticket_;
+  int nfill_ = 0, nldchunk_ = 0;  // fill chunks; log-det chunks per problem
+  int64_t ntot_ = 0;              // compact panel entries per problem
   int64_t launches_ = 0;
 };
 

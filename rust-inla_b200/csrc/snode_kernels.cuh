@@ -20,6 +20,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "dense_ldlt.cuh"
 #include "devsym.hpp"
 
 namespace inla {
@@ -34,56 +35,98 @@ __device__ __forceinline__ int sn_m(const DevSym& S, int s) { return S.rowptr[s 
 // value fill: every panel entry written exactly once (value or zero)
 // ---------------------------------------------------------------------------
 
-// vals: [B][nnz] full-CSC values; pmap: compact panel index -> input entry or -1.
-__global__ void k_fill_panels(DevSym S, const int* __restrict__ pmap, const double* __restrict__ vals,
-                              int64_t vstride, double* __restrict__ F, int64_t fstride) {
-  const int s = blockIdx.x, b = blockIdx.y;
-  const int k = sn_k(S, s), m = sn_m(S, s);
-  const int64_t mk = (int64_t)m * k;
-  const int* pm = pmap + S.lptr[s];
-  const double* v = vals + (int64_t)b * vstride;
-  double* Fs = F + (int64_t)b * fstride + S.fptr[s];
-  for (int64_t e = threadIdx.x; e < mk; e += blockDim.x) {
-    int src = pm[e];
-    Fs[e] = src >= 0 ? v[src] : 0.0;
+// The compact panel numbering (entry e of supernode s at lptr[s] + col * m + row)
+// is cut into chunks of kFillChunk entries, one CTA each; csn[c] is the
+// supernode holding the first entry of chunk c (csn[nchunks] = ns - 1). Within
+// its front the entry sits at fptr[s] + (e - lptr[s]) (panel columns first).
+constexpr int kFillChunk = 2048;  // 256 threads x 8 entries
+
+__device__ __forceinline__ int fill_find(const DevSym& S, int lo, int hi, int64_t e) {
+  // largest s in [lo, hi] with lptr[s] <= e
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (S.lptr[mid] <= e) lo = mid;
+    else hi = mid - 1;
   }
+  return lo;
+}
+
+// vals: [B][nnz] full-CSC values; pmap: compact panel index -> input entry or -1.
+__global__ void __launch_bounds__(256) k_fill_panels(DevSym S, const int* __restrict__ csn, int64_t ntot,
+                                                     const int* __restrict__ pmap, const double* __restrict__ vals,
+                                                     int64_t vstride, double* __restrict__ F, int64_t fstride) {
+  const int b = blockIdx.y;
+  const int lo = csn[blockIdx.x], hi = csn[blockIdx.x + 1];
+  const double* v = vals + (int64_t)b * vstride;
+  double* Fb = F + (int64_t)b * fstride;
+  int src[8];
+  int64_t dst[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int64_t e = (int64_t)blockIdx.x * kFillChunk + threadIdx.x + 256 * u;
+    src[u] = -1;
+    dst[u] = -1;
+    if (e < ntot) {
+      const int s = fill_find(S, lo, hi, e);
+      src[u] = pmap[e];
+      dst[u] = S.fptr[s] + (e - S.lptr[s]);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < 8; ++u)
+    if (dst[u] >= 0) Fb[dst[u]] = src[u] >= 0 ? v[src[u]] : 0.0;
 }
 
 // Component model: value(p) = sum_t coef[b][t] * comp[t][p] + sum_q w[b][obs_q] * prod_q
 // over the observation contributions of entry p (A^T diag(w) A on the pattern).
 // diag_add is added on diagonal entries (pdiag[p] != 0), e.g. the 1e-12 jitter of
 // the prior log-determinant (inference.rs:831-837).
-__global__ void k_fill_panels_model(DevSym S, const int* __restrict__ pmap, int ncomp,
-                                    const double* __restrict__ comp, int64_t nnz,
-                                    const double* __restrict__ coef, double diag_add,
-                                    const unsigned char* __restrict__ pdiag,
-                                    const int* __restrict__ cptr, const int* __restrict__ cobs,
-                                    const double* __restrict__ cprod, const double* __restrict__ w,
-                                    int64_t wstride, double* __restrict__ F, int64_t fstride) {
-  const int s = blockIdx.x, b = blockIdx.y;
-  const int k = sn_k(S, s), m = sn_m(S, s);
-  const int64_t mk = (int64_t)m * k;
-  const int* pm = pmap + S.lptr[s];
+__global__ void __launch_bounds__(256) k_fill_panels_model(DevSym S, const int* __restrict__ csn, int64_t ntot,
+                                                           const int* __restrict__ pmap, int ncomp,
+                                                           const double* __restrict__ comp, int64_t nnz,
+                                                           const double* __restrict__ coef, double diag_add,
+                                                           const unsigned char* __restrict__ pdiag,
+                                                           const int* __restrict__ cptr, const int* __restrict__ cobs,
+                                                           const double* __restrict__ cprod,
+                                                           const double* __restrict__ w, int64_t wstride,
+                                                           double* __restrict__ F, int64_t fstride) {
+  const int b = blockIdx.y;
+  const int lo = csn[blockIdx.x], hi = csn[blockIdx.x + 1];
   const double* cb = coef + (int64_t)b * ncomp;
   const double* wb = w ? w + (int64_t)b * wstride : nullptr;
-  double* Fs = F + (int64_t)b * fstride + S.fptr[s];
-  for (int64_t e = threadIdx.x; e < mk; e += blockDim.x) {
-    int src = pm[e];
+  double* Fb = F + (int64_t)b * fstride;
+  int src[8];
+  int64_t dst[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int64_t e = (int64_t)blockIdx.x * kFillChunk + threadIdx.x + 256 * u;
+    src[u] = -1;
+    dst[u] = -1;
+    if (e < ntot) {
+      const int s = fill_find(S, lo, hi, e);
+      src[u] = pmap[e];
+      dst[u] = S.fptr[s] + (e - S.lptr[s]);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    if (dst[u] < 0) continue;
+    const int p = src[u];
     double v = 0.0;
-    if (src >= 0) {
-      for (int t = 0; t < ncomp; ++t) v += cb[t] * comp[(int64_t)t * nnz + src];
-      if (pdiag[src]) v += diag_add;
+    if (p >= 0) {
+      for (int t = 0; t < ncomp; ++t) v += cb[t] * comp[(int64_t)t * nnz + p];
+      if (pdiag[p]) v += diag_add;
       if (wb) {
         double acc = 0.0;
         // design.rs:100-115: observations with a zero or non-finite weight are skipped
-        for (int q = cptr[src]; q < cptr[src + 1]; ++q) {
+        for (int q = cptr[p]; q < cptr[p + 1]; ++q) {
           const double wq = wb[cobs[q]];
           if (wq != 0.0 && isfinite(wq)) acc += wq * cprod[q];
         }
         v += acc;
       }
     }
-    Fs[e] = v;
+    Fb[dst[u]] = v;
   }
 }
 
@@ -91,6 +134,14 @@ __global__ void k_fill_panels_model(DevSym S, const int* __restrict__ pmap, int 
 // small fronts: whole front in shared memory, one CTA per (supernode, problem)
 // ---------------------------------------------------------------------------
 
+// Shared memory of k_factor_small for fronts of up to m rows (bytes).
+__host__ __device__ constexpr int small_factor_smem(int m) {
+  return (m * dense_ld(m) + 16 * dense_uld(m) + kDenseScratch) * 8;
+}
+
+// One CTA per (front, problem): the front in shared memory (leading dimension
+// dense_ld(m)), the children's updates added in fixed order, then the blocked
+// partial LDL^T of the k pivot columns (cta_ldlt).
 template <int NT>
 __global__ void __launch_bounds__(NT) k_factor_small(DevSym S, const int* __restrict__ list,
                                                      double* __restrict__ F, int64_t fstride) {
@@ -99,41 +150,55 @@ __global__ void __launch_bounds__(NT) k_factor_small(DevSym S, const int* __rest
   const int b = blockIdx.y;
   double* Fb = F + (int64_t)b * fstride;
   const int k = sn_k(S, s), m = sn_m(S, s);
+  const int lda = dense_ld(m), uld = dense_uld(m);
+  double* A = sm;
+  double* U = A + m * lda;
+  double* ws = U + 16 * uld;
+  int* rs = reinterpret_cast<int*>(U);  // child relative indices (U is free until the factorization)
   double* Fs = Fb + S.fptr[s];
   const int mm = m * m;
   for (int e = threadIdx.x; e < mm; e += NT) {
-    int col = e / m;
-    sm[e] = col < k ? Fs[e] : 0.0;
+    const int col = e / m, row = e - col * m;
+    if (col < k) cp_async8(&A[row + col * lda], Fs + e);
+    else A[row + col * lda] = 0.0;
   }
+  cp_async_commit();
+  cp_async_wait<0>();
   __syncthreads();
   for (int q = S.child_ptr[s]; q < S.child_ptr[s + 1]; ++q) {
     const int c = S.child_list[q];
     const int kc = sn_k(S, c), mc = sn_m(S, c), rc = mc - kc;
     const double* Uc = Fb + S.fptr[c] + (int64_t)kc * mc + kc;
     const int* relc = S.relx + S.rowptr[c] + kc;
+    for (int t = threadIdx.x; t < rc; t += NT) rs[t] = relc[t];
+    __syncthreads();
     const int rr = rc * rc;
-    for (int e = threadIdx.x; e < rr; e += NT) {
-      int jj = e / rc, ii = e - jj * rc;
-      if (ii >= jj) sm[relc[ii] + relc[jj] * m] += Uc[ii + (int64_t)jj * mc];
+    int e = threadIdx.x;
+    for (; e + 3 * NT < rr; e += 4 * NT) {
+      double v[4];
+      int dst[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int ee = e + u * NT;
+        const int jj = ee / rc, ii = ee - jj * rc;
+        const bool ok = ii >= jj;
+        v[u] = ok ? Uc[ii + (int64_t)jj * mc] : 0.0;
+        dst[u] = ok ? rs[ii] + rs[jj] * lda : -1;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (dst[u] >= 0) A[dst[u]] += v[u];
+    }
+    for (; e < rr; e += NT) {
+      const int jj = e / rc, ii = e - jj * rc;
+      if (ii >= jj) A[rs[ii] + rs[jj] * lda] += Uc[ii + (int64_t)jj * mc];
     }
     __syncthreads();
   }
-  for (int j = 0; j < k; ++j) {
-    const double dinv = 1.0 / sm[j + j * m];
-    const int w = m - j - 1;
-    const int ww = w * w;
-    const double* colj = sm + j * m + j + 1;
-    for (int e = threadIdx.x; e < ww; e += NT) {
-      int tt = e / w, ii = e - tt * w;
-      if (ii >= tt) sm[(j + 1 + ii) + (j + 1 + tt) * m] -= colj[ii] * colj[tt] * dinv;
-    }
-    __syncthreads();
-    for (int i = j + 1 + threadIdx.x; i < m; i += NT) sm[i + j * m] *= dinv;
-  }
-  __syncthreads();
+  cta_ldlt<false>(A, lda, m, k, nullptr, 0, U, uld, ws);
   for (int e = threadIdx.x; e < mm; e += NT) {
-    int col = e / m, row = e - col * m;
-    if (col < k || row >= col) Fs[e] = sm[e];
+    const int col = e / m, row = e - col * m;
+    if (col < k || row >= col) Fs[e] = A[row + col * lda];
   }
 }
 
@@ -358,6 +423,77 @@ __global__ void __launch_bounds__(NT) k_logdet(DevSym S, const double* __restric
   if (threadIdx.x == 0) {
     logdet[b] = red[0];
     status[b] = bad[0];
+  }
+}
+
+// log|Q_b| = sum_j log|d_j| and the status word, over chunks of kLogdetChunk
+// pivots per CTA. Each CTA writes its partial; the CTA that takes the last
+// ticket of problem b adds the partials in chunk order (deterministic), writes
+// the result and resets the ticket for the next launch.
+constexpr int kLogdetChunk = 2048;  // 256 threads x 8 pivots
+__global__ void __launch_bounds__(256) k_logdet_chunks(DevSym S, const double* __restrict__ F, int64_t fstride,
+                                                       double* __restrict__ part, int* __restrict__ pflag,
+                                                       unsigned* __restrict__ ticket, double* __restrict__ logdet,
+                                                       int* __restrict__ status) {
+  __shared__ double red[256];
+  __shared__ int bad[256];
+  __shared__ bool last;
+  const int b = blockIdx.y, nch = gridDim.x;
+  const double* Fb = F + (int64_t)b * fstride;
+  double dv[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int j = blockIdx.x * kLogdetChunk + threadIdx.x + 256 * u;
+    dv[u] = j < S.n ? Fb[S.dpos[j]] : 1.0;
+  }
+  double acc = 0.0;
+  int flag = 0;
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const double ad = fabs(dv[u]);
+    if (!isfinite(dv[u])) flag |= kStatusNotFinite;
+    else if (ad < 1e-14) flag |= kStatusSingular;
+    acc += log(ad);
+  }
+  red[threadIdx.x] = acc;
+  bad[threadIdx.x] = flag;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      red[threadIdx.x] += red[threadIdx.x + o];
+      bad[threadIdx.x] |= bad[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[(int64_t)b * nch + blockIdx.x] = red[0];
+    pflag[(int64_t)b * nch + blockIdx.x] = bad[0];
+    __threadfence();
+    last = atomicAdd(&ticket[b], 1u) == (unsigned)(nch - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double a2 = 0.0;
+  int f2 = 0;
+  for (int c = threadIdx.x; c < nch; c += 256) {
+    a2 += __ldcg(part + (int64_t)b * nch + c);
+    f2 |= __ldcg(pflag + (int64_t)b * nch + c);
+  }
+  red[threadIdx.x] = a2;
+  bad[threadIdx.x] = f2;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      red[threadIdx.x] += red[threadIdx.x + o];
+      bad[threadIdx.x] |= bad[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    logdet[b] = red[0];
+    status[b] = bad[0];
+    ticket[b] = 0u;
   }
 }
 

@@ -1,179 +1,47 @@
-// Large-front kernels (fronts with more than 128 rows), 64-column blocks.
+// Large-front kernels (fronts with more than 96 rows), 64-column blocks.
 //
 // Factorization, per block J = [j0, j0+w) of a front (right-looking):
-//   k_panel64   every CTA factors the w x w diagonal block in shared memory
-//               (the redundant O(w^3) work removes a serial launch), CTA 0
-//               writes it back, each CTA solves its 128 rows
-//               L_i = F_i L_JJ^-T D_J^-1 (one thread per row);
+//   k_gather8   extend-add of the children's updates (once per level);
+//   k_panel64   every CTA factors the w x w diagonal block with the blocked
+//               dense routine (cta_ldlt, which also forms L_JJ^-1); CTA 0
+//               stores the factored block (dcache) and L_JJ^-1 (the inverse-
+//               block cache, reused by the selected inverse); each CTA forms
+//               its 64 rows L_i = F_i L_JJ^-T D_J^-1 as one tensor-core GEMM;
 //   k_update64  F[i,j] -= sum_{t in J} L_it d_t L_jt on 64x64 tiles of the lower
-//               trailing matrix, FP64 tensor-core mma.sync.m8n8k4 tiles.
+//               trailing matrix (tensor-core tiles, operands staged with cp.async).
 // Selected inverse, per block J from right to left (A = rows after J):
-//   k_si_gemm64 G = Sigma[A,A] L[A,J] (tensor-core tiles, Sigma read from its
-//               lower triangle with coalesced loads on both sides of the
-//               diagonal), X = -G L_JJ^-1 per row, Sigma[A,J] = X, and the
-//               tile's partial P = L[I,J]^T X[I,J];
-//   k_si_diag64 P = sum of partials (fixed order), then the in-block Takahashi
+//   k_si_gemm64 G = Sigma[A,A] L[A,J], X = -G L_JJ^-1 (cached inverse block),
+//               Sigma[A,J] = X, and the tile's partial P = L[I,J]^T X[I,J];
+//   k_si_diag64 Sigma_JJ = L_JJ^-T (D^-1 L_JJ^-1 - P), P the fixed-order sum of
+//               the partials: the closed form of the in-block Takahashi
 //               recurrence S_ij = -P_ji - sum_{l in J, l>j} L_lj S_li,
 //               S_jj = 1/d_j - P_jj - sum_{l in J, l>j} L_lj S_lj.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "dense_ldlt.cuh"
 #include "devsym.hpp"
 
 namespace inla {
 namespace {
 
-constexpr int kB64 = 64;       // block-column width
-constexpr int kPanelRows = 128;  // rows per panel CTA (one thread per row)
-constexpr int kPanelSmem = (2 * kB64 * (kB64 + 1) + kB64 * 129 + 2 * kB64) * 8;
+constexpr int kB64 = 64;         // block-column width
+constexpr int kPanelRows = 64;   // rows per panel CTA
+constexpr int kLd64 = dense_ld(kB64);
+constexpr int kULd64 = dense_uld(kB64);
+constexpr int kPanelSmem = (3 * kB64 * kLd64 + 16 * kULd64 + kDenseScratch) * 8;
+constexpr int kUpdSmem = 2 * kB64 * kLd64 * 8;
 constexpr int kSiGemmSmem = 3 * 64 * (kB64 + 1) * 8;
 constexpr int kSiDiagSmem = 3 * kB64 * (kB64 + 1) * 8;
 
 __device__ __forceinline__ int lg_k(const DevSym& S, int s) { return S.first[s + 1] - S.first[s]; }
 __device__ __forceinline__ int lg_m(const DevSym& S, int s) { return S.rowptr[s + 1] - S.rowptr[s]; }
 
-__device__ __forceinline__ void mma884(double& c0, double& c1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(c0), "+d"(c1)
-               : "d"(a), "d"(b));
-}
+__device__ __forceinline__ void mma884(double& c0, double& c1, double a, double b) { dmma884(c0, c1, a, b); }
 
-// Unblocked LDL^T of the w x w block held in smem (leading dimension ld), one
-// barrier per pivot: step j reads column j unscaled and updates columns > j;
-// column j is scaled after the barrier, concurrently with step j+1, which
-// touches columns > j only.
-__device__ __forceinline__ void smem_ldlt(double* sm, int w, int ld) {
-  for (int j = 0; j < w; ++j) {
-    const double dinv = 1.0 / sm[j + j * ld];
-    const int r = w - j - 1;
-    const double* cj = sm + j + 1 + j * ld;
-    for (int e = threadIdx.x; e < r * r; e += blockDim.x) {
-      const int tt = e / r, ii = e - tt * r;
-      if (ii >= tt) sm[(j + 1 + ii) + (j + 1 + tt) * ld] -= cj[ii] * cj[tt] * dinv;
-    }
-    __syncthreads();
-    for (int i = j + 1 + threadIdx.x; i < w; i += blockDim.x) sm[i + j * ld] *= dinv;
-  }
-  __syncthreads();
-}
-
-// Register-resident LDL^T of a w x w block (w <= 64) with 128 threads:
-// thread t owns row i = t % 64 and the columns j = t / 64 + 2b (b < 32) of it.
-// Pivot p: the owners of column p publish it to a double-buffered smem column
-// (one barrier per pivot), then every thread updates its entries (i, j),
-// p < j <= i, with v_ij -= (v_ip / d_p) v_jp. On exit Ds (ld 65) holds unit L
-// below the diagonal and D on it; piv[p] = d_p.
-__device__ __forceinline__ void reg_ldlt64(const double* __restrict__ A, int64_t lda, int w, double* Ds,
-                                           double* colbuf, double* piv) {
-  const int t = threadIdx.x, i = t & 63, q = t >> 6;
-  double v[32];
-#pragma unroll
-  for (int b = 0; b < 32; ++b) {
-    const int j = q + 2 * b;
-    v[b] = (i < w && j <= i) ? A[i + (int64_t)j * lda] : 0.0;
-  }
-  for (int p = 0; p < w; ++p) {
-    double* col = colbuf + (p & 1) * 64;
-    if ((p & 1) == q && i >= p && i < w) {
-      double val = 0.0;
-#pragma unroll
-      for (int b = 0; b < 32; ++b)
-        if (b == (p >> 1)) val = v[b];
-      col[i] = val;
-    }
-    __syncthreads();
-    const double dp = col[p];
-    if (t == 0) piv[p] = dp;
-    const double lip = (i > p && i < w) ? col[i] / dp : 0.0;
-#pragma unroll
-    for (int b = 0; b < 32; ++b) {
-      const int j = q + 2 * b;
-      if (j > p && j <= i) v[b] -= lip * col[j];
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int b = 0; b < 32; ++b) {
-    const int j = q + 2 * b;
-    if (i < w && j <= i) Ds[i + j * (kB64 + 1)] = (j == i) ? piv[j] : v[b] / piv[j];
-  }
-  __syncthreads();
-}
-
-// 64x64 LDL^T with 256 threads, entries register-resident: thread t owns the
-// lower-triangle entries e = t + 256 s (s < 9) of the block (row-major
-// triangular numbering). Pivot p: owners of column p publish it (double-
-// buffered smem column, one barrier), then every owned entry (i, j), j > p,
-// takes v -= col[i] col[j] / d_p. On exit A (smem, ld 65) holds unit L below the
-// diagonal and D on it (entries outside the w x w block are left untouched).
-__device__ __forceinline__ void tri_index(int e, int& i, int& j) {
-  // row-major lower triangle: e = i (i + 1) / 2 + j
-  int r = (int)((sqrtf(8.0f * (float)e + 1.0f) - 1.0f) * 0.5f);
-  while ((r + 1) * (r + 2) / 2 <= e) ++r;
-  while (r * (r + 1) / 2 > e) --r;
-  i = r;
-  j = e - r * (r + 1) / 2;
-}
-
-__device__ __forceinline__ void ldlt64_256(double* A, int w, double* colbuf /*[2][64]*/) {
-  const int t = threadIdx.x;
-  double v[9];
-  int ei[9], ej[9];
-#pragma unroll
-  for (int s = 0; s < 9; ++s) {
-    const int e = t + 256 * s;
-    int i = 64, j = 64;
-    if (e < 2080) tri_index(e, i, j);
-    ei[s] = i;
-    ej[s] = j;
-    v[s] = (i < w && j < w) ? A[i + j * (kB64 + 1)] : 0.0;
-  }
-  for (int p = 0; p < w; ++p) {
-    double* col = colbuf + (p & 1) * 64;
-#pragma unroll
-    for (int s = 0; s < 9; ++s)
-      if (ej[s] == p && ei[s] < w) col[ei[s]] = v[s];
-    __syncthreads();
-    const double dinv = 1.0 / col[p];
-#pragma unroll
-    for (int s = 0; s < 9; ++s)
-      if (ej[s] > p && ei[s] < w) v[s] -= col[ei[s]] * col[ej[s]] * dinv;
-  }
-  __syncthreads();
-  // diagonal first, then L = v / d_j
-#pragma unroll
-  for (int s = 0; s < 9; ++s)
-    if (ei[s] < w && ei[s] == ej[s]) A[ei[s] + ej[s] * (kB64 + 1)] = v[s];
-  __syncthreads();
-#pragma unroll
-  for (int s = 0; s < 9; ++s)
-    if (ei[s] < w && ei[s] > ej[s]) A[ei[s] + ej[s] * (kB64 + 1)] = v[s] / A[ej[s] + ej[s] * (kB64 + 1)];
-  __syncthreads();
-}
-
-// Li = L^-1 of the unit lower w x w block L (smem, ld 65; Li zero-padded to 64x64).
-// 256 threads: 4 per column, the dot product of each substitution step split
-// across the 4 lanes and combined with shuffles.
-__device__ __forceinline__ void linv64(const double* L, double* Li, int w) {
-  const int sub = threadIdx.x & 3;
-  const unsigned gmask = 0xFu << ((threadIdx.x & 31) & ~3);  // the 4 lanes of this column
-  constexpr int ld = kB64 + 1;
-  for (int c = threadIdx.x >> 2; c < kB64; c += blockDim.x >> 2) {
-    for (int r = sub; r < kB64; r += 4) Li[r + c * ld] = (r == c && c < w) ? 1.0 : 0.0;
-    __syncwarp(gmask);
-    if (c < w) {
-      for (int r = c + 1; r < w; ++r) {
-        double a = 0.0;
-        for (int u = c + sub; u < r; u += 4) a += L[r + u * ld] * Li[u + c * ld];
-        a += __shfl_xor_sync(gmask, a, 1);
-        a += __shfl_xor_sync(gmask, a, 2);
-        if (sub == 0) Li[r + c * ld] = -a;
-        __syncwarp(gmask);
-      }
-    }
-  }
-  __syncthreads();
+__device__ __forceinline__ const double* linv_block(const DevSym& S, const double* linv, int b, int s, int blk) {
+  return linv + (int64_t)b * S.lstride + ((int64_t)S.lbo[s] + blk) * (kB64 * kB64);
 }
 
 // Extend-add of the children's updates into parent columns [c0, c1) (the
@@ -263,7 +131,25 @@ __global__ void __launch_bounds__(256) k_si_gather8(DevSym S, const int* __restr
   double* Ss = Sg + (int64_t)b * fstride + S.fptr[s];
   const int* __restrict__ rel = S.relx + S.rowptr[s] + k;
   const int total = (c1 - c0) * r;
-  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+  int e = threadIdx.x;
+  for (; e + 3 * (int)blockDim.x < total; e += 4 * blockDim.x) {
+    double v[4];
+    int64_t dst[4];
+    bool ok[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int ee = e + u * blockDim.x;
+      const int jj = c0 + ee / r, ii = ee - (ee / r) * r;
+      ok[u] = ii >= jj;
+      const int pi = ok[u] ? rel[ii] : 0, pj = ok[u] ? rel[jj] : 0;
+      v[u] = ok[u] ? (pi >= pj ? Sp[pi + (int64_t)pj * mp] : Sp[pj + (int64_t)pi * mp]) : 0.0;
+      dst[u] = (k + ii) + (int64_t)(k + jj) * m;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (ok[u]) Ss[dst[u]] = v[u];
+  }
+  for (; e < total; e += blockDim.x) {
     const int jj = c0 + e / r, ii = e - (e / r) * r;
     if (ii < jj) continue;
     const int pi = rel[ii], pj = rel[jj];
@@ -274,51 +160,57 @@ __global__ void __launch_bounds__(256) k_si_gather8(DevSym S, const int* __restr
 // The factored diagonal block goes to dcache[(list index, problem)] (written by
 // CTA 0): the other CTAs of this launch still read the unfactored block from
 // the front, so it is copied into the front by k_update64 of the same step.
-// Each CTA: LDL^T of the diagonal block (register-resident), L_JJ^-1, then its
-// 128 rows X = F_rows (L_JJ^-T D^-1) as one tensor-core GEMM.
+// Each CTA: blocked LDL^T + inverse of the diagonal block, then its 64 rows
+// X = F_rows (L_JJ^-T D^-1) as one tensor-core GEMM.
 __global__ void __launch_bounds__(256) k_panel64(DevSym S, const int* __restrict__ list, int j0,
                                                  double* __restrict__ F, int64_t fstride,
-                                                 double* __restrict__ dcache) {
+                                                 double* __restrict__ dcache, double* __restrict__ linv) {
   extern __shared__ double smem64[];
-  constexpr int ld = kB64 + 1;
-  double* Ds = smem64;                // [64][65] diagonal block, factored in place
-  double* Li = Ds + kB64 * ld;        // [64][65] L_JJ^-1, then B = L^-T D^-1 (Bm[u][t] at u + t*ld)
-  double* Fa = Li + kB64 * ld;        // [64 cols][129] rows of this CTA: Fa[t * 129 + r]
-  double* colbuf = Fa + kB64 * 129;   // [2][64]
+  constexpr int ld = kLd64;
+  double* Ds = smem64;         // [64 cols][ld]: diagonal block, factored in place
+  double* Li = Ds + kB64 * ld; // L_JJ^-1, then Bm[u + t*ld] = Li[t][u] / d_t
+  double* Fa = Li + kB64 * ld; // rows of this CTA: Fa[t*ld + r] = F[r0 + r, j0 + t]
+  double* U = Fa + kB64 * ld;  // [16][kULd64] scratch of cta_ldlt, then 1 / d_t
+  double* ws = U + 16 * kULd64;
   const int s = list[blockIdx.x], b = blockIdx.y;
   const int k = lg_k(S, s), m = lg_m(S, s);
   if (j0 >= k) return;
   const int w = min(kB64, k - j0);
   const int r0 = j0 + w + blockIdx.z * kPanelRows;
   if (blockIdx.z > 0 && r0 >= m) return;
+  const int rows = max(0, min(kPanelRows, m - r0));
   double* Fs = F + (int64_t)b * fstride + S.fptr[s];
   const double* D0 = Fs + j0 + (int64_t)j0 * m;
   for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) {
     const int c = e >> 6, r = e & 63;
-    Ds[r + c * ld] = (r < w && c < w && r >= c) ? D0[r + (int64_t)c * m] : 0.0;
+    if (r < w && c < w && r >= c) cp_async8(&Ds[r + c * ld], D0 + r + (int64_t)c * m);
+    else Ds[r + c * ld] = 0.0;
+    Li[r + c * ld] = 0.0;
+    if (r < rows && c < w) cp_async8(&Fa[c * ld + r], Fs + (r0 + r) + (int64_t)(j0 + c) * m);
+    else Fa[c * ld + r] = 0.0;
   }
-  const int rows = max(0, min(kPanelRows, m - r0));
-  for (int e = threadIdx.x; e < kB64 * kPanelRows; e += blockDim.x) {
-    const int c = e / kPanelRows, r = e - c * kPanelRows;
-    Fa[c * 129 + r] = (r < rows && c < w) ? Fs[(r0 + r) + (int64_t)(j0 + c) * m] : 0.0;
-  }
+  cp_async_commit();
+  cp_async_wait<0>();
   __syncthreads();
-  ldlt64_256(Ds, w, colbuf);
+  cta_ldlt<true>(Ds, ld, w, w, Li, ld, U, kULd64, ws);
   if (blockIdx.z == 0) {
     double* dc = dcache + ((int64_t)blockIdx.x * gridDim.y + b) * (kB64 * kB64);
+    double* lc = const_cast<double*>(linv_block(S, linv, b, s, j0 / kB64));
     for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) {
       const int c = e >> 6, r = e & 63;
       dc[e] = (r < w && c < w) ? Ds[r + c * ld] : 0.0;
+      lc[e] = Li[r + c * ld];  // zero outside the w x w lower triangle
     }
   }
   if (rows == 0) return;
-  linv64(Ds, Li, w);
-  // B[u][t] = Li[t][u] / d_t  (stored into Li's slot after a barrier: read all first)
+  double* dinv = U;
+  if (threadIdx.x < kB64) dinv[threadIdx.x] = threadIdx.x < w ? 1.0 / Ds[threadIdx.x * (ld + 1)] : 0.0;
+  __syncthreads();
   double bv[16];
 #pragma unroll
   for (int q = 0; q < 16; ++q) {
     const int e = threadIdx.x + 256 * q, u = e & 63, t = e >> 6;
-    bv[q] = (t < w && u < w) ? Li[t + u * ld] / Ds[t + t * ld] : 0.0;
+    bv[q] = Li[t + u * ld] * dinv[t];
   }
   __syncthreads();
 #pragma unroll
@@ -327,31 +219,31 @@ __global__ void __launch_bounds__(256) k_panel64(DevSym S, const int* __restrict
     Li[u + t * ld] = bv[q];
   }
   __syncthreads();
-  // X (128 x 64) = Fa (128 x 64) * B (64 x 64); warp tile 32 x 32
+  // X (64 x 64) = Fa (64 x 64) * Bm; warp tile 32 x 16
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wr = (warp & 3) * 32, wc = (warp >> 2) * 32;
+  const int wr = (warp & 1) * 32, wc = (warp >> 1) * 16;
   const int g = lane >> 2, tg = lane & 3;
-  double acc[4][4][2];
+  double acc[4][2][2];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int q = 0; q < 4; ++q) acc[a][q][0] = acc[a][q][1] = 0.0;
+    for (int q = 0; q < 2; ++q) acc[a][q][0] = acc[a][q][1] = 0.0;
 #pragma unroll 4
   for (int kk = 0; kk < kB64; kk += 4) {
-    double af[4], bf[4];
+    double af[4], bf[2];
 #pragma unroll
-    for (int a = 0; a < 4; ++a) af[a] = Fa[(kk + tg) * 129 + wr + a * 8 + g];
+    for (int a = 0; a < 4; ++a) af[a] = Fa[(kk + tg) * ld + wr + a * 8 + g];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) bf[q] = Li[(kk + tg) + (wc + q * 8 + g) * ld];
+    for (int q = 0; q < 2; ++q) bf[q] = Li[(kk + tg) + (wc + q * 8 + g) * ld];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
-      for (int q = 0; q < 4; ++q) mma884(acc[a][q][0], acc[a][q][1], af[a], bf[q]);
+      for (int q = 0; q < 2; ++q) mma884(acc[a][q][0], acc[a][q][1], af[a], bf[q]);
   }
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
+    for (int q = 0; q < 2; ++q)
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int r = wr + a * 8 + g, t = wc + q * 8 + tg * 2 + h;
@@ -363,8 +255,10 @@ constexpr int kUT64 = 64;
 __global__ void __launch_bounds__(128) k_update64(DevSym S, const int* __restrict__ list, int j0,
                                                  double* __restrict__ F, int64_t fstride,
                                                  const double* __restrict__ dcache) {
-  __shared__ double As[32][kUT64 + 1];  // As[t][i] = L[I0+i, j0+t0+t]
-  __shared__ double Bs[32][kUT64 + 1];  // Bs[t][j] = d_t L[J0+j, j0+t0+t]
+  extern __shared__ double smu[];
+  constexpr int ld = kLd64;
+  double* As = smu;             // As[t*ld + i] = L[I0+i, j0+t]
+  double* Bs = smu + kB64 * ld; // Bs[t*ld + j] = L[J0+j, j0+t]
   __shared__ double dsh[kB64];
   const int s = list[blockIdx.x], b = blockIdx.y;
   const int k = lg_k(S, s), m = lg_m(S, s);
@@ -373,15 +267,15 @@ __global__ void __launch_bounds__(128) k_update64(DevSym S, const int* __restric
   const int c = j0 + w;
   const int T = m - c;
   const double* dc = dcache + ((int64_t)blockIdx.x * gridDim.y + b) * (kB64 * kB64);
+  double* Fs = F + (int64_t)b * fstride + S.fptr[s];
   if (blockIdx.z == 0) {  // factored diagonal block -> front
-    double* D0 = F + (int64_t)b * fstride + S.fptr[s] + j0 + (int64_t)j0 * m;
+    double* D0 = Fs + j0 + (int64_t)j0 * m;
     for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
       const int cc = e / w, r = e - cc * w;
       if (r >= cc) D0[r + (int64_t)cc * m] = dc[r + cc * kB64];
     }
   }
   if (T <= 0) return;
-  for (int t = threadIdx.x; t < kB64; t += blockDim.x) dsh[t] = t < w ? dc[t + t * kB64] : 0.0;
   const int nt = (T + kUT64 - 1) / kUT64;
   const int tile = blockIdx.z;
   if (tile >= nt * (nt + 1) / 2) return;
@@ -392,8 +286,19 @@ __global__ void __launch_bounds__(128) k_update64(DevSym S, const int* __restric
   }
   const int I = J + rem;
   const int I0 = c + I * kUT64, J0 = c + J * kUT64;
-  double* Fs = F + (int64_t)b * fstride + S.fptr[s];
   const double* Lb = Fs + (int64_t)j0 * m;
+  for (int e = threadIdx.x; e < kB64 * kUT64; e += blockDim.x) {
+    const int t = e >> 6, ii = e & 63;
+    const double* col = Lb + (int64_t)t * m;
+    if (t < w && I0 + ii < m) cp_async8(&As[t * ld + ii], col + I0 + ii);
+    else As[t * ld + ii] = 0.0;
+    if (t < w && J0 + ii < m) cp_async8(&Bs[t * ld + ii], col + J0 + ii);
+    else Bs[t * ld + ii] = 0.0;
+  }
+  cp_async_commit();
+  for (int t = threadIdx.x; t < kB64; t += blockDim.x) dsh[t] = t < w ? dc[t + t * kB64] : 0.0;
+  cp_async_wait<0>();
+  __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wi = (warp & 1) * 32, wj = (warp >> 1) * 32;
   const int g = lane >> 2, tg = lane & 3;
@@ -402,32 +307,18 @@ __global__ void __launch_bounds__(128) k_update64(DevSym S, const int* __restric
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int q = 0; q < 4; ++q) acc[a][q][0] = acc[a][q][1] = 0.0;
-  for (int t0 = 0; t0 < w; t0 += 32) {
-    __syncthreads();
-    for (int e = threadIdx.x; e < 32 * kUT64; e += blockDim.x) {
-      const int t = e / kUT64, ii = e - t * kUT64;
-      double av = 0.0, bv = 0.0;
-      if (t0 + t < w) {
-        const int64_t col = (int64_t)(t0 + t) * m;
-        if (I0 + ii < m) av = Lb[I0 + ii + col];
-        if (J0 + ii < m) bv = Lb[J0 + ii + col] * dsh[t0 + t];
-      }
-      As[t][ii] = av;
-      Bs[t][ii] = bv;
-    }
-    __syncthreads();
+#pragma unroll 4
+  for (int kk = 0; kk < kB64; kk += 4) {
+    double af[4], bf[4];
+    const double dk = dsh[kk + tg];
 #pragma unroll
-    for (int kk = 0; kk < 32; kk += 4) {
-      double af[4], bf[4];
+    for (int a = 0; a < 4; ++a) af[a] = As[(kk + tg) * ld + wi + a * 8 + g];
 #pragma unroll
-      for (int a = 0; a < 4; ++a) af[a] = As[kk + tg][wi + a * 8 + g];
+    for (int q = 0; q < 4; ++q) bf[q] = Bs[(kk + tg) * ld + wj + q * 8 + g] * dk;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) bf[q] = Bs[kk + tg][wj + q * 8 + g];
+    for (int a = 0; a < 4; ++a)
 #pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) mma884(acc[a][q][0], acc[a][q][1], af[a], bf[q]);
-    }
+      for (int q = 0; q < 4; ++q) mma884(acc[a][q][0], acc[a][q][1], af[a], bf[q]);
   }
 #pragma unroll
   for (int a = 0; a < 4; ++a)
@@ -558,22 +449,14 @@ __device__ __forceinline__ double sig_lower(const double* Ss, int m, int row, in
 
 constexpr int kSiT = 64;  // rows of A per CTA
 
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
-}
-
 // ppart: [list index][b][tile][64*64] partial P blocks; ptiles = tiles per (front, b).
 // Shared memory: two chunk buffers (Sa + Lb each, double-buffered with
-// cp.async) and G; L_JJ and L[I,J] reuse chunk buffer 0 after the GEMM.
+// cp.async) and G; L_JJ^-1 (from the inverse-block cache) and L[I,J] reuse the
+// chunk buffers after the GEMM.
 __global__ void __launch_bounds__(128) k_si_gemm64(DevSym S, const int* __restrict__ list, int jb,
                                                   const double* __restrict__ F, double* __restrict__ Sg,
-                                                  int64_t fstride, double* __restrict__ ppart, int ptiles) {
+                                                  int64_t fstride, double* __restrict__ ppart, int ptiles,
+                                                  const double* __restrict__ linv) {
   extern __shared__ double smem64[];
   constexpr int kBuf = 64 * (kB64 + 1);  // doubles per chunk buffer (Sa[32][65] + Lb[32][65])
   typedef double Row65[kB64 + 1];
@@ -662,16 +545,16 @@ __global__ void __launch_bounds__(128) k_si_gemm64(DevSym S, const int* __restri
     for (int q = 0; q < 4; ++q)
 #pragma unroll
       for (int h = 0; h < 2; ++h) Gs[wi + a * 8 + g][wj + q * 8 + tg * 2 + h] = acc[a][q][h];
-  // X = -G L_JJ^-1 as a tensor-core GEMM with the explicit inverse of the unit
-  // lower diagonal block
-  double* Lc = smem64;          // L_JJ, column-major ld 65 (chunk buffer 0)
-  double* Li = smem64 + kBuf;   // L_JJ^-1 (chunk buffer 1)
-  for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) {
-    const int c = e >> 6, r = e & 63;
-    Lc[r + c * (kB64 + 1)] = (r < w && c < w && r > c) ? Fs[(j0 + r) + (int64_t)(j0 + c) * m] : 0.0;
+  // X = -G L_JJ^-1 as a tensor-core GEMM with the cached inverse of the unit
+  // lower diagonal block (column-major, ld 65 in chunk buffer 1)
+  double* Li = smem64 + kBuf;
+  {
+    const double* lc = linv_block(S, linv, b, s, bi);
+    for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) cp_async8(&Li[(e & 63) + (e >> 6) * (kB64 + 1)], lc + e);
+    cp_async_commit();
+    cp_async_wait<0>();
   }
   __syncthreads();
-  linv64(Lc, Li, w);
   {
     double xa[4][4][2];
 #pragma unroll
@@ -709,8 +592,11 @@ __global__ void __launch_bounds__(128) k_si_gemm64(DevSym S, const int* __restri
   Row65* Lij = Lt;  // Lij[l][j] = L[I0+l, j0+j]
   for (int e = threadIdx.x; e < kSiT * kB64; e += blockDim.x) {
     const int j = e / kSiT, l = e - j * kSiT;
-    Lij[l][j] = (l < rows && j < w) ? Fs[(I0 + l) + (int64_t)(j0 + j) * m] : 0.0;
+    if (l < rows && j < w) cp_async8(&Lij[l][j], Fs + (I0 + l) + (int64_t)(j0 + j) * m);
+    else Lij[l][j] = 0.0;
   }
+  cp_async_commit();
+  cp_async_wait<0>();
   __syncthreads();
   double pa[4][4][2];
 #pragma unroll
@@ -741,10 +627,11 @@ __global__ void __launch_bounds__(128) k_si_gemm64(DevSym S, const int* __restri
 
 __global__ void __launch_bounds__(256) k_si_diag64(DevSym S, const int* __restrict__ list, int jb,
                                                   const double* __restrict__ F, double* __restrict__ Sg,
-                                                  int64_t fstride, const double* __restrict__ ppart, int ptiles) {
+                                                  int64_t fstride, const double* __restrict__ ppart, int ptiles,
+                                                  const double* __restrict__ linv) {
   // Sigma_JJ = L^-T (D^-1 L^-1 - P), L = L_JJ unit lower, P = L[A,J]^T Sigma[A,J]
-  // (the closed form of the in-block Takahashi recurrence), with L^-1 from
-  // linv64 and the product as a tensor-core GEMM.
+  // (the closed form of the in-block Takahashi recurrence), with L^-1 from the
+  // inverse-block cache and the product as a tensor-core GEMM.
   extern __shared__ double smem64[];
   constexpr int ld = kB64 + 1;
   double* Pm = smem64;            // P, then M = D^-1 L^-1 - P  (Pm[r + c*ld] = entry (r, c))
@@ -760,16 +647,32 @@ __global__ void __launch_bounds__(256) k_si_diag64(DevSym S, const int* __restri
   const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
   double* Ss = Sg + (int64_t)b * fstride + S.fptr[s];
   const double* pp = ppart + ((int64_t)blockIdx.x * gridDim.y + b) * ptiles * (kB64 * kB64);
+  const double* lc = linv_block(S, linv, b, s, bi);
   for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) {
-    const int j = e >> 6, i = e & 63;  // partials are stored row-major: pp[j*64 + i] = P[j][i]
-    double acc = 0.0;
-    for (int z = 0; z < ntiles; ++z) acc += pp[(int64_t)z * kB64 * kB64 + e];
-    Pm[j + i * ld] = acc;
     const int c = e >> 6, r = e & 63;
-    Ld[r + c * ld] = (r < w && c < w && r >= c) ? Fs[(j0 + r) + (int64_t)(j0 + c) * m] : 0.0;
+    if (r < w && c < w && r >= c) cp_async8(&Ld[r + c * ld], Fs + (j0 + r) + (int64_t)(j0 + c) * m);
+    else Ld[r + c * ld] = 0.0;
+    cp_async8(&Li[r + c * ld], lc + e);
   }
+  cp_async_commit();
+  {
+    // partials are stored row-major: pp[j*64 + i] = P[j][i]; fixed summation order over tiles
+    double acc[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+    for (int z = 0; z < ntiles; ++z) {
+      const double* pz = pp + (int64_t)z * kB64 * kB64;
+#pragma unroll
+      for (int q = 0; q < 16; ++q) acc[q] += pz[threadIdx.x + 256 * q];
+    }
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int e = threadIdx.x + 256 * q, j = e >> 6, i = e & 63;
+      Pm[j + i * ld] = acc[q];
+    }
+  }
+  cp_async_wait<0>();
   __syncthreads();
-  linv64(Ld, Li, w);
   for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) {
     const int c = e >> 6, r = e & 63;
     Pm[r + c * ld] = (r < w && c < w) ? Li[r + c * ld] / Ld[r + r * ld] - Pm[r + c * ld] : 0.0;
