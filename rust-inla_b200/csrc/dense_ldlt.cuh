@@ -95,6 +95,32 @@ __device__ __forceinline__ void warp_ldlt16(double* A, int lda, int w, double* L
   __syncwarp();
 }
 
+// One warp: Lam = L^-1 of the unit lower w x w (w <= 16) block of L (shared
+// memory, column-major, leading dimension ldl; the diagonal is not read),
+// identity-padded to 16 x 16 (ld kLamLd). Forward elimination
+// Lam[i,:] -= L[i,p] Lam[p,:] for i > p, one __syncwarp per step; xbuf: 32 doubles.
+__device__ __forceinline__ void warp_trinv16(const double* L, int ldl, int w, double* Lam, double* xbuf) {
+  const int lane = threadIdx.x & 31, r = lane >> 1, h = lane & 1;
+  double li[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) li[q] = (r == h + 2 * q) ? 1.0 : 0.0;
+#pragma unroll 16
+  for (int p = 0; p < 16; ++p) {
+    double* row = xbuf + (p & 1) * 16;
+    const double lrp = (r > p && r < w && p < w) ? L[r + p * ldl] : 0.0;
+    if (r == p) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) row[h + 2 * q] = li[q];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < 8; ++q) li[q] -= lrp * row[h + 2 * q];
+  }
+#pragma unroll
+  for (int q = 0; q < 8; ++q) Lam[r + (h + 2 * q) * kLamLd] = li[q];
+  __syncwarp();
+}
+
 // Lower-triangle tile index: task = I (I + 1) / 2 + J, J <= I.
 __device__ __forceinline__ void tri_decode(int task, int& I, int& J) {
   int t = (int)((sqrtf(8.0f * (float)task + 1.0f) - 1.0f) * 0.5f);

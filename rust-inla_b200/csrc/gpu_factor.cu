@@ -157,8 +157,13 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
   }
   set_smem(k_factor_small<128>, small_factor_smem(kSmallA));
   set_smem(k_factor_small<256>, small_factor_smem(kSmallB));
-  set_smem(k_selinv_small<256>, (kSiSmall * kSiSmall * 2) * 8);
+  set_smem(k_selinv_small<256>, small_selinv_smem(kSiSmall));
   set_smem(k_panel64, kPanelSmem);
+  {
+    int dev = 0;
+    INLA_CUDA(cudaGetDevice(&dev));
+    INLA_CUDA(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev));
+  }
   set_smem(k_update64, kUpdSmem);
   set_smem(k_si_gemm64, kSiGemmSmem);
   set_smem(k_si_diag64, kSiDiagSmem);
@@ -239,8 +244,15 @@ void GpuFactor::run_factor_levels(int B) {
       ++launches_;
       for (int j0 = 0; j0 < P.kmax_large; j0 += kB64) {
         int rows = P.mmax_large - j0;
-        k_panel64<<<dim3(nl, B, std::max(1, cdiv(rows, kPanelRows))), 256, kPanelSmem, stream_>>>(
-            ds_, lst, j0, F_.p, fs, dcache_.p, linv_.p);
+        // rows per CTA: 64 while the launch fits in about one wave (two CTAs per
+        // SM), more once many fronts x problems share it (fewer redundant
+        // diagonal-block factorizations)
+        const int nrb = std::max(1, cdiv(rows, kPanelRows));
+        const int per = std::max(1, (2 * num_sms_) / std::max(1, nl * B));
+        const int nz = std::min(nrb, per);
+        const int rpc = kPanelRows * cdiv(nrb, nz);
+        k_panel64<<<dim3(nl, B, std::max(1, cdiv(rows, rpc))), 256, kPanelSmem, stream_>>>(
+            ds_, lst, j0, rpc, F_.p, fs, dcache_.p, linv_.p);
         int nt = cdiv(rows, kUT64);
         k_update64<<<dim3(nl, B, std::max(1, nt * (nt + 1) / 2)), 128, kUpdSmem, stream_>>>(ds_, lst, j0, F_.p, fs,
                                                                                           dcache_.p);
@@ -350,7 +362,7 @@ void GpuFactor::selinv_levels(int B) {
     const LevelPlan& P = levels_[l];
     if (!P.si_small.empty()) {
       int mm = P.mmax_si_small;
-      k_selinv_small<256><<<dim3((unsigned)P.si_small.size(), B), 256, (mm * mm * 2) * 8, stream_>>>(
+      k_selinv_small<256><<<dim3((unsigned)P.si_small.size(), B), 256, small_selinv_smem(mm), stream_>>>(
           ds_, d_lists_.p + P.off_si_small, F_.p, Sg_.p, fs);
       ++launches_;
     }

@@ -139,6 +139,7 @@ class GpuFactor {
   DBuf<int> status_, ldflag_;
   DBuf<unsigned> ldticket_;
   int nfill_ = 0, nldchunk_ = 0;  // fill chunks; log-det chunks per problem
+  int num_sms_ = 148;
   int64_t ntot_ = 0;              // compact panel entries per problem
   int64_t launches_ = 0;
 };

@@ -14,6 +14,8 @@ inline int cdiv(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 inline unsigned grid1(int64_t n, int threads = 256, int cap = 2048) {
   return (unsigned)std::max(1, std::min<int>(cdiv(n, threads), cap));
 }
+// CTAs of a multi-CTA reduction over len elements (at least one).
+inline unsigned nchunks(int64_t len, int per_cta) { return (unsigned)std::max(1, cdiv(len, per_cta)); }
 }  // namespace
 
 // u[b][j] = sum_a A[a,j] v[b][a]   (A^T in CSR)
@@ -30,45 +32,6 @@ __global__ void k_spmv_at(int n, const int64_t* __restrict__ atp, const int* __r
     }
     u[(int64_t)b * n + j] = s;
   }
-}
-
-// out[b][t] = z_b' M_t x_b
-template <int NT>
-__global__ void __launch_bounds__(NT) k_bilinear_forms(int n, int ncomp, const int64_t* __restrict__ qcp,
-                                                       const int* __restrict__ qri, const double* __restrict__ comp,
-                                                       int64_t nnz, const double* __restrict__ z,
-                                                       const double* __restrict__ x, double* __restrict__ out) {
-  __shared__ double red[NT];
-  const int b = blockIdx.x;
-  double acc[8];
-  for (int t = 0; t < 8; ++t) acc[t] = 0.0;
-  for (int j = threadIdx.x; j < n; j += NT) {
-    const double zj = z[(int64_t)b * n + j];
-    for (int64_t p = qcp[j]; p < qcp[j + 1]; ++p) {
-      const double zx = zj * x[(int64_t)b * n + qri[p]];
-      for (int t = 0; t < ncomp && t < 8; ++t) acc[t] += comp[(int64_t)t * nnz + p] * zx;
-    }
-  }
-  for (int t = 0; t < ncomp && t < 8; ++t) {
-    double s = block_sum<NT>(acc[t], red);
-    if (threadIdx.x == 0) out[(int64_t)b * (ncomp + 1) + t] = s;
-  }
-}
-
-// d loglik / d log(scale) for Gaussian precision scaling: sum_i (1/2 - w_i r_i^2 / 2)
-template <int NT>
-__global__ void __launch_bounds__(NT) k_gauss_dll(int64_t nobs, const double* __restrict__ eta,
-                                                  const double* __restrict__ y, const double* __restrict__ w,
-                                                  double* __restrict__ out) {
-  __shared__ double red[NT];
-  const int b = blockIdx.x;
-  double s = 0.0;
-  for (int64_t i = threadIdx.x; i < nobs; i += NT) {
-    const double r = eta[(int64_t)b * nobs + i] - y[i];
-    s += 0.5 - 0.5 * w[(int64_t)b * nobs + i] * r * r;
-  }
-  s = block_sum<NT>(s, red);
-  if (threadIdx.x == 0) out[b] = s;
 }
 
 __global__ void k_mul(int64_t len, const double* a, const double* b, double* c) {  // c may alias a
@@ -222,6 +185,13 @@ LaplaceEngine::LaplaceEngine(const LaplaceSpec& spec, int max_batch, cudaStream_
   tmp_o_.alloc(B * std::max<int64_t>(nobs, 1));
   sig_.alloc(B * nnz_);
   red_.alloc(B * 4 * (spec_.ncomp + 1) + B * 8);
+  {
+    const int64_t maxch = std::max<int64_t>({1, (nnz_ + kRedChunk - 1) / kRedChunk, (nobs + kRedChunk - 1) / kRedChunk,
+                                             (n + kColChunk - 1) / kColChunk});
+    gpart_.alloc(B * maxch * 9);
+    gtick_.alloc(B);
+    INLA_CUDA(cudaMemsetAsync(gtick_.p, 0, sizeof(unsigned) * B, stream_));
+  }
   stats_.alloc(2 * B);
   alpha_.alloc(B);
   ldp_.alloc(B);
@@ -285,8 +255,8 @@ void LaplaceEngine::eval(int B, const double* coef, const double* p1scale, int f
     F_->selinv(B);
     k_pattern_full<<<dim3(grid1(nnz_), B), 256, 0, stream_>>>(nnz_, F_->d_spos_full(), F_->d_sigma(),
                                                               F_->front_total(), sig_.p);
-    k_trace_contract<256><<<B, 256, 0, stream_>>>(nnz_, T, comp_.p, sig_.p, cptr_.p, cobs_.p, cprod_.p, nullptr,
-                                                  nobs, d_trP);
+    k_trace_contract_g<<<dim3(nchunks(nnz_, kRedChunk), B), 256, 0, stream_>>>(
+        nnz_, T, comp_.p, sig_.p, cptr_.p, cobs_.p, cprod_.p, nullptr, nobs, gpart_.p, gtick_.p, d_trP);
     launches_ += 2;
   }
 
@@ -400,11 +370,14 @@ void LaplaceEngine::eval(int B, const double* coef, const double* p1scale, int f
 
   // ---- marginal likelihood pieces (inference.rs:953-972) ------------------------
   eval_lik(B, x_.p);
-  k_row_sum<256><<<B, 256, 0, stream_>>>(nobs, logp_.p, d_scal);
-  k_quad_forms<256><<<B, 256, 0, stream_>>>((int)n, T, qcp_.p, qri_.p, comp_.p, nnz_, coef_.p, x_.p, d_xMx);
+  k_row_sum_g<<<dim3(nchunks(nobs, kRedChunk), B), 256, 0, stream_>>>(nobs, logp_.p, gpart_.p, gtick_.p, d_scal);
+  k_quad_forms_g<<<dim3(nchunks(n, kColChunk), B), 256, 0, stream_>>>((int)n, T, qcp_.p, qri_.p, comp_.p, nnz_,
+                                                                      coef_.p, nullptr, x_.p, gpart_.p, gtick_.p,
+                                                                      d_xMx);
   launches_ += 2;
   if (spec_.family == FAM_GAUSSIAN && grad) {
-    k_gauss_dll<256><<<B, 256, 0, stream_>>>(nobs, eta_.p, y_.p, w_.p, d_scal + B);
+    k_gauss_dll_g<<<dim3(nchunks(nobs, kRedChunk), B), 256, 0, stream_>>>(nobs, eta_.p, y_.p, w_.p, gpart_.p,
+                                                                          gtick_.p, d_scal + B);
     ++launches_;
   }
   std::vector<double> ldpost(B), ldprior(B), scal(2 * B), xmx((size_t)B * T1);
@@ -418,8 +391,8 @@ void LaplaceEngine::eval(int B, const double* coef, const double* p1scale, int f
     if (grad) {
       k_pattern_full<<<dim3(grid1(nnz_), B), 256, 0, stream_>>>(nnz_, F_->d_spos_full(), F_->d_sigma(),
                                                                 F_->front_total(), sig_.p);
-      k_trace_contract<256><<<B, 256, 0, stream_>>>(nnz_, T, comp_.p, sig_.p, cptr_.p, cobs_.p, cprod_.p, w_.p, nobs,
-                                                    d_trQ);
+      k_trace_contract_g<<<dim3(nchunks(nnz_, kRedChunk), B), 256, 0, stream_>>>(
+          nnz_, T, comp_.p, sig_.p, cptr_.p, cobs_.p, cprod_.p, w_.p, nobs, gpart_.p, gtick_.p, d_trQ);
       launches_ += 2;
       if (spec_.family != FAM_GAUSSIAN) {
         // implicit term: u = A^T (dw .* v), v_i = a_i' Sigma a_i; z = Q_post^-1 u
@@ -428,8 +401,8 @@ void LaplaceEngine::eval(int B, const double* coef, const double* p1scale, int f
         k_mul<<<dim3(grid1(nobs), B), 256, 0, stream_>>>(nobs, tmp_o_.p, dw_.p, tmp_o_.p);
         k_spmv_at<<<dim3(grid1(n), B), 256, 0, stream_>>>((int)n, atp, ati_.p, atv_.p, nobs, tmp_o_.p, tmp_n_.p);
         F_->solve(tmp_n_.p, n, B);
-        k_bilinear_forms<256><<<B, 256, 0, stream_>>>((int)n, T, qcp_.p, qri_.p, comp_.p, nnz_, tmp_n_.p, x_.p,
-                                                      d_zMx);
+        k_quad_forms_g<<<dim3(nchunks(n, kColChunk), B), 256, 0, stream_>>>(
+            (int)n, T, qcp_.p, qri_.p, comp_.p, nnz_, coef_.p, tmp_n_.p, x_.p, gpart_.p, gtick_.p, d_zMx);
         launches_ += 4;
       }
     }

@@ -225,6 +225,148 @@ __device__ __forceinline__ double block_max(double v, double* red) {
   return r;
 }
 
+// Multi-CTA reductions with a fixed summation order. A kernel launched on a
+// grid (nchunk, B) of 256-thread CTAs reduces NQ per-thread values over its
+// CTA (fixed tree), stores them at part[((b * nchunk) + chunk) * NQ + q], and the
+// CTA that takes the last ticket of problem b adds the partials in chunk
+// order and writes out[b * ostride + q] for q < nlo and, when has_last,
+// v[NQ - 1] to out[b * ostride + last_off]; it then resets the ticket.
+constexpr int kRedChunk = 2048;  // elements per CTA (256 threads x 8)
+__device__ __forceinline__ double block_sum256(double v, double* red) { return block_sum<256>(v, red); }
+
+template <int NQ>
+__device__ __forceinline__ void grid_reduce_store(const double (&v)[NQ], int nlo, bool has_last, double* part,
+                                                  unsigned* ticket, double* out, int64_t ostride, int last_off) {
+  __shared__ double red[256];
+  __shared__ bool last;
+  const int b = blockIdx.y, nch = gridDim.x;
+  double* pb = part + ((int64_t)b * nch) * NQ;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    if (q < nlo || (has_last && q == NQ - 1)) {
+      const double sq = block_sum256(v[q], red);
+      if (threadIdx.x == 0) pb[(int64_t)blockIdx.x * NQ + q] = sq;
+    }
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(&ticket[b], 1u) == (unsigned)(nch - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    if (q < nlo || (has_last && q == NQ - 1)) {
+      double a = 0.0;
+      for (int c = threadIdx.x; c < nch; c += 256) a += __ldcg(pb + (int64_t)c * NQ + q);
+      const double sq = block_sum256(a, red);
+      if (threadIdx.x == 0) out[(int64_t)b * ostride + (q < nlo ? q : last_off)] = sq;
+    }
+  }
+  if (threadIdx.x == 0) ticket[b] = 0u;
+}
+
+// sum_i v[b][i] -> out[b]
+__global__ void __launch_bounds__(256) k_row_sum_g(int64_t len, const double* __restrict__ v, double* part,
+                                                   unsigned* ticket, double* __restrict__ out) {
+  const int b = blockIdx.y;
+  double a[1] = {0.0};
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int64_t i = (int64_t)blockIdx.x * kRedChunk + threadIdx.x + 256 * u;
+    if (i < len) a[0] += v[(int64_t)b * len + i];
+  }
+  grid_reduce_store<1>(a, 1, false, part, ticket, out, 1, 0);
+}
+
+// d loglik / d log(scale) for Gaussian precision scaling: sum_i (1/2 - w_i r_i^2 / 2)
+__global__ void __launch_bounds__(256) k_gauss_dll_g(int64_t nobs, const double* __restrict__ eta,
+                                                     const double* __restrict__ y, const double* __restrict__ w,
+                                                     double* part, unsigned* ticket, double* __restrict__ out) {
+  const int b = blockIdx.y;
+  double a[1] = {0.0};
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int64_t i = (int64_t)blockIdx.x * kRedChunk + threadIdx.x + 256 * u;
+    if (i < nobs) {
+      const double r = eta[(int64_t)b * nobs + i] - y[i];
+      a[0] += 0.5 - 0.5 * w[(int64_t)b * nobs + i] * r * r;
+    }
+  }
+  grid_reduce_store<1>(a, 1, false, part, ticket, out, 1, 0);
+}
+
+// x^T M_t x (t < ncomp) and x^T Q x = sum_t coef_t x^T M_t x, columns in chunks of
+// kColChunk: out[b][0] = x^T Q x, out[b][1+t] = x^T M_t x. With z != nullptr the
+// bilinear forms z^T M_t x go to out[b][t] (no total).
+constexpr int kColChunk = 1024;  // 256 threads x 4 columns
+__global__ void __launch_bounds__(256) k_quad_forms_g(int n, int ncomp, const int64_t* __restrict__ qcp,
+                                                      const int* __restrict__ qri, const double* __restrict__ comp,
+                                                      int64_t nnz, const double* __restrict__ coef,
+                                                      const double* __restrict__ z, const double* __restrict__ x,
+                                                      double* part, unsigned* ticket, double* __restrict__ out) {
+  const int b = blockIdx.y;
+  const double* xb = x + (int64_t)b * n;
+  const double* zb = z ? z + (int64_t)b * n : xb;
+  double acc[9];
+#pragma unroll
+  for (int t = 0; t < 9; ++t) acc[t] = 0.0;
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int j = blockIdx.x * kColChunk + threadIdx.x + 256 * u;
+    if (j >= n) continue;
+    const double zj = zb[j];
+    for (int64_t p = qcp[j]; p < qcp[j + 1]; ++p) {
+      const double zx = zj * xb[qri[p]];
+#pragma unroll
+      for (int t = 0; t < 8; ++t)
+        if (t < ncomp) acc[t] += comp[(int64_t)t * nnz + p] * zx;
+    }
+  }
+  const int nc = ncomp < 8 ? ncomp : 8;
+  if (z) {
+    grid_reduce_store<9>(acc, nc, false, part, ticket, out, ncomp + 1, 0);
+  } else {
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+      if (t < nc) acc[8] += coef[(int64_t)b * ncomp + t] * acc[t];
+    grid_reduce_store<9>(acc, nc, true, part, ticket, out + 1, ncomp + 1, -1);
+  }
+}
+
+// Trace contractions of a selected inverse given on the full pattern (both
+// triangles): out[b][t] = sum_p sigma[b][p] comp[t][p] (= tr(Sigma M_t)) and
+// out[b][ncomp] = sum_p sigma[b][p] sum_q w2[b][obs_q] prod_q (= tr(Sigma A^T diag(w2) A)).
+__global__ void __launch_bounds__(256) k_trace_contract_g(int64_t nnz, int ncomp, const double* __restrict__ comp,
+                                                          const double* __restrict__ sigma,
+                                                          const int* __restrict__ cptr, const int* __restrict__ cobs,
+                                                          const double* __restrict__ cprod,
+                                                          const double* __restrict__ w2, int64_t nobs, double* part,
+                                                          unsigned* ticket, double* __restrict__ out) {
+  const int b = blockIdx.y;
+  const double* sb = sigma + (int64_t)b * nnz;
+  double acc[9];
+#pragma unroll
+  for (int t = 0; t < 9; ++t) acc[t] = 0.0;
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int64_t p = (int64_t)blockIdx.x * kRedChunk + threadIdx.x + 256 * u;
+    if (p >= nnz) continue;
+    const double sv = sb[p];
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+      if (t < ncomp) acc[t] += sv * comp[(int64_t)t * nnz + p];
+    if (w2) {
+      double a = 0.0;
+      for (int q = cptr[p]; q < cptr[p + 1]; ++q) a += w2[(int64_t)b * nobs + cobs[q]] * cprod[q];
+      acc[8] += sv * a;
+    }
+  }
+  const int nc = ncomp < 8 ? ncomp : 8;
+  grid_reduce_store<9>(acc, nc, true, part, ticket, out, ncomp + 1, ncomp);
+}
+
 // out[b] = {max|step|, all finite ? 1 : 0}
 template <int NT>
 __global__ void __launch_bounds__(NT) k_step_stats(int n, const double* __restrict__ step, double* __restrict__ out) {

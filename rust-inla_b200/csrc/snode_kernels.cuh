@@ -587,6 +587,20 @@ __device__ __forceinline__ double parent_sigma(const double* Sp, int mp, int pi,
   return pi >= pj ? Sp[pi + (int64_t)pj * mp] : Sp[pj + (int64_t)pi * mp];
 }
 
+// Shared memory of k_selinv_small for fronts of up to m rows (bytes).
+__host__ __device__ constexpr int small_selinv_smem(int m) {
+  return (2 * m * dense_ld(m) + 16 * dense_uld(m) + 2 * 16 * kLamLd + 64 + 16) * 8;
+}
+
+// Selected inverse of a small front, one CTA per (front, problem): Sigma is kept
+// with both triangles in shared memory (Sigma_RR gathered from the parent),
+// and the pivot columns are processed in 16-column blocks J from right to
+// left, A = rows after J:
+//   G = Sigma_AA L_AJ,  X = -G L_JJ^-1 = Sigma_AJ,  P = L_AJ^T X,
+//   Sigma_JJ = L_JJ^-T (D_J^-1 L_JJ^-1 - P)
+// (the block form of the Takahashi recurrence, crates/inla_math/src/sparse_ldlt.rs:366-432),
+// with tensor-core tiles for the products and L_JJ^-1 formed by one warp
+// while the others compute G.
 template <int NT>
 __global__ void __launch_bounds__(NT) k_selinv_small(DevSym S, const int* __restrict__ list,
                                                      const double* __restrict__ F, double* __restrict__ Sg,
@@ -594,51 +608,158 @@ __global__ void __launch_bounds__(NT) k_selinv_small(DevSym S, const int* __rest
   extern __shared__ double smem[];
   const int s = list[blockIdx.x], b = blockIdx.y;
   const int k = sn_k(S, s), m = sn_m(S, s), r = m - k;
-  double* sig = smem;           // m*m, lower used
-  double* Lp = smem + m * m;    // m*k panel
-  __shared__ double red[NT / 32];
+  const int ld = dense_ld(m), uld = dense_uld(m);
+  double* Sm = smem;               // Sigma, both triangles: Sm[i + j*ld]
+  double* Lp = Sm + m * ld;        // L panel: Lp[i + c*ld], c < k
+  double* Xb = Lp + m * ld;        // [16][uld]: G rows of A
+  double* lam = Xb + 16 * uld;     // L_JJ^-1 (ld kLamLd)
+  double* Pm = lam + 16 * kLamLd;  // P, then M = D^-1 L^-1 - P
+  double* xbuf = Pm + 16 * kLamLd; // warp scratch
+  double* dv = xbuf + 64;          // 1 / d_j of the block
   const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
   double* Ss = Sg + (int64_t)b * fstride + S.fptr[s];
-  for (int e = threadIdx.x; e < m * k; e += NT) Lp[e] = Fs[e];
+  for (int e = threadIdx.x; e < m * k; e += NT) {
+    const int c = e / m, i = e - c * m;
+    cp_async8(&Lp[i + c * ld], Fs + e);
+  }
+  cp_async_commit();
   if (r > 0) {
     const int p = S.parent[s];
     const int mp = sn_m(S, p);
     const double* Sp = Sg + (int64_t)b * fstride + S.fptr[p];
     const int* rel = S.relx + S.rowptr[s] + k;
-    for (int e = threadIdx.x; e < r * r; e += NT) {
-      int jj = e / r, ii = e - jj * r;
-      if (ii >= jj) sig[(k + ii) + (k + jj) * m] = parent_sigma(Sp, mp, rel[ii], rel[jj]);
+    const int rr = r * r;
+    int e = threadIdx.x;
+    for (; e + 3 * NT < rr; e += 4 * NT) {
+      double v[4];
+      int ia[4], ja[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int ee = e + u * NT;
+        const int jj = ee / r, ii = ee - jj * r;
+        ia[u] = ii >= jj ? ii : -1;
+        ja[u] = jj;
+        v[u] = ii >= jj ? parent_sigma(Sp, mp, rel[ii], rel[jj]) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (ia[u] >= 0) {
+          Sm[(k + ia[u]) + (k + ja[u]) * ld] = v[u];
+          Sm[(k + ja[u]) + (k + ia[u]) * ld] = v[u];
+        }
+    }
+    for (; e < rr; e += NT) {
+      const int jj = e / r, ii = e - jj * r;
+      if (ii < jj) continue;
+      const double v = parent_sigma(Sp, mp, rel[ii], rel[jj]);
+      Sm[(k + ii) + (k + jj) * ld] = v;
+      Sm[(k + jj) + (k + ii) * ld] = v;
     }
   }
+  cp_async_wait<0>();
   __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int j = k - 1; j >= 0; --j) {
-    const double* Lj = Lp + j * m;
-    for (int i = j + 1 + threadIdx.x; i < m; i += NT) {
-      double acc = 0.0;
-      for (int l = j + 1; l < m; ++l) {
-        double sv = l >= i ? sig[l + i * m] : sig[i + l * m];
-        acc += Lj[l] * sv;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = NT / 32;
+  const int g = lane >> 2, tg = lane & 3;
+  const int nblk = (k + 15) / 16;
+  for (int bi = nblk - 1; bi >= 0; --bi) {
+    const int j0 = bi * 16, j1 = min(k, j0 + 16), w = j1 - j0, na = m - j1;
+    const int T = (na + 7) >> 3;
+    if (warp == 0) {
+      warp_trinv16(Lp + j0 + j0 * ld, ld, w, lam, xbuf);
+      if (lane < 16) dv[lane] = lane < w ? 1.0 / Lp[(j0 + lane) * (ld + 1)] : 0.0;
+    } else {
+      // G = Sigma_AA L_AJ: 8 rows x 16 columns per task, K = na split in two chains
+      for (int task = warp - 1; task < T; task += nw - 1) {
+        const int i = j1 + 8 * task + g;
+        double c[2][2][2] = {};
+        for (int kk = 0; kk < na; kk += 8) {
+#pragma unroll
+          for (int hh = 0; hh < 2; ++hh) {
+            const int l = j1 + kk + 4 * hh + tg;
+            const double a = (i < m && l < m) ? Sm[i + l * ld] : 0.0;
+#pragma unroll
+            for (int ct = 0; ct < 2; ++ct) {
+              const int t = ct * 8 + g;
+              const double bb = (l < m && t < w) ? Lp[l + (j0 + t) * ld] : 0.0;
+              dmma884(c[hh][ct][0], c[hh][ct][1], a, bb);
+            }
+          }
+        }
+#pragma unroll
+        for (int ct = 0; ct < 2; ++ct)
+#pragma unroll
+          for (int h2 = 0; h2 < 2; ++h2) Xb[(ct * 8 + 2 * tg + h2) * uld + 8 * task + g] = c[0][ct][h2] + c[1][ct][h2];
       }
-      sig[i + j * m] = -acc;
     }
     __syncthreads();
-    double acc = 0.0;
-    for (int l = j + 1 + threadIdx.x; l < m; l += NT) acc += Lj[l] * sig[l + j * m];
+    // X = -G L_JJ^-1 -> Sigma_AJ (both triangles)
+    for (int task = warp; task < T; task += nw) {
+      double c[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) red[warp] = acc;
+      for (int kk = 0; kk < 16; kk += 4) {
+        const double a = Xb[(kk + tg) * uld + 8 * task + g];
+#pragma unroll
+        for (int ct = 0; ct < 2; ++ct) dmma884(c[ct][0], c[ct][1], a, lam[(kk + tg) + (ct * 8 + g) * kLamLd]);
+      }
+      const int i = j1 + 8 * task + g;
+#pragma unroll
+      for (int ct = 0; ct < 2; ++ct)
+#pragma unroll
+        for (int h2 = 0; h2 < 2; ++h2) {
+          const int t = ct * 8 + 2 * tg + h2;
+          if (i < m && t < w) {
+            Sm[i + (j0 + t) * ld] = -c[ct][h2];
+            Sm[(j0 + t) + i * ld] = -c[ct][h2];
+          }
+        }
+    }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      double t = 0.0;
-      for (int w = 0; w < NT / 32; ++w) t += red[w];
-      sig[j + j * m] = 1.0 / Lj[j] - t;
+    // P[j][i] = sum_{l in A} L[l, j0+j] X[l, i]  (4 tiles, K = na in two chains)
+    for (int task = warp; task < 4; task += nw) {
+      const int jt = task >> 1, it = task & 1;
+      double c[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+      for (int kk = 0; kk < na; kk += 8) {
+#pragma unroll
+        for (int hh = 0; hh < 2; ++hh) {
+          const int l = j1 + kk + 4 * hh + tg;
+          const double a = (l < m) ? Lp[l + (j0 + jt * 8 + g) * ld] : 0.0;
+          const double bb = (l < m) ? Sm[l + (j0 + it * 8 + g) * ld] : 0.0;
+          dmma884(c[hh][0], c[hh][1], a, bb);
+        }
+      }
+#pragma unroll
+      for (int h2 = 0; h2 < 2; ++h2) Pm[(jt * 8 + g) + (it * 8 + 2 * tg + h2) * kLamLd] = c[0][h2] + c[1][h2];
+    }
+    __syncthreads();
+    // M = D^-1 L_JJ^-1 - P
+    for (int e = threadIdx.x; e < 256; e += NT) {
+      const int rr2 = e & 15, cc = e >> 4;
+      Pm[rr2 + cc * kLamLd] = (rr2 < w && cc < w) ? lam[rr2 + cc * kLamLd] * dv[rr2] - Pm[rr2 + cc * kLamLd] : 0.0;
+    }
+    __syncthreads();
+    // Sigma_JJ = L_JJ^-T M
+    for (int task = warp; task < 4; task += nw) {
+      const int jt = task >> 1, it = task & 1;
+      double c0 = 0.0, c1 = 0.0;
+#pragma unroll
+      for (int kk = 0; kk < 16; kk += 4)
+        dmma884(c0, c1, lam[(kk + tg) + (jt * 8 + g) * kLamLd], Pm[(kk + tg) + (it * 8 + g) * kLamLd]);
+      const int rr2 = jt * 8 + g;
+#pragma unroll
+      for (int h2 = 0; h2 < 2; ++h2) {
+        const int cc = it * 8 + 2 * tg + h2;
+        const double v = h2 ? c1 : c0;
+        if (rr2 < w && cc < w && rr2 >= cc) {
+          Sm[(j0 + rr2) + (j0 + cc) * ld] = v;
+          Sm[(j0 + cc) + (j0 + rr2) * ld] = v;
+        }
+      }
     }
     __syncthreads();
   }
   for (int e = threadIdx.x; e < m * m; e += NT) {
-    int col = e / m, row = e - col * m;
-    if (row >= col) Ss[e] = sig[e];
+    const int col = e / m, row = e - col * m;
+    if (row >= col) Ss[e] = Sm[row + col * ld];
   }
 }
 

@@ -27,10 +27,10 @@ namespace inla {
 namespace {
 
 constexpr int kB64 = 64;         // block-column width
-constexpr int kPanelRows = 64;   // rows per panel CTA
+constexpr int kPanelRows = 64;   // rows per panel GEMM sub-block
 constexpr int kLd64 = dense_ld(kB64);
 constexpr int kULd64 = dense_uld(kB64);
-constexpr int kPanelSmem = (3 * kB64 * kLd64 + 16 * kULd64 + kDenseScratch) * 8;
+constexpr int kPanelSmem = (2 * kB64 * kLd64 + 16 * kULd64 + kDenseScratch) * 8;
 constexpr int kUpdSmem = 2 * kB64 * kLd64 * 8;
 constexpr int kSiGemmSmem = 3 * 64 * (kB64 + 1) * 8;
 constexpr int kSiDiagSmem = 3 * kB64 * (kB64 + 1) * 8;
@@ -160,25 +160,27 @@ __global__ void __launch_bounds__(256) k_si_gather8(DevSym S, const int* __restr
 // The factored diagonal block goes to dcache[(list index, problem)] (written by
 // CTA 0): the other CTAs of this launch still read the unfactored block from
 // the front, so it is copied into the front by k_update64 of the same step.
-// Each CTA: blocked LDL^T + inverse of the diagonal block, then its 64 rows
-// X = F_rows (L_JJ^-T D^-1) as one tensor-core GEMM.
-__global__ void __launch_bounds__(256) k_panel64(DevSym S, const int* __restrict__ list, int j0,
+// Each CTA: blocked LDL^T + inverse of the diagonal block, then the rows
+// [r0, r0 + rpc) (rpc a multiple of 64) in 64-row sub-blocks, each
+// X = F_rows (L_JJ^-T D^-1) as one tensor-core GEMM. The row sub-blocks are
+// staged in the diagonal block's buffer once it is no longer needed, which
+// keeps the CTA at 84 KB of shared memory (two CTAs per SM).
+__global__ void __launch_bounds__(256) k_panel64(DevSym S, const int* __restrict__ list, int j0, int rpc,
                                                  double* __restrict__ F, int64_t fstride,
                                                  double* __restrict__ dcache, double* __restrict__ linv) {
   extern __shared__ double smem64[];
   constexpr int ld = kLd64;
-  double* Ds = smem64;         // [64 cols][ld]: diagonal block, factored in place
+  double* Ds = smem64;         // [64 cols][ld]: diagonal block, factored in place; then row sub-blocks
   double* Li = Ds + kB64 * ld; // L_JJ^-1, then Bm[u + t*ld] = Li[t][u] / d_t
-  double* Fa = Li + kB64 * ld; // rows of this CTA: Fa[t*ld + r] = F[r0 + r, j0 + t]
-  double* U = Fa + kB64 * ld;  // [16][kULd64] scratch of cta_ldlt, then 1 / d_t
+  double* U = Li + kB64 * ld;  // [16][kULd64] scratch of cta_ldlt, then 1 / d_t
   double* ws = U + 16 * kULd64;
   const int s = list[blockIdx.x], b = blockIdx.y;
   const int k = lg_k(S, s), m = lg_m(S, s);
   if (j0 >= k) return;
   const int w = min(kB64, k - j0);
-  const int r0 = j0 + w + blockIdx.z * kPanelRows;
+  const int r0 = j0 + w + blockIdx.z * rpc;
   if (blockIdx.z > 0 && r0 >= m) return;
-  const int rows = max(0, min(kPanelRows, m - r0));
+  const int r1 = min(m, r0 + rpc);
   double* Fs = F + (int64_t)b * fstride + S.fptr[s];
   const double* D0 = Fs + j0 + (int64_t)j0 * m;
   for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) {
@@ -186,8 +188,6 @@ __global__ void __launch_bounds__(256) k_panel64(DevSym S, const int* __restrict
     if (r < w && c < w && r >= c) cp_async8(&Ds[r + c * ld], D0 + r + (int64_t)c * m);
     else Ds[r + c * ld] = 0.0;
     Li[r + c * ld] = 0.0;
-    if (r < rows && c < w) cp_async8(&Fa[c * ld + r], Fs + (r0 + r) + (int64_t)(j0 + c) * m);
-    else Fa[c * ld + r] = 0.0;
   }
   cp_async_commit();
   cp_async_wait<0>();
@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(256) k_panel64(DevSym S, const int* __restrict
       lc[e] = Li[r + c * ld];  // zero outside the w x w lower triangle
     }
   }
-  if (rows == 0) return;
+  if (r0 >= r1) return;
   double* dinv = U;
   if (threadIdx.x < kB64) dinv[threadIdx.x] = threadIdx.x < w ? 1.0 / Ds[threadIdx.x * (ld + 1)] : 0.0;
   __syncthreads();
@@ -218,37 +218,50 @@ __global__ void __launch_bounds__(256) k_panel64(DevSym S, const int* __restrict
     const int e = threadIdx.x + 256 * q, u = e & 63, t = e >> 6;
     Li[u + t * ld] = bv[q];
   }
-  __syncthreads();
-  // X (64 x 64) = Fa (64 x 64) * Bm; warp tile 32 x 16
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wr = (warp & 1) * 32, wc = (warp >> 1) * 16;
   const int g = lane >> 2, tg = lane & 3;
-  double acc[4][2][2];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int q = 0; q < 2; ++q) acc[a][q][0] = acc[a][q][1] = 0.0;
-#pragma unroll 4
-  for (int kk = 0; kk < kB64; kk += 4) {
-    double af[4], bf[2];
-#pragma unroll
-    for (int a = 0; a < 4; ++a) af[a] = Fa[(kk + tg) * ld + wr + a * 8 + g];
-#pragma unroll
-    for (int q = 0; q < 2; ++q) bf[q] = Li[(kk + tg) + (wc + q * 8 + g) * ld];
+  const int wk = (w + 3) & ~3;
+  double* Fa = Ds;  // row sub-block: Fa[t*ld + r] = F[rb + r, j0 + t]
+  for (int rb = r0; rb < r1; rb += kPanelRows) {
+    const int rows = min(kPanelRows, r1 - rb);
+    __syncthreads();  // previous sub-block (or the diagonal block) fully consumed
+    for (int e = threadIdx.x; e < kB64 * kPanelRows; e += blockDim.x) {
+      const int c = e >> 6, r = e & 63;
+      if (r < rows && c < w) cp_async8(&Fa[c * ld + r], Fs + (rb + r) + (int64_t)(j0 + c) * m);
+      else Fa[c * ld + r] = 0.0;
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    // X (64 x 64) = Fa (64 x w) * Bm (w x 64); warp tile 32 x 16
+    double acc[4][2][2];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
-      for (int q = 0; q < 2; ++q) mma884(acc[a][q][0], acc[a][q][1], af[a], bf[q]);
+      for (int q = 0; q < 2; ++q) acc[a][q][0] = acc[a][q][1] = 0.0;
+#pragma unroll 4
+    for (int kk = 0; kk < wk; kk += 4) {
+      double af[4], bf[2];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) af[a] = Fa[(kk + tg) * ld + wr + a * 8 + g];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) bf[q] = Li[(kk + tg) + (wc + q * 8 + g) * ld];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int q = 0; q < 2; ++q) mma884(acc[a][q][0], acc[a][q][1], af[a], bf[q]);
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int q = 0; q < 2; ++q)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int r = wr + a * 8 + g, t = wc + q * 8 + tg * 2 + h;
+          if (r < rows && t < w) Fs[(rb + r) + (int64_t)(j0 + t) * m] = acc[a][q][h];
+        }
   }
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int q = 0; q < 2; ++q)
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int r = wr + a * 8 + g, t = wc + q * 8 + tg * 2 + h;
-        if (r < rows && t < w) Fs[(r0 + r) + (int64_t)(j0 + t) * m] = acc[a][q][h];
-      }
 }
 
 constexpr int kUT64 = 64;
@@ -307,8 +320,9 @@ __global__ void __launch_bounds__(128) k_update64(DevSym S, const int* __restric
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int q = 0; q < 4; ++q) acc[a][q][0] = acc[a][q][1] = 0.0;
-#pragma unroll 4
-  for (int kk = 0; kk < kB64; kk += 4) {
+  const int wk = (w + 3) & ~3;  // only the block's w columns contribute
+#pragma unroll 2
+  for (int kk = 0; kk < wk; kk += 4) {
     double af[4], bf[4];
     const double dk = dsh[kk + tg];
 #pragma unroll
