@@ -38,16 +38,20 @@ enum {
 
 /* Fill-reducing ordering selector. INLA_ORDER_REFERENCE restates
  * choose_symmetric_order (crates/inla_math/src/ordering.rs:149-162):
- * time-major Kronecker -> RCM -> AMD. INLA_ORDER_AMD is the GPU default:
- * the RCM branch yields a path-like elimination tree with no level
- * parallelism. Numeric results do not depend on the ordering beyond rounding. */
+ * time-major Kronecker -> RCM -> AMD (the RCM branch yields a path-like
+ * elimination tree with no level parallelism). INLA_ORDER_ND (nested
+ * dissection; no reference counterpart) is the default of the batched
+ * engines: a shallower elimination tree with fewer pivots on its longest path
+ * than INLA_ORDER_AMD.
+ * Numeric results do not depend on the ordering beyond rounding. */
 enum {
   INLA_ORDER_REFERENCE = 0,
   INLA_ORDER_AMD = 1,
   INLA_ORDER_RCM = 2,
   INLA_ORDER_NATURAL = 3,
   INLA_ORDER_CUSTOM = 4,
-  INLA_ORDER_TIME_MAJOR = 5
+  INLA_ORDER_TIME_MAJOR = 5,
+  INLA_ORDER_ND = 6
 };
 
 /* Last error message of the calling thread ("" if none). */

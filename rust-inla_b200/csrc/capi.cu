@@ -114,7 +114,7 @@ int inla_choose_symmetric_order(int64_t n, const int64_t* colptr, const int64_t*
 int inla_solver_new(int ordering, inla_solver** out) {
   try {
     if (!out) return fail(INLA_ERR_INVALID, "null output handle");
-    if (ordering < 0 || ordering > INLA_ORDER_TIME_MAJOR) return fail(INLA_ERR_INVALID, "unsupported ordering");
+    if (ordering < 0 || ordering > INLA_ORDER_ND) return fail(INLA_ERR_INVALID, "unsupported ordering");
     auto* s = new inla_solver();
     s->ordering = ordering;
     *out = s;

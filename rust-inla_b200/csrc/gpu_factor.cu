@@ -11,6 +11,9 @@ namespace inla {
 namespace {
 inline int cdiv(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 
+// Parent columns per extend-add CTA: the m-row slice must fit in shared memory.
+inline int gather_cols(int m) { return std::max(1, std::min(kGatherCols, (200 * 1024) / (8 * std::max(m, 1)))); }
+
 template <class K>
 void set_smem(K kernel, int bytes) {
   INLA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
@@ -25,6 +28,7 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
   nnz_ = (int64_t)S.rowidx.size();
   if (n >= (1LL << 31) || (int64_t)S.sn_rows.size() >= (1LL << 31) || nnz_ >= (1LL << 31))
     throw std::runtime_error("problem too large for 32-bit indices");
+  if (S.max_m > 25600) throw std::runtime_error("front with more than 25600 rows (extend-add slice exceeds shared memory)");
 
   std::vector<int> first(ns + 1), rowptr(ns + 1), rows(S.sn_rows.size()), relx(S.sn_rows.size(), -1),
       child_ptr(ns + 1), child_list(S.child_list.size()), parent(ns), uoff(ns + 1, 0), perm(n);
@@ -165,6 +169,7 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
     INLA_CUDA(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev));
   }
   set_smem(k_update64, kUpdSmem);
+  set_smem(k_gather8, 200 * 1024 + 8 * kGatherCols * 8);
   set_smem(k_si_gemm64, kSiGemmSmem);
   set_smem(k_si_diag64, kSiDiagSmem);
   INLA_CUDA(cudaStreamSynchronize(stream_));
@@ -240,7 +245,9 @@ void GpuFactor::run_factor_levels(int B) {
     if (!P.large.empty()) {
       const int nl = (int)P.large.size();
       const int* lst = d_lists_.p + P.off_large;
-      k_gather8<<<dim3(nl, B, cdiv(P.mmax_large, kGatherCols)), 256, 0, stream_>>>(ds_, lst, F_.p, fs);
+      const int gcols = gather_cols(P.mmax_large);
+      k_gather8<<<dim3(nl, B, cdiv(P.mmax_large, gcols)), 256, gcols * P.mmax_large * 8, stream_>>>(ds_, lst, F_.p,
+                                                                                             fs, gcols);
       ++launches_;
       for (int j0 = 0; j0 < P.kmax_large; j0 += kB64) {
         int rows = P.mmax_large - j0;
@@ -376,7 +383,7 @@ void GpuFactor::selinv_levels(int B) {
       const int nblk = cdiv(P.kmax_si_large, kB64);
       const int ptiles = cdiv(P.mmax_si_large, kSiT);
       for (int jb = 0; jb < nblk; ++jb) {
-        k_si_gemm64<<<dim3(nl, B, ptiles), 128, kSiGemmSmem, stream_>>>(ds_, lst, jb, F_.p, Sg_.p, fs, ppart_.p,
+        k_si_gemm64<<<dim3(nl, B, ptiles), 256, kSiGemmSmem, stream_>>>(ds_, lst, jb, F_.p, Sg_.p, fs, ppart_.p,
                                                                         ptiles, linv_.p);
         k_si_diag64<<<dim3(nl, B), 256, kSiDiagSmem, stream_>>>(ds_, lst, jb, F_.p, Sg_.p, fs, ppart_.p, ptiles,
                                                                 linv_.p);

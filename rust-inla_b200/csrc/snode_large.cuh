@@ -32,7 +32,7 @@ constexpr int kLd64 = dense_ld(kB64);
 constexpr int kULd64 = dense_uld(kB64);
 constexpr int kPanelSmem = (2 * kB64 * kLd64 + 16 * kULd64 + kDenseScratch) * 8;
 constexpr int kUpdSmem = 2 * kB64 * kLd64 * 8;
-constexpr int kSiGemmSmem = 3 * 64 * (kB64 + 1) * 8;
+constexpr int kSiGemmSmem = 3 * 64 * (kB64 + 1) * 8;  // three stage buffers
 constexpr int kSiDiagSmem = 3 * kB64 * (kB64 + 1) * 8;
 
 __device__ __forceinline__ int lg_k(const DevSym& S, int s) { return S.first[s + 1] - S.first[s]; }
@@ -44,28 +44,31 @@ __device__ __forceinline__ const double* linv_block(const DevSym& S, const doubl
   return linv + (int64_t)b * S.lstride + ((int64_t)S.lbo[s] + blk) * (kB64 * kB64);
 }
 
-// Extend-add of the children's updates into parent columns [c0, c1) (the
-// update part of those columns is zeroed first). Work is flattened over
-// (source column, row) pairs so each thread keeps several loads in flight;
-// targets are distinct within one child, children are added in fixed order.
+// Extend-add of the children's updates into parent columns [c0, c1) (gcols
+// columns per CTA, at most kGatherCols, fewer when the slice would not fit): the
+// column slice is assembled in shared memory (panel columns start from the
+// filled values, update columns from zero), every child adds its entries in
+// fixed order (targets are distinct within one child), and the slice's lower
+// part is written back once. Work per child is flattened over (source column,
+// row) pairs with eight independent loads in flight per thread.
 constexpr int kGatherCols = 8;
 __global__ void __launch_bounds__(256) k_gather8(DevSym S, const int* __restrict__ list, double* __restrict__ F,
-                                                 int64_t fstride) {
+                                                 int64_t fstride, int gcols) {
+  extern __shared__ double gsl[];  // [gcols][m] column slice
   const int s = list[blockIdx.x], b = blockIdx.y;
   const int k = lg_k(S, s), m = lg_m(S, s);
-  const int c0 = blockIdx.z * kGatherCols;
+  const int c0 = blockIdx.z * gcols;
   if (c0 >= m) return;
-  const int c1 = min(c0 + kGatherCols, m);
+  const int c1 = min(c0 + gcols, m), nc = c1 - c0;
   double* Fb = F + (int64_t)b * fstride;
   double* Fs = Fb + S.fptr[s];
-  {
-    const int z0 = max(c0, k);
-    const int nz = (c1 > z0) ? (c1 - z0) : 0;
-    for (int e = threadIdx.x; e < nz * m; e += blockDim.x) {
-      const int cc = z0 + e / m, row = e - (e / m) * m;
-      if (row >= cc) Fs[row + (int64_t)cc * m] = 0.0;
-    }
+  for (int e = threadIdx.x; e < nc * m; e += blockDim.x) {
+    const int cc = e / m, row = e - cc * m, col = c0 + cc;
+    if (col < k && row >= col) cp_async8(&gsl[e], Fs + row + (int64_t)col * m);
+    else gsl[e] = 0.0;
   }
+  cp_async_commit();
+  cp_async_wait<0>();
   __syncthreads();
   for (int q = S.child_ptr[s]; q < S.child_ptr[s + 1]; ++q) {
     const int c = S.child_list[q];
@@ -90,28 +93,31 @@ __global__ void __launch_bounds__(256) k_gather8(DevSym S, const int* __restrict
       hi = a;
     }
     const int total = (hi - lo) * rc;
-    int e = threadIdx.x;
-    for (; e + 3 * (int)blockDim.x < total; e += 4 * blockDim.x) {
-      double v[4];
-      int64_t dst[4];
-      bool ok[4];
+    for (int e0 = 0; e0 < total; e0 += 8 * (int)blockDim.x) {
+      double v[8];
+      int dst[8];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int ee = e + u * blockDim.x;
-        const int jj = lo + ee / rc, ii = ee - (ee / rc) * rc;
-        ok[u] = ii >= jj;
-        v[u] = ok[u] ? Uc[ii + (int64_t)jj * mc] : 0.0;
-        dst[u] = relc[ii] + (int64_t)relc[jj] * m;
+      for (int u = 0; u < 8; ++u) {
+        const int e = e0 + threadIdx.x + u * blockDim.x;
+        dst[u] = -1;
+        v[u] = 0.0;
+        if (e < total) {
+          const int jj = lo + e / rc, ii = e - (e / rc) * rc;
+          if (ii >= jj) {
+            v[u] = Uc[ii + (int64_t)jj * mc];
+            dst[u] = (relc[jj] - c0) * m + relc[ii];
+          }
+        }
       }
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
-        if (ok[u]) Fs[dst[u]] += v[u];
-    }
-    for (; e < total; e += blockDim.x) {
-      const int jj = lo + e / rc, ii = e - (e / rc) * rc;
-      if (ii >= jj) Fs[relc[ii] + (int64_t)relc[jj] * m] += Uc[ii + (int64_t)jj * mc];
+      for (int u = 0; u < 8; ++u)
+        if (dst[u] >= 0) gsl[dst[u]] += v[u];
     }
     __syncthreads();
+  }
+  for (int e = threadIdx.x; e < nc * m; e += blockDim.x) {
+    const int cc = e / m, row = e - cc * m, col = c0 + cc;
+    if (row >= col) Fs[row + (int64_t)col * m] = gsl[e];
   }
 }
 
@@ -334,16 +340,31 @@ __global__ void __launch_bounds__(128) k_update64(DevSym S, const int* __restric
 #pragma unroll
       for (int q = 0; q < 4; ++q) mma884(acc[a][q][0], acc[a][q][1], af[a], bf[q]);
   }
+  // read 16 target entries before writing any (the loads stay in flight together), twice
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int a0 = 0; a0 < 4; a0 += 2) {
+    double cv[2][4][2];
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
+    for (int a = 0; a < 2; ++a)
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int i = I0 + wi + a * 8 + g;
-        const int j = J0 + wj + q * 8 + tg * 2 + h;
-        if (i < m && j < m && i >= j) Fs[i + (int64_t)j * m] -= acc[a][q][h];
-      }
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int i = I0 + wi + (a0 + a) * 8 + g;
+          const int j = J0 + wj + q * 8 + tg * 2 + h;
+          cv[a][q][h] = (i < m && j < m && i >= j) ? Fs[i + (int64_t)j * m] : 0.0;
+        }
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int i = I0 + wi + (a0 + a) * 8 + g;
+          const int j = J0 + wj + q * 8 + tg * 2 + h;
+          if (i < m && j < m && i >= j) Fs[i + (int64_t)j * m] = cv[a][q][h] - acc[a0 + a][q][h];
+        }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -390,15 +411,13 @@ __global__ void __launch_bounds__(NT) k_fwd32(DevSym S, const int* __restrict__ 
     }
     __syncthreads();
     for (int r = jb + wb + threadIdx.x; r < m; r += NT) {
-      double a0 = 0.0, a1 = 0.0;
+      // all (up to 32) loads of the row issued together, four partial sums
+      double a[4] = {0.0, 0.0, 0.0, 0.0};
       const double* Lr = Fs + r + (int64_t)jb * m;
-      int j = 0;
-      for (; j + 1 < wb; j += 2) {
-        a0 += Lr[(int64_t)j * m] * y[jb + j];
-        a1 += Lr[(int64_t)(j + 1) * m] * y[jb + j + 1];
-      }
-      if (j < wb) a0 += Lr[(int64_t)j * m] * y[jb + j];
-      y[r] -= a0 + a1;
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if (j < wb) a[j & 3] += Lr[(int64_t)j * m] * y[jb + j];
+      y[r] -= (a[0] + a[1]) + (a[2] + a[3]);
     }
     __syncthreads();
   }
@@ -426,8 +445,16 @@ __global__ void __launch_bounds__(NT) k_bwd32(DevSym S, const int* __restrict__ 
     // x_j -= sum_{i >= i0} L_ij x_i for the block's columns (warp per column)
     for (int j = jb + warp; j < jb + wb; j += NT / 32) {
       const double* Lj = Fs + (int64_t)j * m;
-      double acc = 0.0;
-      for (int i = i0 + lane; i < m; i += 32) acc += Lj[i] * x[i];
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+      int i = i0 + lane;
+      for (; i + 96 < m; i += 128) {
+        a0 += Lj[i] * x[i];
+        a1 += Lj[i + 32] * x[i + 32];
+        a2 += Lj[i + 64] * x[i + 64];
+        a3 += Lj[i + 96] * x[i + 96];
+      }
+      for (; i < m; i += 32) a0 += Lj[i] * x[i];
+      double acc = (a0 + a1) + (a2 + a3);
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
       if (lane == 0) x[j] -= acc;
@@ -467,15 +494,17 @@ constexpr int kSiT = 64;  // rows of A per CTA
 // Shared memory: two chunk buffers (Sa + Lb each, double-buffered with
 // cp.async) and G; L_JJ^-1 (from the inverse-block cache) and L[I,J] reuse the
 // chunk buffers after the GEMM.
-__global__ void __launch_bounds__(128) k_si_gemm64(DevSym S, const int* __restrict__ list, int jb,
+__global__ void __launch_bounds__(256) k_si_gemm64(DevSym S, const int* __restrict__ list, int jb,
                                                   const double* __restrict__ F, double* __restrict__ Sg,
                                                   int64_t fstride, double* __restrict__ ppart, int ptiles,
                                                   const double* __restrict__ linv) {
   extern __shared__ double smem64[];
   constexpr int kBuf = 64 * (kB64 + 1);  // doubles per chunk buffer (Sa[32][65] + Lb[32][65])
   typedef double Row65[kB64 + 1];
-  Row65* Gs = reinterpret_cast<Row65*>(smem64 + 2 * kBuf);  // [64][65]: G, then X
-  Row65* Lt = reinterpret_cast<Row65*>(smem64);             // [64][65]: L[j0+u, j0+t]  (after the GEMM)
+  // three stage buffers (Sa[32][65] + Lb[32][65] each) for the G loop; afterwards
+  // buffer 0 holds G (then X), buffer 1 L_JJ^-1 and buffer 2 L[I,J]
+  Row65* Gs = reinterpret_cast<Row65*>(smem64);             // [64][65]: G, then X
+  Row65* Lt = reinterpret_cast<Row65*>(smem64 + 2 * kBuf);  // [64][65]: L[I0+l, j0+j]
   const int s = list[blockIdx.x], b = blockIdx.y;
   const int k = lg_k(S, s), m = lg_m(S, s);
   const int nblk = (k + kB64 - 1) / kB64;
@@ -487,8 +516,10 @@ __global__ void __launch_bounds__(128) k_si_gemm64(DevSym S, const int* __restri
   const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
   double* Ss = Sg + (int64_t)b * fstride + S.fptr[s];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wi = (warp & 1) * 32, wj = (warp >> 1) * 32;
+  // 8 warps, warp tile 32 x 16; warps whose columns lie beyond the block's w skip the products
+  const int wi = (warp & 1) * 32, wj = (warp >> 1) * 16;
   const int g = lane >> 2, tg = lane & 3;
+  const bool wact = wj < w;
 
   // chunk loader: Sigma[I0.., l0..l0+32) (lower-triangle storage) and L[l0.., j0..j0+w)
   auto load_chunk = [&](int l0, int buf) {
@@ -522,76 +553,92 @@ __global__ void __launch_bounds__(128) k_si_gemm64(DevSym S, const int* __restri
     cp_async_commit();
   };
 
-  double acc[4][4][2];
+  double acc[4][2][2];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int q = 0; q < 4; ++q) acc[a][q][0] = acc[a][q][1] = 0.0;
+    for (int q = 0; q < 2; ++q) acc[a][q][0] = acc[a][q][1] = 0.0;
   const int nch = (m - j1 + 31) / 32;
   load_chunk(j1, 0);
+  if (nch > 1) load_chunk(j1 + 32, 1);
   for (int c = 0; c < nch; ++c) {
-    if (c + 1 < nch) {
-      load_chunk(j1 + 32 * (c + 1), (c + 1) & 1);
+    if (c + 2 < nch) {
+      load_chunk(j1 + 32 * (c + 2), (c + 2) % 3);
+      cp_async_wait<2>();
+    } else if (c + 1 < nch) {
       cp_async_wait<1>();
     } else {
       cp_async_wait<0>();
     }
     __syncthreads();
-    const Row65* Sa = reinterpret_cast<const Row65*>(smem64 + (c & 1) * kBuf);
-    const Row65* Lb = reinterpret_cast<const Row65*>(smem64 + (c & 1) * kBuf + 32 * (kB64 + 1));
+    const Row65* Sa = reinterpret_cast<const Row65*>(smem64 + (c % 3) * kBuf);
+    const Row65* Lb = reinterpret_cast<const Row65*>(smem64 + (c % 3) * kBuf + 32 * (kB64 + 1));
+    if (wact) {
 #pragma unroll
-    for (int kk = 0; kk < 32; kk += 4) {
-      double af[4], bf[4];
+      for (int kk = 0; kk < 32; kk += 4) {
+        double af[4], bf[2];
 #pragma unroll
-      for (int a = 0; a < 4; ++a) af[a] = Sa[kk + tg][wi + a * 8 + g];
+        for (int a = 0; a < 4; ++a) af[a] = Sa[kk + tg][wi + a * 8 + g];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) bf[q] = Lb[kk + tg][wj + q * 8 + g];
+        for (int q = 0; q < 2; ++q) bf[q] = Lb[kk + tg][wj + q * 8 + g];
 #pragma unroll
-      for (int a = 0; a < 4; ++a)
+        for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) mma884(acc[a][q][0], acc[a][q][1], af[a], bf[q]);
+          for (int q = 0; q < 2; ++q) mma884(acc[a][q][0], acc[a][q][1], af[a], bf[q]);
+      }
     }
     __syncthreads();
+  }
+  // L_JJ^-1 (cached) and L[I,J] are fetched together, G goes to buffer 0
+  double* Li = smem64 + kBuf;
+  const int rows = min(kSiT, m - I0);
+  Row65* Lij = Lt;  // Lij[l][j] = L[I0+l, j0+j]
+  {
+    const double* lc = linv_block(S, linv, b, s, bi);
+    for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) cp_async8(&Li[(e & 63) + (e >> 6) * (kB64 + 1)], lc + e);
+    for (int e = threadIdx.x; e < kSiT * kB64; e += blockDim.x) {
+      const int j = e / kSiT, l = e - j * kSiT;
+      if (l < rows && j < w) cp_async8(&Lij[l][j], Fs + (I0 + l) + (int64_t)(j0 + j) * m);
+      else Lij[l][j] = 0.0;
+    }
+    cp_async_commit();
   }
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
+    for (int q = 0; q < 2; ++q)
 #pragma unroll
       for (int h = 0; h < 2; ++h) Gs[wi + a * 8 + g][wj + q * 8 + tg * 2 + h] = acc[a][q][h];
   // X = -G L_JJ^-1 as a tensor-core GEMM with the cached inverse of the unit
-  // lower diagonal block (column-major, ld 65 in chunk buffer 1)
-  double* Li = smem64 + kBuf;
-  {
-    const double* lc = linv_block(S, linv, b, s, bi);
-    for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) cp_async8(&Li[(e & 63) + (e >> 6) * (kB64 + 1)], lc + e);
-    cp_async_commit();
-    cp_async_wait<0>();
-  }
+  // lower diagonal block
+  cp_async_wait<0>();
   __syncthreads();
   {
-    double xa[4][4][2];
+    double xa[4][2][2];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
-      for (int q = 0; q < 4; ++q) xa[a][q][0] = xa[a][q][1] = 0.0;
+      for (int q = 0; q < 2; ++q) xa[a][q][0] = xa[a][q][1] = 0.0;
+    const int wk = (w + 3) & ~3;
+    if (wact) {
 #pragma unroll 4
-    for (int kk = 0; kk < kB64; kk += 4) {
-      double af[4], bf[4];
+      for (int kk = 0; kk < wk; kk += 4) {
+        double af[4], bf[2];
 #pragma unroll
-      for (int a = 0; a < 4; ++a) af[a] = Gs[wi + a * 8 + g][kk + tg];
+        for (int a = 0; a < 4; ++a) af[a] = Gs[wi + a * 8 + g][kk + tg];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) bf[q] = Li[(kk + tg) + (wj + q * 8 + g) * (kB64 + 1)];
+        for (int q = 0; q < 2; ++q) bf[q] = Li[(kk + tg) + (wj + q * 8 + g) * (kB64 + 1)];
 #pragma unroll
-      for (int a = 0; a < 4; ++a)
+        for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) mma884(xa[a][q][0], xa[a][q][1], af[a], bf[q]);
+          for (int q = 0; q < 2; ++q) mma884(xa[a][q][0], xa[a][q][1], af[a], bf[q]);
+      }
     }
     __syncthreads();  // all reads of G done before X overwrites it
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
-      for (int q = 0; q < 4; ++q)
+      for (int q = 0; q < 2; ++q)
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const int ii = wi + a * 8 + g, t = wj + q * 8 + tg * 2 + h;
@@ -602,39 +649,32 @@ __global__ void __launch_bounds__(128) k_si_gemm64(DevSym S, const int* __restri
   }
   __syncthreads();
   // partial P[j][i] = sum_{rows l of this tile} L[I0+l, j0+j] X[l, i]  (tensor-core tiles)
-  const int rows = min(kSiT, m - I0);
-  Row65* Lij = Lt;  // Lij[l][j] = L[I0+l, j0+j]
-  for (int e = threadIdx.x; e < kSiT * kB64; e += blockDim.x) {
-    const int j = e / kSiT, l = e - j * kSiT;
-    if (l < rows && j < w) cp_async8(&Lij[l][j], Fs + (I0 + l) + (int64_t)(j0 + j) * m);
-    else Lij[l][j] = 0.0;
-  }
-  cp_async_commit();
-  cp_async_wait<0>();
-  __syncthreads();
-  double pa[4][4][2];
+  double pa[4][2][2];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int q = 0; q < 4; ++q) pa[a][q][0] = pa[a][q][1] = 0.0;
-  const int wr = (warp & 1) * 32, wc = (warp >> 1) * 32;  // output rows j, cols i
+    for (int q = 0; q < 2; ++q) pa[a][q][0] = pa[a][q][1] = 0.0;
+  const int wr = (warp & 1) * 32, wc = (warp >> 1) * 16;  // output rows j, cols i
+  if (wr < w && wc < w) {
+    const int kr = (rows + 3) & ~3;
 #pragma unroll 4
-  for (int kk = 0; kk < kSiT; kk += 4) {
-    double af[4], bf[4];
+    for (int kk = 0; kk < kr; kk += 4) {
+      double af[4], bf[2];
 #pragma unroll
-    for (int a = 0; a < 4; ++a) af[a] = Lij[kk + tg][wr + a * 8 + g];
+      for (int a = 0; a < 4; ++a) af[a] = Lij[kk + tg][wr + a * 8 + g];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) bf[q] = Gs[kk + tg][wc + q * 8 + g];
+      for (int q = 0; q < 2; ++q) bf[q] = Gs[kk + tg][wc + q * 8 + g];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+      for (int a = 0; a < 4; ++a)
 #pragma unroll
-      for (int q = 0; q < 4; ++q) mma884(pa[a][q][0], pa[a][q][1], af[a], bf[q]);
+        for (int q = 0; q < 2; ++q) mma884(pa[a][q][0], pa[a][q][1], af[a], bf[q]);
+    }
   }
   double* pp = ppart + (((int64_t)blockIdx.x * gridDim.y + b) * ptiles + blockIdx.z) * (kB64 * kB64);
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
+    for (int q = 0; q < 2; ++q)
 #pragma unroll
       for (int h = 0; h < 2; ++h) pp[(wr + a * 8 + g) * kB64 + wc + q * 8 + tg * 2 + h] = pa[a][q][h];
 }

@@ -258,6 +258,8 @@ void analyze(int64_t n, const int64_t* colptr, const int64_t* rowidx, const Symb
   S.order_used = kind;
   if (kind == ORDER_AMD) {
     amd_order(n, colptr, rowidx, perm0);
+  } else if (kind == ORDER_ND) {
+    nd_order(n, colptr, rowidx, perm0);
   } else if (kind == ORDER_NATURAL) {
     std::iota(perm0.begin(), perm0.end(), 0);
   } else if (kind == ORDER_CUSTOM) {

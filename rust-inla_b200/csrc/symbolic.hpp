@@ -27,6 +27,7 @@ enum OrderKind : int {
   ORDER_NATURAL = 3,
   ORDER_CUSTOM = 4,      // caller-provided permutation
   ORDER_TIME_MAJOR = 5,
+  ORDER_ND = 6,          // nested dissection (nd.cpp)
 };
 
 struct SymbolicOptions {
@@ -88,6 +89,7 @@ int choose_symmetric_order(int64_t n, const int64_t* colptr, const int64_t* rowi
                            std::vector<int64_t>& fwd);
 
 // Approximate minimum degree on the symmetric pattern; returns perm[new] = old.
+void nd_order(int64_t n, const int64_t* colptr, const int64_t* rowidx, std::vector<int64_t>& perm);
 void amd_order(int64_t n, const int64_t* colptr, const int64_t* rowidx,
                std::vector<int64_t>& perm);
 

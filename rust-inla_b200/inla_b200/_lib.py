@@ -30,6 +30,7 @@ ORDER_RCM = 2
 ORDER_NATURAL = 3
 ORDER_CUSTOM = 4
 ORDER_TIME_MAJOR = 5
+ORDER_ND = 6
 
 _ERROR_NAMES = {
     INLA_ERR_SINGULAR: "Singular",

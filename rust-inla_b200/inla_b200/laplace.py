@@ -74,7 +74,7 @@ class LaplaceModel:
     """Latent Gaussian model ``Q(theta) = sum_t coef_t M_t``, projector ``A``, one family."""
 
     def __init__(self, model, a=None, family="gaussian", y=None, p1=None, p2=None, max_batch=16,
-                 ordering=_lib.ORDER_AMD):
+                 ordering=_lib.ORDER_ND):
         pat = sp.csc_matrix(model.pattern)
         pat.sort_indices()
         self.n = pat.shape[0]

@@ -1,7 +1,7 @@
 """Workload driver for profiling the hot-path kernels (run under ncu).
 
     python -m inla_b200.profile_ops --nx 200 --batch 15 --op factor|solve|selinv|all [--reps R]
-    python -m inla_b200.profile_ops --nx 200 --batch 21 --op laplace-grad
+    python -m inla_b200.profile_ops --nx 200 --batch 21 --op laplace-grad [--ordering amd|nd]
 
 ``factor``/``solve``/``selinv`` run the batched supernodal kernels on the SPDE
 posterior precision ``Q(theta) + 100 A^T A`` (theta at the generating values);
@@ -36,7 +36,10 @@ def main():
     ap.add_argument("--op", default="all")
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--warmup", type=int, default=1)
+    ap.add_argument("--ordering", default="amd", choices=["amd", "nd"])
     a = ap.parse_args()
+    from inla_b200 import _lib
+    order = {"amd": _lib.ORDER_AMD, "nd": _lib.ORDER_ND}[a.ordering]
     p = models.make_spde_problem(nx=a.nx, n_obs=a.nx * a.nx // 2)
     B = a.batch
     stream = torch.cuda.current_stream().cuda_stream
@@ -53,12 +56,12 @@ def main():
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / a.reps
 
-    out = {"nx": a.nx, "B": B}
+    out = {"nx": a.nx, "B": B, "ordering": a.ordering}
     if a.op in ("factor", "solve", "selinv", "all"):
         c, _ = models.spde_coefs(math.log(0.02), math.log(14.14))
         q = (p.model.matrix(c) + 100.0 * (p.a.T @ p.a)).tocsc()
         q.sort_indices()
-        bs = BatchSolver(q, max_batch=B)
+        bs = BatchSolver(q, max_batch=B, ordering=order)
         vals = torch.tensor(np.tile(q.data, (B, 1)), device="cuda")
         ld = torch.zeros(B, dtype=torch.float64, device="cuda")
         st = torch.zeros(B, dtype=torch.int32, device="cuda")
@@ -81,7 +84,7 @@ def main():
                 out[name + "_ms"] = timed(fn)
         del bs
     if a.op == "laplace-grad":
-        lm = LaplaceModel(p.model, a=p.a, family="gaussian", y=p.y, max_batch=B)
+        lm = LaplaceModel(p.model, a=p.a, family="gaussian", y=p.y, max_batch=B, ordering=order)
         th = np.array([4.6, -3.9, 2.6]) + 0.01 * np.random.default_rng(0).standard_normal((B, 3))
         coefs = np.stack([models.spde_coefs(t[1], t[2])[0] for t in th])
         scale = np.exp(th[:, 0])

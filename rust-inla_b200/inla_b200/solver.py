@@ -132,7 +132,7 @@ class GpuSolver:
 class BatchSolver:
     """B problems that share one sparsity pattern (one symbolic analysis)."""
 
-    def __init__(self, pattern, max_batch: int, ordering: int = _lib.ORDER_AMD):
+    def __init__(self, pattern, max_batch: int, ordering: int = _lib.ORDER_ND):
         n, cp, ri, _ = _csc_arrays(pattern)
         h = C.c_void_p()
         check(lib().inla_batch_create(n, lptr(cp), lptr(ri), int(ordering), int(max_batch), C.byref(h)))

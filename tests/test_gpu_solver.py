@@ -39,7 +39,7 @@ def backward_error(q, x, b):
 
 
 @pytest.mark.parametrize("name", sorted({k.split("/")[0] for k in GOLDEN.files}))
-@pytest.mark.parametrize("ordering", [_lib.ORDER_AMD, _lib.ORDER_REFERENCE, _lib.ORDER_NATURAL])
+@pytest.mark.parametrize("ordering", [_lib.ORDER_AMD, _lib.ORDER_REFERENCE, _lib.ORDER_NATURAL, _lib.ORDER_ND])
 def test_golden_known_answers(name, ordering):
     q = golden_matrix(name)
     s = GpuSolver(ordering)
@@ -79,7 +79,7 @@ def _spde_post(nx):
 
 
 @pytest.mark.parametrize("name", list(CASES))
-@pytest.mark.parametrize("ordering", [_lib.ORDER_AMD, _lib.ORDER_REFERENCE])
+@pytest.mark.parametrize("ordering", [_lib.ORDER_AMD, _lib.ORDER_REFERENCE, _lib.ORDER_ND])
 def test_factor_solve_selinv_vs_oracle(name, ordering):
     q = sp.csc_matrix(CASES[name]())
     q.sort_indices()

@@ -72,7 +72,7 @@ def test_choose_symmetric_order_bit_exact(name):
 
 
 @pytest.mark.parametrize("name", list(MATRICES))
-@pytest.mark.parametrize("ordering", [_lib.ORDER_AMD, _lib.ORDER_REFERENCE, _lib.ORDER_NATURAL])
+@pytest.mark.parametrize("ordering", [_lib.ORDER_AMD, _lib.ORDER_REFERENCE, _lib.ORDER_NATURAL, _lib.ORDER_ND])
 def test_symbolic_structure(name, ordering):
     q = MATRICES[name]()
     n = q.shape[0]
@@ -104,6 +104,36 @@ def test_amd_reduces_fill_on_meshes():
     assert a.info()["nnz_l"] <= 1.2 * r.info()["nnz_l"]
     # AMD gives a shallow tree (level parallelism) where RCM gives a chain
     assert a.info()["nlevels"] * 3 < r.info()["nlevels"]
+
+
+def _longest_pivot_path(s):
+    """Pivot columns on the longest root-to-leaf path of the supernodal tree."""
+    first, et = s.supernodes(), s.etree()
+    ns = len(first) - 1
+    col2sn = np.repeat(np.arange(ns), np.diff(first))
+    k = np.diff(first)
+    path = k.astype(np.int64).copy()
+    for t in range(ns):  # postordered: children before parents
+        pc = et[first[t + 1] - 1]
+        if pc >= 0:
+            p = col2sn[pc]
+            path[p] = max(path[p], path[t] + k[p])
+    return int(path.max())
+
+
+def test_nested_dissection_shortens_the_elimination_tree():
+    """On a 2-D mesh, nested dissection gives fewer levels and a shorter pivot
+    chain than AMD at comparable fill (the GPU engine's default ordering)."""
+    p = models.make_spde_problem(nx=60, n_obs=1800)
+    q = (p.model.pattern + p.a.T @ p.a).tocsc()
+    a = GpuSolver(_lib.ORDER_AMD)
+    a.analyze(q)
+    d = GpuSolver(_lib.ORDER_ND)
+    d.analyze(q)
+    assert sorted(d.perm().tolist()) == list(range(q.shape[0]))
+    assert d.info()["nlevels"] < a.info()["nlevels"]
+    assert _longest_pivot_path(d) < _longest_pivot_path(a)
+    assert d.info()["nnz_l"] <= 1.25 * a.info()["nnz_l"]
 
 
 def test_custom_permutation_is_used():
