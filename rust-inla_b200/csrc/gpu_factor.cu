@@ -143,6 +143,35 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
   INLA_CUDA(cudaMemsetAsync(ldticket_.p, 0, sizeof(unsigned) * max_batch_, stream_));
 
   plan_levels();
+  // extend-add range table: for every large front, column chunk z (of the
+  // level's gcols columns) and child, the child's source columns whose parent
+  // column lies in the chunk
+  {
+    std::vector<int64_t> gptr(ns, 0);
+    std::vector<int2> grng;
+    for (const LevelPlan& P : levels_) {
+      if (P.large.empty()) continue;
+      const int gcols = gather_cols(P.mmax_large);
+      for (int s : P.large) {
+        const int m = rowptr[s + 1] - rowptr[s];
+        gptr[s] = (int64_t)grng.size();
+        for (int z = 0; z < cdiv(m, gcols); ++z) {
+          const int c0 = z * gcols, c1 = std::min(c0 + gcols, m);
+          for (int64_t q = S.child_ptr[s]; q < S.child_ptr[s + 1]; ++q) {
+            const int c = (int)S.child_list[q];
+            const int kc = first[c + 1] - first[c], rc = (rowptr[c + 1] - rowptr[c]) - kc;
+            const int* rel = relx.data() + rowptr[c] + kc;
+            const int lo = (int)(std::lower_bound(rel, rel + rc, c0) - rel);
+            const int hi = (int)(std::lower_bound(rel, rel + rc, c1) - rel);
+            grng.push_back(make_int2(lo, hi));
+          }
+        }
+      }
+    }
+    if (grng.empty()) grng.push_back(make_int2(0, 0));
+    d_gptr_.upload(gptr, stream_);
+    d_grng_.upload(grng, stream_);
+  }
 
   F_.alloc((size_t)max_batch_ * ftotal_);
   xp_.alloc((size_t)max_batch_ * n);
@@ -246,8 +275,8 @@ void GpuFactor::run_factor_levels(int B) {
       const int nl = (int)P.large.size();
       const int* lst = d_lists_.p + P.off_large;
       const int gcols = gather_cols(P.mmax_large);
-      k_gather8<<<dim3(nl, B, cdiv(P.mmax_large, gcols)), 256, gcols * P.mmax_large * 8, stream_>>>(ds_, lst, F_.p,
-                                                                                             fs, gcols);
+      k_gather8<<<dim3(nl, B, cdiv(P.mmax_large, gcols)), 256, gcols * P.mmax_large * 8, stream_>>>(
+          ds_, lst, F_.p, fs, gcols, d_gptr_.p, d_grng_.p);
       ++launches_;
       for (int j0 = 0; j0 < P.kmax_large; j0 += kB64) {
         int rows = P.mmax_large - j0;

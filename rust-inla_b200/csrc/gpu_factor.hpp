@@ -133,7 +133,8 @@ class GpuFactor {
   DevSym ds_;
   std::vector<LevelPlan> levels_;
   DBuf<int> d_first_, d_rowptr_, d_rows_, d_relx_, d_child_ptr_, d_child_list_, d_parent_, d_uoff_, d_perm_;
-  DBuf<int64_t> d_fptr_, d_lptr_, d_dpos_, spos_, spos_full_;
+  DBuf<int64_t> d_fptr_, d_lptr_, d_dpos_, spos_, spos_full_, d_gptr_;
+  DBuf<int2> d_grng_;  // extend-add source-column ranges per (front, chunk, child)
   DBuf<int> d_pmap_, d_lists_, d_csn_, d_lbo_;
   DBuf<double> F_, Sg_, xp_, ub_, logdet_, dcache_, ppart_, linv_, ldpart_;
   DBuf<int> status_, ldflag_;

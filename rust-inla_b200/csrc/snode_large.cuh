@@ -32,7 +32,7 @@ constexpr int kLd64 = dense_ld(kB64);
 constexpr int kULd64 = dense_uld(kB64);
 constexpr int kPanelSmem = (2 * kB64 * kLd64 + 16 * kULd64 + kDenseScratch) * 8;
 constexpr int kUpdSmem = 2 * kB64 * kLd64 * 8;
-constexpr int kSiGemmSmem = 3 * 64 * (kB64 + 1) * 8;  // three stage buffers
+constexpr int kSiGemmSmem = 3 * 64 * kLd64 * 8;  // three stage buffers
 constexpr int kSiDiagSmem = 3 * kB64 * (kB64 + 1) * 8;
 
 __device__ __forceinline__ int lg_k(const DevSym& S, int s) { return S.first[s + 1] - S.first[s]; }
@@ -45,7 +45,9 @@ __device__ __forceinline__ const double* linv_block(const DevSym& S, const doubl
 }
 
 // Extend-add of the children's updates into parent columns [c0, c1) (gcols
-// columns per CTA, at most kGatherCols, fewer when the slice would not fit): the
+// columns per CTA, at most kGatherCols, fewer when the slice would not fit;
+// grng[gptr[s] + z * nchildren + q] = the child's source columns whose parent
+// column falls in chunk z, from a host table): the
 // column slice is assembled in shared memory (panel columns start from the
 // filled values, update columns from zero), every child adds its entries in
 // fixed order (targets are distinct within one child), and the slice's lower
@@ -53,7 +55,8 @@ __device__ __forceinline__ const double* linv_block(const DevSym& S, const doubl
 // row) pairs with eight independent loads in flight per thread.
 constexpr int kGatherCols = 8;
 __global__ void __launch_bounds__(256) k_gather8(DevSym S, const int* __restrict__ list, double* __restrict__ F,
-                                                 int64_t fstride, int gcols) {
+                                                 int64_t fstride, int gcols, const int64_t* __restrict__ gptr,
+                                                 const int2* __restrict__ grng) {
   extern __shared__ double gsl[];  // [gcols][m] column slice
   const int s = list[blockIdx.x], b = blockIdx.y;
   const int k = lg_k(S, s), m = lg_m(S, s);
@@ -70,28 +73,16 @@ __global__ void __launch_bounds__(256) k_gather8(DevSym S, const int* __restrict
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
-  for (int q = S.child_ptr[s]; q < S.child_ptr[s + 1]; ++q) {
-    const int c = S.child_list[q];
+  const int q0 = S.child_ptr[s], nch = S.child_ptr[s + 1] - q0;
+  // source-column range of every child for this chunk (host table, no search)
+  const int2* rng = grng + gptr[s] + (int64_t)blockIdx.z * nch;
+  for (int qi = 0; qi < nch; ++qi) {
+    const int c = S.child_list[q0 + qi];
     const int kc = lg_k(S, c), mc = lg_m(S, c), rc = mc - kc;
     const double* __restrict__ Uc = Fb + S.fptr[c] + (int64_t)kc * mc + kc;
     const int* __restrict__ relc = S.relx + S.rowptr[c] + kc;
-    int lo, hi;
-    {
-      int a = 0, z = rc;
-      while (a < z) {
-        const int mid = (a + z) >> 1;
-        if (relc[mid] < c0) a = mid + 1;
-        else z = mid;
-      }
-      lo = a;
-      z = rc;
-      while (a < z) {
-        const int mid = (a + z) >> 1;
-        if (relc[mid] < c1) a = mid + 1;
-        else z = mid;
-      }
-      hi = a;
-    }
+    const int2 lh = rng[qi];
+    const int lo = lh.x, hi = lh.y;
     const int total = (hi - lo) * rc;
     for (int e0 = 0; e0 < total; e0 += 8 * (int)blockDim.x) {
       double v[8];
@@ -499,12 +490,12 @@ __global__ void __launch_bounds__(256) k_si_gemm64(DevSym S, const int* __restri
                                                   int64_t fstride, double* __restrict__ ppart, int ptiles,
                                                   const double* __restrict__ linv) {
   extern __shared__ double smem64[];
-  constexpr int kBuf = 64 * (kB64 + 1);  // doubles per chunk buffer (Sa[32][65] + Lb[32][65])
-  typedef double Row65[kB64 + 1];
-  // three stage buffers (Sa[32][65] + Lb[32][65] each) for the G loop; afterwards
+  constexpr int kBuf = 64 * kLd64;  // doubles per chunk buffer (Sa[32][68] + Lb[32][68])
+  typedef double Row68[kLd64];  // leading dimension 68 == 4 (mod 16): conflict-free fragments
+  // three stage buffers (Sa[32][68] + Lb[32][68] each) for the G loop; afterwards
   // buffer 0 holds G (then X), buffer 1 L_JJ^-1 and buffer 2 L[I,J]
-  Row65* Gs = reinterpret_cast<Row65*>(smem64);             // [64][65]: G, then X
-  Row65* Lt = reinterpret_cast<Row65*>(smem64 + 2 * kBuf);  // [64][65]: L[I0+l, j0+j]
+  Row68* Gs = reinterpret_cast<Row68*>(smem64);             // [64][68]: G, then X
+  Row68* Lt = reinterpret_cast<Row68*>(smem64 + 2 * kBuf);  // [64][68]: L[I0+l, j0+j]
   const int s = list[blockIdx.x], b = blockIdx.y;
   const int k = lg_k(S, s), m = lg_m(S, s);
   const int nblk = (k + kB64 - 1) / kB64;
@@ -523,8 +514,8 @@ __global__ void __launch_bounds__(256) k_si_gemm64(DevSym S, const int* __restri
 
   // chunk loader: Sigma[I0.., l0..l0+32) (lower-triangle storage) and L[l0.., j0..j0+w)
   auto load_chunk = [&](int l0, int buf) {
-    Row65* Sa = reinterpret_cast<Row65*>(smem64 + buf * kBuf);
-    Row65* Lb = reinterpret_cast<Row65*>(smem64 + buf * kBuf + 32 * (kB64 + 1));
+    Row68* Sa = reinterpret_cast<Row68*>(smem64 + buf * kBuf);
+    Row68* Lb = reinterpret_cast<Row68*>(smem64 + buf * kBuf + 32 * kLd64);
     if (I0 >= l0 + 31) {  // on/below the diagonal: stored at (i, l), coalesced over i
       for (int e = threadIdx.x; e < 32 * kSiT; e += blockDim.x) {
         const int l = e / kSiT, ii = e - l * kSiT, row = I0 + ii, col = l0 + l;
@@ -571,8 +562,8 @@ __global__ void __launch_bounds__(256) k_si_gemm64(DevSym S, const int* __restri
       cp_async_wait<0>();
     }
     __syncthreads();
-    const Row65* Sa = reinterpret_cast<const Row65*>(smem64 + (c % 3) * kBuf);
-    const Row65* Lb = reinterpret_cast<const Row65*>(smem64 + (c % 3) * kBuf + 32 * (kB64 + 1));
+    const Row68* Sa = reinterpret_cast<const Row68*>(smem64 + (c % 3) * kBuf);
+    const Row68* Lb = reinterpret_cast<const Row68*>(smem64 + (c % 3) * kBuf + 32 * kLd64);
     if (wact) {
 #pragma unroll
       for (int kk = 0; kk < 32; kk += 4) {
@@ -592,10 +583,10 @@ __global__ void __launch_bounds__(256) k_si_gemm64(DevSym S, const int* __restri
   // L_JJ^-1 (cached) and L[I,J] are fetched together, G goes to buffer 0
   double* Li = smem64 + kBuf;
   const int rows = min(kSiT, m - I0);
-  Row65* Lij = Lt;  // Lij[l][j] = L[I0+l, j0+j]
+  Row68* Lij = Lt;  // Lij[l][j] = L[I0+l, j0+j]
   {
     const double* lc = linv_block(S, linv, b, s, bi);
-    for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) cp_async8(&Li[(e & 63) + (e >> 6) * (kB64 + 1)], lc + e);
+    for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) cp_async8(&Li[(e & 63) + (e >> 6) * kLd64], lc + e);
     for (int e = threadIdx.x; e < kSiT * kB64; e += blockDim.x) {
       const int j = e / kSiT, l = e - j * kSiT;
       if (l < rows && j < w) cp_async8(&Lij[l][j], Fs + (I0 + l) + (int64_t)(j0 + j) * m);
@@ -627,7 +618,7 @@ __global__ void __launch_bounds__(256) k_si_gemm64(DevSym S, const int* __restri
 #pragma unroll
         for (int a = 0; a < 4; ++a) af[a] = Gs[wi + a * 8 + g][kk + tg];
 #pragma unroll
-        for (int q = 0; q < 2; ++q) bf[q] = Li[(kk + tg) + (wj + q * 8 + g) * (kB64 + 1)];
+        for (int q = 0; q < 2; ++q) bf[q] = Li[(kk + tg) + (wj + q * 8 + g) * kLd64];
 #pragma unroll
         for (int a = 0; a < 4; ++a)
 #pragma unroll
