@@ -190,7 +190,7 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
   }
   set_smem(k_factor_small<128>, small_factor_smem(kSmallA));
   set_smem(k_factor_small<256>, small_factor_smem(kSmallB));
-  set_smem(k_selinv_small<256>, small_selinv_smem(kSiSmall));
+  set_smem(k_selinv_small<256>, small_selinv_smem(kSiSmall, kSiSmall));
   set_smem(k_panel64, kPanelSmem);
   {
     int dev = 0;
@@ -234,6 +234,7 @@ void GpuFactor::plan_levels() {
       if (m <= kSiSmall) {
         P.si_small.push_back(s);
         P.mmax_si_small = std::max(P.mmax_si_small, m);
+        P.kmax_si_small = std::max(P.kmax_si_small, k);
       } else {
         P.si_large.push_back(s);
         P.kmax_si_large = std::max(P.kmax_si_large, k);
@@ -398,7 +399,8 @@ void GpuFactor::selinv_levels(int B) {
     const LevelPlan& P = levels_[l];
     if (!P.si_small.empty()) {
       int mm = P.mmax_si_small;
-      k_selinv_small<256><<<dim3((unsigned)P.si_small.size(), B), 256, small_selinv_smem(mm), stream_>>>(
+      k_selinv_small<256><<<dim3((unsigned)P.si_small.size(), B), 256, small_selinv_smem(mm, P.kmax_si_small),
+                            stream_>>>(
           ds_, d_lists_.p + P.off_si_small, F_.p, Sg_.p, fs);
       ++launches_;
     }

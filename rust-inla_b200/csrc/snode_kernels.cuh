@@ -587,9 +587,9 @@ __device__ __forceinline__ double parent_sigma(const double* Sp, int mp, int pi,
   return pi >= pj ? Sp[pi + (int64_t)pj * mp] : Sp[pj + (int64_t)pi * mp];
 }
 
-// Shared memory of k_selinv_small for fronts of up to m rows (bytes).
-__host__ __device__ constexpr int small_selinv_smem(int m) {
-  return (2 * m * dense_ld(m) + 16 * dense_uld(m) + 2 * 16 * kLamLd + 64 + 16) * 8;
+// Shared memory of k_selinv_small for fronts of up to m rows and k pivots (bytes).
+__host__ __device__ constexpr int small_selinv_smem(int m, int k) {
+  return ((m + k) * dense_ld(m) + 16 * dense_uld(m) + 2 * 16 * kLamLd + 64 + 16) * 8;
 }
 
 // Selected inverse of a small front, one CTA per (front, problem): Sigma is kept
@@ -611,7 +611,7 @@ __global__ void __launch_bounds__(NT) k_selinv_small(DevSym S, const int* __rest
   const int ld = dense_ld(m), uld = dense_uld(m);
   double* Sm = smem;               // Sigma, both triangles: Sm[i + j*ld]
   double* Lp = Sm + m * ld;        // L panel: Lp[i + c*ld], c < k
-  double* Xb = Lp + m * ld;        // [16][uld]: G rows of A
+  double* Xb = Lp + k * ld;        // [16][uld]: G rows of A
   double* lam = Xb + 16 * uld;     // L_JJ^-1 (ld kLamLd)
   double* Pm = lam + 16 * kLamLd;  // P, then M = D^-1 L^-1 - P
   double* xbuf = Pm + 16 * kLamLd; // warp scratch

@@ -317,7 +317,9 @@ __global__ void __launch_bounds__(128) k_update64(DevSym S, const int* __restric
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int q = 0; q < 4; ++q) acc[a][q][0] = acc[a][q][1] = 0.0;
-  const int wk = (w + 3) & ~3;  // only the block's w columns contribute
+  // only the block's w columns contribute; warps whose 32 x 32 sub-tile lies above
+  // the diagonal or past the last row have nothing to compute
+  const int wk = (I0 + wi >= m || J0 + wj >= m || (I == J && wj > wi)) ? 0 : (w + 3) & ~3;
 #pragma unroll 2
   for (int kk = 0; kk < wk; kk += 4) {
     double af[4], bf[4];
@@ -510,7 +512,7 @@ __global__ void __launch_bounds__(256) k_si_gemm64(DevSym S, const int* __restri
   // 8 warps, warp tile 32 x 16; warps whose columns lie beyond the block's w skip the products
   const int wi = (warp & 1) * 32, wj = (warp >> 1) * 16;
   const int g = lane >> 2, tg = lane & 3;
-  const bool wact = wj < w;
+  const bool wact = wj < w && I0 + wi < m;
 
   // chunk loader: Sigma[I0.., l0..l0+32) (lower-triangle storage) and L[l0.., j0..j0+w)
   auto load_chunk = [&](int l0, int buf) {
