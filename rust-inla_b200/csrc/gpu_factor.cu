@@ -122,19 +122,24 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
     ds_.lstride = nblk * kB64 * kB64;
     linv_.alloc((size_t)max_batch_ * std::max<int64_t>(ds_.lstride, 1));
   }
-  // value-fill chunks over the compact panel numbering
+  // value-fill chunks over the compact panel numbering (kFillChunk entries for
+  // the input-values fill, kFillModelChunk for the component-model fill)
   {
     ntot_ = S.sn_lptr[ns];
-    nfill_ = std::max(1, cdiv(ntot_, kFillChunk));
-    std::vector<int> csn(nfill_ + 1);
-    int64_t s = 0;
-    for (int c = 0; c < nfill_; ++c) {
-      const int64_t e = (int64_t)c * kFillChunk;
-      while (s + 1 < ns && S.sn_lptr[s + 1] <= e) ++s;
-      csn[c] = (int)s;
-    }
-    csn[nfill_] = (int)(ns - 1);
-    d_csn_.upload(csn, stream_);
+    auto chunk_table = [&](int chunk, int& count, DBuf<int>& dst) {
+      count = std::max(1, cdiv(ntot_, chunk));
+      std::vector<int> csn(count + 1);
+      int64_t s = 0;
+      for (int c = 0; c < count; ++c) {
+        const int64_t e = (int64_t)c * chunk;
+        while (s + 1 < ns && S.sn_lptr[s + 1] <= e) ++s;
+        csn[c] = (int)s;
+      }
+      csn[count] = (int)(ns - 1);
+      dst.upload(csn, stream_);
+    };
+    chunk_table(kFillChunk, nfill_, d_csn_);
+    chunk_table(kFillModelChunk, nfillm_, d_csnm_);
   }
   nldchunk_ = std::max(1, cdiv(n, kLogdetChunk));
   ldpart_.alloc((size_t)max_batch_ * nldchunk_);
@@ -198,6 +203,7 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
     INLA_CUDA(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev));
   }
   set_smem(k_update64, kUpdSmem);
+  set_smem(k_rows64, kRowsSmem);
   set_smem(k_gather8, 200 * 1024 + 8 * kGatherCols * 8);
   set_smem(k_si_gemm64, kSiGemmSmem);
   set_smem(k_si_diag64, kSiDiagSmem);
@@ -281,15 +287,21 @@ void GpuFactor::run_factor_levels(int B) {
       ++launches_;
       for (int j0 = 0; j0 < P.kmax_large; j0 += kB64) {
         int rows = P.mmax_large - j0;
-        // rows per CTA: 64 while the launch fits in about one wave (two CTAs per
-        // SM), more once many fronts x problems share it (fewer redundant
-        // diagonal-block factorizations)
+        // While every (front, problem, 64-row block) gets its own CTA within about
+        // one wave (two CTAs per SM), each row CTA factors the diagonal block
+        // itself (one launch). Beyond that, one CTA per (front, problem) factors
+        // it and k_rows64 forms the rows from the cached factor (no redundant
+        // factorizations).
         const int nrb = std::max(1, cdiv(rows, kPanelRows));
         const int per = std::max(1, (2 * num_sms_) / std::max(1, nl * B));
-        const int nz = std::min(nrb, per);
-        const int rpc = kPanelRows * cdiv(nrb, nz);
-        k_panel64<<<dim3(nl, B, std::max(1, cdiv(rows, rpc))), 256, kPanelSmem, stream_>>>(
-            ds_, lst, j0, rpc, F_.p, fs, dcache_.p, linv_.p);
+        if (per >= nrb) {
+          k_panel64<<<dim3(nl, B, nrb), 256, kPanelSmem, stream_>>>(ds_, lst, j0, kPanelRows, F_.p, fs, dcache_.p,
+                                                                     linv_.p);
+        } else {
+          k_panel64<<<dim3(nl, B, 1), 256, kPanelSmem, stream_>>>(ds_, lst, j0, 0, F_.p, fs, dcache_.p, linv_.p);
+          k_rows64<<<dim3(nl, B, nrb), 256, kRowsSmem, stream_>>>(ds_, lst, j0, F_.p, fs, dcache_.p, linv_.p);
+          ++launches_;
+        }
         int nt = cdiv(rows, kUT64);
         k_update64<<<dim3(nl, B, std::max(1, nt * (nt + 1) / 2)), 128, kUpdSmem, stream_>>>(ds_, lst, j0, F_.p, fs,
                                                                                           dcache_.p);
@@ -349,15 +361,16 @@ void GpuFactor::factor_model(int ncomp, const double* d_comp, const double* d_co
                              const unsigned char* d_pdiag, const int* d_cptr, const int* d_cobs,
                              const double* d_cprod, const double* d_w, int64_t wstride, int B) {
   if (B < 1 || B > max_batch_) throw std::runtime_error("batch size out of range");
+  if (ncomp < 1 || ncomp > 8) throw std::runtime_error("1..8 precision components supported");
   int64_t dbits;
   std::memcpy(&dbits, &diag_add, sizeof(dbits));
   launch_cached({2, B, ncomp, (int64_t)(uintptr_t)d_comp, (int64_t)(uintptr_t)d_coef, dbits,
                  (int64_t)(uintptr_t)d_pdiag, (int64_t)(uintptr_t)d_cptr, (int64_t)(uintptr_t)d_cobs,
                  (int64_t)(uintptr_t)d_cprod, (int64_t)(uintptr_t)d_w, wstride},
                 [&] {
-                  k_fill_panels_model<<<dim3(nfill_, B), 256, 0, stream_>>>(
-                      ds_, d_csn_.p, ntot_, d_pmap_.p, ncomp, d_comp, nnz_, d_coef, diag_add, d_pdiag, d_cptr, d_cobs,
-                      d_cprod, d_w, wstride, F_.p, ftotal_);
+                  k_fill_panels_model<<<dim3(nfillm_), 256, 0, stream_>>>(
+                      ds_, d_csnm_.p, ntot_, d_pmap_.p, ncomp, d_comp, nnz_, d_coef, diag_add, d_pdiag, d_cptr, d_cobs,
+                      d_cprod, d_w, wstride, B, F_.p, ftotal_);
                   ++launches_;
                   run_factor_levels(B);
                 });

@@ -135,11 +135,11 @@ class GpuFactor {
   DBuf<int> d_first_, d_rowptr_, d_rows_, d_relx_, d_child_ptr_, d_child_list_, d_parent_, d_uoff_, d_perm_;
   DBuf<int64_t> d_fptr_, d_lptr_, d_dpos_, spos_, spos_full_, d_gptr_;
   DBuf<int2> d_grng_;  // extend-add source-column ranges per (front, chunk, child)
-  DBuf<int> d_pmap_, d_lists_, d_csn_, d_lbo_;
+  DBuf<int> d_pmap_, d_lists_, d_csn_, d_csnm_, d_lbo_;
   DBuf<double> F_, Sg_, xp_, ub_, logdet_, dcache_, ppart_, linv_, ldpart_;
   DBuf<int> status_, ldflag_;
   DBuf<unsigned> ldticket_;
-  int nfill_ = 0, nldchunk_ = 0;  // fill chunks; log-det chunks per problem
+  int nfill_ = 0, nfillm_ = 0, nldchunk_ = 0;  // fill chunks (values, model); log-det chunks per problem
   int num_sms_ = 148;
   int64_t ntot_ = 0;              // compact panel entries per problem
   int64_t launches_ = 0;

@@ -80,7 +80,9 @@ __global__ void __launch_bounds__(256) k_fill_panels(DevSym S, const int* __rest
 // Component model: value(p) = sum_t coef[b][t] * comp[t][p] + sum_q w[b][obs_q] * prod_q
 // over the observation contributions of entry p (A^T diag(w) A on the pattern).
 // diag_add is added on diagonal entries (pdiag[p] != 0), e.g. the 1e-12 jitter of
-// the prior log-determinant (inference.rs:831-837).
+// the prior log-determinant (inference.rs:831-837). One thread per panel entry
+// fills it for all B problems, so the entry's pattern data is read once.
+constexpr int kFillModelChunk = 512;  // 256 threads x 2 entries
 __global__ void __launch_bounds__(256) k_fill_panels_model(DevSym S, const int* __restrict__ csn, int64_t ntot,
                                                            const int* __restrict__ pmap, int ncomp,
                                                            const double* __restrict__ comp, int64_t nnz,
@@ -88,45 +90,43 @@ __global__ void __launch_bounds__(256) k_fill_panels_model(DevSym S, const int* 
                                                            const unsigned char* __restrict__ pdiag,
                                                            const int* __restrict__ cptr, const int* __restrict__ cobs,
                                                            const double* __restrict__ cprod,
-                                                           const double* __restrict__ w, int64_t wstride,
+                                                           const double* __restrict__ w, int64_t wstride, int B,
                                                            double* __restrict__ F, int64_t fstride) {
-  const int b = blockIdx.y;
   const int lo = csn[blockIdx.x], hi = csn[blockIdx.x + 1];
-  const double* cb = coef + (int64_t)b * ncomp;
-  const double* wb = w ? w + (int64_t)b * wstride : nullptr;
-  double* Fb = F + (int64_t)b * fstride;
-  int src[8];
-  int64_t dst[8];
 #pragma unroll
-  for (int u = 0; u < 8; ++u) {
-    const int64_t e = (int64_t)blockIdx.x * kFillChunk + threadIdx.x + 256 * u;
-    src[u] = -1;
-    dst[u] = -1;
-    if (e < ntot) {
-      const int s = fill_find(S, lo, hi, e);
-      src[u] = pmap[e];
-      dst[u] = S.fptr[s] + (e - S.lptr[s]);
+  for (int u = 0; u < 2; ++u) {
+    const int64_t e = (int64_t)blockIdx.x * kFillModelChunk + threadIdx.x + 256 * u;
+    if (e >= ntot) continue;
+    const int s = fill_find(S, lo, hi, e);
+    const int p = pmap[e];
+    const int64_t dst = S.fptr[s] + (e - S.lptr[s]);
+    if (p < 0) {
+      for (int b = 0; b < B; ++b) F[(int64_t)b * fstride + dst] = 0.0;
+      continue;
     }
-  }
+    double cv[8];
 #pragma unroll
-  for (int u = 0; u < 8; ++u) {
-    if (dst[u] < 0) continue;
-    const int p = src[u];
-    double v = 0.0;
-    if (p >= 0) {
-      for (int t = 0; t < ncomp; ++t) v += cb[t] * comp[(int64_t)t * nnz + p];
-      if (pdiag[p]) v += diag_add;
-      if (wb) {
+    for (int t = 0; t < 8; ++t) cv[t] = t < ncomp ? comp[(int64_t)t * nnz + p] : 0.0;
+    const double dadd = pdiag[p] ? diag_add : 0.0;
+    const int q0 = cptr[p], q1 = cptr[p + 1];
+    for (int b = 0; b < B; ++b) {
+      const double* cb = coef + (int64_t)b * ncomp;
+      double v = dadd;
+#pragma unroll
+      for (int t = 0; t < 8; ++t)
+        if (t < ncomp) v += cb[t] * cv[t];
+      if (w) {
+        const double* wb = w + (int64_t)b * wstride;
         double acc = 0.0;
         // design.rs:100-115: observations with a zero or non-finite weight are skipped
-        for (int q = cptr[p]; q < cptr[p + 1]; ++q) {
+        for (int q = q0; q < q1; ++q) {
           const double wq = wb[cobs[q]];
           if (wq != 0.0 && isfinite(wq)) acc += wq * cprod[q];
         }
         v += acc;
       }
+      F[(int64_t)b * fstride + dst] = v;
     }
-    Fb[dst[u]] = v;
   }
 }
 

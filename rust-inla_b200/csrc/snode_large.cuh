@@ -261,6 +261,80 @@ __global__ void __launch_bounds__(256) k_panel64(DevSym S, const int* __restrict
   }
 }
 
+// Rows of a 64-column block from this step's factored diagonal block (dcache:
+// L_JJ with D on the diagonal, written by k_panel64 launched with rpc = 0;
+// linv: L_JJ^-1): X = F_rows L_JJ^-T D^-1 for the 64 rows of CTA z, one
+// tensor-core GEMM. Used when many fronts x problems share a step, where a
+// factorization per row CTA would be redundant work.
+constexpr int kRowsSmem = 2 * kB64 * kLd64 * 8;
+__global__ void __launch_bounds__(256) k_rows64(DevSym S, const int* __restrict__ list, int j0,
+                                                double* __restrict__ F, int64_t fstride,
+                                                const double* __restrict__ dcache, const double* __restrict__ linv) {
+  extern __shared__ double smr[];
+  constexpr int ld = kLd64;
+  double* Bm = smr;             // Bm[u + t*ld] = L_JJ^-1[t][u] / d_t
+  double* Fa = Bm + kB64 * ld;  // Fa[t*ld + r] = F[r0 + r, j0 + t]
+  __shared__ double dinv[kB64];
+  const int s = list[blockIdx.x], b = blockIdx.y;
+  const int k = lg_k(S, s), m = lg_m(S, s);
+  if (j0 >= k) return;
+  const int w = min(kB64, k - j0);
+  const int r0 = j0 + w + blockIdx.z * kPanelRows;
+  if (r0 >= m) return;
+  const int rows = min(kPanelRows, m - r0);
+  double* Fs = F + (int64_t)b * fstride + S.fptr[s];
+  for (int e = threadIdx.x; e < kB64 * kPanelRows; e += blockDim.x) {
+    const int c = e >> 6, r = e & 63;
+    if (r < rows && c < w) cp_async8(&Fa[c * ld + r], Fs + (r0 + r) + (int64_t)(j0 + c) * m);
+    else Fa[c * ld + r] = 0.0;
+  }
+  cp_async_commit();
+  const double* dc = dcache + ((int64_t)blockIdx.x * gridDim.y + b) * (kB64 * kB64);
+  const double* lc = linv_block(S, linv, b, s, j0 / kB64);
+  if (threadIdx.x < kB64) dinv[threadIdx.x] = threadIdx.x < w ? 1.0 / dc[threadIdx.x * (kB64 + 1)] : 0.0;
+  __syncthreads();
+  double lv[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) lv[q] = lc[threadIdx.x + 256 * q];  // L_JJ^-1 column-major: (t, u) at t + 64 u
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const int e = threadIdx.x + 256 * q, t = e & 63, u = e >> 6;
+    Bm[u + t * ld] = lv[q] * dinv[t];
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wr = (warp & 1) * 32, wc = (warp >> 1) * 16;
+  const int g = lane >> 2, tg = lane & 3;
+  const int wk = (wr >= rows || wc >= w) ? 0 : (w + 3) & ~3;
+  double acc[4][2][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int q = 0; q < 2; ++q) acc[a][q][0] = acc[a][q][1] = 0.0;
+#pragma unroll 4
+  for (int kk = 0; kk < wk; kk += 4) {
+    double af[4], bf[2];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) af[a] = Fa[(kk + tg) * ld + wr + a * 8 + g];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) bf[q] = Bm[(kk + tg) + (wc + q * 8 + g) * ld];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int q = 0; q < 2; ++q) mma884(acc[a][q][0], acc[a][q][1], af[a], bf[q]);
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int r = wr + a * 8 + g, t = wc + q * 8 + tg * 2 + h;
+        if (r < rows && t < w) Fs[(r0 + r) + (int64_t)(j0 + t) * m] = acc[a][q][h];
+      }
+}
+
 constexpr int kUT64 = 64;
 __global__ void __launch_bounds__(128) k_update64(DevSym S, const int* __restrict__ list, int j0,
                                                  double* __restrict__ F, int64_t fstride,
