@@ -258,7 +258,22 @@ def factor_roofline(p, torch, B=21, reps=10):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / reps
     del bs
-    return {"flops_per_launch": flops * B, "ms": ms, "nnz_l": int(s.info()["nnz_l"])}
+    return {"flops_per_launch": flops * B, "ms": ms, "nnz_l": int(s.info()["nnz_l"]), "B": B}
+
+
+TRAFFIC_SUMMARY = Path(__file__).resolve().parent / "profiles" / "traffic_factor_spde200.md"
+
+
+def factor_traffic(B):
+    """DRAM bytes (read + write) of one batched factorization of B problems, from the committed
+    ncu summary (per-problem figure of a smaller capture; batch members use disjoint buffers)."""
+    try:
+        for line in TRAFFIC_SUMMARY.read_text().splitlines():
+            if line.startswith("dram_bytes_per_problem:"):
+                return int(line.split(":")[1]) * B, f"{TRAFFIC_SUMMARY.name} (per-problem DRAM bytes x {B})"
+    except OSError:
+        pass
+    return None, "no ncu traffic summary"
 
 
 def run_ours(args, ws, rank, local, dist):
@@ -344,10 +359,12 @@ def run_ours(args, ws, rank, local, dist):
     peak = measured_dgemm_tflops(torch)
     fr = factor_roofline(p, torch)
     achieved = fr["flops_per_launch"] / (fr["ms"] * 1e-3) / 1e12
+    traffic, tsrc = factor_traffic(fr["B"])
     roof = {"bound": "tensor", "kernel": "batched supernodal LDL^T (B=21 theta-points, nested dissection, sequence of level kernels)",
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
             "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64; the measured-peaks file has no FP64 entry)",
-            "traffic": None, "ms_per_launch": fr["ms"], "flops_per_launch": fr["flops_per_launch"]}
+            "traffic": traffic, "traffic_source": tsrc, "ms_per_launch": fr["ms"],
+            "flops_per_launch": fr["flops_per_launch"]}
 
     cpu = None
     if ws == 1 and args.cpu_seconds > 0:
