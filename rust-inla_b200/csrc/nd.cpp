@@ -78,27 +78,41 @@ void nd_order(int64_t n, const int64_t* colptr, const int64_t* rowidx, std::vect
   std::vector<int64_t> dist(n, -1), dstamp(n, -1);
   int64_t next_task = 0, bfs_id = 0;
 
-  // rooted level structure of the part `task` from `root`; returns the levels
-  auto bfs = [&](int64_t task, int64_t root, std::vector<std::vector<int64_t>>& levels) {
+  // rooted level structure of the part `task` from `root`: nodes in BFS order,
+  // level l = nodes[start[l] .. start[l+1]); dist[] holds the levels of this BFS
+  struct Levels {
+    std::vector<int64_t> nodes, start;
+    int64_t depth() const { return (int64_t)start.size() - 1; }
+    const int64_t* begin(int64_t l) const { return nodes.data() + start[l]; }
+    const int64_t* end(int64_t l) const { return nodes.data() + start[l + 1]; }
+    int64_t size(int64_t l) const { return start[l + 1] - start[l]; }
+  };
+  auto bfs = [&](int64_t task, int64_t root, Levels& L) {
     const int64_t id = bfs_id++;
-    levels.clear();
-    levels.push_back({root});
+    L.nodes.clear();
+    L.start.clear();
+    L.nodes.push_back(root);
+    L.start.push_back(0);
     dstamp[root] = id;
     dist[root] = 0;
-    for (size_t l = 0; l < levels.size(); ++l) {
-      std::vector<int64_t> nxt;
-      for (int64_t u : levels[l])
+    int64_t lev_begin = 0;
+    while (lev_begin < (int64_t)L.nodes.size()) {
+      const int64_t lev_end = (int64_t)L.nodes.size();
+      const int64_t l = (int64_t)L.start.size() - 1;
+      for (int64_t h = lev_begin; h < lev_end; ++h) {
+        const int64_t u = L.nodes[h];
         for (int64_t q = aptr[u]; q < aptr[u + 1]; ++q) {
           const int64_t v = adj[q];
           if (owner[v] != task || dstamp[v] == id) continue;
           dstamp[v] = id;
-          dist[v] = (int64_t)l + 1;
-          nxt.push_back(v);
+          dist[v] = l + 1;
+          L.nodes.push_back(v);
         }
-      if (nxt.empty()) break;
-      levels.push_back(std::move(nxt));
+      }
+      L.start.push_back(lev_end);
+      lev_begin = lev_end;
     }
-    return id;
+    // start has depth + 1 entries: the last one closes the deepest level
   };
   auto part_degree = [&](int64_t task, int64_t u) {
     int64_t d = 0;
@@ -136,7 +150,7 @@ void nd_order(int64_t n, const int64_t* colptr, const int64_t* rowidx, std::vect
     for (int64_t i = 0; i < n; ++i) all[i] = i;
     stack.push_back({std::move(all), false});
   }
-  std::vector<std::vector<int64_t>> levels, best_levels;
+  Levels levels, best_levels;
   while (!stack.empty()) {
     Work wk = std::move(stack.back());
     stack.pop_back();
@@ -178,18 +192,22 @@ void nd_order(int64_t n, const int64_t* colptr, const int64_t* rowidx, std::vect
       }
     }
     // pseudo-peripheral root
+    auto min_degree_last = [&](const Levels& L) {
+      const int64_t l = L.depth() - 1;
+      int64_t cand = *L.begin(l), cd = part_degree(task, cand);
+      for (const int64_t* it = L.begin(l); it != L.end(l); ++it) {
+        const int64_t d = part_degree(task, *it);
+        if (d < cd) cand = *it, cd = d;
+      }
+      return cand;
+    };
     bfs(task, *std::min_element(nodes.begin(), nodes.end()), levels);
     for (int it = 0; it < 3; ++it) {
-      const std::vector<int64_t>& last = levels.back();
-      int64_t cand = last[0], cd = part_degree(task, cand);
-      for (int64_t u : last) {
-        const int64_t d = part_degree(task, u);
-        if (d < cd) cand = u, cd = d;
-      }
-      best_levels = levels;
+      const int64_t cand = min_degree_last(levels);
+      std::swap(levels, best_levels);
       bfs(task, cand, levels);
-      if (levels.size() <= best_levels.size()) {
-        levels.swap(best_levels);
+      if (levels.depth() <= best_levels.depth()) {
+        std::swap(levels, best_levels);
         break;
       }
     }
@@ -200,24 +218,17 @@ void nd_order(int64_t n, const int64_t* colptr, const int64_t* rowidx, std::vect
     const int64_t N = (int64_t)nodes.size();
     std::vector<int64_t> sep, rest;
     int64_t best_size = -1;
-    std::vector<int64_t> roots{levels[0][0]};
-    {
-      const std::vector<int64_t>& last = levels.back();
-      int64_t cand = last[0], cd = part_degree(task, cand);
-      for (int64_t u : last) {
-        const int64_t d = part_degree(task, u);
-        if (d < cd) cand = u, cd = d;
-      }
-      if (cand != roots[0]) roots.push_back(cand);
-    }
-    for (int64_t rt : roots) {
-      bfs(task, rt, levels);
-      const int64_t h = (int64_t)levels.size();
+    int64_t roots[2] = {levels.nodes[0], min_degree_last(levels)};
+    const int nroots = roots[1] != roots[0] ? 2 : 1;
+    std::vector<int64_t> thin;
+    for (int ri = 0; ri < nroots; ++ri) {
+      bfs(task, roots[ri], levels);
+      const int64_t h = levels.depth();
       if (h < 3) continue;
-      std::vector<int64_t> cum(h + 1, 0), thin(h, 0);
-      for (int64_t l = 0; l < h; ++l) cum[l + 1] = cum[l] + (int64_t)levels[l].size();
+      thin.assign(h, 0);
       for (int64_t l = 0; l + 1 < h; ++l)
-        for (int64_t u : levels[l]) {
+        for (const int64_t* it = levels.begin(l); it != levels.end(l); ++it) {
+          const int64_t u = *it;
           bool touches = false;
           for (int64_t q = aptr[u]; q < aptr[u + 1] && !touches; ++q) {
             const int64_t v = adj[q];
@@ -227,18 +238,19 @@ void nd_order(int64_t n, const int64_t* colptr, const int64_t* rowidx, std::vect
         }
       int64_t pick = -1;
       for (int64_t l = 1; l + 1 < h; ++l) {
-        const int64_t below = cum[l], above = N - cum[l + 1];
+        const int64_t below = levels.start[l], above = N - levels.start[l + 1];
         if ((double)std::min(below, above) >= kBalance * (double)N && (pick < 0 || thin[l] < thin[pick])) pick = l;
       }
       if (pick < 0) {
         pick = 1;
-        while (pick + 2 < h && cum[pick + 1] < N / 2) ++pick;
+        while (pick + 2 < h && levels.start[pick + 1] < N / 2) ++pick;
       }
       if (best_size >= 0 && thin[pick] >= best_size) continue;
       best_size = thin[pick];
       sep.clear();
       rest.clear();
-      for (int64_t u : levels[pick]) {
+      for (const int64_t* it = levels.begin(pick); it != levels.end(pick); ++it) {
+        const int64_t u = *it;
         bool touches = false;
         for (int64_t q = aptr[u]; q < aptr[u + 1] && !touches; ++q) {
           const int64_t v = adj[q];
@@ -247,8 +259,7 @@ void nd_order(int64_t n, const int64_t* colptr, const int64_t* rowidx, std::vect
         (touches ? sep : rest).push_back(u);
       }
       for (int64_t l = 0; l < h; ++l)
-        if (l != pick)
-          for (int64_t u : levels[l]) rest.push_back(u);
+        if (l != pick) rest.insert(rest.end(), levels.begin(l), levels.end(l));
     }
     if (sep.empty() || rest.empty()) {
       emit_amd(nodes);
