@@ -160,7 +160,13 @@ int inla_batch_selinv_pattern_dev(inla_batch* h, int B, double* d_sigma, void* s
  * ---------------------------------------------------------------------- */
 typedef struct inla_laplace inla_laplace;
 
-enum { INLA_LAP_VARIANCES = 1, INLA_LAP_GRADIENT = 2 };
+/* INLA_LAP_NO_PRIOR_SHARING: evaluate every member's prior on its own. By default
+ * members whose prior coefficient vectors are proportional (c_b = s c_r, s > 0)
+ * share one prior factorization and selected inverse (log|Q_b| = log|Q_r| +
+ * n log s, tr(Q_b^-1 M_t) = tr(Q_r^-1 M_t) / s; the 1e-12 log-det jitter then acts
+ * as 1e-12 / s on the member). No reference counterpart (the reference
+ * evaluates one theta-point at a time). */
+enum { INLA_LAP_VARIANCES = 1, INLA_LAP_GRADIENT = 2, INLA_LAP_NO_PRIOR_SHARING = 8 };
 
 int inla_laplace_create(int64_t n, const int64_t* colptr, const int64_t* rowidx, int ncomp, const double* comp,
                         int64_t nobs, const int64_t* a_rowptr, const int64_t* a_colidx, const double* a_vals,

@@ -171,6 +171,7 @@ LaplaceEngine::LaplaceEngine(const LaplaceSpec& spec, int max_batch, cudaStream_
   }
   const size_t B = max_batch_;
   coef_.alloc(B * spec_.ncomp);
+  coefp_.alloc(B * spec_.ncomp);
   p1s_.alloc(B);
   x_.alloc(B * n);
   xt_.alloc(B * n);
@@ -248,14 +249,59 @@ void LaplaceEngine::eval(int B, const double* coef, const double* p1scale, int f
   double* d_scal = red_.p + (size_t)4 * B * T1;  // [B][8]: loglik, dll
 
   // ---- prior log-determinant: Q + 1e-12 I (inference.rs:831-837) ----------
-  fill_factor(B, false, 1e-12);
-  INLA_CUDA(cudaMemcpyAsync(ldp_.p, F_->d_logdet(), sizeof(double) * B, cudaMemcpyDeviceToDevice, stream_));
-  INLA_CUDA(cudaMemcpyAsync(stp_.p, F_->d_status(), sizeof(int) * B, cudaMemcpyDeviceToDevice, stream_));
+  // Batch members whose prior coefficient vectors are proportional (c_b = s c_r,
+  // s > 0; e.g. FD-stencil points that differ only in a precision scale) share one
+  // prior factorization: log|Q_b| = log|Q_r| + n log s and tr(Q_b^-1 M_t) =
+  // tr(Q_r^-1 M_t) / s. The 1e-12 jitter of the representative then stands for a
+  // jitter of 1e-12 / s on the member, a log-det difference of about
+  // 1e-12 |1/s - 1| tr(Q_r^-1). Identical vectors (s = 1) are shared exactly.
+  std::vector<int> prep(B);
+  std::vector<double> pscale(B, 1.0);
+  std::vector<int> reps;
+  for (int b = 0; b < B; ++b) {
+    const double* cb = coef + (size_t)b * T;
+    int t0 = 0;
+    while (t0 < T && cb[t0] == 0.0) ++t0;
+    int match = -1;
+    double ratio = 1.0;
+    if (!(flags & LAP_NO_PRIOR_SHARING) && t0 < T) {
+      for (size_t g = 0; g < reps.size() && match < 0; ++g) {
+        const double* cr = coef + (size_t)reps[g] * T;
+        if (cr[t0] == 0.0) continue;
+        const double rt = cb[t0] / cr[t0];
+        if (!(rt > 0.0) || !std::isfinite(rt)) continue;
+        bool same = true;
+        for (int t = 0; t < T && same; ++t) {
+          const double d = cb[t] - rt * cr[t];
+          same = (t < t0) ? cr[t] == 0.0 : std::fabs(d) <= 1e-13 * std::fabs(cb[t]) + 1e-300;
+        }
+        if (same) match = (int)g, ratio = rt;
+      }
+    }
+    if (match < 0) {
+      match = (int)reps.size();
+      reps.push_back(b);
+      ratio = 1.0;
+    }
+    prep[b] = match;
+    pscale[b] = ratio;
+  }
+  const int Bp = (int)reps.size();
+  {
+    std::vector<double> cp((size_t)Bp * T);
+    for (int g = 0; g < Bp; ++g)
+      for (int t = 0; t < T; ++t) cp[(size_t)g * T + t] = coef[(size_t)reps[g] * T + t];
+    INLA_CUDA(cudaMemcpyAsync(coefp_.p, cp.data(), sizeof(double) * Bp * T, cudaMemcpyHostToDevice, stream_));
+  }
+  F_->factor_model(spec_.ncomp, comp_.p, coefp_.p, 1e-12, pdiag_.p, cptr_.p, cobs_.p, cprod_.p, nullptr, spec_.nobs,
+                   Bp);
+  INLA_CUDA(cudaMemcpyAsync(ldp_.p, F_->d_logdet(), sizeof(double) * Bp, cudaMemcpyDeviceToDevice, stream_));
+  INLA_CUDA(cudaMemcpyAsync(stp_.p, F_->d_status(), sizeof(int) * Bp, cudaMemcpyDeviceToDevice, stream_));
   if (grad) {
-    F_->selinv(B);
-    k_pattern_full<<<dim3(grid1(nnz_), B), 256, 0, stream_>>>(nnz_, F_->d_spos_full(), F_->d_sigma(),
-                                                              F_->front_total(), sig_.p);
-    k_trace_contract_g<<<dim3(nchunks(nnz_, kRedChunk), B), 256, 0, stream_>>>(
+    F_->selinv(Bp);
+    k_pattern_full<<<dim3(grid1(nnz_), Bp), 256, 0, stream_>>>(nnz_, F_->d_spos_full(), F_->d_sigma(),
+                                                               F_->front_total(), sig_.p);
+    k_trace_contract_g<<<dim3(nchunks(nnz_, kRedChunk), Bp), 256, 0, stream_>>>(
         nnz_, T, comp_.p, sig_.p, cptr_.p, cobs_.p, cprod_.p, nullptr, nobs, gpart_.p, gtick_.p, d_trP);
     launches_ += 2;
   }
@@ -407,19 +453,35 @@ void LaplaceEngine::eval(int B, const double* coef, const double* p1scale, int f
       }
     }
   }
-  INLA_CUDA(cudaMemcpyAsync(ldprior.data(), ldp_.p, sizeof(double) * B, cudaMemcpyDeviceToHost, stream_));
-  INLA_CUDA(cudaMemcpyAsync(prior_status.data(), stp_.p, sizeof(int) * B, cudaMemcpyDeviceToHost, stream_));
+  INLA_CUDA(cudaMemcpyAsync(ldprior.data(), ldp_.p, sizeof(double) * Bp, cudaMemcpyDeviceToHost, stream_));
+  INLA_CUDA(cudaMemcpyAsync(prior_status.data(), stp_.p, sizeof(int) * Bp, cudaMemcpyDeviceToHost, stream_));
   INLA_CUDA(cudaMemcpyAsync(scal.data(), d_scal, sizeof(double) * 2 * B, cudaMemcpyDeviceToHost, stream_));
   INLA_CUDA(cudaMemcpyAsync(xmx.data(), d_xMx, sizeof(double) * B * T1, cudaMemcpyDeviceToHost, stream_));
   INLA_CUDA(cudaMemcpyAsync(bad.data(), bad_.p, sizeof(int) * B, cudaMemcpyDeviceToHost, stream_));
+  std::vector<double> trp_rep;
   if (grad) {
-    INLA_CUDA(cudaMemcpyAsync(R.trP.data(), d_trP, sizeof(double) * B * T1, cudaMemcpyDeviceToHost, stream_));
+    trp_rep.resize((size_t)Bp * T1);
+    INLA_CUDA(cudaMemcpyAsync(trp_rep.data(), d_trP, sizeof(double) * Bp * T1, cudaMemcpyDeviceToHost, stream_));
     INLA_CUDA(cudaMemcpyAsync(R.trQ.data(), d_trQ, sizeof(double) * B * T1, cudaMemcpyDeviceToHost, stream_));
     if (spec_.family != FAM_GAUSSIAN)
       INLA_CUDA(cudaMemcpyAsync(R.zMx.data(), d_zMx, sizeof(double) * B * T1, cudaMemcpyDeviceToHost, stream_));
   }
   INLA_CUDA(cudaStreamSynchronize(stream_));
   INLA_CUDA(cudaGetLastError());
+  // expand the shared prior results to every batch member (representatives were
+  // evaluated in slots 0..Bp-1)
+  {
+    std::vector<double> ldp_rep(ldprior.begin(), ldprior.begin() + Bp);
+    std::vector<int> stp_rep(prior_status.begin(), prior_status.begin() + Bp);
+    for (int b = 0; b < B; ++b) {
+      const int g = prep[b];
+      const double sc = pscale[b];
+      ldprior[b] = ldp_rep[g] + (double)n * std::log(sc);
+      prior_status[b] = stp_rep[g];
+      if (grad)
+        for (int t = 0; t < T1; ++t) R.trP[(size_t)b * T1 + t] = trp_rep[(size_t)g * T1 + t] / sc;
+    }
+  }
 
   for (int b = 0; b < B; ++b) {
     if (prior_status[b]) R.status[b] = LAP_SINGULAR_PRIOR;

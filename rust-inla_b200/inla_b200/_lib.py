@@ -31,6 +31,7 @@ ORDER_NATURAL = 3
 ORDER_CUSTOM = 4
 ORDER_TIME_MAJOR = 5
 ORDER_ND = 6
+LAP_NO_PRIOR_SHARING = 8
 
 _ERROR_NAMES = {
     INLA_ERR_SINGULAR: "Singular",

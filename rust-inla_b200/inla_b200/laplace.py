@@ -112,7 +112,9 @@ class LaplaceModel:
         except Exception:
             pass
 
-    def eval(self, coefs, p1scale=None, variances=False, gradient=False, mode=True):
+    def eval(self, coefs, p1scale=None, variances=False, gradient=False, mode=True, share_prior=True):
+        """Batched Laplace evaluation. ``share_prior``: members whose prior coefficient
+        vectors are proportional share one prior factorization / selected inverse."""
         coefs = np.atleast_2d(as_f64(coefs))
         B = coefs.shape[0]
         s = None if p1scale is None else as_f64(np.broadcast_to(p1scale, (B,)))
@@ -120,7 +122,7 @@ class LaplaceModel:
         x = np.zeros((B, self.n)) if mode else None
         var = np.zeros((B, self.n)) if variances else None
         gt = np.zeros((B, 4, self.ncomp + 1)) if gradient else None
-        flags = (1 if variances else 0) | (2 if gradient else 0)
+        flags = (1 if variances else 0) | (2 if gradient else 0) | (0 if share_prior else _lib.LAP_NO_PRIOR_SHARING)
         check(lib().inla_laplace_eval(self._h, B, dptr(coefs), None if s is None else dptr(s), flags, dptr(sc),
                                       None if x is None else dptr(x), None if var is None else dptr(var),
                                       None if gt is None else dptr(gt)))

@@ -66,6 +66,26 @@ def test_batch_equals_single(spde_small):
         np.testing.assert_array_equal(one["var"][0], allb["var"][b])
 
 
+def test_shared_prior_matches_separate(spde_small):
+    """Members whose prior coefficient vectors are proportional (FD-stencil points that
+    differ in the noise precision or in tau only) share one prior factorization; the
+    results agree with evaluating every prior on its own."""
+    p, lm = spde_small
+    t = np.array([4.0, -3.0, 2.5])
+    pts = [t, t + [0.05, 0, 0], t - [0.05, 0, 0], t + [0, 0.05, 0], t - [0, 0.05, 0], t + [0, 0, 0.05]]
+    coefs = np.stack([models.spde_coefs(q[1], q[2])[0] for q in pts])
+    scale = np.exp([q[0] for q in pts])
+    a = lm.eval(coefs, scale, gradient=True, share_prior=True)
+    b = lm.eval(coefs, scale, gradient=True, share_prior=False)
+    assert np.all(a["status"] == 0) and np.all(b["status"] == 0)
+    np.testing.assert_allclose(a["logdet_prior"], b["logdet_prior"], rtol=1e-12, atol=0)
+    np.testing.assert_allclose(a["mlik"], b["mlik"], rtol=0, atol=1e-10 * np.max(np.abs(b["logdet_post"])))
+    np.testing.assert_allclose(a["trP"], b["trP"], rtol=1e-9, atol=0)
+    # the posterior side is evaluated per member either way
+    np.testing.assert_array_equal(a["x"], b["x"])
+    np.testing.assert_array_equal(a["trQ"], b["trQ"])
+
+
 def _spde_grad(lm, theta):
     c, dc = models.spde_coefs(theta[1], theta[2])
     dcoef = np.zeros((3, 3))
