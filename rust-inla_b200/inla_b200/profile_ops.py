@@ -37,6 +37,9 @@ def main():
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--ordering", default="amd", choices=["amd", "nd"])
+    ap.add_argument("--stencil", action="store_true",
+                    help="laplace-grad batch shaped like one batched-Newton iteration: 3 candidates x "
+                         "(centre, +-h per coordinate), so stencil points share prior factorizations")
     a = ap.parse_args()
     from inla_b200 import _lib
     order = {"amd": _lib.ORDER_AMD, "nd": _lib.ORDER_ND}[a.ordering]
@@ -85,7 +88,20 @@ def main():
         del bs
     if a.op == "laplace-grad":
         lm = LaplaceModel(p.model, a=p.a, family="gaussian", y=p.y, max_batch=B, ordering=order)
-        th = np.array([4.6, -3.9, 2.6]) + 0.01 * np.random.default_rng(0).standard_normal((B, 3))
+        if a.stencil:
+            base = np.array([4.6, -3.9, 2.6])
+            pts = []
+            for cnd in range(3):
+                c0 = base + 0.1 * cnd
+                pts.append(c0)
+                for kk in range(3):
+                    for sgn in (1, -1):
+                        e = np.zeros(3)
+                        e[kk] = sgn * 1e-3
+                        pts.append(c0 + e)
+            th = np.array(pts[:B])
+        else:
+            th = np.array([4.6, -3.9, 2.6]) + 0.01 * np.random.default_rng(0).standard_normal((B, 3))
         coefs = np.stack([models.spde_coefs(t[1], t[2])[0] for t in th])
         scale = np.exp(th[:, 0])
         out["laplace_grad_ms"] = timed(lambda: lm.eval(coefs, scale, gradient=True, mode=False))
