@@ -359,40 +359,44 @@ void GpuFactor::factor_values(const double* d_vals, int B) {
 
 void GpuFactor::factor_model(int ncomp, const double* d_comp, const double* d_coef, double diag_add,
                              const unsigned char* d_pdiag, const int* d_cptr, const int* d_cobs,
-                             const double* d_cprod, const double* d_w, int64_t wstride, int B) {
+                             const double* d_cprod, const double* d_w, int64_t wstride, int B, int nprior,
+                             double diag_add_post) {
   if (B < 1 || B > max_batch_) throw std::runtime_error("batch size out of range");
+  if (nprior < 0 || nprior > B) throw std::runtime_error("prior count out of range");
   if (ncomp < 1 || ncomp > 8) throw std::runtime_error("1..8 precision components supported");
-  int64_t dbits;
+  int64_t dbits, dpbits;
   std::memcpy(&dbits, &diag_add, sizeof(dbits));
+  std::memcpy(&dpbits, &diag_add_post, sizeof(dpbits));
   launch_cached({2, B, ncomp, (int64_t)(uintptr_t)d_comp, (int64_t)(uintptr_t)d_coef, dbits,
                  (int64_t)(uintptr_t)d_pdiag, (int64_t)(uintptr_t)d_cptr, (int64_t)(uintptr_t)d_cobs,
-                 (int64_t)(uintptr_t)d_cprod, (int64_t)(uintptr_t)d_w, wstride},
+                 (int64_t)(uintptr_t)d_cprod, (int64_t)(uintptr_t)d_w, wstride, nprior, dpbits},
                 [&] {
                   k_fill_panels_model<<<dim3(nfillm_), 256, 0, stream_>>>(
                       ds_, d_csnm_.p, ntot_, d_pmap_.p, ncomp, d_comp, nnz_, d_coef, diag_add, d_pdiag, d_cptr, d_cobs,
-                      d_cprod, d_w, wstride, B, F_.p, ftotal_);
+                      d_cprod, d_w, wstride, B, nprior, diag_add_post, F_.p, ftotal_);
                   ++launches_;
                   run_factor_levels(B);
                 });
 }
 
-void GpuFactor::solve(double* d_x, int64_t xstride, int B) {
-  if (B < 1 || B > max_batch_) throw std::runtime_error("batch size out of range");
+void GpuFactor::solve(double* d_x, int64_t xstride, int B, int slot0) {
+  if (B < 1 || slot0 < 0 || slot0 + B > max_batch_) throw std::runtime_error("batch size out of range");
   const int n = (int)sym_.n;
   const int64_t fs = ftotal_;
+  const double* Fp = F_.p + (int64_t)slot0 * fs;
   dim3 gp(cdiv(n, 256) > 1024 ? 1024 : cdiv(n, 256), B);
-  launch_cached({3, B, (int64_t)(uintptr_t)d_x, xstride}, [&] {
+  launch_cached({3, B, (int64_t)(uintptr_t)d_x, xstride, slot0}, [&] {
     k_permute_in<<<gp, 256, 0, stream_>>>(n, d_perm_.p, d_x, xstride, xp_.p);
     ++launches_;
     for (const LevelPlan& P : levels_) {
       k_fwd32<128><<<dim3((unsigned)P.all.size(), B), 128, P.mmax_all * 8, stream_>>>(
-          ds_, d_lists_.p + P.off_all, F_.p, fs, xp_.p, ub_.p, std::max<int64_t>(usum_, 1));
+          ds_, d_lists_.p + P.off_all, Fp, fs, xp_.p, ub_.p, std::max<int64_t>(usum_, 1));
       ++launches_;
     }
     for (int l = (int)levels_.size() - 1; l >= 0; --l) {
       const LevelPlan& P = levels_[l];
       k_bwd32<128><<<dim3((unsigned)P.all.size(), B), 128, P.mmax_all * 8, stream_>>>(ds_, d_lists_.p + P.off_all,
-                                                                                    F_.p, fs, xp_.p);
+                                                                                    Fp, fs, xp_.p);
       ++launches_;
     }
     k_permute_out<<<gp, 256, 0, stream_>>>(n, d_perm_.p, xp_.p, d_x, xstride);
@@ -400,53 +404,57 @@ void GpuFactor::solve(double* d_x, int64_t xstride, int B) {
   });
 }
 
-void GpuFactor::selinv(int B) {
-  if (B < 1 || B > max_batch_) throw std::runtime_error("batch size out of range");
+void GpuFactor::selinv(int B, int slot0) {
+  if (B < 1 || slot0 < 0 || slot0 + B > max_batch_) throw std::runtime_error("batch size out of range");
   Sg_.alloc((size_t)max_batch_ * ftotal_);  // outside any capture
-  launch_cached({4, B}, [&] { selinv_levels(B); });
+  launch_cached({4, B, slot0}, [&] { selinv_levels(B, slot0); });
 }
 
-void GpuFactor::selinv_levels(int B) {
+void GpuFactor::selinv_levels(int B, int slot0) {
   const int64_t fs = ftotal_;
+  const double* Fp = F_.p + (int64_t)slot0 * fs;
+  double* Sp = Sg_.p + (int64_t)slot0 * fs;
+  const double* Lp = linv_.p + (int64_t)slot0 * ds_.lstride;
   for (int l = (int)levels_.size() - 1; l >= 0; --l) {
     const LevelPlan& P = levels_[l];
     if (!P.si_small.empty()) {
       int mm = P.mmax_si_small;
       k_selinv_small<256><<<dim3((unsigned)P.si_small.size(), B), 256, small_selinv_smem(mm, P.kmax_si_small),
                             stream_>>>(
-          ds_, d_lists_.p + P.off_si_small, F_.p, Sg_.p, fs);
+          ds_, d_lists_.p + P.off_si_small, Fp, Sp, fs);
       ++launches_;
     }
     if (!P.si_large.empty()) {
       const int nl = (int)P.si_large.size();
       const int* lst = d_lists_.p + P.off_si_large;
       if (P.rmax_si_large > 0) {
-        k_si_gather8<<<dim3(nl, B, cdiv(P.rmax_si_large, kGatherCols)), 256, 0, stream_>>>(ds_, lst, Sg_.p, fs);
+        k_si_gather8<<<dim3(nl, B, cdiv(P.rmax_si_large, kGatherCols)), 256, 0, stream_>>>(ds_, lst, Sp, fs);
         ++launches_;
       }
       const int nblk = cdiv(P.kmax_si_large, kB64);
       const int ptiles = cdiv(P.mmax_si_large, kSiT);
       for (int jb = 0; jb < nblk; ++jb) {
-        k_si_gemm64<<<dim3(nl, B, ptiles), 256, kSiGemmSmem, stream_>>>(ds_, lst, jb, F_.p, Sg_.p, fs, ppart_.p,
-                                                                        ptiles, linv_.p);
-        k_si_diag64<<<dim3(nl, B), 256, kSiDiagSmem, stream_>>>(ds_, lst, jb, F_.p, Sg_.p, fs, ppart_.p, ptiles,
-                                                                linv_.p);
+        k_si_gemm64<<<dim3(nl, B, ptiles), 256, kSiGemmSmem, stream_>>>(ds_, lst, jb, Fp, Sp, fs, ppart_.p,
+                                                                        ptiles, Lp);
+        k_si_diag64<<<dim3(nl, B), 256, kSiDiagSmem, stream_>>>(ds_, lst, jb, Fp, Sp, fs, ppart_.p, ptiles,
+                                                                Lp);
         launches_ += 2;
       }
     }
   }
 }
 
-void GpuFactor::extract_diag(double* d_out, int64_t ostride, int B) {
+void GpuFactor::extract_diag(double* d_out, int64_t ostride, int B, int slot0) {
   const int n = (int)sym_.n;
-  k_extract_diag<<<dim3(std::min(cdiv(n, 256), 1024), B), 256, 0, stream_>>>(ds_, Sg_.p, ftotal_, d_out, ostride);
+  k_extract_diag<<<dim3(std::min(cdiv(n, 256), 1024), B), 256, 0, stream_>>>(ds_, Sg_.p + (int64_t)slot0 * ftotal_,
+                                                                              ftotal_, d_out, ostride);
   ++launches_;
   INLA_CUDA(cudaGetLastError());
 }
 
-void GpuFactor::sigma_on_pattern(double* d_out, int B) {
-  k_pattern_values<<<dim3(std::min(cdiv(nnz_, 256), 2048), B), 256, 0, stream_>>>(nnz_, spos_.p, Sg_.p, ftotal_,
-                                                                                  d_out);
+void GpuFactor::sigma_on_pattern(double* d_out, int B, int slot0) {
+  k_pattern_values<<<dim3(std::min(cdiv(nnz_, 256), 2048), B), 256, 0, stream_>>>(
+      nnz_, spos_.p, Sg_.p + (int64_t)slot0 * ftotal_, ftotal_, d_out);
   ++launches_;
   INLA_CUDA(cudaGetLastError());
 }

@@ -85,25 +85,29 @@ class GpuFactor {
   // Factorize B problems whose full-CSC values (input pattern order) are at
   // d_vals [B][nnz] on the device. Results stay resident.
   void factor_values(const double* d_vals, int B);
-  // Factorize from the component model (see k_fill_panels_model).
+  // Factorize from the component model (see k_fill_panels_model): problems
+  // [0, nprior) get diag_add and no observation term, problems [nprior, B)
+  // diag_add_post and the weights w + (b - nprior) * wstride (if d_w).
   void factor_model(int ncomp, const double* d_comp, const double* d_coef, double diag_add,
                     const unsigned char* d_pdiag, const int* d_cptr, const int* d_cobs, const double* d_cprod,
-                    const double* d_w, int64_t wstride, int B);
+                    const double* d_w, int64_t wstride, int B, int nprior = 0, double diag_add_post = 0.0);
   // Front offset of every input entry's lower twin (both triangles), for
   // reading Sigma / L on the full pattern.
   const int64_t* d_spos_full() const { return spos_full_.p; }
   // log|Q_b| and status words (after factor_*) -> device arrays of length B.
   const double* d_logdet() const { return logdet_.p; }
   const int* d_status() const { return status_.p; }
+  // The operations below act on the B problems in slots [slot0, slot0 + B) of
+  // the last factorization (e.g. the posterior part of a prior + posterior batch).
   // Solve Q_b x = rhs_b in place; d_x is [B][xstride] in original order.
-  void solve(double* d_x, int64_t xstride, int B);
+  void solve(double* d_x, int64_t xstride, int B, int slot0 = 0);
   // Selected inverse on the filled pattern; then extract diag / pattern values.
-  void selinv(int B);
-  void extract_diag(double* d_out, int64_t ostride, int B);
-  void sigma_on_pattern(double* d_out, int B);  // [B][nnz], lower entries, upper = 0
+  void selinv(int B, int slot0 = 0);
+  void extract_diag(double* d_out, int64_t ostride, int B, int slot0 = 0);
+  void sigma_on_pattern(double* d_out, int B, int slot0 = 0);  // [B][nnz], lower entries, upper = 0
   const int64_t* d_spos() const { return spos_.p; }
   double* d_front() { return F_.p; }
-  double* d_sigma() { return Sg_.p; }
+  double* d_sigma(int slot0 = 0) { return Sg_.p + (int64_t)slot0 * ftotal_; }
 
   // Launch counters (kernels issued by this engine since construction).
   int64_t launches() const { return launches_; }
@@ -115,7 +119,7 @@ class GpuFactor {
  private:
   void plan_levels();
   void run_factor_levels(int B);
-  void selinv_levels(int B);
+  void selinv_levels(int B, int slot0);
   template <class Body>
   void launch_cached(const std::vector<int64_t>& key, Body&& body);
 

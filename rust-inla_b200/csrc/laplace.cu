@@ -60,7 +60,9 @@ LaplaceEngine::LaplaceEngine(const LaplaceSpec& spec, int max_batch, cudaStream_
   SymbolicOptions opt;
   opt.ordering = spec_.ordering;
   analyze(n, spec_.colptr.data(), spec_.rowidx.data(), opt, nullptr, sym);
-  F_.reset(new GpuFactor(sym, max_batch, stream_));
+  // twice the slots: a Gaussian evaluation factorizes prior representatives and
+  // posterior problems in one batch
+  F_.reset(new GpuFactor(sym, 2 * max_batch, stream_));
 
   auto find = [&](int64_t row, int64_t col) -> int64_t {
     auto b = spec_.rowidx.begin() + spec_.colptr[col], e = spec_.rowidx.begin() + spec_.colptr[col + 1];
@@ -172,6 +174,7 @@ LaplaceEngine::LaplaceEngine(const LaplaceSpec& spec, int max_batch, cudaStream_
   const size_t B = max_batch_;
   coef_.alloc(B * spec_.ncomp);
   coefp_.alloc(B * spec_.ncomp);
+  coefall_.alloc(2 * B * spec_.ncomp);
   p1s_.alloc(B);
   x_.alloc(B * n);
   xt_.alloc(B * n);
@@ -205,7 +208,7 @@ LaplaceEngine::~LaplaceEngine() = default;
 
 void LaplaceEngine::fill_factor(int B, bool posterior, double diag_add) {
   F_->factor_model(spec_.ncomp, comp_.p, coef_.p, diag_add, pdiag_.p, cptr_.p, cobs_.p, cprod_.p,
-                   posterior ? w_.p : nullptr, spec_.nobs, B);
+                   posterior ? w_.p : nullptr, spec_.nobs, B, posterior ? 0 : B, diag_add);
 }
 
 void LaplaceEngine::eval_lik(int B, const double* d_xsrc) {
@@ -293,17 +296,29 @@ void LaplaceEngine::eval(int B, const double* coef, const double* p1scale, int f
       for (int t = 0; t < T; ++t) cp[(size_t)g * T + t] = coef[(size_t)reps[g] * T + t];
     INLA_CUDA(cudaMemcpyAsync(coefp_.p, cp.data(), sizeof(double) * Bp * T, cudaMemcpyHostToDevice, stream_));
   }
-  F_->factor_model(spec_.ncomp, comp_.p, coefp_.p, 1e-12, pdiag_.p, cptr_.p, cobs_.p, cprod_.p, nullptr, spec_.nobs,
-                   Bp);
-  INLA_CUDA(cudaMemcpyAsync(ldp_.p, F_->d_logdet(), sizeof(double) * Bp, cudaMemcpyDeviceToDevice, stream_));
-  INLA_CUDA(cudaMemcpyAsync(stp_.p, F_->d_status(), sizeof(int) * Bp, cudaMemcpyDeviceToDevice, stream_));
-  if (grad) {
-    F_->selinv(Bp);
-    k_pattern_full<<<dim3(grid1(nnz_), Bp), 256, 0, stream_>>>(nnz_, F_->d_spos_full(), F_->d_sigma(),
+  // Gaussian likelihood: the posterior precision does not depend on the mode, so
+  // the prior representatives (slots [0, Bp)) and the posterior problems (slots
+  // [Bp, Bp + B)) are factorized -- and, for the gradient, selectively inverted --
+  // in one batched launch sequence: the latency-bound top levels of the
+  // elimination tree are paid once instead of twice.
+  const bool merged = spec_.family == FAM_GAUSSIAN;
+  const int post0 = merged ? Bp : 0;  // slot of the first posterior problem
+  auto prior_traces = [&]() {
+    k_pattern_full<<<dim3(grid1(nnz_), Bp), 256, 0, stream_>>>(nnz_, F_->d_spos_full(), F_->d_sigma(0),
                                                                F_->front_total(), sig_.p);
     k_trace_contract_g<<<dim3(nchunks(nnz_, kRedChunk), Bp), 256, 0, stream_>>>(
         nnz_, T, comp_.p, sig_.p, cptr_.p, cobs_.p, cprod_.p, nullptr, nobs, gpart_.p, gtick_.p, d_trP);
     launches_ += 2;
+  };
+  if (!merged) {
+    F_->factor_model(spec_.ncomp, comp_.p, coefp_.p, 1e-12, pdiag_.p, cptr_.p, cobs_.p, cprod_.p, nullptr,
+                     spec_.nobs, Bp, Bp);
+    INLA_CUDA(cudaMemcpyAsync(ldp_.p, F_->d_logdet(), sizeof(double) * Bp, cudaMemcpyDeviceToDevice, stream_));
+    INLA_CUDA(cudaMemcpyAsync(stp_.p, F_->d_status(), sizeof(int) * Bp, cudaMemcpyDeviceToDevice, stream_));
+    if (grad) {
+      F_->selinv(Bp);
+      prior_traces();
+    }
   }
 
   // ---- mode --------------------------------------------------------------------
@@ -326,13 +341,26 @@ void LaplaceEngine::eval(int B, const double* coef, const double* p1scale, int f
   auto fetch = [&]() {
     INLA_CUDA(cudaMemcpyAsync(st.data(), stats_.p, sizeof(double) * 2 * B, cudaMemcpyDeviceToHost, stream_));
     INLA_CUDA(cudaMemcpyAsync(bad.data(), bad_.p, sizeof(int) * B, cudaMemcpyDeviceToHost, stream_));
-    INLA_CUDA(cudaMemcpyAsync(pst.data(), F_->d_status(), sizeof(int) * B, cudaMemcpyDeviceToHost, stream_));
+    INLA_CUDA(cudaMemcpyAsync(pst.data(), F_->d_status() + post0, sizeof(int) * B, cudaMemcpyDeviceToHost, stream_));
     INLA_CUDA(cudaStreamSynchronize(stream_));
   };
   std::vector<char> active(B, 1);
   if (spec_.family == FAM_GAUSSIAN) {
-    // closed form (inference.rs:845-870): one Newton system from x = 0
-    newton_system(x_.p);
+    // closed form (inference.rs:845-870): one Newton system from x = 0, with the
+    // prior representatives in the same factorization
+    eval_lik(B, x_.p);
+    INLA_CUDA(cudaMemcpyAsync(coefall_.p, coefp_.p, sizeof(double) * Bp * T, cudaMemcpyDeviceToDevice, stream_));
+    INLA_CUDA(cudaMemcpyAsync(coefall_.p + (size_t)Bp * T, coef_.p, sizeof(double) * B * T,
+                              cudaMemcpyDeviceToDevice, stream_));
+    F_->factor_model(spec_.ncomp, comp_.p, coefall_.p, 1e-12, pdiag_.p, cptr_.p, cobs_.p, cprod_.p, w_.p, spec_.nobs,
+                     Bp + B, Bp, 0.0);
+    INLA_CUDA(cudaMemcpyAsync(ldp_.p, F_->d_logdet(), sizeof(double) * Bp, cudaMemcpyDeviceToDevice, stream_));
+    INLA_CUDA(cudaMemcpyAsync(stp_.p, F_->d_status(), sizeof(int) * Bp, cudaMemcpyDeviceToDevice, stream_));
+    k_newton_rhs<<<dim3(grid1(n), B), 256, 0, stream_>>>((int)n, T, qcp_.p, qri_.p, comp_.p, nnz_, coef_.p, atp,
+                                                         ati_.p, atv_.p, nobs, grad_.p, x_.p, step_.p);
+    F_->solve(step_.p, n, B, post0);
+    k_step_stats<256><<<B, 256, 0, stream_>>>((int)n, step_.p, stats_.p);
+    launches_ += 2;
     INLA_CUDA(cudaMemcpyAsync(x_.p, step_.p, sizeof(double) * B * n, cudaMemcpyDeviceToDevice, stream_));
     fetch();
     for (int b = 0; b < B; ++b) {
@@ -427,15 +455,20 @@ void LaplaceEngine::eval(int B, const double* coef, const double* p1scale, int f
     ++launches_;
   }
   std::vector<double> ldpost(B), ldprior(B), scal(2 * B), xmx((size_t)B * T1);
-  INLA_CUDA(cudaMemcpyAsync(ldpost.data(), F_->d_logdet(), sizeof(double) * B, cudaMemcpyDeviceToHost, stream_));
-  INLA_CUDA(cudaMemcpyAsync(pst.data(), F_->d_status(), sizeof(int) * B, cudaMemcpyDeviceToHost, stream_));
+  INLA_CUDA(cudaMemcpyAsync(ldpost.data(), F_->d_logdet() + post0, sizeof(double) * B, cudaMemcpyDeviceToHost,
+                            stream_));
+  INLA_CUDA(cudaMemcpyAsync(pst.data(), F_->d_status() + post0, sizeof(int) * B, cudaMemcpyDeviceToHost, stream_));
 
   // ---- selected inverse of Q_post: variances and trace pieces --------------------
+  if (merged && grad) {
+    F_->selinv(Bp + B, 0);  // prior representatives and posterior problems together
+    prior_traces();
+  }
   if (want_var) {
-    F_->selinv(B);
-    F_->extract_diag(var_.p, n, B);
+    if (!(merged && grad)) F_->selinv(B, post0);
+    F_->extract_diag(var_.p, n, B, post0);
     if (grad) {
-      k_pattern_full<<<dim3(grid1(nnz_), B), 256, 0, stream_>>>(nnz_, F_->d_spos_full(), F_->d_sigma(),
+      k_pattern_full<<<dim3(grid1(nnz_), B), 256, 0, stream_>>>(nnz_, F_->d_spos_full(), F_->d_sigma(post0),
                                                                 F_->front_total(), sig_.p);
       k_trace_contract_g<<<dim3(nchunks(nnz_, kRedChunk), B), 256, 0, stream_>>>(
           nnz_, T, comp_.p, sig_.p, cptr_.p, cobs_.p, cprod_.p, w_.p, nobs, gpart_.p, gtick_.p, d_trQ);

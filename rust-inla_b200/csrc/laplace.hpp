@@ -91,7 +91,7 @@ class LaplaceEngine {
   DBuf<unsigned char> pdiag_;
   // per-batch work
   DBuf<double> coef_, p1s_, x_, xt_, step_, eta_, logp_, grad_, w_, dw_, var_, sig_, red_, stats_, alpha_, tmp_n_,
-      tmp_o_, ldp_, gpart_, coefp_;
+      tmp_o_, ldp_, gpart_, coefp_, coefall_;
   DBuf<unsigned> gtick_;  // grid-reduction partials and tickets
   DBuf<int> bad_, stp_;
   int64_t launches_ = 0;

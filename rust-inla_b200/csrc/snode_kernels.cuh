@@ -80,8 +80,11 @@ __global__ void __launch_bounds__(256) k_fill_panels(DevSym S, const int* __rest
 // Component model: value(p) = sum_t coef[b][t] * comp[t][p] + sum_q w[b][obs_q] * prod_q
 // over the observation contributions of entry p (A^T diag(w) A on the pattern).
 // diag_add is added on diagonal entries (pdiag[p] != 0), e.g. the 1e-12 jitter of
-// the prior log-determinant (inference.rs:831-837). One thread per panel entry
-// fills it for all B problems, so the entry's pattern data is read once.
+// the prior log-determinant (inference.rs:831-837). Problems [0, nprior) are prior
+// precisions (diag_add, no observation term); problems [nprior, B) add
+// diag_add_post and take their weights from w + (b - nprior) * wstride (if w).
+// One thread per panel entry fills it for all B problems, so the entry's pattern
+// data is read once.
 constexpr int kFillModelChunk = 512;  // 256 threads x 2 entries
 __global__ void __launch_bounds__(256) k_fill_panels_model(DevSym S, const int* __restrict__ csn, int64_t ntot,
                                                            const int* __restrict__ pmap, int ncomp,
@@ -91,6 +94,7 @@ __global__ void __launch_bounds__(256) k_fill_panels_model(DevSym S, const int* 
                                                            const int* __restrict__ cptr, const int* __restrict__ cobs,
                                                            const double* __restrict__ cprod,
                                                            const double* __restrict__ w, int64_t wstride, int B,
+                                                           int nprior, double diag_add_post,
                                                            double* __restrict__ F, int64_t fstride) {
   const int lo = csn[blockIdx.x], hi = csn[blockIdx.x + 1];
 #pragma unroll
@@ -107,16 +111,16 @@ __global__ void __launch_bounds__(256) k_fill_panels_model(DevSym S, const int* 
     double cv[8];
 #pragma unroll
     for (int t = 0; t < 8; ++t) cv[t] = t < ncomp ? comp[(int64_t)t * nnz + p] : 0.0;
-    const double dadd = pdiag[p] ? diag_add : 0.0;
+    const bool isdiag = pdiag[p] != 0;
     const int q0 = cptr[p], q1 = cptr[p + 1];
     for (int b = 0; b < B; ++b) {
       const double* cb = coef + (int64_t)b * ncomp;
-      double v = dadd;
+      double v = isdiag ? (b < nprior ? diag_add : diag_add_post) : 0.0;
 #pragma unroll
       for (int t = 0; t < 8; ++t)
         if (t < ncomp) v += cb[t] * cv[t];
-      if (w) {
-        const double* wb = w + (int64_t)b * wstride;
+      if (w && b >= nprior) {
+        const double* wb = w + (int64_t)(b - nprior) * wstride;
         double acc = 0.0;
         // design.rs:100-115: observations with a zero or non-finite weight are skipped
         for (int q = q0; q < q1; ++q) {
