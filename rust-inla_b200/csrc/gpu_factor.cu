@@ -204,6 +204,8 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
   }
   set_smem(k_update64, kUpdSmem);
   set_smem(k_rows64, kRowsSmem);
+  set_smem(k_fwd32<128>, (int)((S.max_m + 2 + 32 * 33) * 8));
+  set_smem(k_bwd32<128>, (int)((S.max_m + 2 + 32 * 33) * 8));
   set_smem(k_gather8, 200 * 1024 + 8 * kGatherCols * 8);
   set_smem(k_si_gemm64, kSiGemmSmem);
   set_smem(k_si_diag64, kSiDiagSmem);
@@ -389,13 +391,13 @@ void GpuFactor::solve(double* d_x, int64_t xstride, int B, int slot0) {
     k_permute_in<<<gp, 256, 0, stream_>>>(n, d_perm_.p, d_x, xstride, xp_.p);
     ++launches_;
     for (const LevelPlan& P : levels_) {
-      k_fwd32<128><<<dim3((unsigned)P.all.size(), B), 128, P.mmax_all * 8, stream_>>>(
+      k_fwd32<128><<<dim3((unsigned)P.all.size(), B), 128, (P.mmax_all + 2 + 32 * 33) * 8, stream_>>>(
           ds_, d_lists_.p + P.off_all, Fp, fs, xp_.p, ub_.p, std::max<int64_t>(usum_, 1));
       ++launches_;
     }
     for (int l = (int)levels_.size() - 1; l >= 0; --l) {
       const LevelPlan& P = levels_[l];
-      k_bwd32<128><<<dim3((unsigned)P.all.size(), B), 128, P.mmax_all * 8, stream_>>>(ds_, d_lists_.p + P.off_all,
+      k_bwd32<128><<<dim3((unsigned)P.all.size(), B), 128, (P.mmax_all + 2 + 32 * 33) * 8, stream_>>>(ds_, d_lists_.p + P.off_all,
                                                                                     Fp, fs, xp_.p);
       ++launches_;
     }

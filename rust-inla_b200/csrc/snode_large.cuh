@@ -441,7 +441,7 @@ __global__ void __launch_bounds__(128) k_update64(DevSym S, const int* __restric
 // ---------------------------------------------------------------------------
 
 template <int NT>
-__global__ void __launch_bounds__(NT) k_fwd32(DevSym S, const int* __restrict__ list, const double* __restrict__ F,
+__global__ void __launch_bounds__(NT, 8) k_fwd32(DevSym S, const int* __restrict__ list, const double* __restrict__ F,
                                               int64_t fstride, double* __restrict__ xp, double* __restrict__ ub,
                                               int64_t ustride) {
   extern __shared__ double y[];
@@ -461,18 +461,20 @@ __global__ void __launch_bounds__(NT) k_fwd32(DevSym S, const int* __restrict__ 
     __syncthreads();
   }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* Ls = y + ((m + 1) & ~1);  // [32][33] strictly lower part of the block's diagonal tile
   for (int jb = 0; jb < k; jb += 32) {
     const int wb = min(32, k - jb);
+    for (int e = threadIdx.x; e < 32 * 32; e += NT) {
+      const int r = e & 31, c = e >> 5;
+      Ls[r * 33 + c] = (c < r && r < wb) ? Fs[(jb + r) + (int64_t)(jb + c) * m] : 0.0;
+    }
+    __syncthreads();
     if (warp == 0) {
-      double Lrow[32];
-#pragma unroll
-      for (int j = 0; j < 32; ++j)
-        Lrow[j] = (j < lane && lane < wb) ? Fs[(jb + lane) + (int64_t)(jb + j) * m] : 0.0;
       double yi = lane < wb ? y[jb + lane] : 0.0;
-#pragma unroll
+#pragma unroll 8
       for (int j = 0; j < 32; ++j) {
         const double yj = __shfl_sync(0xffffffffu, yi, j);
-        if (j < lane) yi -= Lrow[j] * yj;
+        yi -= Ls[lane * 33 + j] * yj;
       }
       if (lane < wb) y[jb + lane] = yi;
     }
@@ -495,7 +497,7 @@ __global__ void __launch_bounds__(NT) k_fwd32(DevSym S, const int* __restrict__ 
 }
 
 template <int NT>
-__global__ void __launch_bounds__(NT) k_bwd32(DevSym S, const int* __restrict__ list, const double* __restrict__ F,
+__global__ void __launch_bounds__(NT, 8) k_bwd32(DevSym S, const int* __restrict__ list, const double* __restrict__ F,
                                               int64_t fstride, double* __restrict__ xp) {
   extern __shared__ double x[];
   const int s = list[blockIdx.x], b = blockIdx.y;
@@ -506,6 +508,7 @@ __global__ void __launch_bounds__(NT) k_bwd32(DevSym S, const int* __restrict__ 
   for (int t = threadIdx.x; t < m; t += NT) x[t] = xb[R[t]];
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* Ls = x + ((m + 1) & ~1);  // [32][33] strictly lower part of the block's diagonal tile
   const int nblk = (k + 31) / 32;
   for (int bi = nblk - 1; bi >= 0; --bi) {
     const int jb = bi * 32, wb = min(32, k - jb), i0 = jb + wb;
@@ -527,17 +530,18 @@ __global__ void __launch_bounds__(NT) k_bwd32(DevSym S, const int* __restrict__ 
       if (lane == 0) x[j] -= acc;
     }
     __syncthreads();
+    for (int e = threadIdx.x; e < 32 * 32; e += NT) {
+      const int r = e & 31, c = e >> 5;
+      Ls[r * 33 + c] = (c < r && r < wb) ? Fs[(jb + r) + (int64_t)(jb + c) * m] : 0.0;
+    }
+    __syncthreads();
     if (warp == 0) {
       // lane j holds x_{jb+j}; unit upper L_JJ^T solved from the last row up
-      double Lcol[32];
-#pragma unroll
-      for (int i = 0; i < 32; ++i)
-        Lcol[i] = (i > lane && i < wb && lane < wb) ? Fs[(jb + i) + (int64_t)(jb + lane) * m] : 0.0;
       double xj = lane < wb ? x[jb + lane] : 0.0;
-#pragma unroll
+#pragma unroll 8
       for (int i = 31; i >= 0; --i) {
         const double xi = __shfl_sync(0xffffffffu, xj, i);
-        if (i > lane) xj -= Lcol[i] * xi;
+        xj -= Ls[i * 33 + lane] * xi;
       }
       if (lane < wb) x[jb + lane] = xj;
     }
