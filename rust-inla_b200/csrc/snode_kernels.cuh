@@ -606,7 +606,7 @@ __host__ __device__ constexpr int small_selinv_smem(int m, int k) {
 // with tensor-core tiles for the products and L_JJ^-1 formed by one warp
 // while the others compute G.
 template <int NT>
-__global__ void __launch_bounds__(NT) k_selinv_small(DevSym S, const int* __restrict__ list,
+__global__ void __launch_bounds__(NT, 4) k_selinv_small(DevSym S, const int* __restrict__ list,
                                                      const double* __restrict__ F, double* __restrict__ Sg,
                                                      int64_t fstride) {
   extern __shared__ double smem[];
