@@ -465,31 +465,28 @@ void InlaDriver::newton(std::vector<double>& x, const FitOptions& opt, int& iter
       for (double& v : p) v *= delta / pmax;
       slope *= delta / pmax;
     }
+    // Backtracking on alpha = 1, 1/2, 1/4: each candidate is one batch (its point
+    // and the 2m gradient-stencil points for the next Hessian); shorter steps
+    // are evaluated only when the longer one fails the sufficient-decrease test.
     static const double kA[3] = {1.0, 0.5, 0.25};
-    std::vector<std::vector<double>> cands;
-    for (double a : kA) {
-      std::vector<double> c(x);
-      for (int i = 0; i < m; ++i) c[i] += a * p[i];
-      cands.push_back(c);
-    }
-    std::vector<double> fc, gc, Hc;
-    eval_stencils(cands, h, fc, gc, Hc);
+    std::vector<double> fc, gc, Hc, xc;
     int best = -1;
-    for (int k = 0; k < 3; ++k)
-      if (fc[k] < 1e11 && fc[k] <= f + 1e-4 * kA[k] * slope) {
-        best = k;
-        break;
-      }
+    for (int k = 0; k < 3 && best < 0; ++k) {
+      xc = x;
+      for (int i = 0; i < m; ++i) xc[i] += kA[k] * p[i];
+      eval_stencils({xc}, h, fc, gc, Hc);
+      if (fc[0] < 1e11 && fc[0] <= f + 1e-4 * kA[k] * slope) best = k;
+    }
     if (best < 0) {
       delta *= 0.25;
       if (delta < 1e-8) break;
       continue;
     }
     const double fprev = f;
-    x = cands[best];
-    f = fc[best];
-    g.assign(gc.begin() + (size_t)best * m, gc.begin() + (size_t)(best + 1) * m);
-    H.assign(Hc.begin() + (size_t)best * m * m, Hc.begin() + (size_t)(best + 1) * m * m);
+    x = xc;
+    f = fc[0];
+    g.assign(gc.begin(), gc.begin() + m);
+    H.assign(Hc.begin(), Hc.begin() + (size_t)m * m);
     if (std::getenv("INLA_DEBUG"))
       std::fprintf(stderr, "newton it=%d f=%.10g |g|=%.3g delta=%.3g alpha=%.3g capped=%d\n", it, f, gmax, delta,
                    kA[best], (int)capped);
