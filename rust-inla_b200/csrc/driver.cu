@@ -436,7 +436,7 @@ void InlaDriver::newton(std::vector<double>& x, const FitOptions& opt, int& iter
   std::vector<double> f1, g, H;
   eval_stencils({x}, h, f1, g, H);
   double f = f1[0];
-  double delta = 1.0;  // trust bound on max |step| (theta lives on log scales)
+  double delta = 2.0;  // trust bound on max |step| (theta lives on log scales: a factor e^2 per step)
   iters = 0;
   for (int it = 0; it < opt.max_iter; ++it) {
     iters = it + 1;
