@@ -1,5 +1,8 @@
 // Host orchestration of the batched supernodal kernels.
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "gpu_factor.hpp"
@@ -22,6 +25,7 @@ void set_smem(K kernel, int bytes) {
 
 GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
     : sym_(sym), max_batch_(max_batch), stream_(stream) {
+  const auto tstart = std::chrono::steady_clock::now();
   if (max_batch < 1) throw std::runtime_error("max_batch must be >= 1");
   const Symbolic& S = sym_;
   const int64_t ns = S.nsuper, n = S.n;
@@ -75,6 +79,7 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
       spos[p] = spos_full[p];
     }
 
+  const auto tm1 = std::chrono::steady_clock::now();
   d_first_.upload(first, stream_);
   d_rowptr_.upload(rowptr, stream_);
   d_rows_.upload(rows, stream_);
@@ -106,6 +111,7 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
   ds_.dpos = d_dpos_.p;
   ds_.perm = d_perm_.p;
 
+  const auto tm2 = std::chrono::steady_clock::now();
   // inverse-block cache: one 64 x 64 block per 64 pivot columns of every large front
   {
     std::vector<int> lbo(ns, -1);
@@ -147,6 +153,7 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
   ldticket_.alloc((size_t)max_batch_);
   INLA_CUDA(cudaMemsetAsync(ldticket_.p, 0, sizeof(unsigned) * max_batch_, stream_));
 
+  const auto tm3 = std::chrono::steady_clock::now();
   plan_levels();
   // extend-add range table: for every large front, column chunk z (of the
   // level's gcols columns) and child, the child's source columns whose parent
@@ -178,6 +185,7 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
     d_grng_.upload(grng, stream_);
   }
 
+  const auto ta = std::chrono::steady_clock::now();
   F_.alloc((size_t)max_batch_ * ftotal_);
   xp_.alloc((size_t)max_batch_ * n);
   ub_.alloc((size_t)max_batch_ * std::max<int64_t>(usum_, 1));
@@ -210,6 +218,14 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
   set_smem(k_si_gemm64, kSiGemmSmem);
   set_smem(k_si_diag64, kSiDiagSmem);
   INLA_CUDA(cudaStreamSynchronize(stream_));
+  if (std::getenv("INLA_DEBUG"))
+    std::fprintf(stderr, "device factor: maps %.1f ms, symbolic uploads %.1f ms, caches %.1f ms, levels %.1f ms, buffers %.1f ms (%d slots)\n",
+                 std::chrono::duration<double, std::milli>(tm1 - tstart).count(),
+                 std::chrono::duration<double, std::milli>(tm2 - tm1).count(),
+                 std::chrono::duration<double, std::milli>(tm3 - tm2).count(),
+                 std::chrono::duration<double, std::milli>(ta - tm3).count(),
+                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ta).count(),
+                 max_batch_);
 }
 
 GpuFactor::~GpuFactor() {

@@ -1,6 +1,9 @@
 // Batched Laplace engine: host control of the device Newton loop.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 
@@ -56,13 +59,20 @@ LaplaceEngine::LaplaceEngine(const LaplaceSpec& spec, int max_batch, cudaStream_
     if (!std::is_sorted(spec_.rowidx.begin() + spec_.colptr[c], spec_.rowidx.begin() + spec_.colptr[c + 1]))
       throw std::runtime_error("laplace: pattern row indices must be sorted");
 
+  const auto t0 = std::chrono::steady_clock::now();
   Symbolic sym;
   SymbolicOptions opt;
   opt.ordering = spec_.ordering;
   analyze(n, spec_.colptr.data(), spec_.rowidx.data(), opt, nullptr, sym);
+  const auto t1 = std::chrono::steady_clock::now();
   // twice the slots: a Gaussian evaluation factorizes prior representatives and
   // posterior problems in one batch
   F_.reset(new GpuFactor(sym, 2 * max_batch, stream_));
+  const auto t2 = std::chrono::steady_clock::now();
+  if (std::getenv("INLA_DEBUG"))
+    std::fprintf(stderr, "laplace setup: symbolic %.1f ms, device factor %.1f ms\n",
+                 std::chrono::duration<double, std::milli>(t1 - t0).count(),
+                 std::chrono::duration<double, std::milli>(t2 - t1).count());
 
   auto find = [&](int64_t row, int64_t col) -> int64_t {
     auto b = spec_.rowidx.begin() + spec_.colptr[col], e = spec_.rowidx.begin() + spec_.colptr[col + 1];
