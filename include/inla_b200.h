@@ -173,6 +173,26 @@ int inla_laplace_create(int64_t n, const int64_t* colptr, const int64_t* rowidx,
                         int family, const double* y, const double* p1, const double* p2, int ordering,
                         int max_batch, inla_laplace** out);
 void inla_laplace_free(inla_laplace* h);
+/* Hard linear constraints C x = e for every later evaluation and fit: the
+ * Augmented method of find_latent_mode_a_with_solver (inference.rs:804-830,
+ * 867-869, 902-904, 949-951; constraints.rs:268-353). The working prior is
+ * Q + kappa C^T C with kappa = 3.059023205018258e6 (HARD_CONSTRAINT_KAPPA); the
+ * prior log-determinant is log|Q + kappa C^T C| without the 1e-12 jitter;
+ * Newton trial points and the mode are projected onto C x = e. c: [k][n]
+ * row-major dense (ConstraintSpec.a), e: [k] (ConstraintSpec.e); k = 0 removes
+ * the constraints. Both methods below give the reference's results; they
+ * differ in how Q + kappa C^T C is held (a new symbolic analysis either way):
+ *  INLA_CONSTR_AUGMENTED: as the reference, kappa C^T C added on the pattern
+ *    widened by its support (sum over rows of nnz(row)^2 <= 2^26 entries);
+ *  INLA_CONSTR_BORDERED (no reference counterpart): the sparse bordered matrix
+ *    [[Q, C^T], [C, -I/kappa]] of order n + k, whose Schur complement is
+ *    Q + kappa C^T C, so no constrained block densifies;
+ *  INLA_CONSTR_AUTO: augmented up to 2^22 added entries, else bordered.
+ * Limits: k <= 1024, at most 7 model components. INLA_ERR_INVALID for a singular
+ * C C^T (pivot below 1e-14, constraints.rs:369-371); the previous constraints
+ * then stay. */
+enum { INLA_CONSTR_AUTO = 0, INLA_CONSTR_AUGMENTED = 1, INLA_CONSTR_BORDERED = 2 };
+int inla_laplace_set_constraints(inla_laplace* h, int k, const double* c, const double* e, int method);
 /* scalars: [B][8] = {mlik, log|Q+1e-12 I|, log|Q_post|, loglik, x'Qx, newton iterations,
  * status (0 ok, 1 singular prior, 2 singular posterior, 3 invalid likelihood, 4 non-finite
  * step, 5 not converged), d loglik / d log p1scale}. x, var: [B][n] or NULL (modes and
@@ -188,7 +208,8 @@ enum {
   INLA_PRIOR_PC_PREC = 1,   /* p = {u, alpha}: priors.rs:532-548 */
   INLA_PRIOR_LOGGAMMA = 2,  /* p = {shape, rate}: priors.rs:836-855 */
   INLA_PRIOR_PC_SPDE = 3,   /* p = {r0, alpha_r, s0, alpha_s}, slots (log tau, log kappa): priors.rs:127-147,813-834 */
-  INLA_PRIOR_GAUSSIAN = 4   /* p = {mean, precision} */
+  INLA_PRIOR_GAUSSIAN = 4,  /* p = {mean, precision} */
+  INLA_PRIOR_PC_COR1 = 5    /* p = {u, alpha}, theta = logit-type ((1 + rho) / 2): priors.rs:611-704 */
 };
 typedef struct {
   int kind;

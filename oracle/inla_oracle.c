@@ -627,7 +627,7 @@ static int project_constraints(int64_t n, double* x, int kc, const double* cA, c
     int piv = i;
     for (int rr = i + 1; rr < kc; ++rr)
       if (fabs(g[rr * kc + i]) > fabs(g[piv * kc + i])) piv = rr;
-    if (fabs(g[piv * kc + i]) < 1e-300) {
+    if (fabs(g[piv * kc + i]) < 1e-14) { /* constraints.rs:369-371 */
       free(r);
       free(g);
       return 1;
@@ -663,7 +663,11 @@ static int project_constraints(int64_t n, double* x, int kc, const double* cA, c
   return 0;
 }
 
-/* constraints.rs:275-313: Q + kappa A^T A, HARD_CONSTRAINT_KAPPA = exp(15) */
+int orc_project_constraints(int64_t n, double* x, int kc, const double* cA, const double* ce) {
+  return project_constraints(n, x, kc, cA, ce);
+}
+
+/* constraints.rs:275-313: Q + kappa A^T A, HARD_CONSTRAINT_KAPPA = 3.059023205018258e6 (its comment says exp(15)) */
 static void augment(const csc_t* q, int kc, const double* cA, csc_t* out) {
   const double kappa = 3.059023205018258e6;
   const int64_t n = q->n;

@@ -53,6 +53,8 @@ double orc_log_gamma(double z);
 /* ---- Laplace mode (inference.rs:776-975) ----
  * Q: full symmetric CSC; A: CSR n_obs x n (acp == NULL => identity);
  * constraints: kc rows of dense cA (kc x n) and ce (kc), kc = 0 for none. */
+/* constraints.rs:316-353: x <- x - C^T (C C^T)^-1 (C x - e); nonzero when C C^T is singular. */
+int orc_project_constraints(int64_t n, double* x, int kc, const double* cA, const double* ce);
 int orc_laplace(int64_t n, const int64_t* qcp, const int64_t* qri, const double* qv, int64_t nobs,
                 const int64_t* acp, const int64_t* aci, const double* av, int family, const double* y,
                 const double* p1, const double* p2, int kc, const double* cA, const double* ce, int max_iter,

@@ -57,6 +57,7 @@ def lib():
             "orc_takahashi_pattern": (C.c_int, [C.c_void_p, LP, LP, DP]),
             "orc_eval_lik": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, DP, DP, DP]),
             "orc_log_gamma": (C.c_double, [C.c_double]),
+            "orc_project_constraints": (C.c_int, [C.c_int64, DP, C.c_int, DP, DP]),
             "orc_laplace": (C.c_int, [C.c_int64, LP, LP, DP, C.c_int64, LP, LP, DP, C.c_int, DP, DP, DP,
                                       C.c_int, DP, DP, C.c_int, C.c_double, LP, DP, DP, DP]),
         }
@@ -187,6 +188,16 @@ def eval_lik(family, eta, y, p1=1.0, p2=1.0):
     if rc:
         raise OracleError("likelihood evaluation failed")
     return lp.value, g.value, h.value
+
+
+def project_constraints(x, c, e):
+    """constraints.rs:316-353 on a copy of ``x``."""
+    x = _f64(x).copy()
+    c = _f64(np.atleast_2d(c))
+    e = _f64(np.broadcast_to(e, (c.shape[0],)))
+    if lib().orc_project_constraints(len(x), _p(x), c.shape[0], _p(c), _p(e)):
+        raise OracleError("project_constraints: singular A A^T")
+    return x
 
 
 def log_gamma(z: float) -> float:
@@ -353,17 +364,70 @@ def ccd_design(m, f0=1.0):
     return np.array(pts), np.array(ws)
 
 
-def integrate(mode, hessian, eval_node, f0=1.0):
+def grid_design(m, step, threshold, evaluator):
+    """inla_math/src/integration.rs:64-156: m = 1 walks +step, then -step, while the
+    log-density drop from the centre stays <= threshold; m = 2 walks the axes, then keeps
+    the grid points within the threshold; m > 2 falls back to CCD with f0 = 2.5. Weights 1."""
+    if m == 0:
+        raise ValueError("Grid requires at least 1 factor")
+    if m > 2:
+        return ccd_design(m, 2.5)
+    g0 = evaluator([0.0] * m)
+    pts = []
+    if m == 1:
+        pts.append([0.0])
+        for sgn in (1.0, -1.0):
+            k = 1
+            while True:
+                z = [sgn * k * step]
+                if g0 - evaluator(z) > threshold:
+                    break
+                pts.append(z)
+                k += 1
+    else:
+        ext = []
+        for axis, sgn in ((0, 1.0), (0, -1.0), (1, 1.0), (1, -1.0)):
+            k = 0
+            while True:
+                z = [0.0, 0.0]
+                z[axis] = sgn * (k + 1) * step
+                if g0 - evaluator(z) > threshold:
+                    break
+                k += 1
+            ext.append(k)
+        max_i, min_i, max_j, min_j = ext
+        for i in range(-min_i, max_i + 1):
+            for j in range(-min_j, max_j + 1):
+                z = [i * step, j * step]
+                if g0 - evaluator(z) <= threshold:
+                    pts.append(z)
+    return np.array(pts), np.ones(len(pts))
+
+
+def integrate(mode, hessian, eval_node, f0=1.0, strategy="ccd"):
     """run_inla_inference_a_cancellable node map + aggregation (inference.rs:1262-1466).
 
-    ``eval_node(theta) -> (x_star, variances, log_post)``.
+    ``eval_node(theta) -> (x_star, variances, log_post)``; ``strategy`` "ccd" (f0) or
+    "grid" (step f0, threshold 4.0, evaluator = log_post at the mapped node).
     """
     m = len(mode)
     sigma = np.linalg.inv(-np.asarray(hessian))
     lam, V = np.linalg.eigh(sigma)
-    z, w = ccd_design(m, f0)
-    thetas = [np.asarray(mode) + V @ (np.sqrt(np.abs(lam)) * zk) for zk in z]
-    res = [eval_node(t) for t in thetas]
+    to_theta = lambda zk: np.asarray(mode) + V @ (np.sqrt(np.abs(lam)) * np.asarray(zk, dtype=float))
+    cache = {}
+
+    def node(zk):
+        key = tuple(float(v) for v in zk)
+        if key not in cache:
+            cache[key] = eval_node(to_theta(zk))
+        return cache[key]
+
+    if strategy == "grid":
+        z, w = grid_design(m, f0, 4.0, lambda zk: node(zk)[2])
+    else:
+        z, w = ccd_design(m, f0)
+    thetas = [to_theta(zk) for zk in z]
+    res = [node(zk) for zk in z]
     lps = np.array([r[2] for r in res])
     mx = lps.max()
     dens = np.exp(lps - mx)
@@ -385,6 +449,41 @@ def pc_prec_log_dens(theta, u, alpha):
     """priors.rs:532-548 with lambda = -ln(alpha)/u (priors.rs:78-86)."""
     lam = -math.log(alpha) / u
     return math.log(lam) - math.log(2.0) - lam * math.exp(-0.5 * theta) - 0.5 * theta
+
+
+def pc_cor1_lambda(u, alpha):
+    """priors.rs:611-660: scan, then 60 golden-section steps on the squared residual."""
+    if not -1.0 < u < 1.0 or not math.sqrt((1.0 - u) / 2.0) < alpha < 1.0:
+        raise ValueError("pc.cor1: invalid (u, alpha)")
+    fun = lambda lam: ((1.0 - math.exp(-lam * math.sqrt(1.0 - u))) / (1.0 - math.exp(-lam * math.sqrt(2.0)))
+                       - alpha) ** 2
+    best, bf = 1.0, fun(1.0)
+    for i in range(110):
+        lam = 1e-7 + (10.0 - 1e-7) * i / 99.0 if i < 100 else 10.0 + 90.0 * (i - 100) / 9.0
+        f = fun(lam)
+        if f < bf:
+            best, bf = lam, f
+    lo, hi = max(best * 0.5, 1e-8), best * 2.0
+    for _ in range(60):
+        m1, m2 = lo + 0.382 * (hi - lo), lo + 0.618 * (hi - lo)
+        if fun(m1) < fun(m2):
+            hi = m2
+        else:
+            lo = m1
+    lam = 0.5 * (lo + hi)
+    if fun(lam) > 1e-6:
+        raise ValueError("pc.cor1: failed to solve lambda")
+    return lam
+
+
+def pc_cor1_log_dens(theta, u, alpha):
+    """priors.rs:662-683: density of rho = 2 e^theta / (1 + e^theta) - 1 with its Jacobian."""
+    lam = pc_cor1_lambda(u, alpha)
+    e = math.exp(theta)
+    rho = 2.0 * e / (1.0 + e) - 1.0
+    s = math.sqrt(1.0 - rho)
+    return (math.log(lam) - lam * s - math.log(1.0 - math.exp(-math.sqrt(2.0) * lam)) - math.log(2.0 * s)
+            + math.log(2.0) + theta - 2.0 * math.log1p(e))
 
 
 def loggamma_log_dens(theta, shape, rate):

@@ -13,13 +13,66 @@ using namespace inla;
 struct inla_laplace {
   cudaStream_t stream = nullptr;
   std::unique_ptr<LaplaceEngine> eng;
+  LaplaceSpec spec;  // the caller's model, before any constraint augmentation
+  int max_batch = 0;
 };
 
 namespace {
 
-// priors.rs:532-548 (pc.prec), 813-834 (pc.spde, d = 2), 836-855 (loggamma)
+// pc.cor1 rate from P(rho > u) = alpha (priors.rs:611-660): coarse scan of lambda, then 60
+// golden-section steps on the squared residual; NaN when the residual stays above 1e-6.
+double pc_cor1_lambda(double u, double alpha) {
+  if (!(u > -1.0 && u < 1.0)) return NAN;
+  const double amin = std::sqrt((1.0 - u) / 2.0);
+  if (!(alpha > amin && alpha < 1.0)) return NAN;
+  auto fun = [&](double lam) {
+    const double ff = (1.0 - std::exp(-lam * std::sqrt(1.0 - u))) / (1.0 - std::exp(-lam * M_SQRT2));
+    return (ff - alpha) * (ff - alpha);
+  };
+  double best = 1.0, bf = fun(best);
+  for (int i = 0; i < 110; ++i) {
+    const double lam = i < 100 ? 1e-7 + (10.0 - 1e-7) * i / 99.0 : 10.0 + 90.0 * (i - 100) / 9.0;
+    const double f = fun(lam);
+    if (f < bf) bf = f, best = lam;
+  }
+  double lo = std::max(best * 0.5, 1e-8), hi = best * 2.0;
+  for (int it = 0; it < 60; ++it) {
+    const double m1 = lo + 0.382 * (hi - lo), m2 = lo + 0.618 * (hi - lo);
+    if (fun(m1) < fun(m2)) hi = m2;
+    else lo = m1;
+  }
+  const double lam = 0.5 * (lo + hi);
+  return fun(lam) > 1e-6 ? NAN : lam;
+}
+
+// log density of pc.cor1 on theta with rho = 2 e^theta / (1 + e^theta) - 1 (priors.rs:662-683)
+double pc_cor1_theta(double th, double lam) {
+  const double e = std::exp(th), rho = 2.0 * e / (1.0 + e) - 1.0;
+  if (!(rho > -1.0 && rho < 1.0)) return NAN;
+  const double s = std::sqrt(1.0 - rho);
+  return std::log(lam) - lam * s - std::log(1.0 - std::exp(-M_SQRT2 * lam)) - std::log(2.0 * s) + M_LN2 + th -
+         2.0 * std::log1p(e);
+}
+
+// priors.rs:532-548 (pc.prec), 813-834 (pc.spde, d = 2), 836-855 (loggamma), 611-704 (pc.cor1)
 double prior_one(const inla_prior_spec& s, const double* th, double* g) {
   switch (s.kind) {
+    case INLA_PRIOR_PC_COR1: {
+      const double lam = pc_cor1_lambda(s.p[0], s.p[1]);
+      const double t = th[s.slot];
+      const double v = pc_cor1_theta(t, lam);
+      if (g) {
+        const double e = std::exp(t), rho = 2.0 * e / (1.0 + e) - 1.0;
+        const double sq = std::sqrt(std::max(1.0 - rho, 0.0));
+        if (sq < 1e-8) {  // central difference near rho = 1 (priors.rs:690-696)
+          const double h = 1e-5;
+          g[s.slot] += (pc_cor1_theta(t + h, lam) - pc_cor1_theta(t - h, lam)) / (2.0 * h);
+        } else {
+          g[s.slot] += (lam * sq + 1.0) * (1.0 + rho) / 4.0 - rho;
+        }
+      }
+      return v;
+    }
     case INLA_PRIOR_PC_PREC: {
       const double lam = -std::log(s.p[1]) / s.p[0];
       const double e = std::exp(-0.5 * th[s.slot]);
@@ -134,6 +187,8 @@ int inla_laplace_create(int64_t n, const int64_t* colptr, const int64_t* rowidx,
     h = new inla_laplace();
     INLA_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     h->eng.reset(new LaplaceEngine(sp, max_batch, h->stream));
+    h->spec = std::move(sp);
+    h->max_batch = max_batch;
     *out = h;
     return INLA_OK;
   } catch (...) {
@@ -148,6 +203,43 @@ void inla_laplace_free(inla_laplace* h) {
   h->eng.reset();
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
+}
+
+int inla_laplace_set_constraints(inla_laplace* h, int k, const double* c, const double* e, int method) {
+  try {
+    if (!h || !h->eng) return fail(INLA_ERR_INVALID, "null handle");
+    if (k < 0 || (k > 0 && (!c || !e))) return fail(INLA_ERR_INVALID, "invalid constraint arguments");
+    if (method < INLA_CONSTR_AUTO || method > INLA_CONSTR_BORDERED)
+      return fail(INLA_ERR_INVALID, "unknown constraint method");
+    const int64_t n = h->spec.n;
+    LaplaceSpec sp = h->spec;
+    sp.kc = k;
+    sp.cA.assign(c ? c : nullptr, c ? c + (size_t)k * n : nullptr);
+    sp.ce.assign(e ? e : nullptr, e ? e + k : nullptr);
+    sp.cmethod = method;
+    const LaplaceSpec& prev = h->eng->spec();
+    LaplaceSpec keep = h->spec;  // previous constraints, restored if the new set is rejected
+    keep.kc = prev.kc;
+    keep.cA = prev.cA;
+    keep.ce = prev.ce;
+    keep.cmethod = prev.cmethod;
+    INLA_CUDA(cudaStreamSynchronize(h->stream));
+    h->eng.reset();
+    try {
+      h->eng.reset(new LaplaceEngine(sp, h->max_batch, h->stream));
+    } catch (...) {
+      int code = map_exception();
+      try {
+        h->eng.reset(new LaplaceEngine(keep, h->max_batch, h->stream));
+      } catch (...) {
+        h->eng.reset();
+      }
+      return code;
+    }
+    return INLA_OK;
+  } catch (...) {
+    return map_exception();
+  }
 }
 
 int inla_laplace_eval(inla_laplace* h, int B, const double* coef, const double* p1scale, int flags, double* scalars,
@@ -180,10 +272,9 @@ int inla_laplace_eval(inla_laplace* h, int B, const double* coef, const double* 
         std::memcpy(gt + 3 * T1, &R.zMx[(size_t)b * T1], sizeof(double) * T1);
       }
     }
-    if (x)
-      INLA_CUDA(cudaMemcpyAsync(x, E.d_x(), sizeof(double) * B * E.n(), cudaMemcpyDeviceToHost, E.stream()));
-    if (var)
-      INLA_CUDA(cudaMemcpyAsync(var, E.d_var(), sizeof(double) * B * E.n(), cudaMemcpyDeviceToHost, E.stream()));
+    const size_t w = sizeof(double) * E.n(), pitch = sizeof(double) * E.xstride();
+    if (x) INLA_CUDA(cudaMemcpy2DAsync(x, w, E.d_x(), pitch, w, B, cudaMemcpyDeviceToHost, E.stream()));
+    if (var) INLA_CUDA(cudaMemcpy2DAsync(var, w, E.d_var(), pitch, w, B, cudaMemcpyDeviceToHost, E.stream()));
     INLA_CUDA(cudaStreamSynchronize(E.stream()));
     return INLA_OK;
   } catch (...) {

@@ -659,10 +659,11 @@ void InlaDriver::fit(const double* theta0, const FitOptions& opt, FitResult& out
       std::vector<LaplaceOut> keep;
       evaluate(Bc, thetas.data() + (size_t)k0 * m, false, true, fk.data() + k0, nullptr, &keep);
       const LaplaceOut& R = keep.back();
-      INLA_CUDA(cudaMemcpyAsync(means.data() + (size_t)k0 * n, eng_.d_x(), sizeof(double) * Bc * n,
-                                cudaMemcpyDeviceToHost, eng_.stream()));
-      INLA_CUDA(cudaMemcpyAsync(vars.data() + (size_t)k0 * n, eng_.d_var(), sizeof(double) * Bc * n,
-                                cudaMemcpyDeviceToHost, eng_.stream()));
+      const size_t w = sizeof(double) * n, pitch = sizeof(double) * eng_.xstride();
+      INLA_CUDA(cudaMemcpy2DAsync(means.data() + (size_t)k0 * n, w, eng_.d_x(), pitch, w, Bc,
+                                  cudaMemcpyDeviceToHost, eng_.stream()));
+      INLA_CUDA(cudaMemcpy2DAsync(vars.data() + (size_t)k0 * n, w, eng_.d_var(), pitch, w, Bc,
+                                  cudaMemcpyDeviceToHost, eng_.stream()));
       INLA_CUDA(cudaStreamSynchronize(eng_.stream()));
       for (int b = 0; b < Bc; ++b) {
         const int k = k0 + b;

@@ -9,6 +9,12 @@
 // step cap 10, at most 12 halvings while the objective is non-finite,
 // convergence when max|dx| < tol or max|step| < tol, confirmation
 // refactorization at x*, mlik = loglik - x*'Qx*/2 + log|Q|/2 - log|Q_post|/2.
+//
+// Hard constraints follow the reference's Augmented method (inference.rs:819-830,
+// constraints.rs:268-353): the working prior is Q + kappa C^T C with kappa = 3.059023205018258e6,
+// held here as one more fixed component (coefficient 1) on a pattern widened by
+// the support of C^T C; the prior log-determinant takes no jitter; every Newton
+// trial point and the final mode are projected onto C x = e.
 #pragma once
 #include <memory>
 #include <vector>
@@ -31,7 +37,28 @@ struct LaplaceSpec {
   int max_iter = 200;
   double tol = 1e-5;
   int ordering = ORDER_AMD;
+  // hard linear constraints C x = e (ConstraintSpec, crates/inla_math/src/constraints.rs:16-25):
+  // kc rows of the dense row-major kc x n matrix cA, right-hand side ce (kc = 0: none)
+  int kc = 0;
+  std::vector<double> cA, ce;
+  int cmethod = 0;  // ConstraintMethodGpu
 };
+
+// How Q + kappa C^T C is held (the results are the same up to rounding):
+//  CONSTR_AUGMENTED: as the reference builds it -- kappa C^T C added on a pattern widened by
+//    its support (every constrained block becomes dense);
+//  CONSTR_BORDERED: the sparse bordered matrix M = [[Q, C^T], [C, -I/kappa]] of order n + k,
+//    whose Schur complement is Q + kappa C^T C: log|Q + kappa C^T C| = log|det M| + k log kappa,
+//    the leading n x n block of M^-1 is (Q + kappa C^T C)^-1, and the system M [x; l] = [b; 0]
+//    solves (Q + kappa C^T C) x = b. The elimination order puts, per constraint row, its
+//    latest-eliminated supported node after the k border nodes, so that the nodes eliminated
+//    before the border carry a positive definite block even when Q is intrinsic;
+//  CONSTR_AUTO: augmented while kappa C^T C adds at most 2^22 entries, else bordered.
+enum ConstraintMethodGpu : int { CONSTR_AUTO = 0, CONSTR_AUGMENTED = 1, CONSTR_BORDERED = 2 };
+
+// HARD_CONSTRAINT_KAPPA (constraints.rs:268): the literal 3.059023205018258e6, which its
+// comment calls exp(15) (that is 3.269e6); results must match the literal
+constexpr double kHardConstraintKappa = 3.059023205018258e6;
 
 enum LaplaceFlags : int { LAP_VARIANCES = 1, LAP_GRADIENT = 2, LAP_MODE = 4, LAP_NO_PRIOR_SHARING = 8 };
 
@@ -62,10 +89,14 @@ class LaplaceEngine {
   // coef: [B][ncomp] host; p1scale: [B] host (nullptr = 1).
   void eval(int B, const double* coef, const double* p1scale, int flags, LaplaceOut& out);
 
-  int64_t n() const { return spec_.n; }
+  int64_t n() const { return n_; }               // latent dimension of the caller's model
+  int64_t xstride() const { return spec_.n; }    // per-problem stride of d_x / d_var (n + k when bordered)
+  bool bordered() const { return border_; }
   int64_t nobs() const { return spec_.nobs; }
   int64_t nnz() const { return nnz_; }
-  int ncomp() const { return spec_.ncomp; }
+  int ncomp() const { return nuser_; }  // components the caller supplies coefficients for
+  int nconstr() const { return spec_.kc; }
+  const LaplaceSpec& spec() const { return spec_; }
   int family() const { return spec_.family; }
   int max_batch() const { return max_batch_; }
   const double* d_x() const { return x_.p; }      // [B][n] modes
@@ -78,8 +109,20 @@ class LaplaceEngine {
  private:
   void fill_factor(int B, bool posterior, double diag_add);
   void eval_lik(int B, const double* d_xsrc);
+  void augment_constraints();         // host, once: C, C^T, (C C^T)^-1, then one of
+  void augment_dense();               //   widen the pattern by supp(C^T C), append kappa C^T C
+  void augment_bordered();            //   border the pattern with C and -I/kappa (order n + k)
+  void project(int B, double* d_x);   // x <- x - C^T (C C^T)^-1 (C x - e) for B problems
 
   LaplaceSpec spec_;
+  int nuser_ = 0;
+  int64_t n_ = 0;        // the caller's latent dimension
+  bool border_ = false;  // CONSTR_BORDERED in use
+  std::vector<int64_t> border_perm_;  // elimination order of the bordered matrix
+  // host copies of C (CSR) for the two constructions
+  std::vector<int64_t> h_crp_;
+  std::vector<int> h_cci_;
+  std::vector<double> h_cv_;
   int max_batch_;
   cudaStream_t stream_;
   int64_t nnz_ = 0;
@@ -93,6 +136,10 @@ class LaplaceEngine {
   DBuf<double> coef_, p1s_, x_, xt_, step_, eta_, logp_, grad_, w_, dw_, var_, sig_, red_, stats_, alpha_, tmp_n_,
       tmp_o_, ldp_, gpart_, coefp_, coefall_;
   DBuf<unsigned> gtick_;  // grid-reduction partials and tickets
+  // constraints: C and C^T in CSR, e, (C C^T)^-1, residuals [B][kc], max |x_trial - x| [B]
+  DBuf<int64_t> crp_, ctp_;
+  DBuf<int> cci_, cta_;
+  DBuf<double> cv_, ctv_, ce_, cginv_, cres_, mdiff_;
   DBuf<int> bad_, stp_;
   int64_t launches_ = 0;
   std::vector<double> h_buf_;

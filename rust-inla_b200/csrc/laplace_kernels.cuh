@@ -369,12 +369,13 @@ __global__ void __launch_bounds__(256) k_trace_contract_g(int64_t nnz, int ncomp
 
 // out[b] = {max|step|, all finite ? 1 : 0}
 template <int NT>
-__global__ void __launch_bounds__(NT) k_step_stats(int n, const double* __restrict__ step, double* __restrict__ out) {
+__global__ void __launch_bounds__(NT) k_step_stats(int n, int64_t stride, const double* __restrict__ step,
+                                                  double* __restrict__ out) {
   __shared__ double red[NT];
   const int b = blockIdx.x;
   double mx = 0.0, fin = 1.0;
   for (int j = threadIdx.x; j < n; j += NT) {
-    double s = step[(int64_t)b * n + j];
+    double s = step[(int64_t)b * stride + j];
     if (!isfinite(s)) fin = 0.0;
     else mx = fmax(mx, fabs(s));
   }
@@ -383,6 +384,63 @@ __global__ void __launch_bounds__(NT) k_step_stats(int n, const double* __restri
   if (threadIdx.x == 0) {
     out[2 * b] = mx;
     out[2 * b + 1] = fin;
+  }
+}
+
+// max |a - b| over the first n entries per problem (Newton convergence on the accepted,
+// projected trial point)
+template <int NT>
+__global__ void __launch_bounds__(NT) k_max_abs_diff(int n, int64_t stride, const double* __restrict__ a,
+                                                    const double* __restrict__ c, double* __restrict__ out) {
+  __shared__ double red[NT];
+  const int b = blockIdx.x;
+  double mx = 0.0;
+  for (int j = threadIdx.x; j < n; j += NT)
+    mx = fmax(mx, fabs(a[(int64_t)b * stride + j] - c[(int64_t)b * stride + j]));
+  mx = block_max<NT>(mx, red);
+  if (threadIdx.x == 0) out[b] = mx;
+}
+
+// Constraint residual r[b][a] = (C x_b)_a - e_a, one CTA per (row a, problem b), fixed
+// summation order (constraints.rs:324-333). C in CSR: rows of ConstraintSpec.a without zeros.
+// With border > 0 it instead sets the border entry x[b][n + a] = border * (C x_b)_a, the
+// multiplier kappa C x of the bordered system (M x = [Q x + kappa C^T C x; 0]).
+template <int NT>
+__global__ void __launch_bounds__(NT) k_constr_resid(int n, int64_t stride, int k, const int64_t* __restrict__ crp,
+                                                    const int* __restrict__ cci, const double* __restrict__ cv,
+                                                    const double* __restrict__ ce, double border,
+                                                    double* __restrict__ x, double* __restrict__ r) {
+  __shared__ double red[NT];
+  const int a = blockIdx.x, b = blockIdx.y;
+  double* xb = x + (int64_t)b * stride;
+  double s = 0.0;
+  for (int64_t p = crp[a] + threadIdx.x; p < crp[a + 1]; p += NT) s += cv[p] * xb[cci[p]];
+  s = block_sum<NT>(s, red);
+  if (threadIdx.x == 0) {
+    if (border > 0.0) xb[n + a] = border * s;
+    else r[(int64_t)b * k + a] = s - ce[a];
+  }
+}
+
+// x_b <- x_b - C^T lambda_b, lambda_b = (C C^T)^-1 r_b (constraints.rs:343-351). Every CTA
+// forms lambda_b in shared memory (k doubles) from the precomputed inverse; C^T in CSR.
+__global__ void k_constr_apply(int n, int64_t stride, int k, const int64_t* __restrict__ ctp,
+                               const int* __restrict__ cta, const double* __restrict__ ctv,
+                               const double* __restrict__ ginv, const double* __restrict__ r,
+                               double* __restrict__ x) {
+  extern __shared__ double lam[];
+  const int b = blockIdx.y;
+  const double* rb = r + (int64_t)b * k;
+  for (int a = threadIdx.x; a < k; a += blockDim.x) {
+    double s = 0.0;
+    for (int j = 0; j < k; ++j) s += ginv[(int64_t)a * k + j] * rb[j];
+    lam[a] = s;
+  }
+  __syncthreads();
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    double corr = 0.0;
+    for (int64_t p = ctp[c]; p < ctp[c + 1]; ++p) corr += ctv[p] * lam[cta[p]];
+    x[(int64_t)b * stride + c] -= corr;
   }
 }
 

@@ -18,6 +18,7 @@ from . import _lib
 from ._lib import as_f64, as_i64, check, dptr, lib, lptr
 
 FAMILIES = {"gaussian": 0, "poisson": 1, "binomial": 2, "nbinomial": 3}
+CONSTRAINT_METHODS = {"auto": 0, "augmented": 1, "bordered": 2}
 
 THETA_MAP = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
                         C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p)
@@ -27,6 +28,7 @@ PRIOR_PC_PREC = 1
 PRIOR_LOGGAMMA = 2
 PRIOR_PC_SPDE = 3
 PRIOR_GAUSSIAN = 4
+PRIOR_PC_COR1 = 5
 
 
 class PriorSpec(C.Structure):
@@ -100,6 +102,26 @@ class LaplaceModel:
         self._h = h
         self.max_batch = max_batch
         self.family = family
+        self.constraints = None
+
+    def set_constraints(self, c, e=None, method="auto"):
+        """Hard constraints ``C x = e`` (``c``: k x n dense, ``e``: k, default 0) by the
+        reference's Augmented method: working prior Q + κ CᵀC with κ = 3.059023205018258e6,
+        projection of every Newton trial point and of the mode (inference.rs:804-951).
+        ``method``: "augmented" (κ CᵀC on the widened pattern, as the reference), "bordered"
+        (the sparse bordered matrix [[Q, Cᵀ], [C, -I/κ]]) or "auto". ``c=None`` removes them."""
+        if c is None:
+            check(lib().inla_laplace_set_constraints(self._h, 0, None, None, 0))
+            self.constraints = None
+            return
+        c = np.atleast_2d(as_f64(c))
+        if c.shape[1] != self.n:
+            raise ValueError(f"constraint matrix has {c.shape[1]} columns, latent dimension is {self.n}")
+        k = c.shape[0]
+        e = np.zeros(k) if e is None else as_f64(np.broadcast_to(e, (k,)))
+        meth = CONSTRAINT_METHODS[method] if isinstance(method, str) else int(method)
+        check(lib().inla_laplace_set_constraints(self._h, k, dptr(c), dptr(e), meth))
+        self.constraints = (c, e)
 
     def close(self):
         if getattr(self, "_h", None):

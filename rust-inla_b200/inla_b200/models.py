@@ -16,6 +16,13 @@ Reference behaviour restated here (inputs only; none of this is timed):
 * Besag graph Laplacian — crates/inla_stats/src/besag.rs:127-152.
 * AR1 conditional-precision form ``tau * tridiag(1, 1+rho^2, ..., 1; -rho)`` —
   crates/inla_stats/src/ar1.rs:9-69.
+* ``scale.model`` — crates/inla_math/src/design.rs:140-195.
+* Grouped effects: ``kron(Q_group, Q_main)``, group-major latent order with the
+  main index fastest — crates/inla_stats/src/structured.rs:475-540; group AR1
+  ``rho = 2 / (1 + e^-theta) - 1`` — structured.rs:348-356; per-group copies of
+  the main model's component sum-to-zero rows — structured.rs:782-807, 884-963.
+* Sum-to-zero constraint rows and block embedding —
+  crates/inla_math/src/constraints.rs:49-68, 111-149.
 """
 from __future__ import annotations
 
@@ -314,3 +321,217 @@ def make_spde_problem(nx: int = 200, n_obs: int = 20_000, seed: int = SEED_BASE 
              "log_kappa": float(np.log(kappa)), "x": x}
     return SpdeProblem(model=model, a=a, y=y, verts=verts, tris=tris, truth=truth,
                        theta_init=np.zeros(3))
+
+
+# ---------------------------------------------------------------------------
+# intrinsic models: scale.model and constraints
+# ---------------------------------------------------------------------------
+
+def scale_model(r: sp.spmatrix):
+    """``scale_model_csc`` (design.rs:150-195): ``fac = exp(mean(log(diag(ginv(R)))))``
+    over the positive finite entries, eigenvalues above ``sqrt(eps) * max(max_lam, 1)``
+    kept; returns ``(fac * R, fac)``. (The reference diagonalizes by Jacobi sweeps, here
+    by LAPACK: the factor agrees to rounding.)"""
+    n = r.shape[0]
+    if n == 1:
+        return sp.identity(1, format="csc"), 1.0
+    lam, v = np.linalg.eigh(np.asarray(sp.csr_matrix(r).todense()))
+    max_lam = max(abs(max(float(lam.max()), 0.0)), 1.0)
+    tol = np.sqrt(np.finfo(np.float64).eps) * max_lam
+    keep = lam > tol
+    d = (v[:, keep] ** 2) @ (1.0 / lam[keep])
+    ok = (d > 0.0) & np.isfinite(d)
+    if not ok.any():
+        raise ValueError("scale_model: ginv has no positive diagonal")
+    fac = float(np.exp(np.mean(np.log(d[ok]))))
+    return (fac * sp.csc_matrix(r)).tocsc(), fac
+
+
+def sum_to_zero_constraint(n: int, k: int = 1):
+    """``sum_to_zero_constraint`` (constraints.rs:111-149): row 0 = 1/sqrt(n); row 1 (k=2)
+    the centred index scaled to unit norm. Returns ``(C [k x n], e [k])``."""
+    if n <= 0 or k not in (1, 2):
+        raise ValueError("sum_to_zero_constraint: n > 0 and k in {1, 2}")
+    c = np.zeros((k, n))
+    c[0] = 1.0 / np.sqrt(n)
+    if k == 2:
+        v = np.arange(n, dtype=float) - (n - 1) / 2.0
+        scale = np.sqrt(np.sum(v * v))
+        if scale < 1e-14:
+            raise ValueError("sum_to_zero_constraint: degenerate linear row")
+        c[1] = v / scale
+    return c, np.zeros(k)
+
+
+def plane_constraint_2d(nrow: int, ncol: int):
+    """``plane_constraint_2d`` (constraints.rs:219-266) for a column-major lattice
+    (``node = j * nrow + i``): constant, row trend, column trend, each unit norm."""
+    if nrow <= 0 or ncol <= 0:
+        raise ValueError("plane_constraint_2d: nrow and ncol must be > 0")
+    n = nrow * ncol
+    j, i = np.meshgrid(np.arange(ncol), np.arange(nrow), indexing="ij")
+    vi = (i.ravel() - (nrow - 1) / 2.0).astype(float)
+    vj = (j.ravel() - (ncol - 1) / 2.0).astype(float)
+    si, sj = np.sqrt(np.sum(vi * vi)), np.sqrt(np.sum(vj * vj))
+    if si < 1e-14 or sj < 1e-14:
+        raise ValueError("plane_constraint_2d: degenerate row/col trend")
+    c = np.stack([np.full(n, 1.0 / np.sqrt(n)), vi / si, vj / sj])
+    return c, np.zeros(3)
+
+
+def embed_constraint(c: np.ndarray, full_n: int, offset: int) -> np.ndarray:
+    """``ConstraintSpec::embed`` (constraints.rs:49-68): place the block at ``offset``."""
+    c = np.atleast_2d(c)
+    if offset + c.shape[1] > full_n:
+        raise ValueError("embed: block exceeds full dimension")
+    out = np.zeros((c.shape[0], full_n))
+    out[:, offset:offset + c.shape[1]] = c
+    return out
+
+
+@dataclass
+class BesagProblem:
+    model: LatentModel
+    a: sp.csr_matrix      # n_obs x n projector [1 | x | I]
+    y: np.ndarray
+    constraint: tuple     # (C [1 x n], e [1]): sum-to-zero on the region block
+    scale: float          # scale.model factor of the Besag structure
+    truth: dict
+
+
+BESAG_FIXED_PREC = 1e-4  # precision of the intercept and covariate effects
+
+
+def make_besag_problem(nr: int = 30, nc: int = 30, seed: int = SEED_BASE + 1, tau_true: float = 2.0,
+                       beta0: float = 0.5, beta1: float = 0.3) -> BesagProblem:
+    """Poisson GLMM ``y ~ 1 + x + f(region, besag, scale.model)`` on an ``nr x nc`` rook
+    lattice with a sum-to-zero constraint on the Besag block.
+
+    Latent layout [intercept, x-effect, region (nr*nc)] (fixed effects first, precision
+    1e-4); ``Q(theta) = M0 + exp(theta) M1`` with ``M0 = diag(1e-4, 1e-4, 0, ...)`` and
+    ``M1 = blockdiag(0, 0, fac * R)``. Draw order: covariate x (n_region), Besag
+    innovations (n_region - 1, on the scaled structure's non-null eigenvectors, tau_true),
+    Poisson counts.
+    """
+    rng = np.random.default_rng(seed)
+    adj = lattice_adjacency(nr, nc)
+    r = besag_structure(adj)
+    rs, fac = scale_model(r)
+    nreg = nr * nc
+    n = nreg + 2
+    x = rng.standard_normal(nreg)
+    lam, v = np.linalg.eigh(np.asarray(rs.todense()))
+    tol = np.sqrt(np.finfo(np.float64).eps) * max(float(lam.max()), 1.0)
+    keep = lam > tol
+    z = rng.standard_normal(int(keep.sum()))
+    u = v[:, keep] @ (z / np.sqrt(tau_true * lam[keep]))
+    eta = beta0 + beta1 * x + u
+    y = rng.poisson(np.exp(eta)).astype(float)
+    rows = np.repeat(np.arange(nreg), 3)
+    cols = np.stack([np.zeros(nreg, dtype=int), np.ones(nreg, dtype=int), 2 + np.arange(nreg)], axis=1).ravel()
+    vals = np.stack([np.ones(nreg), x, np.ones(nreg)], axis=1).ravel()
+    a = sp.csr_matrix((vals, (rows, cols)), shape=(nreg, n))
+    d0 = np.zeros(n)
+    d0[:2] = BESAG_FIXED_PREC
+    m0 = sp.diags(d0).tocsc()
+    m1 = sp.block_diag([sp.csc_matrix((2, 2)), rs]).tocsc()
+    ata = (a.T @ a).tocsc()
+    model = build_latent(n, [m0, m1], "besag", extra_pattern=[ata], info={"nr": nr, "nc": nc})
+    c, e = sum_to_zero_constraint(nreg, 1)
+    cons = (embed_constraint(c, n, 2), e)
+    truth = {"log_tau": float(np.log(tau_true)), "u": u, "beta": (beta0, beta1), "x": x}
+    return BesagProblem(model=model, a=a, y=y, constraint=cons, scale=fac, truth=truth)
+
+
+def besag_coefs(log_tau: float):
+    """Coefficients of :func:`make_besag_problem`'s components and d/d log_tau."""
+    t = float(np.exp(log_tau))
+    return np.array([1.0, t]), np.array([[0.0, t]])
+
+
+@dataclass
+class GroupProblem:
+    model: LatentModel
+    a: sp.csr_matrix      # n_obs x n projector [1 | I | I]
+    y: np.ndarray
+    ntrials: float
+    constraint: tuple     # (C [T x n], e [T]): sum-to-zero of the spatial block per time
+    dims: tuple           # (n_space, T)
+    truth: dict
+
+
+def group_constraint(n_space: int, T: int, offset: int, n: int):
+    """``grouped_constraints`` (structured.rs:884-963) for a connected Besag main model and an
+    AR1 group model (no constraint of its own): row t is 1/sqrt(n_space) on time slice t."""
+    c = np.zeros((T, n))
+    w = 1.0 / np.sqrt(n_space)
+    for t in range(T):
+        c[t, offset + t * n_space:offset + (t + 1) * n_space] = w
+    return c, np.zeros(T)
+
+
+def make_group_problem(nr: int = 50, nc: int = 50, T: int = 40, seed: int = SEED_BASE + 3, rho: float = 0.8,
+                       tau_b: float = 1.0, tau_g: float = 1.0, tau_iid: float = 4.0, beta0: float = 0.0,
+                       ntrials: float = 10.0) -> GroupProblem:
+    """Space-time group model: Besag on an ``nr x nc`` rook lattice grouped by AR1 over ``T``
+    times, plus iid and an intercept; binomial likelihood with ``ntrials`` trials, one
+    observation per space-time cell.
+
+    Latent layout [intercept, group effect (T * n_space, group-major), iid (T * n_space)];
+    ``Q(theta) = M_int + tau_b tau_g (K0 + rho^2 K1 - rho K2) + tau_iid M_iid`` with
+    ``K_i = kron(AR1 piece_i, R)``. theta = [log tau_b, log tau_g, logit-type rho, log tau_iid].
+    Draw order: per-eigenvector AR1 paths of the spatial field (n_space - 1 paths of length
+    T), iid effects, binomial counts.
+    """
+    rng = np.random.default_rng(seed)
+    r = besag_structure(lattice_adjacency(nr, nc))
+    ns = nr * nc
+    nst = ns * T
+    n = 1 + 2 * nst
+    lam, v = np.linalg.eigh(np.asarray(r.todense()))
+    keep = lam > np.sqrt(np.finfo(np.float64).eps) * max(float(lam.max()), 1.0)
+    lk, vk = lam[keep], v[:, keep]
+    z = np.zeros((T, len(lk)))
+    z[0] = rng.standard_normal(len(lk)) / np.sqrt(1.0 - rho * rho)
+    for t in range(1, T):
+        z[t] = rho * z[t - 1] + rng.standard_normal(len(lk))
+    u = (z / np.sqrt(tau_b * tau_g * lk)) @ vk.T          # (T, ns), row t = time slice t
+    w = rng.standard_normal(nst) / np.sqrt(tau_iid)
+    eta = beta0 + u.ravel() + w
+    y = rng.binomial(int(ntrials), 1.0 / (1.0 + np.exp(-eta))).astype(float)
+    rows = np.repeat(np.arange(nst), 3)
+    cols = np.stack([np.zeros(nst, dtype=np.int64), 1 + np.arange(nst), 1 + nst + np.arange(nst)], axis=1).ravel()
+    a = sp.csr_matrix((np.ones(3 * nst), (rows, cols)), shape=(nst, n))
+    m0, m1, m2 = ar1_components(T)
+    z1 = sp.csc_matrix((1, 1))
+    zst = sp.csc_matrix((nst, nst))
+    ks = [sp.block_diag([z1, sp.kron(mi, r, format="csc"), zst]).tocsc() for mi in (m0, m1, m2)]
+    dint = np.zeros(n)
+    dint[0] = BESAG_FIXED_PREC
+    m_int = sp.diags(dint).tocsc()
+    m_iid = sp.diags(np.r_[np.zeros(1 + nst), np.ones(nst)]).tocsc()
+    ata = (a.T @ a).tocsc()
+    model = build_latent(n, [m_int] + ks + [m_iid], "besag_x_ar1", extra_pattern=[ata],
+                         info={"nr": nr, "nc": nc, "T": T})
+    cons = group_constraint(ns, T, 1, n)
+    truth = {"rho": rho, "tau_b": tau_b, "tau_g": tau_g, "tau_iid": tau_iid, "u": u, "w": w}
+    return GroupProblem(model=model, a=a, y=y, ntrials=ntrials, constraint=cons, dims=(ns, T), truth=truth)
+
+
+def group_coefs(theta):
+    """Coefficients of :func:`make_group_problem`'s components and their theta-derivatives
+    (rho clamped to +-0.999 as structured.rs:353 does; the derivative is then 0)."""
+    tb, tg, tr, ti = (float(v) for v in theta)
+    s = np.exp(tb + tg)
+    rho_raw = 2.0 / (1.0 + np.exp(-tr)) - 1.0
+    rho = float(np.clip(rho_raw, -0.999, 0.999))
+    drho = (1.0 - rho_raw * rho_raw) / 2.0 if rho == rho_raw else 0.0
+    tau_iid = np.exp(ti)
+    c = np.array([1.0, s, s * rho * rho, -s * rho, tau_iid])
+    dc = np.zeros((4, 5))
+    dc[0, 1:4] = c[1:4]
+    dc[1, 1:4] = c[1:4]
+    dc[2, 2] = s * 2.0 * rho * drho
+    dc[2, 3] = -s * drho
+    dc[3, 4] = tau_iid
+    return c, dc
