@@ -202,6 +202,29 @@ int inla_laplace_eval(inla_laplace* h, int B, const double* coef, const double* 
                       double* scalars, double* x, double* var, double* grad_terms);
 
 /* ------------------------------------------------------------------------
+ * Independent models of uneven size in one engine (no reference counterpart:
+ * the reference fits each model on its own). G models are given as one
+ * block-diagonal latent field: model g owns latent nodes [lat_off[g],
+ * lat_off[g+1]) and observations [obs_off[g], obs_off[g+1]); the pattern,
+ * components and the projector A (CSR) must not couple models. One symbolic
+ * analysis (an elimination forest with one tree per model, each model's block
+ * ordered on its own) serves every evaluation; each level launch works on the
+ * fronts of all models. Per theta-set and model the evaluation is
+ * find_latent_mode_a_with_solver (inference.rs:776-975) with that model's
+ * coefficients and family scale.
+ * ---------------------------------------------------------------------- */
+typedef struct inla_multi inla_multi;
+int inla_multi_create(int G, const int64_t* lat_off, const int64_t* obs_off, const int64_t* colptr,
+                      const int64_t* rowidx, int ncomp, const double* comp, const int64_t* a_rowptr,
+                      const int64_t* a_colidx, const double* a_vals, int family, const double* y, const double* p1,
+                      const double* p2, int ordering, int max_batch, inla_multi** out);
+void inla_multi_free(inla_multi* h);
+/* coef: [B][G][ncomp]; p1scale: [B][G] or NULL; scalars: [B][G][8] (layout of
+ * inla_laplace_eval); x, var: [B][n] or NULL; grad_terms: [B][G][4][ncomp+1] or NULL. */
+int inla_multi_eval(inla_multi* h, int B, const double* coef, const double* p1scale, int flags, double* scalars,
+                    double* x, double* var, double* grad_terms);
+
+/* ------------------------------------------------------------------------
  * Hyperpriors (crates/inla_stats/src/priors.rs): log pi(theta) and gradient.
  * ---------------------------------------------------------------------- */
 enum {

@@ -1,0 +1,111 @@
+// extern "C" boundary of the multi-model Laplace engine (independent models of uneven size).
+#include <cstring>
+#include <memory>
+
+#include "capi_common.hpp"
+#include "inla_b200.h"
+#include "multi.hpp"
+
+using namespace inla;
+
+struct inla_multi {
+  cudaStream_t stream = nullptr;
+  std::unique_ptr<MultiLaplace> eng;
+};
+
+extern "C" {
+
+int inla_multi_create(int G, const int64_t* lat_off, const int64_t* obs_off, const int64_t* colptr,
+                      const int64_t* rowidx, int ncomp, const double* comp, const int64_t* a_rowptr,
+                      const int64_t* a_colidx, const double* a_vals, int family, const double* y, const double* p1,
+                      const double* p2, int ordering, int max_batch, inla_multi** out) {
+  inla_multi* h = nullptr;
+  try {
+    if (!out || G < 1 || !lat_off || !obs_off || !colptr || !rowidx || !comp || !a_rowptr || max_batch < 1)
+      return fail(INLA_ERR_INVALID, "invalid argument");
+    MultiSpec sp;
+    sp.G = G;
+    sp.lat_off.assign(lat_off, lat_off + G + 1);
+    sp.obs_off.assign(obs_off, obs_off + G + 1);
+    sp.n = lat_off[G];
+    sp.nobs = obs_off[G];
+    if (sp.n <= 0 || sp.nobs < 0) return fail(INLA_ERR_INVALID, "invalid offsets");
+    if (ncomp < 1 || ncomp > 8) return fail(INLA_ERR_INVALID, "1..8 precision components supported");
+    if (ordering < 0 || ordering > INLA_ORDER_ND || ordering == INLA_ORDER_CUSTOM)
+      return fail(INLA_ERR_INVALID, "unsupported ordering");
+    if (sp.nobs > 0 && (!y || !a_colidx || !a_vals)) return fail(INLA_ERR_INVALID, "null observation arrays");
+    sp.colptr.assign(colptr, colptr + sp.n + 1);
+    sp.rowidx.assign(rowidx, rowidx + colptr[sp.n]);
+    sp.ncomp = ncomp;
+    sp.comp.assign(comp, comp + (size_t)ncomp * colptr[sp.n]);
+    sp.acp.assign(a_rowptr, a_rowptr + sp.nobs + 1);
+    if (sp.nobs > 0) {
+      sp.aci.assign(a_colidx, a_colidx + a_rowptr[sp.nobs]);
+      sp.av.assign(a_vals, a_vals + a_rowptr[sp.nobs]);
+      sp.y.assign(y, y + sp.nobs);
+      if (p1) sp.p1.assign(p1, p1 + sp.nobs);
+      if (p2) sp.p2.assign(p2, p2 + sp.nobs);
+    }
+    sp.family = family;
+    sp.ordering = ordering;
+    h = new inla_multi();
+    INLA_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->eng.reset(new MultiLaplace(sp, max_batch, h->stream));
+    *out = h;
+    return INLA_OK;
+  } catch (...) {
+    int code = map_exception();
+    inla_multi_free(h);
+    return code;
+  }
+}
+
+void inla_multi_free(inla_multi* h) {
+  if (!h) return;
+  h->eng.reset();
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+int inla_multi_eval(inla_multi* h, int B, const double* coef, const double* p1scale, int flags, double* scalars,
+                    double* x, double* var, double* grad_terms) {
+  try {
+    if (!h || !h->eng) return fail(INLA_ERR_INVALID, "null handle");
+    MultiLaplace& E = *h->eng;
+    if (B < 1 || B > E.max_batch()) return fail(INLA_ERR_DIM_MISMATCH, "batch size out of range");
+    if (!coef || !scalars) return fail(INLA_ERR_INVALID, "null coefficient or output array");
+    if (var) flags |= LAP_VARIANCES;
+    MultiOut R;
+    const int64_t before = E.launches();
+    E.eval(B, coef, p1scale, flags, R);
+    g_launches += E.launches() - before;
+    const size_t BG = (size_t)B * E.G();
+    const int T1 = E.ncomp() + 1;
+    for (size_t q = 0; q < BG; ++q) {
+      double* s = scalars + q * 8;
+      s[0] = R.mlik[q];
+      s[1] = R.ld_prior[q];
+      s[2] = R.ld_post[q];
+      s[3] = R.loglik[q];
+      s[4] = R.quad[q];
+      s[5] = R.iters[q];
+      s[6] = R.status[q];
+      s[7] = R.dll[q];
+      if (grad_terms) {
+        double* gt = grad_terms + q * 4 * T1;
+        std::memcpy(gt, &R.trP[q * T1], sizeof(double) * T1);
+        std::memcpy(gt + T1, &R.trQ[q * T1], sizeof(double) * T1);
+        std::memcpy(gt + 2 * T1, &R.xMx[q * T1], sizeof(double) * T1);
+        std::memcpy(gt + 3 * T1, &R.zMx[q * T1], sizeof(double) * T1);
+      }
+    }
+    if (x) INLA_CUDA(cudaMemcpyAsync(x, E.d_x(), sizeof(double) * B * E.n(), cudaMemcpyDeviceToHost, E.stream()));
+    if (var) INLA_CUDA(cudaMemcpyAsync(var, E.d_var(), sizeof(double) * B * E.n(), cudaMemcpyDeviceToHost, E.stream()));
+    INLA_CUDA(cudaStreamSynchronize(E.stream()));
+    return INLA_OK;
+  } catch (...) {
+    return map_exception();
+  }
+}
+
+}  // extern "C"

@@ -378,7 +378,7 @@ void GpuFactor::factor_values(const double* d_vals, int B) {
 void GpuFactor::factor_model(int ncomp, const double* d_comp, const double* d_coef, double diag_add,
                              const unsigned char* d_pdiag, const int* d_cptr, const int* d_cobs,
                              const double* d_cprod, const double* d_w, int64_t wstride, int B, int nprior,
-                             double diag_add_post) {
+                             double diag_add_post, const int* d_pseg, int nseg) {
   if (B < 1 || B > max_batch_) throw std::runtime_error("batch size out of range");
   if (nprior < 0 || nprior > B) throw std::runtime_error("prior count out of range");
   if (ncomp < 1 || ncomp > 8) throw std::runtime_error("1..8 precision components supported");
@@ -387,11 +387,12 @@ void GpuFactor::factor_model(int ncomp, const double* d_comp, const double* d_co
   std::memcpy(&dpbits, &diag_add_post, sizeof(dpbits));
   launch_cached({2, B, ncomp, (int64_t)(uintptr_t)d_comp, (int64_t)(uintptr_t)d_coef, dbits,
                  (int64_t)(uintptr_t)d_pdiag, (int64_t)(uintptr_t)d_cptr, (int64_t)(uintptr_t)d_cobs,
-                 (int64_t)(uintptr_t)d_cprod, (int64_t)(uintptr_t)d_w, wstride, nprior, dpbits},
+                 (int64_t)(uintptr_t)d_cprod, (int64_t)(uintptr_t)d_w, wstride, nprior, dpbits,
+                 (int64_t)(uintptr_t)d_pseg, nseg},
                 [&] {
                   k_fill_panels_model<<<dim3(nfillm_), 256, 0, stream_>>>(
                       ds_, d_csnm_.p, ntot_, d_pmap_.p, ncomp, d_comp, nnz_, d_coef, diag_add, d_pdiag, d_cptr, d_cobs,
-                      d_cprod, d_w, wstride, B, nprior, diag_add_post, F_.p, ftotal_);
+                      d_cprod, d_w, wstride, B, nprior, diag_add_post, d_pseg, nseg, F_.p, ftotal_);
                   ++launches_;
                   run_factor_levels(B);
                 });

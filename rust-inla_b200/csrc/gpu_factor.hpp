@@ -90,7 +90,10 @@ class GpuFactor {
   // diag_add_post and the weights w + (b - nprior) * wstride (if d_w).
   void factor_model(int ncomp, const double* d_comp, const double* d_coef, double diag_add,
                     const unsigned char* d_pdiag, const int* d_cptr, const int* d_cobs, const double* d_cprod,
-                    const double* d_w, int64_t wstride, int B, int nprior = 0, double diag_add_post = 0.0);
+                    const double* d_w, int64_t wstride, int B, int nprior = 0, double diag_add_post = 0.0,
+                    const int* d_pseg = nullptr, int nseg = 1);
+  // Device view of the symbolic analysis (pivot offsets, permutation, ...).
+  const DevSym& dev_sym() const { return ds_; }
   // Front offset of every input entry's lower twin (both triangles), for
   // reading Sigma / L on the full pattern.
   const int64_t* d_spos_full() const { return spos_full_.p; }

@@ -21,28 +21,6 @@ inline unsigned grid1(int64_t n, int threads = 256, int cap = 2048) {
 inline unsigned nchunks(int64_t len, int per_cta) { return (unsigned)std::max(1, cdiv(len, per_cta)); }
 }  // namespace
 
-// u[b][j] = sum_a A[a,j] v[b][a]   (A^T in CSR)
-__global__ void k_spmv_at(int n, const int64_t* __restrict__ atp, const int* __restrict__ ati,
-                          const double* __restrict__ atv, int64_t nobs, const double* __restrict__ v,
-                          double* __restrict__ u) {
-  const int b = blockIdx.y;
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-    double s = 0.0;
-    if (atp) {
-      for (int64_t a = atp[j]; a < atp[j + 1]; ++a) s += atv[a] * v[(int64_t)b * nobs + ati[a]];
-    } else {
-      s = v[(int64_t)b * nobs + j];
-    }
-    u[(int64_t)b * n + j] = s;
-  }
-}
-
-__global__ void k_mul(int64_t len, const double* a, const double* b, double* c) {  // c may alias a
-  const int bb = blockIdx.y;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x)
-    c[(int64_t)bb * len + i] = a[(int64_t)bb * len + i] * b[(int64_t)bb * len + i];
-}
-
 LaplaceEngine::LaplaceEngine(const LaplaceSpec& spec, int max_batch, cudaStream_t stream)
     : spec_(spec), max_batch_(max_batch), stream_(stream) {
   if (spec_.n <= 0 || (int64_t)spec_.colptr.size() != spec_.n + 1) throw std::runtime_error("laplace: invalid pattern");
@@ -461,17 +439,17 @@ void LaplaceEngine::augment_bordered() {
   border_ = true;
 }
 
-void LaplaceEngine::project(int B, double* d_x) {
+void LaplaceEngine::project(int B, double* d_x, bool final) {
   const int k = spec_.kc;
   if (k == 0) return;
-  k_constr_resid<256><<<dim3(k, B), 256, 0, stream_>>>((int)n_, spec_.n, k, crp_.p, cci_.p, cv_.p, ce_.p, 0.0,
+  k_constr_resid<256><<<dim3(k, B), 256, 0, stream_>>>((int)n_, spec_.n, k, crp_.p, cci_.p, cv_.p, ce_.p, 0, 0.0,
                                                        d_x, cres_.p);
   k_constr_apply<<<dim3(grid1(n_, 256, 2 * 148), B), 256, sizeof(double) * k, stream_>>>(
       (int)n_, spec_.n, k, ctp_.p, cta_.p, ctv_.p, cginv_.p, cres_.p, d_x);
   launches_ += 2;
-  if (border_) {  // multiplier kappa C x of the projected point
-    k_constr_resid<256><<<dim3(k, B), 256, 0, stream_>>>((int)n_, spec_.n, k, crp_.p, cci_.p, cv_.p, ce_.p,
-                                                         kHardConstraintKappa, d_x, cres_.p);
+  if (border_) {
+    k_constr_resid<256><<<dim3(k, B), 256, 0, stream_>>>((int)n_, spec_.n, k, crp_.p, cci_.p, cv_.p, ce_.p, 1,
+                                                         final ? kHardConstraintKappa : 0.0, d_x, cres_.p);
     ++launches_;
   }
 }
@@ -645,7 +623,7 @@ void LaplaceEngine::eval(int B, const double* coef, const double* p1scale, int f
     k_step_stats<256><<<B, 256, 0, stream_>>>((int)n_, n, step_.p, stats_.p);
     launches_ += 2;
     INLA_CUDA(cudaMemcpyAsync(x_.p, step_.p, sizeof(double) * B * n, cudaMemcpyDeviceToDevice, stream_));
-    project(B, x_.p);  // inference.rs:867-869
+    project(B, x_.p, true);  // inference.rs:867-869
     fetch();
     for (int b = 0; b < B; ++b) {
       R.iters[b] = 1;
@@ -732,7 +710,7 @@ void LaplaceEngine::eval(int B, const double* coef, const double* p1scale, int f
     // confirmation refactorization at x* (inference.rs:923-937)
     eval_lik(B, x_.p);
     fill_factor(B, true, 0.0);
-    project(B, x_.p);  // inference.rs:949-951
+    project(B, x_.p, true);  // inference.rs:949-951
   }
 
   // ---- marginal likelihood pieces (inference.rs:953-972) ------------------------

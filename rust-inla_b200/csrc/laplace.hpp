@@ -112,7 +112,11 @@ class LaplaceEngine {
   void augment_constraints();         // host, once: C, C^T, (C C^T)^-1, then one of
   void augment_dense();               //   widen the pattern by supp(C^T C), append kappa C^T C
   void augment_bordered();            //   border the pattern with C and -I/kappa (order n + k)
-  void project(int B, double* d_x);   // x <- x - C^T (C C^T)^-1 (C x - e) for B problems
+  // x <- x - C^T (C C^T)^-1 (C x - e) for B problems; bordered, the multiplier entries are set to
+  // kappa C x when `final` (the mode, whose x^T M x is then x^T (Q + kappa C^T C) x) and to 0
+  // otherwise (Newton iterates: the right-hand side b - M x is then [A^T g - Q x; -C x] and the
+  // solve returns the new multiplier directly, with no kappa-sized terms in the right-hand side)
+  void project(int B, double* d_x, bool final = false);
 
   LaplaceSpec spec_;
   int nuser_ = 0;

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 namespace inla {
+namespace {  // each including translation unit gets its own copies of the kernels
 
 enum Family : int { FAM_GAUSSIAN = 0, FAM_POISSON = 1, FAM_BINOMIAL = 2, FAM_NBINOMIAL = 3 };
 
@@ -186,6 +187,28 @@ __global__ void k_newton_rhs(int n, int ncomp, const int64_t* __restrict__ qcp, 
     }
     rhs[(int64_t)b * n + j] = s - qx;
   }
+}
+
+// u[b][j] = sum_a A[a,j] v[b][a]   (A^T in CSR)
+__global__ void k_spmv_at(int n, const int64_t* __restrict__ atp, const int* __restrict__ ati,
+                          const double* __restrict__ atv, int64_t nobs, const double* __restrict__ v,
+                          double* __restrict__ u) {
+  const int b = blockIdx.y;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    if (atp) {
+      for (int64_t a = atp[j]; a < atp[j + 1]; ++a) s += atv[a] * v[(int64_t)b * nobs + ati[a]];
+    } else {
+      s = v[(int64_t)b * nobs + j];
+    }
+    u[(int64_t)b * n + j] = s;
+  }
+}
+
+__global__ void k_mul(int64_t len, const double* a, const double* b, double* c) {  // c may alias a
+  const int bb = blockIdx.y;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x)
+    c[(int64_t)bb * len + i] = a[(int64_t)bb * len + i] * b[(int64_t)bb * len + i];
 }
 
 // Newton update with the reference's step cap: x_trial = x + alpha step.
@@ -403,12 +426,13 @@ __global__ void __launch_bounds__(NT) k_max_abs_diff(int n, int64_t stride, cons
 
 // Constraint residual r[b][a] = (C x_b)_a - e_a, one CTA per (row a, problem b), fixed
 // summation order (constraints.rs:324-333). C in CSR: rows of ConstraintSpec.a without zeros.
-// With border > 0 it instead sets the border entry x[b][n + a] = border * (C x_b)_a, the
-// multiplier kappa C x of the bordered system (M x = [Q x + kappa C^T C x; 0]).
+// With set_border it instead sets the border entry x[b][n + a] = border * (C x_b)_a of a
+// bordered system: border = kappa gives the multiplier kappa C x (M x = [Q x + kappa C^T C x;
+// 0]), border = 0 clears it.
 template <int NT>
 __global__ void __launch_bounds__(NT) k_constr_resid(int n, int64_t stride, int k, const int64_t* __restrict__ crp,
                                                     const int* __restrict__ cci, const double* __restrict__ cv,
-                                                    const double* __restrict__ ce, double border,
+                                                    const double* __restrict__ ce, int set_border, double border,
                                                     double* __restrict__ x, double* __restrict__ r) {
   __shared__ double red[NT];
   const int a = blockIdx.x, b = blockIdx.y;
@@ -417,7 +441,7 @@ __global__ void __launch_bounds__(NT) k_constr_resid(int n, int64_t stride, int 
   for (int64_t p = crp[a] + threadIdx.x; p < crp[a + 1]; p += NT) s += cv[p] * xb[cci[p]];
   s = block_sum<NT>(s, red);
   if (threadIdx.x == 0) {
-    if (border > 0.0) xb[n + a] = border * s;
+    if (set_border) xb[n + a] = border * s;
     else r[(int64_t)b * k + a] = s - ce[a];
   }
 }
@@ -540,4 +564,5 @@ __global__ void k_predictor_var(int64_t nobs, const int64_t* __restrict__ acp, c
   }
 }
 
+}  // namespace
 }  // namespace inla

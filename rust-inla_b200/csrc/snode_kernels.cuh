@@ -84,7 +84,8 @@ __global__ void __launch_bounds__(256) k_fill_panels(DevSym S, const int* __rest
 // precisions (diag_add, no observation term); problems [nprior, B) add
 // diag_add_post and take their weights from w + (b - nprior) * wstride (if w).
 // One thread per panel entry fills it for all B problems, so the entry's pattern
-// data is read once.
+// data is read once. With pseg (independent models held block-diagonally) the
+// coefficients are per model: coef[(b * nseg + pseg[p]) * ncomp + t].
 constexpr int kFillModelChunk = 512;  // 256 threads x 2 entries
 __global__ void __launch_bounds__(256) k_fill_panels_model(DevSym S, const int* __restrict__ csn, int64_t ntot,
                                                            const int* __restrict__ pmap, int ncomp,
@@ -95,6 +96,7 @@ __global__ void __launch_bounds__(256) k_fill_panels_model(DevSym S, const int* 
                                                            const double* __restrict__ cprod,
                                                            const double* __restrict__ w, int64_t wstride, int B,
                                                            int nprior, double diag_add_post,
+                                                           const int* __restrict__ pseg, int nseg,
                                                            double* __restrict__ F, int64_t fstride) {
   const int lo = csn[blockIdx.x], hi = csn[blockIdx.x + 1];
 #pragma unroll
@@ -113,8 +115,9 @@ __global__ void __launch_bounds__(256) k_fill_panels_model(DevSym S, const int* 
     for (int t = 0; t < 8; ++t) cv[t] = t < ncomp ? comp[(int64_t)t * nnz + p] : 0.0;
     const bool isdiag = pdiag[p] != 0;
     const int q0 = cptr[p], q1 = cptr[p + 1];
+    const int sg = pseg ? pseg[p] : 0;
     for (int b = 0; b < B; ++b) {
-      const double* cb = coef + (int64_t)b * ncomp;
+      const double* cb = coef + ((int64_t)b * nseg + sg) * ncomp;
       double v = isdiag ? (b < nprior ? diag_add : diag_add_post) : 0.0;
 #pragma unroll
       for (int t = 0; t < 8; ++t)

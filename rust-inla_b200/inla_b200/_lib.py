@@ -96,6 +96,10 @@ SIGNATURES = [
                                       C.c_int, C.POINTER(P)]),
     ("inla_laplace_free", None, [P]),
     ("inla_laplace_set_constraints", C.c_int, [P, C.c_int, DP, DP, C.c_int]),
+    ("inla_multi_create", C.c_int, [C.c_int, LP, LP, LP, LP, C.c_int, DP, LP, LP, DP, C.c_int, DP, DP, DP,
+                                    C.c_int, C.c_int, C.POINTER(P)]),
+    ("inla_multi_free", None, [P]),
+    ("inla_multi_eval", C.c_int, [P, C.c_int, DP, DP, C.c_int, DP, DP, DP, DP]),
     ("inla_laplace_eval", C.c_int, [P, C.c_int, DP, DP, C.c_int, DP, DP, DP, DP]),
     ("inla_prior_log_density", C.c_double, [P, C.c_int, DP, C.c_int, DP]),
     ("inla_log_prior_set", C.c_double, [DP, C.c_int, DP, P]),

@@ -535,3 +535,75 @@ def group_coefs(theta):
     dc[2, 3] = -s * drho
     dc[3, 4] = tau_iid
     return c, dc
+
+
+@dataclass
+class MultiProblem:
+    models: list          # LatentModel per model: [intercept, AR1 (n_k), iid (n_k)]
+    a: list               # projectors [1 | I | I] (n_k x (2 n_k + 1))
+    y: list
+    truth: dict
+
+
+def ar1_iid_model(nk: int) -> tuple:
+    """Latent [intercept, AR1 (nk), iid (nk)] with components [M_int, K0, K1, K2, M_iid]
+    (AR1 pieces of ar1_components) and the projector [1 | I | I]."""
+    n = 1 + 2 * nk
+    m0, m1, m2 = ar1_components(nk)
+    z1, zk = sp.csc_matrix((1, 1)), sp.csc_matrix((nk, nk))
+    ks = [sp.block_diag([z1, mi, zk]).tocsc() for mi in (m0, m1, m2)]
+    d = np.zeros(n)
+    d[0] = BESAG_FIXED_PREC
+    m_int = sp.diags(d).tocsc()
+    m_iid = sp.diags(np.r_[np.zeros(1 + nk), np.ones(nk)]).tocsc()
+    rows = np.repeat(np.arange(nk), 3)
+    cols = np.stack([np.zeros(nk, dtype=np.int64), 1 + np.arange(nk), 1 + nk + np.arange(nk)], axis=1).ravel()
+    a = sp.csr_matrix((np.ones(3 * nk), (rows, cols)), shape=(nk, n))
+    model = build_latent(n, [m_int] + ks + [m_iid], "ar1_iid", extra_pattern=[(a.T @ a).tocsc()], info={"nk": nk})
+    return model, a
+
+
+def make_multi_problem(G: int = 512, seed: int = SEED_BASE + 4, n_lo: int = 200, n_hi: int = 5000,
+                       tau_iid: float = 10.0, beta0: float = 0.5) -> MultiProblem:
+    """Uneven batch of independent Poisson models, each AR1(n_k) + iid(n_k) + intercept with
+    n_obs = n_k: n_k = floor(exp(U(ln n_lo, ln n_hi))), rho_k ~ U(0.3, 0.95),
+    tau_k ~ LogNormal(0, 0.5). Draw order: all n_k, all rho_k, all tau_k, then per model the
+    AR1 path (stationary start), the iid effects and the counts."""
+    rng = np.random.default_rng(seed)
+    nks = np.floor(np.exp(rng.uniform(np.log(n_lo), np.log(n_hi), size=G))).astype(int)
+    rhos = rng.uniform(0.3, 0.95, size=G)
+    taus = rng.lognormal(0.0, 0.5, size=G)
+    models, As, ys = [], [], []
+    for nk, rho, tau in zip(nks, rhos, taus):
+        model, a = ar1_iid_model(int(nk))
+        e = rng.standard_normal(int(nk)) / np.sqrt(tau)
+        x = np.empty(int(nk))
+        x[0] = e[0] / np.sqrt(1.0 - rho * rho)
+        for t in range(1, int(nk)):
+            x[t] = rho * x[t - 1] + e[t]
+        v = rng.standard_normal(int(nk)) / np.sqrt(tau_iid)
+        y = rng.poisson(np.exp(beta0 + x + v)).astype(float)
+        models.append(model)
+        As.append(a)
+        ys.append(y)
+    return MultiProblem(models=models, a=As, y=ys,
+                        truth={"n": nks, "rho": rhos, "tau": taus, "tau_iid": tau_iid, "beta0": beta0})
+
+
+def ar1_iid_coefs(theta):
+    """theta = [log tau, logit-type rho, log tau_iid] -> coefficients of :func:`ar1_iid_model`'s
+    components [M_int, K0, K1, K2, M_iid] and their theta-derivatives (3 x 5); rho =
+    2 / (1 + e^-theta) - 1 clamped to +-0.999 as structured.rs:348-356."""
+    lt, tr, li = (float(v) for v in theta)
+    tau = np.exp(lt)
+    rho_raw = 2.0 / (1.0 + np.exp(-tr)) - 1.0
+    rho = float(np.clip(rho_raw, -0.999, 0.999))
+    drho = (1.0 - rho_raw * rho_raw) / 2.0 if rho == rho_raw else 0.0
+    ti = np.exp(li)
+    c = np.array([1.0, tau, tau * rho * rho, -tau * rho, ti])
+    dc = np.zeros((3, 5))
+    dc[0, 1:4] = c[1:4]
+    dc[1, 2] = tau * 2.0 * rho * drho
+    dc[1, 3] = -tau * drho
+    dc[2, 4] = ti
+    return c, dc

@@ -166,3 +166,28 @@ def test_group_problem_layout():
         fd = (models.group_coefs(np.array([0.1, -0.2, 1.3, 0.7]) + d)[0]
               - models.group_coefs(np.array([0.1, -0.2, 1.3, 0.7]) - d)[0]) / (2 * h)
         np.testing.assert_allclose(dcoef[i], fd, rtol=1e-7, atol=1e-9)
+
+
+def test_multi_problem_layout():
+    """Independent AR1 + iid + intercept models of uneven size: latent [intercept, AR1,
+    iid], A = [1 | I | I], sizes log-uniform in [n_lo, n_hi), coefficient derivatives."""
+    p = models.make_multi_problem(G=6, n_lo=20, n_hi=60, seed=3)
+    assert len(p.models) == len(p.a) == len(p.y) == 6
+    for m, a, y, nk in zip(p.models, p.a, p.y, p.truth["n"]):
+        assert 20 <= nk < 60 and m.n == 2 * nk + 1 and a.shape == (nk, m.n) and len(y) == nk
+        d = a.toarray()
+        np.testing.assert_array_equal(d[:, 0], 1.0)
+        np.testing.assert_array_equal(d[:, 1:1 + nk], np.eye(nk))
+        np.testing.assert_array_equal(d[:, 1 + nk:], np.eye(nk))
+    th = np.array([0.3, 1.1, 2.0])
+    c, dc = models.ar1_iid_coefs(th)
+    q = p.models[0].matrix(c).toarray()
+    nk = p.truth["n"][0]
+    rho = 2.0 / (1.0 + math.exp(-1.1)) - 1.0
+    np.testing.assert_allclose(q[1:1 + nk, 1:1 + nk], models.ar1_precision(nk, rho, math.exp(0.3)).toarray(),
+                               rtol=1e-14, atol=1e-14)
+    for i in range(3):
+        e = np.zeros(3)
+        e[i] = 1e-6
+        fd = (models.ar1_iid_coefs(th + e)[0] - models.ar1_iid_coefs(th - e)[0]) / 2e-6
+        np.testing.assert_allclose(dc[i], fd, rtol=1e-7, atol=1e-9)
