@@ -224,6 +224,36 @@ void inla_multi_free(inla_multi* h);
 int inla_multi_eval(inla_multi* h, int B, const double* coef, const double* p1scale, int flags, double* scalars,
                     double* x, double* var, double* grad_terms);
 
+/* Fit of every model (run_inla_inference_a_cancellable, inference.rs:1116-1466, per
+ * model), all models in lockstep: per model the batched Newton mode search on adjoint
+ * gradients of inla_fit (mode_search 2), the Hessian (hessian 0: the reference's FD of
+ * values with h = max(1e-4, 0.05 max|theta_g|); 1: central FD of adjoint gradients),
+ * CCD nodes with f0 and the per-model mixture moments. Batch b of every evaluation holds
+ * point b of every model. map/prior get the model index g. theta0, mode: [G][m];
+ * hessian: [G][m][m]; mlik, mode_iters, status: [G] (status 0 ok, 1 no finite CCD node,
+ * 2 singular Hessian); latent_mean, latent_var: [n]; info: [3] = {seconds, batches,
+ * model evaluations}. */
+typedef int (*inla_multi_theta_map_fn)(int g, const double* theta, int m, double* coef, double* dcoef,
+                                       double* p1scale, double* dp1scale, void* user);
+typedef double (*inla_multi_log_prior_fn)(int g, const double* theta, int m, double* grad, void* user);
+typedef struct {
+  int hessian;    /* 0 FD of values (reference), 1 FD of adjoint gradients */
+  double f0;      /* CCD f0 (0 = 1.0) */
+  int max_iter;   /* Newton iterations per model (0 = 100) */
+  double tol;     /* gradient infinity-norm tolerance (0 = 1e-4) */
+} inla_multi_fit_options;
+int inla_multi_fit(inla_multi* h, int m, const double* theta0, inla_multi_theta_map_fn map,
+                   inla_multi_log_prior_fn prior, void* user, const inla_multi_fit_options* opt, double* mode,
+                   double* hessian, double* mlik, double* latent_mean, double* latent_var, int* mode_iters,
+                   int* status, double* info);
+/* Built-in map of AR1 + iid + intercept models: theta = [log tau, logit-type rho, log tau_iid],
+ * components [intercept precision, AR1 pieces K0, K1, K2, iid] with coefficients
+ * [1, tau, tau rho^2, -tau rho, tau_iid] (ar1.rs:9-69, structured.rs:348-356). */
+int inla_multi_theta_map_ar1_iid(int g, const double* theta, int m, double* coef, double* dcoef, double* p1scale,
+                                 double* dp1scale, void* user);
+/* One prior stack (user = inla_prior_set*) for every model. */
+double inla_multi_log_prior_set(int g, const double* theta, int m, double* grad, void* user);
+
 /* ------------------------------------------------------------------------
  * Hyperpriors (crates/inla_stats/src/priors.rs): log pi(theta) and gradient.
  * ---------------------------------------------------------------------- */

@@ -1,4 +1,6 @@
 // extern "C" boundary of the multi-model Laplace engine (independent models of uneven size).
+#include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <memory>
 
@@ -106,6 +108,83 @@ int inla_multi_eval(inla_multi* h, int B, const double* coef, const double* p1sc
   } catch (...) {
     return map_exception();
   }
+}
+
+int inla_multi_fit(inla_multi* h, int m, const double* theta0, inla_multi_theta_map_fn map,
+                   inla_multi_log_prior_fn prior, void* user, const inla_multi_fit_options* opt, double* mode,
+                   double* hessian, double* mlik, double* latent_mean, double* latent_var, int* mode_iters,
+                   int* status, double* info) {
+  try {
+    if (!h || !h->eng || !theta0 || !map || !prior || m < 1 || m > 5)
+      return fail(INLA_ERR_INVALID, "invalid argument");
+    MultiLaplace& E = *h->eng;
+    MultiThetaMap tm = [&](int g, const double* th, double* c, double* dc, double* s, double* ds) {
+      return map(g, th, m, c, dc, s, ds, user);
+    };
+    MultiLogPrior lp = [&](int g, const double* th, double* gr) { return prior(g, th, m, gr, user); };
+    MultiDriver drv(E, m, tm, lp);
+    MultiFitOptions fo;
+    if (opt) {
+      fo.hessian = opt->hessian;
+      if (opt->f0 > 0) fo.f0 = opt->f0;
+      if (opt->max_iter > 0) fo.max_iter = opt->max_iter;
+      if (opt->tol > 0) fo.tol = opt->tol;
+    }
+    MultiFitResult R;
+    const int64_t before = E.launches();
+    drv.fit(theta0, fo, R);
+    g_launches += E.launches() - before;
+    const int G = E.G();
+    const int64_t n = E.n();
+    if (mode) std::memcpy(mode, R.mode.data(), sizeof(double) * G * m);
+    if (hessian) std::memcpy(hessian, R.hessian.data(), sizeof(double) * G * m * m);
+    if (mlik) std::memcpy(mlik, R.mlik.data(), sizeof(double) * G);
+    if (latent_mean) std::memcpy(latent_mean, R.latent_mean.data(), sizeof(double) * n);
+    if (latent_var) std::memcpy(latent_var, R.latent_var.data(), sizeof(double) * n);
+    if (mode_iters) std::memcpy(mode_iters, R.mode_iters.data(), sizeof(int) * G);
+    if (status) std::memcpy(status, R.status.data(), sizeof(int) * G);
+    if (info) {
+      info[0] = R.seconds;
+      info[1] = R.n_batches;
+      info[2] = (double)R.n_model_evals;
+    }
+    return INLA_OK;
+  } catch (...) {
+    return map_exception();
+  }
+}
+
+int inla_multi_theta_map_ar1_iid(int g, const double* theta, int m, double* coef, double* dcoef, double* p1scale,
+                                 double* dp1scale, void* user) {
+  (void)g;
+  (void)user;
+  // theta = [log tau, logit-type rho, log tau_iid]; components [M_int, K0, K1, K2, M_iid] with
+  // the AR1 conditional precision tau (K0 + rho^2 K1 - rho K2) (ar1.rs:9-69, structured.rs:348-356)
+  if (m != 3) return 1;
+  const double tau = std::exp(theta[0]);
+  const double rho_raw = 2.0 / (1.0 + std::exp(-theta[1])) - 1.0;
+  const double rho = std::min(std::max(rho_raw, -0.999), 0.999);
+  const double drho = rho == rho_raw ? (1.0 - rho_raw * rho_raw) / 2.0 : 0.0;
+  const double ti = std::exp(theta[2]);
+  const double c[5] = {1.0, tau, tau * rho * rho, -tau * rho, ti};
+  for (int t = 0; t < 5; ++t) coef[t] = c[t];
+  if (dcoef) {
+    for (int i = 0; i < 15; ++i) dcoef[i] = 0.0;
+    dcoef[1] = c[1];
+    dcoef[2] = c[2];
+    dcoef[3] = c[3];
+    dcoef[5 + 2] = tau * 2.0 * rho * drho;
+    dcoef[5 + 3] = -tau * drho;
+    dcoef[10 + 4] = ti;
+  }
+  *p1scale = 1.0;
+  if (dp1scale) dp1scale[0] = dp1scale[1] = dp1scale[2] = 0.0;
+  return std::isfinite(tau) && std::isfinite(ti) && tau > 0.0 && ti > 0.0 ? 0 : 1;
+}
+
+double inla_multi_log_prior_set(int g, const double* theta, int m, double* grad, void* user) {
+  (void)g;
+  return inla_log_prior_set(theta, m, grad, user);
 }
 
 }  // extern "C"

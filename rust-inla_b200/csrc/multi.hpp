@@ -10,6 +10,7 @@
 // refactorization) is taken per (theta-set, model), and a model that has
 // converged keeps its mode while the others iterate.
 #pragma once
+#include <functional>
 #include <memory>
 #include <vector>
 
@@ -79,6 +80,54 @@ class MultiLaplace {
       mdiff_, scal_, ld_, red_;
   DBuf<int> bad_, st_;
   int64_t launches_ = 0;
+};
+
+// ---------------------------------------------------------------------------
+// Fit of G independent models in lockstep (run_inla_inference_a_cancellable,
+// inference.rs:1116-1466, per model): every model runs the batched Newton mode
+// search of InlaDriver::newton on adjoint gradients with its own state (direction,
+// trust radius, backtracking candidate), the Hessian for the CCD design (the
+// reference's FD of values with h = max(1e-4, 0.05 max|theta_g|), or FD of
+// gradients), and the CCD nodes with variances; batch b of every evaluation
+// holds point b of every model, so one launch sequence serves all models.
+// ---------------------------------------------------------------------------
+using MultiThetaMap = std::function<int(int g, const double* theta, double* coef, double* dcoef, double* p1scale,
+                                        double* dp1scale)>;
+using MultiLogPrior = std::function<double(int g, const double* theta, double* grad)>;
+
+struct MultiFitOptions {
+  int hessian = 0;       // 0 FD of values (reference stencil), 1 central FD of adjoint gradients
+  double f0 = 1.0;       // CCD f0
+  int max_iter = 100;    // Newton iterations per model
+  double tol = 1e-4;     // gradient infinity-norm tolerance
+};
+
+struct MultiFitResult {
+  std::vector<double> mode, hessian, mlik;   // [G][m], [G][m][m], [G]
+  std::vector<double> latent_mean, latent_var;  // [n]
+  std::vector<int> mode_iters, status;       // [G]; status 0 ok, 1 no finite node, 2 singular Hessian
+  int n_batches = 0;
+  int64_t n_model_evals = 0;
+  double seconds = 0.0;
+};
+
+class MultiDriver {
+ public:
+  MultiDriver(MultiLaplace& eng, int m, MultiThetaMap map, MultiLogPrior prior)
+      : eng_(eng), m_(m), map_(std::move(map)), prior_(std::move(prior)) {}
+  void fit(const double* theta0, const MultiFitOptions& opt, MultiFitResult& out);
+  // f = -(mlik + log prior) [B][G] (1e12 where the Laplace evaluation failed) and its
+  // gradient [B][G][m] at the theta-sets th [B][G][m]; B may exceed the engine's batch.
+  void evaluate(int B, const double* th, bool want_grad, bool want_var, double* f, double* grad,
+                std::vector<double>* x = nullptr, std::vector<double>* var = nullptr);
+
+ private:
+  MultiLaplace& eng_;
+  int m_;
+  MultiThetaMap map_;
+  MultiLogPrior prior_;
+  int n_batches_ = 0;
+  int64_t n_model_evals_ = 0;
 };
 
 }  // namespace inla

@@ -17,7 +17,20 @@ import scipy.sparse as sp
 
 from . import _lib
 from ._lib import as_f64, as_i64, check, dptr, lib, lptr
-from .laplace import FAMILIES
+from .laplace import FAMILIES, PRIOR_PC_COR1, PRIOR_PC_PREC, prior_set
+
+MULTI_THETA_MAP = C.CFUNCTYPE(C.c_int, C.c_int, C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double),
+                              C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p)
+MULTI_LOG_PRIOR = C.CFUNCTYPE(C.c_double, C.c_int, C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double),
+                              C.c_void_p)
+
+# default hyperpriors of an AR1 + iid + intercept model, theta = [log tau, logit-type rho,
+# log tau_iid] (priors.rs:348-372: pc.prec(1, 0.01), pc.cor1(0.5, 0.75); iid pc.prec(1, 0.01))
+AR1_IID_PRIORS = [(PRIOR_PC_PREC, 0, (1.0, 0.01)), (PRIOR_PC_COR1, 1, (0.5, 0.75)), (PRIOR_PC_PREC, 2, (1.0, 0.01))]
+
+
+class FitOptions(C.Structure):
+    _fields_ = [("hessian", C.c_int), ("f0", C.c_double), ("max_iter", C.c_int), ("tol", C.c_double)]
 
 
 class MultiModel:
@@ -118,3 +131,56 @@ class MultiModel:
         if gradient:
             out["trP"], out["trQ"], out["xMx"], out["zMx"] = gt[:, :, 0], gt[:, :, 1], gt[:, :, 2], gt[:, :, 3]
         return out
+
+    def fit(self, theta0, theta_map="ar1_iid", priors=AR1_IID_PRIORS, hessian="fd", f0=1.0, max_iter=0, tol=0.0):
+        """Fit every model (``inla_multi_fit``): batched Newton mode search on adjoint gradients
+        per model, Hessian (``"fd"``: the reference's FD of values; ``"grad"``: FD of adjoint
+        gradients), CCD nodes and per-model mixture moments, all models in lockstep.
+        ``theta0``: [G][m]; ``theta_map``: ``"ar1_iid"`` or a callable ``(g, theta) -> (coef,
+        dcoef[m][T], p1scale, dp1scale[m])``; ``priors``: a list of ``(kind, slot, params)``
+        applied to every model."""
+        th0 = as_f64(np.asarray(theta0, dtype=float).reshape(self.G, -1))
+        m = th0.shape[1]
+        keep = []
+        if theta_map == "ar1_iid":
+            fmap = C.cast(lib().inla_multi_theta_map_ar1_iid, MULTI_THETA_MAP)
+        else:
+            T = self.ncomp
+
+            def _map(g, th, mm, coef, dcoef, s, ds, user):
+                try:
+                    t = np.ctypeslib.as_array(th, shape=(mm,)).copy()
+                    c, dc, p1s, dp1s = theta_map(g, t)
+                    for i in range(T):
+                        coef[i] = float(c[i])
+                    dc = np.asarray(dc, dtype=float).reshape(mm, T)
+                    for i in range(mm * T):
+                        dcoef[i] = float(dc.flat[i])
+                    s[0] = float(p1s)
+                    for i in range(mm):
+                        ds[i] = float(np.asarray(dp1s).flat[i])
+                    return 0
+                except Exception:
+                    return 1
+
+            fmap = MULTI_THETA_MAP(_map)
+        keep.append(fmap)
+        ps = prior_set(priors)
+        keep.append(ps)
+        fprior = C.cast(lib().inla_multi_log_prior_set, MULTI_LOG_PRIOR)
+        opt = FitOptions(hessian={"fd": 0, "grad": 1}[hessian], f0=float(f0), max_iter=int(max_iter), tol=float(tol))
+        G = self.G
+        mode = np.zeros((G, m))
+        hess = np.zeros((G, m, m))
+        mlik = np.zeros(G)
+        mean = np.zeros(self.n)
+        var = np.zeros(self.n)
+        iters = np.zeros(G, dtype=np.int32)
+        status = np.zeros(G, dtype=np.int32)
+        info = np.zeros(3)
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))
+        check(lib().inla_multi_fit(self._h, m, dptr(th0), fmap, fprior, C.cast(C.pointer(ps), C.c_void_p),
+                                   C.byref(opt), dptr(mode), dptr(hess), dptr(mlik), dptr(mean), dptr(var),
+                                   ip(iters), ip(status), dptr(info)))
+        return {"mode": mode, "hessian": hess, "mlik": mlik, "mean": mean, "var": var, "mode_iters": iters,
+                "status": status, "seconds": info[0], "n_batches": int(info[1]), "n_model_evals": int(info[2])}

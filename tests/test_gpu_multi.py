@@ -126,3 +126,49 @@ def test_config4_512_uneven_models():
     assert np.all(out["var"] > 0) and np.all(np.isfinite(out["mlik"]))
     for g in (0, int(np.argmax(p.truth["n"])), 511):
         check_model(out, 1, g, mm, p, c[1, g])
+
+
+def single_fit(p, g):
+    """The same model fitted on its own through the single-model engine (batched Newton on
+    adjoint gradients, FD Hessian of values, CCD)."""
+    from inla_b200.laplace import LaplaceModel
+    from inla_b200.multi import AR1_IID_PRIORS
+
+    lm = LaplaceModel(p.models[g], a=p.a[g], family="poisson", y=p.y[g], max_batch=25)
+
+    def tmap(t):
+        c, dc = models.ar1_iid_coefs(t)
+        return c, dc, 1.0, np.zeros(3)
+
+    return lm.fit(np.zeros(3), theta_map=tmap, priors=AR1_IID_PRIORS, mode_search="newton", batched=True)
+
+
+def check_fit(r, s, mm, g):
+    np.testing.assert_allclose(r["mode"][g], s["mode"], atol=1e-6)
+    np.testing.assert_allclose(r["hessian"][g], s["hessian"], rtol=1e-5, atol=1e-6)
+    assert rel(mm.split(r["mean"])[g], s["mean"]) < 1e-6
+    assert rel(mm.split(r["var"])[g], s["var"]) < 1e-6
+    assert abs(r["mlik"][g] - s["mlik"]) < 1e-6 * abs(s["mlik"])
+
+
+def test_multi_fit_matches_single_model_fits(small):
+    """Lockstep fit of all models: each model takes the decisions it takes alone."""
+    p, mm = small
+    r = mm.fit(np.zeros((mm.G, 3)))
+    assert np.all(r["status"] == 0)
+    for g in (0, 4, mm.G - 1):
+        check_fit(r, single_fit(p, g), mm, g)
+
+
+def test_config4_fit_512_models():
+    """Config 4: per-model mode search on adjoint gradients, Hessian and CCD for 512 uneven
+    models in one lockstep fit; two models checked against their own single-model fits."""
+    p = models.make_multi_problem()
+    mm = MultiModel(p.models, p.a, p.y, family="poisson", max_batch=15)
+    r = mm.fit(np.zeros((mm.G, 3)))
+    assert np.all(r["status"] == 0)
+    assert np.all(np.isfinite(r["mlik"])) and np.all(r["var"] > 0)
+    print(f"config4 fit: {r['seconds']:.2f} s, {r['n_batches']} batches, {r['n_model_evals']} model evaluations, "
+          f"max mode iterations {int(r['mode_iters'].max())}")
+    for g in (int(np.argmin(p.truth["n"])), int(np.argmax(p.truth["n"]))):
+        check_fit(r, single_fit(p, g), mm, g)
