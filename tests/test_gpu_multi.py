@@ -167,7 +167,10 @@ def test_config4_fit_512_models():
     mm = MultiModel(p.models, p.a, p.y, family="poisson", max_batch=15)
     r = mm.fit(np.zeros((mm.G, 3)))
     assert np.all(r["status"] == 0)
-    assert np.all(np.isfinite(r["mlik"])) and np.all(r["var"] > 0)
+    # the reference's CCD weights for m = 3, f0 = 1 give the centre node weight 1 - 14 w = -0.68
+    # (integration.rs:1-62), so a mixture variance can come out negative where the node
+    # variances differ; parity with the single-model fits is the check
+    assert np.all(np.isfinite(r["mlik"])) and np.all(np.isfinite(r["var"]))
     print(f"config4 fit: {r['seconds']:.2f} s, {r['n_batches']} batches, {r['n_model_evals']} model evaluations, "
           f"max mode iterations {int(r['mode_iters'].max())}")
     for g in (int(np.argmin(p.truth["n"])), int(np.argmax(p.truth["n"]))):
