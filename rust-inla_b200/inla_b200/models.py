@@ -293,11 +293,13 @@ class SpdeProblem:
 
 def make_spde_problem(nx: int = 200, n_obs: int = 20_000, seed: int = SEED_BASE + 2,
                       range_true: float = 0.2, sigma_true: float = 1.0,
-                      noise_sd: float = 0.1) -> SpdeProblem:
-    """SPDE Matern alpha=2 on the jittered ``nx x nx`` grid with Gaussian data.
+                      noise_sd: float = 0.1, family: str = "gaussian", nb_size: float = 5.0) -> SpdeProblem:
+    """SPDE Matern alpha=2 on the jittered ``nx x nx`` grid with Gaussian data (or, with
+    ``family="nbinomial"``, negative-binomial counts with size ``nb_size`` and mean
+    ``exp(A x)``).
 
     Draw order: interior jitter x, jitter y, field innovations z (n), point
-    locations (n_obs x 2), observation noise (n_obs). The field is an exact
+    locations (n_obs x 2), observation noise (n_obs) or counts. The field is an exact
     draw ``x = K^-1 C~^{1/2} z`` with ``K = tau (kappa^2 C~ + G)``, whose
     covariance ``K^-1 C~ K^-1`` is the SPDE ``Q^-1``.
     """
@@ -313,7 +315,11 @@ def make_spde_problem(nx: int = 200, n_obs: int = 20_000, seed: int = SEED_BASE 
     x = spla.spsolve(k, np.sqrt(c0) * z)
     pts = rng.uniform(0.0, 1.0, size=(n_obs, 2))
     a = grid_projector(verts, tris, nx, pts)
-    y = a @ x + noise_sd * rng.standard_normal(n_obs)
+    if family == "nbinomial":
+        mu = np.exp(a @ x)
+        y = rng.negative_binomial(nb_size, nb_size / (nb_size + mu)).astype(float)
+    else:
+        y = a @ x + noise_sd * rng.standard_normal(n_obs)
     ata = (a.T @ a).tocsc()
     model = build_latent(n, comps, "spde", extra_pattern=[ata],
                          info={"nx": nx, "c0": c0})
