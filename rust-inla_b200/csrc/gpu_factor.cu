@@ -6,6 +6,7 @@
 #include <cstring>
 
 #include "gpu_factor.hpp"
+#include "host_par.hpp"
 #include "snode_kernels.cuh"
 #include "snode_large.cuh"
 
@@ -63,21 +64,23 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
   // panel map (compact panel index -> input entry) and front positions of input entries
   std::vector<int> pmap(S.nnz_l_stored, -1);
   std::vector<int64_t> spos(nnz_, -1), spos_full(nnz_, -1);
-  for (int64_t c = 0; c < n; ++c)
-    for (int64_t p = S.colptr[c]; p < S.colptr[c + 1]; ++p) {
-      int64_t i = S.iperm[S.rowidx[p]], j = S.iperm[c];
-      int64_t lo = std::min(i, j), hi = std::max(i, j);
-      int64_t s = S.col_to_sn[lo];
-      const int64_t* R = S.sn_rows.data() + S.sn_rowptr[s];
-      int64_t m = S.sn_rowptr[s + 1] - S.sn_rowptr[s];
-      const int64_t* it = std::lower_bound(R, R + m, hi);
-      if (it == R + m || *it != hi) throw std::runtime_error("entry outside the filled pattern");
-      spos_full[p] = fptr[s] + (lo - S.sn_first[s]) * m + (it - R);
-      int64_t q = S.qmap[p];
-      if (q < 0) continue;
-      pmap[q] = (int)p;
-      spos[p] = spos_full[p];
-    }
+  parallel_for(n, [&](int64_t c0, int64_t c1) {  // disjoint writes: entry p, panel slot qmap[p]
+    for (int64_t c = c0; c < c1; ++c)
+      for (int64_t p = S.colptr[c]; p < S.colptr[c + 1]; ++p) {
+        int64_t i = S.iperm[S.rowidx[p]], j = S.iperm[c];
+        int64_t lo = std::min(i, j), hi = std::max(i, j);
+        int64_t s = S.col_to_sn[lo];
+        const int64_t* R = S.sn_rows.data() + S.sn_rowptr[s];
+        int64_t m = S.sn_rowptr[s + 1] - S.sn_rowptr[s];
+        const int64_t* it = std::lower_bound(R, R + m, hi);
+        if (it == R + m || *it != hi) throw std::runtime_error("entry outside the filled pattern");
+        spos_full[p] = fptr[s] + (lo - S.sn_first[s]) * m + (it - R);
+        int64_t q = S.qmap[p];
+        if (q < 0) continue;
+        pmap[q] = (int)p;
+        spos[p] = spos_full[p];
+      }
+  });
 
   const auto tm1 = std::chrono::steady_clock::now();
   d_first_.upload(first, stream_);

@@ -9,6 +9,7 @@
 
 #include "laplace.hpp"
 #include "laplace_kernels.cuh"
+#include "host_par.hpp"
 
 namespace inla {
 
@@ -101,16 +102,18 @@ LaplaceEngine::LaplaceEngine(const LaplaceSpec& spec, int max_batch, cudaStream_
     opptr[i + 1] = opptr[i] + na * na;
   }
   oppos.resize(opptr[nobs]);
-  for (int64_t i = 0; i < nobs; ++i) {
-    int64_t q = opptr[i];
-    for (int64_t a = acp[i]; a < acp[i + 1]; ++a)
-      for (int64_t c = acp[i]; c < acp[i + 1]; ++c, ++q) {
-        int64_t p = find(aci[a], aci[c]);
-        if (p < 0) throw std::runtime_error("laplace: pattern must contain A^T A");
-        oppos[q] = p;
-        cnt[p + 1]++;
-      }
-  }
+  parallel_for(nobs, [&](int64_t i0, int64_t i1) {  // disjoint writes: the pairs of observation i
+    for (int64_t i = i0; i < i1; ++i) {
+      int64_t q = opptr[i];
+      for (int64_t a = acp[i]; a < acp[i + 1]; ++a)
+        for (int64_t c = acp[i]; c < acp[i + 1]; ++c, ++q) {
+          int64_t p = find(aci[a], aci[c]);
+          if (p < 0) throw std::runtime_error("laplace: pattern must contain A^T A");
+          oppos[q] = p;
+        }
+    }
+  });
+  for (int64_t q = 0; q < opptr[nobs]; ++q) cnt[oppos[q] + 1]++;
   for (int64_t p = 0; p < nnz_; ++p) cnt[p + 1] += cnt[p];
   if (cnt[nnz_] >= (1LL << 31)) throw std::runtime_error("laplace: too many observation contributions");
   std::vector<int> cptr(nnz_ + 1), cobs(cnt[nnz_]);

@@ -7,6 +7,7 @@
 
 #include "multi.hpp"
 #include "multi_kernels.cuh"
+#include "host_par.hpp"
 
 namespace inla {
 
@@ -87,19 +88,25 @@ MultiLaplace::MultiLaplace(const MultiSpec& spec, int max_batch, cudaStream_t st
         if (spec_.aci[a] < spec_.lat_off[g] || spec_.aci[a] >= spec_.lat_off[g + 1])
           throw std::runtime_error("multi: observation of model g touches another model's latent nodes");
 
-  // one elimination order per block, concatenated
-  std::vector<int64_t> perm;
-  perm.reserve(n);
-  for (int g = 0; g < G; ++g) {
-    const int64_t j0 = spec_.lat_off[g], nb = spec_.lat_off[g + 1] - j0;
-    std::vector<int64_t> cp(nb + 1, 0), ri;
-    ri.reserve(spec_.colptr[j0 + nb] - spec_.colptr[j0]);
-    for (int64_t j = 0; j < nb; ++j) {
-      for (int64_t p = spec_.colptr[j0 + j]; p < spec_.colptr[j0 + j + 1]; ++p) ri.push_back(spec_.rowidx[p] - j0);
-      cp[j + 1] = (int64_t)ri.size();
-    }
-    for (int64_t v : block_order(nb, cp, ri, spec_.ordering)) perm.push_back(v + j0);
-  }
+  // one elimination order per block (blocks ordered concurrently), concatenated
+  std::vector<int64_t> perm(n);
+  parallel_for(
+      G,
+      [&](int64_t g0, int64_t g1) {
+        for (int64_t g = g0; g < g1; ++g) {
+          const int64_t j0 = spec_.lat_off[g], nb = spec_.lat_off[g + 1] - j0;
+          std::vector<int64_t> cp(nb + 1, 0), ri;
+          ri.reserve(spec_.colptr[j0 + nb] - spec_.colptr[j0]);
+          for (int64_t j = 0; j < nb; ++j) {
+            for (int64_t p = spec_.colptr[j0 + j]; p < spec_.colptr[j0 + j + 1]; ++p)
+              ri.push_back(spec_.rowidx[p] - j0);
+            cp[j + 1] = (int64_t)ri.size();
+          }
+          const std::vector<int64_t> pb = block_order(nb, cp, ri, spec_.ordering);
+          for (int64_t k = 0; k < nb; ++k) perm[j0 + k] = pb[k] + j0;
+        }
+      },
+      1);
   Symbolic sym;
   SymbolicOptions opt;
   opt.ordering = ORDER_CUSTOM;
@@ -139,16 +146,18 @@ MultiLaplace::MultiLaplace(const MultiSpec& spec, int max_batch, cudaStream_t st
     opptr[i + 1] = opptr[i] + na * na;
   }
   oppos.resize(opptr[nobs]);
-  for (int64_t i = 0; i < nobs; ++i) {
-    int64_t q = opptr[i];
-    for (int64_t a = acp[i]; a < acp[i + 1]; ++a)
-      for (int64_t c = acp[i]; c < acp[i + 1]; ++c, ++q) {
-        const int64_t p = find(aci[a], aci[c]);
-        if (p < 0) throw std::runtime_error("multi: pattern must contain A^T A");
-        oppos[q] = p;
-        cnt[p + 1]++;
-      }
-  }
+  parallel_for(nobs, [&](int64_t i0, int64_t i1) {  // disjoint writes: the pairs of observation i
+    for (int64_t i = i0; i < i1; ++i) {
+      int64_t q = opptr[i];
+      for (int64_t a = acp[i]; a < acp[i + 1]; ++a)
+        for (int64_t c = acp[i]; c < acp[i + 1]; ++c, ++q) {
+          const int64_t p = find(aci[a], aci[c]);
+          if (p < 0) throw std::runtime_error("multi: pattern must contain A^T A");
+          oppos[q] = p;
+        }
+    }
+  });
+  for (int64_t q = 0; q < opptr[nobs]; ++q) cnt[oppos[q] + 1]++;
   for (int64_t p = 0; p < nnz_; ++p) cnt[p + 1] += cnt[p];
   if (cnt[nnz_] >= (1LL << 31)) throw std::runtime_error("multi: too many observation contributions");
   std::vector<int> cptr(nnz_ + 1), cobs(std::max<int64_t>(cnt[nnz_], 1));

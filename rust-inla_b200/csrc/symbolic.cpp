@@ -2,7 +2,12 @@
 // relaxed supernodes, row structures, level schedule and index maps.
 #include "symbolic.hpp"
 
+#include "host_par.hpp"
+
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <deque>
 #include <numeric>
 #include <stdexcept>
@@ -156,7 +161,7 @@ int choose_symmetric_order(int64_t n, const int64_t* colptr, const int64_t* rowi
 
 namespace {
 
-// Upper-triangle pattern of P A P^T by columns: for column j the rows i < j.
+// Upper-triangle pattern of P A P^T by columns: for column j the rows i < j (unsorted).
 void permuted_upper(int64_t n, const int64_t* colptr, const int64_t* rowidx,
                     const std::vector<int64_t>& iperm, std::vector<int64_t>& uptr,
                     std::vector<int64_t>& uidx) {
@@ -180,17 +185,20 @@ void permuted_upper(int64_t n, const int64_t* colptr, const int64_t* rowidx,
       if (i > j) std::swap(i, j);
       uidx[fill[j]++] = i;
     }
-  for (int64_t j = 0; j < n; ++j) std::sort(uidx.begin() + uptr[j], uidx.begin() + uptr[j + 1]);
 }
 
-// Liu's elimination tree with path compression.
-void etree_from_upper(int64_t n, const std::vector<int64_t>& uptr, const std::vector<int64_t>& uidx,
-                      std::vector<int64_t>& parent) {
+// Liu's elimination tree of P A P^T with path compression, read straight from the
+// input columns (full symmetric pattern): column k of P A P^T is input column perm[k],
+// its rows i < k are the permuted rows below k. The tree does not depend on the order
+// in which a column's rows are visited.
+void etree_permuted(int64_t n, const int64_t* colptr, const int64_t* rowidx, const std::vector<int64_t>& perm,
+                    const std::vector<int64_t>& iperm, std::vector<int64_t>& parent) {
   parent.assign(n, -1);
   std::vector<int64_t> anc(n, -1);
-  for (int64_t k = 0; k < n; ++k)
-    for (int64_t p = uptr[k]; p < uptr[k + 1]; ++p) {
-      int64_t i = uidx[p];
+  for (int64_t k = 0; k < n; ++k) {
+    const int64_t c = perm[k];
+    for (int64_t p = colptr[c]; p < colptr[c + 1]; ++p) {
+      int64_t i = iperm[rowidx[p]];
       while (i != -1 && i < k) {
         int64_t next = anc[i];
         anc[i] = k;
@@ -198,6 +206,7 @@ void etree_from_upper(int64_t n, const std::vector<int64_t>& uptr, const std::ve
         i = next;
       }
     }
+  }
 }
 
 void postorder(int64_t n, const std::vector<int64_t>& parent, std::vector<int64_t>& post) {
@@ -232,6 +241,14 @@ void postorder(int64_t n, const std::vector<int64_t>& parent, std::vector<int64_
 
 void analyze(int64_t n, const int64_t* colptr, const int64_t* rowidx, const SymbolicOptions& opt,
              const int64_t* custom_perm, Symbolic& S) {
+  const bool dbg = std::getenv("INLA_DEBUG") != nullptr;
+  auto tprev = std::chrono::steady_clock::now();
+  auto phase = [&](const char* name) {
+    if (!dbg) return;
+    const auto t = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "symbolic: %s %.1f ms\n", name, std::chrono::duration<double, std::milli>(t - tprev).count());
+    tprev = t;
+  };
   if (n <= 0) throw std::runtime_error("symbolic: n must be > 0");
   if (colptr[0] != 0) throw std::runtime_error("symbolic: colptr[0] must be 0");
   for (int64_t c = 0; c < n; ++c) {
@@ -274,22 +291,32 @@ void analyze(int64_t n, const int64_t* colptr, const int64_t* rowidx, const Symb
   } else {  // RCM / time-major give fwd (old -> new)
     for (int64_t o = 0; o < n; ++o) perm0[fwd[o]] = o;
   }
+  phase("ordering");
   std::vector<int64_t> iperm0(n);
   for (int64_t k = 0; k < n; ++k) iperm0[perm0[k]] = k;
 
   // ---- etree + postorder ----------------------------------------------------
   std::vector<int64_t> uptr, uidx, parent0, post;
-  permuted_upper(n, colptr, rowidx, iperm0, uptr, uidx);
-  etree_from_upper(n, uptr, uidx, parent0);
+  etree_permuted(n, colptr, rowidx, perm0, iperm0, parent0);
   postorder(n, parent0, post);
   S.perm.resize(n);
   S.iperm.resize(n);
   for (int64_t k = 0; k < n; ++k) S.perm[k] = perm0[post[k]];
   for (int64_t k = 0; k < n; ++k) S.iperm[S.perm[k]] = k;
+  // the postorder relabels the same tree: parent of k is the relabeled parent of post[k]
+  {
+    std::vector<int64_t> ipost(n);
+    for (int64_t k = 0; k < n; ++k) ipost[post[k]] = k;
+    S.etree.assign(n, -1);
+    for (int64_t k = 0; k < n; ++k) {
+      const int64_t q = parent0[post[k]];
+      S.etree[k] = q == -1 ? -1 : ipost[q];
+    }
+  }
   permuted_upper(n, colptr, rowidx, S.iperm, uptr, uidx);
-  etree_from_upper(n, uptr, uidx, S.etree);
   const std::vector<int64_t>& par = S.etree;
 
+  phase("etree + postorder");
   // ---- column counts (row-subtree traversal) ------------------------------
   S.colcount.assign(n, 1);
   {
@@ -316,6 +343,7 @@ void analyze(int64_t n, const int64_t* colptr, const int64_t* rowidx, const Symb
   }
   S.flops_solve = 4.0 * (double)S.nnz_l + (double)n;
 
+  phase("column counts");
   // ---- fundamental supernodes ---------------------------------------------
   std::vector<int64_t> nchild(n, 0);
   for (int64_t j = 0; j < n; ++j)
@@ -392,6 +420,7 @@ void analyze(int64_t n, const int64_t* colptr, const int64_t* rowidx, const Symb
   for (int64_t s = 0; s < ns; ++s)
     for (int64_t j = S.sn_first[s]; j < S.sn_first[s + 1]; ++j) S.col_to_sn[j] = s;
 
+  phase("supernodes");
   // ---- supernodal row structures + parents ----------------------------------
   // lower pattern of P A P^T by columns: rows > j (from the upper lists).
   std::vector<int64_t> lptr(n + 1, 0), lidx;
@@ -440,6 +469,7 @@ void analyze(int64_t n, const int64_t* colptr, const int64_t* rowidx, const Symb
     }
   }
 
+  phase("row structures");
   // ---- storage offsets, levels, children CSR --------------------------------
   S.sn_rowptr.assign(ns + 1, 0);
   S.sn_lptr.assign(ns + 1, 0);
@@ -479,6 +509,7 @@ void analyze(int64_t n, const int64_t* colptr, const int64_t* rowidx, const Symb
     for (int64_t s = 0; s < ns; ++s) S.level_list[fill[S.sn_level[s]]++] = s;
   }
 
+  phase("offsets + levels");
   // ---- extend-add relative maps ---------------------------------------------
   S.rel_ptr.assign(ns + 1, 0);
   for (int64_t s = 0; s < ns; ++s) {
@@ -506,21 +537,25 @@ void analyze(int64_t n, const int64_t* colptr, const int64_t* rowidx, const Symb
     }
   }
 
+  phase("relative maps");
   // ---- value map: input entry -> L storage ----------------------------------
   S.qmap.assign(nnz, -1);
-  for (int64_t c = 0; c < n; ++c)
-    for (int64_t p = colptr[c]; p < colptr[c + 1]; ++p) {
-      int64_t r = rowidx[p];
-      if (r < c) continue;
-      int64_t i = S.iperm[r], j = S.iperm[c];
-      if (i < j) std::swap(i, j);
-      int64_t s = S.col_to_sn[j];
-      const int64_t* R = S.sn_rows.data() + S.sn_rowptr[s];
-      int64_t m = S.sn_rowptr[s + 1] - S.sn_rowptr[s];
-      const int64_t* it = std::lower_bound(R, R + m, i);
-      if (it == R + m || *it != i) throw std::runtime_error("symbolic: entry outside the filled pattern");
-      S.qmap[p] = S.sn_lptr[s] + (j - S.sn_first[s]) * m + (it - R);
-    }
+  parallel_for(n, [&](int64_t c0, int64_t c1) {
+    for (int64_t c = c0; c < c1; ++c)
+      for (int64_t p = colptr[c]; p < colptr[c + 1]; ++p) {
+        int64_t r = rowidx[p];
+        if (r < c) continue;
+        int64_t i = S.iperm[r], j = S.iperm[c];
+        if (i < j) std::swap(i, j);
+        int64_t s = S.col_to_sn[j];
+        const int64_t* R = S.sn_rows.data() + S.sn_rowptr[s];
+        int64_t m = S.sn_rowptr[s + 1] - S.sn_rowptr[s];
+        const int64_t* it = std::lower_bound(R, R + m, i);
+        if (it == R + m || *it != i) throw std::runtime_error("symbolic: entry outside the filled pattern");
+        S.qmap[p] = S.sn_lptr[s] + (j - S.sn_first[s]) * m + (it - R);
+      }
+  });
+  phase("value map");
 }
 
 }  // namespace inla
