@@ -331,14 +331,19 @@ def run_ours(args, ws, rank, local, dist):
     h2d = 8 * (p.model.comp_values.size + p.y.size + p.a.nnz) + 8 * (p.model.n + 1 + nnz) + 8 * (
         p.a.shape[0] + 1 + p.a.nnz)
     d2h = 8 * (2 * p.model.n + 3 + 9 + 64 * 4 + 6)
+    e2e_parts = []  # per step: model creation, fit, release (seconds)
     for _ in range(args.e2e_steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         lm2 = LaplaceModel(p.model, a=p.a, family="gaussian", y=p.y, max_batch=25)
+        t1 = time.perf_counter()
         r2 = lm2.fit(THETA0, **fit_kw)
+        t2 = time.perf_counter()
         lm2.close()
-        e2e_ms += (time.perf_counter() - t0) * 1e3
+        t3 = time.perf_counter()
+        e2e_ms += (t3 - t0) * 1e3
         e2e_evals += r2["n_evals"]
+        e2e_parts.append([round(t1 - t0, 4), round(t2 - t1, 4), round(t3 - t2, 4)])
     e2e_value = e2e_evals / (e2e_ms * 1e-3) if e2e_ms > 0 else None
 
     if rank != 0:
@@ -387,7 +392,7 @@ def run_ours(args, ws, rank, local, dist):
             "plain_gpu": plain,
             "speedup_vs_plain_gpu": (plain["fit_s"] / fit_s) if plain else None,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                    "fit_s": e2e_ms * 1e-3 / max(args.e2e_steps, 1)},
+                    "fit_s": e2e_ms * 1e-3 / max(args.e2e_steps, 1), "create_fit_close_s": e2e_parts},
             "gpu_launches": int(launches), "clocks": clocks, "roofline": roof, "cpu_baseline": cpu}
     print(json.dumps(line), flush=True)
     return 0

@@ -60,6 +60,14 @@ const char* inla_last_error(void);
 /* Number of kernels this library has launched in the calling process. */
 int64_t inla_kernel_launches(void);
 
+/* Device memory released by freed handles is kept per device and reused by later
+ * handles (creating and freeing handles in a loop then maps no memory); the cache
+ * holds at most half of a device's memory and is emptied automatically when an
+ * allocation fails. This call returns all cached blocks to the driver (for other
+ * users of the GPU in the same process). INLA_NO_MEMORY_CACHE in the environment
+ * disables the cache. No reference counterpart. */
+int inla_release_cached_memory(void);
+
 /* ------------------------------------------------------------------------
  * Ordering restatement (crates/inla_math/src/ordering.rs:149-162).
  * Writes fwd (old -> new) when a custom branch is taken; returns the branch

@@ -99,6 +99,15 @@ const char* inla_last_error(void) { return g_last_error.c_str(); }
 
 int64_t inla_kernel_launches(void) { return g_launches.load(); }
 
+int inla_release_cached_memory(void) {
+  try {
+    device_release_cached();
+    return INLA_OK;
+  } catch (...) {
+    return map_exception();
+  }
+}
+
 int inla_choose_symmetric_order(int64_t n, const int64_t* colptr, const int64_t* rowidx, int64_t* fwd) {
   try {
     check_pattern(n, colptr, rowidx);

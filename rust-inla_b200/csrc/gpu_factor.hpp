@@ -27,6 +27,11 @@ struct CudaError : std::runtime_error {
       throw ::inla::CudaError(std::string(#call) + ": " + cudaGetErrorString(_e), (int)_e); \
   } while (0)
 
+// Device allocation through the library's cache of released blocks (devmem.cu).
+void* device_alloc(size_t bytes);
+void device_free(void* p);
+void device_release_cached();
+
 // Small RAII device buffer.
 template <class T>
 struct DBuf {
@@ -37,7 +42,7 @@ struct DBuf {
   DBuf& operator=(const DBuf&) = delete;
   ~DBuf() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) device_free(p);
     p = nullptr;
     n = 0;
   }
@@ -45,7 +50,7 @@ struct DBuf {
     if (count <= n && p) return;
     release();
     if (count == 0) count = 1;
-    INLA_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    p = static_cast<T*>(device_alloc(count * sizeof(T)));
     n = count;
   }
   void upload(const T* h, size_t count, cudaStream_t st = 0) {

@@ -67,6 +67,7 @@ IP = C.POINTER(C.c_int)
 SIGNATURES = [
     ("inla_last_error", C.c_char_p, []),
     ("inla_kernel_launches", I64, []),
+    ("inla_release_cached_memory", C.c_int, []),
     ("inla_choose_symmetric_order", C.c_int, [I64, LP, LP, LP]),
     ("inla_solver_new", C.c_int, [C.c_int, C.POINTER(P)]),
     ("inla_solver_free", None, [P]),

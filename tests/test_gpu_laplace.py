@@ -193,3 +193,23 @@ def test_torch_autograd_function(spde_small):
     assert abs(float(vb[0]) - float(v)) <= 1e-12 * abs(float(v))
     vb.sum().backward()
     np.testing.assert_allclose(tb.grad[0].numpy(), g, rtol=1e-12, atol=1e-12)
+
+
+def test_reused_device_memory_gives_identical_results(spde_small):
+    """A model created after another one was freed runs on the freed (cached, not cleared)
+    device blocks; its results are bit-identical to a model on fresh blocks."""
+    from inla_b200._lib import check, lib
+
+    p, lm0 = spde_small
+    coefs = np.stack([models.spde_coefs(t[1], t[2])[0] for t in THETAS])
+    scale = np.exp([t[0] for t in THETAS])
+    outs = []
+    for _ in range(3):
+        lm = LaplaceModel(p.model, a=p.a, family="gaussian", y=p.y, max_batch=8)
+        outs.append(lm.eval(coefs, scale, variances=True, gradient=True))
+        lm.close()
+        if len(outs) == 2:
+            check(lib().inla_release_cached_memory())
+    for o in outs[1:]:
+        for k in ("mlik", "logdet_prior", "logdet_post", "x", "var", "trP", "trQ"):
+            np.testing.assert_array_equal(o[k], outs[0][k])
