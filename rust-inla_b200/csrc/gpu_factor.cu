@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 
 #include "gpu_factor.hpp"
 #include "host_par.hpp"
@@ -213,6 +214,17 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
     INLA_CUDA(cudaGetDevice(&dev));
     INLA_CUDA(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev));
   }
+  {  // key of the tuning table: FNV-1a over the supernode partition and row counts
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](int64_t v) {
+      for (int b = 0; b < 8; ++b) h = (h ^ (uint64_t)((v >> (8 * b)) & 0xff)) * 1099511628211ull;
+    };
+    mix(n);
+    mix(ns);
+    mix(num_sms_);
+    for (int64_t s = 0; s <= ns; ++s) mix(S.sn_first[s]), mix(S.sn_rowptr[s]);
+    struct_hash_ = h;
+  }
   set_smem(k_update64, kUpdSmem);
   set_smem(k_rows64, kRowsSmem);
   set_smem(k_fwd32<128>, (int)((S.max_m + 2 + 32 * 33) * 8));
@@ -284,9 +296,10 @@ void GpuFactor::plan_levels() {
   d_lists_.upload(flat, stream_);
 }
 
-void GpuFactor::run_factor_levels(int B) {
+void GpuFactor::run_factor_levels(int B, const std::vector<char>* fuse, cudaEvent_t* ev) {
   const int64_t fs = ftotal_;
-  for (const LevelPlan& P : levels_) {
+  for (size_t li = 0; li < levels_.size(); ++li) {
+    const LevelPlan& P = levels_[li];
     if (!P.small_a.empty()) {
       dim3 g((unsigned)P.small_a.size(), B);
       k_factor_small<128><<<g, 128, small_factor_smem(P.mmax_a), stream_>>>(ds_, d_lists_.p + P.off_small_a, F_.p,
@@ -299,6 +312,7 @@ void GpuFactor::run_factor_levels(int B) {
                                                                              fs);
       ++launches_;
     }
+    if (ev) INLA_CUDA(cudaEventRecord(ev[2 * li], stream_));
     if (!P.large.empty()) {
       const int nl = (int)P.large.size();
       const int* lst = d_lists_.p + P.off_large;
@@ -315,7 +329,8 @@ void GpuFactor::run_factor_levels(int B) {
         // factorizations).
         const int nrb = std::max(1, cdiv(rows, kPanelRows));
         const int per = std::max(1, (2 * num_sms_) / std::max(1, nl * B));
-        if (per >= nrb) {
+        const bool fused = fuse ? (*fuse)[li] != 0 : per >= nrb;
+        if (fused) {
           k_panel64<<<dim3(nl, B, nrb), 256, kPanelSmem, stream_>>>(ds_, lst, j0, kPanelRows, F_.p, fs, dcache_.p,
                                                                      linv_.p);
         } else {
@@ -329,10 +344,75 @@ void GpuFactor::run_factor_levels(int B) {
         launches_ += 2;
       }
     }
+    if (ev) INLA_CUDA(cudaEventRecord(ev[2 * li + 1], stream_));
   }
   k_logdet_chunks<<<dim3(nldchunk_, B), 256, 0, stream_>>>(ds_, F_.p, fs, ldpart_.p, ldflag_.p, ldticket_.p,
                                                            logdet_.p, status_.p);
   ++launches_;
+}
+
+// ---------------------------------------------------------------------------
+// Panel-schedule autotuner. For every level with large fronts the panel step has
+// two forms with bit-identical results: "fused" (each of the nrb row CTAs factors
+// the 64 x 64 diagonal block itself, one launch) and "split" (one CTA per front
+// factors it, k_rows64 forms the rows from the cached factor, two launches). Which
+// is faster depends on the level's fronts, the batch size and the GPU, so on the
+// first factorization at a batch size B the level sequence runs once in each form
+// (after a fill, untimed warm-up first) with CUDA events around every level's
+// large-front work, and each level keeps the faster form. Decisions are kept in a
+// process-wide table keyed by the supernodal structure and B, so later handles on
+// the same pattern reuse them. INLA_NO_AUTOTUNE in the environment keeps the
+// occupancy rule (fused while every row CTA fits in about one wave).
+// ---------------------------------------------------------------------------
+namespace {
+std::mutex g_tune_mu;
+std::map<std::pair<uint64_t, int>, std::vector<char>> g_tune;  // (structure hash, B) -> schedule
+}  // namespace
+
+const std::vector<char>* GpuFactor::schedule(int B, const std::function<void()>& fill) {
+  static const bool off = std::getenv("INLA_NO_AUTOTUNE") != nullptr;
+  if (off) return nullptr;
+  bool any_large = false;
+  for (const LevelPlan& P : levels_) any_large = any_large || !P.large.empty();
+  if (!any_large) return nullptr;
+  auto it = fuse_.find(B);
+  if (it != fuse_.end()) return &it->second;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto g = g_tune.find({struct_hash_, B});
+    if (g != g_tune.end()) return &(fuse_[B] = g->second);
+  }
+  const size_t L = levels_.size();
+  std::vector<cudaEvent_t> ev(2 * L);
+  for (auto& e : ev) INLA_CUDA(cudaEventCreate(&e));
+  std::vector<double> t[2];
+  for (int form = 0; form < 2; ++form) {
+    const std::vector<char> pol(L, (char)form);
+    fill();
+    run_factor_levels(B, &pol, nullptr);  // warm-up (module load, caches)
+    fill();
+    run_factor_levels(B, &pol, ev.data());
+    INLA_CUDA(cudaStreamSynchronize(stream_));
+    t[form].assign(L, 0.0);
+    for (size_t l = 0; l < L; ++l) {
+      float ms = 0.f;
+      INLA_CUDA(cudaEventElapsedTime(&ms, ev[2 * l], ev[2 * l + 1]));
+      t[form][l] = ms;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  std::vector<char> best(L, 0);
+  for (size_t l = 0; l < L; ++l) best[l] = t[1][l] < t[0][l] ? 1 : 0;
+  if (std::getenv("INLA_DEBUG")) {
+    double a = 0, b = 0, c = 0;
+    for (size_t l = 0; l < L; ++l) a += t[0][l], b += t[1][l], c += std::min(t[0][l], t[1][l]);
+    std::fprintf(stderr, "autotune B=%d: split %.3f ms, fused %.3f ms, per-level best %.3f ms\n", B, a, b, c);
+  }
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[{struct_hash_, B}] = best;
+  }
+  return &(fuse_[B] = best);
 }
 
 template <class Body>
@@ -370,11 +450,15 @@ void GpuFactor::launch_cached(const std::vector<int64_t>& key, Body&& body) {
 
 void GpuFactor::factor_values(const double* d_vals, int B) {
   if (B < 1 || B > max_batch_) throw std::runtime_error("batch size out of range");
-  launch_cached({1, B, (int64_t)(uintptr_t)d_vals}, [&] {
+  auto fill = [&] {
     k_fill_panels<<<dim3(nfill_, B), 256, 0, stream_>>>(ds_, d_csn_.p, ntot_, d_pmap_.p, d_vals, nnz_, F_.p,
                                                         ftotal_);
     ++launches_;
-    run_factor_levels(B);
+  };
+  const std::vector<char>* pol = schedule(B, fill);  // settled before any capture
+  launch_cached({1, B, (int64_t)(uintptr_t)d_vals}, [&] {
+    fill();
+    run_factor_levels(B, pol);
   });
 }
 
@@ -388,16 +472,21 @@ void GpuFactor::factor_model(int ncomp, const double* d_comp, const double* d_co
   int64_t dbits, dpbits;
   std::memcpy(&dbits, &diag_add, sizeof(dbits));
   std::memcpy(&dpbits, &diag_add_post, sizeof(dpbits));
+  auto fill = [&] {
+    k_fill_panels_model<<<dim3(nfillm_), 256, 0, stream_>>>(ds_, d_csnm_.p, ntot_, d_pmap_.p, ncomp, d_comp, nnz_,
+                                                            d_coef, diag_add, d_pdiag, d_cptr, d_cobs, d_cprod, d_w,
+                                                            wstride, B, nprior, diag_add_post, d_pseg, nseg, F_.p,
+                                                            ftotal_);
+    ++launches_;
+  };
+  const std::vector<char>* pol = schedule(B, fill);  // settled before any capture
   launch_cached({2, B, ncomp, (int64_t)(uintptr_t)d_comp, (int64_t)(uintptr_t)d_coef, dbits,
                  (int64_t)(uintptr_t)d_pdiag, (int64_t)(uintptr_t)d_cptr, (int64_t)(uintptr_t)d_cobs,
                  (int64_t)(uintptr_t)d_cprod, (int64_t)(uintptr_t)d_w, wstride, nprior, dpbits,
                  (int64_t)(uintptr_t)d_pseg, nseg},
                 [&] {
-                  k_fill_panels_model<<<dim3(nfillm_), 256, 0, stream_>>>(
-                      ds_, d_csnm_.p, ntot_, d_pmap_.p, ncomp, d_comp, nnz_, d_coef, diag_add, d_pdiag, d_cptr, d_cobs,
-                      d_cprod, d_w, wstride, B, nprior, diag_add_post, d_pseg, nseg, F_.p, ftotal_);
-                  ++launches_;
-                  run_factor_levels(B);
+                  fill();
+                  run_factor_levels(B, pol);
                 });
 }
 

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <map>
 #include <memory>
 #include <stdexcept>
@@ -126,7 +127,12 @@ class GpuFactor {
 
  private:
   void plan_levels();
-  void run_factor_levels(int B);
+  // fuse: per level, 1 = each row CTA factors the diagonal block itself, 0 = one CTA
+  // factors it and k_rows64 forms the rows; nullptr = the occupancy rule. ev: events
+  // recorded before and after every level's large-front work (2 per level).
+  void run_factor_levels(int B, const std::vector<char>* fuse = nullptr, cudaEvent_t* ev = nullptr);
+  // Per-level panel schedule for batch size B, measured on first use (see gpu_factor.cu).
+  const std::vector<char>* schedule(int B, const std::function<void()>& fill);
   void selinv_levels(int B, int slot0);
   template <class Body>
   void launch_cached(const std::vector<int64_t>& key, Body&& body);
@@ -137,6 +143,8 @@ class GpuFactor {
   };
   std::map<std::vector<int64_t>, GraphEntry> graphs_;
   bool use_graphs_ = true;
+  std::map<int, std::vector<char>> fuse_;  // tuned panel schedule per batch size
+  uint64_t struct_hash_ = 0;               // key of the process-wide tuning cache
 
   Symbolic sym_;
   int max_batch_;
