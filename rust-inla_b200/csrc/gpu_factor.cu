@@ -251,6 +251,8 @@ void GpuFactor::plan_levels() {
   const Symbolic& S = sym_;
   levels_.assign(S.nlevels, LevelPlan());
   std::vector<int> flat;
+  // fronts of at most kTinyM rows: one warp each (INLA_NO_TINY_FRONTS keeps them on k_factor_small)
+  static const bool tiny_on = std::getenv("INLA_NO_TINY_FRONTS") == nullptr;
   for (int32_t l = 0; l < S.nlevels; ++l) {
     LevelPlan& P = levels_[l];
     for (int64_t t = S.level_ptr[l]; t < S.level_ptr[l + 1]; ++t) {
@@ -259,7 +261,9 @@ void GpuFactor::plan_levels() {
       int m = (int)(S.sn_rowptr[s + 1] - S.sn_rowptr[s]);
       P.all.push_back(s);
       P.mmax_all = std::max(P.mmax_all, m);
-      if (m <= kSmallA) {
+      if (tiny_on && m <= kTinyM) {
+        P.tiny.push_back(s);
+      } else if (m <= kSmallA) {
         P.small_a.push_back(s);
         P.mmax_a = std::max(P.mmax_a, m);
       } else if (m <= kSmallB) {
@@ -286,6 +290,7 @@ void GpuFactor::plan_levels() {
       flat.insert(flat.end(), v.begin(), v.end());
       return off;
     };
+    P.off_tiny = put(P.tiny);
     P.off_small_a = put(P.small_a);
     P.off_small_b = put(P.small_b);
     P.off_large = put(P.large);
@@ -300,6 +305,12 @@ void GpuFactor::run_factor_levels(int B, const std::vector<char>* fuse, cudaEven
   const int64_t fs = ftotal_;
   for (size_t li = 0; li < levels_.size(); ++li) {
     const LevelPlan& P = levels_[li];
+    if (!P.tiny.empty()) {
+      const int nt = (int)P.tiny.size();
+      k_factor_tiny<<<dim3(cdiv(nt, kTinyWarps), B), 32 * kTinyWarps, 0, stream_>>>(ds_, d_lists_.p + P.off_tiny, nt,
+                                                                                 F_.p, fs);
+      ++launches_;
+    }
     if (!P.small_a.empty()) {
       dim3 g((unsigned)P.small_a.size(), B);
       k_factor_small<128><<<g, 128, small_factor_smem(P.mmax_a), stream_>>>(ds_, d_lists_.p + P.off_small_a, F_.p,

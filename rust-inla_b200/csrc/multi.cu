@@ -1,9 +1,13 @@
 // Multi-model Laplace engine: G independent models, one block-diagonal symbolic
 // analysis, B theta-sets, per-(theta-set, model) Newton control.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
+#include <string>
 
 #include "multi.hpp"
 #include "multi_kernels.cuh"
@@ -270,6 +274,9 @@ void MultiLaplace::factor(int B, bool posterior) {
 
 void MultiLaplace::eval(int B, const double* coef, const double* p1scale, int flags, MultiOut& R) {
   if (B < 1 || B > max_batch_) throw std::runtime_error("multi: batch size out of range");
+  const bool dbg = std::getenv("INLA_DEBUG") != nullptr;
+  const auto tstart = std::chrono::steady_clock::now();
+  std::string trace;  // active (theta-set, model) pairs after every Newton iteration
   const int G = spec_.G, T = spec_.ncomp, T1 = T + 1;
   const int64_t n = spec_.n, nobs = spec_.nobs;
   const size_t BG = (size_t)B * G, MG = (size_t)max_batch_ * G;
@@ -396,12 +403,14 @@ void MultiLaplace::eval(int B, const double* coef, const double* p1scale, int fl
       INLA_CUDA(cudaMemcpyAsync(mdiff.data(), mdiff_.p, sizeof(double) * BG, cudaMemcpyDeviceToHost, stream_));
       INLA_CUDA(cudaStreamSynchronize(stream_));
       bool left = false;
+      size_t nleft = 0;
       for (size_t q = 0; q < BG; ++q) {
         if (!active[q]) continue;
         R.iters[q] = it + 1;
         if (mdiff[q] < spec_.tol || max_step[q] < spec_.tol) active[q] = 0;  // converged
-        else left = true;
+        else left = true, ++nleft;
       }
+      if (dbg) trace += " " + std::to_string(nleft);
       if (!left) break;
     }
     for (size_t q = 0; q < BG; ++q)
@@ -462,6 +471,11 @@ void MultiLaplace::eval(int B, const double* coef, const double* p1scale, int fl
   }
   INLA_CUDA(cudaStreamSynchronize(stream_));
   INLA_CUDA(cudaGetLastError());
+  if (dbg)
+    std::fprintf(stderr, "multi eval B=%d G=%d grad=%d var=%d: %.1f ms, active after each Newton iteration:%s\n", B, G,
+                 (int)grad, (int)want_var,
+                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tstart).count(),
+                 trace.c_str());
   for (size_t q = 0; q < BG; ++q) {
     if (stt[q]) R.status[q] = LAP_SINGULAR_PRIOR;
     if (R.status[q] == LAP_OK && stt[MG + q]) R.status[q] = LAP_SINGULAR_POST;

@@ -210,6 +210,72 @@ __global__ void __launch_bounds__(NT) k_factor_small(DevSym S, const int* __rest
 }
 
 // ---------------------------------------------------------------------------
+// tiny fronts (m <= kTinyM rows): one warp per (front, problem), kTinyWarps fronts
+// per CTA. The front is staged in the warp's shared-memory slice (column-major,
+// leading dimension kTinyLd), the children's updates are added in fixed order,
+// then the k pivot steps run right-looking with lane i owning row i:
+//   u_i = A[i][t], A[i][t] = u_i / d_t (i > t), A[i][j] -= (u_i / d_t) u_j for t < j <= i,
+// leaving unit L below the diagonal, D on it and the Schur complement in the
+// trailing block -- the layout k_factor_small leaves. Fronts this small give a
+// CTA-wide blocked factorization almost nothing to share among its warps.
+// ---------------------------------------------------------------------------
+constexpr int kTinyM = 32;
+constexpr int kTinyWarps = 4;
+constexpr int kTinyLd = kTinyM + 1;
+
+__global__ void __launch_bounds__(32 * kTinyWarps) k_factor_tiny(DevSym S, const int* __restrict__ list, int nlist,
+                                                                 double* __restrict__ F, int64_t fstride) {
+  __shared__ double sA[kTinyWarps][kTinyM * kTinyLd];
+  __shared__ double sU[kTinyWarps][kTinyM];
+  __shared__ int sR[kTinyWarps][kTinyM];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int idx = blockIdx.x * kTinyWarps + warp;
+  if (idx >= nlist) return;  // the whole warp leaves; only warp-level synchronization follows
+  const int s = list[idx], b = blockIdx.y;
+  double* Fb = F + (int64_t)b * fstride;
+  double* A = sA[warp];
+  double* U = sU[warp];
+  int* R = sR[warp];
+  const int k = sn_k(S, s), m = sn_m(S, s);
+  double* Fs = Fb + S.fptr[s];
+  const int mm = m * m;
+  for (int e = lane; e < mm; e += 32) {
+    const int col = e / m, row = e - col * m;
+    A[row + col * kTinyLd] = col < k ? Fs[e] : 0.0;
+  }
+  __syncwarp();
+  for (int q = S.child_ptr[s]; q < S.child_ptr[s + 1]; ++q) {
+    const int c = S.child_list[q];
+    const int kc = sn_k(S, c), mc = sn_m(S, c), rc = mc - kc;
+    const double* Uc = Fb + S.fptr[c] + (int64_t)kc * mc + kc;
+    if (lane < rc) R[lane] = S.relx[S.rowptr[c] + kc + lane];
+    __syncwarp();
+    for (int e = lane; e < rc * rc; e += 32) {
+      const int jj = e / rc, ii = e - jj * rc;
+      if (ii >= jj) A[R[ii] + R[jj] * kTinyLd] += Uc[ii + (int64_t)jj * mc];
+    }
+    __syncwarp();
+  }
+  for (int t = 0; t < k; ++t) {
+    const double d = A[t + t * kTinyLd];
+    const bool below = lane > t && lane < m;
+    const double u = below ? A[lane + t * kTinyLd] : 0.0;
+    U[lane] = u;
+    __syncwarp();
+    if (below) {
+      const double l = u / d;
+      A[lane + t * kTinyLd] = l;
+      for (int j = t + 1; j <= lane; ++j) A[lane + j * kTinyLd] -= l * U[j];
+    }
+    __syncwarp();
+  }
+  for (int e = lane; e < mm; e += 32) {
+    const int col = e / m, row = e - col * m;
+    if (col < k || row >= col) Fs[e] = A[row + col * kTinyLd];
+  }
+}
+
+// ---------------------------------------------------------------------------
 // large fronts: blocked right-looking partial LDL^T in global memory
 // ---------------------------------------------------------------------------
 
