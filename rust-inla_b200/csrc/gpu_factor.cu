@@ -261,6 +261,10 @@ void GpuFactor::plan_levels() {
       int m = (int)(S.sn_rowptr[s + 1] - S.sn_rowptr[s]);
       P.all.push_back(s);
       P.mmax_all = std::max(P.mmax_all, m);
+      if (!(tiny_on && m <= kTinyM)) {
+        P.nontiny.push_back(s);
+        P.mmax_nontiny = std::max(P.mmax_nontiny, m);
+      }
       if (tiny_on && m <= kTinyM) {
         P.tiny.push_back(s);
       } else if (m <= kSmallA) {
@@ -295,6 +299,7 @@ void GpuFactor::plan_levels() {
     P.off_small_b = put(P.small_b);
     P.off_large = put(P.large);
     P.off_all = put(P.all);
+    P.off_nontiny = put(P.nontiny);
     P.off_si_small = put(P.si_small);
     P.off_si_large = put(P.si_large);
   }
@@ -510,16 +515,33 @@ void GpuFactor::solve(double* d_x, int64_t xstride, int B, int slot0) {
   launch_cached({3, B, (int64_t)(uintptr_t)d_x, xstride, slot0}, [&] {
     k_permute_in<<<gp, 256, 0, stream_>>>(n, d_perm_.p, d_x, xstride, xp_.p);
     ++launches_;
+    const int64_t us = std::max<int64_t>(usum_, 1);
     for (const LevelPlan& P : levels_) {
-      k_fwd32<128><<<dim3((unsigned)P.all.size(), B), 128, (P.mmax_all + 2 + 32 * 33) * 8, stream_>>>(
-          ds_, d_lists_.p + P.off_all, Fp, fs, xp_.p, ub_.p, std::max<int64_t>(usum_, 1));
-      ++launches_;
+      if (!P.tiny.empty()) {
+        const int nt = (int)P.tiny.size();
+        k_fwd_tiny<<<dim3(cdiv(nt, kTinySweepWarps), B), 32 * kTinySweepWarps, 0, stream_>>>(
+            ds_, d_lists_.p + P.off_tiny, nt, Fp, fs, xp_.p, ub_.p, us);
+        ++launches_;
+      }
+      if (!P.nontiny.empty()) {
+        k_fwd32<128><<<dim3((unsigned)P.nontiny.size(), B), 128, (P.mmax_nontiny + 2 + 32 * 33) * 8, stream_>>>(
+            ds_, d_lists_.p + P.off_nontiny, Fp, fs, xp_.p, ub_.p, us);
+        ++launches_;
+      }
     }
     for (int l = (int)levels_.size() - 1; l >= 0; --l) {
       const LevelPlan& P = levels_[l];
-      k_bwd32<128><<<dim3((unsigned)P.all.size(), B), 128, (P.mmax_all + 2 + 32 * 33) * 8, stream_>>>(ds_, d_lists_.p + P.off_all,
-                                                                                    Fp, fs, xp_.p);
-      ++launches_;
+      if (!P.tiny.empty()) {
+        const int nt = (int)P.tiny.size();
+        k_bwd_tiny<<<dim3(cdiv(nt, kTinySweepWarps), B), 32 * kTinySweepWarps, 0, stream_>>>(
+            ds_, d_lists_.p + P.off_tiny, nt, Fp, fs, xp_.p);
+        ++launches_;
+      }
+      if (!P.nontiny.empty()) {
+        k_bwd32<128><<<dim3((unsigned)P.nontiny.size(), B), 128, (P.mmax_nontiny + 2 + 32 * 33) * 8, stream_>>>(
+            ds_, d_lists_.p + P.off_nontiny, Fp, fs, xp_.p);
+        ++launches_;
+      }
     }
     k_permute_out<<<gp, 256, 0, stream_>>>(n, d_perm_.p, xp_.p, d_x, xstride);
     ++launches_;

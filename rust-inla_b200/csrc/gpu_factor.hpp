@@ -62,8 +62,9 @@ struct DBuf {
 };
 
 struct LevelPlan {
-  std::vector<int> tiny, small_a, small_b, large, all;  // host copies (supernode ids)
-  int off_tiny = 0, off_small_a = 0, off_small_b = 0, off_large = 0, off_all = 0;  // offsets into one device list
+  std::vector<int> tiny, small_a, small_b, large, all, nontiny;  // host copies (supernode ids)
+  int off_tiny = 0, off_small_a = 0, off_small_b = 0, off_large = 0, off_all = 0, off_nontiny = 0;  // offsets into one device list
+  int mmax_nontiny = 0;
   int mmax_a = 0, mmax_b = 0, mmax_all = 0, kmax_large = 0, mmax_large = 0;
   // selected inversion grouping
   std::vector<int> si_small, si_large;

@@ -550,6 +550,86 @@ __global__ void __launch_bounds__(NT, 8) k_bwd32(DevSym S, const int* __restrict
   for (int t = threadIdx.x; t < k; t += NT) xb[f + t] = x[t];
 }
 
+// Sweeps of fronts with m <= 32 rows (one 32-column block): one warp per (front,
+// problem), kTinySweepWarps per CTA. Lane t holds entry t of the front's vector; the
+// arithmetic follows k_fwd32 / k_bwd32 step for step (sequential shuffle chain on the
+// diagonal block, the same four partial sums for the rows below, the same xor tree
+// for the column sums), so the results equal theirs.
+constexpr int kTinySweepWarps = 8;
+
+__global__ void __launch_bounds__(32 * kTinySweepWarps) k_fwd_tiny(DevSym S, const int* __restrict__ list, int nlist,
+                                                                   const double* __restrict__ F, int64_t fstride,
+                                                                   double* __restrict__ xp, double* __restrict__ ub,
+                                                                   int64_t ustride) {
+  __shared__ double sy[kTinySweepWarps][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int idx = blockIdx.x * kTinySweepWarps + warp;
+  if (idx >= nlist) return;  // the whole warp leaves; only warp-level synchronization follows
+  const int s = list[idx], b = blockIdx.y;
+  const int k = lg_k(S, s), m = lg_m(S, s), f = S.first[s];
+  const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
+  double* xb = xp + (int64_t)b * S.n;
+  double* ubb = ub + (int64_t)b * ustride;
+  double* y = sy[warp];
+  y[lane] = lane < k ? xb[f + lane] : 0.0;
+  __syncwarp();
+  for (int q = S.child_ptr[s]; q < S.child_ptr[s + 1]; ++q) {
+    const int c = S.child_list[q];
+    const int kc = lg_k(S, c), rc = lg_m(S, c) - kc;
+    if (lane < rc) y[S.relx[S.rowptr[c] + kc + lane]] += ubb[S.uoff[c] + lane];
+    __syncwarp();
+  }
+  double yi = y[lane];
+  {  // diagonal block: unit lower L_JJ
+    double yd = lane < k ? yi : 0.0;
+    for (int j = 0; j < k; ++j) {
+      const double yj = __shfl_sync(0xffffffffu, yd, j);
+      if (lane > j && lane < k) yd -= Fs[lane + (int64_t)j * m] * yj;
+    }
+    if (lane < k) yi = yd;
+    y[lane] = yi;
+  }
+  __syncwarp();
+  if (lane >= k && lane < m) {  // rows below the block
+    double a[4] = {0.0, 0.0, 0.0, 0.0};
+    const double* Lr = Fs + lane;
+    for (int j = 0; j < k; ++j) a[j & 3] += Lr[(int64_t)j * m] * y[j];
+    yi -= (a[0] + a[1]) + (a[2] + a[3]);
+  }
+  if (lane < k) xb[f + lane] = yi / Fs[lane + (int64_t)lane * m];
+  else if (lane < m) ubb[S.uoff[s] + lane - k] = yi;
+}
+
+__global__ void __launch_bounds__(32 * kTinySweepWarps) k_bwd_tiny(DevSym S, const int* __restrict__ list, int nlist,
+                                                                   const double* __restrict__ F, int64_t fstride,
+                                                                   double* __restrict__ xp) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int idx = blockIdx.x * kTinySweepWarps + warp;
+  if (idx >= nlist) return;  // the whole warp leaves; only warp-level synchronization follows
+  const int s = list[idx], b = blockIdx.y;
+  const int k = lg_k(S, s), m = lg_m(S, s), f = S.first[s];
+  const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
+  double* xb = xp + (int64_t)b * S.n;
+  double xl = lane < m ? xb[S.rows[S.rowptr[s] + lane]] : 0.0;
+  // x_j -= sum_{i >= k} L_ij x_i for the block's columns: as in k_bwd32, lane l holds the
+  // term of row k + l and the butterfly total of lane 0 is used
+  const int ri = k + lane;
+  const double xs = __shfl_sync(0xffffffffu, xl, ri & 31);
+  for (int j = 0; j < k; ++j) {
+    double acc = ri < m ? Fs[ri + (int64_t)j * m] * xs : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    acc = __shfl_sync(0xffffffffu, acc, 0);
+    if (lane == j) xl -= acc;
+  }
+  // unit upper L_JJ^T from the last row up
+  for (int i = k - 1; i >= 0; --i) {
+    const double xi = __shfl_sync(0xffffffffu, xl, i);
+    if (lane < i) xl -= Fs[i + (int64_t)lane * m] * xi;
+  }
+  if (lane < k) xb[f + lane] = xl;
+}
+
 // ---------------------------------------------------------------------------
 // selected inverse
 // ---------------------------------------------------------------------------
