@@ -468,77 +468,6 @@ __global__ void k_constr_apply(int n, int64_t stride, int k, const int64_t* __re
   }
 }
 
-// sum of a [B][len] array per problem
-template <int NT>
-__global__ void __launch_bounds__(NT) k_row_sum(int64_t len, const double* __restrict__ v, double* __restrict__ out) {
-  __shared__ double red[NT];
-  const int b = blockIdx.x;
-  double s = 0.0;
-  for (int64_t i = threadIdx.x; i < len; i += NT) s += v[(int64_t)b * len + i];
-  s = block_sum<NT>(s, red);
-  if (threadIdx.x == 0) out[b] = s;
-}
-
-// x^T Q(theta_b) x and the per-component quadratic forms x^T M_t x
-// out[b][0] = x^T Q x, out[b][1+t] = x^T M_t x
-template <int NT>
-__global__ void __launch_bounds__(NT) k_quad_forms(int n, int ncomp, const int64_t* __restrict__ qcp,
-                                                   const int* __restrict__ qri, const double* __restrict__ comp,
-                                                   int64_t nnz, const double* __restrict__ coef,
-                                                   const double* __restrict__ x, double* __restrict__ out) {
-  __shared__ double red[NT];
-  const int b = blockIdx.x;
-  const double* xb = x + (int64_t)b * n;
-  double acc[8];
-  for (int t = 0; t < 8; ++t) acc[t] = 0.0;
-  for (int j = threadIdx.x; j < n; j += NT) {
-    const double xj = xb[j];
-    for (int64_t p = qcp[j]; p < qcp[j + 1]; ++p) {
-      const double xx = xj * xb[qri[p]];
-      for (int t = 0; t < ncomp && t < 8; ++t) acc[t] += comp[(int64_t)t * nnz + p] * xx;
-    }
-  }
-  double total = 0.0;
-  for (int t = 0; t < ncomp && t < 8; ++t) {
-    double s = block_sum<NT>(acc[t], red);
-    if (threadIdx.x == 0) out[(int64_t)b * (ncomp + 1) + 1 + t] = s;
-    total += coef[(int64_t)b * ncomp + t] * s;
-  }
-  if (threadIdx.x == 0) out[(int64_t)b * (ncomp + 1)] = total;
-}
-
-// Trace contractions of a selected inverse given on the full pattern
-// (both triangles): out[b][t] = sum_p sigma[b][p] comp[t][p]  (= tr(Sigma M_t)),
-// out[b][ncomp] = sum_p sigma[b][p] sum_q w2[b][obs_q] prod_q (= tr(Sigma A^T diag(w2) A)).
-template <int NT>
-__global__ void __launch_bounds__(NT) k_trace_contract(int64_t nnz, int ncomp, const double* __restrict__ comp,
-                                                       const double* __restrict__ sigma,
-                                                       const int* __restrict__ cptr, const int* __restrict__ cobs,
-                                                       const double* __restrict__ cprod,
-                                                       const double* __restrict__ w2, int64_t nobs,
-                                                       double* __restrict__ out) {
-  __shared__ double red[NT];
-  const int b = blockIdx.x;
-  const double* sb = sigma + (int64_t)b * nnz;
-  double acc[9];
-  for (int t = 0; t < 9; ++t) acc[t] = 0.0;
-  for (int64_t p = threadIdx.x; p < nnz; p += NT) {
-    const double s = sb[p];
-    for (int t = 0; t < ncomp && t < 8; ++t) acc[t] += s * comp[(int64_t)t * nnz + p];
-    if (w2) {
-      double a = 0.0;
-      for (int q = cptr[p]; q < cptr[p + 1]; ++q) a += w2[(int64_t)b * nobs + cobs[q]] * cprod[q];
-      acc[8] += s * a;
-    }
-  }
-  for (int t = 0; t < ncomp && t < 8; ++t) {
-    double s = block_sum<NT>(acc[t], red);
-    if (threadIdx.x == 0) out[(int64_t)b * (ncomp + 1) + t] = s;
-  }
-  double s = block_sum<NT>(acc[8], red);
-  if (threadIdx.x == 0) out[(int64_t)b * (ncomp + 1) + ncomp] = s;
-}
-
 // Mirror lower-entry values onto the upper entries of the full pattern:
 // out[b][p] = buf[b][spos_full[p]] (spos_full maps every entry to its lower twin).
 __global__ void k_pattern_full(int64_t nnz, const int64_t* __restrict__ spos_full, const double* __restrict__ buf,

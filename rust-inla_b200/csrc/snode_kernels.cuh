@@ -280,45 +280,6 @@ __global__ void __launch_bounds__(32 * kTinyWarps) k_factor_tiny(DevSym S, const
 // ---------------------------------------------------------------------------
 
 constexpr int kNB = 32;       // block-column width
-constexpr int kGatherCW = 32; // parent columns per gather CTA
-
-// Zero the update part of columns [c0,c1) and pull every child's update into
-// those columns (children in fixed order; targets unique within one child).
-__global__ void k_gather_large(DevSym S, const int* __restrict__ list, double* __restrict__ F,
-                               int64_t fstride) {
-  const int s = list[blockIdx.x], b = blockIdx.y;
-  const int k = sn_k(S, s), m = sn_m(S, s);
-  const int c0 = blockIdx.z * kGatherCW;
-  if (c0 >= m) return;
-  const int c1 = min(c0 + kGatherCW, m);
-  double* Fb = F + (int64_t)b * fstride;
-  double* Fs = Fb + S.fptr[s];
-  for (int col = max(c0, k); col < c1; ++col)
-    for (int row = col + threadIdx.x; row < m; row += blockDim.x) Fs[row + (int64_t)col * m] = 0.0;
-  __syncthreads();
-  for (int q = S.child_ptr[s]; q < S.child_ptr[s + 1]; ++q) {
-    const int c = S.child_list[q];
-    const int kc = sn_k(S, c), mc = sn_m(S, c), rc = mc - kc;
-    const double* Uc = Fb + S.fptr[c] + (int64_t)kc * mc + kc;
-    const int* relc = S.relx + S.rowptr[c] + kc;
-    // source columns whose target column lies in [c0,c1): relc is increasing
-    int lo = 0, hi = rc;
-    {
-      int a = 0, z = rc;
-      while (a < z) { int mid = (a + z) >> 1; if (relc[mid] < c0) a = mid + 1; else z = mid; }
-      lo = a;
-      a = lo; z = rc;
-      while (a < z) { int mid = (a + z) >> 1; if (relc[mid] < c1) a = mid + 1; else z = mid; }
-      hi = a;
-    }
-    for (int jj = lo; jj < hi; ++jj) {
-      const int tj = relc[jj];
-      for (int ii = jj + threadIdx.x; ii < rc; ii += blockDim.x)
-        Fs[relc[ii] + (int64_t)tj * m] += Uc[ii + (int64_t)jj * mc];
-    }
-    __syncthreads();
-  }
-}
 
 // Unblocked LDL^T of the diagonal block [j0, j0+w) of every listed front.
 __global__ void k_diag_large(DevSym S, const int* __restrict__ list, int j0, double* __restrict__ F,
@@ -833,149 +794,6 @@ __global__ void __launch_bounds__(NT, 4) k_selinv_small(DevSym S, const int* __r
   for (int e = threadIdx.x; e < m * m; e += NT) {
     const int col = e / m, row = e - col * m;
     if (row >= col) Ss[e] = Sm[row + col * ld];
-  }
-}
-
-// Large fronts: gather Sigma_RR from the parent into the trailing block.
-__global__ void k_si_gather_large(DevSym S, const int* __restrict__ list, double* __restrict__ Sg,
-                                  int64_t fstride) {
-  const int s = list[blockIdx.x], b = blockIdx.y;
-  const int k = sn_k(S, s), m = sn_m(S, s), r = m - k;
-  if (r == 0) return;
-  const int c0 = blockIdx.z * kGatherCW;
-  if (c0 >= r) return;
-  const int c1 = min(c0 + kGatherCW, r);
-  const int p = S.parent[s];
-  const int mp = sn_m(S, p);
-  const double* Sp = Sg + (int64_t)b * fstride + S.fptr[p];
-  double* Ss = Sg + (int64_t)b * fstride + S.fptr[s];
-  const int* rel = S.relx + S.rowptr[s] + k;
-  for (int jj = c0; jj < c1; ++jj)
-    for (int ii = jj + threadIdx.x; ii < r; ii += blockDim.x)
-      Ss[(k + ii) + (int64_t)(k + jj) * m] = parent_sigma(Sp, mp, rel[ii], rel[jj]);
-}
-
-// Block J = [j0, j1): for rows i in A = [j1, m):
-//   G[i,j] = sum_{l in A} Sigma[i,l] L[l,j];  X = -G L_JJ^{-1};  Sigma[i,j] = X[i,j]
-constexpr int kSiRows = 64;
-__global__ void __launch_bounds__(kSiRows) k_si_panel_large(DevSym S, const int* __restrict__ list, int jb,
-                                                            const double* __restrict__ F, double* __restrict__ Sg,
-                                                            int64_t fstride) {
-  __shared__ double Lt[kNB][kNB + 1];   // L[j0+u, j0+t]
-  __shared__ double Ls[32][kNB + 1];    // chunk of L[A, J]
-  __shared__ double Sc[32][kSiRows + 1];  // chunk of Sigma[rows, l]
-  const int s = list[blockIdx.x], b = blockIdx.y;
-  const int k = sn_k(S, s), m = sn_m(S, s);
-  const int nblk = (k + kNB - 1) / kNB;
-  if (jb >= nblk) return;
-  const int bi = nblk - 1 - jb;  // right-to-left
-  const int j0 = bi * kNB, j1 = min(k, j0 + kNB), w = j1 - j0;
-  const int r0 = j1 + blockIdx.z * kSiRows;
-  if (r0 >= m) return;
-  const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
-  double* Ss = Sg + (int64_t)b * fstride + S.fptr[s];
-  for (int e = threadIdx.x; e < kNB * kNB; e += kSiRows) {
-    int t = e / kNB, u = e - t * kNB;
-    Lt[u][t] = (u < w && t < w) ? Fs[(j0 + u) + (int64_t)(j0 + t) * m] : 0.0;
-  }
-  const int i = r0 + threadIdx.x;
-  double g[kNB];
-#pragma unroll
-  for (int t = 0; t < kNB; ++t) g[t] = 0.0;
-  for (int l0 = j1; l0 < m; l0 += 32) {
-    __syncthreads();
-    for (int e = threadIdx.x; e < 32 * kNB; e += kSiRows) {
-      int t = e / 32, l = e - t * 32;
-      Ls[l][t] = (l0 + l < m && t < w) ? Fs[(l0 + l) + (int64_t)(j0 + t) * m] : 0.0;
-    }
-    for (int e = threadIdx.x; e < 32 * kSiRows; e += kSiRows) {
-      int l = e / kSiRows, ii = e - l * kSiRows;
-      int row = r0 + ii, col = l0 + l;
-      double v = 0.0;
-      if (row < m && col < m) v = row >= col ? Ss[row + (int64_t)col * m] : Ss[col + (int64_t)row * m];
-      Sc[l][ii] = v;
-    }
-    __syncthreads();
-    const int lmax = min(32, m - l0);
-    for (int l = 0; l < lmax; ++l) {
-      const double sv = Sc[l][threadIdx.x];
-#pragma unroll
-      for (int t = 0; t < kNB; ++t) g[t] += sv * Ls[l][t];
-    }
-  }
-  if (i >= m) return;
-  // X L_JJ = -G  (unit lower L_JJ), solved right-to-left
-  double x[kNB];
-#pragma unroll
-  for (int t = kNB - 1; t >= 0; --t) {
-    if (t < w) {
-      double v = -g[t];
-#pragma unroll
-      for (int u = kNB - 1; u > 0; --u)
-        if (u > t && u < w) v -= x[u] * Lt[u][t];
-      x[t] = v;
-    } else {
-      x[t] = 0.0;
-    }
-  }
-#pragma unroll
-  for (int t = 0; t < kNB; ++t)
-    if (t < w) Ss[i + (int64_t)(j0 + t) * m] = x[t];
-}
-
-// Diagonal block of J: P[j,i] = sum_{l in A} L[l,j] Sigma[l,i]; then the
-// in-block recurrence right-to-left.
-__global__ void __launch_bounds__(256) k_si_diag_large(DevSym S, const int* __restrict__ list, int jb,
-                                                       const double* __restrict__ F, double* __restrict__ Sg,
-                                                       int64_t fstride) {
-  __shared__ double P[kNB][kNB + 1];
-  __shared__ double Sd[kNB][kNB + 1];
-  __shared__ double Ld[kNB][kNB + 1];
-  const int s = list[blockIdx.x], b = blockIdx.y;
-  const int k = sn_k(S, s), m = sn_m(S, s);
-  const int nblk = (k + kNB - 1) / kNB;
-  if (jb >= nblk) return;
-  const int bi = nblk - 1 - jb;
-  const int j0 = bi * kNB, j1 = min(k, j0 + kNB), w = j1 - j0;
-  const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
-  double* Ss = Sg + (int64_t)b * fstride + S.fptr[s];
-  // P: warp per (j,i) pair set, lanes over l
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int pr = warp; pr < w * w; pr += 8) {
-    int jj = pr / w, ii = pr - jj * w;
-    double acc = 0.0;
-    if (ii >= jj) {
-      const double* Lc = Fs + (int64_t)(j0 + jj) * m;
-      const double* Sc = Ss + (int64_t)(j0 + ii) * m;
-      for (int l = j1 + lane; l < m; l += 32) acc += Lc[l] * Sc[l];
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) P[jj][ii] = acc;
-  }
-  for (int e = threadIdx.x; e < w * w; e += 256) {
-    int c = e / w, rr = e - c * w;
-    Ld[rr][c] = Fs[(j0 + rr) + (int64_t)(j0 + c) * m];
-  }
-  __syncthreads();
-  for (int j = w - 1; j >= 0; --j) {
-    // S_ij for i in (j, w): -sum_{l in J, l>j} L_lj S_li - P[j][i]
-    for (int i = j + 1 + threadIdx.x; i < w; i += 256) {
-      double acc = P[j][i];
-      for (int l = j + 1; l < w; ++l) acc += Ld[l][j] * (l >= i ? Sd[l][i] : Sd[i][l]);
-      Sd[i][j] = -acc;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double acc = P[j][j];
-      for (int l = j + 1; l < w; ++l) acc += Ld[l][j] * Sd[l][j];
-      Sd[j][j] = 1.0 / Ld[j][j] - acc;
-    }
-    __syncthreads();
-  }
-  for (int e = threadIdx.x; e < w * w; e += 256) {
-    int c = e / w, rr = e - c * w;
-    if (rr >= c) Ss[(j0 + rr) + (int64_t)(j0 + c) * m] = Sd[rr][c];
   }
 }
 
