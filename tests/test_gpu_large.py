@@ -22,7 +22,11 @@ def test_config5_spde600_nbinomial_fit():
     s = GpuSolver(_lib.ORDER_ND)
     s.analyze(p.model.pattern)
     info = s.info()
-    # two slots of fronts and two of selected inverses per batch member (prior + posterior)
+    # two slots of fronts and two of selected inverses per batch member (prior + posterior);
+    # blocks cached by the library for reuse count as free device memory here
+    from inla_b200._lib import check, lib
+
+    check(lib().inla_release_cached_memory())
     per_point = 4 * 8 * info["front_total"]
     free = torch.cuda.mem_get_info()[0]
     admit = int(0.7 * free // per_point)
