@@ -210,14 +210,21 @@ void MultiDriver::fit(const double* theta0, const MultiFitOptions& opt, MultiFit
   out.hessian.assign((size_t)G * m * m, 0.0);
   out.status.assign(G, 0);
   out.mode_iters = iters;
-  if (opt.hessian == 1) {
+  // step per model as the single-model driver: h_g = max(1e-4, 0.05 max |theta_g|)
+  std::vector<double> hstep(G);
+  for (int g = 0; g < G; ++g) {
+    double hh = 1e-4;
+    for (int i = 0; i < m; ++i) hh = std::max(hh, 0.05 * std::fabs(x[(size_t)g * m + i]));
+    hstep[g] = hh;
+  }
+  if (opt.hessian == 1) {  // central differences of the adjoint gradient, 2m points per model
     std::vector<double> hp((size_t)2 * m * G * m), hf((size_t)2 * m * G), hg((size_t)2 * m * G * m);
     for (int i = 0; i < m; ++i)
       for (int s = 0; s < 2; ++s)
         for (int g = 0; g < G; ++g) {
           double* t = &hp[((size_t)(2 * i + s) * G + g) * m];
           for (int j = 0; j < m; ++j) t[j] = x[(size_t)g * m + j];
-          t[i] += s == 0 ? h : -h;
+          t[i] += s == 0 ? hstep[g] : -hstep[g];
         }
     evaluate(2 * m, hp.data(), true, false, hf.data(), hg.data());
     for (int g = 0; g < G; ++g) {
@@ -225,7 +232,7 @@ void MultiDriver::fit(const double* theta0, const MultiFitOptions& opt, MultiFit
       for (int i = 0; i < m; ++i)
         for (int j = 0; j < m; ++j)
           Hg[i * m + j] = -(hg[((size_t)(2 * i) * G + g) * m + j] - hg[((size_t)(2 * i + 1) * G + g) * m + j]) /
-                          (2.0 * h);
+                          (2.0 * hstep[g]);
       for (int i = 0; i < m; ++i)
         for (int j = i + 1; j < m; ++j) Hg[i * m + j] = Hg[j * m + i] = 0.5 * (Hg[i * m + j] + Hg[j * m + i]);
     }
@@ -245,12 +252,8 @@ void MultiDriver::fit(const double* theta0, const MultiFitOptions& opt, MultiFit
         }
       }
     const int K = (int)moves.size();
-    std::vector<double> hg(G), hp((size_t)K * G * m), hf((size_t)K * G);
-    for (int g = 0; g < G; ++g) {
-      double hh = 1e-4;
-      for (int i = 0; i < m; ++i) hh = std::max(hh, 0.05 * std::fabs(x[(size_t)g * m + i]));
-      hg[g] = hh;
-    }
+    const std::vector<double>& hg = hstep;
+    std::vector<double> hp((size_t)K * G * m), hf((size_t)K * G);
     for (int k = 0; k < K; ++k)
       for (int g = 0; g < G; ++g) {
         double* t = &hp[((size_t)k * G + g) * m];

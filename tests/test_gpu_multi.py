@@ -175,3 +175,48 @@ def test_config4_fit_512_models():
           f"max mode iterations {int(r['mode_iters'].max())}")
     for g in (int(np.argmin(p.truth["n"])), int(np.argmax(p.truth["n"]))):
         check_fit(r, single_fit(p, g), mm, g)
+
+
+def test_multi_gaussian_closed_form_matches_oracle():
+    """Gaussian family (closed-form mode, inference.rs:845-870) with a per-model observation
+    precision through p1scale."""
+    p = models.make_multi_problem(G=4, n_hi=600, seed=11)
+    ys = [np.log1p(y) for y in p.y]  # continuous responses on the same models
+    mm = MultiModel(p.models, p.a, ys, family="gaussian", p1=1.0, max_batch=2)
+    th = thetas_for(p, np.random.default_rng(5), 2)
+    c = coefs_of(th)
+    prec = np.array([[2.0, 5.0, 1.5, 3.0], [4.0, 1.0, 2.5, 6.0]])
+    out = mm.eval(c, p1scale=prec, variances=True)
+    assert np.all(out["status"] == 0) and np.all(out["iters"] == 1)
+    for b in range(2):
+        for g in range(4):
+            r = O.laplace(p.models[g].matrix(c[b, g]), p.a[g], "gaussian", ys[g], p1=prec[b, g], want_var=True,
+                          perm=chain_perm(p.truth["n"][g]))
+            assert abs(out["logdet_post"][b, g] - r["logdet_post"]) <= RT_LD * abs(r["logdet_post"])
+            assert abs(out["mlik"][b, g] - r["mlik"]) <= RT_LD * abs(r["logdet_post"])
+            assert rel(mm.split(out["x"][b])[g], r["x"]) < RT_X
+            assert rel(mm.split(out["var"][b])[g], r["var"]) < RT_X
+
+
+def test_multi_fit_python_map_and_gradient_hessian(small):
+    """inla_multi_fit with a Python theta map (per-model callback) and the FD-of-gradient
+    Hessian against the single-model fits with the same options."""
+    from inla_b200.laplace import LaplaceModel
+    from inla_b200.multi import AR1_IID_PRIORS
+
+    p, mm = small
+
+    def tmap_g(g, t):
+        cc, dc = models.ar1_iid_coefs(t)
+        return cc, dc, 1.0, np.zeros(3)
+
+    r = mm.fit(np.zeros((mm.G, 3)), theta_map=tmap_g, hessian="grad")
+    assert np.all(r["status"] == 0)
+    for g in (1, mm.G - 2):
+        lm = LaplaceModel(p.models[g], a=p.a[g], family="poisson", y=p.y[g], max_batch=25)
+        s = lm.fit(np.zeros(3), theta_map=lambda t: tmap_g(g, t), priors=AR1_IID_PRIORS, mode_search="newton",
+                   batched=True, hessian="grad")
+        np.testing.assert_allclose(r["mode"][g], s["mode"], atol=1e-6)
+        np.testing.assert_allclose(r["hessian"][g], s["hessian"], rtol=1e-5, atol=1e-6)
+        assert rel(mm.split(r["mean"])[g], s["mean"]) < 1e-6
+        assert abs(r["mlik"][g] - s["mlik"]) < 1e-6 * abs(s["mlik"])
