@@ -171,3 +171,26 @@ def test_ccd_design_weights():
     assert abs(w.sum() - 1.0) < 1e-12
     z, w = O.ccd_design(4, 1.0)
     assert z.shape == (25, 4)
+
+
+def test_ccd_design_points_reference():
+    """integration.rs:328-347: f0 = 2.5 gives 3 / 9 / 15 points for m = 1 / 2 / 3 with weights
+    summing to 1; for m = 1 the points are 0, +2.5, -2.5."""
+    z, w = O.ccd_design(1, 2.5)
+    assert z.shape == (3, 1)
+    assert z[0, 0] == 0.0 and abs(z[1, 0] - 2.5) < 1e-12 and abs(z[2, 0] + 2.5) < 1e-12
+    assert abs(w.sum() - 1.0) < 1e-12
+    for m, npts in ((2, 9), (3, 15)):
+        z, w = O.ccd_design(m, 2.5)
+        assert z.shape == (npts, m)
+        assert abs(w.sum() - 1.0) < 1e-12
+
+
+def test_grid_design_points_reference():
+    """integration.rs:349-369: spherical Gaussian log-density, step 1, threshold 2: five
+    points for m = 1; for m = 2 every kept point has z1^2 + z2^2 <= 4."""
+    f = lambda z: -0.5 * sum(v * v for v in z)
+    z1, _ = O.grid_design(1, 1.0, 2.0, f)
+    assert len(z1) == 5
+    z2, _ = O.grid_design(2, 1.0, 2.0, f)
+    assert len(z2) > 0 and all(p[0] ** 2 + p[1] ** 2 <= 4.0001 for p in z2)
