@@ -314,6 +314,22 @@ int inla_fit(inla_laplace* h, int m, const double* theta0, inla_theta_map_fn map
              void* user, const inla_fit_options* opt, double* mode, double* hessian, double* latent_mean,
              double* latent_var, double* node_theta, double* node_weight, double* info);
 
+/* Linear predictor of the last inla_fit on h: mixture mean and variance of eta = A x
+ * (predictor_means / predictor_variances of the reference's result, inference.rs:1451-1466),
+ * length nobs each (either pointer may be NULL). INLA_ERR_INVALID before the first fit. */
+int inla_fit_predictor(inla_laplace* h, double* pred_mean, double* pred_var);
+
+/* Host-only mixture of the linear predictor over K integration nodes (no device use):
+ * per node eta_k = A x_k (matvec_csc, design.rs:52-70: columns with x_kj = 0 skipped) and
+ * eta-var_k = sum_j A_ij^2 var_kj (predictor_variances_diag, design.rs:198-210), then
+ * mean = sum_k w_k eta_k and var = sum_k w_k (eta-var_k + (eta_k - mean)^2)
+ * (inference.rs:1451-1466). A is nobs x n in CSR, each row summed in stored order
+ * (ascending columns give the reference's order); a_rowptr NULL means eta = x (nobs = n).
+ * weight: [K] normalised node weights; cond_mean, cond_var: [K][n]; pred_*: [nobs]. */
+int inla_predictor_moments(int64_t nobs, int64_t n, const int64_t* a_rowptr, const int64_t* a_colidx,
+                           const double* a_vals, int K, const double* weight, const double* cond_mean,
+                           const double* cond_var, double* pred_mean, double* pred_var);
+
 /* ------------------------------------------------------------------------
  * Dense LDL^T + log|Q| + solve that allocates no device memory.
  * No counterpart in the reference: it exists for host programs that embed

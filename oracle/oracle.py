@@ -404,11 +404,62 @@ def grid_design(m, step, threshold, evaluator):
     return np.array(pts), np.ones(len(pts))
 
 
-def integrate(mode, hessian, eval_node, f0=1.0, strategy="ccd"):
+def matvec_csc(a, x):
+    """design.rs:52-70: y = A x column by column, columns with x_j == 0 skipped."""
+    a = sp.csc_matrix(a)
+    y = [0.0] * a.shape[0]
+    for j in range(a.shape[1]):
+        xv = float(x[j])
+        if xv == 0.0:
+            continue
+        for p in range(a.indptr[j], a.indptr[j + 1]):
+            y[a.indices[p]] += float(a.data[p]) * xv
+    return np.array(y)
+
+
+def predictor_variances_diag(a, var_x):
+    """design.rs:198-210: sum_j A_ij^2 var_j, column by column."""
+    a = sp.csc_matrix(a)
+    out = [0.0] * a.shape[0]
+    for j in range(a.shape[1]):
+        v = float(var_x[j])
+        for p in range(a.indptr[j], a.indptr[j + 1]):
+            val = float(a.data[p])
+            out[a.indices[p]] += val * val * v
+    return np.array(out)
+
+
+def mixture_moments(weights, cond_mean, cond_var):
+    """inference.rs:1436-1466: mean = sum_k w_k m_k, var = sum_k w_k (v_k + (m_k - mean)^2),
+    k ascending per element."""
+    K = len(weights)
+    cm, cv = np.asarray(cond_mean, dtype=float), np.asarray(cond_var, dtype=float)
+    mean = np.zeros(cm.shape[1])
+    for k in range(K):
+        mean = mean + weights[k] * cm[k]
+    var = np.zeros(cm.shape[1])
+    for k in range(K):
+        d = cm[k] - mean
+        var = var + weights[k] * (cv[k] + d * d)
+    return mean, var
+
+
+def predictor_moments(a, weights, cond_mean, cond_var):
+    """inference.rs:1370-1384 (eta = A x*, eta-var = predictor_variances_diag per node; x* and
+    its variances themselves when there is no A) and 1451-1466 (their mixture)."""
+    if a is None:
+        return mixture_moments(weights, cond_mean, cond_var)
+    eta = [matvec_csc(a, m) for m in cond_mean]
+    ev = [predictor_variances_diag(a, v) for v in cond_var]
+    return mixture_moments(weights, eta, ev)
+
+
+def integrate(mode, hessian, eval_node, f0=1.0, strategy="ccd", a=None):
     """run_inla_inference_a_cancellable node map + aggregation (inference.rs:1262-1466).
 
     ``eval_node(theta) -> (x_star, variances, log_post)``; ``strategy`` "ccd" (f0) or
-    "grid" (step f0, threshold 4.0, evaluator = log_post at the mapped node).
+    "grid" (step f0, threshold 4.0, evaluator = log_post at the mapped node). With the
+    projector ``a`` the result also holds the predictor moments ("pred_mean", "pred_var").
     """
     m = len(mode)
     sigma = np.linalg.inv(-np.asarray(hessian))
@@ -437,8 +488,11 @@ def integrate(mode, hessian, eval_node, f0=1.0, strategy="ccd"):
     vars_ = np.stack([r[1] for r in res])
     mean = nw @ means
     var = nw @ (vars_ + (means - mean) ** 2)
-    return {"thetas": np.array(thetas), "weights": nw, "mean": mean, "var": var, "log_posts": lps,
-            "mlik": mx + math.log(abs(sw))}
+    out = {"thetas": np.array(thetas), "weights": nw, "mean": mean, "var": var, "log_posts": lps,
+           "mlik": mx + math.log(abs(sw))}
+    if a is not None:
+        out["pred_mean"], out["pred_var"] = predictor_moments(a, nw, means, vars_)
+    return out
 
 
 # ---------------------------------------------------------------------------

@@ -4,6 +4,7 @@
 #include <cstring>
 #include <memory>
 
+#include "aggregate.hpp"
 #include "capi_common.hpp"
 #include "driver.hpp"
 #include "inla_b200.h"
@@ -15,6 +16,8 @@ struct inla_laplace {
   std::unique_ptr<LaplaceEngine> eng;
   LaplaceSpec spec;  // the caller's model, before any constraint augmentation
   int max_batch = 0;
+  std::vector<double> pred_mean, pred_var;  // linear predictor moments of the last inla_fit
+  bool fitted = false;
 };
 
 namespace {
@@ -323,6 +326,41 @@ int inla_fit(inla_laplace* h, int m, const double* theta0, inla_theta_map_fn map
       info[4] = R.mode_iters;
       info[5] = K;
     }
+    h->pred_mean = std::move(R.pred_mean);
+    h->pred_var = std::move(R.pred_var);
+    h->fitted = true;
+    return INLA_OK;
+  } catch (...) {
+    return map_exception();
+  }
+}
+
+int inla_fit_predictor(inla_laplace* h, double* pred_mean, double* pred_var) {
+  if (!h || !h->fitted) return fail(INLA_ERR_INVALID, "inla_fit_predictor: no fit on this handle");
+  const size_t bytes = sizeof(double) * h->pred_mean.size();
+  if (pred_mean) std::memcpy(pred_mean, h->pred_mean.data(), bytes);
+  if (pred_var) std::memcpy(pred_var, h->pred_var.data(), bytes);
+  return INLA_OK;
+}
+
+int inla_predictor_moments(int64_t nobs, int64_t n, const int64_t* a_rowptr, const int64_t* a_colidx,
+                           const double* a_vals, int K, const double* weight, const double* cond_mean,
+                           const double* cond_var, double* pred_mean, double* pred_var) {
+  try {
+    if (n < 0 || K < 1 || !weight || !cond_mean || !cond_var || !pred_mean || !pred_var)
+      return fail(INLA_ERR_INVALID, "inla_predictor_moments: invalid argument");
+    if (!a_rowptr) {
+      if (nobs != n) return fail(INLA_ERR_DIM_MISMATCH, "inla_predictor_moments: eta = x needs nobs == n");
+    } else {
+      if (nobs < 0 || !a_colidx || !a_vals || a_rowptr[0] != 0)
+        return fail(INLA_ERR_INVALID, "inla_predictor_moments: invalid CSR");
+      for (int64_t r = 0; r < nobs; ++r)
+        if (a_rowptr[r + 1] < a_rowptr[r]) return fail(INLA_ERR_INVALID, "inla_predictor_moments: invalid CSR");
+      for (int64_t p = 0; p < a_rowptr[nobs]; ++p)
+        if (a_colidx[p] < 0 || a_colidx[p] >= n)
+          return fail(INLA_ERR_DIM_MISMATCH, "inla_predictor_moments: column out of range");
+    }
+    predictor_moments(nobs, n, a_rowptr, a_colidx, a_vals, K, weight, cond_mean, cond_var, pred_mean, pred_var);
     return INLA_OK;
   } catch (...) {
     return map_exception();

@@ -8,6 +8,7 @@
 #include <limits>
 #include <stdexcept>
 
+#include "aggregate.hpp"
 #include "driver.hpp"
 
 namespace inla {
@@ -689,16 +690,15 @@ void InlaDriver::fit(const double* theta0, const FitOptions& opt, FitResult& out
   for (int k = 0; k < K; ++k) nw[k] = zw[k] * dens[k] / sw;
   out.latent_mean.assign(n, 0.0);
   out.latent_var.assign(n, 0.0);
-  for (int64_t i = 0; i < n; ++i) {
-    double mi = 0.0;
-    for (int k = 0; k < K; ++k) mi += nw[k] * means[(size_t)k * n + i];
-    double vi = 0.0;
-    for (int k = 0; k < K; ++k) {
-      const double d = means[(size_t)k * n + i] - mi;
-      vi += nw[k] * (vars[(size_t)k * n + i] + d * d);
-    }
-    out.latent_mean[i] = mi;
-    out.latent_var[i] = vi;
+  mixture_moments(K, n, nw.data(), means.data(), vars.data(), out.latent_mean.data(), out.latent_var.data());
+  // linear predictor eta = A x* per node and its diagonal variance (inference.rs:1370-1384, 1451-1466)
+  {
+    const LaplaceSpec& S = eng_.spec();
+    const int64_t nobs = S.identity_a ? n : S.nobs;
+    out.pred_mean.assign(nobs, 0.0);
+    out.pred_var.assign(nobs, 0.0);
+    predictor_moments(nobs, n, S.identity_a ? nullptr : S.acp.data(), S.aci.data(), S.av.data(), K, nw.data(),
+                      means.data(), vars.data(), out.pred_mean.data(), out.pred_var.data());
   }
   out.mlik = mx + std::log(std::fabs(sw));
   out.node_theta = thetas;

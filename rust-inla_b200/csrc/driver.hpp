@@ -39,6 +39,7 @@ struct FitOptions {
 
 struct FitResult {
   std::vector<double> mode, hessian, latent_mean, latent_var, node_theta, node_weight, node_logpost;
+  std::vector<double> pred_mean, pred_var;  // linear predictor eta = A x: mixture mean and variance
   double mlik = 0.0;
   int n_evals = 0, n_batches = 0, mode_iters = 0;
   double seconds = 0.0;

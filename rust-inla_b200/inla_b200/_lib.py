@@ -108,6 +108,8 @@ SIGNATURES = [
     ("inla_prior_log_density", C.c_double, [P, C.c_int, DP, C.c_int, DP]),
     ("inla_log_prior_set", C.c_double, [DP, C.c_int, DP, P]),
     ("inla_fit", C.c_int, [P, C.c_int, DP, P, P, P, P, DP, DP, DP, DP, DP, DP, DP]),
+    ("inla_fit_predictor", C.c_int, [P, DP, DP]),
+    ("inla_predictor_moments", C.c_int, [I64, I64, LP, LP, DP, C.c_int, DP, DP, DP, DP, DP]),
     ("inla_theta_map_spde", C.c_int, [DP, C.c_int, DP, DP, DP, DP, P]),
     ("inla_dense_ldlt_solve_noalloc", C.c_int, [C.c_int, P, P, P, P, P, P]),
 ]

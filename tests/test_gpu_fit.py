@@ -45,7 +45,7 @@ def test_integration_parity_at_fixed_nodes(problem):
         lp = O.loggamma_log_dens(theta[0], 1.0, 5e-5) + O.pc_spde_log_dens(theta[1], theta[2], 1.0, 0.05, 1.0, 0.01)
         return lr["x"], lr["var"], lr["mlik"] + lp
 
-    ref = O.integrate(r["mode"], r["hessian"], node, f0=1.0)
+    ref = O.integrate(r["mode"], r["hessian"], node, f0=1.0, a=p.a)
     # node sets agree as sets (eigenvector sign conventions may permute them)
     got = sorted(map(tuple, np.round(r["node_theta"], 9)))
     exp = sorted(map(tuple, np.round(ref["thetas"], 9)))
@@ -54,6 +54,10 @@ def test_integration_parity_at_fixed_nodes(problem):
     assert rel(r["mean"], ref["mean"]) < 1e-8
     assert rel(r["var"], ref["var"]) < 1e-8
     assert abs(r["mlik"] - ref["mlik"]) < 1e-8 * abs(ref["mlik"])
+    # linear predictor eta = A x (inference.rs:1451-1466): its mixture mean is A times the latent one
+    assert rel(r["pred_mean"], ref["pred_mean"]) < 1e-8
+    assert rel(r["pred_var"], ref["pred_var"]) < 1e-8
+    assert rel(r["pred_mean"], p.a @ r["mean"]) < 1e-12
 
 
 @pytest.mark.parametrize("search", ["bfgs", "newton"])
