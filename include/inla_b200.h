@@ -319,6 +319,39 @@ int inla_fit(inla_laplace* h, int m, const double* theta0, inla_theta_map_fn map
  * length nobs each (either pointer may be NULL). INLA_ERR_INVALID before the first fit. */
 int inla_fit_predictor(inla_laplace* h, double* pred_mean, double* pred_var);
 
+/* Model-selection criteria of the last inla_fit on h, as the reference computes them at the
+ * end of a fit (inference.rs:1470-1514; model_selection.rs): DIC (compute_dic, 101-150) and
+ * WAIC (compute_waic, 152-211) from the per-node predictors, CPO / PIT (compute_cpo_pit,
+ * 222-325, with the failure heuristic check_cpo_failure_for_obs, 327-396) from the predictors
+ * and their variances, all with the observations rebuilt at the mode (the theta map's p1 scale
+ * there) and D(theta*) at the node with the smallest |z|. what: INLA_MS_* bits (criteria not
+ * asked for are NaN). crit: [8] = {DIC, mean deviance, DIC effective parameters, WAIC, lppd,
+ * WAIC effective parameters, Gaussian-approximation log marginal likelihood
+ * (compute_marginal_log_lik_gaussian, model_selection.rs:25-73; NaN when -H is not positive
+ * definite), CPO failures}; cpo, pit: [nobs], NaN where the reference gives None (either may be
+ * NULL). INLA_ERR_INVALID (with the reference's message) where the reference returns an error:
+ * a likelihood that cannot be evaluated, a non-finite WAIC predictive density. */
+enum { INLA_MS_DIC = 1, INLA_MS_WAIC = 2, INLA_MS_CPO = 4, INLA_MS_ALL = 7 };
+int inla_fit_model_selection(inla_laplace* h, int what, double* crit, double* cpo, double* pit);
+
+/* Host-only: the same criteria from a caller's node results (crit[6] is NaN). family: as in
+ * inla_laplace_create (0 gaussian, 1 poisson, 2 binomial, 3 negative binomial); y, p1, p2: [nobs] (p1 gaussian precision / poisson exposure / binomial trials /
+ * nb size, p2 nb exposure; NULL = 1); weight: [K] normalised; mode_index: the node of D(theta*);
+ * cond_eta, cond_eta_var: [K][nobs]. */
+int inla_model_selection(int family, int64_t nobs, const double* y, const double* p1, const double* p2, int K,
+                         const double* weight, int mode_index, const double* cond_eta, const double* cond_eta_var,
+                         int what, double* crit, double* cpo, double* pit);
+/* compute_marginal_log_lik_gaussian (model_selection.rs:25-73): log_post_mode + m/2 log(2 pi)
+ * - 1/2 log det(neg_hessian), neg_hessian row-major m x m; INLA_ERR_NOT_PD when it is not
+ * positive definite. */
+int inla_mlik_gaussian(double log_post_mode, int m, const double* neg_hessian, double* out);
+/* observation_cdf (model_selection.rs:398-448): F(y | eta, variance) of one observation;
+ * INLA_ERR_INVALID where the reference gives None (negative binomial, invalid rate). */
+int inla_observation_cdf(int family, double y, double p1, double eta, double variance, double* out);
+/* check_cpo_failure_for_obs (model_selection.rs:327-396): 1 when the CPO of this observation is
+ * flagged unreliable at posterior mean mu and variance var of its predictor, else 0. */
+int inla_cpo_failure(int family, double y, double p1, double p2, double mu, double var);
+
 /* Host-only mixture of the linear predictor over K integration nodes (no device use):
  * per node eta_k = A x_k (matvec_csc, design.rs:52-70: columns with x_kj = 0 skipped) and
  * eta-var_k = sum_j A_ij^2 var_kj (predictor_variances_diag, design.rs:198-210), then

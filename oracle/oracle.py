@@ -496,6 +496,221 @@ def integrate(mode, hessian, eval_node, f0=1.0, strategy="ccd", a=None):
 
 
 # ---------------------------------------------------------------------------
+# model selection (crates/inla_stats/src/model_selection.rs)
+# ---------------------------------------------------------------------------
+
+CPO_DIFF = 3.0  # model_selection.rs:7
+
+
+def mlik_gaussian(log_post_mode, neg_hessian, m):
+    """model_selection.rs:25-73: in-place Cholesky of -H (row-major), None when not PD."""
+    if m == 0:
+        return log_post_mode
+    a = [float(v) for v in np.ravel(neg_hessian)]
+    log_det = 0.0
+    for j in range(m):
+        for k in range(j):
+            ljk = a[j * m + k]
+            a[j * m + j] -= ljk * ljk
+        if a[j * m + j] <= 0.0:
+            return None
+        log_det += math.log(a[j * m + j])
+        djj = math.sqrt(a[j * m + j])
+        a[j * m + j] = djj
+        for i in range(j + 1, m):
+            for k in range(j):
+                a[i * m + j] -= a[i * m + k] * a[j * m + k]
+            a[i * m + j] /= djj
+    return log_post_mode + 0.5 * m * math.log(2.0 * math.pi) - 0.5 * log_det
+
+
+def _lik_or_none(family, eta, y, p1, p2):
+    try:
+        return eval_lik(family, eta, y, p1, p2)
+    except OracleError:
+        return None
+
+
+def compute_dic(family, y, p1, p2, cond_eta, weights, mode_index):
+    """model_selection.rs:82-150; None where the reference returns Err."""
+    dev = []
+    for eta in cond_eta:
+        s = 0.0
+        for i in range(len(y)):
+            e = _lik_or_none(family, eta[i], y[i], p1[i], p2[i])
+            if e is None:
+                return None
+            s += e[0]
+        dev.append(-2.0 * s)
+    mean_dev = 0.0
+    for k in range(len(dev)):
+        mean_dev += weights[k] * dev[k]
+    p_eff = mean_dev - dev[mode_index]
+    return {"dic": mean_dev + p_eff, "mean_deviance": mean_dev, "p_eff": p_eff}
+
+
+def compute_waic(family, y, p1, p2, cond_eta, weights):
+    """model_selection.rs:152-211; None where the reference returns Err."""
+    lppd = p_waic = 0.0
+    for i in range(len(y)):
+        lls = []
+        for eta in cond_eta:
+            e = _lik_or_none(family, eta[i], y[i], p1[i], p2[i])
+            if e is None:
+                return None
+            lls.append(e[0])
+        mx = -math.inf
+        for v in lls:
+            mx = v if math.isnan(mx) else (mx if math.isnan(v) else max(mx, v))
+        sw = ml = 0.0
+        for k, v in enumerate(lls):
+            sw += weights[k] * math.exp(v - mx)
+            ml += weights[k] * v
+        if not (math.isfinite(sw) and sw > 0.0):
+            return None
+        lppd += mx + math.log(sw)
+        var = 0.0
+        for k, v in enumerate(lls):
+            d = v - ml
+            var += weights[k] * d * d
+        p_waic += var
+    return {"waic": -2.0 * (lppd - p_waic), "lppd": lppd, "p_eff": p_waic}
+
+
+def normal_cdf(x):
+    """model_selection.rs:450-467 (Abramowitz & Stegun 7.1.26)."""
+    a1, a2, a3, a4, a5, p = 0.254829592, -0.284496736, 1.421413741, -1.453152027, 1.061405429, 0.3275911
+    sign = -1.0 if x < 0.0 else 1.0
+    ax = abs(x)
+    t = 1.0 / (1.0 + p * ax)
+    y = 1.0 - (((((a5 * t + a4) * t) + a3) * t + a2) * t + a1) * t * math.exp(-ax * ax / 2.0)
+    return 0.5 * (1.0 + sign * y)
+
+
+def poisson_cdf(lam, k):
+    """model_selection.rs:470-486."""
+    if lam <= 0.0:
+        return 1.0
+    cdf, log_pmf = 0.0, -lam
+    for j in range(k + 1):
+        cdf += math.exp(log_pmf)
+        if j < k:
+            log_pmf += math.log(lam) - math.log(float(j + 1))
+    return min(cdf, 1.0)
+
+
+def binomial_cdf(n, p, k):
+    """model_selection.rs:488-504 with the reference's Lanczos log-gamma."""
+    if p <= 0.0:
+        return 1.0
+    if p >= 1.0:
+        return 1.0 if k >= n else 0.0
+    cdf = 0.0
+    for j in range(k + 1):
+        lc = log_gamma(n + 1.0) - log_gamma(j + 1.0) - log_gamma(float(n - j) + 1.0)
+        cdf += math.exp(lc + j * math.log(p) + (n - j) * math.log(1.0 - p))
+    return min(cdf, 1.0)
+
+
+def _logistic(x):
+    if x >= 0.0:
+        z = math.exp(-x)
+        return 1.0 / (1.0 + z)
+    z = math.exp(x)
+    return z / (1.0 + z)
+
+
+def observation_cdf(family, y, p1, eta, variance):
+    """model_selection.rs:398-448; None where the reference gives None."""
+    family = FAMILIES.get(family, family)
+    if family == 0:
+        tv = 1.0 / p1 + variance
+        if tv <= 0.0:
+            return None
+        return normal_cdf((y - eta) / math.sqrt(tv))
+    if family == 1:
+        lam = p1 * math.exp(eta)
+        if lam < 0.0 or not math.isfinite(lam):
+            return None
+        yi = math.floor(y)
+        return 0.0 if yi < 0 else poisson_cdf(lam, int(yi))
+    if family == 2:
+        prob = _logistic(eta)
+        n = int(p1) if p1 > 0 else 0
+        yi = math.floor(y)
+        return 0.0 if yi < 0 else binomial_cdf(n, prob, min(int(yi), n))
+    return None
+
+
+def cpo_failure(family, y, p1, p2, mu, var):
+    """check_cpo_failure_for_obs (model_selection.rs:327-396)."""
+    if var <= 0.0 or not math.isfinite(var):
+        return True
+    e = _lik_or_none(family, mu, y, p1, p2)
+    if e is None:
+        return True
+    g, c = e[1], -e[2]
+    tau_loo = 1.0 / var - c
+    if tau_loo <= 0.0 or not math.isfinite(tau_loo):
+        return True
+    var_loo = 1.0 / tau_loo
+    std_loo = math.sqrt(var_loo)
+    mu_loo = var_loo * (mu / var - c * mu + g)
+    ld = []
+    for step in (-3.0, -1.5, 0.0, 1.5, 3.0):
+        x = mu_loo + step * std_loo
+        prior = -0.5 * (x - mu) * (x - mu) / var
+        e = _lik_or_none(family, x, y, p1, p2)
+        if e is None:
+            return True
+        ld.append(prior + e[0])
+    inc = all(not (ld[j] < ld[j - 1]) for j in range(1, 5))
+    dec = all(not (ld[j] > ld[j - 1]) for j in range(1, 5))
+    if inc or dec:
+        return True
+    mx = max(ld)
+    return mx - ld[0] < CPO_DIFF or mx - ld[4] < CPO_DIFF
+
+
+def compute_cpo_pit(family, y, p1, p2, cond_eta, cond_var, weights):
+    """model_selection.rs:222-325: (cpo, pit, n_failures) with None entries."""
+    n, K = len(y), len(weights)
+    cpo, pit, nf = [None] * n, [None] * n, 0
+    for i in range(n):
+        if any(cpo_failure(family, y[i], p1[i], p2[i], cond_eta[k][i], cond_var[k][i]) for k in range(K)):
+            nf += 1
+            continue
+        lls = []
+        for k in range(K):
+            e = _lik_or_none(family, cond_eta[k][i], y[i], p1[i], p2[i])
+            if e is None:
+                break
+            lls.append(e[0])
+        if len(lls) < K or len(lls) < 2:
+            nf += 1
+            continue
+        max_neg = max(-v for v in lls)
+        inv = 0.0
+        for k in range(K):
+            inv += weights[k] * math.exp(-lls[k] - max_neg)
+        inv *= math.exp(max_neg)
+        if not math.isfinite(inv) or inv <= 0.0:
+            nf += 1
+            continue
+        cpo[i] = 1.0 / inv
+        ps, ok = 0.0, True
+        for k in range(K):
+            f = observation_cdf(family, y[i], p1[i], cond_eta[k][i], cond_var[k][i])
+            if f is None:
+                ok = False
+                break
+            ps += weights[k] * f
+        if ok and math.isfinite(ps):
+            pit[i] = min(max(ps, 0.0), 1.0)
+    return cpo, pit, nf
+
+
+# ---------------------------------------------------------------------------
 # hyperpriors (crates/inla_stats/src/priors.rs) and the SPDE theta map
 # ---------------------------------------------------------------------------
 

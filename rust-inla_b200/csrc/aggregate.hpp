@@ -14,6 +14,12 @@ namespace inla {
 void mixture_moments(int K, int64_t len, const double* w, const double* cmean, const double* cvar, double* mean,
                      double* var);
 
+// Per node eta_k = A x_k (columns with x_kj == 0 skipped, as matvec_csc does) and
+// eta-var_k = sum_j A_ij^2 var_kj, each summed in the row's stored order. A: nobs x n in CSR
+// (acp == nullptr: eta = x, nobs == n). cmean, cvar: [K][n]; eta, eta_var: [K][nobs].
+void project_nodes(int64_t nobs, int64_t n, const int64_t* acp, const int64_t* aci, const double* av, int K,
+                   const double* cmean, const double* cvar, double* eta, double* eta_var);
+
 // Linear-predictor moments: per node eta_k = A x_k (columns with x_kj == 0 skipped, as
 // matvec_csc does) and eta-var_k = sum_j A_ij^2 var_kj, each summed in the row's stored order
 // (ascending columns give the reference's order), then mixed as mixture_moments does.

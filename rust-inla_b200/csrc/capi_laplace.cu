@@ -7,6 +7,7 @@
 #include "aggregate.hpp"
 #include "capi_common.hpp"
 #include "driver.hpp"
+#include "model_select.hpp"
 #include "inla_b200.h"
 
 using namespace inla;
@@ -16,7 +17,10 @@ struct inla_laplace {
   std::unique_ptr<LaplaceEngine> eng;
   LaplaceSpec spec;  // the caller's model, before any constraint augmentation
   int max_batch = 0;
-  std::vector<double> pred_mean, pred_var;  // linear predictor moments of the last inla_fit
+  // from the last inla_fit: linear predictor moments and the model-selection inputs
+  std::vector<double> pred_mean, pred_var, cond_eta, cond_eta_var, node_weight;
+  int mode_index = 0;
+  double p1scale_mode = 1.0, mlik_gaussian = 0.0;
   bool fitted = false;
 };
 
@@ -328,6 +332,12 @@ int inla_fit(inla_laplace* h, int m, const double* theta0, inla_theta_map_fn map
     }
     h->pred_mean = std::move(R.pred_mean);
     h->pred_var = std::move(R.pred_var);
+    h->cond_eta = std::move(R.cond_eta);
+    h->cond_eta_var = std::move(R.cond_eta_var);
+    h->node_weight = R.node_weight;
+    h->mode_index = R.mode_index;
+    h->p1scale_mode = R.p1scale_mode;
+    h->mlik_gaussian = R.mlik_gaussian;
     h->fitted = true;
     return INLA_OK;
   } catch (...) {
@@ -341,6 +351,90 @@ int inla_fit_predictor(inla_laplace* h, double* pred_mean, double* pred_var) {
   if (pred_mean) std::memcpy(pred_mean, h->pred_mean.data(), bytes);
   if (pred_var) std::memcpy(pred_var, h->pred_var.data(), bytes);
   return INLA_OK;
+}
+
+namespace {
+
+void fill_crit(const ModelSelection& ms, double mlik_g, double* crit, double* cpo, double* pit, int64_t nobs,
+               int what) {
+  if (crit) {
+    crit[0] = ms.dic;
+    crit[1] = ms.mean_deviance;
+    crit[2] = ms.dic_p_eff;
+    crit[3] = ms.waic;
+    crit[4] = ms.lppd;
+    crit[5] = ms.waic_p_eff;
+    crit[6] = mlik_g;
+    crit[7] = (what & MS_CPO) ? (double)ms.cpo_failures : NAN;
+  }
+  for (int64_t i = 0; i < nobs; ++i) {
+    if (cpo) cpo[i] = (what & MS_CPO) ? ms.cpo[i] : NAN;
+    if (pit) pit[i] = (what & MS_CPO) ? ms.pit[i] : NAN;
+  }
+}
+
+}  // namespace
+
+int inla_fit_model_selection(inla_laplace* h, int what, double* crit, double* cpo, double* pit) {
+  try {
+    if (!h || !h->fitted) return fail(INLA_ERR_INVALID, "inla_fit_model_selection: no fit on this handle");
+    const LaplaceSpec& S = h->spec;
+    ObsView obs;
+    obs.family = S.family;
+    obs.nobs = S.nobs;
+    obs.y = S.y.data();
+    obs.p1 = S.p1.empty() ? nullptr : S.p1.data();
+    obs.p2 = S.p2.empty() ? nullptr : S.p2.data();
+    obs.p1scale = h->p1scale_mode;
+    ModelSelection ms;
+    const std::string err = model_selection(obs, (int)h->node_weight.size(), h->node_weight.data(), h->mode_index,
+                                            h->cond_eta.data(), h->cond_eta_var.data(), what, ms);
+    if (!err.empty()) return fail(INLA_ERR_INVALID, err.c_str());
+    fill_crit(ms, h->mlik_gaussian, crit, cpo, pit, S.nobs, what);
+    return INLA_OK;
+  } catch (...) {
+    return map_exception();
+  }
+}
+
+int inla_model_selection(int family, int64_t nobs, const double* y, const double* p1, const double* p2, int K,
+                         const double* weight, int mode_index, const double* cond_eta, const double* cond_eta_var,
+                         int what, double* crit, double* cpo, double* pit) {
+  try {
+    if (family < 0 || family > 3 || nobs < 0 || (nobs > 0 && !y) || K < 1 || !weight || mode_index < 0 ||
+        mode_index >= K || (nobs > 0 && (!cond_eta || !cond_eta_var)))
+      return fail(INLA_ERR_INVALID, "inla_model_selection: invalid argument");
+    ObsView obs;
+    obs.family = family;
+    obs.nobs = nobs;
+    obs.y = y;
+    obs.p1 = p1;
+    obs.p2 = p2;
+    ModelSelection ms;
+    const std::string err = model_selection(obs, K, weight, mode_index, cond_eta, cond_eta_var, what, ms);
+    if (!err.empty()) return fail(INLA_ERR_INVALID, err.c_str());
+    fill_crit(ms, NAN, crit, cpo, pit, nobs, what);
+    return INLA_OK;
+  } catch (...) {
+    return map_exception();
+  }
+}
+
+int inla_mlik_gaussian(double log_post_mode, int m, const double* neg_hessian, double* out) {
+  if (m < 0 || (m > 0 && !neg_hessian) || !out) return fail(INLA_ERR_INVALID, "inla_mlik_gaussian: invalid argument");
+  if (!mlik_gaussian(log_post_mode, m, neg_hessian, *out))
+    return fail(INLA_ERR_NOT_PD, "negative Hessian is not positive-definite");
+  return INLA_OK;
+}
+
+int inla_observation_cdf(int family, double y, double p1, double eta, double variance, double* out) {
+  if (!out) return fail(INLA_ERR_INVALID, "inla_observation_cdf: invalid argument");
+  return observation_cdf(family, y, p1, eta, variance, *out) ? INLA_OK
+                                                              : fail(INLA_ERR_INVALID, "no CDF for this family");
+}
+
+int inla_cpo_failure(int family, double y, double p1, double p2, double mu, double var) {
+  return cpo_failure(family, y, p1, p2, mu, var) ? 1 : 0;
 }
 
 int inla_predictor_moments(int64_t nobs, int64_t n, const int64_t* a_rowptr, const int64_t* a_colidx,

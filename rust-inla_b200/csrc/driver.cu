@@ -10,6 +10,7 @@
 
 #include "aggregate.hpp"
 #include "driver.hpp"
+#include "model_select.hpp"
 
 namespace inla {
 
@@ -695,10 +696,35 @@ void InlaDriver::fit(const double* theta0, const FitOptions& opt, FitResult& out
   {
     const LaplaceSpec& S = eng_.spec();
     const int64_t nobs = S.identity_a ? n : S.nobs;
+    out.cond_eta.resize((size_t)K * nobs);
+    out.cond_eta_var.resize((size_t)K * nobs);
+    project_nodes(nobs, n, S.identity_a ? nullptr : S.acp.data(), S.aci.data(), S.av.data(), K, means.data(),
+                  vars.data(), out.cond_eta.data(), out.cond_eta_var.data());
     out.pred_mean.assign(nobs, 0.0);
     out.pred_var.assign(nobs, 0.0);
-    predictor_moments(nobs, n, S.identity_a ? nullptr : S.acp.data(), S.aci.data(), S.av.data(), K, nw.data(),
-                      means.data(), vars.data(), out.pred_mean.data(), out.pred_var.data());
+    mixture_moments(K, nobs, nw.data(), out.cond_eta.data(), out.cond_eta_var.data(), out.pred_mean.data(),
+                    out.pred_var.data());
+  }
+  // model-selection inputs (inference.rs:1296-1304, 1470-1485): the node nearest the mode, the
+  // Gaussian-approximation mlik there, and the observations rebuilt at the mode
+  {
+    double best = std::numeric_limits<double>::infinity();
+    for (int k = 0; k < K; ++k) {
+      double s2 = 0.0;
+      for (int j = 0; j < m; ++j) s2 += z[(size_t)k * m + j] * z[(size_t)k * m + j];
+      if (std::sqrt(s2) < best) {
+        best = std::sqrt(s2);
+        out.mode_index = k;
+      }
+    }
+    if (!mlik_gaussian(lp[out.mode_index], m, neg.data(), out.mlik_gaussian))
+      out.mlik_gaussian = std::numeric_limits<double>::quiet_NaN();
+    const int T = eng_.ncomp();
+    std::vector<double> coef(T), dcoef((size_t)m * T), dp1s(m);
+    double p1s = 1.0;
+    out.p1scale_mode = map_(mode.data(), coef.data(), dcoef.data(), &p1s, dp1s.data()) == 0
+                           ? p1s
+                           : std::numeric_limits<double>::quiet_NaN();
   }
   out.mlik = mx + std::log(std::fabs(sw));
   out.node_theta = thetas;

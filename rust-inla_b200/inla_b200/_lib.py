@@ -110,6 +110,12 @@ SIGNATURES = [
     ("inla_fit", C.c_int, [P, C.c_int, DP, P, P, P, P, DP, DP, DP, DP, DP, DP, DP]),
     ("inla_fit_predictor", C.c_int, [P, DP, DP]),
     ("inla_predictor_moments", C.c_int, [I64, I64, LP, LP, DP, C.c_int, DP, DP, DP, DP, DP]),
+    ("inla_fit_model_selection", C.c_int, [P, C.c_int, DP, DP, DP]),
+    ("inla_model_selection", C.c_int, [C.c_int, I64, DP, DP, DP, C.c_int, DP, C.c_int, DP, DP, C.c_int, DP, DP,
+                                       DP]),
+    ("inla_mlik_gaussian", C.c_int, [C.c_double, C.c_int, DP, DP]),
+    ("inla_observation_cdf", C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, DP]),
+    ("inla_cpo_failure", C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]),
     ("inla_theta_map_spde", C.c_int, [DP, C.c_int, DP, DP, DP, DP, P]),
     ("inla_dense_ldlt_solve_noalloc", C.c_int, [C.c_int, P, P, P, P, P, P]),
 ]

@@ -19,6 +19,7 @@ from ._lib import as_f64, as_i64, check, dptr, lib, lptr
 
 FAMILIES = {"gaussian": 0, "poisson": 1, "binomial": 2, "nbinomial": 3}
 CONSTRAINT_METHODS = {"auto": 0, "augmented": 1, "bordered": 2}
+CRITERIA = {"dic": 1, "waic": 2, "cpo": 4}
 
 THETA_MAP = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
                         C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p)
@@ -155,6 +156,13 @@ class LaplaceModel:
             out["trP"], out["trQ"], out["xMx"], out["zMx"] = gt[:, 0], gt[:, 1], gt[:, 2], gt[:, 3]
         return out
 
+    def model_selection(self, criteria="all"):
+        """DIC, WAIC, CPO / PIT and the Gaussian-approximation mlik of the last :meth:`fit`, as the
+        reference computes them at the end of a fit (inference.rs:1470-1514)."""
+        crit, cpo, pit = np.zeros(8), np.zeros(self.nobs), np.zeros(self.nobs)
+        check(lib().inla_fit_model_selection(self._h, _what(criteria), dptr(crit), dptr(cpo), dptr(pit)))
+        return _criteria_dict(crit, cpo, pit)
+
     def fit(self, theta0, theta_map="spde", priors=SPDE_DEFAULT_PRIORS, mode_search="nm", batched=False,
             strategy="ccd", f0=1.0, hessian="fd", max_iter=0, tol=0.0):
         """Full INLA fit; ``theta_map`` is ``"spde"`` or a Python callable
@@ -249,6 +257,61 @@ def predictor_moments(a, weights, cond_mean, cond_var):
     pv = np.zeros(nobs)
     check(lib().inla_predictor_moments(nobs, n, *ap, K, dptr(w), dptr(cm), dptr(cv), dptr(pm), dptr(pv)))
     return pm, pv
+
+
+def _what(criteria):
+    if criteria == "all":
+        return 7
+    return sum(CRITERIA[c] for c in criteria)
+
+
+def _criteria_dict(crit, cpo, pit):
+    return {"dic": crit[0], "mean_deviance": crit[1], "dic_p_eff": crit[2], "waic": crit[3], "lppd": crit[4],
+            "waic_p_eff": crit[5], "mlik_gaussian": crit[6],
+            "cpo_failures": None if np.isnan(crit[7]) else int(crit[7]), "cpo": cpo, "pit": pit}
+
+
+def model_selection(family, y, weights, mode_index, cond_eta, cond_eta_var, p1=None, p2=None, criteria="all"):
+    """DIC, WAIC and CPO / PIT (model_selection.rs:101-325) from node results on the host through
+    ``inla_model_selection``: ``cond_eta``, ``cond_eta_var`` [K][nobs], ``weights`` [K]
+    normalised, D(theta*) at node ``mode_index``. CPO / PIT entries are NaN where the reference
+    gives None; ``mlik_gaussian`` is NaN (see :func:`mlik_gaussian`)."""
+    y = as_f64(y)
+    nobs = len(y)
+    w = as_f64(weights)
+    ce = as_f64(np.reshape(cond_eta, (len(w), nobs)))
+    cv = as_f64(np.reshape(cond_eta_var, (len(w), nobs)))
+    p1a = None if p1 is None else as_f64(np.broadcast_to(p1, (nobs,)))
+    p2a = None if p2 is None else as_f64(np.broadcast_to(p2, (nobs,)))
+    crit, cpo, pit = np.zeros(8), np.zeros(nobs), np.zeros(nobs)
+    check(lib().inla_model_selection(FAMILIES.get(family, family), nobs, dptr(y),
+                                     None if p1a is None else dptr(p1a), None if p2a is None else dptr(p2a),
+                                     len(w), dptr(w), int(mode_index), dptr(ce), dptr(cv), _what(criteria),
+                                     dptr(crit), dptr(cpo), dptr(pit)))
+    return _criteria_dict(crit, cpo, pit)
+
+
+def mlik_gaussian(log_post_mode, neg_hessian):
+    """compute_marginal_log_lik_gaussian (model_selection.rs:25-73)."""
+    h = as_f64(np.atleast_2d(neg_hessian)) if np.size(neg_hessian) else np.zeros(0)
+    m = int(round(np.sqrt(h.size)))
+    out = C.c_double()
+    check(lib().inla_mlik_gaussian(float(log_post_mode), m, dptr(h) if m else None, C.byref(out)))
+    return out.value
+
+
+def observation_cdf(family, y, p1, eta, variance):
+    """observation_cdf (model_selection.rs:398-448); None where the reference gives None."""
+    out = C.c_double()
+    rc = lib().inla_observation_cdf(FAMILIES.get(family, family), float(y), float(p1), float(eta), float(variance),
+                                    C.byref(out))
+    return out.value if rc == 0 else None
+
+
+def cpo_failure(family, y, mu, var, p1=1.0, p2=1.0):
+    """check_cpo_failure_for_obs (model_selection.rs:327-396)."""
+    return bool(lib().inla_cpo_failure(FAMILIES.get(family, family), float(y), float(p1), float(p2), float(mu),
+                                       float(var)))
 
 
 def spde_gradient(out, dcoef, dp1scale, p1scale, prior_grad):

@@ -60,6 +60,37 @@ def test_integration_parity_at_fixed_nodes(problem):
     assert rel(r["pred_mean"], p.a @ r["mean"]) < 1e-12
 
 
+def test_model_selection_parity(problem):
+    """DIC, WAIC, CPO / PIT and the Gaussian-approximation mlik of a fit (inference.rs:1470-1514)
+    against the oracle's restatement on the oracle's node results at the fit's nodes."""
+    p, lm = problem
+    r = lm.fit(THETA0, mode_search="nm", batched=True)
+    ms = lm.model_selection()
+    ce, cv, lps = [], [], []
+    for theta in r["node_theta"]:
+        c = O.spde_coefs(theta[1], theta[2])
+        lr = O.laplace(p.model.matrix(c), p.a, "gaussian", p.y, p1=np.exp(theta[0]), want_var=True)
+        ce.append(O.matvec_csc(p.a, lr["x"]))
+        cv.append(O.predictor_variances_diag(p.a, lr["var"]))
+        lps.append(lr["mlik"] + O.loggamma_log_dens(theta[0], 1.0, 5e-5)
+                   + O.pc_spde_log_dens(theta[1], theta[2], 1.0, 0.05, 1.0, 0.01))
+    k0 = int(np.argmin(np.linalg.norm(r["node_theta"] - r["mode"], axis=1)))
+    n = len(p.y)
+    q1, q2 = np.full(n, np.exp(r["mode"][0])), np.ones(n)
+    w = r["node_weight"]
+    dic = O.compute_dic("gaussian", p.y, q1, q2, ce, w, k0)
+    waic = O.compute_waic("gaussian", p.y, q1, q2, ce, w)
+    close = lambda a, b: abs(a - b) <= 1e-8 * max(1.0, abs(b))
+    assert close(ms["dic"], dic["dic"]) and close(ms["mean_deviance"], dic["mean_deviance"])
+    assert close(ms["waic"], waic["waic"]) and close(ms["lppd"], waic["lppd"])
+    assert close(ms["mlik_gaussian"], O.mlik_gaussian(lps[k0], -np.asarray(r["hessian"]), 3))
+    cpo, pit, nf = O.compute_cpo_pit("gaussian", p.y, q1, q2, ce, cv, w)
+    both = np.array([c is not None for c in cpo]) & ~np.isnan(ms["cpo"])
+    assert abs(ms["cpo_failures"] - nf) <= 1 and both.sum() >= n - nf - 1
+    np.testing.assert_allclose(ms["cpo"][both], [c for c, b in zip(cpo, both) if b], rtol=1e-7)
+    np.testing.assert_allclose(ms["pit"][both], [q for q, b in zip(pit, both) if b], rtol=1e-7, atol=1e-12)
+
+
 @pytest.mark.parametrize("search", ["bfgs", "newton"])
 def test_batched_adjoint_fit_matches_plain(problem, search):
     p, lm = problem
