@@ -127,6 +127,21 @@ int inla_solver_supernodes(const inla_solver* s, int64_t* first, int64_t* count)
 /* nnz of each column of L incl. the diagonal (permuted order). */
 int inla_solver_colcounts(const inla_solver* s, int64_t* counts);
 
+/* scale_model_csc (crates/inla_math/src/design.rs:150-195): fac = exp(mean(log d_i)) over the
+ * positive finite d = diag(Q^+) (Moore-Penrose inverse), Q_scaled = fac Q. The reference
+ * diagonalizes the dense matrix (O(n^3)); here d comes from the sparse LDL^T and selected
+ * inverse of the bordered matrix [[Q, U^T], [U, 0]] on the GPU, whose leading block of the
+ * inverse is Q^+ when the rows of U span null(Q). k = -1 derives U: one constant row per
+ * connected component whose rows sum to ~0 (Besag, rw1, ...); k >= 0 takes the caller's
+ * k x n row-major null_basis (rw2: constant and linear trend). Nodes whose column holds no
+ * nonzero have d = 0 (left out of the mean, as the reference's zero eigenvalues are). n = 1
+ * follows the reference: Q_scaled = [1]. Outputs (each may be NULL): fac; scaled: the values
+ * of fac Q in the input pattern; ginv_diag: d [n]. INLA_ERR_INVALID when a basis row is not in
+ * the null space (|Q u| > 1e-8 |Q|max |u|max) or no d is positive; INLA_ERR_SINGULAR when U
+ * misses part of the null space. */
+int inla_scale_model(int64_t n, const int64_t* colptr, const int64_t* rowidx, const double* values, int k,
+                     const double* null_basis, int ordering, double* fac, double* scaled, double* ginv_diag);
+
 /* ------------------------------------------------------------------------
  * Batched engine: B problems sharing one symbolic analysis (numeric values
  * differ), factorized / solved / selectively inverted in one launch sequence.

@@ -109,6 +109,7 @@ SIGNATURES = [
     ("inla_log_prior_set", C.c_double, [DP, C.c_int, DP, P]),
     ("inla_fit", C.c_int, [P, C.c_int, DP, P, P, P, P, DP, DP, DP, DP, DP, DP, DP]),
     ("inla_fit_predictor", C.c_int, [P, DP, DP]),
+    ("inla_scale_model", C.c_int, [I64, LP, LP, DP, C.c_int, DP, C.c_int, DP, DP, DP]),
     ("inla_predictor_moments", C.c_int, [I64, I64, LP, LP, DP, C.c_int, DP, DP, DP, DP, DP]),
     ("inla_fit_model_selection", C.c_int, [P, C.c_int, DP, DP, DP]),
     ("inla_model_selection", C.c_int, [C.c_int, I64, DP, DP, DP, C.c_int, DP, C.c_int, DP, DP, C.c_int, DP, DP,

@@ -35,6 +35,28 @@ def choose_symmetric_order(q):
     return kind, (fwd if kind in (_lib.ORDER_RCM, _lib.ORDER_TIME_MAJOR) else None)
 
 
+def scale_model(q, null_basis=None, ordering=None):
+    """``scale_model_csc`` (design.rs:150-195) by a sparse selected inverse on the GPU instead of
+    a dense eigendecomposition: ``(fac * Q, fac, diag(Q^+))``. ``null_basis`` (k x n) spans the
+    null space of ``Q``; None derives one constant row per intrinsic connected component."""
+    q = sp.csc_matrix(q)
+    n, cp, ri, v = _csc_arrays(q)
+    if null_basis is None:
+        k, ub = -1, None
+    else:
+        ub = as_f64(np.atleast_2d(null_basis))
+        if ub.shape[1] != n:
+            raise InlaError(_lib.INLA_ERR_DIM_MISMATCH, "null_basis must have n columns")
+        k = ub.shape[0]
+    fac = C.c_double()
+    scaled = np.zeros(len(v))
+    d = np.zeros(n)
+    check(lib().inla_scale_model(n, lptr(cp), lptr(ri), dptr(v), k, None if ub is None or k == 0 else dptr(ub),
+                                 _lib.ORDER_ND if ordering is None else int(ordering), C.byref(fac), dptr(scaled),
+                                 dptr(d)))
+    return sp.csc_matrix((scaled, q.indices.copy(), q.indptr.copy()), shape=q.shape), fac.value, d
+
+
 class GpuSolver:
     """One factor per solver (FaerCpuSolver equivalent, solver.rs:48-99)."""
 
