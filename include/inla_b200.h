@@ -127,6 +127,35 @@ int inla_solver_supernodes(const inla_solver* s, int64_t* first, int64_t* count)
 /* nnz of each column of L incl. the diagonal (permuted order). */
 int inla_solver_colcounts(const inla_solver* s, int64_t* counts);
 
+/* ------------------------------------------------------------------------
+ * 2-D meshes for SPDE models (crates/inla_fmesher/src/fmesher.rs), host only.
+ * ---------------------------------------------------------------------- */
+typedef struct inla_mesh inla_mesh;
+/* build_mesh2d (fmesher.rs:119-158, validation 870-893): xy [nv][2], tri [ntri][3] (0-based).
+ * INLA_ERR_INVALID with the reference's message for fewer than three vertices, an index out of
+ * range, duplicate indices, a near-zero area (|2A| <= 1e-15) or a non-manifold edge. */
+int inla_mesh_create(int64_t nv, const double* xy, int64_t ntri, const int64_t* tri, inla_mesh** out);
+void inla_mesh_free(inla_mesh* m);
+/* nbr [ntri][3]: triangle across the edge opposite vertex e of each triangle, -1 on the boundary. */
+int inla_mesh_neighbors(const inla_mesh* m, int64_t* nbr);
+/* assemble_fem_blocks_diffusion (fmesher.rs:515-626): lumped mass c0, consistent mass c1,
+ * stiffness g1 and boundary term b1, summed per entry in triangle order. triangle_scale [ntri]
+ * (NULL = 1; barrier triangles of range fraction f take f^2, fmesher.rs:913-934) multiplies the
+ * diffusion tensor diffusion = {hxx, hxy, hyy} (NULL = identity). areas [ntri] may be NULL. */
+int inla_mesh_fem(inla_mesh* m, const double* triangle_scale, const double* diffusion, double* areas);
+/* One block of the last inla_mesh_fem in CSC: which 0 c0, 1 c1, 2 g1, 3 b1. Call with NULL
+ * arrays to read nnz first; colptr has nv + 1 entries. */
+int inla_mesh_fem_block(const inla_mesh* m, int which, int64_t* nnz, int64_t* colptr, int64_t* rowidx,
+                        double* vals);
+/* locate_point (fmesher.rs:161-263): triangle of each point by the walk from triangle 0 (-1
+ * outside), bary [npts][3] its barycentric weights (may be NULL). */
+int inla_mesh_locate(const inla_mesh* m, int64_t npts, const double* xy, int64_t* tri, double* bary);
+/* observation_projector_triplets (fmesher.rs:168-219): A (npts x nv) in CSR, each walk starting
+ * from the previous point's triangle, weights with |w| > 1e-15, columns ascending; rowptr
+ * [npts + 1], colidx and vals at most 3 npts. INLA_ERR_INVALID for a point outside the mesh. */
+int inla_mesh_projector(const inla_mesh* m, int64_t npts, const double* xy, int64_t* rowptr, int64_t* colidx,
+                        double* vals);
+
 /* scale_model_csc (crates/inla_math/src/design.rs:150-195): fac = exp(mean(log d_i)) over the
  * positive finite d = diag(Q^+) (Moore-Penrose inverse), Q_scaled = fac Q. The reference
  * diagonalizes the dense matrix (O(n^3)); here d comes from the sparse LDL^T and selected

@@ -789,3 +789,123 @@ def spde_neg_log_posterior(theta, model, a, y, max_iter=200, tol=1e-5, perm=None
         return 1e12
     lp = loggamma_log_dens(theta[0], 1.0, 5e-5) + pc_spde_log_dens(theta[1], theta[2], 1.0, 0.05, 1.0, 0.01)
     return -(r["mlik"] + lp)
+
+
+# ---------------------------------------------------------------------------
+# meshes (crates/inla_fmesher/src/fmesher.rs), pure Python for small meshes
+# ---------------------------------------------------------------------------
+
+GEOM_EPSILON = 1e-15  # fmesher.rs:5
+
+
+def _sa2(a, b, c):
+    """signed_area2 (fmesher.rs:897-899)."""
+    return (b[0] - a[0]) * (c[1] - a[1]) - (b[1] - a[1]) * (c[0] - a[0])
+
+
+def mesh_neighbors(triangles):
+    """build_mesh2d's edge map (fmesher.rs:122-139): nbr[t][e] across the edge opposite vertex e."""
+    nbr = [[-1, -1, -1] for _ in triangles]
+    open_edges = {}
+    for t, tri in enumerate(triangles):
+        for e in range(3):
+            a, b = int(tri[(e + 1) % 3]), int(tri[(e + 2) % 3])
+            if (b, a) in open_edges:
+                ot, oe = open_edges.pop((b, a))
+                nbr[t][e], nbr[ot][oe] = ot, t
+            elif (a, b) in open_edges:
+                raise OracleError(f"non-manifold edge detected between vertices {a} and {b}")
+            else:
+                open_edges[(a, b)] = (t, e)
+    return nbr
+
+
+def fem_blocks(vertices, triangles, triangle_scale=None, diffusion=(1.0, 0.0, 1.0)):
+    """assemble_fem_blocks_diffusion_unchecked (fmesher.rs:544-626) with coalesce (fmesher.rs:89-107):
+    dict of {(row, col): value} for c0, c1, g1, b1, and the areas."""
+    hxx, hxy, hyy = diffusion
+    nbr = mesh_neighbors(triangles)
+    trip = {"c0": [], "c1": [], "g1": [], "b1": []}
+    areas = []
+    for t, tv in enumerate(triangles):
+        s = [tuple(map(float, vertices[int(v)])) for v in tv]
+        e = [(s[2][0] - s[1][0], s[2][1] - s[1][1]), (s[0][0] - s[2][0], s[0][1] - s[2][1]),
+             (s[1][0] - s[0][0], s[1][1] - s[0][1])]
+        area = 0.5 * abs(_sa2(s[0], s[1], s[2]))
+        areas.append(area)
+        fa = 0.5 * abs(e[0][0] * e[1][1] - e[0][1] * e[1][0])
+        fa = area if fa <= GEOM_EPSILON else fa
+        scale = 1.0 if triangle_scale is None else float(triangle_scale[t])
+        eij = [[0.0] * 3 for _ in range(3)]
+        for i in range(3):
+            gi = (e[i][1], -e[i][0])
+            for j in range(i, 3):
+                gj = (e[j][1], -e[j][0])
+                hx = hxx * gi[0] + hxy * gi[1]
+                hy = hxy * gi[0] + hyy * gi[1]
+                eij[i][j] = hx * gj[0] + hy * gj[1]
+                eij[j][i] = eij[i][j]
+        v = [int(x) for x in tv]
+        for i in range(3):
+            trip["c0"].append((v[i], v[i], area / 3.0))
+            trip["c1"].append((v[i], v[i], area / 6.0))
+            trip["g1"].append((v[i], v[i], scale * eij[i][i] / (4.0 * fa)))
+            for j in range(i + 1, 3):
+                trip["c1"] += [(v[i], v[j], area / 12.0), (v[j], v[i], area / 12.0)]
+                vij = scale * eij[i][j] / (4.0 * fa)
+                trip["g1"] += [(v[i], v[j], vij), (v[j], v[i], vij)]
+        bnd = [nbr[t][k] < 0 for k in range(3)]
+        if any(bnd):
+            vij = -1.0 / (4.0 * fa)
+            for i in range(3):
+                for j in range(3):
+                    for k in range(3):
+                        if bnd[k] and i != k:
+                            trip["b1"].append((v[i], v[j], scale * eij[k][j] * vij))
+    out = {"areas": areas}
+    for name, tr in trip.items():
+        merged = {}
+        for r, c, x in sorted(tr, key=lambda q: (q[0], q[1])):   # stable, then summed in order
+            merged[(r, c)] = merged[(r, c)] + x if (r, c) in merged else x
+        out[name] = merged
+    return out
+
+
+def locate_point(vertices, triangles, nbr, start, p):
+    """locate_point_from (fmesher.rs:222-263) + barycentric_coords (822-831): (triangle, bary)."""
+    cur, remaining = start, max(len(triangles) * 3, 1)
+    while remaining > 0:
+        remaining -= 1
+        tv = [int(x) for x in triangles[cur]]
+        a, b, c = (tuple(map(float, vertices[v])) for v in tv)
+        orient = 1.0 if _sa2(a, b, c) >= 0.0 else -1.0
+        most_negative, leaving = 0.0, None
+        for e in range(3):
+            side = orient * _sa2(tuple(map(float, vertices[tv[(e + 1) % 3]])),
+                                 tuple(map(float, vertices[tv[(e + 2) % 3]])), p)
+            if side < most_negative:
+                most_negative, leaving = side, e
+        if most_negative >= -GEOM_EPSILON:
+            den = _sa2(a, b, c)
+            w0 = _sa2(b, c, p) / den
+            w1 = _sa2(c, a, p) / den
+            return cur, (w0, w1, 1.0 - w0 - w1)
+        if leaving is None or nbr[cur][leaving] < 0:
+            return -1, None
+        cur = nbr[cur][leaving]
+    return -1, None
+
+
+def projector_triplets(vertices, triangles, points):
+    """observation_projector_triplets (fmesher.rs:168-219)."""
+    nbr = mesh_neighbors(triangles)
+    trips, start = [], 0
+    for row, p in enumerate(points):
+        t, w = locate_point(vertices, triangles, nbr, start, (float(p[0]), float(p[1])))
+        if t < 0:
+            raise OracleError(f"observation point ({p[0]}, {p[1]}) is outside the mesh")
+        start = t
+        for k in range(3):
+            if abs(w[k]) > GEOM_EPSILON:
+                trips.append((row, int(triangles[t][k]), w[k]))
+    return trips

@@ -1,0 +1,100 @@
+// C ABI of the mesh tools (host code only): mesh topology, FEM blocks, point location and
+// the observation projector (crates/inla_fmesher/src/fmesher.rs).
+#include <cstring>
+#include <memory>
+
+#include "capi_common.hpp"
+#include "inla_b200.h"
+#include "mesh.hpp"
+
+using namespace inla;
+
+struct inla_mesh {
+  Mesh2D m;
+  std::unique_ptr<FemBlocks> fem;
+};
+
+extern "C" {
+
+int inla_mesh_create(int64_t nv, const double* xy, int64_t ntri, const int64_t* tri, inla_mesh** out) {
+  try {
+    if (!out || nv < 0 || ntri < 0 || (nv > 0 && !xy) || (ntri > 0 && !tri))
+      return fail(INLA_ERR_INVALID, "inla_mesh_create: invalid argument");
+    std::unique_ptr<inla_mesh> h(new inla_mesh());
+    const std::string err = build_mesh2d(nv, xy, ntri, tri, h->m);
+    if (!err.empty()) return fail(INLA_ERR_INVALID, err);
+    *out = h.release();
+    return INLA_OK;
+  } catch (...) {
+    return map_exception();
+  }
+}
+
+void inla_mesh_free(inla_mesh* h) { delete h; }
+
+int inla_mesh_neighbors(const inla_mesh* h, int64_t* nbr) {
+  if (!h || !nbr) return fail(INLA_ERR_INVALID, "inla_mesh_neighbors: invalid argument");
+  for (size_t t = 0; t < h->m.nbr.size(); ++t)
+    for (int e = 0; e < 3; ++e) nbr[3 * t + e] = h->m.nbr[t][e];
+  return INLA_OK;
+}
+
+int inla_mesh_fem(inla_mesh* h, const double* triangle_scale, const double* diffusion, double* areas) {
+  try {
+    if (!h) return fail(INLA_ERR_INVALID, "inla_mesh_fem: invalid argument");
+    std::vector<double> scale;
+    if (triangle_scale) scale.assign(triangle_scale, triangle_scale + h->m.tri.size());
+    const double hxx = diffusion ? diffusion[0] : 1.0, hxy = diffusion ? diffusion[1] : 0.0,
+                 hyy = diffusion ? diffusion[2] : 1.0;
+    std::unique_ptr<FemBlocks> f(new FemBlocks());
+    const std::string err = assemble_fem(h->m, scale, hxx, hxy, hyy, *f);
+    if (!err.empty()) return fail(INLA_ERR_INVALID, err);
+    if (areas) std::memcpy(areas, f->area.data(), sizeof(double) * f->area.size());
+    h->fem = std::move(f);
+    return INLA_OK;
+  } catch (...) {
+    return map_exception();
+  }
+}
+
+int inla_mesh_fem_block(const inla_mesh* h, int which, int64_t* nnz, int64_t* colptr, int64_t* rowidx,
+                        double* vals) {
+  if (!h || !h->fem || which < 0 || which > 3) return fail(INLA_ERR_INVALID, "inla_mesh_fem_block: no such block");
+  const CscBlock& b = which == 0 ? h->fem->c0 : which == 1 ? h->fem->c1 : which == 2 ? h->fem->g1 : h->fem->b1;
+  if (nnz) *nnz = (int64_t)b.rowidx.size();
+  if (colptr) std::memcpy(colptr, b.colptr.data(), sizeof(int64_t) * b.colptr.size());
+  if (rowidx) std::memcpy(rowidx, b.rowidx.data(), sizeof(int64_t) * b.rowidx.size());
+  if (vals) std::memcpy(vals, b.val.data(), sizeof(double) * b.val.size());
+  return INLA_OK;
+}
+
+int inla_mesh_locate(const inla_mesh* h, int64_t npts, const double* xy, int64_t* tri, double* bary) {
+  if (!h || npts < 0 || (npts > 0 && (!xy || !tri))) return fail(INLA_ERR_INVALID, "inla_mesh_locate: invalid argument");
+  for (int64_t r = 0; r < npts; ++r) {
+    double w[3];
+    tri[r] = locate_point(h->m, 0, xy[2 * r], xy[2 * r + 1], w);
+    if (bary)
+      for (int k = 0; k < 3; ++k) bary[3 * r + k] = tri[r] >= 0 ? w[k] : NAN;
+  }
+  return INLA_OK;
+}
+
+int inla_mesh_projector(const inla_mesh* h, int64_t npts, const double* xy, int64_t* rowptr, int64_t* colidx,
+                        double* vals) {
+  try {
+    if (!h || npts < 0 || (npts > 0 && !xy) || !rowptr || !colidx || !vals)
+      return fail(INLA_ERR_INVALID, "inla_mesh_projector: invalid argument");
+    std::vector<int64_t> rp, ci;
+    std::vector<double> v;
+    const std::string err = projector(h->m, npts, xy, rp, ci, v);
+    if (!err.empty()) return fail(INLA_ERR_INVALID, err);
+    std::memcpy(rowptr, rp.data(), sizeof(int64_t) * rp.size());
+    std::memcpy(colidx, ci.data(), sizeof(int64_t) * ci.size());
+    std::memcpy(vals, v.data(), sizeof(double) * v.size());
+    return INLA_OK;
+  } catch (...) {
+    return map_exception();
+  }
+}
+
+}  // extern "C"

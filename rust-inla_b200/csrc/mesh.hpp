@@ -1,0 +1,53 @@
+// 2-D triangle meshes for SPDE models: topology, P1 finite-element blocks and the barycentric
+// observation projector, host code.
+//
+// Reference: crates/inla_fmesher/src/fmesher.rs:119-158 (build_mesh2d: validation and
+// edge neighbours), 168-263 (observation_projector_triplets, locate_point_from: a walk across
+// edge neighbours from the previous point's triangle), 544-626 (P1 blocks c0 / c1 / g1 / b1
+// with a per-triangle diffusion scale and a global tensor H), 782-831 (barycentric
+// classification), 870-893 (triangle validation). GEOM_EPSILON = 1e-15 (fmesher.rs:5).
+#pragma once
+#include <array>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace inla {
+
+constexpr double kGeomEps = 1e-15;
+
+struct Mesh2D {
+  std::vector<double> x, y;
+  std::vector<std::array<int64_t, 3>> tri;
+  std::vector<std::array<int64_t, 3>> nbr;  // neighbour across the edge opposite vertex e (-1: boundary)
+};
+
+// One assembled block in CSC (rows sorted within a column).
+struct CscBlock {
+  int64_t n = 0;
+  std::vector<int64_t> colptr, rowidx;
+  std::vector<double> val;
+};
+
+struct FemBlocks {
+  CscBlock c0, c1, g1, b1;
+  std::vector<double> area;
+};
+
+// Empty string on success, else the reference's error message.
+std::string build_mesh2d(int64_t nv, const double* xy, int64_t ntri, const int64_t* tri, Mesh2D& m);
+
+// triangle_scale: [ntri] or empty (all 1); H = [[hxx, hxy], [hxy, hyy]] symmetric positive definite.
+std::string assemble_fem(const Mesh2D& m, const std::vector<double>& triangle_scale, double hxx, double hxy,
+                         double hyy, FemBlocks& out);
+
+// Triangle containing (px, py) by the reference's walk from `start` (-1: outside), with the
+// barycentric weights of the point in that triangle.
+int64_t locate_point(const Mesh2D& m, int64_t start, double px, double py, double bary[3]);
+
+// Projector rows (up to three entries each, weights with |w| > 1e-15, columns ascending).
+// Empty string on success, else the reference's error for the first point outside the mesh.
+std::string projector(const Mesh2D& m, int64_t npts, const double* xy, std::vector<int64_t>& rowptr,
+                      std::vector<int64_t>& colidx, std::vector<double>& val);
+
+}  // namespace inla

@@ -110,6 +110,13 @@ SIGNATURES = [
     ("inla_fit", C.c_int, [P, C.c_int, DP, P, P, P, P, DP, DP, DP, DP, DP, DP, DP]),
     ("inla_fit_predictor", C.c_int, [P, DP, DP]),
     ("inla_scale_model", C.c_int, [I64, LP, LP, DP, C.c_int, DP, C.c_int, DP, DP, DP]),
+    ("inla_mesh_create", C.c_int, [I64, DP, I64, LP, C.POINTER(P)]),
+    ("inla_mesh_free", None, [P]),
+    ("inla_mesh_neighbors", C.c_int, [P, LP]),
+    ("inla_mesh_fem", C.c_int, [P, DP, DP, DP]),
+    ("inla_mesh_fem_block", C.c_int, [P, C.c_int, LP, LP, LP, DP]),
+    ("inla_mesh_locate", C.c_int, [P, I64, DP, LP, DP]),
+    ("inla_mesh_projector", C.c_int, [P, I64, DP, LP, LP, DP]),
     ("inla_predictor_moments", C.c_int, [I64, I64, LP, LP, DP, C.c_int, DP, DP, DP, DP, DP]),
     ("inla_fit_model_selection", C.c_int, [P, C.c_int, DP, DP, DP]),
     ("inla_model_selection", C.c_int, [C.c_int, I64, DP, DP, DP, C.c_int, DP, C.c_int, DP, DP, C.c_int, DP, DP,

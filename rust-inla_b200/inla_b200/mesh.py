@@ -1,0 +1,75 @@
+"""2-D triangle meshes for SPDE models over the C ABI (host code of the library):
+topology, P1 finite-element blocks and the barycentric observation projector
+(crates/inla_fmesher/src/fmesher.rs)."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import scipy.sparse as sp
+
+from ._lib import as_f64, as_i64, check, dptr, lib, lptr
+
+FEM_BLOCKS = ("c0", "c1", "g1", "b1")
+
+
+class Mesh:
+    """``build_mesh2d`` (fmesher.rs:119-158): ``vertices`` [nv][2], ``triangles`` [ntri][3]."""
+
+    def __init__(self, vertices, triangles):
+        self.vertices = as_f64(np.asarray(vertices, dtype=float).reshape(-1, 2))
+        self.triangles = as_i64(np.asarray(triangles).reshape(-1, 3))
+        self.nv, self.ntri = len(self.vertices), len(self.triangles)
+        h = C.c_void_p()
+        check(lib().inla_mesh_create(self.nv, dptr(self.vertices), self.ntri, lptr(self.triangles), C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().inla_mesh_free(h)
+            self._h = None
+
+    @property
+    def neighbors(self):
+        nb = np.zeros((self.ntri, 3), dtype=np.int64)
+        check(lib().inla_mesh_neighbors(self._h, lptr(nb)))
+        return nb
+
+    def fem(self, triangle_scale=None, diffusion=None):
+        """``assemble_fem_blocks_diffusion`` (fmesher.rs:515-626): dict of CSC blocks
+        ``c0``, ``c1``, ``g1``, ``b1`` and the triangle ``areas``."""
+        sc = None if triangle_scale is None else as_f64(np.broadcast_to(triangle_scale, (self.ntri,)))
+        df = None if diffusion is None else as_f64(diffusion)
+        areas = np.zeros(self.ntri)
+        check(lib().inla_mesh_fem(self._h, None if sc is None else dptr(sc), None if df is None else dptr(df),
+                                  dptr(areas)))
+        out = {"areas": areas}
+        for which, name in enumerate(FEM_BLOCKS):
+            nnz = C.c_int64()
+            check(lib().inla_mesh_fem_block(self._h, which, C.byref(nnz), None, None, None))
+            cp = np.zeros(self.nv + 1, dtype=np.int64)
+            ri = np.zeros(nnz.value, dtype=np.int64)
+            v = np.zeros(nnz.value)
+            check(lib().inla_mesh_fem_block(self._h, which, None, lptr(cp), lptr(ri), dptr(v)))
+            out[name] = sp.csc_matrix((v, ri, cp), shape=(self.nv, self.nv))
+        return out
+
+    def locate(self, points):
+        """Triangle of each point (-1 outside) and its barycentric weights (fmesher.rs:161-263)."""
+        p = as_f64(np.asarray(points, dtype=float).reshape(-1, 2))
+        t = np.zeros(len(p), dtype=np.int64)
+        b = np.zeros((len(p), 3))
+        check(lib().inla_mesh_locate(self._h, len(p), dptr(p), lptr(t), dptr(b)))
+        return t, b
+
+    def projector(self, points):
+        """``observation_projector_triplets`` (fmesher.rs:168-219) as a CSR matrix."""
+        p = as_f64(np.asarray(points, dtype=float).reshape(-1, 2))
+        n = len(p)
+        rp = np.zeros(n + 1, dtype=np.int64)
+        ci = np.zeros(3 * n, dtype=np.int64)
+        v = np.zeros(3 * n)
+        check(lib().inla_mesh_projector(self._h, n, dptr(p), lptr(rp), lptr(ci), dptr(v)))
+        nnz = int(rp[-1])
+        return sp.csr_matrix((v[:nnz], ci[:nnz], rp), shape=(n, self.nv))

@@ -1,0 +1,120 @@
+"""Mesh tools of the library (host code, no GPU): the reference's own fmesher tests
+(crates/inla_fmesher/src/fmesher.rs:945-1163), bitwise parity with the oracle's restatement of
+the FEM assembly and the projector walk, and agreement with the numpy input generators."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import oracle as O
+from inla_b200 import InlaError, models
+from inla_b200.mesh import FEM_BLOCKS, Mesh
+
+SQUARE_V = [[0.0, 0.0], [1.0, 0.0], [0.0, 1.0], [1.0, 1.0]]
+SQUARE_T = [[0, 1, 2], [1, 3, 2]]
+
+
+def test_builds_topology_for_two_triangles():
+    """fmesher.rs:945-960."""
+    nb = Mesh(SQUARE_V, SQUARE_T).neighbors
+    assert nb[0][0] == 1 and nb[1][1] == 0
+
+
+def test_locates_point_in_triangle_edge_and_vertex():
+    """fmesher.rs:1065-1095."""
+    m = Mesh(SQUARE_V, SQUARE_T)
+    t, b = m.locate([[0.1, 0.1], [0.5, 0.5], [0.0, 0.0], [2.0, 2.0]])
+    assert t[0] >= 0 and np.all(np.abs(b[0]) > 1e-15)              # strictly inside
+    assert t[1] >= 0 and np.sum(np.abs(b[1]) <= 1e-15) >= 1         # on the shared edge
+    assert t[2] == 0 and np.argmax(b[2]) == 0 and abs(b[2][0] - 1.0) < 1e-15   # vertex 0
+    assert t[3] == -1                                                # outside
+
+
+def test_assembles_fem_blocks_for_square_mesh():
+    """fmesher.rs:1122-1163: areas, lumped mass, identity vs anisotropic vs barrier stiffness."""
+    m = Mesh(SQUARE_V, SQUARE_T)
+    f = m.fem()
+    assert f["areas"].tolist() == [0.5, 0.5]
+    assert f["c0"].diagonal().tolist() == [1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0]
+    assert f["g1"].nnz > 0 and f["b1"].nnz > 0
+    ident = m.fem(diffusion=[1.0, 0.0, 1.0])
+    assert (f["g1"] != ident["g1"]).nnz == 0
+    aniso = m.fem(diffusion=[2.0, 0.0, 0.5])
+    assert f["g1"][0, 0] != aniso["g1"][0, 0]
+    barrier = m.fem(triangle_scale=[0.1 ** 2, 1.0])
+    assert (f["g1"] != barrier["g1"]).nnz > 0
+    assert (f["c0"] != barrier["c0"]).nnz == 0
+
+
+def test_invalid_meshes_raise_the_reference_errors():
+    with pytest.raises(InlaError, match="three vertices"):
+        Mesh([[0, 0], [1, 0]], [])
+    with pytest.raises(InlaError, match="out of range"):
+        Mesh(SQUARE_V, [[0, 1, 7]])
+    with pytest.raises(InlaError, match="duplicate"):
+        Mesh(SQUARE_V, [[0, 1, 1]])
+    with pytest.raises(InlaError, match="near-zero area"):
+        Mesh([[0, 0], [1, 0], [2, 0]], [[0, 1, 2]])
+    with pytest.raises(InlaError, match="non-manifold"):
+        Mesh(SQUARE_V, [[0, 1, 2], [0, 1, 3]])
+    with pytest.raises(InlaError, match="SPD"):
+        Mesh(SQUARE_V, SQUARE_T).fem(diffusion=[1.0, 2.0, 1.0])
+    with pytest.raises(InlaError, match="outside the mesh"):
+        Mesh(SQUARE_V, SQUARE_T).projector([[0.2, 0.2], [1.5, 0.5]])
+
+
+def _jittered(nx, seed):
+    rng = np.random.default_rng(seed)
+    return models.grid_mesh(nx, rng)
+
+
+@pytest.mark.parametrize("scale,diff", [(None, None), ("barrier", (2.0, 0.3, 0.7))])
+def test_fem_blocks_match_oracle_bitwise(scale, diff):
+    v, t = _jittered(12, 5)
+    ts = None
+    if scale == "barrier":
+        ts = np.ones(len(t))
+        ts[::7] = 0.25 ** 2
+    f = Mesh(v, t).fem(triangle_scale=ts, diffusion=diff)
+    ref = O.fem_blocks(v, t, ts, diff if diff is not None else (1.0, 0.0, 1.0))
+    assert f["areas"].tolist() == ref["areas"]
+    for name in FEM_BLOCKS:
+        got = f[name].tocoo()
+        d = {(int(r), int(c)): x for r, c, x in zip(got.row, got.col, got.data)}
+        assert d == ref[name], name
+
+
+def test_fem_matches_input_generator():
+    """The generator's numpy assembly (scipy sums duplicates in its own order)."""
+    v, t = _jittered(40, 7)
+    f = Mesh(v, t).fem()
+    c0, g = models.fem_matrices(v, t)
+    np.testing.assert_allclose(f["c0"].diagonal(), c0, rtol=1e-15)
+    assert abs(f["g1"] - g).max() <= 1e-14 * abs(g).max()
+
+
+def test_projector_matches_oracle_walk_and_generator():
+    nx = 25
+    v, t = _jittered(nx, 9)
+    rng = np.random.default_rng(10)
+    pts = rng.uniform(0.0, 1.0, size=(400, 2))
+    a = Mesh(v, t).projector(pts)
+    ref = sp.coo_matrix(([w for _, _, w in O.projector_triplets(v, t, pts)],
+                         ([r for r, _, _ in O.projector_triplets(v, t, pts)],
+                          [c for _, c, _ in O.projector_triplets(v, t, pts)])), shape=a.shape).tocsr()
+    ref.sort_indices()
+    assert (a != ref).nnz == 0
+    g = models.grid_projector(v, t, nx, pts)
+    assert (a != g).nnz == 0
+    np.testing.assert_allclose(np.asarray(a.sum(1)).ravel(), 1.0, atol=1e-14)
+
+
+def test_projector_at_full_mesh_size():
+    """The 200 x 200 mesh (79 202 triangles) with 20 000 points: rows sum to one and the
+    interpolant of a linear function is exact."""
+    v, t = _jittered(200, 11)
+    rng = np.random.default_rng(12)
+    pts = rng.uniform(0.0, 1.0, size=(20_000, 2))
+    a = Mesh(v, t).projector(pts)
+    np.testing.assert_allclose(np.asarray(a.sum(1)).ravel(), 1.0, atol=1e-13)
+    lin = 0.3 + 1.7 * v[:, 0] - 0.9 * v[:, 1]
+    np.testing.assert_allclose(a @ lin, 0.3 + 1.7 * pts[:, 0] - 0.9 * pts[:, 1], atol=1e-12)
