@@ -298,6 +298,9 @@ int inla_multi_fit(inla_multi* h, int m, const double* theta0, inla_multi_theta_
                    inla_multi_log_prior_fn prior, void* user, const inla_multi_fit_options* opt, double* mode,
                    double* hessian, double* mlik, double* latent_mean, double* latent_var, int* mode_iters,
                    int* status, double* info);
+/* Linear predictor of the last inla_multi_fit: per model the mixture mean and variance of
+ * eta = A x over that model's CCD nodes (inference.rs:1451-1466), [nobs] each (NULL allowed). */
+int inla_multi_fit_predictor(inla_multi* h, double* pred_mean, double* pred_var);
 /* Built-in map of AR1 + iid + intercept models: theta = [log tau, logit-type rho, log tau_iid],
  * components [intercept precision, AR1 pieces K0, K1, K2, iid] with coefficients
  * [1, tau, tau rho^2, -tau rho, tau_iid] (ar1.rs:9-69, structured.rs:348-356). */

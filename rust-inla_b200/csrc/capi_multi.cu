@@ -13,6 +13,8 @@ using namespace inla;
 struct inla_multi {
   cudaStream_t stream = nullptr;
   std::unique_ptr<MultiLaplace> eng;
+  std::vector<double> pred_mean, pred_var;  // linear predictor moments of the last inla_multi_fit
+  bool fitted = false;
 };
 
 extern "C" {
@@ -148,10 +150,21 @@ int inla_multi_fit(inla_multi* h, int m, const double* theta0, inla_multi_theta_
       info[1] = R.n_batches;
       info[2] = (double)R.n_model_evals;
     }
+    h->pred_mean = std::move(R.pred_mean);
+    h->pred_var = std::move(R.pred_var);
+    h->fitted = true;
     return INLA_OK;
   } catch (...) {
     return map_exception();
   }
+}
+
+int inla_multi_fit_predictor(inla_multi* h, double* pred_mean, double* pred_var) {
+  if (!h || !h->fitted) return fail(INLA_ERR_INVALID, "inla_multi_fit_predictor: no fit on this handle");
+  const size_t bytes = sizeof(double) * h->pred_mean.size();
+  if (pred_mean) std::memcpy(pred_mean, h->pred_mean.data(), bytes);
+  if (pred_var) std::memcpy(pred_var, h->pred_var.data(), bytes);
+  return INLA_OK;
 }
 
 int inla_multi_theta_map_ar1_iid(int g, const double* theta, int m, double* coef, double* dcoef, double* p1scale,

@@ -57,6 +57,7 @@ class MultiLaplace {
   int ncomp() const { return spec_.ncomp; }
   int max_batch() const { return max_batch_; }
   const std::vector<int64_t>& lat_off() const { return spec_.lat_off; }
+  const MultiSpec& spec() const { return spec_; }
   const double* d_x() const { return x_.p; }      // [B][n]
   const double* d_var() const { return var_.p; }  // [B][n]
   GpuFactor& factor() { return *F_; }
@@ -105,6 +106,7 @@ struct MultiFitOptions {
 struct MultiFitResult {
   std::vector<double> mode, hessian, mlik;   // [G][m], [G][m][m], [G]
   std::vector<double> latent_mean, latent_var;  // [n]
+  std::vector<double> pred_mean, pred_var;      // [nobs]: linear predictor eta = A x per model
   std::vector<int> mode_iters, status;       // [G]; status 0 ok, 1 no finite node, 2 singular Hessian
   int n_batches = 0;
   int64_t n_model_evals = 0;

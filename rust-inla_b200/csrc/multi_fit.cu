@@ -306,6 +306,9 @@ void MultiDriver::fit(const double* theta0, const MultiFitOptions& opt, MultiFit
   evaluate(K, nodes.data(), false, true, nf.data(), nullptr, &means, &vars);
   out.latent_mean.assign(n, 0.0);
   out.latent_var.assign(n, 0.0);
+  const MultiSpec& S = eng_.spec();
+  out.pred_mean.assign(S.nobs, 0.0);
+  out.pred_var.assign(S.nobs, 0.0);
   out.mlik.assign(G, NAN);
   for (int g = 0; g < G; ++g) {
     std::vector<double> lp(K);
@@ -335,6 +338,33 @@ void MultiDriver::fit(const double* theta0, const MultiFitOptions& opt, MultiFit
       }
       out.latent_mean[i] = mi;
       out.latent_var[i] = vi;
+    }
+    // linear predictor of the model's observations (inference.rs:1370-1384, 1451-1466):
+    // per node eta_k = A x_k and sum_j A_ij^2 var_kj as matvec_csc / predictor_variances_diag
+    // sum them, then the same mixture
+    std::vector<double> eta(K), ev(K);
+    for (int64_t r = S.obs_off[g]; r < S.obs_off[g + 1]; ++r) {
+      for (int k = 0; k < K; ++k) {
+        double e = 0.0, s2 = 0.0;
+        for (int64_t p = S.acp[r]; p < S.acp[r + 1]; ++p) {
+          const double a = S.av[p], xv = means[(size_t)k * n + S.aci[p]];
+          if (xv != 0.0) e += a * xv;
+          s2 += a * a * vars[(size_t)k * n + S.aci[p]];
+        }
+        eta[k] = e;
+        ev[k] = s2;
+      }
+      double mi = 0.0;
+      for (int k = 0; k < K; ++k)
+        if (std::isfinite(lp[k])) mi += nw[k] * eta[k];
+      double vi = 0.0;
+      for (int k = 0; k < K; ++k) {
+        if (!std::isfinite(lp[k])) continue;
+        const double d = eta[k] - mi;
+        vi += nw[k] * (ev[k] + d * d);
+      }
+      out.pred_mean[r] = mi;
+      out.pred_var[r] = vi;
     }
     out.mlik[g] = mx + std::log(std::fabs(sw));
   }

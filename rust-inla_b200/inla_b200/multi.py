@@ -182,5 +182,9 @@ class MultiModel:
         check(lib().inla_multi_fit(self._h, m, dptr(th0), fmap, fprior, C.cast(C.pointer(ps), C.c_void_p),
                                    C.byref(opt), dptr(mode), dptr(hess), dptr(mlik), dptr(mean), dptr(var),
                                    ip(iters), ip(status), dptr(info)))
+        pm = np.zeros(self.nobs)
+        pv = np.zeros(self.nobs)
+        check(lib().inla_multi_fit_predictor(self._h, dptr(pm), dptr(pv)))
         return {"mode": mode, "hessian": hess, "mlik": mlik, "mean": mean, "var": var, "mode_iters": iters,
-                "status": status, "seconds": info[0], "n_batches": int(info[1]), "n_model_evals": int(info[2])}
+                "status": status, "seconds": info[0], "n_batches": int(info[1]), "n_model_evals": int(info[2]),
+                "pred_mean": pm, "pred_var": pv}
