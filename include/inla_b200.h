@@ -156,6 +156,16 @@ int inla_mesh_locate(const inla_mesh* m, int64_t npts, const double* xy, int64_t
 int inla_mesh_projector(const inla_mesh* m, int64_t npts, const double* xy, int64_t* rowptr, int64_t* colidx,
                         double* vals);
 
+/* spde_precision_csc (crates/inla_stats/src/spde.rs:70-140) as the three components of
+ * inla_laplace_create on one pattern: Q(theta) = c_0 C0 + c_1 G1 + c_2 G1 C0^-1 G1 with
+ * (c_0, c_1, c_2) = tau^2 (kappa^4, 2 kappa^2, 1) (inla_theta_map_spde). c0: the lumped mass
+ * diagonal [n]; G1 in CSC with both triangles (e.g. from inla_mesh_fem_block). Call with
+ * colptr / rowidx / comp NULL to read nnz; the pattern (diagonal, G1 and G1 C0^-1 G1, rows
+ * sorted) goes to colptr [n + 1] / rowidx [nnz], the components to comp [3][nnz].
+ * INLA_ERR_INVALID for |c0_i| < 1e-15 ("Zero entry in mass matrix c0 diagonal"). */
+int inla_spde_components(int64_t n, const double* c0, const int64_t* g_colptr, const int64_t* g_rowidx,
+                         const double* g_vals, int64_t* nnz, int64_t* colptr, int64_t* rowidx, double* comp);
+
 /* scale_model_csc (crates/inla_math/src/design.rs:150-195): fac = exp(mean(log d_i)) over the
  * positive finite d = diag(Q^+) (Moore-Penrose inverse), Q_scaled = fac Q. The reference
  * diagonalizes the dense matrix (O(n^3)); here d comes from the sparse LDL^T and selected

@@ -909,3 +909,37 @@ def projector_triplets(vertices, triangles, points):
             if abs(w[k]) > GEOM_EPSILON:
                 trips.append((row, int(triangles[t][k]), w[k]))
     return trips
+
+
+def spde_precision(c0_diag, g1, kappa, tau):
+    """spde_precision_csc (crates/inla_stats/src/spde.rs:70-140) as a dict {(i, j): value}:
+    tau^2 (kappa^4 C0 + 2 kappa^2 G1 + G1 C0^-1 G1), with (G1 C0^-1 G1)_ij summed over
+    ascending k as sum_k (G1_ik (1 / c0_k)) G1_kj."""
+    g = sp.csc_matrix(g1)
+    n = g.shape[0]
+    for v in c0_diag:
+        if abs(v) < 1e-15:
+            raise OracleError("Zero entry in mass matrix c0 diagonal")
+    cinv = [1.0 / float(v) for v in c0_diag]
+    cols = [dict() for _ in range(n)]
+    for j in range(n):
+        for p in range(g.indptr[j], g.indptr[j + 1]):
+            cols[j][int(g.indices[p])] = cols[j].get(int(g.indices[p]), 0.0) + float(g.data[p])
+    gcg = {}
+    for j in range(n):
+        for k in sorted(cols[j]):
+            gkj = cols[j][k]
+            for i, gik in cols[k].items():
+                gcg[(i, j)] = gcg.get((i, j), 0.0) + (gik * cinv[k]) * gkj
+    k2 = kappa * kappa
+    k4 = k2 * k2
+    q = {}
+    for i in range(n):
+        q[(i, i)] = k4 * float(c0_diag[i])
+    for j in range(n):
+        for i, v in cols[j].items():
+            q[(i, j)] = q.get((i, j), 0.0) + 2.0 * k2 * v
+    for key, v in gcg.items():
+        q[key] = q.get(key, 0.0) + v
+    t2 = tau * tau
+    return {key: v * t2 for key, v in q.items()}, gcg

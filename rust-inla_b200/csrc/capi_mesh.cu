@@ -97,4 +97,30 @@ int inla_mesh_projector(const inla_mesh* h, int64_t npts, const double* xy, int6
   }
 }
 
+int inla_spde_components(int64_t n, const double* c0, const int64_t* g_colptr, const int64_t* g_rowidx,
+                         const double* g_vals, int64_t* nnz, int64_t* colptr, int64_t* rowidx, double* comp) {
+  try {
+    if (n <= 0 || !c0 || !g_colptr || !g_rowidx || !g_vals)
+      return fail(INLA_ERR_INVALID, "SPDE requires non-empty FEM blocks");
+    if (g_colptr[0] != 0) return fail(INLA_ERR_INVALID, "inla_spde_components: colptr[0] must be 0");
+    for (int64_t j = 0; j < n; ++j) {
+      if (g_colptr[j + 1] < g_colptr[j]) return fail(INLA_ERR_INVALID, "inla_spde_components: colptr not monotone");
+      for (int64_t p = g_colptr[j]; p < g_colptr[j + 1]; ++p)
+        if (g_rowidx[p] < 0 || g_rowidx[p] >= n)
+          return fail(INLA_ERR_INVALID, "inla_spde_components: row index out of range");
+    }
+    CscBlock pat;
+    std::vector<double> cv;
+    const std::string err = spde_components(n, c0, g_colptr, g_rowidx, g_vals, pat, cv);
+    if (!err.empty()) return fail(INLA_ERR_INVALID, err);
+    if (nnz) *nnz = (int64_t)pat.rowidx.size();
+    if (colptr) std::memcpy(colptr, pat.colptr.data(), sizeof(int64_t) * pat.colptr.size());
+    if (rowidx) std::memcpy(rowidx, pat.rowidx.data(), sizeof(int64_t) * pat.rowidx.size());
+    if (comp) std::memcpy(comp, cv.data(), sizeof(double) * cv.size());
+    return INLA_OK;
+  } catch (...) {
+    return map_exception();
+  }
+}
+
 }  // extern "C"

@@ -219,4 +219,65 @@ std::string projector(const Mesh2D& m, int64_t npts, const double* xy, std::vect
   return std::string();
 }
 
+std::string spde_components(int64_t n, const double* c0, const int64_t* gcp, const int64_t* gri, const double* gv,
+                            CscBlock& pat, std::vector<double>& comp) {
+  if (n <= 0) return "SPDE requires non-empty FEM blocks";
+  std::vector<double> cinv(n);
+  for (int64_t i = 0; i < n; ++i) {
+    if (std::fabs(c0[i]) < 1e-15) return "Zero entry in mass matrix c0 diagonal";
+    cinv[i] = 1.0 / c0[i];
+  }
+  pat = CscBlock();
+  pat.n = n;
+  pat.colptr.assign(n + 1, 0);
+  std::vector<double> vc, vg, vgcg;            // the three components, aligned with pat.rowidx
+  std::vector<double> acc(n, 0.0), gcol(n, 0.0);
+  std::vector<char> mark(n, 0);
+  std::vector<int64_t> rows;
+  std::vector<std::pair<int64_t, double>> kcol;
+  for (int64_t j = 0; j < n; ++j) {
+    rows.clear();
+    auto touch = [&](int64_t i) {
+      if (!mark[i]) {
+        mark[i] = 1;
+        rows.push_back(i);
+      }
+    };
+    touch(j);
+    kcol.clear();
+    for (int64_t p = gcp[j]; p < gcp[j + 1]; ++p) {
+      touch(gri[p]);
+      gcol[gri[p]] += gv[p];
+      kcol.push_back({gri[p], gv[p]});
+    }
+    std::stable_sort(kcol.begin(), kcol.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    // column j of G1 C0^-1 G1: for each G1_kj (k ascending) add (G1_ik cinv_k) G1_kj, with G1_ik
+    // read from column k (G1 is symmetric)
+    for (const auto& kv : kcol) {
+      const int64_t k = kv.first;
+      for (int64_t p = gcp[k]; p < gcp[k + 1]; ++p) {
+        touch(gri[p]);
+        acc[gri[p]] += (gv[p] * cinv[k]) * kv.second;
+      }
+    }
+    std::sort(rows.begin(), rows.end());
+    for (int64_t i : rows) {
+      pat.rowidx.push_back(i);
+      vc.push_back(i == j ? c0[j] : 0.0);
+      vg.push_back(gcol[i]);
+      vgcg.push_back(acc[i]);
+      acc[i] = gcol[i] = 0.0;
+      mark[i] = 0;
+    }
+    pat.colptr[j + 1] = (int64_t)pat.rowidx.size();
+  }
+  const size_t nnz = pat.rowidx.size();
+  pat.val.assign(nnz, 1.0);
+  comp.resize(3 * nnz);
+  std::copy(vc.begin(), vc.end(), comp.begin());
+  std::copy(vg.begin(), vg.end(), comp.begin() + nnz);
+  std::copy(vgcg.begin(), vgcg.end(), comp.begin() + 2 * nnz);
+  return std::string();
+}
+
 }  // namespace inla

@@ -50,4 +50,13 @@ int64_t locate_point(const Mesh2D& m, int64_t start, double px, double py, doubl
 std::string projector(const Mesh2D& m, int64_t npts, const double* xy, std::vector<int64_t>& rowptr,
                       std::vector<int64_t>& colidx, std::vector<double>& val);
 
+// spde_precision_csc (crates/inla_stats/src/spde.rs:70-140) as components on one pattern:
+// Q = tau^2 kappa^4 C0 + 2 tau^2 kappa^2 G1 + tau^2 G1 C0^-1 G1. c0: lumped mass diagonal;
+// G1 in CSC with both triangles. The pattern is the union of the diagonal, G1 and
+// G1 C0^-1 G1 (rows sorted); comp [3][nnz]. Entry (i, j) of G1 C0^-1 G1 is
+// sum_k (G1_ik (1 / c0_k)) G1_kj over ascending k, the order of the reference's sparse
+// products. Empty string on success, else the reference's error.
+std::string spde_components(int64_t n, const double* c0, const int64_t* gcp, const int64_t* gri, const double* gv,
+                            CscBlock& pattern, std::vector<double>& comp);
+
 }  // namespace inla

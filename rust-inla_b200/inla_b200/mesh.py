@@ -73,3 +73,22 @@ class Mesh:
         check(lib().inla_mesh_projector(self._h, n, dptr(p), lptr(rp), lptr(ci), dptr(v)))
         nnz = int(rp[-1])
         return sp.csr_matrix((v[:nnz], ci[:nnz], rp), shape=(n, self.nv))
+
+
+def spde_components(c0, g):
+    """``spde_precision_csc`` (spde.rs:70-140) as components on one pattern through
+    ``inla_spde_components``: ``(pattern, comp_values [3][nnz])`` for C0, G1 and
+    G1 C0^-1 G1, the coefficients being tau^2 (kappa^4, 2 kappa^2, 1)."""
+    c0 = as_f64(c0)
+    g = sp.csc_matrix(g)
+    n = len(c0)
+    cp, ri, v = as_i64(g.indptr), as_i64(g.indices), as_f64(g.data)
+    nnz = C.c_int64()
+    check(lib().inla_spde_components(n, dptr(c0), lptr(cp), lptr(ri), dptr(v), C.byref(nnz), None, None, None))
+    pcp = np.zeros(n + 1, dtype=np.int64)
+    pri = np.zeros(nnz.value, dtype=np.int64)
+    comp = np.zeros((3, nnz.value))
+    check(lib().inla_spde_components(n, dptr(c0), lptr(cp), lptr(ri), dptr(v), None, lptr(pcp), lptr(pri),
+                                     dptr(comp)))
+    pattern = sp.csc_matrix((np.ones(nnz.value), pri, pcp), shape=(n, n))
+    return pattern, comp

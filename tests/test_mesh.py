@@ -118,3 +118,56 @@ def test_projector_at_full_mesh_size():
     np.testing.assert_allclose(np.asarray(a.sum(1)).ravel(), 1.0, atol=1e-13)
     lin = 0.3 + 1.7 * v[:, 0] - 0.9 * v[:, 1]
     np.testing.assert_allclose(a @ lin, 0.3 + 1.7 * pts[:, 0] - 0.9 * pts[:, 1], atol=1e-12)
+
+
+# --- SPDE precision components (crates/inla_stats/src/spde.rs) -----------------------------------
+
+from inla_b200.mesh import spde_components  # noqa: E402
+
+
+def test_projector_interpolates_at_vertices():
+    """spde.rs:149-161: a point at vertex 0 of a single triangle."""
+    a = Mesh([[0.0, 0.0], [1.0, 0.0], [0.0, 1.0]], [[0, 1, 2]]).projector([[0.0, 0.0]])
+    assert a.shape == (1, 3)
+    assert abs(a[0, 0] - 1.0) < 1e-12 and abs(a[0, 1]) < 1e-12
+
+
+def _q_from_components(pattern, comp, kappa, tau):
+    c = tau * tau * np.array([kappa ** 4, 2 * kappa ** 2, 1.0])
+    return sp.csc_matrix((c @ comp, pattern.indices, pattern.indptr), shape=pattern.shape)
+
+
+def test_spde_precision_square_mesh():
+    """spde.rs:163-189: kappa = 1, tau = 2 on the 2-triangle square: positive diagonal; the
+    components give the oracle's restatement of spde_precision_csc."""
+    v = [[0.0, 1.0], [1.0, 1.0], [0.0, 0.0], [1.0, 0.0]]
+    f = Mesh(v, [[0, 2, 1], [1, 2, 3]]).fem()
+    pattern, comp = spde_components(f["c0"].diagonal(), f["g1"])
+    q = _q_from_components(pattern, comp, 1.0, 2.0)
+    assert q.shape == (4, 4) and q.nnz > 0 and np.all(q.diagonal() > 0)
+    ref, _ = O.spde_precision(f["c0"].diagonal(), f["g1"], 1.0, 2.0)
+    dense = np.zeros((4, 4))
+    for (i, j), x in ref.items():
+        dense[i, j] = x
+    np.testing.assert_allclose(q.toarray(), dense, rtol=1e-14, atol=1e-14)
+
+
+def test_spde_components_match_oracle_and_generator():
+    v, t = _jittered(15, 13)
+    f = Mesh(v, t).fem()
+    c0, g = f["c0"].diagonal(), f["g1"]
+    pattern, comp = spde_components(c0, g)
+    _, gcg = O.spde_precision(c0, g, 1.0, 1.0)
+    got = sp.csc_matrix((comp[2], pattern.indices, pattern.indptr), shape=pattern.shape).tocoo()
+    d = {(int(r), int(c)): x for r, c, x in zip(got.row, got.col, got.data)}
+    assert {k: x for k, x in d.items() if k in gcg} == gcg          # bit for bit, same sum order
+    assert all(x == 0.0 for k, x in d.items() if k not in gcg)     # diagonal-only fill
+    lm = models.build_latent(len(c0), models.spde_components(c0, g), "spde")
+    assert (lm.pattern != pattern).nnz == 0
+    np.testing.assert_allclose(comp, lm.comp_values, rtol=1e-13, atol=1e-13 * np.abs(comp).max())
+
+
+def test_spde_components_reject_zero_mass():
+    g = sp.identity(3, format="csc")
+    with pytest.raises(InlaError, match="Zero entry in mass matrix"):
+        spde_components([1.0, 0.0, 1.0], g)
