@@ -156,6 +156,15 @@ int inla_mesh_locate(const inla_mesh* m, int64_t npts, const double* xy, int64_t
 int inla_mesh_projector(const inla_mesh* m, int64_t npts, const double* xy, int64_t* rowptr, int64_t* colidx,
                         double* vals);
 
+/* 1-D meshes (crates/inla_fmesher/src/mesh1d.rs): loc [n] strictly increasing finite knots.
+ * inla_mesh1d_fem: block `which` (0 c0, 1 c1, 2 g1, 3 b1 = empty) in CSC, nnz first with NULL
+ * arrays. inla_mesh1d_projector: A (npts x n) in CSR, rows (1 - w) x_i + w x_{i+1}, locations
+ * outside [loc_0, loc_{n-1}] clamped to the end knots; colidx / vals at most 2 npts. */
+int inla_mesh1d_fem(int64_t n, const double* loc, int which, int64_t* nnz, int64_t* colptr, int64_t* rowidx,
+                    double* vals);
+int inla_mesh1d_projector(int64_t n, const double* loc, int64_t npts, const double* s, int64_t* rowptr,
+                          int64_t* colidx, double* vals);
+
 /* spde_precision_csc (crates/inla_stats/src/spde.rs:70-140) as the three components of
  * inla_laplace_create on one pattern: Q(theta) = c_0 C0 + c_1 G1 + c_2 G1 C0^-1 G1 with
  * (c_0, c_1, c_2) = tau^2 (kappa^4, 2 kappa^2, 1) (inla_theta_map_spde). c0: the lumped mass

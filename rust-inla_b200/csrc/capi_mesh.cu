@@ -97,6 +97,45 @@ int inla_mesh_projector(const inla_mesh* h, int64_t npts, const double* xy, int6
   }
 }
 
+int inla_mesh1d_fem(int64_t n, const double* loc, int which, int64_t* nnz, int64_t* colptr, int64_t* rowidx,
+                    double* vals) {
+  try {
+    if (!loc || which < 0 || which > 3) return fail(INLA_ERR_INVALID, "inla_mesh1d_fem: invalid argument");
+    const std::string err = check_mesh1d(n, loc);
+    if (!err.empty()) return fail(INLA_ERR_INVALID, err);
+    FemBlocks f;
+    assemble_fem1d(n, loc, f);
+    const CscBlock& b = which == 0 ? f.c0 : which == 1 ? f.c1 : which == 2 ? f.g1 : f.b1;
+    if (nnz) *nnz = (int64_t)b.rowidx.size();
+    if (colptr) std::memcpy(colptr, b.colptr.data(), sizeof(int64_t) * b.colptr.size());
+    if (rowidx) std::memcpy(rowidx, b.rowidx.data(), sizeof(int64_t) * b.rowidx.size());
+    if (vals) std::memcpy(vals, b.val.data(), sizeof(double) * b.val.size());
+    return INLA_OK;
+  } catch (...) {
+    return map_exception();
+  }
+}
+
+int inla_mesh1d_projector(int64_t n, const double* loc, int64_t npts, const double* s, int64_t* rowptr,
+                          int64_t* colidx, double* vals) {
+  try {
+    if (!loc || npts < 0 || (npts > 0 && !s) || !rowptr || !colidx || !vals)
+      return fail(INLA_ERR_INVALID, "inla_mesh1d_projector: invalid argument");
+    std::string err = check_mesh1d(n, loc);
+    if (!err.empty()) return fail(INLA_ERR_INVALID, err);
+    std::vector<int64_t> rp, ci;
+    std::vector<double> v;
+    err = projector1d(n, loc, npts, s, rp, ci, v);
+    if (!err.empty()) return fail(INLA_ERR_INVALID, err);
+    std::memcpy(rowptr, rp.data(), sizeof(int64_t) * rp.size());
+    std::memcpy(colidx, ci.data(), sizeof(int64_t) * ci.size());
+    std::memcpy(vals, v.data(), sizeof(double) * v.size());
+    return INLA_OK;
+  } catch (...) {
+    return map_exception();
+  }
+}
+
 int inla_spde_components(int64_t n, const double* c0, const int64_t* g_colptr, const int64_t* g_rowidx,
                          const double* g_vals, int64_t* nnz, int64_t* colptr, int64_t* rowidx, double* comp) {
   try {

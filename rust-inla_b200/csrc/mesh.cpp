@@ -219,6 +219,82 @@ std::string projector(const Mesh2D& m, int64_t npts, const double* xy, std::vect
   return std::string();
 }
 
+std::string check_mesh1d(int64_t n, const double* loc) {
+  if (n < 2) return "1D mesh requires at least two knots";
+  for (int64_t i = 0; i < n; ++i) {
+    if (!std::isfinite(loc[i])) return "1D mesh knot " + std::to_string(i) + " is not finite";
+    if (i > 0 && loc[i] <= loc[i - 1]) return "1D mesh knots must be strictly increasing";
+  }
+  return std::string();
+}
+
+void assemble_fem1d(int64_t n, const double* loc, FemBlocks& out) {
+  std::vector<std::tuple<int64_t, int64_t, double>> c0, c1, g1, b1;
+  out.area.clear();
+  for (int64_t i = 0; i + 1 < n; ++i) {
+    const double h = loc[i + 1] - loc[i];
+    out.area.push_back(h);
+    c0.emplace_back(i, i, h / 2.0);
+    c0.emplace_back(i + 1, i + 1, h / 2.0);
+    c1.emplace_back(i, i, h / 3.0);
+    c1.emplace_back(i + 1, i + 1, h / 3.0);
+    c1.emplace_back(i, i + 1, h / 6.0);
+    c1.emplace_back(i + 1, i, h / 6.0);
+    const double inv_h = 1.0 / h;
+    g1.emplace_back(i, i, inv_h);
+    g1.emplace_back(i + 1, i + 1, inv_h);
+    g1.emplace_back(i, i + 1, -inv_h);
+    g1.emplace_back(i + 1, i, -inv_h);
+  }
+  out.c0 = coalesce(n, c0);
+  out.c1 = coalesce(n, c1);
+  out.g1 = coalesce(n, g1);
+  out.b1 = coalesce(n, b1);
+}
+
+std::string projector1d(int64_t n, const double* loc, int64_t npts, const double* s, std::vector<int64_t>& rowptr,
+                        std::vector<int64_t>& colidx, std::vector<double>& val) {
+  rowptr.assign(npts + 1, 0);
+  colidx.clear();
+  val.clear();
+  for (int64_t r = 0; r < npts; ++r) {
+    const double x = s[r];
+    if (!std::isfinite(x)) return "1D observation location " + std::to_string(r) + " is not finite";
+    int64_t i;
+    double w;
+    if (x <= loc[0]) {
+      i = 0;
+      w = 0.0;
+    } else if (x >= loc[n - 1]) {
+      i = n - 2;
+      w = 1.0;
+    } else {  // bisection for loc[lo] <= x < loc[lo + 1]
+      int64_t lo = 0, hi = n - 1;
+      while (lo + 1 < hi) {
+        const int64_t mid = (lo + hi) / 2;
+        if (loc[mid] <= x) lo = mid;
+        else hi = mid;
+      }
+      i = lo;
+      w = (x - loc[lo]) / (loc[lo + 1] - loc[lo]);
+    }
+    if (std::fabs(w) <= kGeomEps) {
+      colidx.push_back(i);
+      val.push_back(1.0);
+    } else if (std::fabs(w - 1.0) <= kGeomEps) {
+      colidx.push_back(i + 1);
+      val.push_back(1.0);
+    } else {
+      colidx.push_back(i);
+      val.push_back(1.0 - w);
+      colidx.push_back(i + 1);
+      val.push_back(w);
+    }
+    rowptr[r + 1] = (int64_t)colidx.size();
+  }
+  return std::string();
+}
+
 std::string spde_components(int64_t n, const double* c0, const int64_t* gcp, const int64_t* gri, const double* gv,
                             CscBlock& pat, std::vector<double>& comp) {
   if (n <= 0) return "SPDE requires non-empty FEM blocks";

@@ -50,6 +50,14 @@ int64_t locate_point(const Mesh2D& m, int64_t start, double px, double py, doubl
 std::string projector(const Mesh2D& m, int64_t npts, const double* xy, std::vector<int64_t>& rowptr,
                       std::vector<int64_t>& colidx, std::vector<double>& val);
 
+// 1-D meshes (crates/inla_fmesher/src/mesh1d.rs): knots strictly increasing and finite;
+// blocks c0 / c1 / g1 (b1 empty) summed like the 2-D ones; projector rows (1 - w) x_i + w x_{i+1}
+// with locations outside the knot range clamped to the end knots.
+std::string check_mesh1d(int64_t n, const double* loc);
+void assemble_fem1d(int64_t n, const double* loc, FemBlocks& out);
+std::string projector1d(int64_t n, const double* loc, int64_t npts, const double* s, std::vector<int64_t>& rowptr,
+                        std::vector<int64_t>& colidx, std::vector<double>& val);
+
 // spde_precision_csc (crates/inla_stats/src/spde.rs:70-140) as components on one pattern:
 // Q = tau^2 kappa^4 C0 + 2 tau^2 kappa^2 G1 + tau^2 G1 C0^-1 G1. c0: lumped mass diagonal;
 // G1 in CSC with both triangles. The pattern is the union of the diagonal, G1 and

@@ -119,6 +119,8 @@ SIGNATURES = [
     ("inla_mesh_locate", C.c_int, [P, I64, DP, LP, DP]),
     ("inla_mesh_projector", C.c_int, [P, I64, DP, LP, LP, DP]),
     ("inla_spde_components", C.c_int, [I64, DP, LP, LP, DP, LP, LP, LP, DP]),
+    ("inla_mesh1d_fem", C.c_int, [I64, DP, C.c_int, LP, LP, LP, DP]),
+    ("inla_mesh1d_projector", C.c_int, [I64, DP, I64, DP, LP, LP, DP]),
     ("inla_predictor_moments", C.c_int, [I64, I64, LP, LP, DP, C.c_int, DP, DP, DP, DP, DP]),
     ("inla_fit_model_selection", C.c_int, [P, C.c_int, DP, DP, DP]),
     ("inla_model_selection", C.c_int, [C.c_int, I64, DP, DP, DP, C.c_int, DP, C.c_int, DP, DP, C.c_int, DP, DP,

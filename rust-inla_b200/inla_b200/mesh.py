@@ -75,6 +75,37 @@ class Mesh:
         return sp.csr_matrix((v[:nnz], ci[:nnz], rp), shape=(n, self.nv))
 
 
+class Mesh1D:
+    """``build_mesh1d`` (mesh1d.rs:15-34): knots strictly increasing."""
+
+    def __init__(self, loc):
+        self.loc = as_f64(np.ravel(loc))
+        self.n = len(self.loc)
+
+    def fem(self):
+        """``assemble_fem_blocks`` (mesh1d.rs:42-79): CSC blocks ``c0``, ``c1``, ``g1``, ``b1``."""
+        out = {}
+        for which, name in enumerate(FEM_BLOCKS):
+            nnz = C.c_int64()
+            check(lib().inla_mesh1d_fem(self.n, dptr(self.loc), which, C.byref(nnz), None, None, None))
+            cp = np.zeros(self.n + 1, dtype=np.int64)
+            ri = np.zeros(nnz.value, dtype=np.int64)
+            v = np.zeros(nnz.value)
+            check(lib().inla_mesh1d_fem(self.n, dptr(self.loc), which, None, lptr(cp), lptr(ri), dptr(v)))
+            out[name] = sp.csc_matrix((v, ri, cp), shape=(self.n, self.n))
+        return out
+
+    def projector(self, s):
+        """``observation_projector_triplets`` (mesh1d.rs:85-110) as a CSR matrix."""
+        s = as_f64(np.ravel(s))
+        rp = np.zeros(len(s) + 1, dtype=np.int64)
+        ci = np.zeros(2 * len(s), dtype=np.int64)
+        v = np.zeros(2 * len(s))
+        check(lib().inla_mesh1d_projector(self.n, dptr(self.loc), len(s), dptr(s), lptr(rp), lptr(ci), dptr(v)))
+        nnz = int(rp[-1])
+        return sp.csr_matrix((v[:nnz], ci[:nnz], rp), shape=(len(s), self.n))
+
+
 def spde_components(c0, g):
     """``spde_precision_csc`` (spde.rs:70-140) as components on one pattern through
     ``inla_spde_components``: ``(pattern, comp_values [3][nnz])`` for C0, G1 and

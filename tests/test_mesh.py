@@ -171,3 +171,42 @@ def test_spde_components_reject_zero_mass():
     g = sp.identity(3, format="csc")
     with pytest.raises(InlaError, match="Zero entry in mass matrix"):
         spde_components([1.0, 0.0, 1.0], g)
+
+
+# --- 1-D meshes (crates/inla_fmesher/src/mesh1d.rs:143-190) ---------------------------------------
+
+from inla_b200.mesh import Mesh1D  # noqa: E402
+
+
+def test_mesh1d_unit_interval_two_knots():
+    f = Mesh1D([0.0, 1.0]).fem()
+    assert f["c0"][0, 0] == 0.5 and f["c0"][1, 1] == 0.5
+    assert abs(f["g1"][0, 0] - 1.0) < 1e-14 and abs(f["g1"][0, 1] + 1.0) < 1e-14
+    assert f["b1"].nnz == 0
+
+
+def test_mesh1d_projector_at_knots_and_midpoint():
+    a = Mesh1D([0.0, 2.0, 5.0]).projector([0.0, 2.0, 3.5, 5.0, -1.0, 9.0]).toarray()
+    assert abs(a[0, 0] - 1) < 1e-12 and abs(a[1, 1] - 1) < 1e-12
+    assert abs(a[2, 1] - 0.5) < 1e-12 and abs(a[2, 2] - 0.5) < 1e-12
+    assert abs(a[3, 2] - 1) < 1e-12 and abs(a[4, 0] - 1) < 1e-12 and abs(a[5, 2] - 1) < 1e-12
+
+
+def test_mesh1d_rejects_unsorted():
+    with pytest.raises(InlaError):
+        Mesh1D([1.0, 0.0]).fem()
+    with pytest.raises(InlaError):
+        Mesh1D([0.0, 0.0]).projector([0.5])
+
+
+def test_mesh1d_spde_precision_positive_diagonal():
+    """spde.rs:205-213: the 1-D blocks feed the same SPDE components."""
+    f = Mesh1D([0.0, 1.0, 2.0, 3.0]).fem()
+    pattern, comp = spde_components(f["c0"].diagonal(), f["g1"])
+    q = _q_from_components(pattern, comp, 1.0, 2.0)
+    assert q.shape == (4, 4) and np.all(q.diagonal() > 0)
+    rng = np.random.default_rng(14)
+    knots = np.cumsum(rng.uniform(0.1, 1.0, 40))
+    f = Mesh1D(knots).fem()
+    h = np.diff(knots)
+    np.testing.assert_array_equal(f["c0"].diagonal(), np.r_[h / 2, 0.0] + np.r_[0.0, h / 2])
