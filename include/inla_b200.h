@@ -412,7 +412,8 @@ int inla_model_selection(int family, int64_t nobs, const double* y, const double
  * positive definite. */
 int inla_mlik_gaussian(double log_post_mode, int m, const double* neg_hessian, double* out);
 /* observation_cdf (model_selection.rs:398-448): F(y | eta, variance) of one observation;
- * INLA_ERR_INVALID where the reference gives None (negative binomial, invalid rate). */
+ * INLA_ERR_INVALID where the reference gives None (negative binomial, invalid rate), and for a
+ * non-finite y or a count above 1e15 (whose term-by-term CDF sum the reference would loop over). */
 int inla_observation_cdf(int family, double y, double p1, double eta, double variance, double* out);
 /* check_cpo_failure_for_obs (model_selection.rs:327-396): 1 when the CPO of this observation is
  * flagged unreliable at posterior mean mu and variance var of its predictor, else 0. */

@@ -28,7 +28,9 @@ bool lik_at(const ObsView& obs, int64_t i, double eta, Lik& out) {
 }  // namespace
 
 bool observation_cdf(int family, double y, double p1, double eta, double variance, double& out) {
-  if (!std::isfinite(y)) return false;  // the count CDFs below sum up to floor(y)
+  // the count CDFs below sum term by term up to floor(y); counts beyond 1e15 (and non-finite y)
+  // get no CDF instead of a loop of that length
+  if (!std::isfinite(y) || (family != FAM_GAUSSIAN && y > 1e15)) return false;
   switch (family) {
     case FAM_GAUSSIAN: {
       const double total_var = 1.0 / p1 + variance;
@@ -55,7 +57,7 @@ bool observation_cdf(int family, double y, double p1, double eta, double varianc
         out = 0.0;
         return true;
       }
-      out = binomial_cdf(n, prob, std::min((uint64_t)yf, n));
+      out = binomial_cdf(n, prob, yf >= (double)n ? n : (uint64_t)yf);
       return true;
     }
     default:
