@@ -95,3 +95,9 @@ def test_large_lattice_against_oracle_bordered_factor():
     ref = O.Factor(m, perm=full).diag_inv()[:n]
     np.testing.assert_allclose(d, ref, rtol=1e-10)
     assert abs(fac - np.exp(np.mean(np.log(ref)))) < 1e-10 * fac
+
+
+def test_identity_scale_is_one():
+    """design.rs:234-243: Q = I gives ginv = I and a factor of 1."""
+    qs, fac, d = scale_model(sp.identity(4, format="csc"))
+    assert abs(fac - 1.0) < 1e-8 and np.all(np.abs(qs.diagonal() - 1.0) < 1e-8)

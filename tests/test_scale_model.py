@@ -27,3 +27,11 @@ def test_rows_with_the_same_single_support_are_rejected():
         scale_model(r, null_basis=np.vstack([u, u, u]))
     with pytest.raises(InlaError):
         scale_model(sp.csc_matrix((3, 3)))   # no nonzero
+
+
+def test_dense_generator_identity_scale_is_one():
+    """design.rs:234-243 on the generator's dense restatement (models.scale_model)."""
+    from inla_b200 import models
+
+    qs, fac = models.scale_model(sp.identity(4, format="csc"))
+    assert abs(fac - 1.0) < 1e-8 and np.all(np.abs(qs.diagonal() - 1.0) < 1e-8)
