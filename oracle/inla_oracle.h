@@ -1,6 +1,6 @@
 /*
  * CPU ORACLE — test infrastructure only. A plain-C restatement of
- * rust-inla's INLA inner path, used by tests/ (as the checker) and by
+ * rust-inla's INLA inner path, used by tests/ (to check the library) and by
  * bench.py's cpu_baseline / --impl reference leg (as the timed CPU path).
  * It is never linked into, called by or shipped with the product library.
  *
