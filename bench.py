@@ -73,6 +73,20 @@ def dist_setup(args):
     return ws, rank, local, pg
 
 
+def combine_over_ranks(dist, ms, evals, device):
+    """Whole-job figures of the replicas: the slowest rank's device time and the sum of every
+    rank's theta-evaluations. Every rank takes the same two collectives in the same order."""
+    if dist is None:
+        return float(ms), float(evals)
+    import torch
+
+    tmax = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    tsum = torch.tensor([float(evals)], dtype=torch.float64, device=device)
+    dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+    return float(tmax[0]), float(tsum[0])
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -312,15 +326,7 @@ def run_ours(args, ws, rank, local, dist):
     barrier()
     clocks = sampler.stop()
     launches = lib().inla_kernel_launches() - launches0
-    ms_total = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([ms_total, float(evals)], dtype=torch.float64, device="cuda")
-        tmax = t.clone()
-        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
-        ms_total, evals_all = float(tmax[0]), float(t[1])
-    else:
-        evals_all = float(evals)
+    ms_total, evals_all = combine_over_ranks(dist, e0.elapsed_time(e1), evals, "cuda")
     value = evals_all / (ms_total * 1e-3)
     last = fits[-1]
 

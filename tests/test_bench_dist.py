@@ -1,0 +1,77 @@
+"""The replicas-only multi-rank path of bench.py on CPU: two gloo ranks (no GPU), the
+max-over-ranks time and the summed evaluations, and the reference arm's rank-0-only rule."""
+import os
+import socket
+import sys
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, ws, port, out):
+    import datetime
+
+    import torch.distributed as dist
+
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=ws, timeout=datetime.timedelta(seconds=60))
+    try:
+        ms = [12.5, 30.0][rank]
+        evals = [100, 157][rank]
+        out.put((rank, bench.combine_over_ranks(dist, ms, evals, "cpu")))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_take_max_time_and_summed_evaluations():
+    import torch.multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    got = dict(q.get(timeout=10) for _ in range(2))
+    assert got[0] == got[1] == (30.0, 257.0)
+
+
+def test_single_rank_needs_no_collective():
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    assert bench.combine_over_ranks(None, 7.0, 21, "cpu") == (7.0, 21.0)
+
+
+def test_reference_arm_runs_on_rank_zero_only(capsys):
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    class Args:
+        gpus, steps, warmup, cpu_seconds, nx, nobs = 2, 1, 0, 0.1, 10, 50
+
+    assert bench.run_reference(Args(), 2, 1) == 0
+    assert capsys.readouterr().out == ""
+
+
+def test_dist_setup_without_torchrun_is_single_rank(monkeypatch):
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    for k in ("WORLD_SIZE", "RANK", "LOCAL_RANK"):
+        monkeypatch.delenv(k, raising=False)
+    assert bench.dist_setup(None) == (1, 0, 0, None)
