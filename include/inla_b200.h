@@ -400,6 +400,21 @@ int inla_fit_predictor(inla_laplace* h, double* pred_mean, double* pred_var);
 enum { INLA_MS_DIC = 1, INLA_MS_WAIC = 2, INLA_MS_CPO = 4, INLA_MS_ALL = 7 };
 int inla_fit_model_selection(inla_laplace* h, int what, double* crit, double* cpo, double* pit);
 
+/* Marginal densities of the last inla_fit on h on a uniform grid (marginals.rs): kind 0 the
+ * latent entry `index`, 1 the predictor entry `index` (gaussian_mixture_marginal over the nodes,
+ * 73-135), 2 the hyperparameter `index` on the internal scale (hyperpar_marginal_from_nodes,
+ * 137-162). x, y: [n_points] (n_points >= 5); the grid spans mean +- max(n_sd, 1) sd and y has
+ * unit trapezoid mass. The reference's defaults are 201 points and n_sd = 4. */
+int inla_fit_marginal(inla_laplace* h, int kind, int64_t index, int n_points, double n_sd, double* x, double* y);
+/* Host-only forms: a mixture from the caller's node means / variances / weights, a hyperparameter
+ * kernel density from node values, and quantiles of a gridded density (marginal_quantiles,
+ * marginals.rs:202-226; probabilities in (0, 1)). */
+int inla_mixture_marginal(int K, const double* means, const double* vars, const double* weights, int n_points,
+                          double n_sd, double* x, double* y);
+int inla_hyperpar_marginal(int K, const double* theta, const double* weights, int n_points, double n_sd, double* x,
+                           double* y);
+int inla_marginal_quantiles(int n, const double* x, const double* y, int np, const double* probs, double* q);
+
 /* Host-only: the same criteria from a caller's node results (crit[6] is NaN). family: as in
  * inla_laplace_create (0 gaussian, 1 poisson, 2 binomial, 3 negative binomial); y, p1, p2: [nobs] (p1 gaussian precision / poisson exposure / binomial trials /
  * nb size, p2 nb exposure; NULL = 1); weight: [K] normalised; mode_index: the node of D(theta*);

@@ -943,3 +943,85 @@ def spde_precision(c0_diag, g1, kappa, tau):
         q[key] = q.get(key, 0.0) + v
     t2 = tau * tau
     return {key: v * t2 for key, v in q.items()}, gcg
+
+
+# ---------------------------------------------------------------------------
+# one-dimensional marginals (crates/inla_stats/src/marginals.rs)
+# ---------------------------------------------------------------------------
+
+def _phi(x, mu, var):
+    """marginals.rs:73-80."""
+    if not (var > 0.0 and math.isfinite(var)):
+        return 0.0
+    s = math.sqrt(var)
+    z = (x - mu) / s
+    return math.exp(-0.5 * z * z) / (s * math.sqrt(2.0 * math.pi))
+
+
+def _trapezoid(x, y):
+    """Marginal1D::integrate (marginals.rs:20-30)."""
+    s = 0.0
+    for i in range(len(x) - 1):
+        s += 0.5 * (y[i] + y[i + 1]) * (x[i + 1] - x[i])
+    return s
+
+
+def gaussian_mixture_marginal(means, vars_, weights, n_points=201, n_sd=4.0):
+    """marginals.rs:83-135: (x, y) with unit trapezoid mass."""
+    K = len(means)
+    mu = 0.0
+    for k in range(K):
+        mu += weights[k] * means[k]
+    var = 0.0
+    for k in range(K):
+        d = means[k] - mu
+        var += weights[k] * (vars_[k] + d * d)
+    if not (var > 0.0 and math.isfinite(var)):
+        var = 1e-8
+    half = max(n_sd, 1.0) * math.sqrt(var)
+    lo, hi = mu - half, mu + half
+    x, y = [], []
+    for i in range(n_points):
+        xi = lo + (hi - lo) * float(i) / float(n_points - 1)
+        yi = 0.0
+        for k in range(K):
+            yi += weights[k] * _phi(xi, means[k], vars_[k])
+        x.append(xi)
+        y.append(yi)
+    mass = _trapezoid(x, y)
+    if mass > 0.0 and math.isfinite(mass):
+        y = [v / mass for v in y]
+    return np.array(x), np.array(y)
+
+
+def hyperpar_marginal_from_nodes(theta_j, weights, n_points=201, n_sd=4.0):
+    """marginals.rs:137-162."""
+    mu = 0.0
+    for k in range(len(theta_j)):
+        mu += weights[k] * theta_j[k]
+    v = 0.0
+    for k in range(len(theta_j)):
+        d = theta_j[k] - mu
+        v += weights[k] * d * d
+    h2 = max(v, 1e-8) * 1.0
+    return gaussian_mixture_marginal(list(theta_j), [h2] * len(theta_j), weights, n_points, n_sd)
+
+
+def marginal_quantiles(x, y, probs):
+    """marginal_cdf + marginal_quantiles (marginals.rs:183-226)."""
+    f = [0.0] * len(x)
+    for i in range(len(x) - 1):
+        f[i + 1] = f[i] + 0.5 * (y[i] + y[i + 1]) * (x[i + 1] - x[i])
+    mass = f[-1]
+    if mass > 0.0:
+        f = [v / mass for v in f]
+    out = []
+    for p in probs:
+        q = x[-1]
+        for i in range(1, len(f)):
+            if f[i] >= p:
+                t = 0.0 if abs(f[i] - f[i - 1]) < 1e-15 else (p - f[i - 1]) / (f[i] - f[i - 1])
+                q = x[i - 1] + t * (x[i] - x[i - 1])
+                break
+        out.append(q)
+    return np.array(out)

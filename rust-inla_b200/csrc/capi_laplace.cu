@@ -7,6 +7,7 @@
 #include "aggregate.hpp"
 #include "capi_common.hpp"
 #include "driver.hpp"
+#include "marginals.hpp"
 #include "model_select.hpp"
 #include "inla_b200.h"
 
@@ -18,8 +19,8 @@ struct inla_laplace {
   LaplaceSpec spec;  // the caller's model, before any constraint augmentation
   int max_batch = 0;
   // from the last inla_fit: linear predictor moments and the model-selection inputs
-  std::vector<double> pred_mean, pred_var, cond_eta, cond_eta_var, node_weight;
-  int mode_index = 0;
+  std::vector<double> pred_mean, pred_var, cond_eta, cond_eta_var, node_weight, cond_mean, cond_var, node_theta;
+  int mode_index = 0, m = 0;
   double p1scale_mode = 1.0, mlik_gaussian = 0.0;
   bool fitted = false;
 };
@@ -335,6 +336,10 @@ int inla_fit(inla_laplace* h, int m, const double* theta0, inla_theta_map_fn map
     h->cond_eta = std::move(R.cond_eta);
     h->cond_eta_var = std::move(R.cond_eta_var);
     h->node_weight = R.node_weight;
+    h->cond_mean = std::move(R.cond_mean);
+    h->cond_var = std::move(R.cond_var);
+    h->node_theta = R.node_theta;
+    h->m = m;
     h->mode_index = R.mode_index;
     h->p1scale_mode = R.p1scale_mode;
     h->mlik_gaussian = R.mlik_gaussian;
@@ -395,6 +400,60 @@ int inla_fit_model_selection(inla_laplace* h, int what, double* crit, double* cp
   } catch (...) {
     return map_exception();
   }
+}
+
+int inla_fit_marginal(inla_laplace* h, int kind, int64_t index, int n_points, double n_sd, double* x, double* y) {
+  try {
+    if (!h || !h->fitted) return fail(INLA_ERR_INVALID, "inla_fit_marginal: no fit on this handle");
+    if (!x || !y || kind < 0 || kind > 2) return fail(INLA_ERR_INVALID, "inla_fit_marginal: invalid argument");
+    const int K = (int)h->node_weight.size();
+    std::vector<double> mk(K), vk(K);
+    std::string err;
+    if (kind == 2) {
+      if (index < 0 || index >= h->m) return fail(INLA_ERR_INVALID, "hyperparameter index out of range");
+      for (int k = 0; k < K; ++k) mk[k] = h->node_theta[(size_t)k * h->m + index];
+      err = hyperpar_marginal(K, mk.data(), h->node_weight.data(), n_points, n_sd, x, y);
+    } else {
+      const std::vector<double>& cm = kind == 0 ? h->cond_mean : h->cond_eta;
+      const std::vector<double>& cv = kind == 0 ? h->cond_var : h->cond_eta_var;
+      const int64_t len = (int64_t)cm.size() / std::max(K, 1);
+      if (index < 0 || index >= len)
+        return fail(INLA_ERR_INVALID, kind == 0 ? "latent marginal index out of range"
+                                                : "predictor marginal index out of range");
+      for (int k = 0; k < K; ++k) {
+        mk[k] = cm[(size_t)k * len + index];
+        vk[k] = cv[(size_t)k * len + index];
+      }
+      err = mixture_marginal(K, mk.data(), vk.data(), h->node_weight.data(), n_points, n_sd, x, y);
+    }
+    if (!err.empty()) return fail(INLA_ERR_INVALID, err);
+    return INLA_OK;
+  } catch (...) {
+    return map_exception();
+  }
+}
+
+int inla_mixture_marginal(int K, const double* means, const double* vars, const double* weights, int n_points,
+                          double n_sd, double* x, double* y) {
+  if (K < 0 || (K > 0 && (!means || !vars || !weights)) || !x || !y)
+    return fail(INLA_ERR_INVALID, "inla_mixture_marginal: invalid argument");
+  const std::string err = mixture_marginal(K, means, vars, weights, n_points, n_sd, x, y);
+  return err.empty() ? INLA_OK : fail(INLA_ERR_INVALID, err);
+}
+
+int inla_hyperpar_marginal(int K, const double* theta, const double* weights, int n_points, double n_sd, double* x,
+                           double* y) {
+  if (K < 0 || (K > 0 && (!theta || !weights)) || !x || !y)
+    return fail(INLA_ERR_INVALID, "inla_hyperpar_marginal: invalid argument");
+  const std::string err = hyperpar_marginal(K, theta, weights, n_points, n_sd, x, y);
+  return err.empty() ? INLA_OK : fail(INLA_ERR_INVALID, err);
+}
+
+int inla_marginal_quantiles(int n, const double* x, const double* y, int np, const double* probs, double* q) {
+  if (n < 0 || np < 0 || (n > 0 && (!x || !y)) || (np > 0 && (!probs || !q)))
+    return fail(INLA_ERR_INVALID, "inla_marginal_quantiles: invalid argument");
+  const std::string err = marginal_quantiles(n, x, y, np, probs, q);
+  return err.empty() ? INLA_OK : fail(INLA_ERR_INVALID, err);
 }
 
 int inla_model_selection(int family, int64_t nobs, const double* y, const double* p1, const double* p2, int K,

@@ -727,6 +727,8 @@ void InlaDriver::fit(const double* theta0, const FitOptions& opt, FitResult& out
                            : std::numeric_limits<double>::quiet_NaN();
   }
   out.mlik = mx + std::log(std::fabs(sw));
+  out.cond_mean = std::move(means);
+  out.cond_var = std::move(vars);
   out.node_theta = thetas;
   out.node_weight = nw;
   out.node_logpost = lp;

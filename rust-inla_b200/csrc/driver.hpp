@@ -41,6 +41,7 @@ struct FitResult {
   std::vector<double> mode, hessian, latent_mean, latent_var, node_theta, node_weight, node_logpost;
   std::vector<double> pred_mean, pred_var;  // linear predictor eta = A x: mixture mean and variance
   std::vector<double> cond_eta, cond_eta_var;  // [K][nobs] per-node predictor and its variance
+  std::vector<double> cond_mean, cond_var;     // [K][n] per-node mode and marginal variances
   int mode_index = 0;                          // node with the smallest |z| (inference.rs:1296-1304)
   double p1scale_mode = 1.0;                   // likelihood p1 scale at the mode (observations at the mode)
   double mlik_gaussian = 0.0;                  // Gaussian approximation of the log marginal likelihood

@@ -126,6 +126,10 @@ SIGNATURES = [
     ("inla_model_selection", C.c_int, [C.c_int, I64, DP, DP, DP, C.c_int, DP, C.c_int, DP, DP, C.c_int, DP, DP,
                                        DP]),
     ("inla_mlik_gaussian", C.c_int, [C.c_double, C.c_int, DP, DP]),
+    ("inla_fit_marginal", C.c_int, [P, C.c_int, I64, C.c_int, C.c_double, DP, DP]),
+    ("inla_mixture_marginal", C.c_int, [C.c_int, DP, DP, DP, C.c_int, C.c_double, DP, DP]),
+    ("inla_hyperpar_marginal", C.c_int, [C.c_int, DP, DP, C.c_int, C.c_double, DP, DP]),
+    ("inla_marginal_quantiles", C.c_int, [C.c_int, DP, DP, C.c_int, DP, DP]),
     ("inla_observation_cdf", C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, DP]),
     ("inla_cpo_failure", C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]),
     ("inla_theta_map_spde", C.c_int, [DP, C.c_int, DP, DP, DP, DP, P]),

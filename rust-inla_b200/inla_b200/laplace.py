@@ -163,6 +163,14 @@ class LaplaceModel:
         check(lib().inla_fit_model_selection(self._h, _what(criteria), dptr(crit), dptr(cpo), dptr(pit)))
         return _criteria_dict(crit, cpo, pit)
 
+    def marginal(self, kind, index, n_points=201, n_sd=4.0):
+        """Marginal density of the last :meth:`fit` (marginals.rs): ``kind`` "latent",
+        "predictor" or "hyperpar"; returns ``(x, y)``."""
+        x, y = np.zeros(n_points), np.zeros(n_points)
+        check(lib().inla_fit_marginal(self._h, {"latent": 0, "predictor": 1, "hyperpar": 2}[kind], int(index),
+                                      int(n_points), float(n_sd), dptr(x), dptr(y)))
+        return x, y
+
     def fit(self, theta0, theta_map="spde", priors=SPDE_DEFAULT_PRIORS, mode_search="nm", batched=False,
             strategy="ccd", f0=1.0, hessian="fd", max_iter=0, tol=0.0):
         """Full INLA fit; ``theta_map`` is ``"spde"`` or a Python callable
@@ -289,6 +297,33 @@ def model_selection(family, y, weights, mode_index, cond_eta, cond_eta_var, p1=N
                                      len(w), dptr(w), int(mode_index), dptr(ce), dptr(cv), _what(criteria),
                                      dptr(crit), dptr(cpo), dptr(pit)))
     return _criteria_dict(crit, cpo, pit)
+
+
+def mixture_marginal(means, vars_, weights, n_points=201, n_sd=4.0):
+    """gaussian_mixture_marginal (marginals.rs:83-135): ``(x, y)`` on a uniform grid."""
+    m, v, w = as_f64(np.ravel(means)), as_f64(np.ravel(vars_)), as_f64(np.ravel(weights))
+    if not (len(m) == len(v) == len(w)):
+        raise ValueError("mixture means/vars/weights length mismatch")
+    x, y = np.zeros(n_points), np.zeros(n_points)
+    check(lib().inla_mixture_marginal(len(m), dptr(m), dptr(v), dptr(w), int(n_points), float(n_sd), dptr(x),
+                                      dptr(y)))
+    return x, y
+
+
+def hyperpar_marginal(theta, weights, n_points=201, n_sd=4.0):
+    """hyperpar_marginal_from_nodes (marginals.rs:137-162): ``(x, y)``."""
+    t, w = as_f64(np.ravel(theta)), as_f64(np.ravel(weights))
+    x, y = np.zeros(n_points), np.zeros(n_points)
+    check(lib().inla_hyperpar_marginal(len(t), dptr(t), dptr(w), int(n_points), float(n_sd), dptr(x), dptr(y)))
+    return x, y
+
+
+def marginal_quantiles(x, y, probs=(0.025, 0.5, 0.975)):
+    """marginal_quantiles (marginals.rs:202-226)."""
+    x, y, pr = as_f64(np.ravel(x)), as_f64(np.ravel(y)), as_f64(np.ravel(probs))
+    q = np.zeros(len(pr))
+    check(lib().inla_marginal_quantiles(len(x), dptr(x), dptr(y), len(pr), dptr(pr), dptr(q)))
+    return q
 
 
 def mlik_gaussian(log_post_mode, neg_hessian):

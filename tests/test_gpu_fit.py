@@ -91,6 +91,29 @@ def test_model_selection_parity(problem):
     np.testing.assert_allclose(ms["pit"][both], [q for q, b in zip(pit, both) if b], rtol=1e-7, atol=1e-12)
 
 
+def test_fit_marginals_match_oracle(problem):
+    """Latent, predictor and hyperparameter marginals of a fit (marginals.rs:83-162) against the
+    oracle's restatement on the oracle's node results at the fit's nodes."""
+    p, lm = problem
+    r = lm.fit(THETA0, mode_search="nm", batched=True)
+    w = list(r["node_weight"])
+    nodes = []
+    for theta in r["node_theta"]:
+        c = O.spde_coefs(theta[1], theta[2])
+        lr = O.laplace(p.model.matrix(c), p.a, "gaussian", p.y, p1=np.exp(theta[0]), want_var=True)
+        nodes.append((lr["x"], lr["var"], O.matvec_csc(p.a, lr["x"]), O.predictor_variances_diag(p.a, lr["var"])))
+    for kind, idx, pos in [("latent", 0, 0), ("latent", p.model.n - 1, 0), ("predictor", 7, 2)]:
+        x, y = lm.marginal(kind, idx)
+        xo, yo = O.gaussian_mixture_marginal([nd[pos][idx] for nd in nodes], [nd[pos + 1][idx] for nd in nodes], w)
+        np.testing.assert_allclose(x, xo, rtol=1e-7, atol=1e-9 * np.max(np.abs(xo)))
+        np.testing.assert_allclose(y, yo, rtol=1e-6, atol=1e-9 * np.max(yo))
+    for j in range(3):
+        x, y = lm.marginal("hyperpar", j)
+        xo, yo = O.hyperpar_marginal_from_nodes(list(r["node_theta"][:, j]), w)
+        np.testing.assert_allclose(x, xo, rtol=1e-12, atol=1e-12)
+        np.testing.assert_allclose(y, yo, rtol=1e-9, atol=1e-12 * np.max(yo))
+
+
 @pytest.mark.parametrize("search", ["bfgs", "newton"])
 def test_batched_adjoint_fit_matches_plain(problem, search):
     p, lm = problem
