@@ -299,7 +299,9 @@ def run_ours(args, ws, rank, local, dist):
 
     torch.cuda.set_device(local)
     p = make_problem(args)
+    tc = time.perf_counter()
     lm = LaplaceModel(p.model, a=p.a, family="gaussian", y=p.y, max_batch=25)
+    create_first_s = time.perf_counter() - tc  # includes the symbolic analysis the later creations reuse
     fit_kw = dict(mode_search="newton", batched=True, tol=1e-4)
 
     def barrier():
@@ -330,8 +332,10 @@ def run_ours(args, ws, rank, local, dist):
     value = evals_all / (ms_total * 1e-3)
     last = fits[-1]
 
-    # e2e through the public API with host buffers: model creation (symbolic
-    # analysis + H2D of components, projector, data) + fit + D2H of results
+    # e2e through the public API with host buffers: model creation (H2D of the
+    # pattern, components, projector and data, device tables; the symbolic analysis
+    # of this pattern is the process-wide cached one, computed at the first
+    # creation, create_first_s) + fit + D2H of results
     e2e_ms, e2e_evals = 0.0, 0
     nnz = p.model.pattern.nnz
     h2d = 8 * (p.model.comp_values.size + p.y.size + p.a.nnz) + 8 * (p.model.n + 1 + nnz) + 8 * (
@@ -398,7 +402,8 @@ def run_ours(args, ws, rank, local, dist):
             "plain_gpu": plain,
             "speedup_vs_plain_gpu": (plain["fit_s"] / fit_s) if plain else None,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                    "fit_s": e2e_ms * 1e-3 / max(args.e2e_steps, 1), "create_fit_close_s": e2e_parts},
+                    "fit_s": e2e_ms * 1e-3 / max(args.e2e_steps, 1), "create_fit_close_s": e2e_parts,
+                    "create_first_s": round(create_first_s, 4)},
             "gpu_launches": int(launches), "clocks": clocks, "roofline": roof, "cpu_baseline": cpu}
     print(json.dumps(line), flush=True)
     return 0

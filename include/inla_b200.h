@@ -65,7 +65,10 @@ int64_t inla_kernel_launches(void);
  * holds at most half of a device's memory and is emptied automatically when an
  * allocation fails. This call returns all cached blocks to the driver (for other
  * users of the GPU in the same process). INLA_NO_MEMORY_CACHE in the environment
- * disables the cache. No reference counterpart. */
+ * disables the cache. Symbolic analyses are cached the same way, per exact pattern,
+ * ordering, options and permutation (at most 1 GiB of host memory; handles on the
+ * same pattern reuse the analysis), and this call empties that cache too;
+ * INLA_NO_SYMBOLIC_CACHE disables it. No reference counterpart. */
 int inla_release_cached_memory(void);
 
 /* ------------------------------------------------------------------------

@@ -102,6 +102,7 @@ int64_t inla_kernel_launches(void) { return g_launches.load(); }
 int inla_release_cached_memory(void) {
   try {
     device_release_cached();
+    release_symbolic_cache();
     return INLA_OK;
   } catch (...) {
     return map_exception();

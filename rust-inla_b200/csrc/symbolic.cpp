@@ -8,7 +8,11 @@
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <deque>
+#include <list>
+#include <memory>
+#include <mutex>
 #include <numeric>
 #include <stdexcept>
 #include <tuple>
@@ -239,8 +243,8 @@ void postorder(int64_t n, const std::vector<int64_t>& parent, std::vector<int64_
 
 }  // namespace
 
-void analyze(int64_t n, const int64_t* colptr, const int64_t* rowidx, const SymbolicOptions& opt,
-             const int64_t* custom_perm, Symbolic& S) {
+static void analyze_uncached(int64_t n, const int64_t* colptr, const int64_t* rowidx, const SymbolicOptions& opt,
+                             const int64_t* custom_perm, Symbolic& S) {
   const bool dbg = std::getenv("INLA_DEBUG") != nullptr;
   auto tprev = std::chrono::steady_clock::now();
   auto phase = [&](const char* name) {
@@ -556,6 +560,109 @@ void analyze(int64_t n, const int64_t* colptr, const int64_t* rowidx, const Symb
       }
   });
   phase("value map");
+}
+
+// ---- process-wide cache of analyses --------------------------------------
+// The analysis is a deterministic function of (n, colptr, rowidx, opt, custom_perm): the
+// ordering threads do not change its result and nothing else is read. Handles created on the
+// same pattern (a model rebuilt for new data, a solver per worker) therefore take a copy of the
+// cached analysis instead of repeating it. Entries are matched by byte-exact comparison of every
+// input, kept most recently used first, and bounded in bytes; INLA_NO_SYMBOLIC_CACHE disables the
+// cache.
+namespace {
+
+struct SymCacheEntry {
+  int64_t n = 0;
+  std::vector<int64_t> colptr, rowidx, custom;
+  bool has_custom = false;
+  SymbolicOptions opt;
+  Symbolic sym;
+  size_t bytes = 0;
+};
+
+constexpr size_t kSymCacheBytes = size_t(1) << 30;
+
+std::mutex g_sym_mu;
+std::list<SymCacheEntry> g_sym_cache;  // most recently used first
+size_t g_sym_bytes = 0;
+
+template <class T>
+size_t vec_bytes(const std::vector<T>& v) {
+  return v.size() * sizeof(T);
+}
+
+size_t symbolic_bytes(const Symbolic& S) {
+  return vec_bytes(S.perm) + vec_bytes(S.iperm) + vec_bytes(S.etree) + vec_bytes(S.colcount) + vec_bytes(S.sn_first) +
+         vec_bytes(S.sn_rowptr) + vec_bytes(S.sn_rows) + vec_bytes(S.sn_parent) + vec_bytes(S.sn_lptr) +
+         vec_bytes(S.sn_uptr) + vec_bytes(S.sn_level) + vec_bytes(S.col_to_sn) + vec_bytes(S.child_ptr) +
+         vec_bytes(S.child_list) + vec_bytes(S.rel_ptr) + vec_bytes(S.rel) + vec_bytes(S.level_ptr) +
+         vec_bytes(S.level_list) + vec_bytes(S.colptr) + vec_bytes(S.rowidx) + vec_bytes(S.qmap) + sizeof(Symbolic);
+}
+
+bool same_options(const SymbolicOptions& a, const SymbolicOptions& b) {
+  return a.ordering == b.ordering && a.nrelax0 == b.nrelax0 && a.nrelax1 == b.nrelax1 && a.nrelax2 == b.nrelax2 &&
+         a.zrelax0 == b.zrelax0 && a.zrelax1 == b.zrelax1 && a.zrelax2 == b.zrelax2 && a.max_width == b.max_width;
+}
+
+bool same_inputs(const SymCacheEntry& e, int64_t n, const int64_t* colptr, const int64_t* rowidx,
+                 const SymbolicOptions& opt, const int64_t* custom_perm) {
+  if (e.n != n || e.has_custom != (custom_perm != nullptr) || !same_options(e.opt, opt)) return false;
+  const int64_t nnz = colptr[n];
+  if ((int64_t)e.rowidx.size() != nnz) return false;
+  if (std::memcmp(e.colptr.data(), colptr, sizeof(int64_t) * (n + 1)) != 0) return false;
+  if (std::memcmp(e.rowidx.data(), rowidx, sizeof(int64_t) * nnz) != 0) return false;
+  if (custom_perm && std::memcmp(e.custom.data(), custom_perm, sizeof(int64_t) * n) != 0) return false;
+  return true;
+}
+
+bool sym_cache_enabled() {
+  static const bool on = std::getenv("INLA_NO_SYMBOLIC_CACHE") == nullptr;
+  return on;
+}
+
+}  // namespace
+
+void analyze(int64_t n, const int64_t* colptr, const int64_t* rowidx, const SymbolicOptions& opt,
+             const int64_t* custom_perm, Symbolic& S) {
+  // inputs the cache compares must be readable: reject what the analysis would reject
+  if (n <= 0) throw std::runtime_error("symbolic: n must be > 0");
+  if (colptr[0] != 0) throw std::runtime_error("symbolic: colptr[0] must be 0");
+  for (int64_t c = 0; c < n; ++c)
+    if (colptr[c + 1] < colptr[c]) throw std::runtime_error("symbolic: colptr not monotone");
+  if (sym_cache_enabled()) {
+    std::lock_guard<std::mutex> lock(g_sym_mu);
+    for (auto it = g_sym_cache.begin(); it != g_sym_cache.end(); ++it)
+      if (same_inputs(*it, n, colptr, rowidx, opt, custom_perm)) {
+        S = it->sym;
+        g_sym_cache.splice(g_sym_cache.begin(), g_sym_cache, it);
+        return;
+      }
+  }
+  analyze_uncached(n, colptr, rowidx, opt, custom_perm, S);
+  if (!sym_cache_enabled()) return;
+  SymCacheEntry e;
+  e.n = n;
+  e.colptr.assign(colptr, colptr + n + 1);
+  e.rowidx.assign(rowidx, rowidx + colptr[n]);
+  e.has_custom = custom_perm != nullptr;
+  if (custom_perm) e.custom.assign(custom_perm, custom_perm + n);
+  e.opt = opt;
+  e.bytes = symbolic_bytes(S) + vec_bytes(e.colptr) + vec_bytes(e.rowidx) + vec_bytes(e.custom);
+  if (e.bytes > kSymCacheBytes / 2) return;
+  e.sym = S;
+  std::lock_guard<std::mutex> lock(g_sym_mu);
+  g_sym_bytes += e.bytes;
+  g_sym_cache.push_front(std::move(e));
+  while (g_sym_bytes > kSymCacheBytes && !g_sym_cache.empty()) {
+    g_sym_bytes -= g_sym_cache.back().bytes;
+    g_sym_cache.pop_back();
+  }
+}
+
+void release_symbolic_cache() {
+  std::lock_guard<std::mutex> lock(g_sym_mu);
+  g_sym_cache.clear();
+  g_sym_bytes = 0;
 }
 
 }  // namespace inla

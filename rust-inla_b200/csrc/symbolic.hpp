@@ -93,8 +93,10 @@ void nd_order(int64_t n, const int64_t* colptr, const int64_t* rowidx, std::vect
 void amd_order(int64_t n, const int64_t* colptr, const int64_t* rowidx,
                std::vector<int64_t>& perm);
 
-// Full analysis. Throws std::runtime_error on invalid input.
+// Full analysis. Throws std::runtime_error on invalid input. Results are cached process-wide by
+// exact inputs (see symbolic.cpp); release_symbolic_cache() empties the cache.
 void analyze(int64_t n, const int64_t* colptr, const int64_t* rowidx,
              const SymbolicOptions& opt, const int64_t* custom_perm, Symbolic& out);
+void release_symbolic_cache();
 
 }  // namespace inla
