@@ -90,6 +90,11 @@ struct NdCtx {
       lev_begin = lev_end;
     }
   }
+  // dist[] of the nodes of a stored level structure (what bfs() from its root leaves there)
+  void restore_dist(const Levels& L) {
+    for (int64_t l = 0; l < L.depth(); ++l)
+      for (const int64_t* it = L.begin(l); it != L.end(l); ++it) dist[*it] = l;
+  }
   int64_t part_degree(int64_t task, int64_t u) const {
     int64_t d = 0;
     for (int64_t q = aptr[u]; q < aptr[u + 1]; ++q) d += own(adj[q]) == task;
@@ -181,31 +186,50 @@ struct NdCtx {
     const int nroots = roots[1] != roots[0] ? 2 : 1;
     std::vector<int64_t> thin;
     for (int ri = 0; ri < nroots; ++ri) {
-      bfs(task, roots[ri], levels);
+      // the structure rooted at roots[0] is `levels` itself, and the search above usually built
+      // the one rooted at roots[1] already (`best`): a BFS depends only on the part and the root,
+      // so stored structures are reused and only dist[] is rewritten
+      if (ri == 0) {
+        restore_dist(levels);
+      } else if (!best.nodes.empty() && best.nodes[0] == roots[1]) {
+        std::swap(levels, best);
+        restore_dist(levels);
+      } else {
+        bfs(task, roots[ri], levels);
+      }
       const int64_t h = levels.depth();
       if (h < 3) continue;
-      thin.assign(h, 0);
-      for (int64_t l = 0; l + 1 < h; ++l)
-        for (const int64_t* it = levels.begin(l); it != levels.end(l); ++it) {
-          const int64_t u = *it;
-          bool touches = false;
-          for (int64_t q = aptr[u]; q < aptr[u + 1] && !touches; ++q) {
-            const int64_t v = adj[q];
-            touches = own(v) == task && dist[v] == l + 1;
+      // thinned size of level l (nodes with a neighbour in level l + 1), computed only for the
+      // levels that are compared: those inside the balance window and the fallback level
+      thin.assign(h, -1);
+      auto thin_of = [&](int64_t l) {
+        if (thin[l] < 0) {
+          int64_t c = 0;
+          for (const int64_t* it = levels.begin(l); it != levels.end(l); ++it) {
+            const int64_t u = *it;
+            bool touches = false;
+            for (int64_t q = aptr[u]; q < aptr[u + 1] && !touches; ++q) {
+              const int64_t v = adj[q];
+              touches = own(v) == task && dist[v] == l + 1;
+            }
+            c += touches;
           }
-          thin[l] += touches;
+          thin[l] = c;
         }
+        return thin[l];
+      };
       int64_t pick = -1;
       for (int64_t l = 1; l + 1 < h; ++l) {
         const int64_t below = levels.start[l], above = N - levels.start[l + 1];
-        if ((double)std::min(below, above) >= kBalance * (double)N && (pick < 0 || thin[l] < thin[pick])) pick = l;
+        if ((double)std::min(below, above) >= kBalance * (double)N && (pick < 0 || thin_of(l) < thin_of(pick)))
+          pick = l;
       }
       if (pick < 0) {
         pick = 1;
         while (pick + 2 < h && levels.start[pick + 1] < N / 2) ++pick;
       }
-      if (best_size >= 0 && thin[pick] >= best_size) continue;
-      best_size = thin[pick];
+      if (best_size >= 0 && thin_of(pick) >= best_size) continue;
+      best_size = thin_of(pick);
       out.sep.clear();
       out.rest.clear();
       for (const int64_t* it = levels.begin(pick); it != levels.end(pick); ++it) {
