@@ -323,6 +323,11 @@ int inla_multi_fit(inla_multi* h, int m, const double* theta0, inla_multi_theta_
 /* Linear predictor of the last inla_multi_fit: per model the mixture mean and variance of
  * eta = A x over that model's CCD nodes (inference.rs:1451-1466), [nobs] each (NULL allowed). */
 int inla_multi_fit_predictor(inla_multi* h, double* pred_mean, double* pred_var);
+/* Model-selection criteria of model g of the last inla_multi_fit (as inla_fit_model_selection for a
+ * single model: the model's observations at its mode, its node weights, D(theta*) at the node
+ * with the smallest |z|; crit[6] from its own Hessian). cpo, pit: that model's [nobs_g]
+ * observations. INLA_ERR_NONCONVERGED for a model without a finite node. */
+int inla_multi_fit_model_selection(inla_multi* h, int g, int what, double* crit, double* cpo, double* pit);
 /* Built-in map of AR1 + iid + intercept models: theta = [log tau, logit-type rho, log tau_iid],
  * components [intercept precision, AR1 pieces K0, K1, K2, iid] with coefficients
  * [1, tau, tau rho^2, -tau rho, tau_iid] (ar1.rs:9-69, structured.rs:348-356). */

@@ -6,6 +6,7 @@
 
 #include "capi_common.hpp"
 #include "inla_b200.h"
+#include "model_select.hpp"
 #include "multi.hpp"
 
 using namespace inla;
@@ -14,6 +15,8 @@ struct inla_multi {
   cudaStream_t stream = nullptr;
   std::unique_ptr<MultiLaplace> eng;
   std::vector<double> pred_mean, pred_var;  // linear predictor moments of the last inla_multi_fit
+  MultiFitResult last;                      // its model-selection inputs (moved from the fit)
+  int m = 0;
   bool fitted = false;
 };
 
@@ -152,6 +155,8 @@ int inla_multi_fit(inla_multi* h, int m, const double* theta0, inla_multi_theta_
     }
     h->pred_mean = std::move(R.pred_mean);
     h->pred_var = std::move(R.pred_var);
+    h->last = std::move(R);
+    h->m = m;
     h->fitted = true;
     return INLA_OK;
   } catch (...) {
@@ -165,6 +170,59 @@ int inla_multi_fit_predictor(inla_multi* h, double* pred_mean, double* pred_var)
   if (pred_mean) std::memcpy(pred_mean, h->pred_mean.data(), bytes);
   if (pred_var) std::memcpy(pred_var, h->pred_var.data(), bytes);
   return INLA_OK;
+}
+
+int inla_multi_fit_model_selection(inla_multi* h, int g, int what, double* crit, double* cpo, double* pit) {
+  try {
+    if (!h || !h->fitted) return fail(INLA_ERR_INVALID, "inla_multi_fit_model_selection: no fit on this handle");
+    const MultiFitResult& R = h->last;
+    const MultiSpec& S = h->eng->spec();
+    if (g < 0 || g >= S.G) return fail(INLA_ERR_INVALID, "inla_multi_fit_model_selection: model out of range");
+    const int K = R.K;
+    const double* w = &R.node_weight[(size_t)g * K];
+    bool any = false;
+    for (int k = 0; k < K; ++k) any |= w[k] != 0.0;
+    if (!any) return fail(INLA_ERR_NONCONVERGED, "Newton-Raphson did not converge at any integration node");
+    const int64_t o0 = S.obs_off[g], len = S.obs_off[g + 1] - o0;
+    std::vector<double> ce((size_t)K * len), cv((size_t)K * len);
+    for (int k = 0; k < K; ++k)
+      for (int64_t r = 0; r < len; ++r) {
+        ce[(size_t)k * len + r] = R.cond_eta[(size_t)k * S.nobs + o0 + r];
+        cv[(size_t)k * len + r] = R.cond_eta_var[(size_t)k * S.nobs + o0 + r];
+      }
+    ObsView obs;
+    obs.family = S.family;
+    obs.nobs = len;
+    obs.y = S.y.data() + o0;
+    obs.p1 = S.p1.empty() ? nullptr : S.p1.data() + o0;
+    obs.p2 = S.p2.empty() ? nullptr : S.p2.data() + o0;
+    obs.p1scale = R.p1scale_mode[g];
+    ModelSelection ms;
+    const std::string err = model_selection(obs, K, w, R.mode_index, ce.data(), cv.data(), what, ms);
+    if (!err.empty()) return fail(INLA_ERR_INVALID, err);
+    const int m = h->m;
+    std::vector<double> neg((size_t)m * m);
+    for (int i = 0; i < m * m; ++i) neg[i] = -R.hessian[(size_t)g * m * m + i];
+    double mg = NAN;
+    if (!mlik_gaussian(R.logpost_mode[g], m, neg.data(), mg)) mg = NAN;
+    if (crit) {
+      crit[0] = ms.dic;
+      crit[1] = ms.mean_deviance;
+      crit[2] = ms.dic_p_eff;
+      crit[3] = ms.waic;
+      crit[4] = ms.lppd;
+      crit[5] = ms.waic_p_eff;
+      crit[6] = mg;
+      crit[7] = (what & MS_CPO) ? (double)ms.cpo_failures : NAN;
+    }
+    for (int64_t r = 0; r < len; ++r) {
+      if (cpo) cpo[r] = (what & MS_CPO) ? ms.cpo[r] : NAN;
+      if (pit) pit[r] = (what & MS_CPO) ? ms.pit[r] : NAN;
+    }
+    return INLA_OK;
+  } catch (...) {
+    return map_exception();
+  }
 }
 
 int inla_multi_theta_map_ar1_iid(int g, const double* theta, int m, double* coef, double* dcoef, double* p1scale,

@@ -107,6 +107,11 @@ struct MultiFitResult {
   std::vector<double> mode, hessian, mlik;   // [G][m], [G][m][m], [G]
   std::vector<double> latent_mean, latent_var;  // [n]
   std::vector<double> pred_mean, pred_var;      // [nobs]: linear predictor eta = A x per model
+  // model-selection inputs: per-node predictor and its variance [K][nobs], node weights [G][K]
+  // (0 for the nodes of a model without a finite node), the node of D(theta*) and the
+  // likelihood p1 scale at each model's mode [G]
+  std::vector<double> cond_eta, cond_eta_var, node_weight, p1scale_mode, logpost_mode;
+  int K = 0, mode_index = 0;
   std::vector<int> mode_iters, status;       // [G]; status 0 ok, 1 no finite node, 2 singular Hessian
   int n_batches = 0;
   int64_t n_model_evals = 0;

@@ -309,6 +309,23 @@ void MultiDriver::fit(const double* theta0, const MultiFitOptions& opt, MultiFit
   const MultiSpec& S = eng_.spec();
   out.pred_mean.assign(S.nobs, 0.0);
   out.pred_var.assign(S.nobs, 0.0);
+  out.K = K;
+  out.cond_eta.assign((size_t)K * S.nobs, 0.0);
+  out.cond_eta_var.assign((size_t)K * S.nobs, 0.0);
+  out.node_weight.assign((size_t)G * K, 0.0);
+  out.p1scale_mode.assign(G, NAN);
+  out.logpost_mode.assign(G, NAN);
+  {  // the node with the smallest |z| (inference.rs:1296-1304), shared by every model
+    double best = std::numeric_limits<double>::infinity();
+    for (int k = 0; k < K; ++k) {
+      double s2 = 0.0;
+      for (int j = 0; j < m; ++j) s2 += z[(size_t)k * m + j] * z[(size_t)k * m + j];
+      if (std::sqrt(s2) < best) {
+        best = std::sqrt(s2);
+        out.mode_index = k;
+      }
+    }
+  }
   out.mlik.assign(G, NAN);
   for (int g = 0; g < G; ++g) {
     std::vector<double> lp(K);
@@ -353,6 +370,8 @@ void MultiDriver::fit(const double* theta0, const MultiFitOptions& opt, MultiFit
         }
         eta[k] = e;
         ev[k] = s2;
+        out.cond_eta[(size_t)k * S.nobs + r] = e;
+        out.cond_eta_var[(size_t)k * S.nobs + r] = s2;
       }
       double mi = 0.0;
       for (int k = 0; k < K; ++k)
@@ -367,6 +386,15 @@ void MultiDriver::fit(const double* theta0, const MultiFitOptions& opt, MultiFit
       out.pred_var[r] = vi;
     }
     out.mlik[g] = mx + std::log(std::fabs(sw));
+    for (int k = 0; k < K; ++k) out.node_weight[(size_t)g * K + k] = std::isfinite(lp[k]) ? nw[k] : 0.0;
+    out.logpost_mode[g] = lp[out.mode_index];
+    {  // observations rebuilt at the model's mode (inference.rs:1478-1485)
+      const int T = eng_.ncomp();
+      std::vector<double> coef(T), dcoef((size_t)m * T), dp1s(m);
+      double p1s = 1.0;
+      if (map_(g, &out.mode[(size_t)g * m], coef.data(), dcoef.data(), &p1s, dp1s.data()) == 0)
+        out.p1scale_mode[g] = p1s;
+    }
   }
   out.n_batches = n_batches_;
   out.n_model_evals = n_model_evals_;

@@ -103,6 +103,7 @@ SIGNATURES = [
     ("inla_multi_eval", C.c_int, [P, C.c_int, DP, DP, C.c_int, DP, DP, DP, DP]),
     ("inla_multi_fit", C.c_int, [P, C.c_int, DP, P, P, P, P, DP, DP, DP, DP, DP, IP, IP, DP]),
     ("inla_multi_fit_predictor", C.c_int, [P, DP, DP]),
+    ("inla_multi_fit_model_selection", C.c_int, [P, C.c_int, C.c_int, DP, DP, DP]),
     ("inla_multi_theta_map_ar1_iid", C.c_int, [C.c_int, DP, C.c_int, DP, DP, DP, DP, P]),
     ("inla_multi_log_prior_set", C.c_double, [C.c_int, DP, C.c_int, DP, P]),
     ("inla_laplace_eval", C.c_int, [P, C.c_int, DP, DP, C.c_int, DP, DP, DP, DP]),

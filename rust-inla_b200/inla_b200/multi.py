@@ -132,6 +132,17 @@ class MultiModel:
             out["trP"], out["trQ"], out["xMx"], out["zMx"] = gt[:, :, 0], gt[:, :, 1], gt[:, :, 2], gt[:, :, 3]
         return out
 
+    def model_selection(self, g, criteria="all"):
+        """DIC, WAIC, CPO / PIT and the Gaussian-approximation mlik of model ``g`` of the last
+        :meth:`fit` (model_selection.rs, per model as the reference computes them)."""
+        from .laplace import _criteria_dict, _what
+
+        n_g = int(self.obs_off[g + 1] - self.obs_off[g])
+        crit, cpo, pit = np.zeros(8), np.zeros(n_g), np.zeros(n_g)
+        check(lib().inla_multi_fit_model_selection(self._h, int(g), _what(criteria), dptr(crit), dptr(cpo),
+                                                   dptr(pit)))
+        return _criteria_dict(crit, cpo, pit)
+
     def fit(self, theta0, theta_map="ar1_iid", priors=AR1_IID_PRIORS, hessian="fd", f0=1.0, max_iter=0, tol=0.0):
         """Fit every model (``inla_multi_fit``): batched Newton mode search on adjoint gradients
         per model, Hessian (``"fd"``: the reference's FD of values; ``"grad"``: FD of adjoint
