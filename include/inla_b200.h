@@ -408,6 +408,21 @@ int inla_fit_predictor(inla_laplace* h, double* pred_mean, double* pred_var);
 enum { INLA_MS_DIC = 1, INLA_MS_WAIC = 2, INLA_MS_CPO = 4, INLA_MS_ALL = 7 };
 int inla_fit_model_selection(inla_laplace* h, int what, double* crit, double* cpo, double* pit);
 
+/* Posterior precision at the mode (posterior_precision_at, inference.rs:1027-1058, as the
+ * reference's result carries it, 1565-1570): Q(theta*) [+ kappa C^T C with constraints] +
+ * A^T W A, W = -d2 log p(y | eta) at eta = A x of the node nearest the mode, with the
+ * observations as given to inla_laplace_create. CSC on the model's pattern united with the
+ * entries the likelihood and constraint terms add; call with NULL arrays to read nnz first
+ * (colptr has n + 1 entries). */
+int inla_fit_posterior_precision(inla_laplace* h, int64_t* nnz, int64_t* colptr, int64_t* rowidx, double* vals);
+/* Host-only form: Q = sum_t coef_t comp_t on the given pattern, A (NULL = identity), the
+ * observations, the latent point x [n] and kc x n constraint rows c (kc = 0: none). */
+int inla_posterior_precision(int64_t n, const int64_t* colptr, const int64_t* rowidx, int ncomp, const double* comp,
+                             const double* coef, int64_t nobs, const int64_t* a_rowptr, const int64_t* a_colidx,
+                             const double* a_vals, int family, const double* y, const double* p1, const double* p2,
+                             const double* x, int kc, const double* c, int64_t* nnz, int64_t* colptr_out,
+                             int64_t* rowidx_out, double* vals);
+
 /* Marginal densities of the last inla_fit on h on a uniform grid (marginals.rs): kind 0 the
  * latent entry `index`, 1 the predictor entry `index` (gaussian_mixture_marginal over the nodes,
  * 73-135), 2 the hyperparameter `index` on the internal scale (hyperpar_marginal_from_nodes,

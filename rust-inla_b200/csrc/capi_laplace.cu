@@ -9,6 +9,7 @@
 #include "driver.hpp"
 #include "marginals.hpp"
 #include "model_select.hpp"
+#include "posterior.hpp"
 #include "inla_b200.h"
 
 using namespace inla;
@@ -20,6 +21,7 @@ struct inla_laplace {
   int max_batch = 0;
   // from the last inla_fit: linear predictor moments and the model-selection inputs
   std::vector<double> pred_mean, pred_var, cond_eta, cond_eta_var, node_weight, cond_mean, cond_var, node_theta;
+  std::vector<double> coef_mode;
   int mode_index = 0, m = 0;
   double p1scale_mode = 1.0, mlik_gaussian = 0.0;
   bool fitted = false;
@@ -339,6 +341,7 @@ int inla_fit(inla_laplace* h, int m, const double* theta0, inla_theta_map_fn map
     h->cond_mean = std::move(R.cond_mean);
     h->cond_var = std::move(R.cond_var);
     h->node_theta = R.node_theta;
+    h->coef_mode = R.coef_mode;
     h->m = m;
     h->mode_index = R.mode_index;
     h->p1scale_mode = R.p1scale_mode;
@@ -397,6 +400,79 @@ int inla_fit_model_selection(inla_laplace* h, int what, double* crit, double* cp
     if (!err.empty()) return fail(INLA_ERR_INVALID, err.c_str());
     fill_crit(ms, h->mlik_gaussian, crit, cpo, pit, S.nobs, what);
     return INLA_OK;
+  } catch (...) {
+    return map_exception();
+  }
+}
+
+namespace {
+
+int copy_block(const CscBlock& b, int64_t* nnz, int64_t* colptr, int64_t* rowidx, double* vals) {
+  if (nnz) *nnz = (int64_t)b.rowidx.size();
+  if (colptr) std::memcpy(colptr, b.colptr.data(), sizeof(int64_t) * b.colptr.size());
+  if (rowidx) std::memcpy(rowidx, b.rowidx.data(), sizeof(int64_t) * b.rowidx.size());
+  if (vals) std::memcpy(vals, b.val.data(), sizeof(double) * b.val.size());
+  return INLA_OK;
+}
+
+}  // namespace
+
+int inla_fit_posterior_precision(inla_laplace* h, int64_t* nnz, int64_t* colptr, int64_t* rowidx, double* vals) {
+  try {
+    if (!h || !h->fitted) return fail(INLA_ERR_INVALID, "inla_fit_posterior_precision: no fit on this handle");
+    const LaplaceSpec& S = h->spec;
+    const int K = (int)h->node_weight.size();
+    if ((int)h->coef_mode.size() != S.ncomp || K < 1)
+      return fail(INLA_ERR_INVALID, "inla_fit_posterior_precision: the theta map failed at the mode");
+    const int64_t n = S.n;
+    if (!h->eng || (int64_t)h->cond_mean.size() < (int64_t)(h->mode_index + 1) * n)
+      return fail(INLA_ERR_INVALID, "inla_fit_posterior_precision: no node results");
+    const double* x = h->cond_mean.data() + (size_t)h->mode_index * n;
+    const LaplaceSpec& E = h->eng->spec();  // the constraints in force (the base spec has none)
+    CscBlock q;
+    const std::string err = posterior_precision(
+        n, S.colptr.data(), S.rowidx.data(), S.ncomp, S.comp.data(), h->coef_mode.data(), S.nobs,
+        S.identity_a ? nullptr : S.acp.data(), S.aci.data(), S.av.data(), S.family, S.y.data(),
+        S.p1.empty() ? nullptr : S.p1.data(), S.p2.empty() ? nullptr : S.p2.data(), x, E.kc,
+        E.kc > 0 ? E.cA.data() : nullptr, q);
+    if (!err.empty()) return fail(INLA_ERR_INVALID, err);
+    return copy_block(q, nnz, colptr, rowidx, vals);
+  } catch (...) {
+    return map_exception();
+  }
+}
+
+int inla_posterior_precision(int64_t n, const int64_t* colptr, const int64_t* rowidx, int ncomp, const double* comp,
+                             const double* coef, int64_t nobs, const int64_t* a_rowptr, const int64_t* a_colidx,
+                             const double* a_vals, int family, const double* y, const double* p1, const double* p2,
+                             const double* x, int kc, const double* c, int64_t* nnz, int64_t* colptr_out,
+                             int64_t* rowidx_out, double* vals) {
+  try {
+    if (n <= 0 || !colptr || !rowidx || ncomp < 1 || !comp || !coef || !x || nobs < 0 || (nobs > 0 && !y) ||
+        family < 0 || family > 3 || kc < 0 || (kc > 0 && !c))
+      return fail(INLA_ERR_INVALID, "inla_posterior_precision: invalid argument");
+    if (colptr[0] != 0) return fail(INLA_ERR_INVALID, "inla_posterior_precision: colptr[0] must be 0");
+    for (int64_t j = 0; j < n; ++j) {
+      if (colptr[j + 1] < colptr[j]) return fail(INLA_ERR_INVALID, "inla_posterior_precision: colptr not monotone");
+      for (int64_t p = colptr[j]; p < colptr[j + 1]; ++p)
+        if (rowidx[p] < 0 || rowidx[p] >= n) return fail(INLA_ERR_INVALID, "inla_posterior_precision: row index");
+    }
+    if (!a_rowptr) {
+      if (nobs != n) return fail(INLA_ERR_DIM_MISMATCH, "inla_posterior_precision: A = I needs nobs == n");
+    } else {
+      if (!a_colidx || !a_vals || a_rowptr[0] != 0) return fail(INLA_ERR_INVALID, "inla_posterior_precision: A");
+      for (int64_t r = 0; r < nobs; ++r) {
+        if (a_rowptr[r + 1] < a_rowptr[r]) return fail(INLA_ERR_INVALID, "inla_posterior_precision: A row pointer");
+        for (int64_t p = a_rowptr[r]; p < a_rowptr[r + 1]; ++p)
+          if (a_colidx[p] < 0 || a_colidx[p] >= n)
+            return fail(INLA_ERR_DIM_MISMATCH, "inla_posterior_precision: A column out of range");
+      }
+    }
+    CscBlock q;
+    const std::string err = posterior_precision(n, colptr, rowidx, ncomp, comp, coef, nobs, a_rowptr, a_colidx,
+                                                a_vals, family, y, p1, p2, x, kc, c, q);
+    if (!err.empty()) return fail(INLA_ERR_INVALID, err);
+    return copy_block(q, nnz, colptr_out, rowidx_out, vals);
   } catch (...) {
     return map_exception();
   }

@@ -722,9 +722,9 @@ void InlaDriver::fit(const double* theta0, const FitOptions& opt, FitResult& out
     const int T = eng_.ncomp();
     std::vector<double> coef(T), dcoef((size_t)m * T), dp1s(m);
     double p1s = 1.0;
-    out.p1scale_mode = map_(mode.data(), coef.data(), dcoef.data(), &p1s, dp1s.data()) == 0
-                           ? p1s
-                           : std::numeric_limits<double>::quiet_NaN();
+    const bool mapped = map_(mode.data(), coef.data(), dcoef.data(), &p1s, dp1s.data()) == 0;
+    out.p1scale_mode = mapped ? p1s : std::numeric_limits<double>::quiet_NaN();
+    if (mapped) out.coef_mode = coef;
   }
   out.mlik = mx + std::log(std::fabs(sw));
   out.cond_mean = std::move(means);

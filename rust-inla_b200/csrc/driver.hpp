@@ -44,6 +44,7 @@ struct FitResult {
   std::vector<double> cond_mean, cond_var;     // [K][n] per-node mode and marginal variances
   int mode_index = 0;                          // node with the smallest |z| (inference.rs:1296-1304)
   double p1scale_mode = 1.0;                   // likelihood p1 scale at the mode (observations at the mode)
+  std::vector<double> coef_mode;               // component coefficients of Q at the mode
   double mlik_gaussian = 0.0;                  // Gaussian approximation of the log marginal likelihood
   double mlik = 0.0;
   int n_evals = 0, n_batches = 0, mode_iters = 0;

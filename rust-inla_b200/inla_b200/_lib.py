@@ -128,6 +128,9 @@ SIGNATURES = [
                                        DP]),
     ("inla_mlik_gaussian", C.c_int, [C.c_double, C.c_int, DP, DP]),
     ("inla_fit_marginal", C.c_int, [P, C.c_int, I64, C.c_int, C.c_double, DP, DP]),
+    ("inla_fit_posterior_precision", C.c_int, [P, LP, LP, LP, DP]),
+    ("inla_posterior_precision", C.c_int, [I64, LP, LP, C.c_int, DP, DP, I64, LP, LP, DP, C.c_int, DP, DP, DP, DP,
+                                           C.c_int, DP, LP, LP, LP, DP]),
     ("inla_mixture_marginal", C.c_int, [C.c_int, DP, DP, DP, C.c_int, C.c_double, DP, DP]),
     ("inla_hyperpar_marginal", C.c_int, [C.c_int, DP, DP, C.c_int, C.c_double, DP, DP]),
     ("inla_marginal_quantiles", C.c_int, [C.c_int, DP, DP, C.c_int, DP, DP]),

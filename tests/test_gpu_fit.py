@@ -114,6 +114,24 @@ def test_fit_marginals_match_oracle(problem):
         np.testing.assert_allclose(y, yo, rtol=1e-9, atol=1e-12 * np.max(yo))
 
 
+def test_fit_posterior_precision(problem):
+    """Posterior precision at the mode (inference.rs:1027-1058, 1565-1570): Q(theta*) + A^T W A at
+    the latent mode of the node nearest the mode, with the observations as given to the model,
+    against the host assembly on the oracle's mode at that node."""
+    from inla_b200.laplace import posterior_precision
+
+    p, lm = problem
+    r = lm.fit(THETA0, mode_search="nm", batched=True)
+    qp = lm.posterior_precision()
+    k0 = int(np.argmin(np.linalg.norm(r["node_theta"] - r["mode"], axis=1)))
+    th = r["node_theta"][k0]
+    x = O.laplace(p.model.matrix(O.spde_coefs(th[1], th[2])), p.a, "gaussian", p.y, p1=np.exp(th[0]))["x"]
+    c, _ = models.spde_coefs(r["mode"][1], r["mode"][2])
+    ref = posterior_precision(p.model, c, x, a=p.a, family="gaussian", y=p.y)
+    d = (qp - ref).toarray()
+    assert np.max(np.abs(d)) <= 1e-8 * np.max(np.abs(ref.toarray()))
+
+
 @pytest.mark.parametrize("search", ["bfgs", "newton"])
 def test_batched_adjoint_fit_matches_plain(problem, search):
     p, lm = problem
