@@ -342,6 +342,35 @@ def posterior_precision(model, coef, x, a=None, family="gaussian", y=None, p1=No
     return sp.csc_matrix((ov, ori, ocp), shape=(n, n))
 
 
+def lincomb_summaries(mean, q_post, combs, solver=None):
+    """lincomb_summaries (posterior.rs:55-92): for each ``(name, [(index, weight), ...])`` the mean
+    a^T mean and sd = sqrt(max(a^T Q^-1 a, 0)) with Q = ``q_post`` factorized once (on the GPU
+    solver unless ``solver``, an object with ``factorize(q)`` and ``solve(b)``, is given), and the
+    Gaussian 2.5 / 50 / 97.5 % points mean -+ 1.96 sd."""
+    from .solver import GpuSolver
+
+    mean = np.asarray(mean, dtype=float)
+    n = len(mean)
+    q = sp.csc_matrix(q_post)
+    if q.shape != (n, n):
+        raise ValueError(f"lincomb: Q is {q.shape[0]}x{q.shape[1]}, latent mean has length {n}")
+    s = GpuSolver() if solver is None else solver
+    s.factorize(q)
+    out = []
+    for name, weights in combs:
+        a = np.zeros(n)
+        for i, w in weights:
+            if not 0 <= i < n:
+                raise ValueError(f"lincomb '{name}': index {i} out of range [0, {n})")
+            if not np.isfinite(w):
+                raise ValueError(f"lincomb '{name}': non-finite weight")
+            a[i] += w
+        m = float(a @ mean)
+        sd = float(np.sqrt(max(float(a @ s.solve(a)), 0.0)))
+        out.append({"name": name, "mean": m, "sd": sd, "q025": m - 1.96 * sd, "q50": m, "q975": m + 1.96 * sd})
+    return out
+
+
 def mixture_marginal(means, vars_, weights, n_points=201, n_sd=4.0):
     """gaussian_mixture_marginal (marginals.rs:83-135): ``(x, y)`` on a uniform grid."""
     m, v, w = as_f64(np.ravel(means)), as_f64(np.ravel(vars_)), as_f64(np.ravel(weights))

@@ -132,6 +132,23 @@ def test_fit_posterior_precision(problem):
     assert np.max(np.abs(d)) <= 1e-8 * np.max(np.abs(ref.toarray()))
 
 
+def test_lincomb_summaries_on_the_gpu_solver(problem):
+    """lincomb_summaries (posterior.rs:55-92) with the posterior precision factorized on the GPU
+    solver: sd against a dense inverse."""
+    from inla_b200.laplace import lincomb_summaries
+
+    p, lm = problem
+    r = lm.fit(THETA0, mode_search="nm", batched=True)
+    q = lm.posterior_precision()
+    res = lincomb_summaries(r["mean"], q, [("x0", [(0, 1.0)]), ("pair", [(5, 1.0), (17, -0.5)])])
+    cov = np.linalg.inv(q.toarray())
+    a = np.zeros(q.shape[0])
+    a[5], a[17] = 1.0, -0.5
+    assert abs(res[0]["sd"] - np.sqrt(cov[0, 0])) <= 1e-9 * np.sqrt(cov[0, 0])
+    assert abs(res[1]["sd"] - np.sqrt(a @ cov @ a)) <= 1e-9 * np.sqrt(a @ cov @ a)
+    assert res[1]["mean"] == pytest.approx(a @ r["mean"], rel=1e-14, abs=1e-14)
+
+
 @pytest.mark.parametrize("search", ["bfgs", "newton"])
 def test_batched_adjoint_fit_matches_plain(problem, search):
     p, lm = problem

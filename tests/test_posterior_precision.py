@@ -62,3 +62,32 @@ def test_invalid_observation_is_an_error():
     model = models.build_latent(n, [sp.identity(n, format="csc")], "iid")
     with pytest.raises(InlaError, match="likelihood"):
         posterior_precision(model, [1.0], np.zeros(n), a=None, family="poisson", y=[-1.0, 0.0, 1.0])
+
+
+class _DenseSolver:
+    """A dense stand-in for the GPU solver, to test the lincomb bookkeeping on the CPU."""
+
+    def factorize(self, q):
+        self.q = q.toarray()
+
+    def solve(self, b):
+        return np.linalg.solve(self.q, b)
+
+
+def test_lincomb_summaries_bookkeeping():
+    """posterior.rs:55-92: mean, sd and the Gaussian quantiles; duplicate indices add up."""
+    from inla_b200.laplace import lincomb_summaries
+
+    rng = np.random.default_rng(6)
+    b = rng.normal(size=(5, 5))
+    q = sp.csc_matrix(b @ b.T + 5 * np.eye(5))
+    mean = rng.normal(size=5)
+    combs = [("first", [(0, 1.0)]), ("diff", [(1, 1.0), (3, -1.0), (1, 0.5)])]
+    res = lincomb_summaries(mean, q, combs, solver=_DenseSolver())
+    cov = np.linalg.inv(q.toarray())
+    a = np.array([0.0, 1.5, 0.0, -1.0, 0.0])
+    assert res[0]["mean"] == mean[0] and abs(res[0]["sd"] - np.sqrt(cov[0, 0])) < 1e-12
+    assert abs(res[1]["mean"] - a @ mean) < 1e-14 and abs(res[1]["sd"] - np.sqrt(a @ cov @ a)) < 1e-12
+    assert abs(res[1]["q975"] - res[1]["mean"] - 1.96 * res[1]["sd"]) < 1e-14
+    with pytest.raises(ValueError, match="out of range"):
+        lincomb_summaries(mean, q, [("bad", [(9, 1.0)])], solver=_DenseSolver())
