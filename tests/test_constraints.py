@@ -191,3 +191,23 @@ def test_multi_problem_layout():
         e[i] = 1e-6
         fd = (models.ar1_iid_coefs(th + e)[0] - models.ar1_iid_coefs(th - e)[0]) / 2e-6
         np.testing.assert_allclose(dc[i], fd, rtol=1e-7, atol=1e-9)
+
+
+def test_group_block_is_group_major_kronecker():
+    """structured.rs grouped_iid_ar1_uses_group_major_kronecker_order: the grouped block of Q is
+    kron(Q_group, Q_main) with Q_group the AR1 precision (ar1.rs:9-69: tau at the ends,
+    tau (1 + rho^2) inside, -tau rho off the diagonal) and rho = 2 / (1 + e^-theta) - 1."""
+    p = models.make_group_problem(nr=3, nc=4, T=3, seed=2)
+    theta = [0.2, -0.1, 0.6, 0.3]
+    c, _ = models.group_coefs(theta)
+    q = p.model.matrix(c).toarray()
+    ns, T = p.dims
+    rho = 2.0 / (1.0 + np.exp(-theta[2])) - 1.0
+    q_group = models.ar1_precision(T, rho, np.exp(theta[1])).toarray()
+    assert q_group[0, 0] == np.exp(theta[1]) and q_group[0, 1] == -np.exp(theta[1]) * rho
+    r = models.besag_structure(models.lattice_adjacency(3, 4)).toarray()
+    expected = np.kron(q_group, np.exp(theta[0]) * r)
+    block = q[1:1 + ns * T, 1:1 + ns * T]
+    np.testing.assert_allclose(block, expected, rtol=1e-14, atol=1e-14)
+    assert q[0, 0] == models.BESAG_FIXED_PREC
+    np.testing.assert_allclose(np.diag(q)[1 + ns * T:], np.exp(theta[3]), rtol=1e-15)
