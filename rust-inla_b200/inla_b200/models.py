@@ -254,9 +254,11 @@ def lattice_adjacency(nr: int, nc: int) -> sp.csr_matrix:
 
 
 def besag_structure(adj: sp.spmatrix) -> sp.csc_matrix:
-    """Graph Laplacian ``R = D - W`` (intrinsic Besag structure)."""
+    """Graph Laplacian ``R = D - W`` (intrinsic Besag structure), with a unit diagonal for
+    regions without neighbours (besag.rs:127-152: singletons are N(0, 1 / tau))."""
     adj = sp.csr_matrix(adj)
     deg = np.asarray(adj.sum(axis=1)).ravel()
+    deg = np.where(deg == 0, 1.0, deg)
     return (sp.diags(deg) - adj).tocsc()
 
 

@@ -211,3 +211,16 @@ def test_group_block_is_group_major_kronecker():
     np.testing.assert_allclose(block, expected, rtol=1e-14, atol=1e-14)
     assert q[0, 0] == models.BESAG_FIXED_PREC
     np.testing.assert_allclose(np.diag(q)[1 + ns * T:], np.exp(theta[3]), rtol=1e-15)
+
+
+def test_besag_precision_reference_cases():
+    """besag.rs:177-196 (4-cycle, tau = 1.5: diagonal 3.0, neighbour -1.5, others 0) and
+    besag.rs:199-206 (a singleton region gets the diagonal tau)."""
+    cyc = sp.csr_matrix(np.array([[0, 1, 0, 1], [1, 0, 1, 0], [0, 1, 0, 1], [1, 0, 1, 0]], dtype=float))
+    q = 1.5 * models.besag_structure(cyc).toarray()
+    assert abs(q[0, 0] - 3.0) < 1e-12 and abs(q[0, 1] + 1.5) < 1e-12 and abs(q[0, 2]) < 1e-12
+    adj = np.zeros((6, 6))
+    for i, j in [(0, 1), (1, 2), (3, 4)]:
+        adj[i, j] = adj[j, i] = 1.0
+    q = 2.0 * models.besag_structure(sp.csr_matrix(adj)).toarray()
+    assert q[5, 5] == 2.0 and q[0, 0] == 2.0 and q[1, 1] == 4.0
