@@ -210,3 +210,28 @@ def test_mesh1d_spde_precision_positive_diagonal():
     f = Mesh1D(knots).fem()
     h = np.diff(knots)
     np.testing.assert_array_equal(f["c0"].diagonal(), np.r_[h / 2, 0.0] + np.r_[0.0, h / 2])
+
+
+def test_barrier_spde_reduces_covariance_across_strip():
+    """structured.rs barrier_spde_reduces_covariance_across_strip: on a 7 x 2 vertex lattice,
+    triangles whose centroid has 0.35 <= x < 0.65 become barrier triangles (range fraction 0.1,
+    stiffness scale 0.01); the covariance between the two ends of the strip drops below half."""
+    nxv, nyv = 7, 2
+    v = np.array([[i / (nxv - 1), j / (nxv - 1)] for j in range(nyv) for i in range(nxv)])
+    t = []
+    for j in range(nyv - 1):
+        for i in range(nxv - 1):
+            a, b, c, d = j * nxv + i, j * nxv + i + 1, (j + 1) * nxv + i, (j + 1) * nxv + i + 1
+            t += [[a, b, d], [a, d, c]]
+    t = np.array(t)
+    cx = v[t].mean(axis=1)[:, 0]
+    barrier = (cx >= 0.35) & (cx < 0.65)
+    assert barrier.any()
+    m = Mesh(v, t)
+    covs = []
+    for scale in (None, np.where(barrier, 0.1 ** 2, 1.0)):
+        f = m.fem(triangle_scale=scale)
+        pattern, comp = spde_components(f["c0"].diagonal(), f["g1"])
+        q = _q_from_components(pattern, comp, 1.0, 1.0).toarray()
+        covs.append(abs(np.linalg.inv(q)[0, nxv - 1]))
+    assert covs[1] < 0.5 * covs[0], covs
