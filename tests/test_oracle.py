@@ -194,3 +194,33 @@ def test_grid_design_points_reference():
     assert len(z1) == 5
     z2, _ = O.grid_design(2, 1.0, 2.0, f)
     assert len(z2) > 0 and all(p[0] ** 2 + p[1] ** 2 <= 4.0001 for p in z2)
+
+
+def test_likelihood_known_answers_reference():
+    """inference.rs evaluates_{gaussian,poisson,binomial,negative_binomial}_likelihood on the
+    oracle, and the library's host likelihood through its Hessian (the posterior precision of
+    Q = 0 at eta) and its log-density (a one-node deviance)."""
+    import scipy.sparse as sp
+
+    from inla_b200 import models
+    from inla_b200.laplace import model_selection, posterior_precision
+
+    lp, g, h = O.eval_lik("gaussian", 1.5, 1.0, 2.0)
+    assert abs(g + 1.0) < 1e-12 and abs(h + 2.0) < 1e-12
+    for fam, eta, y, p1 in [("poisson", 0.2, 3.0, 2.0), ("binomial", 0.3, 4.0, 10.0)]:
+        assert all(np.isfinite(O.eval_lik(fam, eta, y, p1)))
+    mu, r, y = 2.0, 3.0, 4.0
+    lp, g, h = O.eval_lik("nbinomial", math.log(2.0), y, r, 1.0)
+    d1 = y / mu - (y + r) / (mu + r)
+    d2 = -y / (mu * mu) + (y + r) / ((mu + r) * (mu + r))
+    assert abs(g - d1 * mu) < 1e-12 and abs(h - (d2 * mu * mu + d1 * mu)) < 1e-12
+    # the library's host likelihoods (shared with the device kernels) at the same points
+    cases = [("gaussian", 1.5, 1.0, 2.0, 1.0), ("poisson", 0.2, 3.0, 2.0, 1.0), ("binomial", 0.3, 4.0, 10.0, 1.0),
+             ("nbinomial", math.log(2.0), 4.0, 3.0, 1.0)]
+    zero = models.build_latent(1, [sp.identity(1, format="csc")], "iid")
+    for fam, eta, yy, p1, p2 in cases:
+        lp, g, h = O.eval_lik(fam, eta, yy, p1, p2)
+        q = posterior_precision(zero, [0.0], [eta], a=None, family=fam, y=[yy], p1=[p1], p2=[p2]).toarray()
+        assert abs(q[0, 0] + h) <= 1e-13 * max(1.0, abs(h)), fam
+        dev = model_selection(fam, [yy], [1.0], 0, [[eta]], [[0.1]], p1=[p1], p2=[p2], criteria=["dic"])
+        assert abs(dev["mean_deviance"] + 2.0 * lp) <= 1e-12 * max(1.0, abs(lp)), fam
