@@ -166,3 +166,10 @@ def test_single_node_fails_every_cpo_and_errors_propagate():
         model_selection("poisson", [-1.0, 2.0], W2, 0, MODES2, np.full((2, 2), 0.1))
     with pytest.raises(InlaError):
         model_selection("gaussian", Y2, W2, 2, MODES2, np.full((2, 2), 0.1), p1=2.0)   # mode index out of range
+
+
+def test_compute_flags_skip_criteria():
+    """inference.rs compute_flags_skip_dic_waic_cpo: criteria not asked for stay NaN / None."""
+    r = model_selection("gaussian", Y2, W2, 0, MODES2, np.full((2, 2), 0.1), p1=2.0, criteria=[])
+    assert np.isnan(r["dic"]) and np.isnan(r["waic"]) and r["cpo_failures"] is None
+    assert np.all(np.isnan(r["cpo"])) and np.all(np.isnan(r["pit"]))
