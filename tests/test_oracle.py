@@ -224,3 +224,29 @@ def test_likelihood_known_answers_reference():
         assert abs(q[0, 0] + h) <= 1e-13 * max(1.0, abs(h)), fam
         dev = model_selection(fam, [yy], [1.0], 0, [[eta]], [[0.1]], p1=[p1], p2=[p2], criteria=["dic"])
         assert abs(dev["mean_deviance"] + 2.0 * lp) <= 1e-12 * max(1.0, abs(lp)), fam
+
+
+BINOMIAL_YS = [3., 5., 4., 2., 5., 6., 3., 4., 5., 3., 4., 6., 2., 5., 4., 3., 5., 4., 6., 3., 4., 5.,
+               3., 4., 5., 2., 6., 4., 3., 5., 4., 3., 5., 4., 6., 3., 4., 5., 3., 4., 5., 2., 6., 4.,
+               3., 5., 4., 3., 5., 4., 6., 3., 4., 5.]
+
+
+def test_binomial_identity_mode_converges():
+    """inference.rs binomial_identity_mode_converges: Q = I (n = 20), y alternating 4 / 6 of 10."""
+    n = 20
+    y = [4.0 if i % 2 == 0 else 6.0 for i in range(n)]
+    r = O.laplace(sp.identity(n, format="csc"), None, "binomial", y, p1=10.0, max_iter=100, tol=1e-6)
+    assert np.isfinite(r["mlik"]) and np.all(np.isfinite(r["x"]))
+    assert abs(np.mean(r["x"])) < 1.0
+
+
+def test_binomial_mode_across_prior_strengths():
+    """inference.rs binomial_mode_across_prior_strengths: the mode search converges for
+    tau in {1e-4, 1e-2, 1, 1e2, 1e4} and with an explicit A = I."""
+    n = len(BINOMIAL_YS)
+    for tau in (1e-4, 1e-2, 1.0, 1e2, 1e4):
+        r = O.laplace(tau * sp.identity(n, format="csc"), None, "binomial", BINOMIAL_YS, p1=10.0, max_iter=100)
+        assert np.isfinite(r["mlik"])
+    r = O.laplace(sp.identity(n, format="csc"), sp.identity(n, format="csr"), "binomial", BINOMIAL_YS, p1=10.0,
+                  max_iter=100)
+    assert np.isfinite(r["mlik"])
