@@ -371,6 +371,35 @@ def sum_to_zero_constraint(n: int, k: int = 1):
     return c, np.zeros(k)
 
 
+def component_constraints(adj: sp.spmatrix):
+    """component_constraints (structured.rs:782-806): one sum-to-zero row per connected
+    component of more than one node, weight 1 / sqrt(size) on its nodes, components in order of
+    their first node; singletons stay unconstrained. Returns ``(C [k x n], e [k])`` or None."""
+    adj = sp.csr_matrix(adj)
+    n = adj.shape[0]
+    seen = np.zeros(n, dtype=bool)
+    rows = []
+    for s0 in range(n):
+        if seen[s0]:
+            continue
+        comp, stack = [], [s0]
+        seen[s0] = True
+        while stack:
+            u = stack.pop()
+            comp.append(u)
+            for v in adj.indices[adj.indptr[u]:adj.indptr[u + 1]]:
+                if not seen[v]:
+                    seen[v] = True
+                    stack.append(v)
+        if len(comp) > 1:
+            r = np.zeros(n)
+            r[comp] = 1.0 / np.sqrt(len(comp))
+            rows.append(r)
+    if not rows:
+        return None
+    return np.array(rows), np.zeros(len(rows))
+
+
 def plane_constraint_2d(nrow: int, ncol: int):
     """``plane_constraint_2d`` (constraints.rs:219-266) for a column-major lattice
     (``node = j * nrow + i``): constant, row trend, column trend, each unit norm."""

@@ -224,3 +224,17 @@ def test_besag_precision_reference_cases():
         adj[i, j] = adj[j, i] = 1.0
     q = 2.0 * models.besag_structure(sp.csr_matrix(adj)).toarray()
     assert q[5, 5] == 2.0 and q[0, 0] == 2.0 and q[1, 1] == 4.0
+
+
+def test_besag_constraints_follow_connected_components():
+    """structured.rs besag_constraints_follow_connected_components: components {0,1,2}, {3,4},
+    {5}; two rows, the singleton unconstrained."""
+    adj = np.zeros((6, 6))
+    for i, j in [(0, 1), (1, 2), (3, 4)]:
+        adj[i, j] = adj[j, i] = 1.0
+    c, e = models.component_constraints(sp.csr_matrix(adj))
+    assert c.shape == (2, 6) and np.all(e == 0.0)
+    assert c[0, 5] == 0.0 and c[1, 5] == 0.0
+    assert np.all(c[0, :3] > 0) and np.all(c[1, 3:5] > 0)
+    np.testing.assert_allclose(c[0, :3], 1 / np.sqrt(3)) and np.testing.assert_allclose(c[1, 3:5], 1 / np.sqrt(2))
+    assert models.component_constraints(sp.csr_matrix((3, 3))) is None
