@@ -45,17 +45,20 @@ constexpr int64_t kParallelMin = 4096;  // smallest part handed to a thread
 // task id in `owner`; concurrent parts are disjoint, so dist/dstamp entries of a
 // part are only touched by its thread, while owner stamps of neighbouring parts
 // are read (atomically) to test membership.
+// Node ids, levels, task ids and BFS stamps are 32-bit (half the memory traffic of the sweeps);
+// nd_order rejects graphs with 2^31 or more nodes.
 struct NdCtx {
-  std::vector<int64_t> aptr, adj;
-  std::vector<std::atomic<int64_t>> owner;
-  std::vector<int64_t> dist, dstamp;
-  std::atomic<int64_t> next_task{0}, bfs_id{0};
+  std::vector<int64_t> aptr;
+  std::vector<int32_t> adj;
+  std::vector<std::atomic<int32_t>> owner;
+  std::vector<int32_t> dist, dstamp;
+  std::atomic<int32_t> next_task{0}, bfs_id{0};
 
   explicit NdCtx(int64_t n) : owner(n), dist(n, -1), dstamp(n, -1) {
     for (auto& o : owner) o.store(-1, std::memory_order_relaxed);
   }
-  int64_t own(int64_t v) const { return owner[v].load(std::memory_order_relaxed); }
-  void stamp(int64_t v, int64_t t) { owner[v].store(t, std::memory_order_relaxed); }
+  int32_t own(int64_t v) const { return owner[v].load(std::memory_order_relaxed); }
+  void stamp(int64_t v, int64_t t) { owner[v].store((int32_t)t, std::memory_order_relaxed); }
 
   // rooted level structure: nodes in BFS order, level l = nodes[start[l] .. start[l+1])
   struct Levels {
@@ -321,8 +324,9 @@ void nd_order(int64_t n, const int64_t* colptr, const int64_t* rowidx, std::vect
       ++deg[r];
       ++deg[c];
     }
+  if (n >= (int64_t)INT32_MAX) throw std::runtime_error("nested dissection: graph too large");
   std::vector<int64_t>& aptr = cx.aptr;
-  std::vector<int64_t>& adj = cx.adj;
+  std::vector<int32_t>& adj = cx.adj;
   aptr.assign(n + 1, 0);
   for (int64_t i = 0; i < n; ++i) aptr[i + 1] = aptr[i] + deg[i];
   adj.assign(aptr[n], 0);
@@ -331,19 +335,19 @@ void nd_order(int64_t n, const int64_t* colptr, const int64_t* rowidx, std::vect
     for (int64_t p = colptr[c]; p < colptr[c + 1]; ++p) {
       const int64_t r = rowidx[p];
       if (r == c) continue;
-      adj[fill[r]++] = c;
-      adj[fill[c]++] = r;
+      adj[fill[r]++] = (int32_t)c;
+      adj[fill[c]++] = (int32_t)r;
     }
   {
     std::vector<int64_t> nptr(n + 1, 0);
     int64_t w = 0;
     for (int64_t i = 0; i < n; ++i) {
-      int64_t* b = adj.data() + aptr[i];
-      int64_t* e = adj.data() + aptr[i + 1];
+      int32_t* b = adj.data() + aptr[i];
+      int32_t* e = adj.data() + aptr[i + 1];
       std::sort(b, e);
       e = std::unique(b, e);
       nptr[i] = w;
-      for (int64_t* q = b; q < e; ++q) adj[w++] = *q;
+      for (int32_t* q = b; q < e; ++q) adj[w++] = *q;
     }
     nptr[n] = w;
     adj.resize(w);
