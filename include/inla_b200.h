@@ -310,11 +310,18 @@ int inla_multi_eval(inla_multi* h, int B, const double* coef, const double* p1sc
 typedef int (*inla_multi_theta_map_fn)(int g, const double* theta, int m, double* coef, double* dcoef,
                                        double* p1scale, double* dp1scale, void* user);
 typedef double (*inla_multi_log_prior_fn)(int g, const double* theta, int m, double* grad, void* user);
+/* Cancellation poll (the check_cancel callback of run_inla_inference_a_cancellable,
+ * inference.rs:1116-1130): called before every batched evaluation; a nonzero return stops the
+ * fit, which returns INLA_ERR_CANCELLED ("Operation cancelled by user") and leaves its outputs
+ * unwritten. */
+typedef int (*inla_cancel_fn)(void* cancel_user);
 typedef struct {
   int hessian;    /* 0 FD of values (reference), 1 FD of adjoint gradients */
   double f0;      /* CCD f0 (0 = 1.0) */
   int max_iter;   /* Newton iterations per model (0 = 100) */
   double tol;     /* gradient infinity-norm tolerance (0 = 1e-4) */
+  inla_cancel_fn cancel; /* NULL: never cancelled */
+  void* cancel_user;
 } inla_multi_fit_options;
 int inla_multi_fit(inla_multi* h, int m, const double* theta0, inla_multi_theta_map_fn map,
                    inla_multi_log_prior_fn prior, void* user, const inla_multi_fit_options* opt, double* mode,
@@ -380,10 +387,18 @@ typedef struct {
   int max_iter;    /* 0 = 200 (NM) / 100 (BFGS) */
   double tol;      /* 0 = 1e-6 (NM f-spread) / 1e-4 (BFGS gradient inf-norm) */
   double nm_step;  /* 0 = 0.1 */
+  inla_cancel_fn cancel; /* polled before every evaluation (NULL: never cancelled) */
+  void* cancel_user;
 } inla_fit_options;
 
 /* node_theta: up to [64][m]; node_weight: up to [64]; info: [6] = {mlik, seconds,
- * theta-evaluations, batches, mode-search iterations, integration nodes}. */
+ * theta-evaluations, batches, mode-search iterations, integration nodes}.
+ * m = 0 (no hyperparameters, inference.rs:1135-1239): one Laplace evaluation at the empty
+ * theta with marginal variances, no mode search, Hessian or integration design; mlik is the
+ * Laplace marginal likelihood (no prior term), info[5] = 0 integration nodes (node_theta and
+ * node_weight are not written), the predictor, model selection and marginals of the fit use
+ * that single node with weight 1, and a failed Laplace evaluation is an error. theta0, mode
+ * and hessian may be NULL then. */
 int inla_fit(inla_laplace* h, int m, const double* theta0, inla_theta_map_fn map, inla_log_prior_fn prior,
              void* user, const inla_fit_options* opt, double* mode, double* hessian, double* latent_mean,
              double* latent_var, double* node_theta, double* node_weight, double* info);
@@ -482,8 +497,10 @@ int inla_predictor_moments(int64_t nobs, int64_t n, const int64_t* a_rowptr, con
  * stream) without synchronizing. Limit: n <= 1024 (larger n returns
  * INLA_ERR_DIM_MISMATCH). The factor lives in a fixed 8 MiB static device
  * scratch per GPU, shared by every call and kept until process exit: calls
- * whose GPU work overlaps race on it. The first call on a device resolves
- * the scratch addresses; make it before any stream capture.
+ * whose GPU work overlaps race on it (calls queued on one stream run in
+ * order and do not). The first call on a device resolves the scratch
+ * addresses; make it before any stream capture (a first call on a capturing
+ * stream returns INLA_ERR_INVALID).
  * ---------------------------------------------------------------------- */
 int inla_dense_ldlt_solve_noalloc(int n, const double* d_q, const double* d_rhs, double* d_x, double* d_logdet,
                                   int* d_status, void* stream);

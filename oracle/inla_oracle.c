@@ -164,6 +164,152 @@ int orc_choose_order(int64_t n, const int64_t* cp, const int64_t* ri, int64_t* f
   return 1;
 }
 
+/* Minimum-degree fill-reducing order for the reference's AMD branch
+ * (ordering.rs:149-162 returns CholeskyOrder::Amd; faer 0.24 then computes
+ * an approximate-minimum-degree permutation, sparse_ldlt.rs:151-186). faer
+ * is not vendored here, so this is a plain exact-external-degree minimum
+ * degree on the quotient graph (George & Liu 1989): eliminated nodes become
+ * elements, elements reached from a pivot are absorbed into it, and every
+ * variable adjacent to the pivot gets its exact external degree recomputed.
+ * Ties take the most recently inserted node of the smallest degree bucket.
+ * The permutation differs from faer's; fill is of the same order. Writes
+ * perm[new] = old. */
+typedef struct {
+  int64_t *a, n, cap;
+} ivec_t;
+static void iv_push(ivec_t* v, int64_t x) {
+  if (v->n == v->cap) {
+    v->cap = v->cap ? 2 * v->cap : 4;
+    v->a = (int64_t*)realloc(v->a, sizeof(int64_t) * v->cap);
+  }
+  v->a[v->n++] = x;
+}
+
+void orc_min_degree(int64_t n, const int64_t* cp, const int64_t* ri, int64_t* perm) {
+  ivec_t* vadj = (ivec_t*)calloc(n, sizeof(ivec_t)); /* variable neighbours */
+  ivec_t* eadj = (ivec_t*)calloc(n, sizeof(ivec_t)); /* adjacent elements */
+  ivec_t* evar = (ivec_t*)calloc(n, sizeof(ivec_t)); /* variables of element e */
+  char* state = (char*)calloc(n, 1);                  /* 0 variable, 1 element, 2 absorbed */
+  int64_t* deg = (int64_t*)malloc(sizeof(int64_t) * n);
+  int64_t* head = (int64_t*)malloc(sizeof(int64_t) * (n + 1));
+  int64_t* next = (int64_t*)malloc(sizeof(int64_t) * n);
+  int64_t* prev = (int64_t*)malloc(sizeof(int64_t) * n);
+  int64_t* inlp = (int64_t*)calloc(n, sizeof(int64_t));
+  int64_t* seen = (int64_t*)calloc(n, sizeof(int64_t));
+  int64_t stamp_lp = 0, stamp = 0;
+  for (int64_t c = 0; c < n; ++c)
+    for (int64_t p = cp[c]; p < cp[c + 1]; ++p)
+      if (ri[p] != c) iv_push(&vadj[c], ri[p]);
+  /* duplicates in a column would count twice: the degree is recomputed exactly below */
+  for (int64_t d = 0; d <= n; ++d) head[d] = -1;
+  for (int64_t i = 0; i < n; ++i) {
+    ++stamp;
+    int64_t cnt = 0;
+    seen[i] = stamp;
+    for (int64_t t = 0; t < vadj[i].n; ++t)
+      if (seen[vadj[i].a[t]] != stamp) seen[vadj[i].a[t]] = stamp, ++cnt;
+    deg[i] = cnt;
+    prev[i] = -1;
+    next[i] = head[cnt];
+    if (head[cnt] >= 0) prev[head[cnt]] = i;
+    head[cnt] = i;
+  }
+  int64_t mind = 0;
+  for (int64_t k = 0; k < n; ++k) {
+    while (head[mind] < 0) ++mind;
+    const int64_t p = head[mind];
+    head[mind] = next[p];
+    if (next[p] >= 0) prev[next[p]] = -1;
+    perm[k] = p;
+    state[p] = 1;
+    /* the new element: variables adjacent to p directly or through its elements */
+    ++stamp_lp;
+    inlp[p] = stamp_lp;
+    ivec_t lp = {0, 0, 0};
+    for (int64_t t = 0; t < vadj[p].n; ++t) {
+      const int64_t v = vadj[p].a[t];
+      if (state[v] == 0 && inlp[v] != stamp_lp) inlp[v] = stamp_lp, iv_push(&lp, v);
+    }
+    for (int64_t t = 0; t < eadj[p].n; ++t) {
+      const int64_t e = eadj[p].a[t];
+      if (state[e] != 1) continue;
+      for (int64_t u = 0; u < evar[e].n; ++u) {
+        const int64_t v = evar[e].a[u];
+        if (state[v] == 0 && inlp[v] != stamp_lp) inlp[v] = stamp_lp, iv_push(&lp, v);
+      }
+      state[e] = 2; /* absorbed into p */
+      free(evar[e].a);
+      evar[e].a = NULL;
+      evar[e].n = evar[e].cap = 0;
+    }
+    free(vadj[p].a);
+    free(eadj[p].a);
+    vadj[p].a = eadj[p].a = NULL;
+    vadj[p].n = eadj[p].n = 0;
+    evar[p] = lp;
+    for (int64_t t = 0; t < lp.n; ++t) {
+      const int64_t i = lp.a[t];
+      /* elements: drop absorbed ones, add p */
+      int64_t w = 0;
+      for (int64_t u = 0; u < eadj[i].n; ++u)
+        if (state[eadj[i].a[u]] == 1) eadj[i].a[w++] = eadj[i].a[u];
+      eadj[i].n = w;
+      iv_push(&eadj[i], p);
+      /* variables: drop eliminated ones and those now reached through element p */
+      w = 0;
+      for (int64_t u = 0; u < vadj[i].n; ++u) {
+        const int64_t v = vadj[i].a[u];
+        if (state[v] == 0 && inlp[v] != stamp_lp) vadj[i].a[w++] = v;
+      }
+      vadj[i].n = w;
+      /* exact external degree */
+      ++stamp;
+      seen[i] = stamp;
+      int64_t cnt = 0;
+      for (int64_t u = 0; u < vadj[i].n; ++u) {
+        const int64_t v = vadj[i].a[u];
+        if (seen[v] != stamp) seen[v] = stamp, ++cnt;
+      }
+      for (int64_t u = 0; u < eadj[i].n; ++u) {
+        ivec_t* ev = &evar[eadj[i].a[u]];
+        int64_t w2 = 0;
+        for (int64_t z = 0; z < ev->n; ++z) {
+          const int64_t v = ev->a[z];
+          if (state[v] != 0) continue; /* eliminated since: drop from the element */
+          ev->a[w2++] = v;
+          if (seen[v] != stamp) seen[v] = stamp, ++cnt;
+        }
+        ev->n = w2;
+      }
+      /* move i to its new bucket */
+      if (prev[i] >= 0) next[prev[i]] = next[i];
+      else head[deg[i]] = next[i];
+      if (next[i] >= 0) prev[next[i]] = prev[i];
+      deg[i] = cnt;
+      prev[i] = -1;
+      next[i] = head[cnt];
+      if (head[cnt] >= 0) prev[head[cnt]] = i;
+      head[cnt] = i;
+      if (cnt < mind) mind = cnt;
+    }
+  }
+  for (int64_t i = 0; i < n; ++i) {
+    free(vadj[i].a);
+    free(eadj[i].a);
+    free(evar[i].a);
+  }
+  free(vadj);
+  free(eadj);
+  free(evar);
+  free(state);
+  free(deg);
+  free(head);
+  free(next);
+  free(prev);
+  free(inlp);
+  free(seen);
+}
+
 /* ------------------------------------------------------------------------ */
 /* LDL^T (up-looking, simplicial)                                           */
 /* ------------------------------------------------------------------------ */

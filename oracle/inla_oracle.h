@@ -27,6 +27,8 @@ int orc_try_time_major(int64_t n, const int64_t* cp, const int64_t* ri, int64_t*
 void orc_rcm(int64_t n, const int64_t* cp, const int64_t* ri, int64_t* fwd);
 /* 5 = time-major, 2 = RCM (fwd written), 1 = AMD */
 int orc_choose_order(int64_t n, const int64_t* cp, const int64_t* ri, int64_t* fwd);
+/* Minimum-degree order for the AMD branch (perm[new] = old); not faer's AMD. */
+void orc_min_degree(int64_t n, const int64_t* cp, const int64_t* ri, int64_t* perm);
 
 /* ---- sparse LDL^T (simplicial, up-looking) ---- */
 typedef struct orc_factor orc_factor;

@@ -48,6 +48,7 @@ def lib():
             "orc_try_time_major": (C.c_int, [C.c_int64, LP, LP, LP]),
             "orc_rcm": (None, [C.c_int64, LP, LP, LP]),
             "orc_choose_order": (C.c_int, [C.c_int64, LP, LP, LP]),
+            "orc_min_degree": (None, [C.c_int64, LP, LP, LP]),
             "orc_factor_create": (C.c_int, [C.c_int64, LP, LP, DP, LP, C.POINTER(C.c_void_p)]),
             "orc_factor_free": (None, [C.c_void_p]),
             "orc_factor_nnz": (C.c_int64, [C.c_void_p]),
@@ -109,6 +110,25 @@ def rcm(q):
     fwd = np.zeros(n, dtype=np.int64)
     lib().orc_rcm(n, _p(cp, LP), _p(ri, LP), _p(fwd, LP))
     return fwd
+
+
+def min_degree_perm(q):
+    """perm[new] = old: a minimum-degree order standing in for faer's AMD (not bit-identical)."""
+    n, cp, ri, _ = _csc(q)
+    perm = np.zeros(n, dtype=np.int64)
+    lib().orc_min_degree(n, _p(cp, LP), _p(ri, LP), _p(perm, LP))
+    return perm
+
+
+def reference_perm(q):
+    """perm[new] = old following the reference's choice (ordering.rs:149-162): time-major or RCM
+    where it picks them, a minimum-degree order where it picks AMD."""
+    k, fwd = choose_order(q)
+    if fwd is None:
+        return min_degree_perm(q)
+    perm = np.empty(q.shape[0], dtype=np.int64)
+    perm[fwd] = np.arange(q.shape[0])
+    return perm
 
 
 def default_perm(q):

@@ -296,7 +296,7 @@ int inla_fit(inla_laplace* h, int m, const double* theta0, inla_theta_map_fn map
              void* user, const inla_fit_options* opt, double* mode, double* hessian, double* latent_mean,
              double* latent_var, double* node_theta, double* node_weight, double* info) {
   try {
-    if (!h || !h->eng || !theta0 || !map || !prior || !opt || m < 1 || m > 5)
+    if (!h || !h->eng || (!theta0 && m > 0) || !map || !prior || !opt || m < 0 || m > 5)
       return fail(INLA_ERR_INVALID, "invalid argument");
     LaplaceEngine& E = *h->eng;
     ThetaMap tm = [&](const double* th, double* c, double* dc, double* s, double* ds) {
@@ -313,14 +313,19 @@ int inla_fit(inla_laplace* h, int m, const double* theta0, inla_theta_map_fn map
     fo.max_iter = opt->max_iter > 0 ? opt->max_iter : (opt->mode_search ? 100 : 200);
     fo.tol = opt->tol > 0 ? opt->tol : (opt->mode_search ? 1e-4 : 1e-6);
     fo.nm_step = opt->nm_step > 0 ? opt->nm_step : 0.1;
+    if (opt->cancel) {
+      inla_cancel_fn cf = opt->cancel;
+      void* cu = opt->cancel_user;
+      fo.cancel = [cf, cu] { return cf(cu) != 0; };
+    }
     FitResult R;
     int64_t before = E.launches();
     drv.fit(theta0, fo, R);
     g_launches += E.launches() - before;
     const int64_t n = E.n();
-    const int K = (int)R.node_weight.size();
-    if (mode) std::memcpy(mode, R.mode.data(), sizeof(double) * m);
-    if (hessian) std::memcpy(hessian, R.hessian.data(), sizeof(double) * m * m);
+    const int K = (int)R.node_theta.size() / std::max(m, 1);  // m = 0: no integration nodes
+    if (mode && m > 0) std::memcpy(mode, R.mode.data(), sizeof(double) * m);
+    if (hessian && m > 0) std::memcpy(hessian, R.hessian.data(), sizeof(double) * m * m);
     if (latent_mean) std::memcpy(latent_mean, R.latent_mean.data(), sizeof(double) * n);
     if (latent_var) std::memcpy(latent_var, R.latent_var.data(), sizeof(double) * n);
     if (node_theta) std::memcpy(node_theta, R.node_theta.data(), sizeof(double) * std::min(K, 64) * m);

@@ -134,6 +134,11 @@ int inla_multi_fit(inla_multi* h, int m, const double* theta0, inla_multi_theta_
       if (opt->f0 > 0) fo.f0 = opt->f0;
       if (opt->max_iter > 0) fo.max_iter = opt->max_iter;
       if (opt->tol > 0) fo.tol = opt->tol;
+      if (opt->cancel) {
+        inla_cancel_fn cf = opt->cancel;
+        void* cu = opt->cancel_user;
+        fo.cancel = [cf, cu] { return cf(cu) != 0; };
+      }
     }
     MultiFitResult R;
     const int64_t before = E.launches();

@@ -9,7 +9,9 @@
 #include <stdexcept>
 
 #include "aggregate.hpp"
+#include "capi_common.hpp"
 #include "driver.hpp"
+#include "inla_b200.h"
 #include "model_select.hpp"
 
 namespace inla {
@@ -127,12 +129,17 @@ void symmetric_eigen(const std::vector<double>& a0, int m, std::vector<double>& 
 // evaluation of f = -(mlik + log prior) (inla_stats/src/hyper_opt.rs:21-47)
 // ---------------------------------------------------------------------------
 
+void InlaDriver::check_cancel() const {
+  if (cancel_ && cancel_()) throw InlaError(INLA_ERR_CANCELLED, "Operation cancelled by user");
+}
+
 void InlaDriver::evaluate(int K, const double* thetas, bool want_grad, bool batched, double* f, double* grad,
                           std::vector<LaplaceOut>* keep) {
   const int T = eng_.ncomp(), m = m_;
   const int Bmax = batched ? eng_.max_batch() : 1;
   std::vector<double> coef, dcoef, p1s, dp1s, gp(m);
   for (int k0 = 0; k0 < K; k0 += Bmax) {
+    check_cancel();  // before every evaluation, as evaluate_neg_log_posterior (hyper_opt.rs:21-24)
     const int Bc = std::min(Bmax, K - k0);
     coef.assign((size_t)Bc * T, 0.0);
     dcoef.assign((size_t)Bc * m * T, 0.0);
@@ -565,6 +572,57 @@ void InlaDriver::grad_hessian(const std::vector<double>& mode, double h, bool ba
 }
 
 // ---------------------------------------------------------------------------
+// fit without hyperparameters (inference.rs:1135-1239): one Laplace node
+// ---------------------------------------------------------------------------
+
+void InlaDriver::fit_single_node(FitResult& out) {
+  const int64_t n = eng_.n();
+  const int T = eng_.ncomp();
+  check_cancel();
+  std::vector<double> coef(T, 0.0), p1s(1, 1.0), dp1s(1, 0.0), dcoef(1, 0.0);
+  if (map_(nullptr, coef.data(), dcoef.data(), &p1s[0], dp1s.data()) != 0)
+    throw std::runtime_error("theta map failed at the empty theta");
+  LaplaceOut R;
+  eng_.eval(1, coef.data(), p1s.data(), LAP_VARIANCES, R);
+  n_evals_ += 1;
+  n_batches_ += 1;
+  // find_latent_mode_a_with_solver(...)? : a failed mode search is the fit's error
+  if (R.status[0] != LAP_OK || !std::isfinite(R.mlik[0]))
+    throw InlaError((R.status[0] == LAP_SINGULAR_PRIOR || R.status[0] == LAP_SINGULAR_POST) ? INLA_ERR_SINGULAR : INLA_ERR_NONCONVERGED,
+                    "Laplace mode search failed at the single node");
+  std::vector<double> means(n), vars(n);
+  const size_t w = sizeof(double) * n;
+  INLA_CUDA(cudaMemcpyAsync(means.data(), eng_.d_x(), w, cudaMemcpyDeviceToHost, eng_.stream()));
+  INLA_CUDA(cudaMemcpyAsync(vars.data(), eng_.d_var(), w, cudaMemcpyDeviceToHost, eng_.stream()));
+  INLA_CUDA(cudaStreamSynchronize(eng_.stream()));
+  out.mode.clear();
+  out.hessian.clear();
+  out.mode_iters = 0;
+  out.latent_mean = means;
+  out.latent_var = vars;
+  const LaplaceSpec& S = eng_.spec();
+  const int64_t nobs = S.identity_a ? n : S.nobs;
+  out.cond_eta.resize(nobs);
+  out.cond_eta_var.resize(nobs);
+  project_nodes(nobs, n, S.identity_a ? nullptr : S.acp.data(), S.aci.data(), S.av.data(), 1, means.data(),
+                vars.data(), out.cond_eta.data(), out.cond_eta_var.data());
+  out.pred_mean = out.cond_eta;
+  out.pred_var = out.cond_eta_var;
+  out.mode_index = 0;
+  out.p1scale_mode = p1s[0];
+  out.coef_mode = coef;
+  out.mlik = R.mlik[0];
+  out.mlik_gaussian = R.mlik[0];  // marginal_log_lik_gaussian = marginal_log_lik (inference.rs:1224)
+  out.cond_mean = std::move(means);
+  out.cond_var = std::move(vars);
+  out.node_theta.clear();
+  out.node_weight = {1.0};  // single-node weight for the predictor / model selection / marginals
+  out.node_logpost = {R.mlik[0]};
+  out.n_evals = n_evals_;
+  out.n_batches = n_batches_;
+}
+
+// ---------------------------------------------------------------------------
 // fit (inference.rs:1116-1466)
 // ---------------------------------------------------------------------------
 
@@ -573,6 +631,12 @@ void InlaDriver::fit(const double* theta0, const FitOptions& opt, FitResult& out
   const int m = m_;
   const int64_t n = eng_.n();
   n_evals_ = n_batches_ = 0;
+  cancel_ = opt.cancel;
+  if (m == 0) {
+    fit_single_node(out);
+    out.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return;
+  }
   std::vector<double> mode(theta0, theta0 + m);
   int iters = 0;
   if (opt.mode_search == 0) nelder_mead(mode, opt, iters);

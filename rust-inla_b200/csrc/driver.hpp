@@ -35,6 +35,9 @@ struct FitOptions {
   int max_iter = 200;   // NM iterations (hyper_opt.rs:34) / BFGS iterations
   double tol = 1e-6;    // NM f-spread tolerance / BFGS gradient infinity-norm tolerance
   double nm_step = 0.1;
+  // Polled before every evaluation; returning true stops the fit with INLA_ERR_CANCELLED
+  // (check_cancel of inference.rs:1116-1130, hyper_opt.rs:21-47).
+  std::function<bool()> cancel;
 };
 
 struct FitResult {
@@ -71,12 +74,15 @@ class InlaDriver {
                      std::vector<double>& g, std::vector<double>& H);
   void fd_hessian(const std::vector<double>& mode, double h, bool batched, std::vector<double>& H);
   void grad_hessian(const std::vector<double>& mode, double h, bool batched, std::vector<double>& H);
+  void fit_single_node(FitResult& out);  // m = 0
+  void check_cancel() const;
 
   LaplaceEngine& eng_;
   int m_;
   ThetaMap map_;
   LogPrior prior_;
   int n_evals_ = 0, n_batches_ = 0;
+  std::function<bool()> cancel_;
 };
 
 // integration.rs restatements

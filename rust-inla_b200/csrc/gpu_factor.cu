@@ -19,9 +19,22 @@ inline int cdiv(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 // Parent columns per extend-add CTA: the m-row slice must fit in shared memory.
 inline int gather_cols(int m) { return std::max(1, std::min(kGatherCols, (200 * 1024) / (8 * std::max(m, 1)))); }
 
+// The dynamic shared-memory limit is an attribute of the kernel on the current
+// device, shared by every engine in the process. Engines of different sizes
+// need different limits, so the attribute only ever rises: a smaller engine
+// built later must not lower it below what a larger one still launches with.
+std::mutex g_smem_mu;
+std::map<std::pair<const void*, int>, int> g_smem_set;  // (kernel, device) -> limit set
+
 template <class K>
 void set_smem(K kernel, int bytes) {
+  int dev = 0;
+  INLA_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_smem_mu);
+  int& cur = g_smem_set[{(const void*)kernel, dev}];
+  if (bytes <= cur) return;
   INLA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  cur = bytes;
 }
 }  // namespace
 
@@ -433,7 +446,7 @@ const std::vector<char>* GpuFactor::schedule(int B, const std::function<void()>&
 
 template <class Body>
 void GpuFactor::launch_cached(const std::vector<int64_t>& key, Body&& body) {
-  if (!use_graphs_) {
+  if (!use_graphs_ || uncaptured_.count(key)) {
     body();
     INLA_CUDA(cudaGetLastError());
     return;
@@ -442,23 +455,43 @@ void GpuFactor::launch_cached(const std::vector<int64_t>& key, Body&& body) {
   if (it == graphs_.end()) {
     const int64_t before = launches_;
     INLA_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    bool host_error = false;
     try {
       body();
     } catch (...) {
-      cudaGraph_t g = nullptr;
-      cudaStreamEndCapture(stream_, &g);
-      if (g) cudaGraphDestroy(g);
-      launches_ = before;
-      throw;
+      host_error = true;
     }
+    // A launch rejected during capture (configuration, resources, a call that
+    // capture does not allow) returns its error here and invalidates the capture.
+    const cudaError_t launch_err = cudaGetLastError();
     cudaGraph_t g = nullptr;
-    INLA_CUDA(cudaStreamEndCapture(stream_, &g));
+    const cudaError_t end_err = cudaStreamEndCapture(stream_, &g);
+    const int64_t captured = launches_ - before;
+    launches_ = before;
+    if (host_error || launch_err != cudaSuccess || end_err != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();  // the capture's errors are not sticky: clear them
+      // Keep the handle usable: this key runs without a graph from now on. A
+      // host-side exception of the body surfaces again, with its message, from
+      // the direct run.
+      const cudaError_t why = launch_err != cudaSuccess ? launch_err : end_err;
+      std::fprintf(stderr, "inla_b200: CUDA graph capture of launch sequence %lld failed (%s); running it uncaptured\n",
+                   (long long)key[0], host_error ? "host exception" : cudaGetErrorString(why));
+      uncaptured_.insert(key);
+      ++capture_failures_;
+      body();
+      const cudaError_t run_err = cudaGetLastError();
+      if (run_err != cudaSuccess)
+        throw CudaError(std::string("launch sequence failed (capture: ") + cudaGetErrorString(why) +
+                            "; direct run: " + cudaGetErrorString(run_err) + ")",
+                        (int)run_err);
+      return;
+    }
     cudaGraphExec_t ex = nullptr;
     cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) throw CudaError(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e), (int)e);
-    it = graphs_.emplace(key, GraphEntry{ex, launches_ - before}).first;
-    launches_ = before;
+    it = graphs_.emplace(key, GraphEntry{ex, captured}).first;
   }
   INLA_CUDA(cudaGraphLaunch(it->second.exec, stream_));
   launches_ += it->second.nkernels;

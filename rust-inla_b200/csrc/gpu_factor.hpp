@@ -7,6 +7,7 @@
 #include <functional>
 #include <map>
 #include <memory>
+#include <set>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -125,6 +126,8 @@ class GpuFactor {
   // Replay the fixed launch sequences (fill+factor, solve, selected inverse)
   // from CUDA graphs captured on first use (default on).
   void set_use_graphs(bool on) { use_graphs_ = on; }
+  // Launch sequences whose capture failed and that now run without a graph.
+  int64_t capture_failures() const { return capture_failures_; }
 
  private:
   void plan_levels();
@@ -143,6 +146,8 @@ class GpuFactor {
     int64_t nkernels;
   };
   std::map<std::vector<int64_t>, GraphEntry> graphs_;
+  std::set<std::vector<int64_t>> uncaptured_;  // sequences whose capture failed: run directly
+  int64_t capture_failures_ = 0;
   bool use_graphs_ = true;
   std::map<int, std::vector<char>> fuse_;  // tuned panel schedule per batch size
   uint64_t struct_hash_ = 0;               // key of the process-wide tuning cache

@@ -101,6 +101,7 @@ struct MultiFitOptions {
   double f0 = 1.0;       // CCD f0
   int max_iter = 100;    // Newton iterations per model
   double tol = 1e-4;     // gradient infinity-norm tolerance
+  std::function<bool()> cancel;  // polled before every evaluation; true stops with INLA_ERR_CANCELLED
 };
 
 struct MultiFitResult {
@@ -135,6 +136,7 @@ class MultiDriver {
   MultiLogPrior prior_;
   int n_batches_ = 0;
   int64_t n_model_evals_ = 0;
+  std::function<bool()> cancel_;
 };
 
 }  // namespace inla

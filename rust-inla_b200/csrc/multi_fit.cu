@@ -6,7 +6,9 @@
 #include <cstdlib>
 #include <limits>
 
+#include "capi_common.hpp"
 #include "driver.hpp"
+#include "inla_b200.h"
 #include "multi.hpp"
 
 namespace inla {
@@ -20,6 +22,7 @@ void MultiDriver::evaluate(int B, const double* th, bool want_grad, bool want_va
   if (xs) xs->assign((size_t)B * n, 0.0);
   if (vs) vs->assign((size_t)B * n, 0.0);
   for (int b0 = 0; b0 < B; b0 += Bmax) {
+    if (cancel_ && cancel_()) throw InlaError(INLA_ERR_CANCELLED, "Operation cancelled by user");
     const int Bc = std::min(Bmax, B - b0);
     const size_t BG = (size_t)Bc * G;
     coef.assign(BG * T, 0.0);
@@ -85,6 +88,7 @@ void MultiDriver::fit(const double* theta0, const MultiFitOptions& opt, MultiFit
   const std::vector<int64_t>& lo = eng_.lat_off();
   const double h = 1e-3;  // gradient stencil of the mode search
   n_batches_ = 0;
+  cancel_ = opt.cancel;
   n_model_evals_ = 0;
 
   // ---- mode search: InlaDriver::newton per model, all models in lockstep ----------

@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <mutex>
 #include <string>
@@ -53,7 +54,7 @@ struct NoAllocScratch {
   double* vec = nullptr;
   int* gi = nullptr;
   int64_t* gl = nullptr;
-  bool ready = false;
+  std::atomic<bool> ready{false};  // set once, under g_scratch_mu, after the addresses
 };
 NoAllocScratch g_scratch[kMaxDevices];
 std::mutex g_scratch_mu;
@@ -129,10 +130,24 @@ extern "C" int inla_dense_ldlt_solve_noalloc(int n, const double* d_q, const dou
                                            "; use inla_solver_* or inla_batch_* for larger systems");
   if (!d_q || !d_logdet || !d_status) return fail(INLA_ERR_INVALID, "null input or output pointer");
   if ((d_rhs == nullptr) != (d_x == nullptr)) return fail(INLA_ERR_INVALID, "rhs and x must both be given or both NULL");
+  cudaStream_t st = (cudaStream_t)stream;
   NoAllocScratch* s = nullptr;
+  {
+    int dev = -1;
+    if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < kMaxDevices && !g_scratch[dev].ready) {
+      // the one-time set-up may not run inside a stream capture
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      const cudaError_t e = cudaStreamIsCapturing(st, &cs);
+      if (e != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        return fail(INLA_ERR_INVALID,
+                    "the first call on a device resolves the static scratch and cannot run while the stream is "
+                    "being captured; make one call on this device before the capture begins");
+      }
+    }
+  }
   int rc = scratch_for_current_device(&s);
   if (rc != INLA_OK) return rc;
-  cudaStream_t st = (cudaStream_t)stream;
   const int N = kNoAllocMaxN;
   DevSym ds;
   ds.n = n;

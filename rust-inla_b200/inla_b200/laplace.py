@@ -24,6 +24,7 @@ CRITERIA = {"dic": 1, "waic": 2, "cpo": 4}
 THETA_MAP = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
                         C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p)
 LOG_PRIOR = C.CFUNCTYPE(C.c_double, C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double), C.c_void_p)
+CANCEL = C.CFUNCTYPE(C.c_int, C.c_void_p)
 
 PRIOR_PC_PREC = 1
 PRIOR_LOGGAMMA = 2
@@ -42,7 +43,8 @@ class PriorSet(C.Structure):
 
 class FitOptions(C.Structure):
     _fields_ = [("mode_search", C.c_int), ("batched", C.c_int), ("strategy", C.c_int), ("f0", C.c_double),
-                ("hessian", C.c_int), ("max_iter", C.c_int), ("tol", C.c_double), ("nm_step", C.c_double)]
+                ("hessian", C.c_int), ("max_iter", C.c_int), ("tol", C.c_double), ("nm_step", C.c_double),
+                ("cancel", CANCEL), ("cancel_user", C.c_void_p)]
 
 
 def prior_set(specs) -> PriorSet:
@@ -183,10 +185,14 @@ class LaplaceModel:
         return x, y
 
     def fit(self, theta0, theta_map="spde", priors=SPDE_DEFAULT_PRIORS, mode_search="nm", batched=False,
-            strategy="ccd", f0=1.0, hessian="fd", max_iter=0, tol=0.0):
+            strategy="ccd", f0=1.0, hessian="fd", max_iter=0, tol=0.0, cancel=None):
         """Full INLA fit; ``theta_map`` is ``"spde"`` or a Python callable
         ``theta -> (coef, dcoef[m][T], p1scale, dp1scale[m])``; ``priors`` a list of
-        ``(kind, slot, params)`` or a callable ``theta -> (logp, grad)``."""
+        ``(kind, slot, params)`` or a callable ``theta -> (logp, grad)``. ``cancel`` is an
+        optional callable polled before every evaluation (the reference's ``check_cancel``);
+        a true result stops the fit with ``InlaError`` code ``INLA_ERR_CANCELLED``. An empty
+        ``theta0`` fits the model without hyperparameters: one Laplace node of weight 1
+        (inference.rs:1135-1239)."""
         th0 = as_f64(theta0)
         m = len(th0)
         keep = []
@@ -197,7 +203,7 @@ class LaplaceModel:
 
             def _map(th, mm, coef, dcoef, s, ds, user):
                 try:
-                    t = np.ctypeslib.as_array(th, shape=(mm,)).copy()
+                    t = np.ctypeslib.as_array(th, shape=(mm,)).copy() if mm > 0 else np.zeros(0)
                     c, dc, p1s, dp1s = theta_map(t)
                     for i in range(T):
                         coef[i] = float(c[i])
@@ -216,7 +222,7 @@ class LaplaceModel:
         user = None
         if callable(priors):
             def _prior(th, mm, g, u):
-                t = np.ctypeslib.as_array(th, shape=(mm,)).copy()
+                t = np.ctypeslib.as_array(th, shape=(mm,)).copy() if mm > 0 else np.zeros(0)
                 v, gr = priors(t)
                 if g:
                     for i in range(mm):
@@ -233,6 +239,10 @@ class LaplaceModel:
         opt = FitOptions(mode_search={"nm": 0, "bfgs": 1, "newton": 2}[mode_search], batched=int(bool(batched)),
                          strategy={"ccd": 0, "grid": 1}[strategy], f0=float(f0),
                          hessian={"fd": 0, "grad": 1}[hessian], max_iter=int(max_iter), tol=float(tol), nm_step=0.0)
+        if cancel is not None:
+            fcancel = CANCEL(lambda u: 1 if cancel() else 0)
+            keep.append(fcancel)
+            opt.cancel = fcancel
         mode = np.zeros(m)
         hess = np.zeros((m, m))
         mean = np.zeros(self.n)

@@ -29,8 +29,12 @@ MULTI_LOG_PRIOR = C.CFUNCTYPE(C.c_double, C.c_int, C.POINTER(C.c_double), C.c_in
 AR1_IID_PRIORS = [(PRIOR_PC_PREC, 0, (1.0, 0.01)), (PRIOR_PC_COR1, 1, (0.5, 0.75)), (PRIOR_PC_PREC, 2, (1.0, 0.01))]
 
 
+CANCEL = C.CFUNCTYPE(C.c_int, C.c_void_p)
+
+
 class FitOptions(C.Structure):
-    _fields_ = [("hessian", C.c_int), ("f0", C.c_double), ("max_iter", C.c_int), ("tol", C.c_double)]
+    _fields_ = [("hessian", C.c_int), ("f0", C.c_double), ("max_iter", C.c_int), ("tol", C.c_double),
+                ("cancel", CANCEL), ("cancel_user", C.c_void_p)]
 
 
 class MultiModel:
@@ -143,7 +147,8 @@ class MultiModel:
                                                    dptr(pit)))
         return _criteria_dict(crit, cpo, pit)
 
-    def fit(self, theta0, theta_map="ar1_iid", priors=AR1_IID_PRIORS, hessian="fd", f0=1.0, max_iter=0, tol=0.0):
+    def fit(self, theta0, theta_map="ar1_iid", priors=AR1_IID_PRIORS, hessian="fd", f0=1.0, max_iter=0, tol=0.0,
+            cancel=None):
         """Fit every model (``inla_multi_fit``): batched Newton mode search on adjoint gradients
         per model, Hessian (``"fd"``: the reference's FD of values; ``"grad"``: FD of adjoint
         gradients), CCD nodes and per-model mixture moments, all models in lockstep.
@@ -180,6 +185,10 @@ class MultiModel:
         keep.append(ps)
         fprior = C.cast(lib().inla_multi_log_prior_set, MULTI_LOG_PRIOR)
         opt = FitOptions(hessian={"fd": 0, "grad": 1}[hessian], f0=float(f0), max_iter=int(max_iter), tol=float(tol))
+        if cancel is not None:  # polled before every evaluation; true stops with INLA_ERR_CANCELLED
+            fcancel = CANCEL(lambda u: 1 if cancel() else 0)
+            keep.append(fcancel)
+            opt.cancel = fcancel
         G = self.G
         mode = np.zeros((G, m))
         hess = np.zeros((G, m, m))

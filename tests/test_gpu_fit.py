@@ -168,3 +168,50 @@ def test_fit_with_gradient_hessian(problem):
     a = lm.fit(THETA0, mode_search="bfgs", batched=True, tol=1e-5, hessian="fd")
     b = lm.fit(THETA0, mode_search="bfgs", batched=True, tol=1e-5, hessian="grad")
     np.testing.assert_allclose(a["hessian"], b["hessian"], rtol=0.1, atol=0.5)
+
+
+def test_fit_cancellation_stops_and_leaves_the_handle_usable(problem):
+    """check_cancel (inference.rs:1116-1130, hyper_opt.rs:21-24): polled before every
+    evaluation; a cancel stops the fit with the Cancelled status."""
+    from inla_b200 import _lib
+
+    p, lm = problem
+    polls = []
+
+    def cancel():
+        polls.append(1)
+        return len(polls) > 3
+
+    with pytest.raises(_lib.InlaError) as e:
+        lm.fit(THETA0, mode_search="nm", batched=False, cancel=cancel)
+    assert e.value.code == _lib.INLA_ERR_CANCELLED
+    assert len(polls) == 4  # three evaluations ran, the fourth poll cancelled
+    with pytest.raises(_lib.InlaError) as e:
+        lm.fit(THETA0, mode_search="newton", batched=True, cancel=lambda: True)
+    assert e.value.code == _lib.INLA_ERR_CANCELLED
+    r = lm.fit(THETA0, mode_search="newton", batched=True, tol=1e-5, cancel=lambda: False)
+    plain = lm.fit(THETA0, mode_search="nm", batched=False)
+    np.testing.assert_allclose(r["mode"], plain["mode"], atol=5e-2)
+
+
+def test_fit_without_hyperparameters_is_one_laplace_node(problem):
+    """m = 0 (inference.rs:1135-1239): one Laplace evaluation with variances, weight 1, the
+    Laplace mlik without a prior term, no integration nodes."""
+    p, lm = problem
+    th = np.array([4.0, -3.0, 2.5])
+    c = O.spde_coefs(th[1], th[2])
+    r = lm.fit(np.zeros(0), theta_map=lambda t: (c, np.zeros((0, 3)), np.exp(th[0]), np.zeros(0)),
+               priors=lambda t: (0.0, np.zeros(0)), batched=True)
+    ref = O.laplace(p.model.matrix(c), p.a, "gaussian", p.y, p1=np.exp(th[0]), want_var=True)
+    assert abs(r["mlik"] - ref["mlik"]) <= 1e-10 * abs(ref["logdet_post"])
+    assert np.max(np.abs(r["mean"] - ref["x"])) <= 1e-8 * np.max(np.abs(ref["x"]))
+    assert np.max(np.abs(r["var"] - ref["var"]) / ref["var"]) <= 1e-8
+    assert r["node_theta"].shape[0] == 0 and r["n_evals"] == 1 and r["mode"].shape == (0,)
+    np.testing.assert_allclose(r["pred_mean"], O.matvec_csc(p.a, ref["x"]), rtol=1e-8, atol=1e-10)
+    np.testing.assert_allclose(r["pred_var"], O.predictor_variances_diag(p.a, ref["var"]), rtol=1e-8)
+    ms = lm.model_selection()
+    assert ms["mlik_gaussian"] == pytest.approx(r["mlik"], rel=1e-15)
+    n = len(p.y)
+    q1 = np.full(n, np.exp(th[0]))
+    dic = O.compute_dic("gaussian", p.y, q1, np.ones(n), [O.matvec_csc(p.a, ref["x"])], [1.0], 0)
+    assert abs(ms["dic"] - dic["dic"]) <= 1e-8 * max(1.0, abs(dic["dic"]))

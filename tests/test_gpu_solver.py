@@ -204,3 +204,34 @@ def test_deterministic_bitwise():
     r = np.cos(np.arange(q.shape[0]))
     np.testing.assert_array_equal(a.solve(r), b.solve(r))
     np.testing.assert_array_equal(a.diag_inv(), b.diag_inv())
+
+
+def test_small_handle_built_later_does_not_break_a_large_one():
+    """Two engines in one process: a large-front engine, then a small one, then a first
+    factorization and solve of the large engine at a batch size it has not launched yet
+    (a new captured launch sequence). The sweep kernels' shared-memory limit must still
+    admit the large engine's fronts."""
+    import math
+
+    p = models.make_spde_problem(nx=60, n_obs=1800)
+    c, _ = models.spde_coefs(math.log(0.05), math.log(10.0))
+    q = (p.model.matrix(c) + 40.0 * (p.a.T @ p.a)).tocsc()
+    q.sort_indices()
+    big = BatchSolver(q, max_batch=3, ordering=_lib.ORDER_ND)
+    ld1, st1 = big.factorize(q.data)
+    assert st1[0] == 0
+    small = GpuSolver()
+    small.factorize(ar1_q(40, 0.5, 1.0))
+    assert small.info()["max_m"] < 40
+    vals = np.stack([q.data, 2.0 * q.data])
+    ld2, st2 = big.factorize(vals)  # batch size 2: first capture of this sequence
+    assert np.all(st2 == 0)
+    rhs = np.stack([np.sin(np.arange(q.shape[0]) * 0.1), np.cos(np.arange(q.shape[0]) * 0.2)])
+    xs = big.solve(rhs)
+    f = O.Factor(q, perm=O.default_perm(q))
+    ref = f.logdet()
+    assert abs(ld2[0] - ref) <= LOGDET_RTOL * abs(ref)
+    assert abs(ld2[1] - (ref + q.shape[0] * math.log(2.0))) <= LOGDET_RTOL * abs(ref)
+    assert backward_error(q, xs[0], rhs[0]) < 1e-14
+    assert backward_error(2.0 * q, xs[1], rhs[1]) < 1e-14
+    assert rel(xs[0], f.solve(rhs[0])) < SIGMA_RTOL
