@@ -460,6 +460,22 @@ int inla_marginal_quantiles(int n, const double* x, const double* y, int np, con
 int inla_model_selection(int family, int64_t nobs, const double* y, const double* p1, const double* p2, int K,
                          const double* weight, int mode_index, const double* cond_eta, const double* cond_eta_var,
                          int what, double* crit, double* cpo, double* pit);
+/* Device forms of the two entry points above: every array is a device pointer, the work is
+ * queued on `stream` (NULL = default stream). inla_predictor_moments_dev also returns the
+ * per-node predictor d_cond_eta / d_cond_eta_var [K][nobs] (A in CSR with int64 row pointers
+ * and int32 column indices; d_a_rowptr NULL means eta = x, nobs = n); it does not
+ * synchronize. inla_model_selection_dev takes the node weights on the host, synchronizes the
+ * stream and writes crit / cpo / pit on the host; its sums over observations use a fixed
+ * reduction order (identical run to run, equal to the host form to rounding). The predictor
+ * moments equal the host form bit for bit. */
+int inla_predictor_moments_dev(int64_t nobs, int64_t n, const int64_t* d_a_rowptr, const int* d_a_colidx,
+                               const double* d_a_vals, int K, const double* d_weight, const double* d_cond_mean,
+                               const double* d_cond_var, double* d_cond_eta, double* d_cond_eta_var,
+                               double* d_pred_mean, double* d_pred_var, void* stream);
+int inla_model_selection_dev(int family, int64_t nobs, const double* d_y, const double* d_p1, const double* d_p2,
+                             int K, const double* weight, int mode_index, const double* d_cond_eta,
+                             const double* d_cond_eta_var, int what, double* crit, double* cpo, double* pit,
+                             void* stream);
 /* compute_marginal_log_lik_gaussian (model_selection.rs:25-73): log_post_mode + m/2 log(2 pi)
  * - 1/2 log det(neg_hessian), neg_hessian row-major m x m; INLA_ERR_NOT_PD when it is not
  * positive definite. */

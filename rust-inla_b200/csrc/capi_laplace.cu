@@ -5,6 +5,7 @@
 #include <memory>
 
 #include "aggregate.hpp"
+#include "aggregate_dev.hpp"
 #include "capi_common.hpp"
 #include "driver.hpp"
 #include "marginals.hpp"
@@ -25,6 +26,9 @@ struct inla_laplace {
   int mode_index = 0, m = 0;
   double p1scale_mode = 1.0, mlik_gaussian = 0.0;
   bool fitted = false;
+  // device copies of cond_eta / cond_eta_var: the criteria of the fit are computed on the device
+  DBuf<double> d_cond_eta, d_cond_eta_var;
+  AggScratch agg;
 };
 
 namespace {
@@ -319,6 +323,8 @@ int inla_fit(inla_laplace* h, int m, const double* theta0, inla_theta_map_fn map
       fo.cancel = [cf, cu] { return cf(cu) != 0; };
     }
     FitResult R;
+    R.d_cond_eta = &h->d_cond_eta;
+    R.d_cond_eta_var = &h->d_cond_eta_var;
     int64_t before = E.launches();
     drv.fit(theta0, fo, R);
     g_launches += E.launches() - before;
@@ -400,8 +406,22 @@ int inla_fit_model_selection(inla_laplace* h, int what, double* crit, double* cp
     obs.p2 = S.p2.empty() ? nullptr : S.p2.data();
     obs.p1scale = h->p1scale_mode;
     ModelSelection ms;
-    const std::string err = model_selection(obs, (int)h->node_weight.size(), h->node_weight.data(), h->mode_index,
-                                            h->cond_eta.data(), h->cond_eta_var.data(), what, ms);
+    std::string err;
+    if (h->eng && h->d_cond_eta.p) {  // on the device, from the fit's per-node predictors
+      const LaplaceEngine& E = *h->eng;
+      DevObs dobs;
+      dobs.family = S.family;
+      dobs.nobs = S.nobs;
+      dobs.y = E.d_y();
+      dobs.p1 = E.d_p1();
+      dobs.p2 = E.d_p2();
+      dobs.p1scale = h->p1scale_mode;
+      err = dev_model_selection(E.stream(), dobs, (int)h->node_weight.size(), h->node_weight.data(), h->mode_index,
+                                h->d_cond_eta.p, h->d_cond_eta_var.p, what, h->agg, ms);
+    } else {
+      err = model_selection(obs, (int)h->node_weight.size(), h->node_weight.data(), h->mode_index,
+                            h->cond_eta.data(), h->cond_eta_var.data(), what, ms);
+    }
     if (!err.empty()) return fail(INLA_ERR_INVALID, err.c_str());
     fill_crit(ms, h->mlik_gaussian, crit, cpo, pit, S.nobs, what);
     return INLA_OK;
@@ -602,3 +622,61 @@ int inla_predictor_moments(int64_t nobs, int64_t n, const int64_t* a_rowptr, con
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// device forms of the post-node aggregation (caller's device buffers)
+// ---------------------------------------------------------------------------
+
+namespace {
+AggScratch& thread_agg_scratch() {
+  static thread_local AggScratch sc;
+  return sc;
+}
+}  // namespace
+
+int inla_predictor_moments_dev(int64_t nobs, int64_t n, const int64_t* d_a_rowptr, const int* d_a_colidx,
+                               const double* d_a_vals, int K, const double* d_weight, const double* d_cond_mean,
+                               const double* d_cond_var, double* d_cond_eta, double* d_cond_eta_var,
+                               double* d_pred_mean, double* d_pred_var, void* stream) {
+  try {
+    if (nobs < 1 || n < 1 || K < 1 || !d_weight || !d_cond_mean || !d_cond_var || !d_cond_eta || !d_cond_eta_var ||
+        !d_pred_mean || !d_pred_var || (d_a_rowptr && (!d_a_colidx || !d_a_vals)) || (!d_a_rowptr && nobs != n))
+      return fail(INLA_ERR_INVALID, "inla_predictor_moments_dev: invalid argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    DevCsrA A;
+    A.rp = d_a_rowptr;
+    A.ci = d_a_colidx;
+    A.v = d_a_vals;
+    dev_project_nodes(st, nobs, A, K, d_cond_mean, n, d_cond_var, n, d_cond_eta, d_cond_eta_var);
+    dev_mixture_moments(st, K, nobs, d_weight, d_cond_eta, nobs, d_cond_eta_var, nobs, d_pred_mean, d_pred_var);
+    g_launches += 2;
+    return INLA_OK;
+  } catch (...) {
+    return map_exception();
+  }
+}
+
+int inla_model_selection_dev(int family, int64_t nobs, const double* d_y, const double* d_p1, const double* d_p2,
+                             int K, const double* weight, int mode_index, const double* d_cond_eta,
+                             const double* d_cond_eta_var, int what, double* crit, double* cpo, double* pit,
+                             void* stream) {
+  try {
+    if (family < 0 || family > 3 || nobs < 0 || (nobs > 0 && !d_y) || K < 1 || !weight || mode_index < 0 ||
+        mode_index >= K || (nobs > 0 && (!d_cond_eta || !d_cond_eta_var)))
+      return fail(INLA_ERR_INVALID, "inla_model_selection_dev: invalid argument");
+    DevObs obs;
+    obs.family = family;
+    obs.nobs = nobs;
+    obs.y = d_y;
+    obs.p1 = d_p1;
+    obs.p2 = d_p2;
+    ModelSelection ms;
+    const std::string err = dev_model_selection((cudaStream_t)stream, obs, K, weight, mode_index, d_cond_eta,
+                                                d_cond_eta_var, what, thread_agg_scratch(), ms);
+    if (!err.empty()) return fail(INLA_ERR_INVALID, err.c_str());
+    fill_crit(ms, NAN, crit, cpo, pit, nobs, what);
+    return INLA_OK;
+  } catch (...) {
+    return map_exception();
+  }
+}

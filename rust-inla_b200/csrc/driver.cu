@@ -9,6 +9,7 @@
 #include <stdexcept>
 
 #include "aggregate.hpp"
+#include "aggregate_dev.hpp"
 #include "capi_common.hpp"
 #include "driver.hpp"
 #include "inla_b200.h"
@@ -604,8 +605,24 @@ void InlaDriver::fit_single_node(FitResult& out) {
   const int64_t nobs = S.identity_a ? n : S.nobs;
   out.cond_eta.resize(nobs);
   out.cond_eta_var.resize(nobs);
-  project_nodes(nobs, n, S.identity_a ? nullptr : S.acp.data(), S.aci.data(), S.av.data(), 1, means.data(),
-                vars.data(), out.cond_eta.data(), out.cond_eta_var.data());
+  {  // eta = A x* and its diagonal variance on the device (inference.rs:1142-1151)
+    DBuf<double> eta_local, etav_local;
+    DBuf<double>& d_eta = out.d_cond_eta ? *out.d_cond_eta : eta_local;
+    DBuf<double>& d_etav = out.d_cond_eta_var ? *out.d_cond_eta_var : etav_local;
+    d_eta.alloc(nobs);
+    d_etav.alloc(nobs);
+    DevCsrA A;
+    A.rp = eng_.d_acp();
+    A.ci = eng_.d_aci();
+    A.v = eng_.d_av();
+    dev_project_nodes(eng_.stream(), nobs, A, 1, eng_.d_x(), eng_.xstride(), eng_.d_var(), eng_.xstride(), d_eta.p,
+                      d_etav.p);
+    INLA_CUDA(cudaMemcpyAsync(out.cond_eta.data(), d_eta.p, sizeof(double) * nobs, cudaMemcpyDeviceToHost,
+                              eng_.stream()));
+    INLA_CUDA(cudaMemcpyAsync(out.cond_eta_var.data(), d_etav.p, sizeof(double) * nobs, cudaMemcpyDeviceToHost,
+                              eng_.stream()));
+    INLA_CUDA(cudaStreamSynchronize(eng_.stream()));
+  }
   out.pred_mean = out.cond_eta;
   out.pred_var = out.cond_eta_var;
   out.mode_index = 0;
@@ -715,8 +732,13 @@ void InlaDriver::fit(const double* theta0, const FitOptions& opt, FitResult& out
       thetas[(size_t)k * m + i] = mode[i] + d;
     }
 
-  // node evaluations (inference.rs:1306-1397): x*, Takahashi variances, log posterior
+  // node evaluations (inference.rs:1306-1397): x*, Takahashi variances, log posterior. The
+  // node results stay on the device for the aggregation below; the host keeps a copy for the
+  // marginals of the fit.
   std::vector<double> lp(K), means((size_t)K * n), vars((size_t)K * n);
+  DBuf<double> d_means, d_vars;
+  d_means.alloc((size_t)K * n);
+  d_vars.alloc((size_t)K * n);
   {
     const int Bmax = opt.batched ? eng_.max_batch() : 1;
     std::vector<double> fk(K);
@@ -726,22 +748,25 @@ void InlaDriver::fit(const double* theta0, const FitOptions& opt, FitResult& out
       evaluate(Bc, thetas.data() + (size_t)k0 * m, false, true, fk.data() + k0, nullptr, &keep);
       const LaplaceOut& R = keep.back();
       const size_t w = sizeof(double) * n, pitch = sizeof(double) * eng_.xstride();
-      INLA_CUDA(cudaMemcpy2DAsync(means.data() + (size_t)k0 * n, w, eng_.d_x(), pitch, w, Bc,
-                                  cudaMemcpyDeviceToHost, eng_.stream()));
-      INLA_CUDA(cudaMemcpy2DAsync(vars.data() + (size_t)k0 * n, w, eng_.d_var(), pitch, w, Bc,
-                                  cudaMemcpyDeviceToHost, eng_.stream()));
-      INLA_CUDA(cudaStreamSynchronize(eng_.stream()));
+      INLA_CUDA(cudaMemcpy2DAsync(d_means.p + (size_t)k0 * n, w, eng_.d_x(), pitch, w, Bc, cudaMemcpyDeviceToDevice,
+                                  eng_.stream()));
+      INLA_CUDA(cudaMemcpy2DAsync(d_vars.p + (size_t)k0 * n, w, eng_.d_var(), pitch, w, Bc, cudaMemcpyDeviceToDevice,
+                                  eng_.stream()));
       for (int b = 0; b < Bc; ++b) {
         const int k = k0 + b;
         if (R.status[b] != LAP_OK || fk[k] >= 1e12) {
           lp[k] = -std::numeric_limits<double>::infinity();
-          std::fill(means.begin() + (size_t)k * n, means.begin() + (size_t)(k + 1) * n, 0.0);
-          std::fill(vars.begin() + (size_t)k * n, vars.begin() + (size_t)(k + 1) * n, 1.0);
+          INLA_CUDA(cudaMemsetAsync(d_means.p + (size_t)k * n, 0, w, eng_.stream()));
+          std::vector<double> ones(n, 1.0);
+          INLA_CUDA(cudaMemcpyAsync(d_vars.p + (size_t)k * n, ones.data(), w, cudaMemcpyHostToDevice, eng_.stream()));
+          INLA_CUDA(cudaStreamSynchronize(eng_.stream()));  // `ones` is released at the end of this block
         } else {
           lp[k] = -fk[k];
         }
       }
     }
+    INLA_CUDA(cudaMemcpyAsync(means.data(), d_means.p, sizeof(double) * K * n, cudaMemcpyDeviceToHost, eng_.stream()));
+    INLA_CUDA(cudaMemcpyAsync(vars.data(), d_vars.p, sizeof(double) * K * n, cudaMemcpyDeviceToHost, eng_.stream()));
   }
   double mx = -std::numeric_limits<double>::infinity();
   for (double v : lp) mx = std::max(mx, v);
@@ -753,21 +778,40 @@ void InlaDriver::fit(const double* theta0, const FitOptions& opt, FitResult& out
     sw += zw[k] * dens[k];
   }
   for (int k = 0; k < K; ++k) nw[k] = zw[k] * dens[k] / sw;
-  out.latent_mean.assign(n, 0.0);
-  out.latent_var.assign(n, 0.0);
-  mixture_moments(K, n, nw.data(), means.data(), vars.data(), out.latent_mean.data(), out.latent_var.data());
-  // linear predictor eta = A x* per node and its diagonal variance (inference.rs:1370-1384, 1451-1466)
+  // mixture moments of the latent field and the linear predictor eta = A x per node with its
+  // diagonal variance (inference.rs:1370-1384, 1436-1466), on the device
   {
+    cudaStream_t st = eng_.stream();
     const LaplaceSpec& S = eng_.spec();
     const int64_t nobs = S.identity_a ? n : S.nobs;
+    DBuf<double> d_w, d_lat, d_pred, eta_local, etav_local;
+    d_w.upload(nw.data(), K, st);
+    d_lat.alloc(2 * (size_t)n);
+    d_pred.alloc(2 * (size_t)nobs);
+    DBuf<double>& d_eta = out.d_cond_eta ? *out.d_cond_eta : eta_local;
+    DBuf<double>& d_etav = out.d_cond_eta_var ? *out.d_cond_eta_var : etav_local;
+    d_eta.alloc((size_t)K * nobs);
+    d_etav.alloc((size_t)K * nobs);
+    dev_mixture_moments(st, K, n, d_w.p, d_means.p, n, d_vars.p, n, d_lat.p, d_lat.p + n);
+    DevCsrA A;
+    A.rp = eng_.d_acp();
+    A.ci = eng_.d_aci();
+    A.v = eng_.d_av();
+    dev_project_nodes(st, nobs, A, K, d_means.p, n, d_vars.p, n, d_eta.p, d_etav.p);
+    dev_mixture_moments(st, K, nobs, d_w.p, d_eta.p, nobs, d_etav.p, nobs, d_pred.p, d_pred.p + nobs);
+    out.latent_mean.resize(n);
+    out.latent_var.resize(n);
+    out.pred_mean.resize(nobs);
+    out.pred_var.resize(nobs);
     out.cond_eta.resize((size_t)K * nobs);
     out.cond_eta_var.resize((size_t)K * nobs);
-    project_nodes(nobs, n, S.identity_a ? nullptr : S.acp.data(), S.aci.data(), S.av.data(), K, means.data(),
-                  vars.data(), out.cond_eta.data(), out.cond_eta_var.data());
-    out.pred_mean.assign(nobs, 0.0);
-    out.pred_var.assign(nobs, 0.0);
-    mixture_moments(K, nobs, nw.data(), out.cond_eta.data(), out.cond_eta_var.data(), out.pred_mean.data(),
-                    out.pred_var.data());
+    INLA_CUDA(cudaMemcpyAsync(out.latent_mean.data(), d_lat.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    INLA_CUDA(cudaMemcpyAsync(out.latent_var.data(), d_lat.p + n, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    INLA_CUDA(cudaMemcpyAsync(out.pred_mean.data(), d_pred.p, sizeof(double) * nobs, cudaMemcpyDeviceToHost, st));
+    INLA_CUDA(cudaMemcpyAsync(out.pred_var.data(), d_pred.p + nobs, sizeof(double) * nobs, cudaMemcpyDeviceToHost, st));
+    INLA_CUDA(cudaMemcpyAsync(out.cond_eta.data(), d_eta.p, sizeof(double) * K * nobs, cudaMemcpyDeviceToHost, st));
+    INLA_CUDA(cudaMemcpyAsync(out.cond_eta_var.data(), d_etav.p, sizeof(double) * K * nobs, cudaMemcpyDeviceToHost, st));
+    INLA_CUDA(cudaStreamSynchronize(st));
   }
   // model-selection inputs (inference.rs:1296-1304, 1470-1485): the node nearest the mode, the
   // Gaussian-approximation mlik there, and the observations rebuilt at the mode

@@ -41,6 +41,10 @@ struct FitOptions {
 };
 
 struct FitResult {
+  // device copies of the per-node predictor and its variance [K][nobs] (filled when set; the
+  // model-selection criteria of the fit read them on the device)
+  DBuf<double>* d_cond_eta = nullptr;
+  DBuf<double>* d_cond_eta_var = nullptr;
   std::vector<double> mode, hessian, latent_mean, latent_var, node_theta, node_weight, node_logpost;
   std::vector<double> pred_mean, pred_var;  // linear predictor eta = A x: mixture mean and variance
   std::vector<double> cond_eta, cond_eta_var;  // [K][nobs] per-node predictor and its variance

@@ -102,6 +102,13 @@ class LaplaceEngine {
   const double* d_x() const { return x_.p; }      // [B][n] modes
   const double* d_var() const { return var_.p; }  // [B][n] marginal variances
   const double* d_eta() const { return eta_.p; }  // [B][nobs] predictor at the mode
+  // the model's A (CSR; d_acp() is nullptr when eta = x) and observations on the device
+  const int64_t* d_acp() const { return spec_.identity_a ? nullptr : acp_.p; }
+  const int* d_aci() const { return aci_.p; }
+  const double* d_av() const { return av_.p; }
+  const double* d_y() const { return y_.p; }
+  const double* d_p1() const { return spec_.p1.empty() ? nullptr : p1_.p; }
+  const double* d_p2() const { return spec_.p2.empty() ? nullptr : p2_.p; }
   GpuFactor& factor() { return *F_; }
   int64_t launches() const { return launches_ + F_->launches(); }
   cudaStream_t stream() const { return stream_; }

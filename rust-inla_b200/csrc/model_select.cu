@@ -7,12 +7,11 @@
 #include "host_par.hpp"
 #include "likelihood.cuh"
 #include "model_select.hpp"
+#include "model_select_core.cuh"
 
 namespace inla {
 
 namespace {
-
-constexpr double kCpoDiff = 3.0;  // CPO_DIFF (model_selection.rs:7)
 
 struct Lik {
   double logp, grad, hess;
@@ -28,103 +27,17 @@ bool lik_at(const ObsView& obs, int64_t i, double eta, Lik& out) {
 }  // namespace
 
 bool observation_cdf(int family, double y, double p1, double eta, double variance, double& out) {
-  // the count CDFs below sum term by term up to floor(y); counts beyond 1e15 (and non-finite y)
-  // get no CDF instead of a loop of that length
-  if (!std::isfinite(y) || (family != FAM_GAUSSIAN && y > 1e15)) return false;
-  switch (family) {
-    case FAM_GAUSSIAN: {
-      const double total_var = 1.0 / p1 + variance;
-      if (total_var <= 0.0) return false;
-      out = normal_cdf((y - eta) / std::sqrt(total_var));
-      return true;
-    }
-    case FAM_POISSON: {
-      const double lambda = p1 * std::exp(eta);
-      if (lambda < 0.0 || !std::isfinite(lambda)) return false;
-      const double yf = std::floor(y);
-      if (yf < 0.0) {
-        out = 0.0;
-        return true;
-      }
-      out = poisson_cdf(lambda, (uint64_t)yf);
-      return true;
-    }
-    case FAM_BINOMIAL: {
-      const double prob = d_logistic(eta);
-      const uint64_t n = (std::isfinite(p1) && p1 > 0.0) ? (uint64_t)p1 : 0;  // f64 as u64 saturates at 0
-      const double yf = std::floor(y);
-      if (yf < 0.0) {
-        out = 0.0;
-        return true;
-      }
-      out = binomial_cdf(n, prob, yf >= (double)n ? n : (uint64_t)yf);
-      return true;
-    }
-    default:
-      return false;  // negative binomial: no CDF in the reference
-  }
+  return ms_observation_cdf(family, y, p1, eta, variance, out);
 }
 
-double normal_cdf(double x) {
-  // Abramowitz & Stegun 7.1.26 rational approximation of erf, as the reference uses
-  const double A1 = 0.254829592, A2 = -0.284496736, A3 = 1.421413741, A4 = -1.453152027, A5 = 1.061405429,
-               P = 0.3275911;
-  const double sign = x < 0.0 ? -1.0 : 1.0;
-  const double ax = std::fabs(x);
-  const double t = 1.0 / (1.0 + P * ax);
-  const double y = 1.0 - (((((A5 * t + A4) * t) + A3) * t + A2) * t + A1) * t * std::exp(-ax * ax / 2.0);
-  return 0.5 * (1.0 + sign * y);
-}
+double normal_cdf(double x) { return ms_normal_cdf(x); }
 
-double poisson_cdf(double lambda, uint64_t k) {
-  if (lambda <= 0.0) return 1.0;
-  double cdf = 0.0, log_pmf = -lambda;
-  for (uint64_t j = 0; j <= k; ++j) {
-    cdf += std::exp(log_pmf);
-    if (j < k) log_pmf += std::log(lambda) - std::log((double)(j + 1));
-  }
-  return std::min(cdf, 1.0);
-}
+double poisson_cdf(double lambda, uint64_t k) { return ms_poisson_cdf(lambda, k); }
 
-double binomial_cdf(uint64_t n, double p, uint64_t k) {
-  if (p <= 0.0) return 1.0;
-  if (p >= 1.0) return k >= n ? 1.0 : 0.0;
-  double cdf = 0.0;
-  for (uint64_t j = 0; j <= k; ++j) {
-    const double log_choose =
-        d_log_gamma((double)n + 1.0) - d_log_gamma((double)j + 1.0) - d_log_gamma((double)(n - j) + 1.0);
-    const double log_pmf = log_choose + (double)j * std::log(p) + (double)(n - j) * std::log(1.0 - p);
-    cdf += std::exp(log_pmf);
-  }
-  return std::min(cdf, 1.0);
-}
+double binomial_cdf(uint64_t n, double p, uint64_t k) { return ms_binomial_cdf(n, p, k); }
 
 bool cpo_failure(int family, double y, double p1, double p2, double mu, double var) {
-  if (var <= 0.0 || !std::isfinite(var)) return true;
-  double lp, g, h, dw;
-  if (d_eval_lik(family, mu, y, p1, p2, lp, g, h, dw)) return true;
-  const double c = -h;
-  const double tau_loo = 1.0 / var - c;
-  if (tau_loo <= 0.0 || !std::isfinite(tau_loo)) return true;
-  const double var_loo = 1.0 / tau_loo, std_loo = std::sqrt(var_loo);
-  const double mu_loo = var_loo * (mu / var - c * mu + g);
-  const double steps[5] = {-3.0, -1.5, 0.0, 1.5, 3.0};
-  double ld[5];
-  for (int s = 0; s < 5; ++s) {
-    const double x = mu_loo + steps[s] * std_loo;
-    const double prior = -0.5 * (x - mu) * (x - mu) / var;
-    if (d_eval_lik(family, x, y, p1, p2, lp, g, h, dw)) return true;
-    ld[s] = prior + lp;
-  }
-  bool inc = true, dec = true;
-  for (int s = 1; s < 5; ++s) {
-    if (ld[s] < ld[s - 1]) inc = false;
-    if (ld[s] > ld[s - 1]) dec = false;
-  }
-  if (inc || dec) return true;
-  double mx = -std::numeric_limits<double>::infinity();
-  for (int s = 0; s < 5; ++s) mx = std::fmax(mx, ld[s]);
-  return mx - ld[0] < kCpoDiff || mx - ld[4] < kCpoDiff;
+  return ms_cpo_failure(family, y, p1, p2, mu, var);
 }
 
 bool mlik_gaussian(double log_post_mode, int m, const double* neg_hessian, double& out) {
@@ -239,42 +152,11 @@ std::string model_selection(const ObsView& obs, int K, const double* w, int mode
     out.pit.assign(n, NaN);
     std::vector<char> failed(n, 0);
     parallel_for(n, [&](int64_t i0, int64_t i1) {
-      std::vector<double> lls(K);
       for (int64_t i = i0; i < i1; ++i) {
-        const double y = obs.y[i];
         const double q1 = (obs.p1 ? obs.p1[i] : 1.0) * obs.p1scale, q2 = obs.p2 ? obs.p2[i] : 1.0;
-        bool fail = false;
-        for (int k = 0; k < K && !fail; ++k)
-          fail = cpo_failure(obs.family, y, q1, q2, cond_eta[(size_t)k * n + i], cond_eta_var[(size_t)k * n + i]);
-        Lik e;
-        for (int k = 0; k < K && !fail; ++k) {
-          if (!lik_at(obs, i, cond_eta[(size_t)k * n + i], e)) fail = true;
-          else lls[k] = e.logp;
-        }
-        if (fail || K < 2) {
+        if (!ms_cpo_pit_obs(obs.family, obs.y[i], q1, q2, K, w, cond_eta + i, cond_eta_var + i, n, out.cpo[i],
+                            out.pit[i]))
           failed[i] = 1;
-          continue;
-        }
-        double max_neg = -std::numeric_limits<double>::infinity();
-        for (int k = 0; k < K; ++k) max_neg = std::fmax(max_neg, -lls[k]);
-        double inv = 0.0;
-        for (int k = 0; k < K; ++k) inv += w[k] * std::exp(-lls[k] - max_neg);
-        const double inv_scaled = inv * std::exp(max_neg);
-        if (!std::isfinite(inv_scaled) || inv_scaled <= 0.0) {
-          failed[i] = 1;
-          continue;
-        }
-        out.cpo[i] = 1.0 / inv_scaled;
-        double pit = 0.0;
-        bool pit_ok = true;
-        for (int k = 0; k < K && pit_ok; ++k) {
-          double f;
-          if (observation_cdf(obs.family, y, q1, cond_eta[(size_t)k * n + i], cond_eta_var[(size_t)k * n + i], f))
-            pit += w[k] * f;
-          else
-            pit_ok = false;
-        }
-        if (pit_ok && std::isfinite(pit)) out.pit[i] = std::min(std::max(pit, 0.0), 1.0);
       }
     }, 2048);
     for (int64_t i = 0; i < n; ++i) out.cpo_failures += failed[i];

@@ -126,6 +126,9 @@ SIGNATURES = [
     ("inla_fit_model_selection", C.c_int, [P, C.c_int, DP, DP, DP]),
     ("inla_model_selection", C.c_int, [C.c_int, I64, DP, DP, DP, C.c_int, DP, C.c_int, DP, DP, C.c_int, DP, DP,
                                        DP]),
+    ("inla_predictor_moments_dev", C.c_int, [I64, I64, P, P, P, C.c_int, P, P, P, P, P, P, P, P]),
+    ("inla_model_selection_dev", C.c_int, [C.c_int, I64, P, P, P, C.c_int, DP, C.c_int, P, P, C.c_int, DP, DP, DP,
+                                           P]),
     ("inla_mlik_gaussian", C.c_int, [C.c_double, C.c_int, DP, DP]),
     ("inla_fit_marginal", C.c_int, [P, C.c_int, I64, C.c_int, C.c_double, DP, DP]),
     ("inla_fit_posterior_precision", C.c_int, [P, LP, LP, LP, DP]),
