@@ -217,6 +217,23 @@ int inla_batch_selinv_pattern(inla_batch* h, int B, double* sigma);
  * synchronize the host. Inputs/outputs live in device memory. */
 int inla_batch_factorize_dev(inla_batch* h, int B, const double* d_values, double* d_logdet, int* d_status,
                              void* stream);
+/* Schedule of the numeric factorization (no reference counterpart; the reference runs faer's
+ * factorization per theta-point): *persistent = 1 when the handle factorizes every front of
+ * every batch member in ONE persistent launch (a task queue in elimination-tree order with
+ * bounded dependency waits), 0 when it launches the kernels level by level (fronts too wide
+ * for the persistent kernel's shared memory, or INLA_NO_PERSIST set). Results are the same
+ * bit for bit. A persistent launch whose dependency wait ran out (2 s; INLA_PERSIST_WAIT_MS)
+ * ends early and the call that synchronizes after it returns INLA_ERR_CUDA (status bit 4 in
+ * the _dev status words). */
+int inla_batch_schedule(inla_batch* h, int* persistent);
+/* Process-wide choice for engines (solver, batch, Laplace, many-model handles) created after
+ * the call: on != 0 the persistent schedule where it fits, 0 the level launches. */
+int inla_set_persistent_schedule(int on);
+/* Diagnostic of the bounded waits: runs the persistent factorization once with completion
+ * counts that can never be reached and a wait limit of limit_ms, and returns in *code what
+ * the launch recorded (1: a wait ran out and the launch ended). The handle stays usable;
+ * factorize again before solving. */
+int inla_batch_wait_limit_selftest(inla_batch* h, double limit_ms, int* code);
 int inla_batch_solve_dev(inla_batch* h, int B, double* d_x, void* stream);
 int inla_batch_diag_inv_dev(inla_batch* h, int B, double* d_diag, void* stream);
 int inla_batch_selinv_pattern_dev(inla_batch* h, int B, double* d_sigma, void* stream);

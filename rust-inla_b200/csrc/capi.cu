@@ -38,6 +38,7 @@ int map_exception() {
 
 int status_to_code(int st) {
   if (st == kStatusOk) return INLA_OK;
+  if (st & kStatusSchedule) return INLA_ERR_CUDA;  // the persistent schedule stopped early
   return INLA_ERR_SINGULAR;  // sparse_ldlt.rs:117-120,140-142: tiny or non-finite pivot => Singular
 }
 
@@ -211,6 +212,7 @@ int inla_solver_factorize(inla_solver* s, int64_t n, const int64_t* colptr, cons
     INLA_CUDA(cudaMemcpyAsync(&ld, E.d_logdet(), sizeof(double), cudaMemcpyDeviceToHost, s->stream));
     INLA_CUDA(cudaMemcpyAsync(&st, E.d_status(), sizeof(int), cudaMemcpyDeviceToHost, s->stream));
     INLA_CUDA(cudaStreamSynchronize(s->stream));
+    E.check_schedule();
     int code = status_to_code(st);
     if (code != INLA_OK) return fail(code, "Matrix is singular or structurally rank-deficient");
     s->logdet = ld;
@@ -367,6 +369,29 @@ void inla_batch_free(inla_batch* h) {
   delete h;
 }
 
+int inla_set_persistent_schedule(int on) {
+  set_persistent_default(on != 0);
+  return INLA_OK;
+}
+
+int inla_batch_schedule(inla_batch* h, int* persistent) {
+  if (!h || !h->eng || !persistent) return fail(INLA_ERR_INVALID, "null batch handle or output");
+  *persistent = h->eng->persistent() ? 1 : 0;
+  return INLA_OK;
+}
+
+int inla_batch_wait_limit_selftest(inla_batch* h, double limit_ms, int* code) {
+  try {
+    if (!h || !h->eng || !code || !(limit_ms > 0.0)) return fail(INLA_ERR_INVALID, "invalid argument");
+    if (!h->eng->persistent()) return fail(INLA_ERR_INVALID, "the handle does not use the persistent schedule");
+    *code = h->eng->persist_wait_limit_selftest(limit_ms);
+    h->factored_b = 0;  // the fronts hold nothing usable now
+    return INLA_OK;
+  } catch (...) {
+    return map_exception();
+  }
+}
+
 static void check_batch(inla_batch* h, int B) {
   if (!h || !h->eng) throw InlaError(INLA_ERR_INVALID, "null batch handle");
   if (B < 1 || B > h->eng->max_batch()) throw InlaError(INLA_ERR_DIM_MISMATCH, "batch size out of range");
@@ -408,6 +433,7 @@ int inla_batch_factorize(inla_batch* h, int B, const double* values, double* log
     INLA_CUDA(cudaMemcpyAsync(ld.data(), E.d_logdet(), sizeof(double) * B, cudaMemcpyDeviceToHost, h->stream));
     INLA_CUDA(cudaMemcpyAsync(st.data(), E.d_status(), sizeof(int) * B, cudaMemcpyDeviceToHost, h->stream));
     INLA_CUDA(cudaStreamSynchronize(h->stream));
+    E.check_schedule();
     int code = INLA_OK;
     for (int b = 0; b < B; ++b) {
       if (logdet) logdet[b] = ld[b];

@@ -28,5 +28,6 @@ struct DevSym {
 constexpr int kStatusOk = 0;
 constexpr int kStatusSingular = 1;
 constexpr int kStatusNotFinite = 2;
+constexpr int kStatusSchedule = 4;  // the persistent schedule stopped early (a dependency wait ran out)
 
 }  // namespace inla

@@ -4,12 +4,14 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 
 #include "gpu_factor.hpp"
 #include "host_par.hpp"
 #include "snode_kernels.cuh"
 #include "snode_large.cuh"
+#include "snode_persist.cuh"
 
 namespace inla {
 
@@ -202,6 +204,7 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
     d_grng_.upload(grng, stream_);
   }
 
+  plan_persist();
   const auto ta = std::chrono::steady_clock::now();
   F_.alloc((size_t)max_batch_ * ftotal_);
   xp_.alloc((size_t)max_batch_ * n);
@@ -245,6 +248,14 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
   set_smem(k_gather8, 200 * 1024 + 8 * kGatherCols * 8);
   set_smem(k_si_gemm64, kSiGemmSmem);
   set_smem(k_si_diag64, kSiDiagSmem);
+  if (persist_) {
+    set_smem(k_factor_persist, persist_smem_);
+    int per_sm = 0;
+    INLA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_factor_persist, kPersistThreads,
+                                                            persist_smem_));
+    persist_grid_ = std::max(1, per_sm) * num_sms_;
+    if (per_sm < 1) persist_ = false;
+  }
   INLA_CUDA(cudaStreamSynchronize(stream_));
   if (std::getenv("INLA_DEBUG"))
     std::fprintf(stderr, "device factor: maps %.1f ms, symbolic uploads %.1f ms, caches %.1f ms, levels %.1f ms, buffers %.1f ms (%d slots)\n",
@@ -317,6 +328,195 @@ void GpuFactor::plan_levels() {
     P.off_si_large = put(P.si_large);
   }
   d_lists_.upload(flat, stream_);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent schedule: the task queue of k_factor_persist (see snode_persist.cuh).
+// Per level: tiny fronts in groups of eight, small fronts, then the large fronts phase by
+// phase (extend-add chunks; per 64-column block the diagonal block, the row blocks and the
+// trailing-update tiles). Each phase of a level is one group; within a group the tasks of
+// problem 0 come first, then problem 1, and so on.
+// ---------------------------------------------------------------------------
+namespace {
+// Process-wide default of the schedule for engines built from now on (INLA_NO_PERSIST in the
+// environment starts it off; inla_set_persistent_schedule changes it).
+std::atomic<int> g_persist_default{-1};
+}  // namespace
+
+void set_persistent_default(bool on) { g_persist_default.store(on ? 1 : 0); }
+
+void GpuFactor::plan_persist() {
+  int def = g_persist_default.load();
+  if (def < 0) {
+    def = std::getenv("INLA_NO_PERSIST") ? 0 : 1;
+    int expect = -1;
+    g_persist_default.compare_exchange_strong(expect, def);
+    def = g_persist_default.load();
+  }
+  if (def == 0) return;
+  if (const char* w = std::getenv("INLA_PERSIST_WAIT_MS")) persist_limit_ns_ = (long long)(std::atof(w) * 1e6);
+  const Symbolic& S = sym_;
+  const int ns = (int)S.nsuper;
+  constexpr int kGatherBudget = 110 * 1024;  // bytes of one extend-add column slice
+  int smem = std::max({kPersistTinySmem, small_factor_smem(kSmallB), kPanelSmem, kRowsSmem, kPersistUpdSmem});
+  std::vector<int> gstart{0}, task, tiny, total(ns, 0), lid(ns, -1);
+  std::vector<int64_t> gptr(ns, 0);
+  std::vector<int2> grng;
+  int nlarge = 0;
+  auto push = [&](int type, int sn, int sub, int need, int j0, int gcols) {
+    task.insert(task.end(), {type, sn, sub, need, j0, gcols});
+  };
+  auto close_group = [&] {
+    const int cnt = (int)(task.size() / 6);
+    if (cnt > gstart.back()) gstart.push_back(cnt);
+  };
+  struct Phase {
+    int type, count, j0;
+  };
+  for (const LevelPlan& P : levels_) {
+    for (size_t i = 0; i < P.tiny.size(); i += kPersistTinyWarps) {
+      const int cnt = (int)std::min<size_t>(kPersistTinyWarps, P.tiny.size() - i);
+      push(PT_TINY, (int)tiny.size(), cnt, 0, 0, 0);
+      for (int u = 0; u < cnt; ++u) {
+        tiny.push_back(P.tiny[i + u]);
+        total[P.tiny[i + u]] = 1;
+      }
+    }
+    close_group();
+    for (const std::vector<int>* v : {&P.small_a, &P.small_b})
+      for (int sn : *v) {
+        push(PT_SMALL, sn, 0, 0, 0, 0);
+        total[sn] = 1;
+      }
+    close_group();
+    if (P.large.empty()) continue;
+    // phases of every large front: 0 extend-add, then (diagonal, rows, update) per block
+    std::vector<std::vector<Phase>> ph(P.large.size());
+    std::vector<int> gc(P.large.size());
+    size_t maxp = 0;
+    for (size_t f = 0; f < P.large.size(); ++f) {
+      const int sn = P.large[f];
+      const int k = (int)(S.sn_first[sn + 1] - S.sn_first[sn]), m = (int)(S.sn_rowptr[sn + 1] - S.sn_rowptr[sn]);
+      const int gcols = std::max(1, std::min(kGatherCols, kGatherBudget / (8 * m)));
+      gc[f] = gcols;
+      smem = std::max(smem, gcols * m * 8);
+      lid[sn] = nlarge++;
+      const int nz = cdiv(m, gcols);
+      gptr[sn] = (int64_t)grng.size();
+      for (int z = 0; z < nz; ++z) {
+        const int c0 = z * gcols, c1 = std::min(c0 + gcols, m);
+        for (int64_t q = S.child_ptr[sn]; q < S.child_ptr[sn + 1]; ++q) {
+          const int c = (int)S.child_list[q];
+          const int kc = (int)(S.sn_first[c + 1] - S.sn_first[c]);
+          const int rc = (int)(S.sn_rowptr[c + 1] - S.sn_rowptr[c]) - kc;
+          const int32_t* rel = S.rel.data() + S.rel_ptr[c];
+          const int lo = (int)(std::lower_bound(rel, rel + rc, c0) - rel);
+          const int hi = (int)(std::lower_bound(rel, rel + rc, c1) - rel);
+          grng.push_back(make_int2(lo, hi));
+        }
+      }
+      ph[f].push_back({PT_GATHER, nz, 0});
+      for (int j0 = 0; j0 < k; j0 += kB64) {
+        const int w = std::min(kB64, k - j0), below = std::max(m - j0 - w, 0);
+        const int nt = cdiv(below, kUT64);
+        ph[f].push_back({PT_DIAG, 1, j0});
+        ph[f].push_back({PT_ROWS, cdiv(below, kPanelRows), j0});
+        ph[f].push_back({PT_UPDATE, std::max(1, nt * (nt + 1) / 2), j0});
+      }
+      maxp = std::max(maxp, ph[f].size());
+      int tot = 0;
+      for (const Phase& x : ph[f]) tot += x.count;
+      total[sn] = tot;
+    }
+    std::vector<int> done(P.large.size(), 0);
+    for (size_t p = 0; p < maxp; ++p) {
+      for (size_t f = 0; f < P.large.size(); ++f) {
+        if (p >= ph[f].size()) continue;
+        const Phase& x = ph[f][p];
+        for (int u = 0; u < x.count; ++u) push(x.type, P.large[f], u, done[f], x.j0, gc[f]);
+        done[f] += x.count;
+      }
+      close_group();
+    }
+  }
+  if (smem > 227 * 1024) return;  // a front too wide for the schedule's shared memory: keep the level launches
+  const size_t dc_doubles = (size_t)std::max(nlarge, 1) * max_batch_ * kB64 * kB64;
+  if (dc_doubles * 8 > ((size_t)4 << 30)) return;
+  if (tiny.empty()) tiny.push_back(0);
+  if (grng.empty()) grng.push_back(make_int2(0, 0));
+  persist_groups_ = (int)gstart.size() - 1;
+  if (persist_groups_ < 1) return;
+  d_pgstart_.upload(gstart, stream_);
+  d_ptask_.upload(task, stream_);
+  d_ptiny_.upload(tiny, stream_);
+  d_ptotal_.upload(total, stream_);
+  d_plid_.upload(lid, stream_);
+  d_pgptr_.upload(gptr, stream_);
+  d_pgrng_.upload(grng, stream_);
+  d_pstate_.alloc(2 + (size_t)max_batch_ * ns);
+  INLA_CUDA(cudaMemsetAsync(d_pstate_.p, 0, sizeof(int) * (2 + (size_t)max_batch_ * ns), stream_));
+  dcache_p_.alloc(dc_doubles);
+  persist_smem_ = smem;
+  persist_ = true;
+}
+
+void GpuFactor::run_factor_persist(int B, const int* total_override, long long limit_ns) {
+  const int ns = (int)sym_.nsuper;
+  // head and the completion counts start at zero; the error record (word 0) stays until read
+  INLA_CUDA(cudaMemsetAsync(d_pstate_.p + 1, 0, sizeof(int) * (1 + (size_t)B * ns), stream_));
+  PersistArgs a;
+  a.S = ds_;
+  a.F = F_.p;
+  a.fstride = ftotal_;
+  a.B = B;
+  a.ngroups = persist_groups_;
+  a.gstart = d_pgstart_.p;
+  a.task = reinterpret_cast<const PersistTask*>(d_ptask_.p);
+  a.tiny_list = d_ptiny_.p;
+  a.total = total_override ? total_override : d_ptotal_.p;
+  a.prog = d_pstate_.p + 2;
+  a.head = reinterpret_cast<unsigned*>(d_pstate_.p + 1);
+  a.err = d_pstate_.p;
+  a.dcache = dcache_p_.p;
+  a.lid = d_plid_.p;
+  a.linv = linv_.p;
+  a.gptr = d_pgptr_.p;
+  a.grng = d_pgrng_.p;
+  a.limit_ns = limit_ns > 0 ? limit_ns : persist_limit_ns_;
+  k_factor_persist<<<persist_grid_, kPersistThreads, persist_smem_, stream_>>>(a);
+  k_logdet_chunks<<<dim3(nldchunk_, B), 256, 0, stream_>>>(ds_, F_.p, ftotal_, ldpart_.p, ldflag_.p, ldticket_.p,
+                                                           logdet_.p, status_.p, d_pstate_.p);
+  launches_ += 2;
+}
+
+void GpuFactor::check_schedule() {
+  if (!persist_) return;
+  int err = 0;
+  INLA_CUDA(cudaMemcpyAsync(&err, d_pstate_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+  INLA_CUDA(cudaStreamSynchronize(stream_));
+  if (err == 0) return;
+  INLA_CUDA(cudaMemsetAsync(d_pstate_.p, 0, sizeof(int), stream_));
+  INLA_CUDA(cudaStreamSynchronize(stream_));
+  throw CudaError("persistent factorization stopped: a dependency wait ran out (code " + std::to_string(err) + ")",
+                  (int)cudaErrorLaunchTimeout);
+}
+
+int GpuFactor::persist_wait_limit_selftest(double limit_ms) {
+  if (!persist_) return -1;
+  const int ns = (int)sym_.nsuper;
+  // completion counts no front can reach: every front with children waits until the limit
+  std::vector<int> never(ns, 1 << 30);
+  DBuf<int> d_never;
+  d_never.upload(never, stream_);
+  INLA_CUDA(cudaMemsetAsync(F_.p, 0, sizeof(double) * ftotal_, stream_));  // a defined input for the fronts that run
+  run_factor_persist(1, d_never.p, (long long)(limit_ms * 1e6));
+  INLA_CUDA(cudaGetLastError());
+  int err = 0;
+  INLA_CUDA(cudaMemcpyAsync(&err, d_pstate_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+  INLA_CUDA(cudaStreamSynchronize(stream_));
+  INLA_CUDA(cudaMemsetAsync(d_pstate_.p, 0, sizeof(int), stream_));
+  INLA_CUDA(cudaStreamSynchronize(stream_));
+  return err;
 }
 
 void GpuFactor::run_factor_levels(int B, const std::vector<char>* fuse, cudaEvent_t* ev) {
@@ -504,10 +704,11 @@ void GpuFactor::factor_values(const double* d_vals, int B) {
                                                         ftotal_);
     ++launches_;
   };
-  const std::vector<char>* pol = schedule(B, fill);  // settled before any capture
+  const std::vector<char>* pol = persist_ ? nullptr : schedule(B, fill);  // settled before any capture
   launch_cached({1, B, (int64_t)(uintptr_t)d_vals}, [&] {
     fill();
-    run_factor_levels(B, pol);
+    if (persist_) run_factor_persist(B);
+    else run_factor_levels(B, pol);
   });
 }
 
@@ -528,14 +729,15 @@ void GpuFactor::factor_model(int ncomp, const double* d_comp, const double* d_co
                                                             ftotal_);
     ++launches_;
   };
-  const std::vector<char>* pol = schedule(B, fill);  // settled before any capture
+  const std::vector<char>* pol = persist_ ? nullptr : schedule(B, fill);  // settled before any capture
   launch_cached({2, B, ncomp, (int64_t)(uintptr_t)d_comp, (int64_t)(uintptr_t)d_coef, dbits,
                  (int64_t)(uintptr_t)d_pdiag, (int64_t)(uintptr_t)d_cptr, (int64_t)(uintptr_t)d_cobs,
                  (int64_t)(uintptr_t)d_cprod, (int64_t)(uintptr_t)d_w, wstride, nprior, dpbits,
                  (int64_t)(uintptr_t)d_pseg, nseg},
                 [&] {
                   fill();
-                  run_factor_levels(B, pol);
+                  if (persist_) run_factor_persist(B);
+                  else run_factor_levels(B, pol);
                 });
 }
 

@@ -34,6 +34,9 @@ void* device_alloc(size_t bytes);
 void device_free(void* p);
 void device_release_cached();
 
+// Default schedule of the engines built from now on: persistent (true) or level launches.
+void set_persistent_default(bool on);
+
 // Small RAII device buffer.
 template <class T>
 struct DBuf {
@@ -129,6 +132,17 @@ class GpuFactor {
   // Launch sequences whose capture failed and that now run without a graph.
   int64_t capture_failures() const { return capture_failures_; }
 
+  // Persistent schedule (snode_persist.cuh): the whole factorization as one launch. On by
+  // default when the fronts fit its shared-memory budget (INLA_NO_PERSIST=1 keeps the level
+  // launches). After a synchronization point, check_schedule() throws if a dependency wait
+  // of an earlier persistent launch ran out (and clears the record).
+  bool persistent() const { return persist_; }
+  void check_schedule();
+  // Diagnostic: one persistent launch whose dependencies can never complete, with a wait
+  // limit of limit_ms; returns the error code the launch recorded (1: a wait ran out) after
+  // clearing it. The engine stays usable.
+  int persist_wait_limit_selftest(double limit_ms);
+
  private:
   void plan_levels();
   // fuse: per level, 1 = each row CTA factors the diagonal block itself, 0 = one CTA
@@ -138,6 +152,8 @@ class GpuFactor {
   // Per-level panel schedule for batch size B, measured on first use (see gpu_factor.cu).
   const std::vector<char>* schedule(int B, const std::function<void()>& fill);
   void selinv_levels(int B, int slot0);
+  void plan_persist();
+  void run_factor_persist(int B, const int* total_override = nullptr, long long limit_ns = 0);
   template <class Body>
   void launch_cached(const std::vector<int64_t>& key, Body&& body);
 
@@ -169,6 +185,14 @@ class GpuFactor {
   int num_sms_ = 148;
   int64_t ntot_ = 0;              // compact panel entries per problem
   int64_t launches_ = 0;
+  // persistent schedule
+  bool persist_ = false;
+  int persist_smem_ = 0, persist_grid_ = 0, persist_groups_ = 0;
+  long long persist_limit_ns_ = 2000000000LL;
+  DBuf<int> d_pgstart_, d_ptask_, d_ptiny_, d_ptotal_, d_plid_, d_pstate_;  // pstate: err, head, prog[B][ns]
+  DBuf<int64_t> d_pgptr_;
+  DBuf<int2> d_pgrng_;
+  DBuf<double> dcache_p_;
 };
 
 }  // namespace inla

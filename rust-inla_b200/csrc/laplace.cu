@@ -775,6 +775,7 @@ void LaplaceEngine::eval(int B, const double* coef, const double* p1scale, int f
   }
   INLA_CUDA(cudaStreamSynchronize(stream_));
   INLA_CUDA(cudaGetLastError());
+  F_->check_schedule();  // a persistent factorization whose dependency wait ran out is an error
   // expand the shared prior results to every batch member (representatives were
   // evaluated in slots 0..Bp-1)
   {

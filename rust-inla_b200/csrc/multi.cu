@@ -471,6 +471,7 @@ void MultiLaplace::eval(int B, const double* coef, const double* p1scale, int fl
   }
   INLA_CUDA(cudaStreamSynchronize(stream_));
   INLA_CUDA(cudaGetLastError());
+  F_->check_schedule();  // a persistent factorization whose dependency wait ran out is an error
   if (dbg)
     std::fprintf(stderr, "multi eval B=%d G=%d grad=%d var=%d: %.1f ms, active after each Newton iteration:%s\n", B, G,
                  (int)grad, (int)want_var,

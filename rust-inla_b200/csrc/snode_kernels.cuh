@@ -150,11 +150,8 @@ __host__ __device__ constexpr int small_factor_smem(int m) {
 // dense_ld(m)), the children's updates added in fixed order, then the blocked
 // partial LDL^T of the k pivot columns (cta_ldlt).
 template <int NT>
-__global__ void __launch_bounds__(NT) k_factor_small(DevSym S, const int* __restrict__ list,
-                                                     double* __restrict__ F, int64_t fstride) {
-  extern __shared__ double sm[];
-  const int s = list[blockIdx.x];
-  const int b = blockIdx.y;
+__device__ __forceinline__ void factor_small_body(const DevSym& S, int s, int b, double* __restrict__ F,
+                                                  int64_t fstride, double* sm) {
   double* Fb = F + (int64_t)b * fstride;
   const int k = sn_k(S, s), m = sn_m(S, s);
   const int lda = dense_ld(m), uld = dense_uld(m);
@@ -209,6 +206,13 @@ __global__ void __launch_bounds__(NT) k_factor_small(DevSym S, const int* __rest
   }
 }
 
+template <int NT>
+__global__ void __launch_bounds__(NT) k_factor_small(DevSym S, const int* __restrict__ list,
+                                                     double* __restrict__ F, int64_t fstride) {
+  extern __shared__ double sm[];
+  factor_small_body<NT>(S, list[blockIdx.x], blockIdx.y, F, fstride, sm);
+}
+
 // ---------------------------------------------------------------------------
 // tiny fronts (m <= kTinyM rows): one warp per (front, problem), kTinyWarps fronts
 // per CTA. The front is staged in the warp's shared-memory slice (column-major,
@@ -223,19 +227,12 @@ constexpr int kTinyM = 32;
 constexpr int kTinyWarps = 4;
 constexpr int kTinyLd = kTinyM + 1;
 
-__global__ void __launch_bounds__(32 * kTinyWarps) k_factor_tiny(DevSym S, const int* __restrict__ list, int nlist,
-                                                                 double* __restrict__ F, int64_t fstride) {
-  __shared__ double sA[kTinyWarps][kTinyM * kTinyLd];
-  __shared__ double sU[kTinyWarps][kTinyM];
-  __shared__ int sR[kTinyWarps][kTinyM];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int idx = blockIdx.x * kTinyWarps + warp;
-  if (idx >= nlist) return;  // the whole warp leaves; only warp-level synchronization follows
-  const int s = list[idx], b = blockIdx.y;
+// One warp: front s of problem b in the warp's shared slices A [kTinyM x kTinyLd], U [kTinyM]
+// and R [kTinyM] (ints). Only warp-level synchronization inside.
+__device__ __forceinline__ void factor_tiny_warp(const DevSym& S, int s, int b, double* __restrict__ F,
+                                                 int64_t fstride, double* A, double* U, int* R) {
+  const int lane = threadIdx.x & 31;
   double* Fb = F + (int64_t)b * fstride;
-  double* A = sA[warp];
-  double* U = sU[warp];
-  int* R = sR[warp];
   const int k = sn_k(S, s), m = sn_m(S, s);
   double* Fs = Fb + S.fptr[s];
   const int mm = m * m;
@@ -273,6 +270,17 @@ __global__ void __launch_bounds__(32 * kTinyWarps) k_factor_tiny(DevSym S, const
     const int col = e / m, row = e - col * m;
     if (col < k || row >= col) Fs[e] = A[row + col * kTinyLd];
   }
+}
+
+__global__ void __launch_bounds__(32 * kTinyWarps) k_factor_tiny(DevSym S, const int* __restrict__ list, int nlist,
+                                                                 double* __restrict__ F, int64_t fstride) {
+  __shared__ double sA[kTinyWarps][kTinyM * kTinyLd];
+  __shared__ double sU[kTinyWarps][kTinyM];
+  __shared__ int sR[kTinyWarps][kTinyM];
+  const int warp = threadIdx.x >> 5;
+  const int idx = blockIdx.x * kTinyWarps + warp;
+  if (idx >= nlist) return;  // the whole warp leaves; only warp-level synchronization follows
+  factor_tiny_warp(S, list[idx], blockIdx.y, F, fstride, sA[warp], sU[warp], sR[warp]);
 }
 
 // ---------------------------------------------------------------------------
@@ -468,7 +476,8 @@ constexpr int kLogdetChunk = 2048;  // 256 threads x 8 pivots
 __global__ void __launch_bounds__(256) k_logdet_chunks(DevSym S, const double* __restrict__ F, int64_t fstride,
                                                        double* __restrict__ part, int* __restrict__ pflag,
                                                        unsigned* __restrict__ ticket, double* __restrict__ logdet,
-                                                       int* __restrict__ status) {
+                                                       int* __restrict__ status,
+                                                       const int* __restrict__ sched_err = nullptr) {
   __shared__ double red[256];
   __shared__ int bad[256];
   __shared__ bool last;
@@ -526,7 +535,7 @@ __global__ void __launch_bounds__(256) k_logdet_chunks(DevSym S, const double* _
   }
   if (threadIdx.x == 0) {
     logdet[b] = red[0];
-    status[b] = bad[0];
+    status[b] = bad[0] | ((sched_err && __ldcg(sched_err) != 0) ? kStatusSchedule : 0);
     ticket[b] = 0u;
   }
 }

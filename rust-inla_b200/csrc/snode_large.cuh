@@ -54,13 +54,12 @@ __device__ __forceinline__ const double* linv_block(const DevSym& S, const doubl
 // part is written back once. Work per child is flattened over (source column,
 // row) pairs with eight independent loads in flight per thread.
 constexpr int kGatherCols = 8;
-__global__ void __launch_bounds__(256) k_gather8(DevSym S, const int* __restrict__ list, double* __restrict__ F,
-                                                 int64_t fstride, int gcols, const int64_t* __restrict__ gptr,
-                                                 const int2* __restrict__ grng) {
-  extern __shared__ double gsl[];  // [gcols][m] column slice
-  const int s = list[blockIdx.x], b = blockIdx.y;
+// Chunk z of front s, problem b (any block size; gsl: [gcols][m] doubles of shared memory).
+__device__ __forceinline__ void gather8_body(const DevSym& S, int s, int b, int z, double* __restrict__ F,
+                                             int64_t fstride, int gcols, const int64_t* __restrict__ gptr,
+                                             const int2* __restrict__ grng, double* gsl) {
   const int k = lg_k(S, s), m = lg_m(S, s);
-  const int c0 = blockIdx.z * gcols;
+  const int c0 = z * gcols;
   if (c0 >= m) return;
   const int c1 = min(c0 + gcols, m), nc = c1 - c0;
   double* Fb = F + (int64_t)b * fstride;
@@ -75,7 +74,7 @@ __global__ void __launch_bounds__(256) k_gather8(DevSym S, const int* __restrict
   __syncthreads();
   const int q0 = S.child_ptr[s], nch = S.child_ptr[s + 1] - q0;
   // source-column range of every child for this chunk (host table, no search)
-  const int2* rng = grng + gptr[s] + (int64_t)blockIdx.z * nch;
+  const int2* rng = grng + gptr[s] + (int64_t)z * nch;
   for (int qi = 0; qi < nch; ++qi) {
     const int c = S.child_list[q0 + qi];
     const int kc = lg_k(S, c), mc = lg_m(S, c), rc = mc - kc;
@@ -110,6 +109,13 @@ __global__ void __launch_bounds__(256) k_gather8(DevSym S, const int* __restrict
     const int cc = e / m, row = e - cc * m, col = c0 + cc;
     if (row >= col) Fs[row + (int64_t)col * m] = gsl[e];
   }
+}
+
+__global__ void __launch_bounds__(256) k_gather8(DevSym S, const int* __restrict__ list, double* __restrict__ F,
+                                                 int64_t fstride, int gcols, const int64_t* __restrict__ gptr,
+                                                 const int2* __restrict__ grng) {
+  extern __shared__ double gsl[];  // [gcols][m] column slice
+  gather8_body(S, list[blockIdx.x], blockIdx.y, blockIdx.z, F, fstride, gcols, gptr, grng, gsl);
 }
 
 // Sigma restricted to the below-rows of s, gathered from the parent's Sigma
@@ -162,21 +168,21 @@ __global__ void __launch_bounds__(256) k_si_gather8(DevSym S, const int* __restr
 // X = F_rows (L_JJ^-T D^-1) as one tensor-core GEMM. The row sub-blocks are
 // staged in the diagonal block's buffer once it is no longer needed, which
 // keeps the CTA at 84 KB of shared memory (two CTAs per SM).
-__global__ void __launch_bounds__(256) k_panel64(DevSym S, const int* __restrict__ list, int j0, int rpc,
-                                                 double* __restrict__ F, int64_t fstride,
-                                                 double* __restrict__ dcache, double* __restrict__ linv) {
-  extern __shared__ double smem64[];
+// Block J = [j0, j0 + 64) of front s, problem b, row CTA z (256 threads). dc: this front's and
+// problem's slot of the factored-diagonal-block cache (written when z == 0).
+__device__ __forceinline__ void panel64_body(const DevSym& S, int s, int b, int z, int j0, int rpc,
+                                             double* __restrict__ F, int64_t fstride, double* __restrict__ dc,
+                                             double* __restrict__ linv, double* smem64) {
   constexpr int ld = kLd64;
   double* Ds = smem64;         // [64 cols][ld]: diagonal block, factored in place; then row sub-blocks
   double* Li = Ds + kB64 * ld; // L_JJ^-1, then Bm[u + t*ld] = Li[t][u] / d_t
   double* U = Li + kB64 * ld;  // [16][kULd64] scratch of cta_ldlt, then 1 / d_t
   double* ws = U + 16 * kULd64;
-  const int s = list[blockIdx.x], b = blockIdx.y;
   const int k = lg_k(S, s), m = lg_m(S, s);
   if (j0 >= k) return;
   const int w = min(kB64, k - j0);
-  const int r0 = j0 + w + blockIdx.z * rpc;
-  if (blockIdx.z > 0 && r0 >= m) return;
+  const int r0 = j0 + w + z * rpc;
+  if (z > 0 && r0 >= m) return;
   const int r1 = min(m, r0 + rpc);
   double* Fs = F + (int64_t)b * fstride + S.fptr[s];
   const double* D0 = Fs + j0 + (int64_t)j0 * m;
@@ -190,8 +196,7 @@ __global__ void __launch_bounds__(256) k_panel64(DevSym S, const int* __restrict
   cp_async_wait<0>();
   __syncthreads();
   cta_ldlt<true>(Ds, ld, w, w, Li, ld, U, kULd64, ws);
-  if (blockIdx.z == 0) {
-    double* dc = dcache + ((int64_t)blockIdx.x * gridDim.y + b) * (kB64 * kB64);
+  if (z == 0) {
     double* lc = const_cast<double*>(linv_block(S, linv, b, s, j0 / kB64));
     for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) {
       const int c = e >> 6, r = e & 63;
@@ -261,25 +266,32 @@ __global__ void __launch_bounds__(256) k_panel64(DevSym S, const int* __restrict
   }
 }
 
+__global__ void __launch_bounds__(256) k_panel64(DevSym S, const int* __restrict__ list, int j0, int rpc,
+                                                 double* __restrict__ F, int64_t fstride,
+                                                 double* __restrict__ dcache, double* __restrict__ linv) {
+  extern __shared__ double smem64[];
+  double* dc = dcache + ((int64_t)blockIdx.x * gridDim.y + blockIdx.y) * (kB64 * kB64);
+  panel64_body(S, list[blockIdx.x], blockIdx.y, blockIdx.z, j0, rpc, F, fstride, dc, linv, smem64);
+}
+
 // Rows of a 64-column block from this step's factored diagonal block (dcache:
 // L_JJ with D on the diagonal, written by k_panel64 launched with rpc = 0;
 // linv: L_JJ^-1): X = F_rows L_JJ^-T D^-1 for the 64 rows of CTA z, one
 // tensor-core GEMM. Used when many fronts x problems share a step, where a
 // factorization per row CTA would be redundant work.
-constexpr int kRowsSmem = 2 * kB64 * kLd64 * 8;
-__global__ void __launch_bounds__(256) k_rows64(DevSym S, const int* __restrict__ list, int j0,
-                                                double* __restrict__ F, int64_t fstride,
-                                                const double* __restrict__ dcache, const double* __restrict__ linv) {
-  extern __shared__ double smr[];
+constexpr int kRowsSmem = (2 * kB64 * kLd64 + kB64) * 8;
+// Row block z of block J of front s, problem b (256 threads); dc as in panel64_body.
+__device__ __forceinline__ void rows64_body(const DevSym& S, int s, int b, int z, int j0, double* __restrict__ F,
+                                            int64_t fstride, const double* __restrict__ dc,
+                                            const double* __restrict__ linv, double* smr) {
   constexpr int ld = kLd64;
-  double* Bm = smr;             // Bm[u + t*ld] = L_JJ^-1[t][u] / d_t
-  double* Fa = Bm + kB64 * ld;  // Fa[t*ld + r] = F[r0 + r, j0 + t]
-  __shared__ double dinv[kB64];
-  const int s = list[blockIdx.x], b = blockIdx.y;
+  double* Bm = smr;               // Bm[u + t*ld] = L_JJ^-1[t][u] / d_t
+  double* Fa = Bm + kB64 * ld;    // Fa[t*ld + r] = F[r0 + r, j0 + t]
+  double* dinv = Fa + kB64 * ld;  // [kB64]
   const int k = lg_k(S, s), m = lg_m(S, s);
   if (j0 >= k) return;
   const int w = min(kB64, k - j0);
-  const int r0 = j0 + w + blockIdx.z * kPanelRows;
+  const int r0 = j0 + w + z * kPanelRows;
   if (r0 >= m) return;
   const int rows = min(kPanelRows, m - r0);
   double* Fs = F + (int64_t)b * fstride + S.fptr[s];
@@ -289,7 +301,6 @@ __global__ void __launch_bounds__(256) k_rows64(DevSym S, const int* __restrict_
     else Fa[c * ld + r] = 0.0;
   }
   cp_async_commit();
-  const double* dc = dcache + ((int64_t)blockIdx.x * gridDim.y + b) * (kB64 * kB64);
   const double* lc = linv_block(S, linv, b, s, j0 / kB64);
   if (threadIdx.x < kB64) dinv[threadIdx.x] = threadIdx.x < w ? 1.0 / dc[threadIdx.x * (kB64 + 1)] : 0.0;
   __syncthreads();
@@ -333,6 +344,14 @@ __global__ void __launch_bounds__(256) k_rows64(DevSym S, const int* __restrict_
         const int r = wr + a * 8 + g, t = wc + q * 8 + tg * 2 + h;
         if (r < rows && t < w) Fs[(r0 + r) + (int64_t)(j0 + t) * m] = acc[a][q][h];
       }
+}
+
+__global__ void __launch_bounds__(256) k_rows64(DevSym S, const int* __restrict__ list, int j0,
+                                                double* __restrict__ F, int64_t fstride,
+                                                const double* __restrict__ dcache, const double* __restrict__ linv) {
+  extern __shared__ double smr[];
+  const double* dc = dcache + ((int64_t)blockIdx.x * gridDim.y + blockIdx.y) * (kB64 * kB64);
+  rows64_body(S, list[blockIdx.x], blockIdx.y, blockIdx.z, j0, F, fstride, dc, linv, smr);
 }
 
 constexpr int kUT64 = 64;
