@@ -428,6 +428,9 @@ def run_ours(args, ws, rank, local, dist):
                          f"in {el:.1f}s, {threads} threads, minimum-degree order; {CPU_KIND_NOTE}"}
 
     fit_s = ms_total * 1e-3 / args.steps
+    # where one fit's time goes (host wall clock per phase, averaged over the timed fits)
+    phases = {k: sum(f["phase_s"][k] for f in fits) / len(fits) for k in fits[0]["phase_s"]}
+    phases["host_between_phases"] = sum(f["seconds"] for f in fits) / len(fits) - sum(phases.values())
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -435,7 +438,8 @@ def run_ours(args, ws, rank, local, dist):
             "config": bench_config(p, args, ws),
             "method": "batched Newton on adjoint gradients (FD-of-gradient Hessian), full step first with "
                       "half / quarter steps on failure; FD Hessian and CCD nodes in one batch each",
-            "fit_s": fit_s, "theta_evals_per_fit": evals / args.steps, "mode": last["mode"].tolist(),
+            "fit_s": fit_s, "fit_breakdown_s": phases, "theta_evals_per_fit": evals / args.steps,
+            "mode": last["mode"].tolist(),
             "plain_gpu": plain,
             "speedup_vs_plain_gpu": (plain["fit_s"] / fit_s) if plain else None,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),

@@ -424,6 +424,10 @@ int inla_fit(inla_laplace* h, int m, const double* theta0, inla_theta_map_fn map
  * (predictor_means / predictor_variances of the reference's result, inference.rs:1451-1466),
  * length nobs each (either pointer may be NULL). INLA_ERR_INVALID before the first fit. */
 int inla_fit_predictor(inla_laplace* h, double* pred_mean, double* pred_var);
+/* Wall seconds of the phases of the last inla_fit on h (no reference counterpart): out4 =
+ * {mode search, Hessian, integration design + node evaluations, aggregation}; they add up to
+ * info[1] of inla_fit up to the host bookkeeping between them. */
+int inla_fit_phase_seconds(inla_laplace* h, double* out4);
 
 /* Model-selection criteria of the last inla_fit on h, as the reference computes them at the
  * end of a fit (inference.rs:1470-1514; model_selection.rs): DIC (compute_dic, 101-150) and

@@ -26,6 +26,7 @@ struct inla_laplace {
   int mode_index = 0, m = 0;
   double p1scale_mode = 1.0, mlik_gaussian = 0.0;
   bool fitted = false;
+  double phase_s[4] = {0.0, 0.0, 0.0, 0.0};
   // device copies of cond_eta / cond_eta_var: the criteria of the fit are computed on the device
   DBuf<double> d_cond_eta, d_cond_eta_var;
   AggScratch agg;
@@ -357,11 +358,18 @@ int inla_fit(inla_laplace* h, int m, const double* theta0, inla_theta_map_fn map
     h->mode_index = R.mode_index;
     h->p1scale_mode = R.p1scale_mode;
     h->mlik_gaussian = R.mlik_gaussian;
+    std::memcpy(h->phase_s, R.phase_s, sizeof(h->phase_s));
     h->fitted = true;
     return INLA_OK;
   } catch (...) {
     return map_exception();
   }
+}
+
+int inla_fit_phase_seconds(inla_laplace* h, double* out4) {
+  if (!h || !h->fitted || !out4) return fail(INLA_ERR_INVALID, "inla_fit_phase_seconds: no fit on this handle");
+  std::memcpy(out4, h->phase_s, sizeof(h->phase_s));
+  return INLA_OK;
 }
 
 int inla_fit_predictor(inla_laplace* h, double* pred_mean, double* pred_var) {

@@ -654,6 +654,9 @@ void InlaDriver::fit(const double* theta0, const FitOptions& opt, FitResult& out
     out.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return;
   }
+  auto since = [](std::chrono::steady_clock::time_point a) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - a).count();
+  };
   std::vector<double> mode(theta0, theta0 + m);
   int iters = 0;
   if (opt.mode_search == 0) nelder_mead(mode, opt, iters);
@@ -661,11 +664,15 @@ void InlaDriver::fit(const double* theta0, const FitOptions& opt, FitResult& out
   else newton(mode, opt, iters);
   out.mode = mode;
   out.mode_iters = iters;
+  out.phase_s[0] = since(t0);
+  const auto t1 = std::chrono::steady_clock::now();
 
   double hh = 1e-4;  // inference.rs:1264
   for (double t : mode) hh = std::max(hh, 0.05 * std::fabs(t));
   if (opt.hessian == 0) fd_hessian(mode, hh, opt.batched != 0, out.hessian);
   else grad_hessian(mode, hh, opt.batched != 0, out.hessian);
+  out.phase_s[1] = since(t1);
+  const auto t2 = std::chrono::steady_clock::now();
 
   std::vector<double> neg(m * m), sigma;
   for (int i = 0; i < m * m; ++i) neg[i] = -out.hessian[i];
@@ -768,6 +775,8 @@ void InlaDriver::fit(const double* theta0, const FitOptions& opt, FitResult& out
     INLA_CUDA(cudaMemcpyAsync(means.data(), d_means.p, sizeof(double) * K * n, cudaMemcpyDeviceToHost, eng_.stream()));
     INLA_CUDA(cudaMemcpyAsync(vars.data(), d_vars.p, sizeof(double) * K * n, cudaMemcpyDeviceToHost, eng_.stream()));
   }
+  out.phase_s[2] = since(t2);  // design + node evaluations (the host copy of the node results included)
+  const auto t3 = std::chrono::steady_clock::now();
   double mx = -std::numeric_limits<double>::infinity();
   for (double v : lp) mx = std::max(mx, v);
   if (!std::isfinite(mx)) throw std::runtime_error("Newton-Raphson did not converge at any integration node");
@@ -842,6 +851,7 @@ void InlaDriver::fit(const double* theta0, const FitOptions& opt, FitResult& out
   out.node_logpost = lp;
   out.n_evals = n_evals_;
   out.n_batches = n_batches_;
+  out.phase_s[3] = since(t3);
   out.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 

@@ -56,6 +56,10 @@ struct FitResult {
   double mlik = 0.0;
   int n_evals = 0, n_batches = 0, mode_iters = 0;
   double seconds = 0.0;
+  // wall seconds of the fit's phases: mode search, Hessian, integration design + node
+  // evaluations, aggregation (mixture, predictor, model-selection inputs); they add up to
+  // `seconds` up to the host bookkeeping between them
+  double phase_s[4] = {0.0, 0.0, 0.0, 0.0};
 };
 
 class InlaDriver {

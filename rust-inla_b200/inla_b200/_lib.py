@@ -114,6 +114,7 @@ SIGNATURES = [
     ("inla_log_prior_set", C.c_double, [DP, C.c_int, DP, P]),
     ("inla_fit", C.c_int, [P, C.c_int, DP, P, P, P, P, DP, DP, DP, DP, DP, DP, DP]),
     ("inla_fit_predictor", C.c_int, [P, DP, DP]),
+    ("inla_fit_phase_seconds", C.c_int, [P, DP]),
     ("inla_scale_model", C.c_int, [I64, LP, LP, DP, C.c_int, DP, C.c_int, DP, DP, DP]),
     ("inla_mesh_create", C.c_int, [I64, DP, I64, LP, C.POINTER(P)]),
     ("inla_mesh_free", None, [P]),

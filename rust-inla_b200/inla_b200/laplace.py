@@ -256,7 +256,10 @@ class LaplaceModel:
         pm = np.zeros(self.nobs)
         pv = np.zeros(self.nobs)
         check(lib().inla_fit_predictor(self._h, dptr(pm), dptr(pv)))
-        return {"mode": mode, "hessian": hess, "mean": mean, "var": var, "node_theta": nth[:k], "node_weight": nw[:k],
+        phases = np.zeros(4)
+        check(lib().inla_fit_phase_seconds(self._h, dptr(phases)))
+        return {"phase_s": dict(zip(["mode_search", "hessian", "nodes", "aggregation"], phases.tolist())),
+                "mode": mode, "hessian": hess, "mean": mean, "var": var, "node_theta": nth[:k], "node_weight": nw[:k],
                 "mlik": info[0], "seconds": info[1], "n_evals": int(info[2]), "n_batches": int(info[3]),
                 "mode_iters": int(info[4]), "pred_mean": pm, "pred_var": pv}
 
