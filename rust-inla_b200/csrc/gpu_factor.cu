@@ -460,7 +460,13 @@ void GpuFactor::plan_persist() {
   persist_ = true;
 }
 
-void GpuFactor::run_factor_persist(int B, const int* total_override, long long limit_ns) {
+void GpuFactor::set_front_groups(const std::vector<int>& fseg) {
+  if ((int64_t)fseg.size() != sym_.nsuper) throw std::runtime_error("one group per front expected");
+  d_fseg_.upload(fseg, stream_);
+}
+
+void GpuFactor::run_factor_persist(int B, const int* total_override, long long limit_ns,
+                                   const unsigned char* active, int nseg) {
   const int ns = (int)sym_.nsuper;
   // head and the completion counts start at zero; the error record (word 0) stays until read
   INLA_CUDA(cudaMemsetAsync(d_pstate_.p + 1, 0, sizeof(int) * (1 + (size_t)B * ns), stream_));
@@ -483,6 +489,9 @@ void GpuFactor::run_factor_persist(int B, const int* total_override, long long l
   a.gptr = d_pgptr_.p;
   a.grng = d_pgrng_.p;
   a.limit_ns = limit_ns > 0 ? limit_ns : persist_limit_ns_;
+  a.active = active;
+  a.fseg = d_fseg_.p;
+  a.nseg = nseg;
   k_factor_persist<<<persist_grid_, kPersistThreads, persist_smem_, stream_>>>(a);
   k_logdet_chunks<<<dim3(nldchunk_, B), 256, 0, stream_>>>(ds_, F_.p, ftotal_, ldpart_.p, ldflag_.p, ldticket_.p,
                                                            logdet_.p, status_.p, d_pstate_.p);
@@ -715,28 +724,29 @@ void GpuFactor::factor_values(const double* d_vals, int B) {
 void GpuFactor::factor_model(int ncomp, const double* d_comp, const double* d_coef, double diag_add,
                              const unsigned char* d_pdiag, const int* d_cptr, const int* d_cobs,
                              const double* d_cprod, const double* d_w, int64_t wstride, int B, int nprior,
-                             double diag_add_post, const int* d_pseg, int nseg) {
+                             double diag_add_post, const int* d_pseg, int nseg, const unsigned char* d_active) {
   if (B < 1 || B > max_batch_) throw std::runtime_error("batch size out of range");
   if (nprior < 0 || nprior > B) throw std::runtime_error("prior count out of range");
   if (ncomp < 1 || ncomp > 8) throw std::runtime_error("1..8 precision components supported");
   int64_t dbits, dpbits;
   std::memcpy(&dbits, &diag_add, sizeof(dbits));
   std::memcpy(&dpbits, &diag_add_post, sizeof(dpbits));
+  if (!can_skip_groups()) d_active = nullptr;  // the level launches factorize every pair
   auto fill = [&] {
     k_fill_panels_model<<<dim3(nfillm_), 256, 0, stream_>>>(ds_, d_csnm_.p, ntot_, d_pmap_.p, ncomp, d_comp, nnz_,
                                                             d_coef, diag_add, d_pdiag, d_cptr, d_cobs, d_cprod, d_w,
                                                             wstride, B, nprior, diag_add_post, d_pseg, nseg, F_.p,
-                                                            ftotal_);
+                                                            ftotal_, d_fseg_.p, d_active);
     ++launches_;
   };
   const std::vector<char>* pol = persist_ ? nullptr : schedule(B, fill);  // settled before any capture
   launch_cached({2, B, ncomp, (int64_t)(uintptr_t)d_comp, (int64_t)(uintptr_t)d_coef, dbits,
                  (int64_t)(uintptr_t)d_pdiag, (int64_t)(uintptr_t)d_cptr, (int64_t)(uintptr_t)d_cobs,
                  (int64_t)(uintptr_t)d_cprod, (int64_t)(uintptr_t)d_w, wstride, nprior, dpbits,
-                 (int64_t)(uintptr_t)d_pseg, nseg},
+                 (int64_t)(uintptr_t)d_pseg, nseg, (int64_t)(uintptr_t)d_active},
                 [&] {
                   fill();
-                  if (persist_) run_factor_persist(B);
+                  if (persist_) run_factor_persist(B, nullptr, 0, d_active, nseg);
                   else run_factor_levels(B, pol);
                 });
 }

@@ -102,7 +102,12 @@ class GpuFactor {
   void factor_model(int ncomp, const double* d_comp, const double* d_coef, double diag_add,
                     const unsigned char* d_pdiag, const int* d_cptr, const int* d_cobs, const double* d_cprod,
                     const double* d_w, int64_t wstride, int B, int nprior = 0, double diag_add_post = 0.0,
-                    const int* d_pseg = nullptr, int nseg = 1);
+                    const int* d_pseg = nullptr, int nseg = 1, const unsigned char* d_active = nullptr);
+  // Model of every front when the pattern holds independent models block-diagonally: lets
+  // factor_model skip the fronts of inactive (problem, model) pairs (d_active [B][nseg]),
+  // which then keep their previous factor. Honoured by the persistent schedule only.
+  void set_front_groups(const std::vector<int>& fseg);
+  bool can_skip_groups() const { return persist_ && d_fseg_.p != nullptr; }
   // Device view of the symbolic analysis (pivot offsets, permutation, ...).
   const DevSym& dev_sym() const { return ds_; }
   // Front offset of every input entry's lower twin (both triangles), for
@@ -153,7 +158,8 @@ class GpuFactor {
   const std::vector<char>* schedule(int B, const std::function<void()>& fill);
   void selinv_levels(int B, int slot0);
   void plan_persist();
-  void run_factor_persist(int B, const int* total_override = nullptr, long long limit_ns = 0);
+  void run_factor_persist(int B, const int* total_override = nullptr, long long limit_ns = 0,
+                          const unsigned char* active = nullptr, int nseg = 1);
   template <class Body>
   void launch_cached(const std::vector<int64_t>& key, Body&& body);
 
@@ -193,6 +199,7 @@ class GpuFactor {
   DBuf<int64_t> d_pgptr_;
   DBuf<int2> d_pgrng_;
   DBuf<double> dcache_p_;
+  DBuf<int> d_fseg_;
 };
 
 }  // namespace inla

@@ -129,6 +129,12 @@ MultiLaplace::MultiLaplace(const MultiSpec& spec, int max_batch, cudaStream_t st
   std::vector<int64_t> eoff(G + 1);
   for (int g = 0; g <= G; ++g) eoff[g] = spec_.colptr[spec_.lat_off[g]];
   F_.reset(new GpuFactor(sym, max_batch, stream_));
+  {  // the model of every front, so that converged (theta-set, model) pairs can be skipped
+    std::vector<int> fseg(sym.nsuper);
+    for (int64_t sn = 0; sn < sym.nsuper; ++sn) fseg[sn] = segc[sym.perm[sym.sn_first[sn]]];
+    F_->set_front_groups(fseg);
+  }
+  active_.alloc((size_t)max_batch * G);
 
   // observation structures: contributions of A^T diag(w) A on the pattern, A^T, row pairs
   auto find = [&](int64_t row, int64_t col) -> int64_t {
@@ -262,10 +268,11 @@ void MultiLaplace::eval_lik(int B, const double* d_xsrc) {
 
 // prior (Q + 1e-12 I, inference.rs:831-837) or posterior (Q + A^T W A) factorization of
 // B theta-sets, then the per-model log-determinants and pivot gates
-void MultiLaplace::factor(int B, bool posterior) {
+void MultiLaplace::factor(int B, bool posterior, bool skip) {
   const int G = spec_.G;
   F_->factor_model(spec_.ncomp, comp_.p, coef_.p, posterior ? 0.0 : 1e-12, pdiag_.p, cptr_.p, cobs_.p, cprod_.p,
-                   posterior ? w_.p : nullptr, spec_.nobs, B, posterior ? 0 : B, 0.0, pseg_.p, G);
+                   posterior ? w_.p : nullptr, spec_.nobs, B, posterior ? 0 : B, 0.0, pseg_.p, G,
+                   posterior && skip ? active_.p : nullptr);
   const size_t o = posterior ? (size_t)max_batch_ * G : 0;
   k_seg_logdet<256><<<dim3(G, B), 256, 0, stream_>>>(F_->dev_sym(), F_->d_front(), F_->front_total(), poff_.p, G,
                                                      ld_.p + o, st_.p + o);
@@ -319,9 +326,13 @@ void MultiLaplace::eval(int B, const double* coef, const double* p1scale, int fl
   INLA_CUDA(cudaMemsetAsync(x_.p, 0, sizeof(double) * B * n, stream_));
   std::vector<double> st(2 * BG), mdiff(BG);
   std::vector<int> bad(BG), pst(BG);
+  // Newton systems after the first factorize only the pairs still iterating; a converged pair
+  // keeps its last factor (its step is not taken: alpha = 0)
+  static const bool no_skip = std::getenv("INLA_NO_PAIR_SKIP") != nullptr;
+  bool skip_next = false;
   auto newton_system = [&](const double* d_x) {
     eval_lik(B, d_x);
-    factor(B, true);
+    factor(B, true, skip_next && !no_skip);
     k_mnewton_rhs<<<dim3(GN, B), 256, 0, stream_>>>((int)n, T, G, segc_.p, qcp_.p, qri_.p, comp_.p, nnz_, coef_.p,
                                                     atp_.p, ati_.p, atv_.p, nobs, grad_.p, d_x, step_.p);
     F_->solve(step_.p, n, B);
@@ -412,6 +423,13 @@ void MultiLaplace::eval(int B, const double* coef, const double* p1scale, int fl
       }
       if (dbg) trace += " " + std::to_string(nleft);
       if (!left) break;
+      if (F_->can_skip_groups()) {
+        std::vector<unsigned char> act(BG);
+        for (size_t q = 0; q < BG; ++q) act[q] = active[q] ? 1 : 0;
+        INLA_CUDA(cudaMemcpyAsync(active_.p, act.data(), BG, cudaMemcpyHostToDevice, stream_));
+        INLA_CUDA(cudaStreamSynchronize(stream_));  // `act` is released at the end of this block
+        skip_next = true;
+      }
     }
     for (size_t q = 0; q < BG; ++q)
       if (active[q] && R.status[q] == LAP_OK) R.status[q] = LAP_NONCONVERGED;

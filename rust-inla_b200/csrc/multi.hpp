@@ -66,7 +66,8 @@ class MultiLaplace {
 
  private:
   void eval_lik(int B, const double* d_xsrc);
-  void factor(int B, bool posterior);
+  // posterior with `skip`: the pairs whose mask entry (active_, [B][G]) is 0 keep their factor
+  void factor(int B, bool posterior, bool skip = false);
 
   MultiSpec spec_;
   int max_batch_;
@@ -76,7 +77,7 @@ class MultiLaplace {
   DBuf<double> comp_, y_, p1_, p2_, av_, atv_, cprod_;
   DBuf<int64_t> qcp_, acp_, atp_, opptr_, oppos_, latoff_, obsoff_, poff_, eoff_;
   DBuf<int> qri_, aci_, ati_, cptr_, cobs_, segc_, sego_, pseg_;
-  DBuf<unsigned char> pdiag_;
+  DBuf<unsigned char> pdiag_, active_;
   DBuf<double> coef_, p1s_, x_, xt_, step_, eta_, logp_, grad_, w_, dw_, var_, sig_, tmp_n_, tmp_o_, stats_, alpha_,
       mdiff_, scal_, ld_, red_;
   DBuf<int> bad_, st_;

@@ -97,7 +97,9 @@ __global__ void __launch_bounds__(256) k_fill_panels_model(DevSym S, const int* 
                                                            const double* __restrict__ w, int64_t wstride, int B,
                                                            int nprior, double diag_add_post,
                                                            const int* __restrict__ pseg, int nseg,
-                                                           double* __restrict__ F, int64_t fstride) {
+                                                           double* __restrict__ F, int64_t fstride,
+                                                           const int* __restrict__ fseg = nullptr,
+                                                           const unsigned char* __restrict__ active = nullptr) {
   const int lo = csn[blockIdx.x], hi = csn[blockIdx.x + 1];
 #pragma unroll
   for (int u = 0; u < 2; ++u) {
@@ -106,8 +108,12 @@ __global__ void __launch_bounds__(256) k_fill_panels_model(DevSym S, const int* 
     const int s = fill_find(S, lo, hi, e);
     const int p = pmap[e];
     const int64_t dst = S.fptr[s] + (e - S.lptr[s]);
+    // with `active` ([B][nseg]), the fronts of inactive (problem, model) pairs keep their
+    // last factor: they are neither filled nor factorized
+    const int fs = active ? fseg[s] : 0;
     if (p < 0) {
-      for (int b = 0; b < B; ++b) F[(int64_t)b * fstride + dst] = 0.0;
+      for (int b = 0; b < B; ++b)
+        if (!active || active[(int64_t)b * nseg + fs]) F[(int64_t)b * fstride + dst] = 0.0;
       continue;
     }
     double cv[8];
@@ -117,6 +123,7 @@ __global__ void __launch_bounds__(256) k_fill_panels_model(DevSym S, const int* 
     const int q0 = cptr[p], q1 = cptr[p + 1];
     const int sg = pseg ? pseg[p] : 0;
     for (int b = 0; b < B; ++b) {
+      if (active && !active[(int64_t)b * nseg + fs]) continue;
       const double* cb = coef + ((int64_t)b * nseg + sg) * ncomp;
       double v = isdiag ? (b < nprior ? diag_add : diag_add_post) : 0.0;
 #pragma unroll

@@ -65,6 +65,11 @@ struct PersistArgs {
   const int64_t* gptr;      // extend-add chunk table of this schedule
   const int2* grng;
   long long limit_ns;       // longest wait for one dependency
+  // optional: fronts of inactive (problem, model) pairs are skipped (counted done, left as
+  // they are); active [B][nseg], fseg [ns] the model of each front
+  const unsigned char* active;
+  const int* fseg;
+  int nseg;
 };
 
 constexpr int kPersistThreads = 256;
@@ -239,10 +244,12 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_factor_persist(PersistAr
     }
     __syncthreads();
     if (!sh_go) break;
-    switch (T.type) {
+    const bool skip = a.active && T.type != PT_TINY && !a.active[(int64_t)b * a.nseg + a.fseg[T.s]];
+    if (!skip) switch (T.type) {
       case PT_TINY: {
         const int warp = threadIdx.x >> 5;
-        if (warp < T.sub) {
+        if (warp < T.sub &&
+            (!a.active || a.active[(int64_t)b * a.nseg + a.fseg[a.tiny_list[T.s + warp]]])) {
           double* A = psm + warp * kPersistTinySlice;
           factor_tiny_warp(S, a.tiny_list[T.s + warp], b, a.F, a.fstride, A, A + kTinyM * kTinyLd,
                            reinterpret_cast<int*>(A + kTinyM * kTinyLd + kTinyM));
