@@ -302,7 +302,9 @@ void GpuFactor::plan_levels() {
         P.kmax_large = std::max(P.kmax_large, k);
         P.mmax_large = std::max(P.mmax_large, m);
       }
-      if (m <= kSiSmall) {
+      if (tiny_on && m <= kTinyM) {
+        P.si_tiny.push_back(s);
+      } else if (m <= kSiSmall) {
         P.si_small.push_back(s);
         P.mmax_si_small = std::max(P.mmax_si_small, m);
         P.kmax_si_small = std::max(P.kmax_si_small, k);
@@ -324,6 +326,7 @@ void GpuFactor::plan_levels() {
     P.off_large = put(P.large);
     P.off_all = put(P.all);
     P.off_nontiny = put(P.nontiny);
+    P.off_si_tiny = put(P.si_tiny);
     P.off_si_small = put(P.si_small);
     P.off_si_large = put(P.si_large);
   }
@@ -806,6 +809,12 @@ void GpuFactor::selinv_levels(int B, int slot0) {
   const double* Lp = linv_.p + (int64_t)slot0 * ds_.lstride;
   for (int l = (int)levels_.size() - 1; l >= 0; --l) {
     const LevelPlan& P = levels_[l];
+    if (!P.si_tiny.empty()) {
+      const int nt = (int)P.si_tiny.size();
+      k_selinv_tiny<<<dim3(cdiv(nt, kTinySiWarps), B), 32 * kTinySiWarps, 0, stream_>>>(
+          ds_, d_lists_.p + P.off_si_tiny, nt, Fp, Sp, fs);
+      ++launches_;
+    }
     if (!P.si_small.empty()) {
       int mm = P.mmax_si_small;
       k_selinv_small<256><<<dim3((unsigned)P.si_small.size(), B), 256, small_selinv_smem(mm, P.kmax_si_small),

@@ -71,8 +71,8 @@ struct LevelPlan {
   int mmax_nontiny = 0;
   int mmax_a = 0, mmax_b = 0, mmax_all = 0, kmax_large = 0, mmax_large = 0;
   // selected inversion grouping
-  std::vector<int> si_small, si_large;
-  int off_si_small = 0, off_si_large = 0, mmax_si_small = 0, kmax_si_small = 0, kmax_si_large = 0, mmax_si_large = 0, rmax_si_large = 0;
+  std::vector<int> si_tiny, si_small, si_large;
+  int off_si_tiny = 0, off_si_small = 0, off_si_large = 0, mmax_si_small = 0, kmax_si_small = 0, kmax_si_large = 0, mmax_si_large = 0, rmax_si_large = 0;
 };
 
 class GpuFactor {

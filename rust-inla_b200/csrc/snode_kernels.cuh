@@ -813,6 +813,67 @@ __global__ void __launch_bounds__(NT, 4) k_selinv_small(DevSym S, const int* __r
   }
 }
 
+// Selected inverse of tiny fronts (m <= kTinyM), one warp per (front, problem), the
+// Takahashi recurrence of sparse_ldlt.rs:376-432 restricted to the front: for the pivot
+// columns j from right to left, lane i > j forms S_ij = -sum_{l > j} L_lj S_li, then
+// S_jj = 1/d_j - sum_{l > j} L_lj S_lj (a fixed shuffle tree), with Sigma kept with both
+// triangles in the warp's shared slice and Sigma of the below-rows gathered from the parent.
+constexpr int kTinySiWarps = 2;  // two 32 x 33 slices per warp: 33.8 KB of static shared memory
+__global__ void __launch_bounds__(32 * kTinySiWarps) k_selinv_tiny(DevSym S, const int* __restrict__ list, int nlist,
+                                                                  const double* __restrict__ F,
+                                                                  double* __restrict__ Sg, int64_t fstride) {
+  __shared__ double sS[kTinySiWarps][kTinyM * kTinyLd];
+  __shared__ double sL[kTinySiWarps][kTinyM * kTinyLd];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int idx = blockIdx.x * kTinySiWarps + warp;
+  if (idx >= nlist) return;  // the whole warp leaves; only warp-level synchronization follows
+  const int s = list[idx], b = blockIdx.y;
+  const int k = sn_k(S, s), m = sn_m(S, s), r = m - k;
+  double* Sm = sS[warp];
+  double* L = sL[warp];
+  const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
+  double* Ss = Sg + (int64_t)b * fstride + S.fptr[s];
+  for (int e = lane; e < m * k; e += 32) {
+    const int c = e / m, i = e - c * m;
+    L[i + c * kTinyLd] = Fs[e];
+  }
+  if (r > 0) {
+    const int p = S.parent[s];
+    const int mp = sn_m(S, p);
+    const double* Sp = Sg + (int64_t)b * fstride + S.fptr[p];
+    const int* rel = S.relx + S.rowptr[s] + k;
+    for (int e = lane; e < r * r; e += 32) {
+      const int jj = e / r, ii = e - jj * r;
+      if (ii < jj) continue;
+      const double v = parent_sigma(Sp, mp, rel[ii], rel[jj]);
+      Sm[(k + ii) + (k + jj) * kTinyLd] = v;
+      Sm[(k + jj) + (k + ii) * kTinyLd] = v;
+    }
+  }
+  __syncwarp();
+  for (int j = k - 1; j >= 0; --j) {
+    const bool mine = lane > j && lane < m;
+    double acc = 0.0;
+    if (mine)
+      for (int l = j + 1; l < m; ++l) acc += L[l + j * kTinyLd] * Sm[l + lane * kTinyLd];
+    __syncwarp();
+    if (mine) {
+      Sm[lane + j * kTinyLd] = -acc;
+      Sm[j + lane * kTinyLd] = -acc;
+    }
+    __syncwarp();
+    double t = mine ? L[lane + j * kTinyLd] * Sm[lane + j * kTinyLd] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0) Sm[j + j * kTinyLd] = 1.0 / L[j + j * kTinyLd] - t;
+    __syncwarp();
+  }
+  for (int e = lane; e < m * m; e += 32) {
+    const int col = e / m, row = e - col * m;
+    if (row >= col) Ss[e] = Sm[row + col * kTinyLd];
+  }
+}
+
 // diag(Q^-1) in original order
 __global__ void k_extract_diag(DevSym S, const double* __restrict__ Sg, int64_t fstride, double* __restrict__ out,
                                int64_t ostride) {
