@@ -226,6 +226,12 @@ int inla_batch_factorize_dev(inla_batch* h, int B, const double* d_values, doubl
  * ends early and the call that synchronizes after it returns INLA_ERR_CUDA (status bit 4 in
  * the _dev status words). */
 int inla_batch_schedule(inla_batch* h, int* persistent);
+/* Host-only check of the persistent schedule of a solver's symbolic analysis (after
+ * inla_solver_analyze; no device use): walking the task queue in order, every task's
+ * dependencies are complete when it is reached and every front ends complete.
+ * info3 = {tasks per problem, shared memory bytes, 1 if the schedule fits}. INLA_ERR_INTERNAL
+ * with the first violation otherwise. */
+int inla_solver_check_schedule(const inla_solver* s, int64_t* info3);
 /* Process-wide choice for engines (solver, batch, Laplace, many-model handles) created after
  * the call: on != 0 the persistent schedule where it fits, 0 the level launches. */
 int inla_set_persistent_schedule(int on);

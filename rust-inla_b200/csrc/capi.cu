@@ -329,6 +329,26 @@ int inla_solver_supernodes(const inla_solver* s, int64_t* first, int64_t* count)
   return INLA_OK;
 }
 
+int inla_solver_check_schedule(const inla_solver* s, int64_t* info3) {
+  try {
+    if (!s || !s->sym) return fail(INLA_ERR_NOT_FACTORED, "no symbolic analysis yet");
+    std::vector<int> flat;
+    const std::vector<LevelPlan> levels = make_level_plans(*s->sym, flat);
+    PersistPlan pl;
+    const bool fits = make_persist_plan(*s->sym, levels, pl);
+    const std::string err = check_persist_plan(*s->sym, pl);
+    if (info3) {
+      info3[0] = (int64_t)(pl.task.size() / 6);
+      info3[1] = pl.smem;
+      info3[2] = fits ? 1 : 0;
+    }
+    if (!err.empty()) return fail(INLA_ERR_INTERNAL, "persistent schedule: " + err);
+    return INLA_OK;
+  } catch (...) {
+    return map_exception();
+  }
+}
+
 int inla_solver_colcounts(const inla_solver* s, int64_t* counts) {
   if (!s || !s->sym) return fail(INLA_ERR_NOT_FACTORED, "no symbolic analysis yet");
   std::memcpy(counts, s->sym->colcount.data(), sizeof(int64_t) * s->sym->n);

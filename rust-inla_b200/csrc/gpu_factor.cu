@@ -271,14 +271,15 @@ GpuFactor::~GpuFactor() {
   for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second.exec);
 }
 
-void GpuFactor::plan_levels() {
-  const Symbolic& S = sym_;
-  levels_.assign(S.nlevels, LevelPlan());
-  std::vector<int> flat;
+// Level plans of a symbolic analysis (host lists; offsets into the flattened device list).
+std::vector<LevelPlan> make_level_plans(const Symbolic& S, std::vector<int>& flat) {
+  std::vector<LevelPlan> levels(S.nlevels);
+  flat.clear();
   // fronts of at most kTinyM rows: one warp each (INLA_NO_TINY_FRONTS keeps them on k_factor_small)
   static const bool tiny_on = std::getenv("INLA_NO_TINY_FRONTS") == nullptr;
+  constexpr int kSmallA = GpuFactor::kSmallA, kSmallB = GpuFactor::kSmallB, kSiSmall = GpuFactor::kSiSmall;
   for (int32_t l = 0; l < S.nlevels; ++l) {
-    LevelPlan& P = levels_[l];
+    LevelPlan& P = levels[l];
     for (int64_t t = S.level_ptr[l]; t < S.level_ptr[l + 1]; ++t) {
       int s = (int)S.level_list[t];
       int k = (int)(S.sn_first[s + 1] - S.sn_first[s]);
@@ -330,6 +331,12 @@ void GpuFactor::plan_levels() {
     P.off_si_small = put(P.si_small);
     P.off_si_large = put(P.si_large);
   }
+  return levels;
+}
+
+void GpuFactor::plan_levels() {
+  std::vector<int> flat;
+  levels_ = make_level_plans(sym_, flat);
   d_lists_.upload(flat, stream_);
 }
 
@@ -348,48 +355,42 @@ std::atomic<int> g_persist_default{-1};
 
 void set_persistent_default(bool on) { g_persist_default.store(on ? 1 : 0); }
 
-void GpuFactor::plan_persist() {
-  int def = g_persist_default.load();
-  if (def < 0) {
-    def = std::getenv("INLA_NO_PERSIST") ? 0 : 1;
-    int expect = -1;
-    g_persist_default.compare_exchange_strong(expect, def);
-    def = g_persist_default.load();
-  }
-  if (def == 0) return;
-  if (const char* w = std::getenv("INLA_PERSIST_WAIT_MS")) persist_limit_ns_ = (long long)(std::atof(w) * 1e6);
-  const Symbolic& S = sym_;
+// The task queue of the persistent schedule for one problem (host arrays).
+bool make_persist_plan(const Symbolic& S, const std::vector<LevelPlan>& levels, PersistPlan& out) {
   const int ns = (int)S.nsuper;
   constexpr int kGatherBudget = 110 * 1024;  // bytes of one extend-add column slice
-  int smem = std::max({kPersistTinySmem, small_factor_smem(kSmallB), kPanelSmem, kRowsSmem, kPersistUpdSmem});
-  std::vector<int> gstart{0}, task, tiny, total(ns, 0), lid(ns, -1);
-  std::vector<int64_t> gptr(ns, 0);
-  std::vector<int2> grng;
-  int nlarge = 0;
+  int smem = std::max({kPersistTinySmem, small_factor_smem(GpuFactor::kSmallB), kPanelSmem, kRowsSmem,
+                       kPersistUpdSmem});
+  PersistPlan& pl = out;
+  pl = PersistPlan();
+  pl.gstart = {0};
+  pl.total.assign(ns, 0);
+  pl.lid.assign(ns, -1);
+  pl.gptr.assign(ns, 0);
   auto push = [&](int type, int sn, int sub, int need, int j0, int gcols) {
-    task.insert(task.end(), {type, sn, sub, need, j0, gcols});
+    pl.task.insert(pl.task.end(), {type, sn, sub, need, j0, gcols});
   };
   auto close_group = [&] {
-    const int cnt = (int)(task.size() / 6);
-    if (cnt > gstart.back()) gstart.push_back(cnt);
+    const int cnt = (int)(pl.task.size() / 6);
+    if (cnt > pl.gstart.back()) pl.gstart.push_back(cnt);
   };
   struct Phase {
     int type, count, j0;
   };
-  for (const LevelPlan& P : levels_) {
+  for (const LevelPlan& P : levels) {
     for (size_t i = 0; i < P.tiny.size(); i += kPersistTinyWarps) {
       const int cnt = (int)std::min<size_t>(kPersistTinyWarps, P.tiny.size() - i);
-      push(PT_TINY, (int)tiny.size(), cnt, 0, 0, 0);
+      push(PT_TINY, (int)pl.tiny.size(), cnt, 0, 0, 0);
       for (int u = 0; u < cnt; ++u) {
-        tiny.push_back(P.tiny[i + u]);
-        total[P.tiny[i + u]] = 1;
+        pl.tiny.push_back(P.tiny[i + u]);
+        pl.total[P.tiny[i + u]] = 1;
       }
     }
     close_group();
     for (const std::vector<int>* v : {&P.small_a, &P.small_b})
       for (int sn : *v) {
         push(PT_SMALL, sn, 0, 0, 0, 0);
-        total[sn] = 1;
+        pl.total[sn] = 1;
       }
     close_group();
     if (P.large.empty()) continue;
@@ -403,9 +404,9 @@ void GpuFactor::plan_persist() {
       const int gcols = std::max(1, std::min(kGatherCols, kGatherBudget / (8 * m)));
       gc[f] = gcols;
       smem = std::max(smem, gcols * m * 8);
-      lid[sn] = nlarge++;
+      pl.lid[sn] = pl.nlarge++;
       const int nz = cdiv(m, gcols);
-      gptr[sn] = (int64_t)grng.size();
+      pl.gptr[sn] = (int64_t)pl.grng.size();
       for (int z = 0; z < nz; ++z) {
         const int c0 = z * gcols, c1 = std::min(c0 + gcols, m);
         for (int64_t q = S.child_ptr[sn]; q < S.child_ptr[sn + 1]; ++q) {
@@ -415,7 +416,7 @@ void GpuFactor::plan_persist() {
           const int32_t* rel = S.rel.data() + S.rel_ptr[c];
           const int lo = (int)(std::lower_bound(rel, rel + rc, c0) - rel);
           const int hi = (int)(std::lower_bound(rel, rel + rc, c1) - rel);
-          grng.push_back(make_int2(lo, hi));
+          pl.grng.push_back(make_int2(lo, hi));
         }
       }
       ph[f].push_back({PT_GATHER, nz, 0});
@@ -429,7 +430,7 @@ void GpuFactor::plan_persist() {
       maxp = std::max(maxp, ph[f].size());
       int tot = 0;
       for (const Phase& x : ph[f]) tot += x.count;
-      total[sn] = tot;
+      pl.total[sn] = tot;
     }
     std::vector<int> done(P.large.size(), 0);
     for (size_t p = 0; p < maxp; ++p) {
@@ -442,24 +443,98 @@ void GpuFactor::plan_persist() {
       close_group();
     }
   }
-  if (smem > 227 * 1024) return;  // a front too wide for the schedule's shared memory: keep the level launches
-  const size_t dc_doubles = (size_t)std::max(nlarge, 1) * max_batch_ * kB64 * kB64;
+  pl.smem = smem;
+  if (pl.tiny.empty()) pl.tiny.push_back(0);
+  if (pl.grng.empty()) pl.grng.push_back(make_int2(0, 0));
+  return smem <= 227 * 1024 && pl.gstart.size() > 1;
+}
+
+// Host check of the schedule's invariants: processed one task at a time in queue order (one
+// problem), every task's dependencies are complete when it is reached (so the smallest
+// unfinished task of the GPU queue can always run), every front ends with its completion count,
+// and every table index is in range. Returns an empty string or the first violation.
+std::string check_persist_plan(const Symbolic& S, const PersistPlan& pl) {
+  const int ns = (int)S.nsuper;
+  const int ntask = (int)(pl.task.size() / 6);
+  if (pl.gstart.back() != ntask) return "group table does not cover the tasks";
+  for (size_t g = 0; g + 1 < pl.gstart.size(); ++g)
+    if (pl.gstart[g + 1] <= pl.gstart[g]) return "empty or decreasing group " + std::to_string(g);
+  std::vector<int> prog(ns, 0);
+  auto children_done = [&](int sn) {
+    for (int64_t q = S.child_ptr[sn]; q < S.child_ptr[sn + 1]; ++q) {
+      const int c = (int)S.child_list[q];
+      if (prog[c] != pl.total[c]) return false;
+    }
+    return true;
+  };
+  for (int t = 0; t < ntask; ++t) {
+    const int* T = pl.task.data() + 6 * t;
+    const int type = T[0], sn = T[1], sub = T[2], need = T[3];
+    const std::string at = "task " + std::to_string(t) + ": ";
+    if (type == PT_TINY) {
+      if (sub < 1 || sub > kPersistTinyWarps || sn < 0 || sn + sub > (int)pl.tiny.size()) return at + "tiny range";
+      for (int u = 0; u < sub; ++u) {
+        const int f = pl.tiny[sn + u];
+        if (f < 0 || f >= ns || !children_done(f)) return at + "tiny front before its children";
+        const int m = (int)(S.sn_rowptr[f + 1] - S.sn_rowptr[f]);
+        if (m > kTinyM) return at + "front too large for a warp";
+      }
+      for (int u = 0; u < sub; ++u) ++prog[pl.tiny[sn + u]];
+      continue;
+    }
+    if (sn < 0 || sn >= ns) return at + "front out of range";
+    const int k = (int)(S.sn_first[sn + 1] - S.sn_first[sn]), m = (int)(S.sn_rowptr[sn + 1] - S.sn_rowptr[sn]);
+    if (type == PT_SMALL) {
+      if (m > GpuFactor::kSmallB) return at + "front too large for the small body";
+      if (!children_done(sn)) return at + "small front before its children";
+    } else if (type == PT_GATHER) {
+      if (pl.lid[sn] < 0 || !children_done(sn)) return at + "extend-add before the children";
+      const int gcols = T[5], nch = (int)(S.child_ptr[sn + 1] - S.child_ptr[sn]);
+      if (gcols < 1 || (int64_t)gcols * m * 8 > pl.smem) return at + "extend-add slice exceeds shared memory";
+      if (sub >= cdiv(m, gcols) || pl.gptr[sn] + (int64_t)(sub + 1) * nch > (int64_t)pl.grng.size())
+        return at + "extend-add chunk out of range";
+      if (need != 0 || prog[sn] != sub) return at + "extend-add count";
+    } else if (type == PT_DIAG || type == PT_ROWS || type == PT_UPDATE) {
+      if (pl.lid[sn] < 0) return at + "step of a front that is not large";
+      if (T[4] < 0 || T[4] >= k || T[4] % kB64) return at + "block column out of range";
+      if (prog[sn] < need) return at + "phase before its predecessors";
+    } else {
+      return at + "unknown task type";
+    }
+    ++prog[sn];
+  }
+  for (int sn = 0; sn < ns; ++sn)
+    if (pl.total[sn] < 1 || prog[sn] != pl.total[sn]) return "front " + std::to_string(sn) + " incomplete";
+  return std::string();
+}
+
+void GpuFactor::plan_persist() {
+  int def = g_persist_default.load();
+  if (def < 0) {
+    def = std::getenv("INLA_NO_PERSIST") ? 0 : 1;
+    int expect = -1;
+    g_persist_default.compare_exchange_strong(expect, def);
+    def = g_persist_default.load();
+  }
+  if (def == 0) return;
+  if (const char* w = std::getenv("INLA_PERSIST_WAIT_MS")) persist_limit_ns_ = (long long)(std::atof(w) * 1e6);
+  PersistPlan pl;
+  if (!make_persist_plan(sym_, levels_, pl)) return;  // a front too wide for the schedule's shared memory
+  const int ns = (int)sym_.nsuper;
+  const size_t dc_doubles = (size_t)std::max(pl.nlarge, 1) * max_batch_ * kB64 * kB64;
   if (dc_doubles * 8 > ((size_t)4 << 30)) return;
-  if (tiny.empty()) tiny.push_back(0);
-  if (grng.empty()) grng.push_back(make_int2(0, 0));
-  persist_groups_ = (int)gstart.size() - 1;
-  if (persist_groups_ < 1) return;
-  d_pgstart_.upload(gstart, stream_);
-  d_ptask_.upload(task, stream_);
-  d_ptiny_.upload(tiny, stream_);
-  d_ptotal_.upload(total, stream_);
-  d_plid_.upload(lid, stream_);
-  d_pgptr_.upload(gptr, stream_);
-  d_pgrng_.upload(grng, stream_);
+  persist_groups_ = (int)pl.gstart.size() - 1;
+  d_pgstart_.upload(pl.gstart, stream_);
+  d_ptask_.upload(pl.task, stream_);
+  d_ptiny_.upload(pl.tiny, stream_);
+  d_ptotal_.upload(pl.total, stream_);
+  d_plid_.upload(pl.lid, stream_);
+  d_pgptr_.upload(pl.gptr, stream_);
+  d_pgrng_.upload(pl.grng, stream_);
   d_pstate_.alloc(2 + (size_t)max_batch_ * ns);
   INLA_CUDA(cudaMemsetAsync(d_pstate_.p, 0, sizeof(int) * (2 + (size_t)max_batch_ * ns), stream_));
   dcache_p_.alloc(dc_doubles);
-  persist_smem_ = smem;
+  persist_smem_ = pl.smem;
   persist_ = true;
 }
 

@@ -75,6 +75,19 @@ struct LevelPlan {
   int off_si_tiny = 0, off_si_small = 0, off_si_large = 0, mmax_si_small = 0, kmax_si_small = 0, kmax_si_large = 0, mmax_si_large = 0, rmax_si_large = 0;
 };
 
+// Task queue of the persistent schedule for one problem (snode_persist.cuh): 6 ints per task
+// {type, front, sub, need, j0, gcols}, group starts, tiny-front list, completion counts per
+// front, large-front index, extend-add chunk table, shared memory in bytes.
+struct PersistPlan {
+  std::vector<int> gstart, task, tiny, total, lid;
+  std::vector<int64_t> gptr;
+  std::vector<int2> grng;
+  int nlarge = 0, smem = 0;
+};
+std::vector<LevelPlan> make_level_plans(const Symbolic& S, std::vector<int>& flat);
+bool make_persist_plan(const Symbolic& S, const std::vector<LevelPlan>& levels, PersistPlan& out);
+std::string check_persist_plan(const Symbolic& S, const PersistPlan& pl);
+
 class GpuFactor {
  public:
   // Size classes (rows of the front): <= kSmallA uses 128 threads, <= kSmallB 256

@@ -91,6 +91,7 @@ SIGNATURES = [
     ("inla_batch_selinv_pattern", C.c_int, [P, C.c_int, DP]),
     ("inla_batch_factorize_dev", C.c_int, [P, C.c_int, P, P, P, P]),
     ("inla_batch_schedule", C.c_int, [P, IP]),
+    ("inla_solver_check_schedule", C.c_int, [P, LP]),
     ("inla_set_persistent_schedule", C.c_int, [C.c_int]),
     ("inla_batch_wait_limit_selftest", C.c_int, [P, C.c_double, IP]),
     ("inla_batch_solve_dev", C.c_int, [P, C.c_int, P, P]),
