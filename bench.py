@@ -444,7 +444,9 @@ def run_ours(args, ws, rank, local, dist):
             "speedup_vs_plain_gpu": (plain["fit_s"] / fit_s) if plain else None,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "fit_s": e2e_ms * 1e-3 / max(args.e2e_steps, 1), "create_fit_close_s": e2e_parts,
-                    "create_first_s": round(create_first_s, 4)},
+                    "create_first_s": round(create_first_s, 4),
+                    "note": "model creation inside every e2e step; the symbolic analysis of the pattern is the "
+                            "process-wide cached one from the first creation (create_first_s includes it)"},
             "gpu_launches": int(launches), "clocks": clocks, "roofline": roof, "cpu_baseline": cpu}
     print(json.dumps(line), flush=True)
     return 0
