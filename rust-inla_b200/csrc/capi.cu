@@ -336,7 +336,13 @@ int inla_solver_check_schedule(const inla_solver* s, int64_t* info3) {
     const std::vector<LevelPlan> levels = make_level_plans(*s->sym, flat);
     PersistPlan pl;
     const bool fits = make_persist_plan(*s->sym, levels, pl);
-    const std::string err = check_persist_plan(*s->sym, pl);
+    std::string err = check_persist_plan(*s->sym, pl);
+    if (err.empty()) {
+      PersistPlan sp;
+      make_solve_plan(*s->sym, levels, sp);
+      err = check_solve_plan(*s->sym, sp);
+      if (!err.empty()) err = "solve: " + err;
+    }
     if (info3) {
       info3[0] = (int64_t)(pl.task.size() / 6);
       info3[1] = pl.smem;

@@ -256,6 +256,13 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
     persist_grid_ = std::max(1, per_sm) * num_sms_;
     if (per_sm < 1) persist_ = false;
   }
+  if (solve_persist_) {
+    set_smem(k_solve_persist, solve_smem_);
+    int per_sm = 0;
+    INLA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve_persist, kPersistThreads, solve_smem_));
+    solve_grid_ = std::max(1, per_sm) * num_sms_;
+    if (per_sm < 1) solve_persist_ = false;
+  }
   INLA_CUDA(cudaStreamSynchronize(stream_));
   if (std::getenv("INLA_DEBUG"))
     std::fprintf(stderr, "device factor: maps %.1f ms, symbolic uploads %.1f ms, caches %.1f ms, levels %.1f ms, buffers %.1f ms (%d slots)\n",
@@ -508,6 +515,86 @@ std::string check_persist_plan(const Symbolic& S, const PersistPlan& pl) {
   return std::string();
 }
 
+void make_solve_plan(const Symbolic& S, const std::vector<LevelPlan>& levels, PersistPlan& pl) {
+  pl = PersistPlan();
+  pl.gstart = {0};
+  auto push = [&](int type, int sn, int sub) { pl.task.insert(pl.task.end(), {type, sn, sub, 0, 0, 0}); };
+  auto close_group = [&] {
+    const int cnt = (int)(pl.task.size() / 6);
+    if (cnt > pl.gstart.back()) pl.gstart.push_back(cnt);
+  };
+  auto tiny_tasks = [&](const std::vector<int>& v, int type) {
+    for (size_t i = 0; i < v.size(); i += kPersistTinyWarps) {
+      const int cnt = (int)std::min<size_t>(kPersistTinyWarps, v.size() - i);
+      push(type, (int)pl.tiny.size(), cnt);
+      for (int u = 0; u < cnt; ++u) pl.tiny.push_back(v[i + u]);
+    }
+    close_group();
+  };
+  int mmax = 0;
+  for (const LevelPlan& P : levels) {
+    tiny_tasks(P.tiny, ST_FWD_TINY);
+    for (int sn : P.nontiny) push(ST_FWD, sn, 0);
+    close_group();
+    mmax = std::max(mmax, P.mmax_nontiny);
+  }
+  for (size_t l = levels.size(); l-- > 0;) {
+    for (int sn : levels[l].nontiny) push(ST_BWD, sn, 0);
+    close_group();
+    tiny_tasks(levels[l].tiny, ST_BWD_TINY);
+  }
+  pl.smem = std::max(kPersistTinyWarps * 32, mmax + 2 + 32 * 33) * 8;
+  if (pl.tiny.empty()) pl.tiny.push_back(0);
+}
+
+// As check_persist_plan, for the solve queue: forward tasks after their children's forward
+// tasks, backward tasks after their parent's backward task (roots: after their own forward).
+std::string check_solve_plan(const Symbolic& S, const PersistPlan& pl) {
+  const int ns = (int)S.nsuper;
+  const int ntask = (int)(pl.task.size() / 6);
+  if (pl.gstart.back() != ntask) return "group table does not cover the tasks";
+  std::vector<int> pf(ns, 0), pb(ns, 0);
+  auto ready = [&](int type, int sn) {
+    if (type == ST_FWD_TINY || type == ST_FWD) {
+      for (int64_t q = S.child_ptr[sn]; q < S.child_ptr[sn + 1]; ++q)
+        if (pf[S.child_list[q]] != 1) return false;
+      return pf[sn] == 0;
+    }
+    const int64_t p = S.sn_parent[sn];
+    return pb[sn] == 0 && (p < 0 ? pf[sn] == 1 : pb[p] == 1);
+  };
+  for (int t = 0; t < ntask; ++t) {
+    const int* T = pl.task.data() + 6 * t;
+    const bool tiny = T[0] == ST_FWD_TINY || T[0] == ST_BWD_TINY;
+    const bool fwd = T[0] == ST_FWD_TINY || T[0] == ST_FWD;
+    const int cnt = tiny ? T[2] : 1;
+    for (int u = 0; u < cnt; ++u) {
+      const int sn = tiny ? pl.tiny[T[1] + u] : T[1];
+      if (sn < 0 || sn >= ns || !ready(T[0], sn)) return "task " + std::to_string(t) + " before its dependencies";
+      if (tiny && S.sn_rowptr[sn + 1] - S.sn_rowptr[sn] > kTinyM) return "tiny task with a wide front";
+      (fwd ? pf : pb)[sn] = 1;
+    }
+  }
+  for (int sn = 0; sn < ns; ++sn)
+    if (pf[sn] != 1 || pb[sn] != 1) return "front " + std::to_string(sn) + " not swept";
+  return std::string();
+}
+
+void GpuFactor::plan_solve_persist() {
+  PersistPlan pl;
+  make_solve_plan(sym_, levels_, pl);
+  if (pl.smem > 227 * 1024 || pl.gstart.size() < 2) return;
+  const int ns = (int)sym_.nsuper;
+  solve_groups_ = (int)pl.gstart.size() - 1;
+  d_sgstart_.upload(pl.gstart, stream_);
+  d_stask_.upload(pl.task, stream_);
+  d_stiny_.upload(pl.tiny, stream_);
+  d_sstate_.alloc(2 + 2 * (size_t)max_batch_ * ns);
+  INLA_CUDA(cudaMemsetAsync(d_sstate_.p, 0, sizeof(int) * (2 + 2 * (size_t)max_batch_ * ns), stream_));
+  solve_smem_ = pl.smem;
+  solve_persist_ = true;
+}
+
 void GpuFactor::plan_persist() {
   int def = g_persist_default.load();
   if (def < 0) {
@@ -536,6 +623,7 @@ void GpuFactor::plan_persist() {
   dcache_p_.alloc(dc_doubles);
   persist_smem_ = pl.smem;
   persist_ = true;
+  plan_solve_persist();
 }
 
 void GpuFactor::set_front_groups(const std::vector<int>& fseg) {
@@ -578,12 +666,15 @@ void GpuFactor::run_factor_persist(int B, const int* total_override, long long l
 
 void GpuFactor::check_schedule() {
   if (!persist_) return;
-  int err = 0;
+  int err = 0, serr = 0;
   INLA_CUDA(cudaMemcpyAsync(&err, d_pstate_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+  if (solve_persist_) INLA_CUDA(cudaMemcpyAsync(&serr, d_sstate_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_));
   INLA_CUDA(cudaStreamSynchronize(stream_));
-  if (err == 0) return;
+  if (err == 0 && serr == 0) return;
   INLA_CUDA(cudaMemsetAsync(d_pstate_.p, 0, sizeof(int), stream_));
+  if (solve_persist_) INLA_CUDA(cudaMemsetAsync(d_sstate_.p, 0, sizeof(int), stream_));
   INLA_CUDA(cudaStreamSynchronize(stream_));
+  if (err == 0) err = serr;
   throw CudaError("persistent factorization stopped: a dependency wait ran out (code " + std::to_string(err) + ")",
                   (int)cudaErrorLaunchTimeout);
 }
@@ -835,6 +926,34 @@ void GpuFactor::solve(double* d_x, int64_t xstride, int B, int slot0) {
   const int64_t fs = ftotal_;
   const double* Fp = F_.p + (int64_t)slot0 * fs;
   dim3 gp(cdiv(n, 256) > 1024 ? 1024 : cdiv(n, 256), B);
+  if (solve_persist_) {
+    launch_cached({3, B, (int64_t)(uintptr_t)d_x, xstride, slot0}, [&] {
+      const int ns = (int)sym_.nsuper;
+      k_permute_in<<<gp, 256, 0, stream_>>>(n, d_perm_.p, d_x, xstride, xp_.p);
+      INLA_CUDA(cudaMemsetAsync(d_sstate_.p + 1, 0, sizeof(int) * (1 + 2 * (size_t)B * ns), stream_));
+      SolveArgs a;
+      a.S = ds_;
+      a.F = Fp;
+      a.fstride = fs;
+      a.B = B;
+      a.ngroups = solve_groups_;
+      a.gstart = d_sgstart_.p;
+      a.task = reinterpret_cast<const PersistTask*>(d_stask_.p);
+      a.tiny_list = d_stiny_.p;
+      a.xp = xp_.p;
+      a.ub = ub_.p;
+      a.ustride = std::max<int64_t>(usum_, 1);
+      a.progf = d_sstate_.p + 2;
+      a.progb = d_sstate_.p + 2 + (size_t)B * ns;
+      a.head = reinterpret_cast<unsigned*>(d_sstate_.p + 1);
+      a.err = d_sstate_.p;
+      a.limit_ns = persist_limit_ns_;
+      k_solve_persist<<<solve_grid_, kPersistThreads, solve_smem_, stream_>>>(a);
+      k_permute_out<<<gp, 256, 0, stream_>>>(n, d_perm_.p, xp_.p, d_x, xstride);
+      launches_ += 3;
+    });
+    return;
+  }
   launch_cached({3, B, (int64_t)(uintptr_t)d_x, xstride, slot0}, [&] {
     k_permute_in<<<gp, 256, 0, stream_>>>(n, d_perm_.p, d_x, xstride, xp_.p);
     ++launches_;

@@ -87,6 +87,9 @@ struct PersistPlan {
 std::vector<LevelPlan> make_level_plans(const Symbolic& S, std::vector<int>& flat);
 bool make_persist_plan(const Symbolic& S, const std::vector<LevelPlan>& levels, PersistPlan& out);
 std::string check_persist_plan(const Symbolic& S, const PersistPlan& pl);
+// Task queue of the persistent triangular solve (forward sweep bottom-up, then backward).
+void make_solve_plan(const Symbolic& S, const std::vector<LevelPlan>& levels, PersistPlan& out);
+std::string check_solve_plan(const Symbolic& S, const PersistPlan& pl);
 
 class GpuFactor {
  public:
@@ -213,6 +216,11 @@ class GpuFactor {
   DBuf<int2> d_pgrng_;
   DBuf<double> dcache_p_;
   DBuf<int> d_fseg_;
+  // persistent solve
+  bool solve_persist_ = false;
+  int solve_smem_ = 0, solve_grid_ = 0, solve_groups_ = 0;
+  DBuf<int> d_sgstart_, d_stask_, d_stiny_, d_sstate_;  // sstate: err, head, progf[B][ns], progb[B][ns]
+  void plan_solve_persist();
 };
 
 }  // namespace inla

@@ -459,12 +459,11 @@ __global__ void __launch_bounds__(128) k_update64(DevSym S, const int* __restric
 // (two barriers per block instead of one per column)
 // ---------------------------------------------------------------------------
 
+// Forward sweep of front s, problem b (NT threads; y: m + 2 + 32 * 33 doubles of shared memory).
 template <int NT>
-__global__ void __launch_bounds__(NT, 8) k_fwd32(DevSym S, const int* __restrict__ list, const double* __restrict__ F,
-                                              int64_t fstride, double* __restrict__ xp, double* __restrict__ ub,
-                                              int64_t ustride) {
-  extern __shared__ double y[];
-  const int s = list[blockIdx.x], b = blockIdx.y;
+__device__ __forceinline__ void fwd32_body(const DevSym& S, int s, int b, const double* __restrict__ F,
+                                           int64_t fstride, double* __restrict__ xp, double* __restrict__ ub,
+                                           int64_t ustride, double* y) {
   const int k = lg_k(S, s), m = lg_m(S, s), f = S.first[s];
   const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
   double* xb = xp + (int64_t)b * S.n;
@@ -516,10 +515,17 @@ __global__ void __launch_bounds__(NT, 8) k_fwd32(DevSym S, const int* __restrict
 }
 
 template <int NT>
-__global__ void __launch_bounds__(NT, 8) k_bwd32(DevSym S, const int* __restrict__ list, const double* __restrict__ F,
-                                              int64_t fstride, double* __restrict__ xp) {
-  extern __shared__ double x[];
-  const int s = list[blockIdx.x], b = blockIdx.y;
+__global__ void __launch_bounds__(NT, 8) k_fwd32(DevSym S, const int* __restrict__ list, const double* __restrict__ F,
+                                              int64_t fstride, double* __restrict__ xp, double* __restrict__ ub,
+                                              int64_t ustride) {
+  extern __shared__ double y[];
+  fwd32_body<NT>(S, list[blockIdx.x], blockIdx.y, F, fstride, xp, ub, ustride, y);
+}
+
+// Backward sweep of front s, problem b (NT threads; x: m + 2 + 32 * 33 doubles of shared memory).
+template <int NT>
+__device__ __forceinline__ void bwd32_body(const DevSym& S, int s, int b, const double* __restrict__ F,
+                                           int64_t fstride, double* __restrict__ xp, double* x) {
   const int k = lg_k(S, s), m = lg_m(S, s), f = S.first[s];
   const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
   double* xb = xp + (int64_t)b * S.n;
@@ -569,6 +575,13 @@ __global__ void __launch_bounds__(NT, 8) k_bwd32(DevSym S, const int* __restrict
   for (int t = threadIdx.x; t < k; t += NT) xb[f + t] = x[t];
 }
 
+template <int NT>
+__global__ void __launch_bounds__(NT, 8) k_bwd32(DevSym S, const int* __restrict__ list, const double* __restrict__ F,
+                                              int64_t fstride, double* __restrict__ xp) {
+  extern __shared__ double x[];
+  bwd32_body<NT>(S, list[blockIdx.x], blockIdx.y, F, fstride, xp, x);
+}
+
 // Sweeps of fronts with m <= 32 rows (one 32-column block): one warp per (front,
 // problem), kTinySweepWarps per CTA. Lane t holds entry t of the front's vector; the
 // arithmetic follows k_fwd32 / k_bwd32 step for step (sequential shuffle chain on the
@@ -576,20 +589,15 @@ __global__ void __launch_bounds__(NT, 8) k_bwd32(DevSym S, const int* __restrict
 // for the column sums), so the results equal theirs.
 constexpr int kTinySweepWarps = 8;
 
-__global__ void __launch_bounds__(32 * kTinySweepWarps) k_fwd_tiny(DevSym S, const int* __restrict__ list, int nlist,
-                                                                   const double* __restrict__ F, int64_t fstride,
-                                                                   double* __restrict__ xp, double* __restrict__ ub,
-                                                                   int64_t ustride) {
-  __shared__ double sy[kTinySweepWarps][32];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int idx = blockIdx.x * kTinySweepWarps + warp;
-  if (idx >= nlist) return;  // the whole warp leaves; only warp-level synchronization follows
-  const int s = list[idx], b = blockIdx.y;
+// One warp: forward sweep of tiny front s, problem b (y: 32 doubles of shared memory).
+__device__ __forceinline__ void fwd_tiny_warp(const DevSym& S, int s, int b, const double* __restrict__ F,
+                                              int64_t fstride, double* __restrict__ xp, double* __restrict__ ub,
+                                              int64_t ustride, double* y) {
+  const int lane = threadIdx.x & 31;
   const int k = lg_k(S, s), m = lg_m(S, s), f = S.first[s];
   const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
   double* xb = xp + (int64_t)b * S.n;
   double* ubb = ub + (int64_t)b * ustride;
-  double* y = sy[warp];
   y[lane] = lane < k ? xb[f + lane] : 0.0;
   __syncwarp();
   for (int q = S.child_ptr[s]; q < S.child_ptr[s + 1]; ++q) {
@@ -619,13 +627,21 @@ __global__ void __launch_bounds__(32 * kTinySweepWarps) k_fwd_tiny(DevSym S, con
   else if (lane < m) ubb[S.uoff[s] + lane - k] = yi;
 }
 
-__global__ void __launch_bounds__(32 * kTinySweepWarps) k_bwd_tiny(DevSym S, const int* __restrict__ list, int nlist,
+__global__ void __launch_bounds__(32 * kTinySweepWarps) k_fwd_tiny(DevSym S, const int* __restrict__ list, int nlist,
                                                                    const double* __restrict__ F, int64_t fstride,
-                                                                   double* __restrict__ xp) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+                                                                   double* __restrict__ xp, double* __restrict__ ub,
+                                                                   int64_t ustride) {
+  __shared__ double sy[kTinySweepWarps][32];
+  const int warp = threadIdx.x >> 5;
   const int idx = blockIdx.x * kTinySweepWarps + warp;
   if (idx >= nlist) return;  // the whole warp leaves; only warp-level synchronization follows
-  const int s = list[idx], b = blockIdx.y;
+  fwd_tiny_warp(S, list[idx], blockIdx.y, F, fstride, xp, ub, ustride, sy[warp]);
+}
+
+// One warp: backward sweep of tiny front s, problem b (registers and shuffles only).
+__device__ __forceinline__ void bwd_tiny_warp(const DevSym& S, int s, int b, const double* __restrict__ F,
+                                              int64_t fstride, double* __restrict__ xp) {
+  const int lane = threadIdx.x & 31;
   const int k = lg_k(S, s), m = lg_m(S, s), f = S.first[s];
   const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
   double* xb = xp + (int64_t)b * S.n;
@@ -647,6 +663,15 @@ __global__ void __launch_bounds__(32 * kTinySweepWarps) k_bwd_tiny(DevSym S, con
     if (lane < i) xl -= Fs[i + (int64_t)lane * m] * xi;
   }
   if (lane < k) xb[f + lane] = xl;
+}
+
+__global__ void __launch_bounds__(32 * kTinySweepWarps) k_bwd_tiny(DevSym S, const int* __restrict__ list, int nlist,
+                                                                   const double* __restrict__ F, int64_t fstride,
+                                                                   double* __restrict__ xp) {
+  const int warp = threadIdx.x >> 5;
+  const int idx = blockIdx.x * kTinySweepWarps + warp;
+  if (idx >= nlist) return;  // the whole warp leaves; only warp-level synchronization follows
+  bwd_tiny_warp(S, list[idx], blockIdx.y, F, fstride, xp);
 }
 
 // ---------------------------------------------------------------------------

@@ -289,3 +289,113 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_factor_persist(PersistAr
 
 }  // namespace
 }  // namespace inla
+
+namespace inla {
+namespace {
+
+// ---------------------------------------------------------------------------
+// Persistent triangular solve: the forward sweep bottom-up and the backward sweep top-down as
+// one task queue (tiny fronts eight per task, one warp each; other fronts one CTA each). A
+// forward task waits for its children's forward tasks; a backward task waits for its
+// parent's backward task (a root: for its own forward task). Same bounded waits and
+// completion counting as the factorization; the bodies are the level kernels' bodies.
+// ---------------------------------------------------------------------------
+enum SolveTaskType : int { ST_FWD_TINY = 0, ST_FWD = 1, ST_BWD = 2, ST_BWD_TINY = 3 };
+
+struct SolveArgs {
+  DevSym S;
+  const double* F;
+  int64_t fstride;
+  int B;
+  int ngroups;
+  const int* gstart;
+  const PersistTask* task;
+  const int* tiny_list;
+  double* xp;
+  double* ub;
+  int64_t ustride;
+  int* progf;  // [B][ns] forward sweep done
+  int* progb;  // [B][ns] backward sweep done
+  unsigned* head;
+  int* err;
+  long long limit_ns;
+};
+
+__device__ bool solve_wait(const SolveArgs& a, int type, int sn, int b) {
+  const DevSym& S = a.S;
+  const int64_t o = (int64_t)b * S.ns;
+  if (type == ST_FWD_TINY || type == ST_FWD) {
+    for (int q = S.child_ptr[sn]; q < S.child_ptr[sn + 1]; ++q)
+      if (!wait_at_least(a.progf + o + S.child_list[q], 1, a.err, a.limit_ns)) return false;
+    return true;
+  }
+  const int p = S.parent[sn];
+  if (p < 0 || p >= S.ns) return wait_at_least(a.progf + o + sn, 1, a.err, a.limit_ns);
+  return wait_at_least(a.progb + o + p, 1, a.err, a.limit_ns);
+}
+
+__global__ void __launch_bounds__(kPersistThreads, 2) k_solve_persist(SolveArgs a) {
+  extern __shared__ double ssm[];
+  __shared__ int sh_task, sh_go;
+  const DevSym& S = a.S;
+  const int per = a.gstart[a.ngroups];
+  const long long total = (long long)a.B * per;
+  for (;;) {
+    if (threadIdx.x == 0) sh_task = (int)atomicAdd(a.head, 1u);
+    __syncthreads();
+    const long long t = sh_task;
+    if (t >= total) break;
+    const int q = (int)(t / a.B);
+    int lo = 0, hi = a.ngroups;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (a.gstart[mid] <= q) lo = mid;
+      else hi = mid;
+    }
+    const int g = lo, cnt = a.gstart[g + 1] - a.gstart[g];
+    const long long j = t - (long long)a.B * a.gstart[g];
+    const int b = (int)(j / cnt), i = (int)(j - (long long)b * cnt);
+    const PersistTask T = a.task[a.gstart[g] + i];
+    const bool tiny = T.type == ST_FWD_TINY || T.type == ST_BWD_TINY;
+    if (threadIdx.x == 0) {
+      bool ok = true;
+      if (tiny) {
+        for (int u = 0; u < T.sub && ok; ++u) ok = solve_wait(a, T.type, a.tiny_list[T.s + u], b);
+      } else {
+        ok = solve_wait(a, T.type, T.s, b);
+      }
+      sh_go = ok;
+    }
+    __syncthreads();
+    if (!sh_go) break;
+    const int warp = threadIdx.x >> 5;
+    switch (T.type) {
+      case ST_FWD_TINY:
+        if (warp < T.sub)
+          fwd_tiny_warp(S, a.tiny_list[T.s + warp], b, a.F, a.fstride, a.xp, a.ub, a.ustride, ssm + 32 * warp);
+        break;
+      case ST_FWD:
+        fwd32_body<kPersistThreads>(S, T.s, b, a.F, a.fstride, a.xp, a.ub, a.ustride, ssm);
+        break;
+      case ST_BWD:
+        bwd32_body<kPersistThreads>(S, T.s, b, a.F, a.fstride, a.xp, ssm);
+        break;
+      default:
+        if (warp < T.sub) bwd_tiny_warp(S, a.tiny_list[T.s + warp], b, a.F, a.fstride, a.xp);
+        break;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      int* pc = (T.type == ST_FWD_TINY || T.type == ST_FWD ? a.progf : a.progb) + (int64_t)b * S.ns;
+      if (tiny) {
+        for (int u = 0; u < T.sub; ++u) atomicAdd(pc + a.tiny_list[T.s + u], 1);
+      } else {
+        atomicAdd(pc + T.s, 1);
+      }
+    }
+  }
+}
+
+}  // namespace
+}  // namespace inla
