@@ -222,7 +222,8 @@ int inla_batch_factorize_dev(inla_batch* h, int B, const double* d_values, doubl
  * every batch member in ONE persistent launch (a task queue in elimination-tree order with
  * bounded dependency waits), 0 when it launches the kernels level by level (fronts too wide
  * for the persistent kernel's shared memory, or INLA_NO_PERSIST set). Results are the same
- * bit for bit. A persistent launch whose dependency wait ran out (2 s; INLA_PERSIST_WAIT_MS)
+ * bit for bit; *persistent = 1 means the schedule is available (with mode 1 each batch size
+ * then uses the faster of the two). A persistent launch whose dependency wait ran out (2 s; INLA_PERSIST_WAIT_MS)
  * ends early and the call that synchronizes after it returns INLA_ERR_CUDA (status bit 4 in
  * the _dev status words). */
 int inla_batch_schedule(inla_batch* h, int* persistent);
@@ -233,8 +234,10 @@ int inla_batch_schedule(inla_batch* h, int* persistent);
  * with the first violation otherwise. */
 int inla_solver_check_schedule(const inla_solver* s, int64_t* info3);
 /* Process-wide choice for engines (solver, batch, Laplace, many-model handles) created after
- * the call: on != 0 the persistent schedule where it fits, 0 the level launches. */
-int inla_set_persistent_schedule(int on);
+ * the call: 0 the level launches; 1 (default) measured per batch size -- on its first
+ * factorization at a batch size an engine times both schedules and keeps the faster for that
+ * structure and size; 2 the persistent schedule wherever it fits. */
+int inla_set_persistent_schedule(int mode);
 /* Diagnostic of the bounded waits: runs the persistent factorization once with completion
  * counts that can never be reached and a wait limit of limit_ms, and returns in *code what
  * the launch recorded (1: a wait ran out and the launch ended). The handle stays usable;

@@ -395,8 +395,9 @@ void inla_batch_free(inla_batch* h) {
   delete h;
 }
 
-int inla_set_persistent_schedule(int on) {
-  set_persistent_default(on != 0);
+int inla_set_persistent_schedule(int mode) {
+  if (mode < 0 || mode > 2) return fail(INLA_ERR_INVALID, "schedule mode must be 0, 1 or 2");
+  set_persistent_default(mode);
   return INLA_OK;
 }
 

@@ -23,7 +23,17 @@ struct DevSym {
   // for fronts that have no cached blocks.
   const int* lbo = nullptr;        // ns
   int64_t lstride = 0;
+  // Optional (independent models held block-diagonally): the factorization skips the fronts
+  // of the (problem, model) pairs whose entry of active ([B][nseg]) is 0; fseg: model of
+  // each front. Those fronts keep their previous contents.
+  const unsigned char* active = nullptr;
+  const int* fseg = nullptr;
+  int nseg = 1;
 };
+
+__host__ __device__ inline bool front_skipped(const DevSym& S, int s, int b) {
+  return S.active && !S.active[(int64_t)b * S.nseg + S.fseg[s]];
+}
 
 constexpr int kStatusOk = 0;
 constexpr int kStatusSingular = 1;

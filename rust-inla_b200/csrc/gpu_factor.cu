@@ -355,12 +355,16 @@ void GpuFactor::plan_levels() {
 // problem 0 come first, then problem 1, and so on.
 // ---------------------------------------------------------------------------
 namespace {
-// Process-wide default of the schedule for engines built from now on (INLA_NO_PERSIST in the
-// environment starts it off; inla_set_persistent_schedule changes it).
+// Process-wide schedule mode for engines built from now on: 0 level launches only, 1 measured
+// per batch size (default), 2 persistent wherever it fits. INLA_NO_PERSIST in the environment
+// starts it at 0; inla_set_persistent_schedule changes it.
 std::atomic<int> g_persist_default{-1};
+// measured choice per (supernodal structure, batch size): true = persistent
+std::mutex g_sched_mu;
+std::map<std::pair<uint64_t, int>, bool> g_sched;
 }  // namespace
 
-void set_persistent_default(bool on) { g_persist_default.store(on ? 1 : 0); }
+void set_persistent_default(int mode) { g_persist_default.store(mode < 0 ? 0 : (mode > 2 ? 2 : mode)); }
 
 // The task queue of the persistent schedule for one problem (host arrays).
 bool make_persist_plan(const Symbolic& S, const std::vector<LevelPlan>& levels, PersistPlan& out) {
@@ -604,6 +608,7 @@ void GpuFactor::plan_persist() {
     def = g_persist_default.load();
   }
   if (def == 0) return;
+  persist_mode_ = def;
   if (const char* w = std::getenv("INLA_PERSIST_WAIT_MS")) persist_limit_ns_ = (long long)(std::atof(w) * 1e6);
   PersistPlan pl;
   if (!make_persist_plan(sym_, levels_, pl)) return;  // a front too wide for the schedule's shared memory
@@ -655,13 +660,61 @@ void GpuFactor::run_factor_persist(int B, const int* total_override, long long l
   a.gptr = d_pgptr_.p;
   a.grng = d_pgrng_.p;
   a.limit_ns = limit_ns > 0 ? limit_ns : persist_limit_ns_;
-  a.active = active;
-  a.fseg = d_fseg_.p;
-  a.nseg = nseg;
+  if (active) {
+    a.S.active = active;
+    a.S.fseg = d_fseg_.p;
+    a.S.nseg = nseg;
+  }
   k_factor_persist<<<persist_grid_, kPersistThreads, persist_smem_, stream_>>>(a);
   k_logdet_chunks<<<dim3(nldchunk_, B), 256, 0, stream_>>>(ds_, F_.p, ftotal_, ldpart_.p, ldflag_.p, ldticket_.p,
                                                            logdet_.p, status_.p, d_pstate_.p);
   launches_ += 2;
+}
+
+// Persistent or level launches for batch size B: fixed by the mode, or measured on the
+// first factorization at B (the level sequence in its tuned form and the persistent launch,
+// each after a warm-up, with CUDA events on the engine's stream) and kept for the structure
+// and B. The triangular solve follows the same choice.
+bool GpuFactor::use_persist(int B, const std::function<void()>& fill) {
+  if (!persist_) return false;
+  if (persist_mode_ == 2) return true;
+  auto it = persist_at_.find(B);
+  if (it != persist_at_.end()) return it->second;
+  {
+    std::lock_guard<std::mutex> lk(g_sched_mu);
+    auto g = g_sched.find({struct_hash_, B});
+    if (g != g_sched.end()) return persist_at_[B] = g->second;
+  }
+  const std::vector<char>* pol = schedule(B, fill);
+  cudaEvent_t e[4];
+  for (auto& x : e) INLA_CUDA(cudaEventCreate(&x));
+  fill();
+  run_factor_levels(B, pol);  // warm-up
+  fill();
+  INLA_CUDA(cudaEventRecord(e[0], stream_));
+  run_factor_levels(B, pol);
+  INLA_CUDA(cudaEventRecord(e[1], stream_));
+  fill();
+  run_factor_persist(B);  // warm-up
+  fill();
+  INLA_CUDA(cudaEventRecord(e[2], stream_));
+  run_factor_persist(B);
+  INLA_CUDA(cudaEventRecord(e[3], stream_));
+  INLA_CUDA(cudaStreamSynchronize(stream_));
+  float tl = 0.f, tp = 0.f;
+  INLA_CUDA(cudaEventElapsedTime(&tl, e[0], e[1]));
+  INLA_CUDA(cudaEventElapsedTime(&tp, e[2], e[3]));
+  for (auto& x : e) cudaEventDestroy(x);
+  check_schedule();
+  const bool pick = tp < tl;
+  if (std::getenv("INLA_DEBUG"))
+    std::fprintf(stderr, "schedule B=%d: level launches %.3f ms, persistent %.3f ms -> %s\n", B, tl, tp,
+                 pick ? "persistent" : "levels");
+  {
+    std::lock_guard<std::mutex> lk(g_sched_mu);
+    g_sched[{struct_hash_, B}] = pick;
+  }
+  return persist_at_[B] = pick;
 }
 
 void GpuFactor::check_schedule() {
@@ -882,10 +935,11 @@ void GpuFactor::factor_values(const double* d_vals, int B) {
                                                         ftotal_);
     ++launches_;
   };
-  const std::vector<char>* pol = persist_ ? nullptr : schedule(B, fill);  // settled before any capture
-  launch_cached({1, B, (int64_t)(uintptr_t)d_vals}, [&] {
+  const bool per = use_persist(B, fill);  // settled before any capture
+  const std::vector<char>* pol = per ? nullptr : schedule(B, fill);
+  launch_cached({1, B, (int64_t)(uintptr_t)d_vals, per}, [&] {
     fill();
-    if (persist_) run_factor_persist(B);
+    if (per) run_factor_persist(B);
     else run_factor_levels(B, pol);
   });
 }
@@ -900,23 +954,37 @@ void GpuFactor::factor_model(int ncomp, const double* d_comp, const double* d_co
   int64_t dbits, dpbits;
   std::memcpy(&dbits, &diag_add, sizeof(dbits));
   std::memcpy(&dpbits, &diag_add_post, sizeof(dpbits));
-  if (!can_skip_groups()) d_active = nullptr;  // the level launches factorize every pair
+
+  const unsigned char* fill_mask = nullptr;  // the measurements below fill and factorize every pair
   auto fill = [&] {
     k_fill_panels_model<<<dim3(nfillm_), 256, 0, stream_>>>(ds_, d_csnm_.p, ntot_, d_pmap_.p, ncomp, d_comp, nnz_,
                                                             d_coef, diag_add, d_pdiag, d_cptr, d_cobs, d_cprod, d_w,
                                                             wstride, B, nprior, diag_add_post, d_pseg, nseg, F_.p,
-                                                            ftotal_, d_fseg_.p, d_active);
+                                                            ftotal_, d_fseg_.p, fill_mask);
     ++launches_;
   };
-  const std::vector<char>* pol = persist_ ? nullptr : schedule(B, fill);  // settled before any capture
+  const bool per = use_persist(B, fill);  // settled before any capture
+  if (!d_fseg_.p) d_active = nullptr;
+  fill_mask = d_active;
+  const std::vector<char>* pol = per ? nullptr : schedule(B, fill);
   launch_cached({2, B, ncomp, (int64_t)(uintptr_t)d_comp, (int64_t)(uintptr_t)d_coef, dbits,
                  (int64_t)(uintptr_t)d_pdiag, (int64_t)(uintptr_t)d_cptr, (int64_t)(uintptr_t)d_cobs,
                  (int64_t)(uintptr_t)d_cprod, (int64_t)(uintptr_t)d_w, wstride, nprior, dpbits,
-                 (int64_t)(uintptr_t)d_pseg, nseg, (int64_t)(uintptr_t)d_active},
+                 (int64_t)(uintptr_t)d_pseg, nseg, (int64_t)(uintptr_t)d_active, per},
                 [&] {
                   fill();
-                  if (persist_) run_factor_persist(B, nullptr, 0, d_active, nseg);
-                  else run_factor_levels(B, pol);
+                  if (per) {
+                    run_factor_persist(B, nullptr, 0, d_active, nseg);
+                  } else {
+                    const DevSym plain = ds_;
+                    if (d_active) {  // the level kernels read the mask through the device view
+                      ds_.active = d_active;
+                      ds_.fseg = d_fseg_.p;
+                      ds_.nseg = nseg;
+                    }
+                    run_factor_levels(B, pol);
+                    ds_ = plain;
+                  }
                 });
 }
 
@@ -926,8 +994,10 @@ void GpuFactor::solve(double* d_x, int64_t xstride, int B, int slot0) {
   const int64_t fs = ftotal_;
   const double* Fp = F_.p + (int64_t)slot0 * fs;
   dim3 gp(cdiv(n, 256) > 1024 ? 1024 : cdiv(n, 256), B);
-  if (solve_persist_) {
-    launch_cached({3, B, (int64_t)(uintptr_t)d_x, xstride, slot0}, [&] {
+  auto pa = persist_at_.find(B);
+  const bool per = solve_persist_ && (persist_mode_ == 2 || (pa != persist_at_.end() && pa->second));
+  if (per) {
+    launch_cached({3, B, (int64_t)(uintptr_t)d_x, xstride, slot0, 1}, [&] {
       const int ns = (int)sym_.nsuper;
       k_permute_in<<<gp, 256, 0, stream_>>>(n, d_perm_.p, d_x, xstride, xp_.p);
       INLA_CUDA(cudaMemsetAsync(d_sstate_.p + 1, 0, sizeof(int) * (1 + 2 * (size_t)B * ns), stream_));

@@ -34,8 +34,9 @@ void* device_alloc(size_t bytes);
 void device_free(void* p);
 void device_release_cached();
 
-// Default schedule of the engines built from now on: persistent (true) or level launches.
-void set_persistent_default(bool on);
+// Schedule of the engines built from now on: 0 level launches, 1 measured per batch size, 2
+// persistent wherever it fits.
+void set_persistent_default(int mode);
 
 // Small RAII device buffer.
 template <class T>
@@ -121,9 +122,9 @@ class GpuFactor {
                     const int* d_pseg = nullptr, int nseg = 1, const unsigned char* d_active = nullptr);
   // Model of every front when the pattern holds independent models block-diagonally: lets
   // factor_model skip the fronts of inactive (problem, model) pairs (d_active [B][nseg]),
-  // which then keep their previous factor. Honoured by the persistent schedule only.
+  // which then keep their previous factor.
   void set_front_groups(const std::vector<int>& fseg);
-  bool can_skip_groups() const { return persist_ && d_fseg_.p != nullptr; }
+  bool can_skip_groups() const { return d_fseg_.p != nullptr; }
   // Device view of the symbolic analysis (pivot offsets, permutation, ...).
   const DevSym& dev_sym() const { return ds_; }
   // Front offset of every input entry's lower twin (both triangles), for
@@ -158,6 +159,9 @@ class GpuFactor {
   // launches). After a synchronization point, check_schedule() throws if a dependency wait
   // of an earlier persistent launch ran out (and clears the record).
   bool persistent() const { return persist_; }
+  // Whether factorizations (and solves) at batch size B use the persistent launch: the mode's
+  // fixed answer, or measured once per structure and B (see gpu_factor.cu).
+  bool use_persist(int B, const std::function<void()>& fill);
   void check_schedule();
   // Diagnostic: one persistent launch whose dependencies can never complete, with a wait
   // limit of limit_ms; returns the error code the launch recorded (1: a wait ran out) after
@@ -209,6 +213,8 @@ class GpuFactor {
   int64_t launches_ = 0;
   // persistent schedule
   bool persist_ = false;
+  int persist_mode_ = 1;
+  std::map<int, bool> persist_at_;  // measured choice per batch size
   int persist_smem_ = 0, persist_grid_ = 0, persist_groups_ = 0;
   long long persist_limit_ns_ = 2000000000LL;
   DBuf<int> d_pgstart_, d_ptask_, d_ptiny_, d_ptotal_, d_plid_, d_pstate_;  // pstate: err, head, prog[B][ns]

@@ -159,6 +159,7 @@ __host__ __device__ constexpr int small_factor_smem(int m) {
 template <int NT>
 __device__ __forceinline__ void factor_small_body(const DevSym& S, int s, int b, double* __restrict__ F,
                                                   int64_t fstride, double* sm) {
+  if (front_skipped(S, s, b)) return;
   double* Fb = F + (int64_t)b * fstride;
   const int k = sn_k(S, s), m = sn_m(S, s);
   const int lda = dense_ld(m), uld = dense_uld(m);
@@ -238,6 +239,7 @@ constexpr int kTinyLd = kTinyM + 1;
 // and R [kTinyM] (ints). Only warp-level synchronization inside.
 __device__ __forceinline__ void factor_tiny_warp(const DevSym& S, int s, int b, double* __restrict__ F,
                                                  int64_t fstride, double* A, double* U, int* R) {
+  if (front_skipped(S, s, b)) return;
   const int lane = threadIdx.x & 31;
   double* Fb = F + (int64_t)b * fstride;
   const int k = sn_k(S, s), m = sn_m(S, s);

@@ -58,6 +58,7 @@ constexpr int kGatherCols = 8;
 __device__ __forceinline__ void gather8_body(const DevSym& S, int s, int b, int z, double* __restrict__ F,
                                              int64_t fstride, int gcols, const int64_t* __restrict__ gptr,
                                              const int2* __restrict__ grng, double* gsl) {
+  if (front_skipped(S, s, b)) return;
   const int k = lg_k(S, s), m = lg_m(S, s);
   const int c0 = z * gcols;
   if (c0 >= m) return;
@@ -120,12 +121,11 @@ __global__ void __launch_bounds__(256) k_gather8(DevSym S, const int* __restrict
 
 // Sigma restricted to the below-rows of s, gathered from the parent's Sigma
 // front into the trailing block (lower triangle), columns [c0, c1) of it.
-__global__ void __launch_bounds__(256) k_si_gather8(DevSym S, const int* __restrict__ list, double* __restrict__ Sg,
-                                                    int64_t fstride) {
-  const int s = list[blockIdx.x], b = blockIdx.y;
+__device__ __forceinline__ void si_gather8_body(const DevSym& S, int s, int b, int z, double* __restrict__ Sg,
+                                                int64_t fstride) {
   const int k = lg_k(S, s), m = lg_m(S, s), r = m - k;
   if (r == 0) return;
-  const int c0 = blockIdx.z * kGatherCols;
+  const int c0 = z * kGatherCols;
   if (c0 >= r) return;
   const int c1 = min(c0 + kGatherCols, r);
   const int p = S.parent[s];
@@ -160,6 +160,11 @@ __global__ void __launch_bounds__(256) k_si_gather8(DevSym S, const int* __restr
   }
 }
 
+__global__ void __launch_bounds__(256) k_si_gather8(DevSym S, const int* __restrict__ list, double* __restrict__ Sg,
+                                                    int64_t fstride) {
+  si_gather8_body(S, list[blockIdx.x], blockIdx.y, blockIdx.z, Sg, fstride);
+}
+
 // The factored diagonal block goes to dcache[(list index, problem)] (written by
 // CTA 0): the other CTAs of this launch still read the unfactored block from
 // the front, so it is copied into the front by k_update64 of the same step.
@@ -173,7 +178,8 @@ __global__ void __launch_bounds__(256) k_si_gather8(DevSym S, const int* __restr
 __device__ __forceinline__ void panel64_body(const DevSym& S, int s, int b, int z, int j0, int rpc,
                                              double* __restrict__ F, int64_t fstride, double* __restrict__ dc,
                                              double* __restrict__ linv, double* smem64) {
-  constexpr int ld = kLd64;
+  constexpr int ld = kLd64;  if (front_skipped(S, s, b)) return;
+
   double* Ds = smem64;         // [64 cols][ld]: diagonal block, factored in place; then row sub-blocks
   double* Li = Ds + kB64 * ld; // L_JJ^-1, then Bm[u + t*ld] = Li[t][u] / d_t
   double* U = Li + kB64 * ld;  // [16][kULd64] scratch of cta_ldlt, then 1 / d_t
@@ -284,6 +290,7 @@ constexpr int kRowsSmem = (2 * kB64 * kLd64 + kB64) * 8;
 __device__ __forceinline__ void rows64_body(const DevSym& S, int s, int b, int z, int j0, double* __restrict__ F,
                                             int64_t fstride, const double* __restrict__ dc,
                                             const double* __restrict__ linv, double* smr) {
+  if (front_skipped(S, s, b)) return;
   constexpr int ld = kLd64;
   double* Bm = smr;               // Bm[u + t*ld] = L_JJ^-1[t][u] / d_t
   double* Fa = Bm + kB64 * ld;    // Fa[t*ld + r] = F[r0 + r, j0 + t]
@@ -364,6 +371,7 @@ __global__ void __launch_bounds__(128) k_update64(DevSym S, const int* __restric
   double* Bs = smu + kB64 * ld; // Bs[t*ld + j] = L[J0+j, j0+t]
   __shared__ double dsh[kB64];
   const int s = list[blockIdx.x], b = blockIdx.y;
+  if (front_skipped(S, s, b)) return;
   const int k = lg_k(S, s), m = lg_m(S, s);
   if (j0 >= k) return;
   const int w = min(kB64, k - j0);
@@ -689,24 +697,24 @@ constexpr int kSiT = 64;  // rows of A per CTA
 // Shared memory: two chunk buffers (Sa + Lb each, double-buffered with
 // cp.async) and G; L_JJ^-1 (from the inverse-block cache) and L[I,J] reuse the
 // chunk buffers after the GEMM.
-__global__ void __launch_bounds__(256) k_si_gemm64(DevSym S, const int* __restrict__ list, int jb,
-                                                  const double* __restrict__ F, double* __restrict__ Sg,
-                                                  int64_t fstride, double* __restrict__ ppart, int ptiles,
-                                                  const double* __restrict__ linv) {
-  extern __shared__ double smem64[];
+// Row tile z of block jb of front s, problem b (256 threads); pp: this front's and problem's
+// partial-P blocks (tile z at pp + z * 4096).
+__device__ __forceinline__ void si_gemm64_body(const DevSym& S, int s, int b, int z, int jb,
+                                               const double* __restrict__ F, double* __restrict__ Sg,
+                                               int64_t fstride, double* __restrict__ pp_front,
+                                               const double* __restrict__ linv, double* smem64) {
   constexpr int kBuf = 64 * kLd64;  // doubles per chunk buffer (Sa[32][68] + Lb[32][68])
   typedef double Row68[kLd64];  // leading dimension 68 == 4 (mod 16): conflict-free fragments
   // three stage buffers (Sa[32][68] + Lb[32][68] each) for the G loop; afterwards
   // buffer 0 holds G (then X), buffer 1 L_JJ^-1 and buffer 2 L[I,J]
   Row68* Gs = reinterpret_cast<Row68*>(smem64);             // [64][68]: G, then X
   Row68* Lt = reinterpret_cast<Row68*>(smem64 + 2 * kBuf);  // [64][68]: L[I0+l, j0+j]
-  const int s = list[blockIdx.x], b = blockIdx.y;
   const int k = lg_k(S, s), m = lg_m(S, s);
   const int nblk = (k + kB64 - 1) / kB64;
   if (jb >= nblk) return;
   const int bi = nblk - 1 - jb;
   const int j0 = bi * kB64, j1 = min(k, j0 + kB64), w = j1 - j0;
-  const int I0 = j1 + blockIdx.z * kSiT;
+  const int I0 = j1 + z * kSiT;
   if (I0 >= m) return;
   const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
   double* Ss = Sg + (int64_t)b * fstride + S.fptr[s];
@@ -865,7 +873,7 @@ __global__ void __launch_bounds__(256) k_si_gemm64(DevSym S, const int* __restri
         for (int q = 0; q < 2; ++q) mma884(pa[a][q][0], pa[a][q][1], af[a], bf[q]);
     }
   }
-  double* pp = ppart + (((int64_t)blockIdx.x * gridDim.y + b) * ptiles + blockIdx.z) * (kB64 * kB64);
+  double* pp = pp_front + (int64_t)z * (kB64 * kB64);
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -874,19 +882,27 @@ __global__ void __launch_bounds__(256) k_si_gemm64(DevSym S, const int* __restri
       for (int h = 0; h < 2; ++h) pp[(wr + a * 8 + g) * kB64 + wc + q * 8 + tg * 2 + h] = pa[a][q][h];
 }
 
-__global__ void __launch_bounds__(256) k_si_diag64(DevSym S, const int* __restrict__ list, int jb,
+__global__ void __launch_bounds__(256) k_si_gemm64(DevSym S, const int* __restrict__ list, int jb,
                                                   const double* __restrict__ F, double* __restrict__ Sg,
-                                                  int64_t fstride, const double* __restrict__ ppart, int ptiles,
+                                                  int64_t fstride, double* __restrict__ ppart, int ptiles,
                                                   const double* __restrict__ linv) {
-  // Sigma_JJ = L^-T (D^-1 L^-1 - P), L = L_JJ unit lower, P = L[A,J]^T Sigma[A,J]
-  // (the closed form of the in-block Takahashi recurrence), with L^-1 from the
-  // inverse-block cache and the product as a tensor-core GEMM.
   extern __shared__ double smem64[];
+  double* pp = ppart + ((int64_t)blockIdx.x * gridDim.y + blockIdx.y) * ptiles * (kB64 * kB64);
+  si_gemm64_body(S, list[blockIdx.x], blockIdx.y, blockIdx.z, jb, F, Sg, fstride, pp, linv, smem64);
+}
+
+// Sigma_JJ = L^-T (D^-1 L^-1 - P), L = L_JJ unit lower, P = L[A,J]^T Sigma[A,J]
+// (the closed form of the in-block Takahashi recurrence), with L^-1 from the
+// inverse-block cache and the product as a tensor-core GEMM. Block jb of front s, problem b
+// (256 threads); pp_front as in si_gemm64_body.
+__device__ __forceinline__ void si_diag64_body(const DevSym& S, int s, int b, int jb, const double* __restrict__ F,
+                                               double* __restrict__ Sg, int64_t fstride,
+                                               const double* __restrict__ pp_front,
+                                               const double* __restrict__ linv, double* smem64) {
   constexpr int ld = kB64 + 1;
   double* Pm = smem64;            // P, then M = D^-1 L^-1 - P  (Pm[r + c*ld] = entry (r, c))
   double* Ld = Pm + kB64 * ld;    // L_JJ with D on the diagonal
   double* Li = Ld + kB64 * ld;    // L_JJ^-1
-  const int s = list[blockIdx.x], b = blockIdx.y;
   const int k = lg_k(S, s), m = lg_m(S, s);
   const int nblk = (k + kB64 - 1) / kB64;
   if (jb >= nblk) return;
@@ -895,7 +911,7 @@ __global__ void __launch_bounds__(256) k_si_diag64(DevSym S, const int* __restri
   const int ntiles = (m - j1 + kSiT - 1) / kSiT;
   const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
   double* Ss = Sg + (int64_t)b * fstride + S.fptr[s];
-  const double* pp = ppart + ((int64_t)blockIdx.x * gridDim.y + b) * ptiles * (kB64 * kB64);
+  const double* pp = pp_front;
   const double* lc = linv_block(S, linv, b, s, bi);
   for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) {
     const int c = e >> 6, r = e & 63;
@@ -958,6 +974,15 @@ __global__ void __launch_bounds__(256) k_si_diag64(DevSym S, const int* __restri
           if (r < w && c < w && r >= c) Ss[(j0 + r) + (int64_t)(j0 + c) * m] = acc[a][q][h];
         }
   }
+}
+
+__global__ void __launch_bounds__(256) k_si_diag64(DevSym S, const int* __restrict__ list, int jb,
+                                                  const double* __restrict__ F, double* __restrict__ Sg,
+                                                  int64_t fstride, const double* __restrict__ ppart, int ptiles,
+                                                  const double* __restrict__ linv) {
+  extern __shared__ double smem64[];
+  const double* pp = ppart + ((int64_t)blockIdx.x * gridDim.y + blockIdx.y) * ptiles * (kB64 * kB64);
+  si_diag64_body(S, list[blockIdx.x], blockIdx.y, jb, F, Sg, fstride, pp, linv, smem64);
 }
 
 }  // namespace

@@ -65,11 +65,6 @@ struct PersistArgs {
   const int64_t* gptr;      // extend-add chunk table of this schedule
   const int2* grng;
   long long limit_ns;       // longest wait for one dependency
-  // optional: fronts of inactive (problem, model) pairs are skipped (counted done, left as
-  // they are); active [B][nseg], fseg [ns] the model of each front
-  const unsigned char* active;
-  const int* fseg;
-  int nseg;
 };
 
 constexpr int kPersistThreads = 256;
@@ -121,6 +116,7 @@ __device__ bool wait_children(const PersistArgs& a, int s, int b) {
 __device__ __forceinline__ void update64w8_body(const DevSym& S, int s, int b, int tile, int j0,
                                                 double* __restrict__ F, int64_t fstride,
                                                 const double* __restrict__ dc, double* smu) {
+  if (front_skipped(S, s, b)) return;
   constexpr int ld = kLd64;
   double* As = smu;              // As[t*ld + i] = L[I0+i, j0+t]
   double* Bs = smu + kB64 * ld;  // Bs[t*ld + j] = L[J0+j, j0+t]
@@ -244,12 +240,11 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_factor_persist(PersistAr
     }
     __syncthreads();
     if (!sh_go) break;
-    const bool skip = a.active && T.type != PT_TINY && !a.active[(int64_t)b * a.nseg + a.fseg[T.s]];
-    if (!skip) switch (T.type) {
+    // (the bodies skip the fronts of inactive (problem, model) pairs themselves: DevSym::active)
+    switch (T.type) {
       case PT_TINY: {
         const int warp = threadIdx.x >> 5;
-        if (warp < T.sub &&
-            (!a.active || a.active[(int64_t)b * a.nseg + a.fseg[a.tiny_list[T.s + warp]]])) {
+        if (warp < T.sub) {
           double* A = psm + warp * kPersistTinySlice;
           factor_tiny_warp(S, a.tiny_list[T.s + warp], b, a.F, a.fstride, A, A + kTinyM * kTinyLd,
                            reinterpret_cast<int*>(A + kTinyM * kTinyLd + kTinyM));

@@ -34,7 +34,7 @@ def test_group_adjoint_vs_oracle_fd_small():
 
     def mlik(tt):
         q = p.model.matrix(models.group_coefs(tt)[0])
-        return O.laplace(q, p.a, "binomial", p.y, p1=p.ntrials, constraints=p.constraint, tol=1e-12)["mlik"]
+        return O.laplace(q, p.a, "binomial", p.y, p1=p.ntrials, constraints=p.constraint, tol=1e-10)["mlik"]
 
     h = 1e-4
     fd = np.array([(mlik(t + h * e) - mlik(t - h * e)) / (2 * h) for e in np.eye(4)])

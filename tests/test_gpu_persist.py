@@ -17,7 +17,7 @@ pytestmark = pytest.mark.gpu
 
 
 def make(q, B, persistent, ordering=_lib.ORDER_ND):
-    _lib.check(_lib.lib().inla_set_persistent_schedule(1 if persistent else 0))
+    _lib.check(_lib.lib().inla_set_persistent_schedule(2 if persistent else 0))
     try:
         bs = BatchSolver(q, max_batch=B, ordering=ordering)
     finally:
