@@ -405,7 +405,8 @@ typedef double (*inla_log_prior_fn)(const double* theta, int m, double* grad, vo
 
 typedef struct {
   int mode_search; /* 0 Nelder-Mead on values (reference), 1 BFGS on adjoint gradients,
-                      2 batched Newton (adjoint gradients + FD-of-gradient Hessians, one batch per iteration) */
+                      2 batched Newton (adjoint gradients + central FD-of-gradient Hessians, 2m + 1 points
+                      per batch), 3 the same with forward differences (m + 1 points per batch) */
   int batched;     /* 0 one theta-point per evaluation (plain drop-in), 1 batched theta-sets */
   int strategy;    /* 0 CCD, 1 grid (m <= 2; CCD f0 = 2.5 above) */
   double f0;       /* CCD f0 / grid step (0 = 1.0) */

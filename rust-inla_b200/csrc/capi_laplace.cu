@@ -301,7 +301,8 @@ int inla_fit(inla_laplace* h, int m, const double* theta0, inla_theta_map_fn map
              void* user, const inla_fit_options* opt, double* mode, double* hessian, double* latent_mean,
              double* latent_var, double* node_theta, double* node_weight, double* info) {
   try {
-    if (!h || !h->eng || (!theta0 && m > 0) || !map || !prior || !opt || m < 0 || m > 5)
+    if (!h || !h->eng || (!theta0 && m > 0) || !map || !prior || !opt || m < 0 || m > 5 || opt->mode_search < 0 ||
+        opt->mode_search > 3)
       return fail(INLA_ERR_INVALID, "invalid argument");
     LaplaceEngine& E = *h->eng;
     ThetaMap tm = [&](const double* th, double* c, double* dc, double* s, double* ds) {

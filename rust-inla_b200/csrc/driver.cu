@@ -403,14 +403,15 @@ void InlaDriver::bfgs(std::vector<double>& x, const FitOptions& opt, int& iters)
 // ---------------------------------------------------------------------------
 
 void InlaDriver::eval_stencils(const std::vector<std::vector<double>>& centers, double h, std::vector<double>& f,
-                               std::vector<double>& g, std::vector<double>& H) {
-  const int m = m_, C = (int)centers.size(), per = 1 + 2 * m;
+                               std::vector<double>& g, std::vector<double>& H, bool one_sided) {
+  const int m = m_, C = (int)centers.size(), per = one_sided ? 1 + m : 1 + 2 * m;
   std::vector<double> pts;
   pts.reserve((size_t)C * per * m);
   for (const auto& c : centers) {
     pts.insert(pts.end(), c.begin(), c.end());
     for (int i = 0; i < m; ++i)
       for (double s : {1.0, -1.0}) {
+        if (one_sided && s < 0) continue;
         std::vector<double> t(c);
         t[i] += s * h;
         pts.insert(pts.end(), t.begin(), t.end());
@@ -428,10 +429,12 @@ void InlaDriver::eval_stencils(const std::vector<std::vector<double>>& centers, 
     bool bad = !(fk[b0] < 1e11);
     for (int i = 0; i < m; ++i) g[(size_t)c * m + i] = gk[(size_t)b0 * m + i];
     for (int i = 0; i < m; ++i) {
-      const int kp = b0 + 1 + 2 * i, km = kp + 1;
+      // central differences of the gradient, or forward differences from the centre
+      const int kp = one_sided ? b0 + 1 + i : b0 + 1 + 2 * i, km = one_sided ? b0 : kp + 1;
+      const double den = one_sided ? h : 2.0 * h;
       if (!(fk[kp] < 1e11) || !(fk[km] < 1e11)) bad = true;
       for (int j = 0; j < m; ++j)
-        H[(size_t)c * m * m + i * m + j] = (gk[(size_t)kp * m + j] - gk[(size_t)km * m + j]) / (2.0 * h);
+        H[(size_t)c * m * m + i * m + j] = (gk[(size_t)kp * m + j] - gk[(size_t)km * m + j]) / den;
     }
     double* Hc = &H[(size_t)c * m * m];
     for (int i = 0; i < m; ++i)
@@ -443,8 +446,9 @@ void InlaDriver::eval_stencils(const std::vector<std::vector<double>>& centers, 
 void InlaDriver::newton(std::vector<double>& x, const FitOptions& opt, int& iters) {
   const int m = m_;
   const double h = 1e-3;
+  const bool one_sided = opt.mode_search == 3;  // m + 1 stencil points per candidate instead of 2m + 1
   std::vector<double> f1, g, H;
-  eval_stencils({x}, h, f1, g, H);
+  eval_stencils({x}, h, f1, g, H, one_sided);
   double f = f1[0];
   double delta = 2.0;  // trust bound on max |step| (theta lives on log scales: a factor e^2 per step)
   iters = 0;
@@ -484,7 +488,7 @@ void InlaDriver::newton(std::vector<double>& x, const FitOptions& opt, int& iter
     for (int k = 0; k < 3 && best < 0; ++k) {
       xc = x;
       for (int i = 0; i < m; ++i) xc[i] += kA[k] * p[i];
-      eval_stencils({xc}, h, fc, gc, Hc);
+      eval_stencils({xc}, h, fc, gc, Hc, one_sided);
       if (fc[0] < 1e11 && fc[0] <= f + 1e-4 * kA[k] * slope) best = k;
     }
     if (best < 0) {
@@ -661,7 +665,7 @@ void InlaDriver::fit(const double* theta0, const FitOptions& opt, FitResult& out
   int iters = 0;
   if (opt.mode_search == 0) nelder_mead(mode, opt, iters);
   else if (opt.mode_search == 1) bfgs(mode, opt, iters);
-  else newton(mode, opt, iters);
+  else newton(mode, opt, iters);  // 2: central gradient stencil, 3: forward stencil
   out.mode = mode;
   out.mode_iters = iters;
   out.phase_s[0] = since(t0);

@@ -28,6 +28,7 @@ using LogPrior = std::function<double(const double* theta, double* grad)>;
 
 struct FitOptions {
   int mode_search = 0;  // 0 Nelder-Mead (reference), 1 BFGS on adjoint gradients, 2 batched Newton
+                        // (central FD-of-gradient Hessian), 3 batched Newton (forward FD-of-gradient)
   int batched = 0;      // 0: one theta-point per evaluation; 1: batched theta-sets
   int strategy = 0;     // 0 CCD, 1 grid
   double f0 = 1.0;      // CCD f0 (reference default 1.0) / grid step
@@ -79,7 +80,7 @@ class InlaDriver {
   void bfgs(std::vector<double>& theta, const FitOptions& opt, int& iters);
   void newton(std::vector<double>& theta, const FitOptions& opt, int& iters);
   void eval_stencils(const std::vector<std::vector<double>>& centers, double h, std::vector<double>& f,
-                     std::vector<double>& g, std::vector<double>& H);
+                     std::vector<double>& g, std::vector<double>& H, bool one_sided = false);
   void fd_hessian(const std::vector<double>& mode, double h, bool batched, std::vector<double>& H);
   void grad_hessian(const std::vector<double>& mode, double h, bool batched, std::vector<double>& H);
   void fit_single_node(FitResult& out);  // m = 0

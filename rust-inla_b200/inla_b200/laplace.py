@@ -236,7 +236,7 @@ class LaplaceModel:
             fprior = C.cast(lib().inla_log_prior_set, LOG_PRIOR)
             user = C.cast(C.pointer(ps), C.c_void_p)
         keep.append(fprior)
-        opt = FitOptions(mode_search={"nm": 0, "bfgs": 1, "newton": 2}[mode_search], batched=int(bool(batched)),
+        opt = FitOptions(mode_search={"nm": 0, "bfgs": 1, "newton": 2, "newton1": 3}[mode_search], batched=int(bool(batched)),
                          strategy={"ccd": 0, "grid": 1}[strategy], f0=float(f0),
                          hessian={"fd": 0, "grad": 1}[hessian], max_iter=int(max_iter), tol=float(tol), nm_step=0.0)
         if cancel is not None:
