@@ -140,52 +140,25 @@ __device__ __forceinline__ void tri_decode(int task, int& I, int& J) {
 // ws: kDenseScratch doubles. Ends with a barrier.
 template <bool kInv>
 __device__ __forceinline__ void cta_ldlt(double* A, int lda, int m, int kp, double* Li, int ldi, double* U, int ldu, double* ws) {
-  // Look-ahead schedule (at least two warps): after the panel of block o is formed, warp 0
-  // applies the block's trailing update to the next 16 x 16 diagonal block only and factors it
-  // with warp_ldlt16 while the other warps apply the rest of the trailing update (and the
-  // inverse accumulation). Every entry gets the same products in the same order as the
-  // plain right-looking loop, so the factor is unchanged; the serial pivot chain of the next
-  // block runs under the trailing update instead of after it (two CTA barriers per block).
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int g = lane >> 2, tg = lane & 3;
   double* xbuf = ws;
   double* lam = ws + 64;
   double* dv = lam + 16 * kLamLd;
   double* di = dv + 16;
-  // 8 x 8 trailing tile (I, J) of block o: A[i, jc..jc+1] -= L_bk U_bk^T
-  auto trailing_tile = [&](int o, int w, int base, int I, int J) {
-    const int i = base + 8 * I + g, jb = 8 * J + g;
-    double c0 = 0.0, c1 = 0.0;
-#pragma unroll
-    for (int kk = 0; kk < 16; kk += 4) {
-      const int u = kk + tg;
-      const double a = (u < w && i < m) ? A[i + (int64_t)(o + u) * lda] : 0.0;
-      const double b = U[u * ldu + jb];
-      dmma884(c0, c1, a, b);
-    }
-    const int jc = base + 8 * J + 2 * tg;
-    if (i < m) {
-      if (jc < m && i >= jc) A[i + (int64_t)jc * lda] -= c0;
-      if (jc + 1 < m && i >= jc + 1) A[i + (int64_t)(jc + 1) * lda] -= c1;
-    }
-  };
-  // warp 0: factor the diagonal block at o (width w) and store its inverse block (kInv)
-  auto factor_diag = [&](int o, int w) {
-    warp_ldlt16(A + o + (int64_t)o * lda, lda, w, lam, dv, di, xbuf);
-    if (kInv) {
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const int e = lane + 32 * q, rr = e & 15, cc = e >> 4;
-        if (rr < w && cc < w) Li[(o + rr) + (int64_t)(o + cc) * ldi] = lam[rr + cc * kLamLd];
-      }
-    }
-  };
-  if (kp > 0) {
-    if (warp == 0) factor_diag(0, min(16, kp));
-    __syncthreads();
-  }
   for (int o = 0; o < kp; o += 16) {
     const int w = min(16, kp - o);
+    if (warp == 0) {
+      warp_ldlt16(A + o + (int64_t)o * lda, lda, w, lam, dv, di, xbuf);
+      if (kInv) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int e = lane + 32 * q, rr = e & 15, cc = e >> 4;
+          if (rr < w && cc < w) Li[(o + rr) + (int64_t)(o + cc) * ldi] = lam[rr + cc * kLamLd];
+        }
+      }
+    }
+    __syncthreads();
     const int base = o + w, nb = m - base, T = (nb + 7) >> 3;
     // U_bk = A_bk Lam^T and L_bk = U_bk D^-1 (8-row tasks, 16 columns each)
     for (int task = warp; task < T; task += nw) {
@@ -234,45 +207,44 @@ __device__ __forceinline__ void cta_ldlt(double* A, int lda, int m, int kp, doub
     }
     __syncthreads();
     if (nb <= 0) break;
+    // trailing update A_bb -= L_bk U_bk^T (lower 8 x 8 tiles)
     const int ntask = T * (T + 1) / 2;
-    // the next block's diagonal tiles (I, J < 2): tasks 0..2 in the triangular order
-    const bool ahead = base < kp && nw > 1;
-    const int nahead = ahead ? min(ntask, 3) : 0;
-    if (ahead && warp == 0) {
-      for (int task = 0; task < nahead; ++task) {
-        int I, J;
-        tri_decode(task, I, J);
-        trailing_tile(o, w, base, I, J);
-      }
-      __syncwarp();
-      factor_diag(base, min(16, kp - base));
-    } else {
-      // trailing update A_bb -= L_bk U_bk^T (lower 8 x 8 tiles) without the look-ahead tiles
-      const int w0 = ahead ? warp - 1 : warp, nwk = ahead ? nw - 1 : nw;
-      for (int task = nahead + w0; task < ntask; task += nwk) {
-        int I, J;
-        tri_decode(task, I, J);
-        trailing_tile(o, w, base, I, J);
-      }
-      if (kInv) {
-        // Li_b[:, :base] -= L_bk Li_k[:, :base]  (rows of later blocks inside kp)
-        const int nbi = kp - base, Ti = (nbi + 7) >> 3, Tc = (base + 7) >> 3;
-        for (int task = w0; task < Ti * Tc; task += nwk) {
-          const int I = task / Tc, Jc = task - I * Tc;
-          const int i = base + 8 * I + g;
-          double c0 = 0.0, c1 = 0.0;
+    for (int task = warp; task < ntask; task += nw) {
+      int I, J;
+      tri_decode(task, I, J);
+      const int i = base + 8 * I + g, jb = 8 * J + g;
+      double c0 = 0.0, c1 = 0.0;
 #pragma unroll
-          for (int kk = 0; kk < 16; kk += 4) {
-            const int u = kk + tg;
-            const double a = (u < w && i < kp) ? A[i + (int64_t)(o + u) * lda] : 0.0;
-            const double b = (u < w) ? Li[(o + u) + (int64_t)(8 * Jc + g) * ldi] : 0.0;
-            dmma884(c0, c1, a, b);
-          }
-          const int jc = 8 * Jc + 2 * tg;
-          if (i < kp) {
-            if (jc < base) Li[i + (int64_t)jc * ldi] -= c0;
-            if (jc + 1 < base) Li[i + (int64_t)(jc + 1) * ldi] -= c1;
-          }
+      for (int kk = 0; kk < 16; kk += 4) {
+        const int u = kk + tg;
+        const double a = (u < w && i < m) ? A[i + (int64_t)(o + u) * lda] : 0.0;
+        const double b = U[u * ldu + jb];
+        dmma884(c0, c1, a, b);
+      }
+      const int jc = base + 8 * J + 2 * tg;
+      if (i < m) {
+        if (jc < m && i >= jc) A[i + (int64_t)jc * lda] -= c0;
+        if (jc + 1 < m && i >= jc + 1) A[i + (int64_t)(jc + 1) * lda] -= c1;
+      }
+    }
+    if (kInv) {
+      // Li_b[:, :base] -= L_bk Li_k[:, :base]  (rows of later blocks inside kp)
+      const int nbi = kp - base, Ti = (nbi + 7) >> 3, Tc = (base + 7) >> 3;
+      for (int task = warp; task < Ti * Tc; task += nw) {
+        const int I = task / Tc, Jc = task - I * Tc;
+        const int i = base + 8 * I + g;
+        double c0 = 0.0, c1 = 0.0;
+#pragma unroll
+        for (int kk = 0; kk < 16; kk += 4) {
+          const int u = kk + tg;
+          const double a = (u < w && i < kp) ? A[i + (int64_t)(o + u) * lda] : 0.0;
+          const double b = (u < w) ? Li[(o + u) + (int64_t)(8 * Jc + g) * ldi] : 0.0;
+          dmma884(c0, c1, a, b);
+        }
+        const int jc = 8 * Jc + 2 * tg;
+        if (i < kp) {
+          if (jc < base) Li[i + (int64_t)jc * ldi] -= c0;
+          if (jc + 1 < base) Li[i + (int64_t)(jc + 1) * ldi] -= c1;
         }
       }
     }
