@@ -7,8 +7,9 @@
 //               stores the factored block (dcache) and L_JJ^-1 (the inverse-
 //               block cache, reused by the selected inverse); each CTA forms
 //               its 64 rows L_i = F_i L_JJ^-T D_J^-1 as one tensor-core GEMM;
-//   k_update64  F[i,j] -= sum_{t in J} L_it d_t L_jt on 64x64 tiles of the lower
-//               trailing matrix (tensor-core tiles, operands staged with cp.async).
+//   update      F[i,j] -= sum_{t in J} L_it d_t L_jt on 64x64 tiles of the lower
+//               trailing matrix (tensor-core tiles, operands staged with cp.async;
+//               update64w8_body in snode_persist.cuh, launched as k_update64w8).
 // Selected inverse, per block J from right to left (A = rows after J):
 //   k_si_gemm64 G = Sigma[A,A] L[A,J], X = -G L_JJ^-1 (cached inverse block),
 //               Sigma[A,J] = X, and the tile's partial P = L[I,J]^T X[I,J];
@@ -31,7 +32,6 @@ constexpr int kPanelRows = 64;   // rows per panel GEMM sub-block
 constexpr int kLd64 = dense_ld(kB64);
 constexpr int kULd64 = dense_uld(kB64);
 constexpr int kPanelSmem = (2 * kB64 * kLd64 + 16 * kULd64 + kDenseScratch) * 8;
-constexpr int kUpdSmem = 2 * kB64 * kLd64 * 8;
 constexpr int kSiGemmSmem = 3 * 64 * kLd64 * 8;  // three stage buffers
 constexpr int kSiDiagSmem = 3 * kB64 * (kB64 + 1) * 8;
 
@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(256) k_si_gather8(DevSym S, const int* __restr
 
 // The factored diagonal block goes to dcache[(list index, problem)] (written by
 // CTA 0): the other CTAs of this launch still read the unfactored block from
-// the front, so it is copied into the front by k_update64 of the same step.
+// the front, so it is copied into the front by the trailing update (tile 0) of the same step.
 // Each CTA: blocked LDL^T + inverse of the diagonal block, then the rows
 // [r0, r0 + rpc) (rpc a multiple of 64) in 64-row sub-blocks, each
 // X = F_rows (L_JJ^-T D^-1) as one tensor-core GEMM. The row sub-blocks are
@@ -362,104 +362,6 @@ __global__ void __launch_bounds__(256) k_rows64(DevSym S, const int* __restrict_
 }
 
 constexpr int kUT64 = 64;
-__global__ void __launch_bounds__(128) k_update64(DevSym S, const int* __restrict__ list, int j0,
-                                                 double* __restrict__ F, int64_t fstride,
-                                                 const double* __restrict__ dcache) {
-  extern __shared__ double smu[];
-  constexpr int ld = kLd64;
-  double* As = smu;             // As[t*ld + i] = L[I0+i, j0+t]
-  double* Bs = smu + kB64 * ld; // Bs[t*ld + j] = L[J0+j, j0+t]
-  __shared__ double dsh[kB64];
-  const int s = list[blockIdx.x], b = blockIdx.y;
-  if (front_skipped(S, s, b)) return;
-  const int k = lg_k(S, s), m = lg_m(S, s);
-  if (j0 >= k) return;
-  const int w = min(kB64, k - j0);
-  const int c = j0 + w;
-  const int T = m - c;
-  const double* dc = dcache + ((int64_t)blockIdx.x * gridDim.y + b) * (kB64 * kB64);
-  double* Fs = F + (int64_t)b * fstride + S.fptr[s];
-  if (blockIdx.z == 0) {  // factored diagonal block -> front
-    double* D0 = Fs + j0 + (int64_t)j0 * m;
-    for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
-      const int cc = e / w, r = e - cc * w;
-      if (r >= cc) D0[r + (int64_t)cc * m] = dc[r + cc * kB64];
-    }
-  }
-  if (T <= 0) return;
-  const int nt = (T + kUT64 - 1) / kUT64;
-  const int tile = blockIdx.z;
-  if (tile >= nt * (nt + 1) / 2) return;
-  int J = 0, rem = tile;
-  while (rem >= nt - J) {
-    rem -= nt - J;
-    ++J;
-  }
-  const int I = J + rem;
-  const int I0 = c + I * kUT64, J0 = c + J * kUT64;
-  const double* Lb = Fs + (int64_t)j0 * m;
-  for (int e = threadIdx.x; e < kB64 * kUT64; e += blockDim.x) {
-    const int t = e >> 6, ii = e & 63;
-    const double* col = Lb + (int64_t)t * m;
-    if (t < w && I0 + ii < m) cp_async8(&As[t * ld + ii], col + I0 + ii);
-    else As[t * ld + ii] = 0.0;
-    if (t < w && J0 + ii < m) cp_async8(&Bs[t * ld + ii], col + J0 + ii);
-    else Bs[t * ld + ii] = 0.0;
-  }
-  cp_async_commit();
-  for (int t = threadIdx.x; t < kB64; t += blockDim.x) dsh[t] = t < w ? dc[t + t * kB64] : 0.0;
-  cp_async_wait<0>();
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wi = (warp & 1) * 32, wj = (warp >> 1) * 32;
-  const int g = lane >> 2, tg = lane & 3;
-  double acc[4][4][2];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int q = 0; q < 4; ++q) acc[a][q][0] = acc[a][q][1] = 0.0;
-  // only the block's w columns contribute; warps whose 32 x 32 sub-tile lies above
-  // the diagonal or past the last row have nothing to compute
-  const int wk = (I0 + wi >= m || J0 + wj >= m || (I == J && wj > wi)) ? 0 : (w + 3) & ~3;
-#pragma unroll 2
-  for (int kk = 0; kk < wk; kk += 4) {
-    double af[4], bf[4];
-    const double dk = dsh[kk + tg];
-#pragma unroll
-    for (int a = 0; a < 4; ++a) af[a] = As[(kk + tg) * ld + wi + a * 8 + g];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) bf[q] = Bs[(kk + tg) * ld + wj + q * 8 + g] * dk;
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) mma884(acc[a][q][0], acc[a][q][1], af[a], bf[q]);
-  }
-  // read 16 target entries before writing any (the loads stay in flight together), twice
-#pragma unroll
-  for (int a0 = 0; a0 < 4; a0 += 2) {
-    double cv[2][4][2];
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int i = I0 + wi + (a0 + a) * 8 + g;
-          const int j = J0 + wj + q * 8 + tg * 2 + h;
-          cv[a][q][h] = (i < m && j < m && i >= j) ? Fs[i + (int64_t)j * m] : 0.0;
-        }
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int i = I0 + wi + (a0 + a) * 8 + g;
-          const int j = J0 + wj + q * 8 + tg * 2 + h;
-          if (i < m && j < m && i >= j) Fs[i + (int64_t)j * m] = cv[a][q][h] - acc[a0 + a][q][h];
-        }
-  }
-}
 
 // ---------------------------------------------------------------------------
 // triangular sweeps in 32-column blocks: the diagonal block is solved by one

@@ -112,7 +112,8 @@ __device__ bool wait_children(const PersistArgs& a, int s, int b) {
 }
 
 // Trailing update tile `tile` of block J of front s, problem b, over eight warps (32 x 16
-// warp tiles); the same products in the same order as k_update64.
+// warp tiles): every entry accumulates its products over K in the same order as any other warp
+// tiling of the same step, so the result does not depend on the tiling.
 __device__ __forceinline__ void update64w8_body(const DevSym& S, int s, int b, int tile, int j0,
                                                 double* __restrict__ F, int64_t fstride,
                                                 const double* __restrict__ dc, double* smu) {
