@@ -238,6 +238,14 @@ int inla_solver_check_schedule(const inla_solver* s, int64_t* info3);
  * factorization at a batch size an engine times both schedules and keeps the faster for that
  * structure and size; 2 the persistent schedule wherever it fits. */
 int inla_set_persistent_schedule(int mode);
+/* Process-wide panel form of the level launches for engines created after the call: -1
+ * (default) the autotuner's per-level choice (on the first factorization at a batch size the
+ * level sequence is timed in each form and every level keeps the fastest); 0 split (diagonal
+ * block, rows, trailing update: three launches per 64-column step); 1 fused (every row CTA
+ * factors the diagonal block: two launches); 2 look-ahead (rows, then the trailing update
+ * whose first tile also factors the next diagonal block: two launches). All forms give
+ * bit-identical factors. */
+int inla_set_panel_form(int form);
 /* Diagnostic of the bounded waits: runs the persistent factorization once with completion
  * counts that can never be reached and a wait limit of limit_ms, and returns in *code what
  * the launch recorded (1: a wait ran out and the launch ended). The handle stays usable;

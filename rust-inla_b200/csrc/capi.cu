@@ -401,6 +401,12 @@ int inla_set_persistent_schedule(int mode) {
   return INLA_OK;
 }
 
+int inla_set_panel_form(int form) {
+  if (form < -1 || form > 2) return fail(INLA_ERR_INVALID, "panel form must be -1, 0, 1 or 2");
+  set_panel_form(form);
+  return INLA_OK;
+}
+
 int inla_batch_schedule(inla_batch* h, int* persistent) {
   if (!h || !h->eng || !persistent) return fail(INLA_ERR_INVALID, "null batch handle or output");
   *persistent = h->eng->persistent() ? 1 : 0;

@@ -18,6 +18,12 @@ namespace inla {
 namespace {
 inline int cdiv(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 
+// Panel forms of a level's large fronts (entries of the per-level schedule).
+constexpr char kFormSplit = 0, kFormFused = 1, kFormLookahead = 2, kNumForms = 3;
+// Process-wide panel form for engines built from now on: -1 the autotuner's choice per level
+// (default), otherwise that form at every level.
+std::atomic<int> g_panel_form{-1};
+
 // Trailing-update tile on eight warps (32 x 16 warp tiles; the body the persistent schedule
 // runs too), two CTAs per SM: 16 warps per SM where the four-warp form with 32 x 32 warp tiles
 // fitted 12 (168 registers, 70 KB of staging). Measured on the SPDE 200^2 factorization: 7 %
@@ -28,6 +34,20 @@ __global__ void __launch_bounds__(256, 2) k_update64w8(DevSym S, const int* __re
   extern __shared__ double smu[];
   const double* dc = dcache + ((int64_t)blockIdx.x * gridDim.y + blockIdx.y) * (kB64 * kB64);
   update64w8_body(S, list[blockIdx.x], blockIdx.y, blockIdx.z, j0, F, fstride, dc, smu);
+}
+
+// The same update with look-ahead: tile 0 of every (front, problem) also factors the next
+// diagonal block (D and L into the other cache slot, L^-1 into the inverse-block cache), so the
+// pivot chain of block J + 1 runs while the other tiles of step J are updated and the step
+// after needs no diagonal-block launch. Results are bit-identical to the split form.
+__global__ void __launch_bounds__(256, 2) k_update64la(DevSym S, const int* __restrict__ list, int j0,
+                                                         double* __restrict__ F, int64_t fstride,
+                                                         const double* __restrict__ dcache,
+                                                         double* __restrict__ dcache_next, double* __restrict__ linv) {
+  extern __shared__ double smu[];
+  const int64_t slot = ((int64_t)blockIdx.x * gridDim.y + blockIdx.y) * (kB64 * kB64);
+  update64w8_body<true>(S, list[blockIdx.x], blockIdx.y, blockIdx.z, j0, F, fstride, dcache + slot, smu,
+                        dcache_next + slot, linv);
 }
 
 // Parent columns per extend-add CTA: the m-row slice must fit in shared memory.
@@ -216,6 +236,7 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
     d_grng_.upload(grng, stream_);
   }
 
+  panel_form_ = g_panel_form.load();
   plan_persist();
   const auto ta = std::chrono::steady_clock::now();
   F_.alloc((size_t)max_batch_ * ftotal_);
@@ -230,7 +251,9 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
       nlmax = std::max<int64_t>(nlmax, (int64_t)P.large.size());
       ppmax = std::max<int64_t>(ppmax, (int64_t)P.si_large.size() * cdiv(P.mmax_si_large, kSiT));
     }
-    dcache_.alloc((size_t)nlmax * max_batch_ * kB64 * kB64);
+    // two slots: the look-ahead form factors block J + 1 while step J still reads block J
+    dslot_ = nlmax * max_batch_ * kB64 * kB64;
+    dcache_.alloc((size_t)(2 * dslot_));
     ppart_.alloc((size_t)ppmax * max_batch_ * kB64 * kB64);
   }
   set_smem(k_factor_small<128>, small_factor_smem(kSmallA));
@@ -254,6 +277,7 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
     struct_hash_ = h;
   }
   set_smem(k_update64w8, kPersistUpdSmem);
+  set_smem(k_update64la, kPanelSmem);
   set_smem(k_rows64, kRowsSmem);
   set_smem(k_fwd32<128>, (int)((S.max_m + 2 + 32 * 33) * 8));
   set_smem(k_bwd32<128>, (int)((S.max_m + 2 + 32 * 33) * 8));
@@ -377,6 +401,8 @@ std::map<std::pair<uint64_t, int>, bool> g_sched;
 }  // namespace
 
 void set_persistent_default(int mode) { g_persist_default.store(mode < 0 ? 0 : (mode > 2 ? 2 : mode)); }
+
+void set_panel_form(int form) { g_panel_form.store(form < 0 || form >= kNumForms ? -1 : form); }
 
 // The task queue of the persistent schedule for one problem (host arrays).
 bool make_persist_plan(const Symbolic& S, const std::vector<LevelPlan>& levels, PersistPlan& out) {
@@ -792,16 +818,33 @@ void GpuFactor::run_factor_levels(int B, const std::vector<char>* fuse, cudaEven
       k_gather8<<<dim3(nl, B, cdiv(P.mmax_large, gcols)), 256, gcols * P.mmax_large * 8, stream_>>>(
           ds_, lst, F_.p, fs, gcols, d_gptr_.p, d_grng_.p);
       ++launches_;
+      const int form = fuse ? (*fuse)[li] : -1;
       for (int j0 = 0; j0 < P.kmax_large; j0 += kB64) {
         int rows = P.mmax_large - j0;
+        const int nrb = std::max(1, cdiv(rows, kPanelRows));
+        int nt = cdiv(rows, kUT64);
+        const dim3 ug(nl, B, std::max(1, nt * (nt + 1) / 2));
+        if (form == kFormLookahead) {
+          // block 0 by one CTA per (front, problem); every later diagonal block by tile 0 of
+          // the previous step's update
+          double* cur = dcache_.p + ((j0 / kB64) & 1) * dslot_;
+          double* nxt = dcache_.p + (((j0 / kB64) + 1) & 1) * dslot_;
+          if (j0 == 0) {
+            k_panel64<<<dim3(nl, B, 1), 256, kPanelSmem, stream_>>>(ds_, lst, j0, 0, F_.p, fs, cur, linv_.p);
+            ++launches_;
+          }
+          k_rows64<<<dim3(nl, B, nrb), 256, kRowsSmem, stream_>>>(ds_, lst, j0, F_.p, fs, cur, linv_.p);
+          k_update64la<<<ug, 256, kPanelSmem, stream_>>>(ds_, lst, j0, F_.p, fs, cur, nxt, linv_.p);
+          launches_ += 2;
+          continue;
+        }
         // While every (front, problem, 64-row block) gets its own CTA within about
         // one wave (two CTAs per SM), each row CTA factors the diagonal block
         // itself (one launch). Beyond that, one CTA per (front, problem) factors
         // it and k_rows64 forms the rows from the cached factor (no redundant
         // factorizations).
-        const int nrb = std::max(1, cdiv(rows, kPanelRows));
         const int per = std::max(1, (2 * num_sms_) / std::max(1, nl * B));
-        const bool fused = fuse ? (*fuse)[li] != 0 : per >= nrb;
+        const bool fused = form >= 0 ? form == kFormFused : per >= nrb;
         if (fused) {
           k_panel64<<<dim3(nl, B, nrb), 256, kPanelSmem, stream_>>>(ds_, lst, j0, kPanelRows, F_.p, fs, dcache_.p,
                                                                      linv_.p);
@@ -810,9 +853,7 @@ void GpuFactor::run_factor_levels(int B, const std::vector<char>* fuse, cudaEven
           k_rows64<<<dim3(nl, B, nrb), 256, kRowsSmem, stream_>>>(ds_, lst, j0, F_.p, fs, dcache_.p, linv_.p);
           ++launches_;
         }
-        int nt = cdiv(rows, kUT64);
-        k_update64w8<<<dim3(nl, B, std::max(1, nt * (nt + 1) / 2)), 256, kPersistUpdSmem, stream_>>>(
-            ds_, lst, j0, F_.p, fs, dcache_.p);
+        k_update64w8<<<ug, 256, kPersistUpdSmem, stream_>>>(ds_, lst, j0, F_.p, fs, dcache_.p);
         launches_ += 2;
       }
     }
@@ -825,16 +866,19 @@ void GpuFactor::run_factor_levels(int B, const std::vector<char>* fuse, cudaEven
 
 // ---------------------------------------------------------------------------
 // Panel-schedule autotuner. For every level with large fronts the panel step has
-// two forms with bit-identical results: "fused" (each of the nrb row CTAs factors
-// the 64 x 64 diagonal block itself, one launch) and "split" (one CTA per front
-// factors it, k_rows64 forms the rows from the cached factor, two launches). Which
-// is faster depends on the level's fronts, the batch size and the GPU, so on the
-// first factorization at a batch size B the level sequence runs once in each form
+// three forms with bit-identical results: "split" (one CTA per front factors the
+// 64 x 64 diagonal block, k_rows64 forms the rows from the cached factor, then the
+// trailing update: three launches per step), "fused" (each of the nrb row CTAs
+// factors the diagonal block itself, then the update: two launches) and
+// "look-ahead" (rows, then the update whose tile-0 CTAs factor the next diagonal
+// block: two launches per step plus one for the first block). Which is faster
+// depends on the level's fronts, the batch size and the GPU, so on the first
+// factorization at a batch size B the level sequence runs once in each form
 // (after a fill, untimed warm-up first) with CUDA events around every level's
-// large-front work, and each level keeps the faster form. Decisions are kept in a
+// large-front work, and each level keeps the fastest form. Decisions are kept in a
 // process-wide table keyed by the supernodal structure and B, so later handles on
 // the same pattern reuse them. INLA_NO_AUTOTUNE in the environment keeps the
-// occupancy rule (fused while every row CTA fits in about one wave).
+// occupancy rule (fused while every row CTA fits in about one wave, else split).
 // ---------------------------------------------------------------------------
 namespace {
 std::mutex g_tune_mu;
@@ -849,6 +893,7 @@ const std::vector<char>* GpuFactor::schedule(int B, const std::function<void()>&
   if (!any_large) return nullptr;
   auto it = fuse_.find(B);
   if (it != fuse_.end()) return &it->second;
+  if (panel_form_ >= 0) return &(fuse_[B] = std::vector<char>(levels_.size(), (char)panel_form_));
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto g = g_tune.find({struct_hash_, B});
@@ -857,8 +902,8 @@ const std::vector<char>* GpuFactor::schedule(int B, const std::function<void()>&
   const size_t L = levels_.size();
   std::vector<cudaEvent_t> ev(2 * L);
   for (auto& e : ev) INLA_CUDA(cudaEventCreate(&e));
-  std::vector<double> t[2];
-  for (int form = 0; form < 2; ++form) {
+  std::vector<double> t[kNumForms];
+  for (int form = 0; form < kNumForms; ++form) {
     const std::vector<char> pol(L, (char)form);
     fill();
     run_factor_levels(B, &pol, nullptr);  // warm-up (module load, caches)
@@ -873,13 +918,18 @@ const std::vector<char>* GpuFactor::schedule(int B, const std::function<void()>&
     }
   }
   for (auto& e : ev) cudaEventDestroy(e);
-  std::vector<char> best(L, 0);
-  for (size_t l = 0; l < L; ++l) best[l] = t[1][l] < t[0][l] ? 1 : 0;
-  if (std::getenv("INLA_DEBUG")) {
-    double a = 0, b = 0, c = 0;
-    for (size_t l = 0; l < L; ++l) a += t[0][l], b += t[1][l], c += std::min(t[0][l], t[1][l]);
-    std::fprintf(stderr, "autotune B=%d: split %.3f ms, fused %.3f ms, per-level best %.3f ms\n", B, a, b, c);
+  std::vector<char> best(L, kFormSplit);
+  double tot[kNumForms] = {0.0, 0.0, 0.0}, tbest = 0.0;
+  for (size_t l = 0; l < L; ++l) {
+    for (int f = 0; f < kNumForms; ++f) {
+      tot[f] += t[f][l];
+      if (t[f][l] < t[(int)best[l]][l]) best[l] = (char)f;
+    }
+    tbest += t[(int)best[l]][l];
   }
+  if (std::getenv("INLA_DEBUG"))
+    std::fprintf(stderr, "autotune B=%d: split %.3f ms, fused %.3f ms, look-ahead %.3f ms, per-level best %.3f ms\n",
+                 B, tot[kFormSplit], tot[kFormFused], tot[kFormLookahead], tbest);
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune[{struct_hash_, B}] = best;

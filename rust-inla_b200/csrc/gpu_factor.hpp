@@ -37,6 +37,9 @@ void device_release_cached();
 // Schedule of the engines built from now on: 0 level launches, 1 measured per batch size, 2
 // persistent wherever it fits.
 void set_persistent_default(int mode);
+// Panel form of the level launches for engines built from now on: -1 autotuned per level
+// (default), 0 split, 1 fused, 2 look-ahead (bit-identical results).
+void set_panel_form(int form);
 
 // Small RAII device buffer.
 template <class T>
@@ -221,6 +224,8 @@ class GpuFactor {
   DBuf<int64_t> d_pgptr_;
   DBuf<int2> d_pgrng_;
   DBuf<double> dcache_p_;
+  int64_t dslot_ = 0;  // doubles per slot of dcache_ (two slots)
+  int panel_form_ = -1;  // forced panel form (set_panel_form at construction), -1 autotuned
   DBuf<int> d_fseg_;
   // persistent solve
   bool solve_persist_ = false;

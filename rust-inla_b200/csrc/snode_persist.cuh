@@ -114,9 +114,20 @@ __device__ bool wait_children(const PersistArgs& a, int s, int b) {
 // Trailing update tile `tile` of block J of front s, problem b, over eight warps (32 x 16
 // warp tiles): every entry accumulates its products over K in the same order as any other warp
 // tiling of the same step, so the result does not depend on the tiling.
+//
+// kNext (look-ahead): tile 0 holds the next diagonal block [c, c + w') (w' = min(64, k - c))
+// once its update is done, so that CTA factors it right away, exactly as k_panel64 with no
+// rows would after this launch: the updated values go to shared memory as well as to the
+// front, cta_ldlt<true> factors them, and the CTA writes the factored block into the front,
+// D and L to dc_next (the cache slot of the next step; dc is this step's) and L^-1 to the
+// inverse-block cache. The other tiles of this launch read only block column J and their own
+// targets, so nothing else reads the block while it is factored. smu: kPanelSmem bytes.
+template <bool kNext = false>
 __device__ __forceinline__ void update64w8_body(const DevSym& S, int s, int b, int tile, int j0,
                                                 double* __restrict__ F, int64_t fstride,
-                                                const double* __restrict__ dc, double* smu) {
+                                                const double* __restrict__ dc, double* smu,
+                                                double* __restrict__ dc_next = nullptr,
+                                                double* __restrict__ linv = nullptr) {
   if (front_skipped(S, s, b)) return;
   constexpr int ld = kLd64;
   double* As = smu;              // As[t*ld + i] = L[I0+i, j0+t]
@@ -202,6 +213,39 @@ __device__ __forceinline__ void update64w8_body(const DevSym& S, int s, int b, i
         const int j = J0 + wj + q * 8 + tg * 2 + h;
         if (i < m && j < m && i >= j) Fs[i + (int64_t)j * m] = cv[a][q][h] - acc[a][q][h];
       }
+  if (kNext && tile == 0 && c < k) {
+    const int wn = min(kB64, k - c);
+    double* Ds = smu;             // [64 cols][ld]: the next diagonal block, factored in place
+    double* Li = Ds + kB64 * ld;  // its L^-1
+    double* U = Li + kB64 * ld;
+    double* ws = U + 16 * kULd64;
+    __syncthreads();  // the operand tiles are consumed
+    for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) {
+      Ds[(e & 63) + (e >> 6) * ld] = 0.0;
+      Li[(e & 63) + (e >> 6) * ld] = 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int q = 0; q < 2; ++q)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int r = wi + a * 8 + g, cc = wj + q * 8 + tg * 2 + h;  // I0 == J0 == c for tile 0
+          if (r < wn && cc < wn && r >= cc) Ds[r + cc * ld] = cv[a][q][h] - acc[a][q][h];
+        }
+    __syncthreads();
+    cta_ldlt<true>(Ds, ld, wn, wn, Li, ld, U, kULd64, ws);
+    double* D0 = Fs + c + (int64_t)c * m;
+    double* lc = const_cast<double*>(linv_block(S, linv, b, s, c / kB64));
+    for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) {
+      const int cc = e >> 6, r = e & 63;
+      const double v = (r < wn && cc < wn) ? Ds[r + cc * ld] : 0.0;
+      dc_next[e] = v;
+      lc[e] = Li[r + cc * ld];
+      if (r < wn && cc < wn && r >= cc) D0[r + (int64_t)cc * m] = v;
+    }
+  }
 }
 
 __global__ void __launch_bounds__(kPersistThreads, 2) k_factor_persist(PersistArgs a) {

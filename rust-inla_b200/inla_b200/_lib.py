@@ -93,6 +93,7 @@ SIGNATURES = [
     ("inla_batch_schedule", C.c_int, [P, IP]),
     ("inla_solver_check_schedule", C.c_int, [P, LP]),
     ("inla_set_persistent_schedule", C.c_int, [C.c_int]),
+    ("inla_set_panel_form", C.c_int, [C.c_int]),
     ("inla_batch_wait_limit_selftest", C.c_int, [P, C.c_double, IP]),
     ("inla_batch_solve_dev", C.c_int, [P, C.c_int, P, P]),
     ("inla_batch_diag_inv_dev", C.c_int, [P, C.c_int, P, P]),
