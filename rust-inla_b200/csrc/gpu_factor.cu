@@ -246,15 +246,27 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
   status_.alloc(max_batch_);
 
   {
-    int64_t nlmax = 1, ppmax = 1;
+    int64_t nlmax = 1, ppmax = 1, gpmax = 1, cmax = 1;
+    int sms = 0, dev = 0;
+    INLA_CUDA(cudaGetDevice(&dev));
+    INLA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     for (const LevelPlan& P : levels_) {
       nlmax = std::max<int64_t>(nlmax, (int64_t)P.large.size());
       ppmax = std::max<int64_t>(ppmax, (int64_t)P.si_large.size() * cdiv(P.mmax_si_large, kSiT));
+      const int64_t nls = (int64_t)P.si_large.size(), pt = cdiv(P.mmax_si_large, kSiT);
+      // split launches have nls * B * pt <= SM count: B <= bmax
+      const int64_t bmax = std::min<int64_t>(max_batch_, sms / std::max<int64_t>(1, nls * pt));
+      const int sm = si_nsplit(cdiv(P.mmax_si_large, 32), bmax >= 1);
+      if (sm > 1) gpmax = std::max<int64_t>(gpmax, nls * pt * sm * bmax);
+      cmax = std::max<int64_t>(cmax, nls * pt);
     }
     // two slots: the look-ahead form factors block J + 1 while step J still reads block J
     dslot_ = nlmax * max_batch_ * kB64 * kB64;
     dcache_.alloc((size_t)(2 * dslot_));
     ppart_.alloc((size_t)ppmax * max_batch_ * kB64 * kB64);
+    gpart_.alloc((size_t)gpmax * kB64 * kB64);
+    sicnt_.alloc((size_t)cmax * max_batch_);
+    INLA_CUDA(cudaMemsetAsync(sicnt_.p, 0, sizeof(int) * (size_t)cmax * max_batch_, stream_));
   }
   set_smem(k_factor_small<128>, small_factor_smem(kSmallA));
   set_smem(k_factor_small<256>, small_factor_smem(kSmallB));
@@ -282,7 +294,7 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
   set_smem(k_fwd32<128>, (int)((S.max_m + 2 + 32 * 33) * 8));
   set_smem(k_bwd32<128>, (int)((S.max_m + 2 + 32 * 33) * 8));
   set_smem(k_gather8, 200 * 1024 + 8 * kGatherCols * 8);
-  set_smem(k_si_gemm64, kSiGemmSmem);
+  set_smem(k_si_step64, kSiGemmSmem);
   set_smem(k_si_diag64, kSiDiagSmem);
   if (persist_) {
     set_smem(k_factor_persist, persist_smem_);
@@ -1157,9 +1169,13 @@ void GpuFactor::selinv_levels(int B, int slot0) {
       }
       const int nblk = cdiv(P.kmax_si_large, kB64);
       const int ptiles = cdiv(P.mmax_si_large, kSiT);
+      // the K range of G is split over several CTAs only where one CTA per (front, problem,
+      // row tile) would not give every SM one (the top of the tree at small batch sizes)
+      const bool split = (int64_t)nl * B * ptiles <= num_sms_;
+      const int smax = si_nsplit(cdiv(P.mmax_si_large, 32), split);
       for (int jb = 0; jb < nblk; ++jb) {
-        k_si_gemm64<<<dim3(nl, B, ptiles), 256, kSiGemmSmem, stream_>>>(ds_, lst, jb, Fp, Sp, fs, ppart_.p,
-                                                                        ptiles, Lp);
+        k_si_step64<<<dim3(nl, B, ptiles * smax), 256, kSiGemmSmem, stream_>>>(
+            ds_, lst, jb, Fp, Sp, fs, ppart_.p, ptiles, Lp, gpart_.p, sicnt_.p, smax, split ? 1 : 0);
         k_si_diag64<<<dim3(nl, B), 256, kSiDiagSmem, stream_>>>(ds_, lst, jb, Fp, Sp, fs, ppart_.p, ptiles,
                                                                 Lp);
         launches_ += 2;

@@ -209,6 +209,8 @@ class GpuFactor {
   DBuf<int> d_pmap_, d_lists_, d_csn_, d_csnm_, d_lbo_;
   DBuf<double> F_, Sg_, xp_, ub_, logdet_, dcache_, ppart_, linv_, ldpart_;
   DBuf<int> status_, ldflag_;
+  DBuf<double> gpart_;  // split-K pieces of the selected inverse's G (narrow levels)
+  DBuf<int> sicnt_;     // arrival counters of the selected inverse's step kernel (kept zeroed)
   DBuf<unsigned> ldticket_;
   int nfill_ = 0, nfillm_ = 0, nldchunk_ = 0;  // fill chunks (values, model); log-det chunks per problem
   int num_sms_ = 148;

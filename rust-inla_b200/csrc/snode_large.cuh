@@ -11,12 +11,14 @@
 //               trailing matrix (tensor-core tiles, operands staged with cp.async;
 //               update64w8_body in snode_persist.cuh, launched as k_update64w8).
 // Selected inverse, per block J from right to left (A = rows after J):
-//   k_si_gemm64 G = Sigma[A,A] L[A,J], X = -G L_JJ^-1 (cached inverse block),
-//               Sigma[A,J] = X, and the tile's partial P = L[I,J]^T X[I,J];
+//   k_si_step64 G = Sigma[A,A] L[A,J] per 64-row tile of A (the K range split over
+//               several CTAs where the launch would leave SMs idle), X = -G L_JJ^-1
+//               (cached inverse block), Sigma[A,J] = X, and the tile's partial
+//               P = L[I,J]^T X[I,J];
 //   k_si_diag64 Sigma_JJ = L_JJ^-T (D^-1 L_JJ^-1 - P), P the fixed-order sum of
 //               the partials: the closed form of the in-block Takahashi
-//               recurrence S_ij = -P_ji - sum_{l in J, l>j} L_lj S_li,
-//               S_jj = 1/d_j - P_jj - sum_{l in J, l>j} L_lj S_lj.
+//   recurrence S_ij = -P_ji - sum_{l in J, l>j} L_lj S_li,
+//   S_jj = 1/d_j - P_jj - sum_{l in J, l>j} L_lj S_lj.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -595,20 +597,141 @@ __device__ __forceinline__ double sig_lower(const double* Ss, int m, int row, in
 
 constexpr int kSiT = 64;  // rows of A per CTA
 
-// ppart: [list index][b][tile][64*64] partial P blocks; ptiles = tiles per (front, b).
-// Shared memory: two chunk buffers (Sa + Lb each, double-buffered with
-// cp.async) and G; L_JJ^-1 (from the inverse-block cache) and L[I,J] reuse the
-// chunk buffers after the GEMM.
-// Row tile z of block jb of front s, problem b (256 threads); pp: this front's and problem's
-// partial-P blocks (tile z at pp + z * 4096).
-__device__ __forceinline__ void si_gemm64_body(const DevSym& S, int s, int b, int z, int jb,
+// Split of the K loop of G = Sigma[I,A] L[A,J]: a front whose A spans at least
+// kSiSplitMinChunks chunks of 32 rows has its K range cut into pieces of kSiChunksPerSplit
+// chunks, one CTA each, when the launch allows it (the host allows it where one CTA per row
+// tile would leave SMs idle). The pieces are summed in a fixed order, so a given launch shape
+// always gives the same result; split and unsplit steps differ by rounding only.
+constexpr int kSiChunksPerSplit = 4;
+constexpr int kSiSplitMinChunks = 8;
+__host__ __device__ inline int si_nsplit(int nch, bool allow) {
+  return (allow && nch >= kSiSplitMinChunks) ? (nch + kSiChunksPerSplit - 1) / kSiChunksPerSplit : 1;
+}
+
+// Sigma_JJ = L^-T (D^-1 L^-1 - P), L = L_JJ unit lower, P = L[A,J]^T Sigma[A,J]
+// (the closed form of the in-block Takahashi recurrence), with L^-1 from the
+// inverse-block cache and the product as a tensor-core GEMM. Block jb of front s, problem b
+// (256 threads); pp_front: the tiles' partial P blocks (tile z at pp_front + z * 4096), read
+// through L2 because other CTAs of the same launch wrote them.
+__device__ __forceinline__ void si_diag64_body(const DevSym& S, int s, int b, int jb, const double* __restrict__ F,
+                                               double* __restrict__ Sg, int64_t fstride,
+                                               const double* __restrict__ pp_front,
+                                               const double* __restrict__ linv, double* smem64) {
+  constexpr int ld = kB64 + 1;
+  double* Pm = smem64;            // P, then M = D^-1 L^-1 - P  (Pm[r + c*ld] = entry (r, c))
+  double* Ld = Pm + kB64 * ld;    // L_JJ with D on the diagonal
+  double* Li = Ld + kB64 * ld;    // L_JJ^-1
+  const int k = lg_k(S, s), m = lg_m(S, s);
+  const int nblk = (k + kB64 - 1) / kB64;
+  if (jb >= nblk) return;
+  const int bi = nblk - 1 - jb;
+  const int j0 = bi * kB64, j1 = min(k, j0 + kB64), w = j1 - j0;
+  const int ntiles = (m - j1 + kSiT - 1) / kSiT;
+  const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
+  double* Ss = Sg + (int64_t)b * fstride + S.fptr[s];
+  const double* pp = pp_front;
+  const double* lc = linv_block(S, linv, b, s, bi);
+  for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) {
+    const int c = e >> 6, r = e & 63;
+    if (r < w && c < w && r >= c) cp_async8(&Ld[r + c * ld], Fs + (j0 + r) + (int64_t)(j0 + c) * m);
+    else Ld[r + c * ld] = 0.0;
+    cp_async8(&Li[r + c * ld], lc + e);
+  }
+  cp_async_commit();
+  {
+    // partials are stored row-major: pp[j*64 + i] = P[j][i]; fixed summation order over tiles
+    double acc[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+    for (int z = 0; z < ntiles; ++z) {
+      const double* pz = pp + (int64_t)z * kB64 * kB64;
+#pragma unroll
+      for (int q = 0; q < 16; ++q) acc[q] += __ldcg(pz + threadIdx.x + 256 * q);
+    }
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int e = threadIdx.x + 256 * q, j = e >> 6, i = e & 63;
+      Pm[j + i * ld] = acc[q];
+    }
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) {
+    const int c = e >> 6, r = e & 63;
+    Pm[r + c * ld] = (r < w && c < w) ? Li[r + c * ld] / Ld[r + r * ld] - Pm[r + c * ld] : 0.0;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp < 4) {
+    const int wr = (warp & 1) * 32, wc = (warp >> 1) * 32;
+    const int g = lane >> 2, tg = lane & 3;
+    double acc[4][4][2];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[a][q][0] = acc[a][q][1] = 0.0;
+#pragma unroll 4
+    for (int kk = 0; kk < kB64; kk += 4) {
+      double af[4], bf[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) af[a] = Li[(kk + tg) + (wr + a * 8 + g) * ld];  // (L^-1)^T
+#pragma unroll
+      for (int q = 0; q < 4; ++q) bf[q] = Pm[(kk + tg) + (wc + q * 8 + g) * ld];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) mma884(acc[a][q][0], acc[a][q][1], af[a], bf[q]);
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int r = wr + a * 8 + g, c = wc + q * 8 + tg * 2 + h;
+          if (r < w && c < w && r >= c) Ss[(j0 + r) + (int64_t)(j0 + c) * m] = acc[a][q][h];
+        }
+  }
+}
+
+// Last-arrival count: every thread's global writes are fenced, then one thread counts the
+// CTA in; true in the CTA whose arrival completes the count (it then resets the counter for
+// the next launch and reads what the others wrote). Nothing waits on another CTA.
+__device__ __forceinline__ bool si_arrive_last(int* counter, int expected, int* sh_flag) {
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int t = atomicAdd(counter, 1);
+    *sh_flag = (t == expected - 1);
+    if (t == expected - 1) *counter = 0;
+  }
+  __syncthreads();
+  const bool last = *sh_flag != 0;
+  if (last) __threadfence();
+  return last;
+}
+
+// Off-diagonal part of one 64-column step of the selected inverse of the large fronts (block
+// jb counted from the right). CTA z = I * smax + sp handles row tile I of A (64 rows) and
+// K piece sp:
+//   G_I = Sigma[I,A] L[A,J] over its K piece (chunks of 32 rows, three cp.async stages);
+//   with a split K the pieces go to gp_front and the last piece to arrive sums them in piece
+//   order; X = -G_I L_JJ^-1 (cached inverse block) is Sigma[I,J]; the tile's partial
+//   P_I = L[I,J]^T X goes to pp_front (k_si_diag64 then forms Sigma_JJ).
+// Every sum has a fixed order, so the result does not depend on which CTA arrives last; with
+// one piece (smax == 1) the arithmetic is the single-CTA K loop.
+// cnt_front: ptiles zeroed counters (one per tile), left zeroed again.
+// Shared memory: three chunk buffers (Sa[32][68] + Lb[32][68] each) for the G loop;
+// afterwards buffer 0 holds G (then X), buffer 1 L_JJ^-1 and buffer 2 L[I,J].
+__device__ __forceinline__ void si_step64_body(const DevSym& S, int s, int b, int z, int jb,
                                                const double* __restrict__ F, double* __restrict__ Sg,
                                                int64_t fstride, double* __restrict__ pp_front,
-                                               const double* __restrict__ linv, double* smem64) {
+                                               const double* __restrict__ linv, double* smem64,
+                                               double* __restrict__ gp_front, int* cnt_front, int ptiles,
+                                               int smax, bool allow_split) {
+  __shared__ int sh_last;
   constexpr int kBuf = 64 * kLd64;  // doubles per chunk buffer (Sa[32][68] + Lb[32][68])
   typedef double Row68[kLd64];  // leading dimension 68 == 4 (mod 16): conflict-free fragments
-  // three stage buffers (Sa[32][68] + Lb[32][68] each) for the G loop; afterwards
-  // buffer 0 holds G (then X), buffer 1 L_JJ^-1 and buffer 2 L[I,J]
   Row68* Gs = reinterpret_cast<Row68*>(smem64);             // [64][68]: G, then X
   Row68* Lt = reinterpret_cast<Row68*>(smem64 + 2 * kBuf);  // [64][68]: L[I0+l, j0+j]
   const int k = lg_k(S, s), m = lg_m(S, s);
@@ -616,8 +739,14 @@ __device__ __forceinline__ void si_gemm64_body(const DevSym& S, int s, int b, in
   if (jb >= nblk) return;
   const int bi = nblk - 1 - jb;
   const int j0 = bi * kB64, j1 = min(k, j0 + kB64), w = j1 - j0;
-  const int I0 = j1 + z * kSiT;
-  if (I0 >= m) return;
+  const int ntiles = (m - j1 + kSiT - 1) / kSiT;
+  if (ntiles == 0) return;
+  const int nch = (m - j1 + 31) / 32;
+  const int ns = si_nsplit(nch, allow_split);
+  const int I = z / smax, sp = z - I * smax;
+  if (I >= ntiles || sp >= ns) return;
+  const int I0 = j1 + I * kSiT;
+  const int cb = sp * kSiChunksPerSplit, ce = ns == 1 ? nch : min(nch, cb + kSiChunksPerSplit);
   const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
   double* Ss = Sg + (int64_t)b * fstride + S.fptr[s];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -663,14 +792,14 @@ __device__ __forceinline__ void si_gemm64_body(const DevSym& S, int s, int b, in
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int q = 0; q < 2; ++q) acc[a][q][0] = acc[a][q][1] = 0.0;
-  const int nch = (m - j1 + 31) / 32;
-  load_chunk(j1, 0);
-  if (nch > 1) load_chunk(j1 + 32, 1);
-  for (int c = 0; c < nch; ++c) {
-    if (c + 2 < nch) {
-      load_chunk(j1 + 32 * (c + 2), (c + 2) % 3);
+  const int nc = ce - cb;
+  load_chunk(j1 + 32 * cb, 0);
+  if (nc > 1) load_chunk(j1 + 32 * (cb + 1), 1);
+  for (int c = 0; c < nc; ++c) {
+    if (c + 2 < nc) {
+      load_chunk(j1 + 32 * (cb + c + 2), (c + 2) % 3);
       cp_async_wait<2>();
-    } else if (c + 1 < nch) {
+    } else if (c + 1 < nc) {
       cp_async_wait<1>();
     } else {
       cp_async_wait<0>();
@@ -694,6 +823,16 @@ __device__ __forceinline__ void si_gemm64_body(const DevSym& S, int s, int b, in
     }
     __syncthreads();
   }
+  if (ns > 1) {  // this piece to gp_front; the last piece of the tile sums them in order
+    double* gp = gp_front + (int64_t)(I * smax + sp) * (kB64 * kB64);
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int q = 0; q < 2; ++q)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) gp[(wi + a * 8 + g) * kB64 + wj + q * 8 + tg * 2 + h] = acc[a][q][h];
+    if (!si_arrive_last(cnt_front + I, ns, &sh_last)) return;
+  }
   // L_JJ^-1 (cached) and L[I,J] are fetched together, G goes to buffer 0
   double* Li = smem64 + kBuf;
   const int rows = min(kSiT, m - I0);
@@ -708,12 +847,21 @@ __device__ __forceinline__ void si_gemm64_body(const DevSym& S, int s, int b, in
     }
     cp_async_commit();
   }
+  if (ns > 1) {
+    const double* gq = gp_front + (int64_t)(I * smax) * (kB64 * kB64);
+    for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) {
+      double v = __ldcg(gq + e);
+      for (int q = 1; q < ns; ++q) v += __ldcg(gq + (int64_t)q * (kB64 * kB64) + e);
+      Gs[e >> 6][e & 63] = v;
+    }
+  } else {
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int q = 0; q < 2; ++q)
+      for (int q = 0; q < 2; ++q)
 #pragma unroll
-      for (int h = 0; h < 2; ++h) Gs[wi + a * 8 + g][wj + q * 8 + tg * 2 + h] = acc[a][q][h];
+        for (int h = 0; h < 2; ++h) Gs[wi + a * 8 + g][wj + q * 8 + tg * 2 + h] = acc[a][q][h];
+  }
   // X = -G L_JJ^-1 as a tensor-core GEMM with the cached inverse of the unit
   // lower diagonal block
   cp_async_wait<0>();
@@ -775,7 +923,7 @@ __device__ __forceinline__ void si_gemm64_body(const DevSym& S, int s, int b, in
         for (int q = 0; q < 2; ++q) mma884(pa[a][q][0], pa[a][q][1], af[a], bf[q]);
     }
   }
-  double* pp = pp_front + (int64_t)z * (kB64 * kB64);
+  double* pp = pp_front + (int64_t)I * (kB64 * kB64);
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -784,98 +932,19 @@ __device__ __forceinline__ void si_gemm64_body(const DevSym& S, int s, int b, in
       for (int h = 0; h < 2; ++h) pp[(wr + a * 8 + g) * kB64 + wc + q * 8 + tg * 2 + h] = pa[a][q][h];
 }
 
-__global__ void __launch_bounds__(256) k_si_gemm64(DevSym S, const int* __restrict__ list, int jb,
+// ppart: [list index][b][tile][64*64] partial P blocks; gpart: [list index][b][tile][piece]
+// [64*64] pieces of G (used when smax > 1); cnt: [list index][b][ptiles] counters.
+__global__ void __launch_bounds__(256) k_si_step64(DevSym S, const int* __restrict__ list, int jb,
                                                   const double* __restrict__ F, double* __restrict__ Sg,
                                                   int64_t fstride, double* __restrict__ ppart, int ptiles,
-                                                  const double* __restrict__ linv) {
+                                                  const double* __restrict__ linv, double* __restrict__ gpart,
+                                                  int* __restrict__ cnt, int smax, int allow_split) {
   extern __shared__ double smem64[];
-  double* pp = ppart + ((int64_t)blockIdx.x * gridDim.y + blockIdx.y) * ptiles * (kB64 * kB64);
-  si_gemm64_body(S, list[blockIdx.x], blockIdx.y, blockIdx.z, jb, F, Sg, fstride, pp, linv, smem64);
-}
-
-// Sigma_JJ = L^-T (D^-1 L^-1 - P), L = L_JJ unit lower, P = L[A,J]^T Sigma[A,J]
-// (the closed form of the in-block Takahashi recurrence), with L^-1 from the
-// inverse-block cache and the product as a tensor-core GEMM. Block jb of front s, problem b
-// (256 threads); pp_front as in si_gemm64_body.
-__device__ __forceinline__ void si_diag64_body(const DevSym& S, int s, int b, int jb, const double* __restrict__ F,
-                                               double* __restrict__ Sg, int64_t fstride,
-                                               const double* __restrict__ pp_front,
-                                               const double* __restrict__ linv, double* smem64) {
-  constexpr int ld = kB64 + 1;
-  double* Pm = smem64;            // P, then M = D^-1 L^-1 - P  (Pm[r + c*ld] = entry (r, c))
-  double* Ld = Pm + kB64 * ld;    // L_JJ with D on the diagonal
-  double* Li = Ld + kB64 * ld;    // L_JJ^-1
-  const int k = lg_k(S, s), m = lg_m(S, s);
-  const int nblk = (k + kB64 - 1) / kB64;
-  if (jb >= nblk) return;
-  const int bi = nblk - 1 - jb;
-  const int j0 = bi * kB64, j1 = min(k, j0 + kB64), w = j1 - j0;
-  const int ntiles = (m - j1 + kSiT - 1) / kSiT;
-  const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
-  double* Ss = Sg + (int64_t)b * fstride + S.fptr[s];
-  const double* pp = pp_front;
-  const double* lc = linv_block(S, linv, b, s, bi);
-  for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) {
-    const int c = e >> 6, r = e & 63;
-    if (r < w && c < w && r >= c) cp_async8(&Ld[r + c * ld], Fs + (j0 + r) + (int64_t)(j0 + c) * m);
-    else Ld[r + c * ld] = 0.0;
-    cp_async8(&Li[r + c * ld], lc + e);
-  }
-  cp_async_commit();
-  {
-    // partials are stored row-major: pp[j*64 + i] = P[j][i]; fixed summation order over tiles
-    double acc[16];
-#pragma unroll
-    for (int q = 0; q < 16; ++q) acc[q] = 0.0;
-    for (int z = 0; z < ntiles; ++z) {
-      const double* pz = pp + (int64_t)z * kB64 * kB64;
-#pragma unroll
-      for (int q = 0; q < 16; ++q) acc[q] += pz[threadIdx.x + 256 * q];
-    }
-#pragma unroll
-    for (int q = 0; q < 16; ++q) {
-      const int e = threadIdx.x + 256 * q, j = e >> 6, i = e & 63;
-      Pm[j + i * ld] = acc[q];
-    }
-  }
-  cp_async_wait<0>();
-  __syncthreads();
-  for (int e = threadIdx.x; e < kB64 * kB64; e += blockDim.x) {
-    const int c = e >> 6, r = e & 63;
-    Pm[r + c * ld] = (r < w && c < w) ? Li[r + c * ld] / Ld[r + r * ld] - Pm[r + c * ld] : 0.0;
-  }
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (warp < 4) {
-    const int wr = (warp & 1) * 32, wc = (warp >> 1) * 32;
-    const int g = lane >> 2, tg = lane & 3;
-    double acc[4][4][2];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) acc[a][q][0] = acc[a][q][1] = 0.0;
-#pragma unroll 4
-    for (int kk = 0; kk < kB64; kk += 4) {
-      double af[4], bf[4];
-#pragma unroll
-      for (int a = 0; a < 4; ++a) af[a] = Li[(kk + tg) + (wr + a * 8 + g) * ld];  // (L^-1)^T
-#pragma unroll
-      for (int q = 0; q < 4; ++q) bf[q] = Pm[(kk + tg) + (wc + q * 8 + g) * ld];
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) mma884(acc[a][q][0], acc[a][q][1], af[a], bf[q]);
-    }
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int r = wr + a * 8 + g, c = wc + q * 8 + tg * 2 + h;
-          if (r < w && c < w && r >= c) Ss[(j0 + r) + (int64_t)(j0 + c) * m] = acc[a][q][h];
-        }
-  }
+  const int64_t slot = (int64_t)blockIdx.x * gridDim.y + blockIdx.y;
+  si_step64_body(S, list[blockIdx.x], blockIdx.y, blockIdx.z, jb, F, Sg, fstride,
+                 ppart + slot * ptiles * (kB64 * kB64), linv, smem64,
+                 gpart + slot * ptiles * smax * (kB64 * kB64), cnt + slot * ptiles, ptiles, smax,
+                 allow_split != 0);
 }
 
 __global__ void __launch_bounds__(256) k_si_diag64(DevSym S, const int* __restrict__ list, int jb,

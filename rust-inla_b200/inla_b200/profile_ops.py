@@ -40,6 +40,8 @@ def main():
     ap.add_argument("--stencil", action="store_true",
                     help="laplace-grad batch shaped like one batched-Newton iteration: 3 candidates x "
                          "(centre, +-h per coordinate), so stencil points share prior factorizations")
+    ap.add_argument("--panel-form", type=int, default=-1, choices=[-1, 0, 1, 2],
+                    help="panel form of the level launches: -1 autotuned, 0 split, 1 fused, 2 look-ahead")
     a = ap.parse_args()
     from inla_b200 import _lib
     order = {"amd": _lib.ORDER_AMD, "nd": _lib.ORDER_ND}[a.ordering]
@@ -64,6 +66,7 @@ def main():
         c, _ = models.spde_coefs(math.log(0.02), math.log(14.14))
         q = (p.model.matrix(c) + 100.0 * (p.a.T @ p.a)).tocsc()
         q.sort_indices()
+        check(lib().inla_set_panel_form(a.panel_form))
         bs = BatchSolver(q, max_batch=B, ordering=order)
         vals = torch.tensor(np.tile(q.data, (B, 1)), device="cuda")
         ld = torch.zeros(B, dtype=torch.float64, device="cuda")
