@@ -293,6 +293,8 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
   set_smem(k_rows64, kRowsSmem);
   set_smem(k_fwd32<128>, (int)((S.max_m + 2 + 32 * 33) * 8));
   set_smem(k_bwd32<128>, (int)((S.max_m + 2 + 32 * 33) * 8));
+  set_smem(k_fwd64<256>, (int)((S.max_m + 2) * 8));
+  set_smem(k_bwd64<256>, (int)((S.max_m + 2) * 8));
   set_smem(k_gather8, 200 * 1024 + 8 * kGatherCols * 8);
   set_smem(k_si_step64, kSiGemmSmem);
   set_smem(k_si_diag64, kSiDiagSmem);
@@ -1084,6 +1086,7 @@ void GpuFactor::solve(double* d_x, int64_t xstride, int B, int slot0) {
       a.gstart = d_sgstart_.p;
       a.task = reinterpret_cast<const PersistTask*>(d_stask_.p);
       a.tiny_list = d_stiny_.p;
+      a.linv = linv_.p + (int64_t)slot0 * ds_.lstride;
       a.xp = xp_.p;
       a.ub = ub_.p;
       a.ustride = std::max<int64_t>(usum_, 1);
@@ -1102,6 +1105,9 @@ void GpuFactor::solve(double* d_x, int64_t xstride, int B, int slot0) {
     k_permute_in<<<gp, 256, 0, stream_>>>(n, d_perm_.p, d_x, xstride, xp_.p);
     ++launches_;
     const int64_t us = std::max<int64_t>(usum_, 1);
+    const double* Lp = linv_.p + (int64_t)slot0 * ds_.lstride;
+    // fronts of up to kSmallB rows (contiguous lists small_a, small_b) in 32-column blocks by one
+    // CTA each; larger fronts in 64-column blocks with their cached inverse blocks
     for (const LevelPlan& P : levels_) {
       if (!P.tiny.empty()) {
         const int nt = (int)P.tiny.size();
@@ -1109,9 +1115,15 @@ void GpuFactor::solve(double* d_x, int64_t xstride, int B, int slot0) {
             ds_, d_lists_.p + P.off_tiny, nt, Fp, fs, xp_.p, ub_.p, us);
         ++launches_;
       }
-      if (!P.nontiny.empty()) {
-        k_fwd32<128><<<dim3((unsigned)P.nontiny.size(), B), 128, (P.mmax_nontiny + 2 + 32 * 33) * 8, stream_>>>(
-            ds_, d_lists_.p + P.off_nontiny, Fp, fs, xp_.p, ub_.p, us);
+      const int nsm = (int)(P.small_a.size() + P.small_b.size());
+      if (nsm > 0) {
+        k_fwd32<128><<<dim3((unsigned)nsm, B), 128, (std::max(P.mmax_a, P.mmax_b) + 2 + 32 * 33) * 8, stream_>>>(
+            ds_, d_lists_.p + P.off_small_a, Fp, fs, xp_.p, ub_.p, us);
+        ++launches_;
+      }
+      if (!P.large.empty()) {
+        k_fwd64<256><<<dim3((unsigned)P.large.size(), B), 256, (P.mmax_large + 2) * 8, stream_>>>(
+            ds_, d_lists_.p + P.off_large, Fp, fs, Lp, xp_.p, ub_.p, us);
         ++launches_;
       }
     }
@@ -1123,9 +1135,15 @@ void GpuFactor::solve(double* d_x, int64_t xstride, int B, int slot0) {
             ds_, d_lists_.p + P.off_tiny, nt, Fp, fs, xp_.p);
         ++launches_;
       }
-      if (!P.nontiny.empty()) {
-        k_bwd32<128><<<dim3((unsigned)P.nontiny.size(), B), 128, (P.mmax_nontiny + 2 + 32 * 33) * 8, stream_>>>(
-            ds_, d_lists_.p + P.off_nontiny, Fp, fs, xp_.p);
+      const int nsm = (int)(P.small_a.size() + P.small_b.size());
+      if (nsm > 0) {
+        k_bwd32<128><<<dim3((unsigned)nsm, B), 128, (std::max(P.mmax_a, P.mmax_b) + 2 + 32 * 33) * 8, stream_>>>(
+            ds_, d_lists_.p + P.off_small_a, Fp, fs, xp_.p);
+        ++launches_;
+      }
+      if (!P.large.empty()) {
+        k_bwd64<256><<<dim3((unsigned)P.large.size(), B), 256, (P.mmax_large + 2) * 8, stream_>>>(
+            ds_, d_lists_.p + P.off_large, Fp, fs, Lp, xp_.p);
         ++launches_;
       }
     }

@@ -494,6 +494,131 @@ __global__ void __launch_bounds__(NT, 8) k_bwd32(DevSym S, const int* __restrict
   bwd32_body<NT>(S, list[blockIdx.x], blockIdx.y, F, fstride, xp, x);
 }
 
+// Sweeps of the large fronts (those with cached 64 x 64 inverse blocks), 64-column blocks:
+// the diagonal block is applied as a product with its cached inverse L_JJ^-1 (no sequential
+// substitution chain), and the rows below (forward) or the column sums (backward) are spread
+// over the CTA. NT threads; NT / 64 threads share one row of the inverse-block product (their
+// partial sums are combined by shuffles in a fixed order). Shared memory: m + 2 doubles.
+template <int NT>
+__device__ __forceinline__ double inv_block_dot(const double* __restrict__ lc, const double* v, int wb, bool trans) {
+  constexpr int kP = NT / 64;
+  const int r = threadIdx.x / kP, q = threadIdx.x % kP;
+  double acc = 0.0;
+  if (r < wb) {
+    if (!trans) {  // (L^-1 v)_r = sum_{c <= r} L^-1[r][c] v_c
+      for (int c = q; c <= r; c += kP) acc += lc[r + 64 * c] * v[c];
+    } else {  // (L^-T v)_r = sum_{c >= r} L^-1[c][r] v_c
+      for (int c = r + q; c < wb; c += kP) acc += lc[c + 64 * r] * v[c];
+    }
+  }
+#pragma unroll
+  for (int o = 1; o < kP; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  return acc;
+}
+
+// Forward sweep of large front s, problem b (NT = 256 threads).
+template <int NT>
+__device__ __forceinline__ void fwd64_body(const DevSym& S, int s, int b, const double* __restrict__ F,
+                                           int64_t fstride, const double* __restrict__ linv,
+                                           double* __restrict__ xp, double* __restrict__ ub, int64_t ustride,
+                                           double* y) {
+  static_assert(NT % 64 == 0 && NT / 64 <= 32, "whole rows of the inverse-block product per warp");
+  const int k = lg_k(S, s), m = lg_m(S, s), f = S.first[s];
+  const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
+  double* xb = xp + (int64_t)b * S.n;
+  double* ubb = ub + (int64_t)b * ustride;
+  for (int t = threadIdx.x; t < m; t += NT) y[t] = t < k ? xb[f + t] : 0.0;
+  __syncthreads();
+  for (int q = S.child_ptr[s]; q < S.child_ptr[s + 1]; ++q) {
+    const int c = S.child_list[q];
+    const int kc = lg_k(S, c), rc = lg_m(S, c) - kc;
+    const int* relc = S.relx + S.rowptr[c] + kc;
+    const double* uc = ubb + S.uoff[c];
+    for (int t = threadIdx.x; t < rc; t += NT) y[relc[t]] += uc[t];
+    __syncthreads();
+  }
+  const int nblk = (k + kB64 - 1) / kB64;
+  for (int bi = 0; bi < nblk; ++bi) {
+    const int jb = bi * kB64, wb = min(kB64, k - jb);
+    const double v = inv_block_dot<NT>(linv_block(S, linv, b, s, bi), y + jb, wb, false);
+    __syncthreads();  // every read of y_J is done
+    if (threadIdx.x % (NT / 64) == 0 && threadIdx.x / (NT / 64) < wb) y[jb + threadIdx.x / (NT / 64)] = v;
+    __syncthreads();
+    // rows below: one thread per row, all loads of the row issued together, eight partial sums
+    for (int r = jb + wb + threadIdx.x; r < m; r += NT) {
+      double a[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+      const double* Lr = Fs + r + (int64_t)jb * m;
+      for (int j0 = 0; j0 < wb; j0 += 8) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+          if (j0 + u < wb) a[u] += Lr[(int64_t)(j0 + u) * m] * y[jb + j0 + u];
+      }
+      y[r] -= ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+    }
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < m; t += NT) {
+    if (t < k) xb[f + t] = y[t] / Fs[t + (int64_t)t * m];
+    else ubb[S.uoff[s] + t - k] = y[t];
+  }
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_fwd64(DevSym S, const int* __restrict__ list, const double* __restrict__ F,
+                                             int64_t fstride, const double* __restrict__ linv, double* __restrict__ xp,
+                                             double* __restrict__ ub, int64_t ustride) {
+  extern __shared__ double y[];
+  fwd64_body<NT>(S, list[blockIdx.x], blockIdx.y, F, fstride, linv, xp, ub, ustride, y);
+}
+
+// Backward sweep of large front s, problem b (NT = 256 threads).
+template <int NT>
+__device__ __forceinline__ void bwd64_body(const DevSym& S, int s, int b, const double* __restrict__ F,
+                                           int64_t fstride, const double* __restrict__ linv,
+                                           double* __restrict__ xp, double* x) {
+  const int k = lg_k(S, s), m = lg_m(S, s), f = S.first[s];
+  const double* Fs = F + (int64_t)b * fstride + S.fptr[s];
+  double* xb = xp + (int64_t)b * S.n;
+  const int* R = S.rows + S.rowptr[s];
+  for (int t = threadIdx.x; t < m; t += NT) x[t] = xb[R[t]];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nblk = (k + kB64 - 1) / kB64;
+  for (int bi = nblk - 1; bi >= 0; --bi) {
+    const int jb = bi * kB64, wb = min(kB64, k - jb), i0 = jb + wb;
+    // x_j -= sum_{i >= i0} L_ij x_i for the block's columns (warp per column)
+    for (int j = jb + warp; j < jb + wb; j += NT / 32) {
+      const double* Lj = Fs + (int64_t)j * m;
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+      int i = i0 + lane;
+      for (; i + 96 < m; i += 128) {
+        a0 += Lj[i] * x[i];
+        a1 += Lj[i + 32] * x[i + 32];
+        a2 += Lj[i + 64] * x[i + 64];
+        a3 += Lj[i + 96] * x[i + 96];
+      }
+      for (; i < m; i += 32) a0 += Lj[i] * x[i];
+      double acc = (a0 + a1) + (a2 + a3);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) x[j] -= acc;
+    }
+    __syncthreads();
+    const double v = inv_block_dot<NT>(linv_block(S, linv, b, s, bi), x + jb, wb, true);
+    __syncthreads();
+    if (threadIdx.x % (NT / 64) == 0 && threadIdx.x / (NT / 64) < wb) x[jb + threadIdx.x / (NT / 64)] = v;
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < k; t += NT) xb[f + t] = x[t];
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_bwd64(DevSym S, const int* __restrict__ list, const double* __restrict__ F,
+                                             int64_t fstride, const double* __restrict__ linv, double* __restrict__ xp) {
+  extern __shared__ double x[];
+  bwd64_body<NT>(S, list[blockIdx.x], blockIdx.y, F, fstride, linv, xp, x);
+}
+
 // Sweeps of fronts with m <= 32 rows (one 32-column block): one warp per (front,
 // problem), kTinySweepWarps per CTA. Lane t holds entry t of the front's vector; the
 // arithmetic follows k_fwd32 / k_bwd32 step for step (sequential shuffle chain on the

@@ -351,6 +351,7 @@ struct SolveArgs {
   const int* gstart;
   const PersistTask* task;
   const int* tiny_list;
+  const double* linv;  // inverse-block cache of the factorization (large fronts)
   double* xp;
   double* ub;
   int64_t ustride;
@@ -415,10 +416,12 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_solve_persist(SolveArgs 
           fwd_tiny_warp(S, a.tiny_list[T.s + warp], b, a.F, a.fstride, a.xp, a.ub, a.ustride, ssm + 32 * warp);
         break;
       case ST_FWD:
-        fwd32_body<kPersistThreads>(S, T.s, b, a.F, a.fstride, a.xp, a.ub, a.ustride, ssm);
+        if (S.lbo[T.s] >= 0) fwd64_body<kPersistThreads>(S, T.s, b, a.F, a.fstride, a.linv, a.xp, a.ub, a.ustride, ssm);
+        else fwd32_body<kPersistThreads>(S, T.s, b, a.F, a.fstride, a.xp, a.ub, a.ustride, ssm);
         break;
       case ST_BWD:
-        bwd32_body<kPersistThreads>(S, T.s, b, a.F, a.fstride, a.xp, ssm);
+        if (S.lbo[T.s] >= 0) bwd64_body<kPersistThreads>(S, T.s, b, a.F, a.fstride, a.linv, a.xp, ssm);
+        else bwd32_body<kPersistThreads>(S, T.s, b, a.F, a.fstride, a.xp, ssm);
         break;
       default:
         if (warp < T.sub) bwd_tiny_warp(S, a.tiny_list[T.s + warp], b, a.F, a.fstride, a.xp);
