@@ -516,8 +516,9 @@ __device__ __forceinline__ double inv_block_dot(const double* __restrict__ lc, c
   return acc;
 }
 
-// Forward sweep of large front s, problem b (NT = 256 threads).
-template <int NT>
+// Forward sweep of large front s, problem b (NT = 256 threads). kDeep: two rows per pass
+// instead of one (more loads in flight, more registers); the result is the same either way.
+template <int NT, bool kDeep = true>
 __device__ __forceinline__ void fwd64_body(const DevSym& S, int s, int b, const double* __restrict__ F,
                                            int64_t fstride, const double* __restrict__ linv,
                                            double* __restrict__ xp, double* __restrict__ ub, int64_t ustride,
@@ -544,16 +545,31 @@ __device__ __forceinline__ void fwd64_body(const DevSym& S, int s, int b, const 
     __syncthreads();  // every read of y_J is done
     if (threadIdx.x % (NT / 64) == 0 && threadIdx.x / (NT / 64) < wb) y[jb + threadIdx.x / (NT / 64)] = v;
     __syncthreads();
-    // rows below: one thread per row, all loads of the row issued together, eight partial sums
-    for (int r = jb + wb + threadIdx.x; r < m; r += NT) {
+    // rows below: one thread per row, two rows per pass with 32 loads of each in flight (the
+    // panel streams from DRAM: the loads in flight set the rate), eight partial sums per row
+    for (int r = jb + wb + threadIdx.x; r < m; r += (kDeep ? 2 : 1) * NT) {
+      const int r2 = r + NT;
+      const bool two = kDeep && r2 < m;
       double a[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+      double c[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
       const double* Lr = Fs + r + (int64_t)jb * m;
-      for (int j0 = 0; j0 < wb; j0 += 8) {
+      for (int j0 = 0; j0 < wb; j0 += 32) {
+        double la[32], lb[kDeep ? 32 : 1];
 #pragma unroll
-        for (int u = 0; u < 8; ++u)
-          if (j0 + u < wb) a[u] += Lr[(int64_t)(j0 + u) * m] * y[jb + j0 + u];
+        for (int u = 0; u < 32; ++u) {
+          const bool ok = j0 + u < wb;
+          la[u] = ok ? Lr[(int64_t)(j0 + u) * m] : 0.0;
+          if (kDeep) lb[kDeep ? u : 0] = ok && two ? Lr[(int64_t)(j0 + u) * m + NT] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 32; ++u) {
+          const double yj = j0 + u < wb ? y[jb + j0 + u] : 0.0;
+          a[u & 7] += la[u] * yj;
+          if (kDeep) c[u & 7] += lb[kDeep ? u : 0] * yj;
+        }
       }
       y[r] -= ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+      if (two) y[r2] -= ((c[0] + c[1]) + (c[2] + c[3])) + ((c[4] + c[5]) + (c[6] + c[7]));
     }
     __syncthreads();
   }
@@ -564,15 +580,17 @@ __device__ __forceinline__ void fwd64_body(const DevSym& S, int s, int b, const 
 }
 
 template <int NT>
-__global__ void __launch_bounds__(NT) k_fwd64(DevSym S, const int* __restrict__ list, const double* __restrict__ F,
+__global__ void __launch_bounds__(NT, 1) k_fwd64(DevSym S, const int* __restrict__ list, const double* __restrict__ F,
                                              int64_t fstride, const double* __restrict__ linv, double* __restrict__ xp,
                                              double* __restrict__ ub, int64_t ustride) {
   extern __shared__ double y[];
-  fwd64_body<NT>(S, list[blockIdx.x], blockIdx.y, F, fstride, linv, xp, ub, ustride, y);
+  fwd64_body<NT, true>(S, list[blockIdx.x], blockIdx.y, F, fstride, linv, xp, ub, ustride, y);
 }
 
-// Backward sweep of large front s, problem b (NT = 256 threads).
-template <int NT>
+// Backward sweep of large front s, problem b (NT = 256 threads). kDeep: four rows per pass
+// instead of two (more loads in flight); every lane still visits its rows in increasing
+// order, so the result is the same either way.
+template <int NT, bool kDeep = true>
 __device__ __forceinline__ void bwd64_body(const DevSym& S, int s, int b, const double* __restrict__ F,
                                            int64_t fstride, const double* __restrict__ linv,
                                            double* __restrict__ xp, double* x) {
@@ -586,22 +604,40 @@ __device__ __forceinline__ void bwd64_body(const DevSym& S, int s, int b, const 
   const int nblk = (k + kB64 - 1) / kB64;
   for (int bi = nblk - 1; bi >= 0; --bi) {
     const int jb = bi * kB64, wb = min(kB64, k - jb), i0 = jb + wb;
-    // x_j -= sum_{i >= i0} L_ij x_i for the block's columns (warp per column)
-    for (int j = jb + warp; j < jb + wb; j += NT / 32) {
-      const double* Lj = Fs + (int64_t)j * m;
-      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-      int i = i0 + lane;
-      for (; i + 96 < m; i += 128) {
-        a0 += Lj[i] * x[i];
-        a1 += Lj[i + 32] * x[i + 32];
-        a2 += Lj[i + 64] * x[i + 64];
-        a3 += Lj[i + 96] * x[i + 96];
-      }
-      for (; i < m; i += 32) a0 += Lj[i] * x[i];
-      double acc = (a0 + a1) + (a2 + a3);
+    // x_j -= sum_{i >= i0} L_ij x_i for the block's columns: warp w takes the columns
+    // j = jb + w + (NT / 32) c, all of them at once (lane l: rows i0 + l + 32 t, four rows per
+    // pass), so that every lane keeps kR * kC loads in flight; a butterfly per column at the end
+    {
+      constexpr int kW = NT / 32, kC = 64 / kW;  // columns per warp
+      double acc[kC];
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-      if (lane == 0) x[j] -= acc;
+      for (int c = 0; c < kC; ++c) acc[c] = 0.0;
+      constexpr int kR = kDeep ? 4 : 2;  // rows per lane and pass
+      for (int i = i0 + lane; i < m; i += 32 * kR) {
+        double lv[kR][kC], xv[kR];
+#pragma unroll
+        for (int t = 0; t < kR; ++t) {
+          const int it = i + 32 * t;
+          xv[t] = it < m ? x[it] : 0.0;
+#pragma unroll
+          for (int c = 0; c < kC; ++c) {
+            const int j = warp + kW * c;
+            lv[t][c] = (it < m && j < wb) ? Fs[it + (int64_t)(jb + j) * m] : 0.0;
+          }
+        }
+#pragma unroll
+        for (int t = 0; t < kR; ++t)
+#pragma unroll
+          for (int c = 0; c < kC; ++c) acc[c] += lv[t][c] * xv[t];
+      }
+#pragma unroll
+      for (int c = 0; c < kC; ++c) {
+        double v = acc[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        const int j = warp + kW * c;
+        if (lane == 0 && j < wb) x[jb + j] -= v;
+      }
     }
     __syncthreads();
     const double v = inv_block_dot<NT>(linv_block(S, linv, b, s, bi), x + jb, wb, true);
@@ -613,10 +649,10 @@ __device__ __forceinline__ void bwd64_body(const DevSym& S, int s, int b, const 
 }
 
 template <int NT>
-__global__ void __launch_bounds__(NT) k_bwd64(DevSym S, const int* __restrict__ list, const double* __restrict__ F,
+__global__ void __launch_bounds__(NT, 1) k_bwd64(DevSym S, const int* __restrict__ list, const double* __restrict__ F,
                                              int64_t fstride, const double* __restrict__ linv, double* __restrict__ xp) {
   extern __shared__ double x[];
-  bwd64_body<NT>(S, list[blockIdx.x], blockIdx.y, F, fstride, linv, xp, x);
+  bwd64_body<NT, true>(S, list[blockIdx.x], blockIdx.y, F, fstride, linv, xp, x);
 }
 
 // Sweeps of fronts with m <= 32 rows (one 32-column block): one warp per (front,

@@ -416,11 +416,11 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_solve_persist(SolveArgs 
           fwd_tiny_warp(S, a.tiny_list[T.s + warp], b, a.F, a.fstride, a.xp, a.ub, a.ustride, ssm + 32 * warp);
         break;
       case ST_FWD:
-        if (S.lbo[T.s] >= 0) fwd64_body<kPersistThreads>(S, T.s, b, a.F, a.fstride, a.linv, a.xp, a.ub, a.ustride, ssm);
+        if (S.lbo[T.s] >= 0) fwd64_body<kPersistThreads, false>(S, T.s, b, a.F, a.fstride, a.linv, a.xp, a.ub, a.ustride, ssm);
         else fwd32_body<kPersistThreads>(S, T.s, b, a.F, a.fstride, a.xp, a.ub, a.ustride, ssm);
         break;
       case ST_BWD:
-        if (S.lbo[T.s] >= 0) bwd64_body<kPersistThreads>(S, T.s, b, a.F, a.fstride, a.linv, a.xp, ssm);
+        if (S.lbo[T.s] >= 0) bwd64_body<kPersistThreads, false>(S, T.s, b, a.F, a.fstride, a.linv, a.xp, ssm);
         else bwd32_body<kPersistThreads>(S, T.s, b, a.F, a.fstride, a.xp, ssm);
         break;
       default:
