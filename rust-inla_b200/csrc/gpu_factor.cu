@@ -293,8 +293,10 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
   set_smem(k_rows64, kRowsSmem);
   set_smem(k_fwd32<128>, (int)((S.max_m + 2 + 32 * 33) * 8));
   set_smem(k_bwd32<128>, (int)((S.max_m + 2 + 32 * 33) * 8));
-  set_smem(k_fwd64<256>, (int)((S.max_m + 2) * 8));
-  set_smem(k_bwd64<256>, (int)((S.max_m + 2) * 8));
+  set_smem(k_fwd64<256, true>, (int)((S.max_m + 2) * 8));
+  set_smem(k_fwd64<256, false>, (int)((S.max_m + 2) * 8));
+  set_smem(k_bwd64<256, true>, (int)((S.max_m + 2) * 8));
+  set_smem(k_bwd64<256, false>, (int)((S.max_m + 2) * 8));
   set_smem(k_gather8, 200 * 1024 + 8 * kGatherCols * 8);
   set_smem(k_si_step64, kSiGemmSmem);
   set_smem(k_si_diag64, kSiDiagSmem);
@@ -1122,8 +1124,12 @@ void GpuFactor::solve(double* d_x, int64_t xstride, int B, int slot0) {
         ++launches_;
       }
       if (!P.large.empty()) {
-        k_fwd64<256><<<dim3((unsigned)P.large.size(), B), 256, (P.mmax_large + 2) * 8, stream_>>>(
-            ds_, d_lists_.p + P.off_large, Fp, fs, Lp, xp_.p, ub_.p, us);
+        const dim3 g((unsigned)P.large.size(), B);
+        const int sm = (P.mmax_large + 2) * 8;
+        if ((int64_t)P.large.size() * B <= num_sms_)
+          k_fwd64<256, true><<<g, 256, sm, stream_>>>(ds_, d_lists_.p + P.off_large, Fp, fs, Lp, xp_.p, ub_.p, us);
+        else
+          k_fwd64<256, false><<<g, 256, sm, stream_>>>(ds_, d_lists_.p + P.off_large, Fp, fs, Lp, xp_.p, ub_.p, us);
         ++launches_;
       }
     }
@@ -1142,8 +1148,12 @@ void GpuFactor::solve(double* d_x, int64_t xstride, int B, int slot0) {
         ++launches_;
       }
       if (!P.large.empty()) {
-        k_bwd64<256><<<dim3((unsigned)P.large.size(), B), 256, (P.mmax_large + 2) * 8, stream_>>>(
-            ds_, d_lists_.p + P.off_large, Fp, fs, Lp, xp_.p);
+        const dim3 g((unsigned)P.large.size(), B);
+        const int sm = (P.mmax_large + 2) * 8;
+        if ((int64_t)P.large.size() * B <= num_sms_)
+          k_bwd64<256, true><<<g, 256, sm, stream_>>>(ds_, d_lists_.p + P.off_large, Fp, fs, Lp, xp_.p);
+        else
+          k_bwd64<256, false><<<g, 256, sm, stream_>>>(ds_, d_lists_.p + P.off_large, Fp, fs, Lp, xp_.p);
         ++launches_;
       }
     }

@@ -516,8 +516,9 @@ __device__ __forceinline__ double inv_block_dot(const double* __restrict__ lc, c
   return acc;
 }
 
-// Forward sweep of large front s, problem b (NT = 256 threads). kDeep: two rows per pass
-// instead of one (more loads in flight, more registers); the result is the same either way.
+// Forward sweep of large front s, problem b (NT = 256 threads). kDeep: two rows per pass and
+// 32 loads per row instead of one row and 16 (more loads in flight, more registers); the
+// result is the same either way.
 template <int NT, bool kDeep = true>
 __device__ __forceinline__ void fwd64_body(const DevSym& S, int s, int b, const double* __restrict__ F,
                                            int64_t fstride, const double* __restrict__ linv,
@@ -545,24 +546,26 @@ __device__ __forceinline__ void fwd64_body(const DevSym& S, int s, int b, const 
     __syncthreads();  // every read of y_J is done
     if (threadIdx.x % (NT / 64) == 0 && threadIdx.x / (NT / 64) < wb) y[jb + threadIdx.x / (NT / 64)] = v;
     __syncthreads();
-    // rows below: one thread per row, two rows per pass with 32 loads of each in flight (the
-    // panel streams from DRAM: the loads in flight set the rate), eight partial sums per row
+    // rows below: one thread per row (kDeep: two rows per pass, 32 loads of each in flight;
+    // otherwise one row, 16 loads: the panel streams from DRAM, so the loads in flight set the
+    // rate), eight partial sums per row in column order
     for (int r = jb + wb + threadIdx.x; r < m; r += (kDeep ? 2 : 1) * NT) {
       const int r2 = r + NT;
       const bool two = kDeep && r2 < m;
       double a[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
       double c[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
       const double* Lr = Fs + r + (int64_t)jb * m;
-      for (int j0 = 0; j0 < wb; j0 += 32) {
-        double la[32], lb[kDeep ? 32 : 1];
+      constexpr int kJ = kDeep ? 32 : 16;  // loads of a row per pass
+      for (int j0 = 0; j0 < wb; j0 += kJ) {
+        double la[kJ], lb[kDeep ? kJ : 1];
 #pragma unroll
-        for (int u = 0; u < 32; ++u) {
+        for (int u = 0; u < kJ; ++u) {
           const bool ok = j0 + u < wb;
           la[u] = ok ? Lr[(int64_t)(j0 + u) * m] : 0.0;
           if (kDeep) lb[kDeep ? u : 0] = ok && two ? Lr[(int64_t)(j0 + u) * m + NT] : 0.0;
         }
 #pragma unroll
-        for (int u = 0; u < 32; ++u) {
+        for (int u = 0; u < kJ; ++u) {
           const double yj = j0 + u < wb ? y[jb + j0 + u] : 0.0;
           a[u & 7] += la[u] * yj;
           if (kDeep) c[u & 7] += lb[kDeep ? u : 0] * yj;
@@ -579,12 +582,16 @@ __device__ __forceinline__ void fwd64_body(const DevSym& S, int s, int b, const 
   }
 }
 
-template <int NT>
-__global__ void __launch_bounds__(NT, 1) k_fwd64(DevSym S, const int* __restrict__ list, const double* __restrict__ F,
-                                             int64_t fstride, const double* __restrict__ linv, double* __restrict__ xp,
-                                             double* __restrict__ ub, int64_t ustride) {
+// kDeep: the register-hungry form (one CTA per SM) for launches with few CTAs; the other
+// (two CTAs per SM) for wide levels. Both give the same result.
+template <int NT, bool kDeep>
+__global__ void __launch_bounds__(NT, kDeep ? 1 : 2) k_fwd64(DevSym S, const int* __restrict__ list,
+                                                             const double* __restrict__ F, int64_t fstride,
+                                                             const double* __restrict__ linv,
+                                                             double* __restrict__ xp, double* __restrict__ ub,
+                                                             int64_t ustride) {
   extern __shared__ double y[];
-  fwd64_body<NT, true>(S, list[blockIdx.x], blockIdx.y, F, fstride, linv, xp, ub, ustride, y);
+  fwd64_body<NT, kDeep>(S, list[blockIdx.x], blockIdx.y, F, fstride, linv, xp, ub, ustride, y);
 }
 
 // Backward sweep of large front s, problem b (NT = 256 threads). kDeep: four rows per pass
@@ -648,11 +655,13 @@ __device__ __forceinline__ void bwd64_body(const DevSym& S, int s, int b, const 
   for (int t = threadIdx.x; t < k; t += NT) xb[f + t] = x[t];
 }
 
-template <int NT>
-__global__ void __launch_bounds__(NT, 1) k_bwd64(DevSym S, const int* __restrict__ list, const double* __restrict__ F,
-                                             int64_t fstride, const double* __restrict__ linv, double* __restrict__ xp) {
+template <int NT, bool kDeep>
+__global__ void __launch_bounds__(NT, kDeep ? 1 : 2) k_bwd64(DevSym S, const int* __restrict__ list,
+                                                             const double* __restrict__ F, int64_t fstride,
+                                                             const double* __restrict__ linv,
+                                                             double* __restrict__ xp) {
   extern __shared__ double x[];
-  bwd64_body<NT, true>(S, list[blockIdx.x], blockIdx.y, F, fstride, linv, xp, x);
+  bwd64_body<NT, kDeep>(S, list[blockIdx.x], blockIdx.y, F, fstride, linv, xp, x);
 }
 
 // Sweeps of fronts with m <= 32 rows (one 32-column block): one warp per (front,
