@@ -67,8 +67,9 @@ int64_t inla_kernel_launches(void);
  * users of the GPU in the same process). INLA_NO_MEMORY_CACHE in the environment
  * disables the cache. Symbolic analyses are cached the same way, per exact pattern,
  * ordering, options and permutation (at most 1 GiB of host memory; handles on the
- * same pattern reuse the analysis), and this call empties that cache too;
- * INLA_NO_SYMBOLIC_CACHE disables it. No reference counterpart. */
+ * same pattern reuse the analysis), and this call empties that cache too, together with the
+ * engine tables derived from each cached analysis (panel map, front positions: at most 1 GiB);
+ * INLA_NO_SYMBOLIC_CACHE disables both. No reference counterpart. */
 int inla_release_cached_memory(void);
 
 /* ------------------------------------------------------------------------

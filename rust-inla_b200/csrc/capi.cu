@@ -104,6 +104,7 @@ int inla_release_cached_memory(void) {
   try {
     device_release_cached();
     release_symbolic_cache();
+    release_host_maps();
     return INLA_OK;
   } catch (...) {
     return map_exception();

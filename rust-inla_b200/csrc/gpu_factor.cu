@@ -5,6 +5,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <atomic>
+#include <list>
 #include <mutex>
 
 #include "gpu_factor.hpp"
@@ -72,20 +73,43 @@ void set_smem(K kernel, int bytes) {
 }
 }  // namespace
 
-GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
-    : sym_(sym), max_batch_(max_batch), stream_(stream) {
-  const auto tstart = std::chrono::steady_clock::now();
-  if (max_batch < 1) throw std::runtime_error("max_batch must be >= 1");
-  const Symbolic& S = sym_;
-  const int64_t ns = S.nsuper, n = S.n;
-  nnz_ = (int64_t)S.rowidx.size();
-  if (n >= (1LL << 31) || (int64_t)S.sn_rows.size() >= (1LL << 31) || nnz_ >= (1LL << 31))
-    throw std::runtime_error("problem too large for 32-bit indices");
-  if (S.max_m > 25600) throw std::runtime_error("front with more than 25600 rows (extend-add slice exceeds shared memory)");
+// Host tables of a symbolic analysis that the engine uploads (32-bit supernode arrays, front
+// offsets, the panel map and the front positions of the input entries). They depend on the
+// analysis only, so they are built once per analysis id and shared by every engine created on
+// it (a model rebuilt on the same mesh skips the ~10-20 ms of building them); at most
+// kMapsCacheBytes are kept, most recently used first.
+namespace {
+constexpr size_t kMapsCacheBytes = size_t(1) << 30;
+std::mutex g_maps_mu;
+std::list<std::pair<uint64_t, std::shared_ptr<const HostMaps>>> g_maps;
+size_t g_maps_bytes = 0;
 
-  std::vector<int> first(ns + 1), rowptr(ns + 1), rows(S.sn_rows.size()), relx(S.sn_rows.size(), -1),
-      child_ptr(ns + 1), child_list(S.child_list.size()), parent(ns), uoff(ns + 1, 0), perm(n);
-  std::vector<int64_t> fptr(ns + 1, 0), lptr(ns + 1), dpos(n);
+size_t host_maps_bytes(const HostMaps& M) {
+  return sizeof(int) * (M.first.size() + M.rowptr.size() + M.rows.size() + M.relx.size() + M.child_ptr.size() +
+                        M.child_list.size() + M.parent.size() + M.uoff.size() + M.perm.size() + M.pmap.size()) +
+         sizeof(int64_t) * (M.fptr.size() + M.lptr.size() + M.dpos.size() + M.spos.size() + M.spos_full.size());
+}
+
+std::shared_ptr<const HostMaps> build_host_maps(const Symbolic& S) {
+  auto out = std::make_shared<HostMaps>();
+  HostMaps& M = *out;
+  const int64_t ns = S.nsuper, n = S.n;
+  const int64_t nnz_ = (int64_t)S.rowidx.size();
+  std::vector<int>&first = M.first, &rowptr = M.rowptr, &rows = M.rows, &relx = M.relx, &child_ptr = M.child_ptr,
+                   &child_list = M.child_list, &parent = M.parent, &uoff = M.uoff, &perm = M.perm;
+  std::vector<int64_t>&fptr = M.fptr, &lptr = M.lptr, &dpos = M.dpos;
+  first.resize(ns + 1);
+  rowptr.resize(ns + 1);
+  rows.resize(S.sn_rows.size());
+  relx.assign(S.sn_rows.size(), -1);
+  child_ptr.resize(ns + 1);
+  child_list.resize(S.child_list.size());
+  parent.resize(ns);
+  uoff.assign(ns + 1, 0);
+  perm.resize(n);
+  fptr.assign(ns + 1, 0);
+  lptr.resize(ns + 1);
+  dpos.resize(n);
   for (int64_t s = 0; s <= ns; ++s) {
     first[s] = (int)S.sn_first[s];
     rowptr[s] = (int)S.sn_rowptr[s];
@@ -106,12 +130,13 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
     }
   }
   for (int64_t j = 0; j < n; ++j) perm[j] = (int)S.perm[j];
-  ftotal_ = fptr[ns];
-  usum_ = uoff[ns];
 
   // panel map (compact panel index -> input entry) and front positions of input entries
-  std::vector<int> pmap(S.nnz_l_stored, -1);
-  std::vector<int64_t> spos(nnz_, -1), spos_full(nnz_, -1);
+  std::vector<int>& pmap = M.pmap;
+  std::vector<int64_t>&spos = M.spos, &spos_full = M.spos_full;
+  pmap.assign(S.nnz_l_stored, -1);
+  spos.assign(nnz_, -1);
+  spos_full.assign(nnz_, -1);
   parallel_for(n, [&](int64_t c0, int64_t c1) {  // disjoint writes: entry p, panel slot qmap[p]
     for (int64_t c = c0; c < c1; ++c)
       for (int64_t p = S.colptr[c]; p < S.colptr[c + 1]; ++p) {
@@ -129,6 +154,64 @@ GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
         spos[p] = spos_full[p];
       }
   });
+  return out;
+}
+}  // namespace
+
+void release_host_maps() {
+  std::lock_guard<std::mutex> lk(g_maps_mu);
+  g_maps.clear();
+  g_maps_bytes = 0;
+}
+
+std::shared_ptr<const HostMaps> host_maps(const Symbolic& S) {
+  // without the symbolic cache every engine has an analysis of its own: nothing to share
+  static const bool on = std::getenv("INLA_NO_SYMBOLIC_CACHE") == nullptr;
+  if (!on) return build_host_maps(S);
+  if (S.id != 0) {
+    std::lock_guard<std::mutex> lk(g_maps_mu);
+    for (auto it = g_maps.begin(); it != g_maps.end(); ++it)
+      if (it->first == S.id) {
+        g_maps.splice(g_maps.begin(), g_maps, it);
+        return g_maps.front().second;
+      }
+  }
+  std::shared_ptr<const HostMaps> m = build_host_maps(S);
+  if (S.id != 0) {
+    const size_t bytes = host_maps_bytes(*m);
+    std::lock_guard<std::mutex> lk(g_maps_mu);
+    if (bytes <= kMapsCacheBytes / 2) {
+      g_maps.emplace_front(S.id, m);
+      g_maps_bytes += bytes;
+      while (g_maps_bytes > kMapsCacheBytes && g_maps.size() > 1) {
+        g_maps_bytes -= host_maps_bytes(*g_maps.back().second);
+        g_maps.pop_back();
+      }
+    }
+  }
+  return m;
+}
+
+GpuFactor::GpuFactor(const Symbolic& sym, int max_batch, cudaStream_t stream)
+    : sym_(sym), max_batch_(max_batch), stream_(stream) {
+  const auto tstart = std::chrono::steady_clock::now();
+  if (max_batch < 1) throw std::runtime_error("max_batch must be >= 1");
+  const Symbolic& S = sym_;
+  const int64_t ns = S.nsuper, n = S.n;
+  nnz_ = (int64_t)S.rowidx.size();
+  if (n >= (1LL << 31) || (int64_t)S.sn_rows.size() >= (1LL << 31) || nnz_ >= (1LL << 31))
+    throw std::runtime_error("problem too large for 32-bit indices");
+  if (S.max_m > 25600) throw std::runtime_error("front with more than 25600 rows (extend-add slice exceeds shared memory)");
+
+  const std::shared_ptr<const HostMaps> maps = host_maps(S);
+  const HostMaps& M = *maps;
+  const std::vector<int>&first = M.first, &rowptr = M.rowptr, &rows = M.rows, &relx = M.relx,
+                  &child_ptr = M.child_ptr, &child_list = M.child_list, &parent = M.parent, &uoff = M.uoff,
+                  &perm = M.perm, &pmap = M.pmap;
+  const std::vector<int64_t>&fptr = M.fptr, &lptr = M.lptr, &dpos = M.dpos, &spos = M.spos,
+                      &spos_full = M.spos_full;
+  ftotal_ = fptr[ns];
+  usum_ = uoff[ns];
 
   const auto tm1 = std::chrono::steady_clock::now();
   d_first_.upload(first, stream_);

@@ -88,6 +88,17 @@ struct PersistPlan {
   std::vector<int2> grng;
   int nlarge = 0, smem = 0;
 };
+// Host tables of an analysis that an engine uploads: 32-bit copies of the supernode arrays,
+// front offsets fptr (sum m^2) and panel offsets lptr, D positions dpos, the panel map pmap
+// (compact panel index -> input entry) and the front positions of the input entries (spos:
+// entries stored in a panel; spos_full: every entry). Shared by the engines built on one
+// analysis (cached by Symbolic::id).
+struct HostMaps {
+  std::vector<int> first, rowptr, rows, relx, child_ptr, child_list, parent, uoff, perm, pmap;
+  std::vector<int64_t> fptr, lptr, dpos, spos, spos_full;
+};
+std::shared_ptr<const HostMaps> host_maps(const Symbolic& S);
+void release_host_maps();
 std::vector<LevelPlan> make_level_plans(const Symbolic& S, std::vector<int>& flat);
 bool make_persist_plan(const Symbolic& S, const std::vector<LevelPlan>& levels, PersistPlan& out);
 std::string check_persist_plan(const Symbolic& S, const PersistPlan& pl);

@@ -60,6 +60,7 @@ LaplaceEngine::LaplaceEngine(const LaplaceSpec& spec, int max_batch, cudaStream_
                  std::chrono::duration<double, std::milli>(t1 - t0).count(),
                  std::chrono::duration<double, std::milli>(t2 - t1).count());
 
+  const auto t3 = std::chrono::steady_clock::now();
   auto find = [&](int64_t row, int64_t col) -> int64_t {
     auto b = spec_.rowidx.begin() + spec_.colptr[col], e = spec_.rowidx.begin() + spec_.colptr[col + 1];
     auto it = std::lower_bound(b, e, row);
@@ -146,6 +147,7 @@ LaplaceEngine::LaplaceEngine(const LaplaceSpec& spec, int max_batch, cudaStream_
       }
   }
 
+  const auto t4 = std::chrono::steady_clock::now();
   comp_.upload(spec_.comp, stream_);
   y_.upload(spec_.y, stream_);
   if (!spec_.p1.empty()) p1_.upload(spec_.p1, stream_);
@@ -202,6 +204,10 @@ LaplaceEngine::LaplaceEngine(const LaplaceSpec& spec, int max_batch, cudaStream_
   bad_.alloc(B);
   stp_.alloc(B);
   INLA_CUDA(cudaStreamSynchronize(stream_));
+  if (std::getenv("INLA_DEBUG"))
+    std::fprintf(stderr, "laplace setup: observation tables %.1f ms, uploads and buffers %.1f ms\n",
+                 std::chrono::duration<double, std::milli>(t4 - t3).count(),
+                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t4).count());
 }
 
 LaplaceEngine::~LaplaceEngine() = default;

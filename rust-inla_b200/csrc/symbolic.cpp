@@ -5,6 +5,7 @@
 #include "host_par.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -639,6 +640,8 @@ void analyze(int64_t n, const int64_t* colptr, const int64_t* rowidx, const Symb
       }
   }
   analyze_uncached(n, colptr, rowidx, opt, custom_perm, S);
+  static std::atomic<uint64_t> next_id{1};
+  S.id = next_id.fetch_add(1);
   if (!sym_cache_enabled()) return;
   SymCacheEntry e;
   e.n = n;

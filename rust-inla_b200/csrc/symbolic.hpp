@@ -40,6 +40,10 @@ struct SymbolicOptions {
 };
 
 struct Symbolic {
+  // Identity of the analysis: every analysis computed gets a new id, and the copies the
+  // process-wide cache hands out keep the id of the analysis they copy, so equal ids mean equal
+  // contents (tables derived from an analysis can be cached by id). 0: not from analyze().
+  uint64_t id = 0;
   int64_t n = 0;
   int order_used = ORDER_AMD;
   // perm[new] = old ; iperm[old] = new (after postordering)
