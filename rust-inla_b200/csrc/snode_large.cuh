@@ -1111,9 +1111,10 @@ __global__ void __launch_bounds__(256) k_si_step64(DevSym S, const int* __restri
                                                   int* __restrict__ cnt, int smax, int allow_split) {
   extern __shared__ double smem64[];
   const int64_t slot = (int64_t)blockIdx.x * gridDim.y + blockIdx.y;
+  // gpart is sized for split launches only (smax > 1)
   si_step64_body(S, list[blockIdx.x], blockIdx.y, blockIdx.z, jb, F, Sg, fstride,
                  ppart + slot * ptiles * (kB64 * kB64), linv, smem64,
-                 gpart + slot * ptiles * smax * (kB64 * kB64), cnt + slot * ptiles, ptiles, smax,
+                 smax > 1 ? gpart + slot * ptiles * smax * (kB64 * kB64) : gpart, cnt + slot * ptiles, ptiles, smax,
                  allow_split != 0);
 }
 
