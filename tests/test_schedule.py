@@ -53,3 +53,17 @@ def test_other_schedules(q):
 def test_block_diagonal_schedule():
     blocks = [grid_laplacian(8 + i, 7, ridge=0.5) for i in range(12)]
     check(sp.block_diag(blocks).tocsc(), _lib.ORDER_ND)
+
+
+def test_schedule_setters_reject_out_of_range_values():
+    """The process-wide schedule choices (no device needed): persistent-schedule mode 0..2 and
+    panel form -1..2 are accepted, anything else is INLA_ERR_INVALID and leaves the setting as it was."""
+    lib = _lib.lib()
+    for bad in (-1, 3):
+        assert lib.inla_set_persistent_schedule(bad) == _lib.INLA_ERR_INVALID
+    for bad in (-2, 3, 100):
+        assert lib.inla_set_panel_form(bad) == _lib.INLA_ERR_INVALID
+        assert "panel form" in lib.inla_last_error().decode()
+    for ok in (0, 1, 2, -1):
+        assert lib.inla_set_panel_form(ok) == _lib.INLA_OK
+    assert lib.inla_set_persistent_schedule(1) == _lib.INLA_OK
