@@ -504,8 +504,16 @@ void InlaDriver::newton(std::vector<double>& x, const FitOptions& opt, int& iter
     if (std::getenv("INLA_DEBUG"))
       std::fprintf(stderr, "newton it=%d f=%.10g |g|=%.3g delta=%.3g alpha=%.3g capped=%d\n", it, f, gmax, delta,
                    kA[best], (int)capped);
-    if (best == 0 && capped) delta = std::min(4.0 * delta, 8.0);
-    else if (best > 0) delta = std::max(0.25, kA[best] * std::min(pmax, delta));
+    // trust radius from the agreement of the decrease with the quadratic model's prediction
+    // (the ratio test of Nocedal & Wright, Numerical Optimization, 2nd ed., Alg. 4.1): grow it
+    // twofold after a capped full step with ratio > 3/4, shrink it to a quarter of the step
+    // taken when the ratio is below 1/4; along the |eigenvalue|-modified Newton direction the
+    // predicted decrease of the step a * p (p capped by the factor sc) is -a slope (1 - a sc / 2)
+    const double sc = capped ? delta / pmax : 1.0, a = kA[best];
+    const double pred = -a * slope * (1.0 - 0.5 * a * sc), rho = pred > 0 ? (fprev - f) / pred : 0.0;
+    if (rho > 0.75 && capped && best == 0) delta = std::min(2.0 * delta, 8.0);
+    else if (rho < 0.25) delta = std::max(0.25, 0.25 * a * std::min(pmax, delta));
+    else if (best > 0) delta = std::max(0.25, a * std::min(pmax, delta));
     if (std::fabs(fprev - f) < 1e-12 * (1.0 + std::fabs(f))) break;
   }
 }
