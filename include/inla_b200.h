@@ -132,7 +132,7 @@ int inla_solver_supernodes(const inla_solver* s, int64_t* first, int64_t* count)
 int inla_solver_colcounts(const inla_solver* s, int64_t* counts);
 
 /* ------------------------------------------------------------------------
- * 2-D meshes for SPDE models (crates/inla_fmesher/src/fmesher.rs), host only.
+ * 2-D meshes for SPDE models (crates/inla_fmesher/src/fmesher.rs), host forms.
  * ---------------------------------------------------------------------- */
 typedef struct inla_mesh inla_mesh;
 /* build_mesh2d (fmesher.rs:119-158, validation 870-893): xy [nv][2], tri [ntri][3] (0-based).
@@ -178,6 +178,50 @@ int inla_mesh1d_projector(int64_t n, const double* loc, int64_t npts, const doub
  * INLA_ERR_INVALID for |c0_i| < 1e-15 ("Zero entry in mass matrix c0 diagonal"). */
 int inla_spde_components(int64_t n, const double* c0, const int64_t* g_colptr, const int64_t* g_rowidx,
                          const double* g_vals, int64_t* nnz, int64_t* colptr, int64_t* rowidx, double* comp);
+
+/* ------------------------------------------------------------------------
+ * Device forms of the mesh tools, equal bit for bit to the host forms above.
+ * The first device call on a mesh builds its patterns and per-entry contribution lists on the
+ * host (topology only) and copies the mesh to the current device; later calls must run on that
+ * device. Calls on one mesh (or one SPDE plan) must not overlap: they share its scratch.
+ * ---------------------------------------------------------------------- */
+/* Pattern of FEM block `which` (0 c0, 1 c1, 2 g1, 3 b1) in CSC, the same as inla_mesh_fem_block's
+ * after inla_mesh_fem: it depends on the topology only (c1 and g1 share it). Host only; call
+ * with NULL arrays to read nnz; colptr has nv + 1 entries. */
+int inla_mesh_fem_pattern(inla_mesh* m, int which, int64_t* nnz, int64_t* colptr, int64_t* rowidx);
+/* assemble_fem_blocks_diffusion (fmesher.rs:515-626) on the device: the values of c0 / c1 / g1 / b1
+ * on inla_mesh_fem_pattern's patterns (device arrays of nnz doubles; any may be NULL) and d_areas
+ * [ntri] (may be NULL), queued on `stream` without synchronizing. d_triangle_scale: device
+ * [ntri] or NULL (all 1); diffusion: host {hxx, hxy, hyy} or NULL (identity). One thread per
+ * entry sums the entry's per-triangle contributions in triangle order with separately rounded
+ * operations, so every value equals inla_mesh_fem's. INLA_ERR_INVALID for a non-finite or
+ * non-SPD diffusion tensor (the host form's messages). */
+int inla_mesh_fem_dev(inla_mesh* m, const double* d_triangle_scale, const double* diffusion, double* d_areas,
+                      double* d_c0, double* d_c1, double* d_g1, double* d_b1, void* stream);
+/* observation_projector_triplets (fmesher.rs:168-219) on the device: d_xy [npts][2] (device);
+ * A in CSR into d_rowptr [npts + 1], d_colidx / d_vals (at most 3 npts each); *nnz (host) the
+ * entries written. Each point is located by a walk from a triangle near it; a point inside its
+ * triangle by more than rounding can move an edge test keeps that triangle, which every walk
+ * reaches, and the others (on or near edges and vertices, or whose walk left the mesh) are
+ * located again on the host in point order from the previous point's triangle, as
+ * inla_mesh_projector does; the result equals inla_mesh_projector's bit for bit, with the same
+ * INLA_ERR_INVALID for the first point outside the mesh. Synchronizes the stream. */
+int inla_mesh_projector_dev(inla_mesh* m, int64_t npts, const double* d_xy, int64_t* d_rowptr, int64_t* d_colidx,
+                            double* d_vals, int64_t* nnz, void* stream);
+/* spde_precision_csc's components (spde.rs:70-140) on the device for a fixed G1 pattern (host
+ * CSC, rows strictly ascending in each column, e.g. inla_mesh_fem_pattern(m, 2, ...)).
+ * inla_spde_plan_pattern gives the components' pattern, the same as inla_spde_components'
+ * (NULL arrays to read nnz). inla_spde_components_dev: d_c0 [n] the lumped mass diagonal and
+ * d_g_vals the G1 values on its pattern (device) -> d_comp [3][nnz] (C0, G1, G1 C0^-1 G1), equal
+ * to inla_spde_components' bit for bit, queued on `stream`; d_status (device int, may be NULL) is
+ * set to 0, or to 1 when some |c0_i| < 1e-15 (the host form's "Zero entry in mass matrix c0
+ * diagonal"). */
+typedef struct inla_spde_plan inla_spde_plan;
+int inla_spde_plan_create(int64_t n, const int64_t* g_colptr, const int64_t* g_rowidx, inla_spde_plan** out);
+void inla_spde_plan_free(inla_spde_plan* p);
+int inla_spde_plan_pattern(const inla_spde_plan* p, int64_t* nnz, int64_t* colptr, int64_t* rowidx);
+int inla_spde_components_dev(inla_spde_plan* p, const double* d_c0, const double* d_g_vals, double* d_comp,
+                             int* d_status, void* stream);
 
 /* scale_model_csc (crates/inla_math/src/design.rs:150-195): fac = exp(mean(log d_i)) over the
  * positive finite d = diag(Q^+) (Moore-Penrose inverse), Q_scaled = fac Q. The reference

@@ -126,6 +126,13 @@ SIGNATURES = [
     ("inla_mesh_locate", C.c_int, [P, I64, DP, LP, DP]),
     ("inla_mesh_projector", C.c_int, [P, I64, DP, LP, LP, DP]),
     ("inla_spde_components", C.c_int, [I64, DP, LP, LP, DP, LP, LP, LP, DP]),
+    ("inla_mesh_fem_pattern", C.c_int, [P, C.c_int, LP, LP, LP]),
+    ("inla_mesh_fem_dev", C.c_int, [P, P, DP, P, P, P, P, P, P]),
+    ("inla_mesh_projector_dev", C.c_int, [P, I64, P, P, P, P, LP, P]),
+    ("inla_spde_plan_create", C.c_int, [I64, LP, LP, C.POINTER(P)]),
+    ("inla_spde_plan_free", None, [P]),
+    ("inla_spde_plan_pattern", C.c_int, [P, LP, LP, LP]),
+    ("inla_spde_components_dev", C.c_int, [P, P, P, P, P, P]),
     ("inla_mesh1d_fem", C.c_int, [I64, DP, C.c_int, LP, LP, LP, DP]),
     ("inla_mesh1d_projector", C.c_int, [I64, DP, I64, DP, LP, LP, DP]),
     ("inla_predictor_moments", C.c_int, [I64, I64, LP, LP, DP, C.c_int, DP, DP, DP, DP, DP]),

@@ -235,3 +235,51 @@ def test_barrier_spde_reduces_covariance_across_strip():
         q = _q_from_components(pattern, comp, 1.0, 1.0).toarray()
         covs.append(abs(np.linalg.inv(q)[0, nxv - 1]))
     assert covs[1] < 0.5 * covs[0], covs
+
+
+# --- device forms: what needs no GPU (patterns, plan validation, loud failure without a device) ---
+
+from inla_b200.mesh import SpdePlan  # noqa: E402
+
+
+@pytest.mark.parametrize("nx,seed", [(2, 1), (12, 5), (40, 7)])
+def test_device_fem_patterns_equal_the_host_blocks(nx, seed):
+    """The device forms' patterns come from the topology alone and equal the host assembly's."""
+    if nx == 2:
+        m = Mesh(SQUARE_V, SQUARE_T)
+    else:
+        v, t = _jittered(nx, seed)
+        m = Mesh(v, t)
+    f = m.fem(triangle_scale=None)
+    for name in FEM_BLOCKS:
+        cp, ri = m.fem_pattern(name)
+        assert np.array_equal(cp, f[name].indptr) and np.array_equal(ri, f[name].indices), name
+
+
+def test_spde_plan_pattern_equals_the_host_components():
+    v, t = _jittered(20, 3)
+    f = Mesh(v, t).fem()
+    pat, _ = spde_components(f["c0"].diagonal(), f["g1"])
+    plan = SpdePlan(len(v), f["g1"].indptr, f["g1"].indices)
+    assert np.array_equal(plan.colptr, pat.indptr) and np.array_equal(plan.rowidx, pat.indices)
+
+
+def test_spde_plan_rejects_unsorted_or_out_of_range_rows():
+    with pytest.raises(InlaError, match="strictly ascending"):
+        SpdePlan(2, [0, 2, 3], [1, 0, 1])
+    with pytest.raises(InlaError, match="out of range"):
+        SpdePlan(2, [0, 1, 2], [0, 5])
+    with pytest.raises(InlaError, match="non-empty"):
+        SpdePlan(0, [0], [])
+
+
+def test_device_mesh_calls_fail_loudly_without_a_device():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("device present")
+    from inla_b200 import _lib
+
+    m = Mesh(SQUARE_V, SQUARE_T)
+    rc = _lib.lib().inla_mesh_fem_dev(m._h, None, None, None, None, None, None, None, None)
+    assert rc == _lib.INLA_ERR_CUDA
