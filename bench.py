@@ -172,6 +172,7 @@ def cpu_theta_evals(p, seconds: float, threads: int, perm, want_var: bool = Fals
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
 
+    O.set_supernodal(True)  # the supernodal form with per-pattern analyses, as the reference factorizes
     rng = np.random.default_rng(7)
     base = np.array([4.6, -3.9, 2.65])
     thetas = [base + 0.05 * rng.standard_normal(3) for _ in range(4096)]
@@ -203,8 +204,10 @@ def cpu_perm(p):
     return O.reference_perm(p.model.pattern)
 
 
-CPU_KIND_NOTE = ("CPU oracle: C restatement of rust-inla's path with a simplicial up-looking LDL^T and "
-                 "Takahashi recurrence, not faer's supernodal factorization")
+CPU_KIND_NOTE = ("CPU oracle: C restatement of rust-inla's path: a supernodal LDL^T (postordered "
+                 "elimination tree, relaxed supernodes, dense panels; analysis cached per pattern as "
+                 "the reference's pattern cache does) written here, not faer's own code, and the "
+                 "reference's Takahashi recurrence")
 
 
 def bench_config(p, args, ws):

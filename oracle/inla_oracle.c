@@ -5,6 +5,7 @@
 #include "inla_oracle.h"
 
 #include <math.h>
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -319,16 +320,22 @@ struct orc_factor {
   int64_t *perm, *iperm;
   int64_t *lp, *li; /* strictly lower L by column, rows ascending */
   double *lx, *d;
+  struct sn_sym* shared; /* the cached supernodal analysis owning perm, iperm, lp, li, or NULL */
 };
+static void sn_release(struct sn_sym* S);
 
 int64_t orc_factor_nnz(const orc_factor* f) { return f->lp[f->n] + f->n; }
 
 void orc_factor_free(orc_factor* f) {
   if (!f) return;
-  free(f->perm);
-  free(f->iperm);
-  free(f->lp);
-  free(f->li);
+  if (f->shared) {
+    sn_release(f->shared);
+  } else {
+    free(f->perm);
+    free(f->iperm);
+    free(f->lp);
+    free(f->li);
+  }
   free(f->lx);
   free(f->d);
   free(f);
@@ -454,6 +461,435 @@ void orc_solve(const orc_factor* f, const double* b, double* x) {
     for (int64_t p = f->lp[j]; p < f->lp[j + 1]; ++p) w[j] -= f->lx[p] * w[f->li[p]];
   for (int64_t j = 0; j < n; ++j) x[f->perm[j]] = w[j];
   free(w);
+}
+
+/* ------------------------------------------------------------------------ */
+/* LDL^T (supernodal): the CPU baseline's factorization                     */
+/* ------------------------------------------------------------------------ */
+/* The reference factorizes with faer's supernodal LDL^T (sparse_ldlt.rs:196-241 ->
+ * faer 0.24 factorize_numeric_ldlt; faer's source is not available here). This is a plain
+ * supernodal LDL^T of the same matrix, used to time a CPU path shaped like the reference's:
+ * fundamental supernodes (column j joins column j-1's supernode when j is j-1's etree parent and
+ * j-1 has one more strictly-lower entry), one dense column-major panel per supernode holding its
+ * rows, the panel factored column by column, and its Schur complement L21 D L21^T subtracted from
+ * the later supernodes' panels (right-looking). The factor equals orc_factor_create's to
+ * rounding and is stored the same way, so orc_logdet, orc_solve and the Takahashi functions
+ * apply unchanged. Same D gate (sparse_ldlt.rs:117-120). */
+#define ORC_SN_MAXW 128
+#define ORC_SN_ZEROS 0.1
+
+static int g_supernodal = 0;
+void orc_set_supernodal(int on) { g_supernodal = on; }
+
+/* perm composed with a postorder of the elimination tree of the matrix permuted by perm
+ * (children in increasing order): the same fill, and parent-child chains become contiguous. */
+static void postordered_perm(int64_t n, const int64_t* cp, const int64_t* ri, const int64_t* perm, int64_t* out) {
+  int64_t* iperm = (int64_t*)malloc(sizeof(int64_t) * n);
+  for (int64_t k = 0; k < n; ++k) iperm[perm ? perm[k] : k] = k;
+  int64_t* ap = (int64_t*)calloc(n + 1, sizeof(int64_t));
+  for (int64_t c = 0; c < n; ++c)
+    for (int64_t p = cp[c]; p < cp[c + 1]; ++p)
+      if (ri[p] >= c) ap[MAXI(iperm[ri[p]], iperm[c]) + 1]++;
+  for (int64_t k = 0; k < n; ++k) ap[k + 1] += ap[k];
+  int64_t* ai = (int64_t*)malloc(sizeof(int64_t) * (ap[n] + 1));
+  int64_t* fill = (int64_t*)malloc(sizeof(int64_t) * (n + 1));
+  memcpy(fill, ap, sizeof(int64_t) * (n + 1));
+  for (int64_t c = 0; c < n; ++c)
+    for (int64_t p = cp[c]; p < cp[c + 1]; ++p)
+      if (ri[p] >= c) {
+        const int64_t i = iperm[ri[p]], j = iperm[c];
+        ai[fill[MAXI(i, j)]++] = MINI(i, j);
+      }
+  int64_t* parent = (int64_t*)malloc(sizeof(int64_t) * n);
+  int64_t* anc = (int64_t*)malloc(sizeof(int64_t) * n);
+  for (int64_t k = 0; k < n; ++k) { /* etree with path compression */
+    parent[k] = -1;
+    anc[k] = -1;
+    for (int64_t p = ap[k]; p < ap[k + 1]; ++p)
+      for (int64_t i = ai[p]; i != -1 && i < k;) {
+        const int64_t next = anc[i];
+        anc[i] = k;
+        if (next == -1) parent[i] = k;
+        i = next;
+      }
+  }
+  /* children lists (increasing), then an iterative depth-first postorder from each root */
+  int64_t* head = anc; /* reuse */
+  int64_t* nxt = fill;
+  for (int64_t k = 0; k < n; ++k) head[k] = -1;
+  for (int64_t k = n - 1; k >= 0; --k)
+    if (parent[k] != -1) {
+      nxt[k] = head[parent[k]];
+      head[parent[k]] = k;
+    }
+  int64_t* stack = ap; /* n + 1 entries */
+  int64_t cnt = 0;
+  for (int64_t r = 0; r < n; ++r) {
+    if (parent[r] != -1) continue;
+    int64_t top = 0;
+    stack[top++] = r;
+    while (top > 0) {
+      const int64_t v = stack[top - 1];
+      const int64_t c = head[v];
+      if (c == -1) {
+        --top;
+        out[cnt++] = perm ? perm[v] : v;
+      } else {
+        head[v] = nxt[c];
+        stack[top++] = c;
+      }
+    }
+  }
+  free(iperm);
+  free(ap);
+  free(ai);
+  free(fill);
+  free(parent);
+  free(anc);
+}
+
+/* Numeric phase of orc_factor_create_sn: each supernode's panel factored column by column, its
+ * Schur complement subtracted from the later panels, the columns copied into the factor. Built
+ * for AVX2 + FMA and for baseline x86-64, the first the CPU supports chosen at load time. */
+#if defined(__x86_64__) && defined(__GNUC__) && !defined(__clang__)
+__attribute__((target_clones("arch=x86-64-v3", "default")))
+#endif
+static void sn_numeric(orc_factor* f, int64_t ns, const int64_t* sfirst, const int64_t* sn_of, const int64_t* sptr,
+                       const int64_t* srows, const int64_t* poff, double* panel, double* t, double* ucol,
+                       int64_t* pos) {
+  for (int64_t s = 0; s < ns; ++s) {
+    const int64_t c0 = sfirst[s], w = sfirst[s + 1] - c0, m = sptr[s + 1] - sptr[s];
+    double* P = panel + poff[s];
+    const int64_t* R = srows + sptr[s];
+    for (int64_t c = 0; c < w; ++c) { /* column c of the panel */
+      double* Pc = P + c * m;
+      const double d = Pc[c];
+      f->d[c0 + c] = d;
+      for (int64_t r = c + 1; r < m; ++r) {
+        t[r] = Pc[r];
+        Pc[r] = t[r] / d;
+      }
+      for (int64_t c2 = c + 1; c2 < w; ++c2) {
+        const double tc = t[c2];
+        double* P2 = P + c2 * m;
+        for (int64_t r = c2; r < m; ++r) P2[r] -= Pc[r] * tc;
+      }
+    }
+    const int64_t nb = m - w; /* rows below the supernode */
+    for (int64_t a = 0; a < nb;) {
+      const int64_t ts = sn_of[R[w + a]], tf = sfirst[ts], tl = sfirst[ts + 1], tm = sptr[ts + 1] - sptr[ts];
+      const int64_t* TR = srows + sptr[ts];
+      double* TP = panel + poff[ts];
+      int64_t q = 0;
+      for (int64_t b = a; b < nb; ++b) { /* rows below column a lie in the target's rows */
+        while (TR[q] < R[w + b]) ++q;
+        pos[b] = q;
+      }
+      int64_t a_end = a;
+      while (a_end < nb && R[w + a_end] < tl) ++a_end;
+      /* four target columns at a time: each load of L21 feeds four accumulators (rows above a
+       * column's own row are computed and not used) */
+      for (int64_t a2 = a; a2 < a_end; a2 += 4) {
+        const int64_t nc = MINI(4, a_end - a2);
+        double* u0 = ucol;
+        double* u1 = ucol + nb;
+        double* u2 = ucol + 2 * nb;
+        double* u3 = ucol + 3 * nb;
+        for (int64_t b = a2; b < nb; ++b) u0[b] = u1[b] = u2[b] = u3[b] = 0.0;
+        for (int64_t c = 0; c < w; ++c) {
+          const double dc = f->d[c0 + c];
+          const double* Lc = P + c * m + w;
+          const double k0 = dc * Lc[a2], k1 = nc > 1 ? dc * Lc[a2 + 1] : 0.0, k2 = nc > 2 ? dc * Lc[a2 + 2] : 0.0,
+                       k3 = nc > 3 ? dc * Lc[a2 + 3] : 0.0;
+          for (int64_t b = a2; b < nb; ++b) {
+            const double l = Lc[b];
+            u0[b] += l * k0;
+            u1[b] += l * k1;
+            u2[b] += l * k2;
+            u3[b] += l * k3;
+          }
+        }
+        double* us[4] = {u0, u1, u2, u3};
+        for (int64_t j = 0; j < nc; ++j) {
+          double* TPc = TP + (R[w + a2 + j] - tf) * tm;
+          const double* u = us[j];
+          for (int64_t b = a2 + j; b < nb; ++b) TPc[pos[b]] -= u[b];
+        }
+      }
+      a = a_end;
+    }
+    for (int64_t c = 0; c < w; ++c) { /* column c0 + c of L: its structure's rows among R[c+1..m) */
+      const int64_t col = c0 + c;
+      int64_t r = c + 1;
+      for (int64_t p = f->lp[col]; p < f->lp[col + 1]; ++p) {
+        while (R[r] < f->li[p]) ++r;
+        f->lx[p] = P[c * m + r];
+      }
+    }
+  }
+}
+
+/* Structure of a supernodal factor, computed once per (pattern, ordering) and shared, as the
+ * reference refactorizes numerically on an unchanged pattern (scratch.rs:90-119). */
+typedef struct sn_sym {
+  int64_t n, nnz_in;
+  int64_t *key_cp, *key_ri, *key_perm; /* the inputs it was computed from (key_perm NULL: natural) */
+  int64_t *perm, *iperm, *lp, *li;      /* factor order and structure (shared with the factors) */
+  int64_t ns, maxm, npanel;
+  int64_t *sfirst, *sn_of, *sptr, *srows, *poff;
+  int64_t* vmap; /* input entry -> panel position (-1 for entries above the diagonal) */
+  int64_t refs;  /* factors using it; a retired analysis is freed with its last factor */
+  int retired;
+  struct sn_sym* next;
+} sn_sym;
+
+static sn_sym* sn_analyze(int64_t n, const int64_t* cp, const int64_t* ri, const int64_t* perm_in) {
+  sn_sym* S = (sn_sym*)calloc(1, sizeof(sn_sym));
+  S->n = n;
+  S->nnz_in = cp[n];
+  S->key_cp = (int64_t*)malloc(sizeof(int64_t) * (n + 1));
+  memcpy(S->key_cp, cp, sizeof(int64_t) * (n + 1));
+  S->key_ri = (int64_t*)malloc(sizeof(int64_t) * (cp[n] + 1));
+  memcpy(S->key_ri, ri, sizeof(int64_t) * cp[n]);
+  if (perm_in) {
+    S->key_perm = (int64_t*)malloc(sizeof(int64_t) * n);
+    memcpy(S->key_perm, perm_in, sizeof(int64_t) * n);
+  }
+  S->perm = (int64_t*)malloc(sizeof(int64_t) * (n > 0 ? n : 1));
+  postordered_perm(n, cp, ri, perm_in, S->perm);
+  S->iperm = (int64_t*)malloc(sizeof(int64_t) * (n > 0 ? n : 1));
+  for (int64_t k = 0; k < n; ++k) S->iperm[S->perm[k]] = k;
+  const int64_t* iperm = S->iperm;
+  /* row k of the permuted lower triangle: columns lo <= k */
+  int64_t* ap = (int64_t*)calloc(n + 1, sizeof(int64_t));
+  for (int64_t c = 0; c < n; ++c)
+    for (int64_t p = cp[c]; p < cp[c + 1]; ++p)
+      if (ri[p] >= c) ap[MAXI(iperm[ri[p]], iperm[c]) + 1]++;
+  for (int64_t k = 0; k < n; ++k) ap[k + 1] += ap[k];
+  int64_t* ai = (int64_t*)malloc(sizeof(int64_t) * (ap[n] + 1));
+  int64_t* fill = (int64_t*)malloc(sizeof(int64_t) * (n + 1));
+  memcpy(fill, ap, sizeof(int64_t) * (n + 1));
+  for (int64_t c = 0; c < n; ++c)
+    for (int64_t p = cp[c]; p < cp[c + 1]; ++p)
+      if (ri[p] >= c) {
+        const int64_t i = iperm[ri[p]], j = iperm[c];
+        ai[fill[MAXI(i, j)]++] = MINI(i, j);
+      }
+  /* elimination tree and strictly-lower column counts (row subtrees) */
+  int64_t* parent = (int64_t*)malloc(sizeof(int64_t) * (n > 0 ? n : 1));
+  int64_t* flag = (int64_t*)malloc(sizeof(int64_t) * (n > 0 ? n : 1));
+  int64_t* lnz = (int64_t*)calloc(n > 0 ? n : 1, sizeof(int64_t));
+  for (int64_t k = 0; k < n; ++k) {
+    parent[k] = -1;
+    flag[k] = k;
+    for (int64_t p = ap[k]; p < ap[k + 1]; ++p)
+      for (int64_t i = ai[p]; i < k && flag[i] != k; i = parent[i]) {
+        if (parent[i] == -1) parent[i] = k;
+        lnz[i]++;
+        flag[i] = k;
+      }
+  }
+  S->lp = (int64_t*)malloc(sizeof(int64_t) * (n + 1));
+  S->lp[0] = 0;
+  for (int64_t k = 0; k < n; ++k) S->lp[k + 1] = S->lp[k] + lnz[k];
+  S->li = (int64_t*)malloc(sizeof(int64_t) * (S->lp[n] + 1));
+  /* row structures: row k appended to every column of its row subtree (rows ascend) */
+  for (int64_t k = 0; k < n; ++k) {
+    fill[k] = 0;
+    flag[k] = -1;
+  }
+  for (int64_t k = 0; k < n; ++k) {
+    flag[k] = k;
+    for (int64_t p = ap[k]; p < ap[k + 1]; ++p)
+      for (int64_t i = ai[p]; i < k && flag[i] != k; i = parent[i]) {
+        S->li[S->lp[i] + fill[i]++] = k;
+        flag[i] = k;
+      }
+  }
+  /* supernodes: chains j-1 -> j = parent(j-1) of at most ORC_SN_MAXW columns. Column j-1's
+   * structure below j is contained in column j's; a chain's panel holds the chain's columns and
+   * the last column's structure, so a column whose structure is smaller carries explicit zeros
+   * there. A chain grows while those zeros stay within ORC_SN_ZEROS of its panel. */
+  S->sfirst = (int64_t*)malloc(sizeof(int64_t) * (n + 1));
+  S->sn_of = (int64_t*)malloc(sizeof(int64_t) * (n > 0 ? n : 1));
+  int64_t ns = n > 0 ? 1 : 0, zeros = 0;
+  S->sfirst[0] = 0;
+  if (n > 0) S->sn_of[0] = 0;
+  for (int64_t j = 1; j < n; ++j) {
+    const int64_t f0 = S->sfirst[ns - 1], w = j - f0;
+    int join = parent[j - 1] == j && w < ORC_SN_MAXW;
+    if (join) {
+      const int64_t extra = lnz[j] + 1 - lnz[j - 1]; /* rows of struct(j) the chain's columns lack */
+      const int64_t z = zeros + w * extra, m = w + 1 + lnz[j];
+      join = extra == 0 || (double)z <= ORC_SN_ZEROS * (double)(m * (w + 1));
+      if (join) zeros = z;
+    }
+    if (!join) {
+      S->sfirst[ns++] = j;
+      zeros = 0;
+    }
+    S->sn_of[j] = ns - 1;
+  }
+  S->sfirst[ns] = n;
+  S->ns = ns;
+  /* rows of each supernode (its columns, then its last column's structure) and panel offsets */
+  S->sptr = (int64_t*)malloc(sizeof(int64_t) * (ns + 1));
+  S->poff = (int64_t*)malloc(sizeof(int64_t) * (ns + 1));
+  S->sptr[0] = S->poff[0] = 0;
+  S->maxm = 1;
+  for (int64_t s = 0; s < ns; ++s) {
+    const int64_t w = S->sfirst[s + 1] - S->sfirst[s], m = w + lnz[S->sfirst[s + 1] - 1];
+    S->sptr[s + 1] = S->sptr[s] + m;
+    S->poff[s + 1] = S->poff[s] + m * w;
+    S->maxm = MAXI(S->maxm, m);
+  }
+  S->npanel = S->poff[ns];
+  S->srows = (int64_t*)malloc(sizeof(int64_t) * (S->sptr[ns] + 1));
+  for (int64_t s = 0; s < ns; ++s) {
+    const int64_t c0 = S->sfirst[s], last = S->sfirst[s + 1] - 1;
+    for (int64_t c = c0; c <= last; ++c) S->srows[S->sptr[s] + c - c0] = c;
+    memcpy(S->srows + S->sptr[s] + (last - c0 + 1), S->li + S->lp[last], sizeof(int64_t) * lnz[last]);
+  }
+  /* input entry (row >= col) -> position of (hi, lo) in lo's panel */
+  S->vmap = (int64_t*)malloc(sizeof(int64_t) * (cp[n] + 1));
+  for (int64_t c = 0; c < n; ++c)
+    for (int64_t p = cp[c]; p < cp[c + 1]; ++p) {
+      S->vmap[p] = -1;
+      if (ri[p] < c) continue;
+      const int64_t i = iperm[ri[p]], j = iperm[c], hi = MAXI(i, j), lo = MINI(i, j);
+      const int64_t s = S->sn_of[lo], m = S->sptr[s + 1] - S->sptr[s];
+      const int64_t* R = S->srows + S->sptr[s];
+      int64_t a = 0, b = m - 1;
+      while (a < b) {
+        const int64_t mid = (a + b) / 2;
+        if (R[mid] < hi) a = mid + 1;
+        else b = mid;
+      }
+      S->vmap[p] = S->poff[s] + (lo - S->sfirst[s]) * m + a;
+    }
+  free(ap);
+  free(ai);
+  free(fill);
+  free(parent);
+  free(flag);
+  free(lnz);
+  return S;
+}
+
+static void sn_sym_free(sn_sym* S) {
+  free(S->key_cp);
+  free(S->key_ri);
+  free(S->key_perm);
+  free(S->perm);
+  free(S->iperm);
+  free(S->lp);
+  free(S->li);
+  free(S->sfirst);
+  free(S->sn_of);
+  free(S->sptr);
+  free(S->srows);
+  free(S->poff);
+  free(S->vmap);
+  free(S);
+}
+
+/* a few analyses, most recently computed first; one pushed out of the list is freed once no
+ * factor uses it */
+#define ORC_SN_CACHE 8
+static pthread_mutex_t g_sn_mu = PTHREAD_MUTEX_INITIALIZER;
+static sn_sym* g_sn_cache = NULL;
+
+static int sn_same(const sn_sym* S, int64_t n, const int64_t* cp, const int64_t* ri, const int64_t* perm) {
+  if (S->n != n || S->nnz_in != cp[n] || (S->key_perm == NULL) != (perm == NULL)) return 0;
+  if (memcmp(S->key_cp, cp, sizeof(int64_t) * (n + 1)) || memcmp(S->key_ri, ri, sizeof(int64_t) * cp[n])) return 0;
+  return !perm || !memcmp(S->key_perm, perm, sizeof(int64_t) * n);
+}
+
+/* under g_sn_mu */
+static sn_sym* sn_find_ref(int64_t n, const int64_t* cp, const int64_t* ri, const int64_t* perm) {
+  for (sn_sym* S = g_sn_cache; S; S = S->next)
+    if (sn_same(S, n, cp, ri, perm)) {
+      S->refs++;
+      return S;
+    }
+  return NULL;
+}
+
+/* the cached analysis of this input, computed on a miss; the caller holds one reference */
+static sn_sym* sn_acquire(int64_t n, const int64_t* cp, const int64_t* ri, const int64_t* perm) {
+  pthread_mutex_lock(&g_sn_mu);
+  sn_sym* S = sn_find_ref(n, cp, ri, perm);
+  pthread_mutex_unlock(&g_sn_mu);
+  if (S) return S;
+  sn_sym* fresh = sn_analyze(n, cp, ri, perm); /* outside the lock: threads analyze in parallel */
+  pthread_mutex_lock(&g_sn_mu);
+  S = sn_find_ref(n, cp, ri, perm); /* another thread may have inserted it meanwhile */
+  sn_sym* drop = NULL;
+  if (S) {
+    drop = fresh;
+  } else {
+    S = fresh;
+    S->refs = 1;
+    S->next = g_sn_cache;
+    g_sn_cache = S;
+    int count = 0;
+    for (sn_sym** link = &g_sn_cache; *link;) {
+      sn_sym* T = *link;
+      if (++count > ORC_SN_CACHE) { /* unlink; free now or with its last factor */
+        *link = T->next;
+        T->retired = 1;
+        if (T->refs == 0) {
+          T->next = drop;
+          drop = T;
+        }
+      } else {
+        link = &T->next;
+      }
+    }
+  }
+  pthread_mutex_unlock(&g_sn_mu);
+  while (drop) {
+    sn_sym* nx = drop->next;
+    sn_sym_free(drop);
+    drop = nx;
+  }
+  return S;
+}
+
+static void sn_release(sn_sym* S) {
+  pthread_mutex_lock(&g_sn_mu);
+  const int last = --S->refs == 0 && S->retired;
+  pthread_mutex_unlock(&g_sn_mu);
+  if (last) sn_sym_free(S);
+}
+
+int orc_factor_create_sn(int64_t n, const int64_t* cp, const int64_t* ri, const double* vals, const int64_t* perm,
+                         orc_factor** out) {
+  sn_sym* S = sn_acquire(n, cp, ri, perm);
+  orc_factor* f = (orc_factor*)calloc(1, sizeof(orc_factor));
+  f->n = n;
+  f->shared = S;
+  f->perm = S->perm;
+  f->iperm = S->iperm;
+  f->lp = S->lp;
+  f->li = S->li;
+  f->lx = (double*)malloc(sizeof(double) * (S->lp[n] + 1));
+  f->d = (double*)malloc(sizeof(double) * (n > 0 ? n : 1));
+  double* panel = (double*)calloc(S->npanel + 1, sizeof(double));
+  for (int64_t p = 0; p < cp[n]; ++p)
+    if (S->vmap[p] >= 0) panel[S->vmap[p]] += vals[p];
+  double* t = (double*)malloc(sizeof(double) * S->maxm);
+  double* ucol = (double*)malloc(sizeof(double) * 4 * S->maxm);
+  int64_t* pos = (int64_t*)malloc(sizeof(int64_t) * S->maxm);
+  sn_numeric(f, S->ns, S->sfirst, S->sn_of, S->sptr, S->srows, S->poff, panel, t, ucol, pos);
+  free(t);
+  free(ucol);
+  free(pos);
+  free(panel);
+  *out = f;
+  for (int64_t k = 0; k < n; ++k)
+    if (!isfinite(f->d[k]) || fabs(f->d[k]) < 1e-14) return 1;
+  return 0;
 }
 
 /* Filled unit-L with D on the diagonal, columns sorted (sparse_ldlt.rs:312-355). */
@@ -842,6 +1278,7 @@ static int eval_all(int64_t nobs, int family, const double* eta, const double* y
 }
 
 static int factor_csc(const csc_t* m, const int64_t* perm, orc_factor** f) {
+  if (g_supernodal) return orc_factor_create_sn(m->n, m->cp, m->ri, m->v, perm, f);
   return orc_factor_create(m->n, m->cp, m->ri, m->v, perm, f);
 }
 

@@ -36,6 +36,13 @@ typedef struct orc_factor orc_factor;
  * non-finite (sparse_ldlt.rs:117-120). Only entries with row >= col are read. */
 int orc_factor_create(int64_t n, const int64_t* cp, const int64_t* ri, const double* vals, const int64_t* perm,
                       orc_factor** out);
+/* The same factor by a supernodal LDL^T (dense panels, right-looking Schur updates), equal to
+ * orc_factor_create's to rounding; the CPU baseline's factorization. */
+int orc_factor_create_sn(int64_t n, const int64_t* cp, const int64_t* ri, const double* vals, const int64_t* perm,
+                         orc_factor** out);
+/* 1: the Laplace functions below factorize with orc_factor_create_sn (set before any thread
+ * uses the oracle); 0 (default): with orc_factor_create, the form the parity tests pin. */
+void orc_set_supernodal(int on);
 void orc_factor_free(orc_factor* f);
 int64_t orc_factor_nnz(const orc_factor* f);
 double orc_logdet(const orc_factor* f);                      /* ldlt.rs:65-67, sequential */

@@ -50,6 +50,8 @@ def lib():
             "orc_choose_order": (C.c_int, [C.c_int64, LP, LP, LP]),
             "orc_min_degree": (None, [C.c_int64, LP, LP, LP]),
             "orc_factor_create": (C.c_int, [C.c_int64, LP, LP, DP, LP, C.POINTER(C.c_void_p)]),
+            "orc_factor_create_sn": (C.c_int, [C.c_int64, LP, LP, DP, LP, C.POINTER(C.c_void_p)]),
+            "orc_set_supernodal": (None, [C.c_int]),
             "orc_factor_free": (None, [C.c_void_p]),
             "orc_factor_nnz": (C.c_int64, [C.c_void_p]),
             "orc_logdet": (C.c_double, [C.c_void_p]),
@@ -151,15 +153,17 @@ class OracleError(RuntimeError):
 
 
 class Factor:
-    """Simplicial LDL^T of a full-symmetric CSC (only row >= col entries read)."""
+    """Simplicial LDL^T of a full-symmetric CSC (only row >= col entries read); with
+    ``supernodal`` the same factor by the supernodal form (the CPU baseline's)."""
 
-    def __init__(self, q, perm=None):
+    def __init__(self, q, perm=None, supernodal=False):
         n, cp, ri, v = _csc(q)
         self.n = n
         self._q = (cp, ri)
         h = C.c_void_p()
         pp = None if perm is None else _i64(perm)
-        rc = lib().orc_factor_create(n, _p(cp, LP), _p(ri, LP), _p(v), _p(pp, LP), C.byref(h))
+        create = lib().orc_factor_create_sn if supernodal else lib().orc_factor_create
+        rc = create(n, _p(cp, LP), _p(ri, LP), _p(v), _p(pp, LP), C.byref(h))
         self._h = h
         self.singular = rc != 0
 
@@ -192,6 +196,12 @@ class Factor:
         if lib().orc_takahashi_pattern(self._h, _p(cp, LP), _p(ri, LP), _p(out)):
             raise OracleError("Takahashi failed")
         return out
+
+
+def set_supernodal(on: bool):
+    """Factorize with the supernodal form inside ``laplace`` (the CPU baseline); off by default,
+    the simplicial form being the one the parity tests pin. Set before threads use the oracle."""
+    lib().orc_set_supernodal(1 if on else 0)
 
 
 # ---------------------------------------------------------------------------

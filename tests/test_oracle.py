@@ -250,3 +250,78 @@ def test_binomial_mode_across_prior_strengths():
     r = O.laplace(sp.identity(n, format="csc"), sp.identity(n, format="csr"), "binomial", BINOMIAL_YS, p1=10.0,
                   max_iter=100)
     assert np.isfinite(r["mlik"])
+
+
+# --- the supernodal form (the CPU baseline's factorization) ----------------------------------------
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_supernodal_factor_matches_dense_golden(name):
+    """The supernodal form against the same dense LAPACK golden vectors as the simplicial one."""
+    q = golden_matrix(name)
+    f = O.Factor(q, perm=O.default_perm(q), supernodal=True)
+    assert not f.singular
+    assert abs(f.logdet() - GOLDEN[f"{name}/logdet"][0]) <= 1e-10 * max(1.0, abs(GOLDEN[f"{name}/logdet"][0]))
+    b = np.arange(1, q.shape[0] + 1, dtype=float)
+    np.testing.assert_allclose(f.solve(b), GOLDEN[f"{name}/solve"], rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(f.diag_inv(), GOLDEN[f"{name}/diag_inv"], rtol=1e-10, atol=1e-12)
+
+
+@pytest.mark.parametrize("name", list(KNOWN_ANSWER))
+def test_supernodal_factor_equals_simplicial(name):
+    """Same factor to rounding under every ordering, including a singular-pivot report."""
+    q = KNOWN_ANSWER[name][0]()
+    for perm in (None, O.default_perm(q), np.arange(q.shape[0])[::-1].copy()):
+        a, b = O.Factor(q, perm=perm), O.Factor(q, perm=perm, supernodal=True)
+        assert a.nnz() == b.nnz() and a.singular == b.singular
+        assert abs(a.logdet() - b.logdet()) <= 1e-12 * max(1.0, abs(a.logdet()))
+        np.testing.assert_allclose(b.diag_inv(), a.diag_inv(), rtol=1e-11)
+
+
+def test_supernodal_on_spde_patterns_and_threads():
+    """A 60 x 60 SPDE posterior under the reference's order and the natural one (wide relaxed
+    supernodes), factorized from eight threads at once on the shared cached analyses."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import inla_b200.models as M
+
+    p = M.make_spde_problem(nx=60, n_obs=1800)
+    perm = O.reference_perm(p.model.pattern)
+    qs = []
+    for lt, lk in ((-1.0, 1.2), (-3.0, 2.5), (0.5, 0.3)):
+        c, _ = M.spde_coefs(lt, lk)
+        q = (p.model.matrix(c) + 25.0 * (p.a.T @ p.a)).tocsc()
+        q.sort_indices()
+        qs.append(q)
+    ref = [(O.Factor(q, perm=pp).logdet(), O.Factor(q, perm=pp).solve(np.ones(q.shape[0])))
+           for q in qs for pp in (perm, None)]
+
+    def run(k):
+        q, pp = qs[(k // 2) % 3], (perm, None)[k % 2]
+        f = O.Factor(q, perm=pp, supernodal=True)
+        return f.logdet(), f.solve(np.ones(q.shape[0]))
+
+    with ThreadPoolExecutor(max_workers=8) as ex:
+        got = list(ex.map(run, range(48)))
+    for k, (ld, x) in enumerate(got):
+        ld_ref, x_ref = ref[((k // 2) % 3) * 2 + k % 2]
+        assert abs(ld - ld_ref) <= 1e-12 * abs(ld_ref)
+        np.testing.assert_allclose(x, x_ref, rtol=1e-9, atol=1e-12 * np.max(np.abs(x_ref)))
+
+
+def test_supernodal_laplace_equals_simplicial():
+    """The Laplace evaluation the CPU baseline times, with either factorization."""
+    import inla_b200.models as M
+
+    p = M.make_spde_problem(nx=30, n_obs=400)
+    q = p.model.matrix(O.spde_coefs(-1.0, 1.2))
+    perm = O.reference_perm(p.model.pattern)
+    a = O.laplace(q, p.a, "gaussian", p.y, p1=25.0, perm=perm, want_var=True)
+    O.set_supernodal(True)
+    try:
+        b = O.laplace(q, p.a, "gaussian", p.y, p1=25.0, perm=perm, want_var=True)
+    finally:
+        O.set_supernodal(False)
+    for key in a:
+        va, vb = np.asarray(a[key], dtype=float), np.asarray(b[key], dtype=float)
+        np.testing.assert_allclose(vb, va, rtol=1e-10, atol=1e-12 * max(1.0, np.max(np.abs(va))), err_msg=key)
