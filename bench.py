@@ -447,7 +447,9 @@ def run_ours(args, ws, rank, local, dist):
     cpu = None
     if ws == 1 and args.cpu_seconds > 0:
         threads = os.cpu_count() or 1
-        ev, el = cpu_theta_evals(p, args.cpu_seconds, threads, cpu_perm(p))
+        perm = cpu_perm(p)
+        cpu_theta_evals(p, 0.0, threads, perm, count=1)  # untimed: the per-pattern analyses
+        ev, el = cpu_theta_evals(p, args.cpu_seconds, threads, perm)
         cpu = {"value": ev / el, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{ev} oracle Laplace evaluations (prior + posterior LDL^T, solve, mlik: the "
                          f"Nelder-Mead / FD-Hessian evaluation of the reference's fit) at CCD-like theta-points "
