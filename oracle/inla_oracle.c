@@ -582,7 +582,7 @@ static void sn_numeric(orc_factor* f, int64_t ns, const int64_t* sfirst, const i
       double* TP = panel + poff[ts];
       int64_t q = 0;
       for (int64_t b = a; b < nb; ++b) { /* rows below column a lie in the target's rows */
-        while (TR[q] < R[w + b]) ++q;
+        while (q < tm - 1 && TR[q] < R[w + b]) ++q; /* found: the rows are contained */
         pos[b] = q;
       }
       int64_t a_end = a;
@@ -622,7 +622,7 @@ static void sn_numeric(orc_factor* f, int64_t ns, const int64_t* sfirst, const i
       const int64_t col = c0 + c;
       int64_t r = c + 1;
       for (int64_t p = f->lp[col]; p < f->lp[col + 1]; ++p) {
-        while (R[r] < f->li[p]) ++r;
+        while (r < m - 1 && R[r] < f->li[p]) ++r;
         f->lx[p] = P[c * m + r];
       }
     }
