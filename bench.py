@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--nobs", type=int, default=20000)
     ap.add_argument("--no-plain", action="store_true", help="skip the plain GPU drop-in fit")
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="bounded CPU-baseline sample")
+    ap.add_argument("--cpu-fit", action="store_true",
+                    help="reference arm: also time the oracle's whole fit (NM + FD Hessian + CCD; minutes)")
     ap.add_argument("--e2e-steps", type=int, default=4)
     return ap.parse_args()
 
@@ -194,6 +196,48 @@ def cpu_theta_evals(p, seconds: float, threads: int, perm, want_var: bool = Fals
     return done, time.perf_counter() - t0
 
 
+def cpu_whole_fit(p, threads: int, perm):
+    """The reference's whole fit restated by the oracle, wall-clock seconds per stage: Nelder-Mead
+    from theta0 (hyper_opt.rs:15-183), one evaluation at a time; the FD Hessian (hyper_opt.rs:188-259,
+    h = max(1e-4, 0.05 |theta|)); the CCD nodes with the Takahashi variances, mapped over `threads`
+    as inference.rs:1387-1397 maps them over Rayon workers; the mixture (inference.rs:1419-1466)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    O.set_supernodal(True)
+    count = [0]
+
+    def f(th):
+        count[0] += 1
+        return O.spde_neg_log_posterior(np.asarray(th), p.model, p.a, p.y, perm=perm)
+
+    def node(theta):
+        r = O.laplace(p.model.matrix(O.spde_coefs(theta[1], theta[2])), p.a, "gaussian", p.y,
+                      p1=math.exp(theta[0]), perm=perm, want_var=True)
+        lp = O.loggamma_log_dens(theta[0], 1.0, 5e-5) + O.pc_spde_log_dens(theta[1], theta[2], 1.0, 0.05, 1.0, 0.01)
+        return r["x"], r["var"], r["mlik"] + lp
+
+    t0 = time.perf_counter()
+    mode = O.nelder_mead(list(THETA0), 0.1, 200, 1e-6, f)
+    t1 = time.perf_counter()
+    h = max(1e-4, max(0.05 * abs(t) for t in mode))
+    hess = O.fd_hessian(mode, f, h)
+    t2 = time.perf_counter()
+    # the CCD nodes as integrate() places them, evaluated in parallel first
+    lam, vec = np.linalg.eigh(np.linalg.inv(-np.asarray(hess)))
+    z, _ = O.ccd_design(len(mode))
+    thetas = [np.asarray(mode) + vec @ (np.sqrt(np.abs(lam)) * np.asarray(zk, dtype=float)) for zk in z]
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        done = dict(zip((tuple(t) for t in thetas), ex.map(node, thetas)))
+    res = O.integrate(mode, hess, lambda th: done[tuple(th)] if tuple(th) in done else node(th), f0=1.0)
+    t3 = time.perf_counter()
+    return {"fit_s": t3 - t0, "stages_s": {"mode_search": t1 - t0, "hessian": t2 - t1, "nodes_and_mixture": t3 - t2},
+            "theta_evals": count[0] + len(thetas), "mode": [float(v) for v in mode], "mlik": float(res["mlik"]),
+            "threads": threads}
+
+
 def cpu_perm(p):
     """The oracle's restatement of the reference's ordering choice on this pattern
     (ordering.rs:149-162 picks AMD here; the oracle's minimum-degree order stands in for
@@ -234,12 +278,14 @@ def run_reference(args, ws, rank):
     value = ev / el
     # the CCD stage of the reference's fit: 15 node evaluations with marginal variances
     nccd, tccd = cpu_theta_evals(p, 0.0, threads, perm, want_var=True, count=15)
+    whole = cpu_whole_fit(p, threads, perm) if args.cpu_fit else None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded SPDE 200x200 jittered mesh, 20k Gaussian obs)",
             "config": bench_config(p, args, ws),
             "ccd_stage_with_variances_s": tccd,
+            **({"cpu_fit": whole} if whole else {}),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": f"{ev} oracle Laplace evaluations (prior + posterior LDL^T, solve, mlik: "
                                        f"the Nelder-Mead / FD-Hessian evaluation of the reference's fit) at "
