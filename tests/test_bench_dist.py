@@ -75,3 +75,27 @@ def test_dist_setup_without_torchrun_is_single_rank(monkeypatch):
     for k in ("WORLD_SIZE", "RANK", "LOCAL_RANK"):
         monkeypatch.delenv(k, raising=False)
     assert bench.dist_setup(None) == (1, 0, 0, None)
+
+
+def test_reference_arm_whole_fit_on_a_small_mesh():
+    """The opt-in whole-fit timing of the reference arm (Nelder-Mead, FD Hessian, CCD nodes over
+    threads) runs on a 15 x 15 mesh and lands on the oracle's own Nelder-Mead mode."""
+    import types
+
+    import numpy as np
+
+    sys.path.insert(0, str(ROOT))
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import bench
+    import oracle as O
+
+    p = bench.make_problem(types.SimpleNamespace(nx=15, nobs=120), standalone=True)
+    perm = bench.cpu_perm(p)
+    try:
+        r = bench.cpu_whole_fit(p, 2, perm)
+    finally:
+        O.set_supernodal(False)  # the oracle's default, the form the parity tests pin
+    mode_ref = O.nelder_mead(list(bench.THETA0), 0.1, 200, 1e-6,
+                             lambda th: O.spde_neg_log_posterior(np.asarray(th), p.model, p.a, p.y, perm=perm))
+    np.testing.assert_allclose(r["mode"], mode_ref, atol=1e-6)
+    assert r["theta_evals"] > 15 and np.isfinite(r["mlik"]) and r["fit_s"] > 0
