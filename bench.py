@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--cpu-fit", action="store_true",
                     help="reference arm: also time the oracle's whole fit (NM + FD Hessian + CCD; minutes)")
     ap.add_argument("--e2e-steps", type=int, default=4)
+    ap.add_argument("--no-other-configs", action="store_true",
+                    help="skip the fits of the grouped 200 001-node model and of the 512 uneven models")
+    ap.add_argument("--other-configs-child", action="store_true", help=argparse.SUPPRESS)
     return ap.parse_args()
 
 
@@ -194,6 +197,77 @@ def cpu_theta_evals(p, seconds: float, threads: int, perm, want_var: bool = Fals
             while time.perf_counter() - t0 < seconds or done == 0:
                 done += sum(ex.map(one, range(done, done + threads)))
     return done, time.perf_counter() - t0
+
+
+def other_config_fits():
+    """Fit seconds of two other workloads on this GPU, each a first fit (it includes the engine's
+    per-batch-size autotuning and graph captures), wall clock between synchronizes:
+    * the space x time group model (Besag 50 x 50 (x) AR1 T = 40 + iid + intercept, n = 200 001,
+      binomial(10), one sum-to-zero row per time held bordered; CCD over 4 hyperparameters, 25 nodes);
+    * 512 independent AR1 + iid + intercept Poisson models of 200 to 5 000 nodes, fitted in lockstep
+      (per-model mode search, Hessian and CCD 15).
+    Each entry holds its result or its error."""
+    import torch
+
+    from inla_b200 import models
+    from inla_b200.laplace import PRIOR_PC_COR1, PRIOR_PC_PREC, LaplaceModel
+    from inla_b200.multi import MultiModel
+
+    out = {}
+    try:
+        t0 = time.perf_counter()
+        p = models.make_group_problem()
+        lm = LaplaceModel(p.model, a=p.a, family="binomial", y=p.y, p1=p.ntrials, max_batch=9)
+        lm.set_constraints(*p.constraint)  # auto: bordered at this size
+        priors = [(PRIOR_PC_PREC, 0, (1.0, 0.01)), (PRIOR_PC_PREC, 1, (1.0, 0.01)), (PRIOR_PC_COR1, 2, (0.5, 0.75)),
+                  (PRIOR_PC_PREC, 3, (1.0, 0.01))]
+
+        def tmap(th):
+            c, dc = models.group_coefs(th)
+            return c, dc, 1.0, np.zeros(4)
+
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        r = lm.fit(np.array([0.0, 0.0, 1.5, 1.0]), theta_map=tmap, priors=priors, mode_search="newton", batched=True)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        out["group_200k_ccd25"] = {"fit_s": t2 - t1, "inputs_and_model_s": t1 - t0, "theta_evals": int(r["n_evals"]),
+                                   "batches": int(r["n_batches"]), "mode": [float(v) for v in r["mode"]],
+                                   "n_latent": int(p.model.n)}
+        lm.close()
+        del lm, p
+    except Exception as e:  # reported, not raised: the main line must still print
+        out["group_200k_ccd25"] = {"error": repr(e)[:300]}
+    try:
+        t0 = time.perf_counter()
+        p = models.make_multi_problem()
+        mm = MultiModel(p.models, p.a, p.y, family="poisson", max_batch=15)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        r = mm.fit(np.zeros((mm.G, 3)))
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        out["multi_512_ccd15"] = {"fit_s": t2 - t1, "inputs_and_model_s": t1 - t0, "models": int(mm.G),
+                                  "batches": int(r["n_batches"]), "model_evals": int(r["n_model_evals"]),
+                                  "all_status_ok": bool(np.all(r["status"] == 0))}
+    except Exception as e:
+        out["multi_512_ccd15"] = {"error": repr(e)[:300]}
+    return out
+
+
+def run_other_configs(timeout_s: float = 900.0):
+    """other_config_fits in a child process, so that nothing in it can stop this line."""
+    import subprocess
+
+    try:
+        r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--other-configs-child"], capture_output=True,
+                           text=True, timeout=timeout_s)
+        lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+        if r.returncode == 0 and lines:
+            return json.loads(lines[-1])
+        return {"error": f"rc={r.returncode}: {(r.stderr or r.stdout)[-300:]}"}
+    except Exception as e:
+        return {"error": repr(e)[:300]}
 
 
 def cpu_whole_fit(p, threads: int, perm):
@@ -501,6 +575,8 @@ def run_ours(args, ws, rank, local, dist):
                          f"Nelder-Mead / FD-Hessian evaluation of the reference's fit) at CCD-like theta-points "
                          f"in {el:.1f}s, {threads} threads, minimum-degree order; {CPU_KIND_NOTE}"}
 
+    others = run_other_configs() if (ws == 1 and not args.no_other_configs) else None
+
     fit_s = ms_total * 1e-3 / args.steps
     # where one fit's time goes (host wall clock per phase, averaged over the timed fits)
     phases = {k: sum(f["phase_s"][k] for f in fits) / len(fits) for k in fits[0]["phase_s"]}
@@ -524,13 +600,17 @@ def run_ours(args, ws, rank, local, dist):
                             "engine tables derived from it are the process-wide cached ones from the first creation "
                             "(create_first_s includes them); the first e2e step also maps fresh device memory, "
                             "because the timed model still holds its own"},
-            "gpu_launches": int(launches), "clocks": clocks, "roofline": roof, "cpu_baseline": cpu}
+            "gpu_launches": int(launches), "clocks": clocks, "roofline": roof, "cpu_baseline": cpu,
+            "other_configs": others}
     print(json.dumps(line), flush=True)
     return 0
 
 
 def main():
     args = parse()
+    if args.other_configs_child:
+        print(json.dumps(other_config_fits()), flush=True)
+        return 0
     ws, rank, local, dist = dist_setup(args)
     try:
         if args.impl == "reference":

@@ -99,3 +99,18 @@ def test_reference_arm_whole_fit_on_a_small_mesh():
                              lambda th: O.spde_neg_log_posterior(np.asarray(th), p.model, p.a, p.y, perm=perm))
     np.testing.assert_allclose(r["mode"], mode_ref, atol=1e-6)
     assert r["theta_evals"] > 15 and np.isfinite(r["mlik"]) and r["fit_s"] > 0
+
+
+def test_other_config_fits_run_in_a_child_and_report_errors():
+    """The extra fits run in a child process whose failure cannot stop the bench line: without a
+    GPU both legs come back as errors in a JSON object."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("device present")
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    r = bench.run_other_configs(timeout_s=300)
+    assert set(r) == {"group_200k_ccd25", "multi_512_ccd15"}, r
+    assert all("error" in v for v in r.values())
