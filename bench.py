@@ -255,7 +255,7 @@ def other_config_fits():
     return out
 
 
-def run_other_configs(timeout_s: float = 900.0):
+def run_other_configs(timeout_s: float = 300.0):
     """other_config_fits in a child process, so that nothing in it can stop this line."""
     import subprocess
 
