@@ -272,8 +272,8 @@ def run_other_configs(timeout_s: float = 300.0):
 
 def cpu_whole_fit(p, threads: int, perm):
     """The reference's whole fit restated by the oracle, wall-clock seconds per stage: Nelder-Mead
-    from theta0 (hyper_opt.rs:15-183), one evaluation at a time; the FD Hessian (hyper_opt.rs:188-259,
-    h = max(1e-4, 0.05 |theta|)); the CCD nodes with the Takahashi variances, mapped over `threads`
+    from theta0 (hyper_opt.rs:15-183), one evaluation at a time with the threads inside each
+    factorization; the FD Hessian (hyper_opt.rs:188-259, h = max(1e-4, 0.05 |theta|)), likewise; the CCD nodes with the Takahashi variances, mapped over `threads`
     as inference.rs:1387-1397 maps them over Rayon workers; the mixture (inference.rs:1419-1466)."""
     from concurrent.futures import ThreadPoolExecutor
 
@@ -281,6 +281,7 @@ def cpu_whole_fit(p, threads: int, perm):
     import oracle as O
 
     O.set_supernodal(True)
+    O.set_threads(threads)  # one evaluation at a time: the threads work inside each factorization
     count = [0]
 
     def f(th):
@@ -299,6 +300,7 @@ def cpu_whole_fit(p, threads: int, perm):
     h = max(1e-4, max(0.05 * abs(t) for t in mode))
     hess = O.fd_hessian(mode, f, h)
     t2 = time.perf_counter()
+    O.set_threads(1)  # the nodes run side by side, one thread each
     # the CCD nodes as integrate() places them, evaluated in parallel first
     lam, vec = np.linalg.eigh(np.linalg.inv(-np.asarray(hess)))
     z, _ = O.ccd_design(len(mode))

@@ -480,6 +480,10 @@ void orc_solve(const orc_factor* f, const double* b, double* x) {
 
 static int g_supernodal = 0;
 void orc_set_supernodal(int on) { g_supernodal = on; }
+/* threads inside one supernodal factorization (1: none), for stages that run one evaluation at
+ * a time, as faer parallelizes one factorization over Rayon (sparse_ldlt.rs:66-72) */
+static int g_sn_threads = 1;
+void orc_set_threads(int t) { g_sn_threads = t < 1 ? 1 : t; }
 
 /* perm composed with a postorder of the elimination tree of the matrix permuted by perm
  * (children in increasing order): the same fill, and parent-child chains become contiguous. */
@@ -569,6 +573,8 @@ static void sn_numeric(orc_factor* f, int64_t ns, const int64_t* sfirst, const i
         t[r] = Pc[r];
         Pc[r] = t[r] / d;
       }
+      const int par = g_sn_threads > 1 && (double)(w - c) * (double)(m - c) > 5e4;
+#pragma omp parallel for schedule(static) num_threads(g_sn_threads) if (par)
       for (int64_t c2 = c + 1; c2 < w; ++c2) {
         const double tc = t[c2];
         double* P2 = P + c2 * m;
@@ -588,13 +594,23 @@ static void sn_numeric(orc_factor* f, int64_t ns, const int64_t* sfirst, const i
       int64_t a_end = a;
       while (a_end < nb && R[w + a_end] < tl) ++a_end;
       /* four target columns at a time: each load of L21 feeds four accumulators (rows above a
-       * column's own row are computed and not used) */
-      for (int64_t a2 = a; a2 < a_end; a2 += 4) {
+       * column's own row are computed and not used). The blocks write different target columns,
+       * so large updates split them over the threads of orc_set_threads. */
+      const int64_t nblk = (a_end - a + 3) / 4;
+      const int par = g_sn_threads > 1 && (double)w * (double)(nb - a) * (double)(a_end - a) > 2e5;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(g_sn_threads) if (par)
+      for (int64_t blk = 0; blk < nblk; ++blk) {
+        const int64_t a2 = a + 4 * blk;
         const int64_t nc = MINI(4, a_end - a2);
-        double* u0 = ucol;
-        double* u1 = ucol + nb;
-        double* u2 = ucol + 2 * nb;
-        double* u3 = ucol + 3 * nb;
+#ifdef _OPENMP
+        double* ub = ucol + (size_t)omp_get_thread_num() * 4 * nb;
+#else
+        double* ub = ucol;
+#endif
+        double* u0 = ub;
+        double* u1 = ub + nb;
+        double* u2 = ub + 2 * nb;
+        double* u3 = ub + 3 * nb;
         for (int64_t b = a2; b < nb; ++b) u0[b] = u1[b] = u2[b] = u3[b] = 0.0;
         for (int64_t c = 0; c < w; ++c) {
           const double dc = f->d[c0 + c];
@@ -879,7 +895,7 @@ int orc_factor_create_sn(int64_t n, const int64_t* cp, const int64_t* ri, const 
   for (int64_t p = 0; p < cp[n]; ++p)
     if (S->vmap[p] >= 0) panel[S->vmap[p]] += vals[p];
   double* t = (double*)malloc(sizeof(double) * S->maxm);
-  double* ucol = (double*)malloc(sizeof(double) * 4 * S->maxm);
+  double* ucol = (double*)malloc(sizeof(double) * 4 * S->maxm * (size_t)g_sn_threads);
   int64_t* pos = (int64_t*)malloc(sizeof(int64_t) * S->maxm);
   sn_numeric(f, S->ns, S->sfirst, S->sn_of, S->sptr, S->srows, S->poff, panel, t, ucol, pos);
   free(t);

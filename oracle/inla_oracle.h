@@ -43,6 +43,8 @@ int orc_factor_create_sn(int64_t n, const int64_t* cp, const int64_t* ri, const 
 /* 1: the Laplace functions below factorize with orc_factor_create_sn (set before any thread
  * uses the oracle); 0 (default): with orc_factor_create, the form the parity tests pin. */
 void orc_set_supernodal(int on);
+/* OpenMP threads inside one supernodal factorization (default 1). */
+void orc_set_threads(int t);
 void orc_factor_free(orc_factor* f);
 int64_t orc_factor_nnz(const orc_factor* f);
 double orc_logdet(const orc_factor* f);                      /* ldlt.rs:65-67, sequential */

@@ -52,6 +52,7 @@ def lib():
             "orc_factor_create": (C.c_int, [C.c_int64, LP, LP, DP, LP, C.POINTER(C.c_void_p)]),
             "orc_factor_create_sn": (C.c_int, [C.c_int64, LP, LP, DP, LP, C.POINTER(C.c_void_p)]),
             "orc_set_supernodal": (None, [C.c_int]),
+            "orc_set_threads": (None, [C.c_int]),
             "orc_factor_free": (None, [C.c_void_p]),
             "orc_factor_nnz": (C.c_int64, [C.c_void_p]),
             "orc_logdet": (C.c_double, [C.c_void_p]),
@@ -196,6 +197,12 @@ class Factor:
         if lib().orc_takahashi_pattern(self._h, _p(cp, LP), _p(ri, LP), _p(out)):
             raise OracleError("Takahashi failed")
         return out
+
+
+def set_threads(t: int):
+    """OpenMP threads inside one supernodal factorization (1: none). Set it above 1 only where
+    evaluations run one at a time, and before threads use the oracle."""
+    lib().orc_set_threads(int(t))
 
 
 def set_supernodal(on: bool):
