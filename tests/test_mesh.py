@@ -242,11 +242,14 @@ def test_barrier_spde_reduces_covariance_across_strip():
 from inla_b200.mesh import SpdePlan  # noqa: E402
 
 
-@pytest.mark.parametrize("nx,seed", [(2, 1), (12, 5), (40, 7)])
+@pytest.mark.parametrize("nx,seed", [(2, 1), (3, 0), (12, 5), (40, 7)])
 def test_device_fem_patterns_equal_the_host_blocks(nx, seed):
-    """The device forms' patterns come from the topology alone and equal the host assembly's."""
+    """The device forms' patterns come from the topology alone and equal the host assembly's
+    (nx = 3: the square plus a vertex no triangle uses, whose columns stay empty)."""
     if nx == 2:
         m = Mesh(SQUARE_V, SQUARE_T)
+    elif nx == 3:
+        m = Mesh(SQUARE_V + [[2.0, 2.0]], SQUARE_T)
     else:
         v, t = _jittered(nx, seed)
         m = Mesh(v, t)
