@@ -78,7 +78,7 @@ def test_dist_setup_without_torchrun_is_single_rank(monkeypatch):
 
 
 def test_reference_arm_whole_fit_on_a_small_mesh():
-    """The opt-in whole-fit timing of the reference arm (Nelder-Mead, FD Hessian, CCD nodes over
+    """The whole-fit timing of the reference arm (Nelder-Mead, FD Hessian, CCD nodes over
     threads) runs on a 15 x 15 mesh and lands on the oracle's own Nelder-Mead mode."""
     import types
 
@@ -114,3 +114,27 @@ def test_other_config_fits_run_in_a_child_and_report_errors():
     r = bench.run_other_configs(timeout_s=300)
     assert set(r) == {"group_200k_ccd25", "multi_512_ccd15"}, r
     assert all("error" in v for v in r.values())
+
+
+def test_reference_arm_line_on_a_tiny_mesh(capsys):
+    """The whole reference arm on rank 0 (10 x 10 mesh): one JSON line with the GPU arm's config
+    keys, the CPU-baseline description and the whole-fit timing."""
+    import json
+
+    sys.path.insert(0, str(ROOT))
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import bench
+    import oracle as O
+
+    class Args:
+        gpus, steps, warmup, cpu_seconds, nx, nobs, no_cpu_fit = 1, 1, 0, 0.1, 10, 50, False
+
+    try:
+        assert bench.run_reference(Args(), 1, 0) == 0
+    finally:
+        O.set_supernodal(False)
+        O.set_threads(1)
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["config"]["workload"] == "spde_200x200_gaussian_ccd15"
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_fit"]["theta_evals"] > 15
