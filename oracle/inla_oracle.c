@@ -468,13 +468,15 @@ void orc_solve(const orc_factor* f, const double* b, double* x) {
 /* ------------------------------------------------------------------------ */
 /* The reference factorizes with faer's supernodal LDL^T (sparse_ldlt.rs:196-241 ->
  * faer 0.24 factorize_numeric_ldlt; faer's source is not available here). This is a plain
- * supernodal LDL^T of the same matrix, used to time a CPU path shaped like the reference's:
- * fundamental supernodes (column j joins column j-1's supernode when j is j-1's etree parent and
- * j-1 has one more strictly-lower entry), one dense column-major panel per supernode holding its
- * rows, the panel factored column by column, and its Schur complement L21 D L21^T subtracted from
- * the later supernodes' panels (right-looking). The factor equals orc_factor_create's to
- * rounding and is stored the same way, so orc_logdet, orc_solve and the Takahashi functions
- * apply unchanged. Same D gate (sparse_ldlt.rs:117-120). */
+ * supernodal LDL^T of the same matrix, used to time a CPU path shaped like the reference's: a
+ * postordered elimination tree, relaxed supernodes along parent chains, one dense column-major
+ * panel per supernode holding its rows, and a left-looking numeric phase over the supernodal
+ * tree (each supernode subtracts the Schur complements L21 D L21^T of the supernodes below it,
+ * then factors its panel column by column), with independent subtrees as OpenMP tasks when
+ * orc_set_threads allows. The analysis is cached per pattern. The factor equals
+ * orc_factor_create's to rounding, is bit-identical for any thread count, and is stored the same
+ * way, so orc_logdet, orc_solve and the Takahashi functions apply unchanged. Same D gate
+ * (sparse_ldlt.rs:117-120). */
 #define ORC_SN_MAXW 128
 #define ORC_SN_ZEROS 0.1
 
@@ -552,99 +554,6 @@ static void postordered_perm(int64_t n, const int64_t* cp, const int64_t* ri, co
   free(anc);
 }
 
-/* Numeric phase of orc_factor_create_sn: each supernode's panel factored column by column, its
- * Schur complement subtracted from the later panels, the columns copied into the factor. Built
- * for AVX2 + FMA and for baseline x86-64, the first the CPU supports chosen at load time. */
-#if defined(__x86_64__) && defined(__GNUC__) && !defined(__clang__)
-__attribute__((target_clones("arch=x86-64-v3", "default")))
-#endif
-static void sn_numeric(orc_factor* f, int64_t ns, const int64_t* sfirst, const int64_t* sn_of, const int64_t* sptr,
-                       const int64_t* srows, const int64_t* poff, double* panel, double* t, double* ucol,
-                       int64_t* pos) {
-  for (int64_t s = 0; s < ns; ++s) {
-    const int64_t c0 = sfirst[s], w = sfirst[s + 1] - c0, m = sptr[s + 1] - sptr[s];
-    double* P = panel + poff[s];
-    const int64_t* R = srows + sptr[s];
-    for (int64_t c = 0; c < w; ++c) { /* column c of the panel */
-      double* Pc = P + c * m;
-      const double d = Pc[c];
-      f->d[c0 + c] = d;
-      for (int64_t r = c + 1; r < m; ++r) {
-        t[r] = Pc[r];
-        Pc[r] = t[r] / d;
-      }
-      const int par = g_sn_threads > 1 && (double)(w - c) * (double)(m - c) > 5e4;
-#pragma omp parallel for schedule(static) num_threads(g_sn_threads) if (par)
-      for (int64_t c2 = c + 1; c2 < w; ++c2) {
-        const double tc = t[c2];
-        double* P2 = P + c2 * m;
-        for (int64_t r = c2; r < m; ++r) P2[r] -= Pc[r] * tc;
-      }
-    }
-    const int64_t nb = m - w; /* rows below the supernode */
-    for (int64_t a = 0; a < nb;) {
-      const int64_t ts = sn_of[R[w + a]], tf = sfirst[ts], tl = sfirst[ts + 1], tm = sptr[ts + 1] - sptr[ts];
-      const int64_t* TR = srows + sptr[ts];
-      double* TP = panel + poff[ts];
-      int64_t q = 0;
-      for (int64_t b = a; b < nb; ++b) { /* rows below column a lie in the target's rows */
-        while (q < tm - 1 && TR[q] < R[w + b]) ++q; /* found: the rows are contained */
-        pos[b] = q;
-      }
-      int64_t a_end = a;
-      while (a_end < nb && R[w + a_end] < tl) ++a_end;
-      /* four target columns at a time: each load of L21 feeds four accumulators (rows above a
-       * column's own row are computed and not used). The blocks write different target columns,
-       * so large updates split them over the threads of orc_set_threads. */
-      const int64_t nblk = (a_end - a + 3) / 4;
-      const int par = g_sn_threads > 1 && (double)w * (double)(nb - a) * (double)(a_end - a) > 2e5;
-#pragma omp parallel for schedule(dynamic, 1) num_threads(g_sn_threads) if (par)
-      for (int64_t blk = 0; blk < nblk; ++blk) {
-        const int64_t a2 = a + 4 * blk;
-        const int64_t nc = MINI(4, a_end - a2);
-#ifdef _OPENMP
-        double* ub = ucol + (size_t)omp_get_thread_num() * 4 * nb;
-#else
-        double* ub = ucol;
-#endif
-        double* u0 = ub;
-        double* u1 = ub + nb;
-        double* u2 = ub + 2 * nb;
-        double* u3 = ub + 3 * nb;
-        for (int64_t b = a2; b < nb; ++b) u0[b] = u1[b] = u2[b] = u3[b] = 0.0;
-        for (int64_t c = 0; c < w; ++c) {
-          const double dc = f->d[c0 + c];
-          const double* Lc = P + c * m + w;
-          const double k0 = dc * Lc[a2], k1 = nc > 1 ? dc * Lc[a2 + 1] : 0.0, k2 = nc > 2 ? dc * Lc[a2 + 2] : 0.0,
-                       k3 = nc > 3 ? dc * Lc[a2 + 3] : 0.0;
-          for (int64_t b = a2; b < nb; ++b) {
-            const double l = Lc[b];
-            u0[b] += l * k0;
-            u1[b] += l * k1;
-            u2[b] += l * k2;
-            u3[b] += l * k3;
-          }
-        }
-        double* us[4] = {u0, u1, u2, u3};
-        for (int64_t j = 0; j < nc; ++j) {
-          double* TPc = TP + (R[w + a2 + j] - tf) * tm;
-          const double* u = us[j];
-          for (int64_t b = a2 + j; b < nb; ++b) TPc[pos[b]] -= u[b];
-        }
-      }
-      a = a_end;
-    }
-    for (int64_t c = 0; c < w; ++c) { /* column c0 + c of L: its structure's rows among R[c+1..m) */
-      const int64_t col = c0 + c;
-      int64_t r = c + 1;
-      for (int64_t p = f->lp[col]; p < f->lp[col + 1]; ++p) {
-        while (r < m - 1 && R[r] < f->li[p]) ++r;
-        f->lx[p] = P[c * m + r];
-      }
-    }
-  }
-}
-
 /* Structure of a supernodal factor, computed once per (pattern, ordering) and shared, as the
  * reference refactorizes numerically on an unchanged pattern (scratch.rs:90-119). */
 typedef struct sn_sym {
@@ -654,6 +563,11 @@ typedef struct sn_sym {
   int64_t ns, maxm, npanel;
   int64_t *sfirst, *sn_of, *sptr, *srows, *poff;
   int64_t* vmap; /* input entry -> panel position (-1 for entries above the diagonal) */
+  /* supernodal tree: children of each supernode (CSR, ascending) and columns per subtree */
+  int64_t *chp, *chl, *subcols, *sparent; /* sparent: -1 at a root */
+  /* updates each supernode receives, in ascending order of the supernode they come from:
+   * (source d, index a of the first of d's rows below its own columns that falls in the target) */
+  int64_t *uptr, *ud, *ua;
   int64_t refs;  /* factors using it; a retired analysis is freed with its last factor */
   int retired;
   struct sn_sym* next;
@@ -766,6 +680,56 @@ static sn_sym* sn_analyze(int64_t n, const int64_t* cp, const int64_t* ri, const
     for (int64_t c = c0; c <= last; ++c) S->srows[S->sptr[s] + c - c0] = c;
     memcpy(S->srows + S->sptr[s] + (last - c0 + 1), S->li + S->lp[last], sizeof(int64_t) * lnz[last]);
   }
+  /* supernodal tree and subtree sizes (children have smaller indices: postorder) */
+  S->chp = (int64_t*)calloc(ns + 1, sizeof(int64_t));
+  S->chl = (int64_t*)malloc(sizeof(int64_t) * (ns + 1));
+  S->subcols = (int64_t*)calloc(ns + 1, sizeof(int64_t));
+  int64_t* spar = (int64_t*)malloc(sizeof(int64_t) * (ns + 1));
+  for (int64_t s2 = 0; s2 < ns; ++s2) {
+    const int64_t pc = parent[S->sfirst[s2 + 1] - 1];
+    spar[s2] = pc < 0 ? -1 : S->sn_of[pc];
+    if (spar[s2] >= 0) S->chp[spar[s2] + 1]++;
+  }
+  for (int64_t s2 = 0; s2 < ns; ++s2) S->chp[s2 + 1] += S->chp[s2];
+  {
+    int64_t* nx = (int64_t*)malloc(sizeof(int64_t) * (ns + 1));
+    memcpy(nx, S->chp, sizeof(int64_t) * (ns + 1));
+    for (int64_t s2 = 0; s2 < ns; ++s2)
+      if (spar[s2] >= 0) S->chl[nx[spar[s2]]++] = s2;
+    free(nx);
+  }
+  for (int64_t s2 = 0; s2 < ns; ++s2) {
+    S->subcols[s2] += S->sfirst[s2 + 1] - S->sfirst[s2];
+    if (spar[s2] >= 0) S->subcols[spar[s2]] += S->subcols[s2];
+  }
+  S->sparent = spar;
+  /* update lists: the rows of d below its columns, grouped by the supernode holding them */
+  S->uptr = (int64_t*)calloc(ns + 1, sizeof(int64_t));
+  for (int pass = 0; pass < 2; ++pass) {
+    int64_t* nx = NULL;
+    if (pass == 1) {
+      for (int64_t s2 = 0; s2 < ns; ++s2) S->uptr[s2 + 1] += S->uptr[s2];
+      S->ud = (int64_t*)malloc(sizeof(int64_t) * (S->uptr[ns] + 1));
+      S->ua = (int64_t*)malloc(sizeof(int64_t) * (S->uptr[ns] + 1));
+      nx = (int64_t*)malloc(sizeof(int64_t) * (ns + 1));
+      memcpy(nx, S->uptr, sizeof(int64_t) * (ns + 1));
+    }
+    for (int64_t d = 0; d < ns; ++d) {
+      const int64_t w = S->sfirst[d + 1] - S->sfirst[d], m = S->sptr[d + 1] - S->sptr[d];
+      const int64_t* R = S->srows + S->sptr[d];
+      for (int64_t a = 0; a < m - w;) {
+        const int64_t t2 = S->sn_of[R[w + a]];
+        if (pass == 0) {
+          S->uptr[t2 + 1]++;
+        } else {
+          S->ud[nx[t2]] = d;
+          S->ua[nx[t2]++] = a;
+        }
+        while (a < m - w && R[w + a] < S->sfirst[t2 + 1]) ++a;
+      }
+    }
+    free(nx);
+  }
   /* input entry (row >= col) -> position of (hi, lo) in lo's panel */
   S->vmap = (int64_t*)malloc(sizeof(int64_t) * (cp[n] + 1));
   for (int64_t c = 0; c < n; ++c)
@@ -806,6 +770,13 @@ static void sn_sym_free(sn_sym* S) {
   free(S->srows);
   free(S->poff);
   free(S->vmap);
+  free(S->chp);
+  free(S->chl);
+  free(S->subcols);
+  free(S->sparent);
+  free(S->uptr);
+  free(S->ud);
+  free(S->ua);
   free(S);
 }
 
@@ -879,6 +850,187 @@ static void sn_release(sn_sym* S) {
   if (last) sn_sym_free(S);
 }
 
+/* ---- numeric phase: left-looking over the supernodal tree ---- */
+/* Built for AVX2 + FMA and for baseline x86-64, the first the CPU supports chosen at load time. */
+#if defined(__x86_64__) && defined(__GNUC__) && !defined(__clang__)
+#define ORC_CLONES __attribute__((target_clones("arch=x86-64-v3", "default")))
+#else
+#define ORC_CLONES
+#endif
+
+/* Accumulate target columns a2 .. a2+nc-1 (nc <= 4) of an update into u (4 nb): each load of
+ * L21 feeds four accumulators (rows above a column's own row are computed and not used), then
+ * subtract them from the target panel. */
+ORC_CLONES
+static void sn_update_block(const double* dd, const double* P, int64_t m, int64_t w, int64_t nb, const int64_t* R,
+                            int64_t a2, int64_t nc, double* TP, int64_t tf, int64_t tm, const int64_t* pos, double* u) {
+  double* u0 = u;
+  double* u1 = u + nb;
+  double* u2 = u + 2 * nb;
+  double* u3 = u + 3 * nb;
+  for (int64_t b = a2; b < nb; ++b) u0[b] = u1[b] = u2[b] = u3[b] = 0.0;
+  for (int64_t c = 0; c < w; ++c) {
+    const double dc = dd[c];
+    const double* Lc = P + c * m + w;
+    const double k0 = dc * Lc[a2], k1 = nc > 1 ? dc * Lc[a2 + 1] : 0.0, k2 = nc > 2 ? dc * Lc[a2 + 2] : 0.0,
+                 k3 = nc > 3 ? dc * Lc[a2 + 3] : 0.0;
+    for (int64_t b = a2; b < nb; ++b) {
+      const double l = Lc[b];
+      u0[b] += l * k0;
+      u1[b] += l * k1;
+      u2[b] += l * k2;
+      u3[b] += l * k3;
+    }
+  }
+  double* us[4] = {u0, u1, u2, u3};
+  for (int64_t j = 0; j < nc; ++j) {
+    double* TPc = TP + (R[w + a2 + j] - tf) * tm;
+    const double* uj = us[j];
+    for (int64_t b = a2 + j; b < nb; ++b) TPc[pos[b]] -= uj[b];
+  }
+}
+
+/* The update of supernode d into supernode s, which holds d's rows below d's own columns from
+ * index a on: U = L21 D L21^T on those rows and s's columns, subtracted from s's panel. A large
+ * one is split by blocks of target columns over the team's threads (a taskloop: it ends before
+ * the next update starts, so every entry still receives its updates in the same order); its
+ * row map is then its own, and each block uses the accumulators of the thread running it. */
+static void sn_update(const orc_factor* f, const sn_sym* S, double* panel, int64_t d, int64_t a, int64_t s,
+                      double* ucol, int64_t* pos, double* scratch_all) {
+  const int64_t c0 = S->sfirst[d], w = S->sfirst[d + 1] - c0, m = S->sptr[d + 1] - S->sptr[d], nb = m - w;
+  const double* P = panel + S->poff[d];
+  const int64_t* R = S->srows + S->sptr[d];
+  const int64_t tf = S->sfirst[s], tl = S->sfirst[s + 1], tm = S->sptr[s + 1] - S->sptr[s];
+  const int64_t* TR = S->srows + S->sptr[s];
+  double* TP = panel + S->poff[s];
+  int64_t a_end = a;
+  while (a_end < nb && R[w + a_end] < tl) ++a_end;
+  const int par = g_sn_threads > 1 && (double)w * (double)(nb - a) * (double)(a_end - a) > 4e5;
+  int64_t* map = par ? (int64_t*)malloc(sizeof(int64_t) * (nb + 1)) : pos;
+  int64_t q = 0;
+  for (int64_t b = a; b < nb; ++b) { /* d's rows from a on lie among s's rows */
+    while (q < tm - 1 && TR[q] < R[w + b]) ++q;
+    map[b] = q;
+  }
+  const double* dd = f->d + c0;
+  if (!par) {
+    for (int64_t a2 = a; a2 < a_end; a2 += 4)
+      sn_update_block(dd, P, m, w, nb, R, a2, MINI(4, a_end - a2), TP, tf, tm, map, ucol);
+    return;
+  }
+  const int64_t nblk = (a_end - a + 3) / 4, stride = 6 * S->maxm;
+#pragma omp taskloop grainsize(1)
+  for (int64_t blk = 0; blk < nblk; ++blk) {
+#ifdef _OPENMP
+    double* u = scratch_all + (int64_t)omp_get_thread_num() * stride + S->maxm;
+#else
+    double* u = scratch_all + S->maxm;
+#endif
+    const int64_t a2 = a + 4 * blk;
+    sn_update_block(dd, P, m, w, nb, R, a2, MINI(4, a_end - a2), TP, tf, tm, map, u);
+  }
+  free(map);
+}
+
+/* Factor supernode s: the updates of the supernodes below it in ascending order of their index
+ * (the same order for any schedule, so the result does not depend on the
+ * schedule), then its panel column by column, then its columns copied into the factor. */
+ORC_CLONES
+static void sn_node(orc_factor* f, const sn_sym* S, double* panel, int64_t s, double* t, double* ucol,
+                    int64_t* pos, double* scratch_all) {
+  for (int64_t k = S->uptr[s]; k < S->uptr[s + 1]; ++k)
+    sn_update(f, S, panel, S->ud[k], S->ua[k], s, ucol, pos, scratch_all);
+  const int64_t c0 = S->sfirst[s], w = S->sfirst[s + 1] - c0, m = S->sptr[s + 1] - S->sptr[s];
+  double* P = panel + S->poff[s];
+  const int64_t* R = S->srows + S->sptr[s];
+  for (int64_t c = 0; c < w; ++c) {
+    double* Pc = P + c * m;
+    const double d = Pc[c];
+    f->d[c0 + c] = d;
+    for (int64_t r = c + 1; r < m; ++r) {
+      t[r] = Pc[r];
+      Pc[r] = t[r] / d;
+    }
+    for (int64_t c2 = c + 1; c2 < w; ++c2) {
+      const double tc = t[c2];
+      double* P2 = P + c2 * m;
+      for (int64_t r = c2; r < m; ++r) P2[r] -= Pc[r] * tc;
+    }
+  }
+  for (int64_t c = 0; c < w; ++c) { /* column c0 + c of L: its structure's rows among R[c+1..m) */
+    const int64_t col = c0 + c;
+    int64_t r = c + 1;
+    for (int64_t p = f->lp[col]; p < f->lp[col + 1]; ++p) {
+      while (r < m - 1 && R[r] < f->li[p]) ++r;
+      f->lx[p] = P[c * m + r];
+    }
+  }
+}
+
+typedef struct {
+  orc_factor* f;
+  const sn_sym* S;
+  double* panel;
+  double* scratch; /* per thread: t [maxm], ucol [4 maxm], pos [maxm] (as int64) */
+  int64_t cutoff;  /* subtrees with at most this many columns run as one task */
+} sn_run_t;
+
+static void sn_run_node(const sn_run_t* ctx, int64_t s) {
+#ifdef _OPENMP
+  const int64_t tid = omp_get_thread_num();
+#else
+  const int64_t tid = 0;
+#endif
+  double* base = ctx->scratch + tid * 6 * ctx->S->maxm;
+  sn_node(ctx->f, ctx->S, ctx->panel, s, base, base + ctx->S->maxm, (int64_t*)(base + 5 * ctx->S->maxm),
+          ctx->scratch);
+}
+
+/* The subtree of s: its children's subtrees as tasks when it is large, else every supernode of
+ * the subtree in index order (postorder: its supernodes are the contiguous range ending at s),
+ * then s. A thread's scratch (t, accumulators, row map) serves one node at a time: a node
+ * reaches a task scheduling point only inside a split update, which by then needs only the
+ * accumulators of whichever thread runs each block, and the node's own row map is allocated. */
+static void sn_run_subtree(const sn_run_t* ctx, int64_t s) {
+  const sn_sym* S = ctx->S;
+  if (S->subcols[s] > ctx->cutoff) {
+    for (int64_t k = S->chp[s]; k < S->chp[s + 1]; ++k) {
+      const int64_t c = S->chl[k];
+#pragma omp task firstprivate(c)
+      sn_run_subtree(ctx, c);
+    }
+#pragma omp taskwait
+  } else {
+    const int64_t first = S->sn_of[S->sfirst[s + 1] - S->subcols[s]];
+    for (int64_t k = first; k < s; ++k) sn_run_node(ctx, k);
+  }
+  sn_run_node(ctx, s);
+}
+
+/* All supernodes: in index order on one thread, or as a task tree over orc_set_threads threads
+ * (the same factor bit for bit either way). */
+static void sn_factor_all(orc_factor* f, const sn_sym* S, double* panel) {
+  const int nt = g_sn_threads;
+  sn_run_t ctx;
+  ctx.f = f;
+  ctx.S = S;
+  ctx.panel = panel;
+  ctx.scratch = (double*)malloc(sizeof(double) * 6 * S->maxm * (size_t)nt);
+  ctx.cutoff = MAXI((int64_t)256, S->n / (16 * (int64_t)nt));
+  if (nt <= 1) {
+    for (int64_t s = 0; s < S->ns; ++s) sn_run_node(&ctx, s);
+  } else {
+#pragma omp parallel num_threads(nt)
+#pragma omp single
+    for (int64_t s = 0; s < S->ns; ++s)
+      if (S->sparent[s] < 0) {
+#pragma omp task firstprivate(s)
+        sn_run_subtree(&ctx, s);
+      }
+  }
+  free(ctx.scratch);
+}
+
 int orc_factor_create_sn(int64_t n, const int64_t* cp, const int64_t* ri, const double* vals, const int64_t* perm,
                          orc_factor** out) {
   sn_sym* S = sn_acquire(n, cp, ri, perm);
@@ -894,13 +1046,7 @@ int orc_factor_create_sn(int64_t n, const int64_t* cp, const int64_t* ri, const 
   double* panel = (double*)calloc(S->npanel + 1, sizeof(double));
   for (int64_t p = 0; p < cp[n]; ++p)
     if (S->vmap[p] >= 0) panel[S->vmap[p]] += vals[p];
-  double* t = (double*)malloc(sizeof(double) * S->maxm);
-  double* ucol = (double*)malloc(sizeof(double) * 4 * S->maxm * (size_t)g_sn_threads);
-  int64_t* pos = (int64_t*)malloc(sizeof(int64_t) * S->maxm);
-  sn_numeric(f, S->ns, S->sfirst, S->sn_of, S->sptr, S->srows, S->poff, panel, t, ucol, pos);
-  free(t);
-  free(ucol);
-  free(pos);
+  sn_factor_all(f, S, panel);
   free(panel);
   *out = f;
   for (int64_t k = 0; k < n; ++k)

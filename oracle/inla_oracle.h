@@ -36,7 +36,7 @@ typedef struct orc_factor orc_factor;
  * non-finite (sparse_ldlt.rs:117-120). Only entries with row >= col are read. */
 int orc_factor_create(int64_t n, const int64_t* cp, const int64_t* ri, const double* vals, const int64_t* perm,
                       orc_factor** out);
-/* The same factor by a supernodal LDL^T (dense panels, right-looking Schur updates), equal to
+/* The same factor by a supernodal LDL^T (dense panels, left-looking over the supernodal tree), equal to
  * orc_factor_create's to rounding; the CPU baseline's factorization. */
 int orc_factor_create_sn(int64_t n, const int64_t* cp, const int64_t* ri, const double* vals, const int64_t* perm,
                          orc_factor** out);

@@ -328,8 +328,10 @@ def test_supernodal_laplace_equals_simplicial():
 
 
 def test_supernodal_threads_inside_one_factorization_give_the_same_bits():
-    """orc_set_threads splits a large supernode's update over threads by target column, so every
-    entry is accumulated in the same order: the factor is bit-identical for any thread count."""
+    """orc_set_threads runs independent subtrees as tasks and splits large updates by target
+    column; every entry still receives its updates in the same order, so the factor is
+    bit-identical for any thread count (minimum-degree order: a bushy tree; natural order: a band
+    of ~100 with large updates)."""
     import inla_b200.models as M
 
     p = M.make_spde_problem(nx=100, n_obs=5000)
@@ -337,11 +339,13 @@ def test_supernodal_threads_inside_one_factorization_give_the_same_bits():
     q = (p.model.matrix(c) + 25.0 * (p.a.T @ p.a)).tocsc()
     q.sort_indices()
     x = np.linspace(-1.0, 1.0, q.shape[0])
-    base = O.Factor(q, supernodal=True)  # the natural order: a band of ~100, updates above the split size
-    try:
-        O.set_threads(4)
-        f = O.Factor(q, supernodal=True)
-    finally:
-        O.set_threads(1)
-    assert f.logdet() == base.logdet()
-    assert np.array_equal(f.solve(x), base.solve(x))
+    for perm in (O.reference_perm(p.model.pattern), None):
+        base = O.Factor(q, perm=perm, supernodal=True)
+        for t in (2, 4, 8):
+            try:
+                O.set_threads(t)
+                f = O.Factor(q, perm=perm, supernodal=True)
+            finally:
+                O.set_threads(1)
+            assert f.logdet() == base.logdet()
+            assert np.array_equal(f.solve(x), base.solve(x))
