@@ -349,3 +349,25 @@ def test_supernodal_threads_inside_one_factorization_give_the_same_bits():
                 O.set_threads(1)
             assert f.logdet() == base.logdet()
             assert np.array_equal(f.solve(x), base.solve(x))
+
+
+def test_oracle_against_superlu_at_a_realistic_size():
+    """An independent pin at n = 10 000 (SPDE 100 x 100 posterior): SuperLU's log|det| (sum of
+    log|U_ii|) and solve against both factorizations of the oracle."""
+    import scipy.sparse.linalg as spla
+
+    import inla_b200.models as M
+
+    p = M.make_spde_problem(nx=100, n_obs=5000)
+    c, _ = M.spde_coefs(-2.0, 2.0)
+    q = (p.model.matrix(c) + 50.0 * (p.a.T @ p.a)).tocsc()
+    q.sort_indices()
+    lu = spla.splu(q, permc_spec="COLAMD")
+    ld_ref = float(np.sum(np.log(np.abs(lu.U.diagonal()))))
+    b = np.cos(np.arange(q.shape[0]))
+    x_ref = lu.solve(b)
+    perm = O.reference_perm(p.model.pattern)
+    for sn in (False, True):
+        f = O.Factor(q, perm=perm, supernodal=sn)
+        assert abs(f.logdet() - ld_ref) <= 1e-10 * abs(ld_ref)
+        np.testing.assert_allclose(f.solve(b), x_ref, rtol=1e-9, atol=1e-12 * np.max(np.abs(x_ref)))
