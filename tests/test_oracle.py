@@ -353,7 +353,8 @@ def test_supernodal_threads_inside_one_factorization_give_the_same_bits():
 
 def test_oracle_against_superlu_at_a_realistic_size():
     """An independent pin at n = 10 000 (SPDE 100 x 100 posterior): SuperLU's log|det| (sum of
-    log|U_ii|) and solve against both factorizations of the oracle."""
+    log|U_ii|) and solve against both factorizations of the oracle, and 16 marginal variances
+    (Q^-1)_ii from SuperLU solves against the oracle's Takahashi diagonal."""
     import scipy.sparse.linalg as spla
 
     import inla_b200.models as M
@@ -367,7 +368,11 @@ def test_oracle_against_superlu_at_a_realistic_size():
     b = np.cos(np.arange(q.shape[0]))
     x_ref = lu.solve(b)
     perm = O.reference_perm(p.model.pattern)
+    idx = np.random.default_rng(3).choice(q.shape[0], 16, replace=False)
+    var_ref = np.array([lu.solve(np.eye(1, q.shape[0], i).ravel())[i] for i in idx])  # (Q^-1 e_i)_i
     for sn in (False, True):
         f = O.Factor(q, perm=perm, supernodal=sn)
         assert abs(f.logdet() - ld_ref) <= 1e-10 * abs(ld_ref)
         np.testing.assert_allclose(f.solve(b), x_ref, rtol=1e-9, atol=1e-12 * np.max(np.abs(x_ref)))
+    # the reference's Takahashi recurrence (sparse_ldlt.rs:376-432) on the simplicial factor
+    np.testing.assert_allclose(O.Factor(q, perm=perm).diag_inv()[idx], var_ref, rtol=1e-9)
