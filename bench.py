@@ -577,7 +577,14 @@ def run_ours(args, ws, rank, local, dist):
                          f"Nelder-Mead / FD-Hessian evaluation of the reference's fit) at CCD-like theta-points "
                          f"in {el:.1f}s, {threads} threads, minimum-degree order; {CPU_KIND_NOTE}"}
 
-    others = run_other_configs() if (ws == 1 and not args.no_other_configs) else None
+    others = None
+    if ws == 1 and not args.no_other_configs:
+        # the child's models need the device memory this process still holds: free the benchmark
+        # model and hand the library's and torch's cached blocks back to the driver first
+        lm.close()
+        lib().inla_release_cached_memory()
+        torch.cuda.empty_cache()
+        others = run_other_configs()
 
     fit_s = ms_total * 1e-3 / args.steps
     # where one fit's time goes (host wall clock per phase, averaged over the timed fits)
