@@ -1276,32 +1276,50 @@ typedef struct {
   int64_t r, c;
   double v;
 } trip_t;
-static int cmp_trip(const void* a, const void* b) {
-  const trip_t *x = (const trip_t*)a, *y = (const trip_t*)b;
-  if (x->c != y->c) return x->c < y->c ? -1 : 1;
-  if (x->r != y->r) return x->r < y->r ? -1 : 1;
-  return 0;
-}
 
-/* triplets -> CSC, duplicates summed */
+/* triplets -> CSC, rows ascending in each column, duplicates summed in insertion order */
 static void csc_from_trips(int64_t n, trip_t* t, int64_t nt, csc_t* out) {
-  qsort(t, (size_t)nt, sizeof(trip_t), cmp_trip);
+  /* stable counting sort by column, then rows ascending within each column (insertion sort:
+   * equal entries keep their insertion order), duplicates summed in that order */
+  int64_t* cnt = (int64_t*)calloc(n + 1, sizeof(int64_t));
+  for (int64_t i = 0; i < nt; ++i) cnt[t[i].c + 1]++;
+  for (int64_t c = 0; c < n; ++c) cnt[c + 1] += cnt[c];
+  trip_t* u = (trip_t*)malloc(sizeof(trip_t) * (nt + 1));
+  int64_t* nx = (int64_t*)malloc(sizeof(int64_t) * (n + 1));
+  memcpy(nx, cnt, sizeof(int64_t) * (n + 1));
+  for (int64_t i = 0; i < nt; ++i) u[nx[t[i].c]++] = t[i];
   out->n = n;
   out->cp = (int64_t*)calloc(n + 1, sizeof(int64_t));
   out->ri = (int64_t*)malloc(sizeof(int64_t) * (nt + 1));
   out->v = (double*)malloc(sizeof(double) * (nt + 1));
   int64_t q = 0;
-  for (int64_t i = 0; i < nt; ++i) {
-    if (i > 0 && t[i].c == t[i - 1].c && t[i].r == t[i - 1].r) {
-      out->v[q - 1] += t[i].v;
-      continue;
+  for (int64_t c = 0; c < n; ++c) {
+    trip_t* col = u + cnt[c];
+    const int64_t len = cnt[c + 1] - cnt[c];
+    for (int64_t i = 1; i < len; ++i) {
+      const trip_t x = col[i];
+      int64_t j = i;
+      while (j > 0 && col[j - 1].r > x.r) {
+        col[j] = col[j - 1];
+        --j;
+      }
+      col[j] = x;
     }
-    out->ri[q] = t[i].r;
-    out->v[q] = t[i].v;
-    out->cp[t[i].c + 1]++;
-    ++q;
+    for (int64_t i = 0; i < len; ++i) {
+      if (i > 0 && col[i].r == col[i - 1].r) {
+        out->v[q - 1] += col[i].v;
+        continue;
+      }
+      out->ri[q] = col[i].r;
+      out->v[q] = col[i].v;
+      out->cp[c + 1]++;
+      ++q;
+    }
   }
   for (int64_t c = 0; c < n; ++c) out->cp[c + 1] += out->cp[c];
+  free(cnt);
+  free(u);
+  free(nx);
 }
 
 /* design.rs:94-120 + 123-139 + ldlt.rs:373-453: Q_post = Q + A^T diag(d) A */
